@@ -1,0 +1,784 @@
+/*
+ * bx_oracle.cpp -- TEST INFRASTRUCTURE ONLY (parity oracle, CPU baseline).
+ *
+ * A C++ restatement of the BATS-R-US "orig" CPU path for the explicit
+ * block-adaptive ideal-MHD update (single fluid, nVar = 8, no B0).  Every
+ * routine cites the Fortran it follows; the arithmetic keeps the Fortran
+ * operation order (the file is compiled with -ffp-contract=off) so that the
+ * CUDA kernels can be checked against it to ~1e-15 relative.
+ *
+ * Nothing in the product (batsrus_b200/, include/) links or calls this file.
+ */
+#include "bx_oracle.h"
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <tuple>
+#include <vector>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+namespace {
+
+// srcEquation/ModEquationMhd.f90:20-35 (0-based here)
+enum { Rho_ = 0, RhoUx_ = 1, RhoUy_ = 2, RhoUz_ = 3, Bx_ = 4, By_ = 5,
+       Bz_ = 6, P_ = 7, nVar = 8, Energy_ = 8, nFlux = 9 };
+// flux slots kept per face: nFlux fluxes, Vdt_, Un (src/ModAdvance.f90:47-59)
+enum { Vdt_ = 9, Un_ = 10, nFaceValue = 11 };
+
+// share/Library ModNumConst::cTiny (library absent from the tree; the
+// published SWMF value 1e-6 is assumed, used only by the HLLD guards)
+const double cTiny = 1.0e-6;
+
+inline double sign25(double x) { return std::copysign(0.25, x); }
+inline double min3(double a, double b, double c) { return std::min(std::min(a, b), c); }
+
+struct Scratch {
+  std::vector<double> Prim;              // Primitive_VGI
+  std::vector<double> Left[3], Right[3]; // LeftState_VX/VY/VZ ...
+  std::vector<double> Flux[3];           // Flux_VXI/VYI/VZI
+  std::vector<double> Source;            // Source_VC (nVar+1)
+  std::vector<double> DivB1;             // DivB1_GB interior
+  int err = 0;
+};
+
+struct Oracle {
+  ora_config c;
+  int nBlock;
+  int nG = 2;
+  int MinI, MaxI, MinJ, MaxJ, MinK, MaxK, nIg, nJg, nKg;
+  long nCellG;  // cells per block with ghosts
+  std::vector<int> lev, ic;  // level, integer coords (3 per block)
+  std::vector<double> xyzMinB, dxyz;  // block corner, cell size (3 per block)
+  std::vector<double> State, StateOld;
+  std::vector<double> DtMax_CB, DtMax_B;
+  std::map<std::tuple<int, int, int, int>, int> node;
+  std::vector<Scratch> scr;
+  double InvGammaMinus1, GammaMinus1;
+  double tSimulation = 0, Dt = 0;
+  int nStep = 0, iStage = 1;
+  int nFace[3][3];  // face array extents per direction
+
+  long cell(int i, int j, int k) const {
+    return (i - MinI) + (long)nIg * ((j - MinJ) + (long)nJg * (k - MinK));
+  }
+  double *st(int b, int i, int j, int k) { return &State[nVar * (cell(i, j, k) + nCellG * b)]; }
+  double *so(int b, int i, int j, int k) { return &StateOld[nVar * (cell(i, j, k) + nCellG * b)]; }
+  long face(int d, int i, int j, int k) const {  // i,j,k 1-based face/cell indexes
+    return (i - 1) + (long)nFace[d][0] * ((j - 1) + (long)nFace[d][1] * (k - 1));
+  }
+  long icell(int i, int j, int k) const {
+    return (i - 1) + (long)c.nI * ((j - 1) + (long)c.nJ * (k - 1));
+  }
+  double cellVolume(int b) const { return dxyz[3 * b] * dxyz[3 * b + 1] * dxyz[3 * b + 2]; }
+  double cellFace(int b, int d) const {
+    // BATL (srcBATL, absent from the tree) sets CellFace_DB = CellVolume_B/CellSize_DB
+    return cellVolume(b) / dxyz[3 * b + d];
+  }
+
+  void init(const ora_config *cfg, int nb, const int *lc) {
+    c = *cfg;
+    nBlock = nb;
+    MinI = 1 - nG; MaxI = c.nI + nG;
+    MinJ = c.nDim > 1 ? 1 - nG : 1; MaxJ = c.nDim > 1 ? c.nJ + nG : 1;
+    MinK = c.nDim > 2 ? 1 - nG : 1; MaxK = c.nDim > 2 ? c.nK + nG : 1;
+    nIg = MaxI - MinI + 1; nJg = MaxJ - MinJ + 1; nKg = MaxK - MinK + 1;
+    nCellG = (long)nIg * nJg * nKg;
+    State.assign(nVar * nCellG * nBlock, 0.0);
+    StateOld = State;
+    DtMax_CB.assign((long)c.nI * c.nJ * c.nK * nBlock, 0.0);
+    DtMax_B.assign(nBlock, 0.0);
+    lev.resize(nBlock); ic.resize(3 * nBlock);
+    xyzMinB.resize(3 * nBlock); dxyz.resize(3 * nBlock);
+    int nCell[3] = {c.nI, c.nJ, c.nK};
+    for (int b = 0; b < nBlock; b++) {
+      lev[b] = lc[4 * b];
+      for (int d = 0; d < 3; d++) ic[3 * b + d] = lc[4 * b + 1 + d];
+      node[std::make_tuple(lev[b], ic[3 * b], ic[3 * b + 1], ic[3 * b + 2])] = b;
+      for (int d = 0; d < 3; d++) {
+        double ext = c.xyzMax[d] - c.xyzMin[d];
+        if (d < c.nDim) {
+          double nb_d = (double)c.nRoot[d] * (double)(1 << lev[b]);
+          double bsize = ext / nb_d;
+          xyzMinB[3 * b + d] = c.xyzMin[d] + ic[3 * b + d] * bsize;
+          dxyz[3 * b + d] = bsize / nCell[d];
+        } else {
+          // BATL: the ignored dimensions span the whole domain
+          xyzMinB[3 * b + d] = c.xyzMin[d];
+          dxyz[3 * b + d] = ext;
+        }
+      }
+    }
+    nFace[0][0] = c.nI + 1; nFace[0][1] = c.nJ; nFace[0][2] = c.nK;
+    nFace[1][0] = c.nI; nFace[1][1] = c.nJ + 1; nFace[1][2] = c.nK;
+    nFace[2][0] = c.nI; nFace[2][1] = c.nJ; nFace[2][2] = c.nK + 1;
+    GammaMinus1 = c.gamma - 1.0;
+    InvGammaMinus1 = 1.0 / GammaMinus1;
+    int nThr = 1;
+#ifdef _OPENMP
+    nThr = c.nThread > 0 ? c.nThread : omp_get_max_threads();
+#endif
+    scr.resize(nThr);
+    for (auto &s : scr) {
+      s.Prim.assign(nVar * nCellG, 0.0);
+      for (int d = 0; d < 3; d++) {
+        long nf = (long)nFace[d][0] * nFace[d][1] * nFace[d][2];
+        s.Left[d].assign(nVar * nf, 0.0);
+        s.Right[d].assign(nVar * nf, 0.0);
+        s.Flux[d].assign(nFaceValue * nf, 0.0);
+      }
+      s.Source.assign((nVar + 1) * (long)c.nI * c.nJ * c.nK, 0.0);
+      s.DivB1.assign((long)c.nI * c.nJ * c.nK, 0.0);
+    }
+  }
+
+  // ------------------------------------------------------------------
+  // exchange_messages (src/ModMessagePass.f90:27-291) for a single-level
+  // grid: same-level copies through the BATL neighbour relation, periodic
+  // wrap, and the float outer boundary (src/ModCellBoundary.f90:518-559).
+  int find_block(int L, int x, int y, int z) const {
+    auto it = node.find(std::make_tuple(L, x, y, z));
+    return it == node.end() ? -1 : it->second;
+  }
+  void exchange_messages() {
+    int nCell[3] = {c.nI, c.nJ, c.nK};
+#pragma omp parallel for schedule(static) num_threads((int)scr.size())
+    for (int b = 0; b < nBlock; b++) {
+      for (int k = MinK; k <= MaxK; k++)
+        for (int j = MinJ; j <= MaxJ; j++)
+          for (int i = MinI; i <= MaxI; i++) {
+            int idx[3] = {i, j, k};
+            bool ghost = false;
+            for (int d = 0; d < c.nDim; d++)
+              if (idx[d] < 1 || idx[d] > nCell[d]) ghost = true;
+            if (!ghost) continue;
+            // source cell: walk to the neighbour block at the same level
+            int L = lev[b];
+            int bc[3] = {ic[3 * b], ic[3 * b + 1], ic[3 * b + 2]};
+            int src[3] = {i, j, k};
+            int srcBlock = b;
+            bool useSelf = false;
+            int selfIdx[3] = {i, j, k};
+            for (int d = 0; d < c.nDim; d++) {
+              int nbl = c.nRoot[d] << L;
+              if (idx[d] < 1 || idx[d] > nCell[d]) {
+                int off = idx[d] < 1 ? -1 : 1;
+                int nb = bc[d] + off;
+                if (nb < 0 || nb >= nbl) {
+                  int side = 2 * d + (off > 0 ? 1 : 0);
+                  if (c.typeBc[side] == ORA_BC_PERIODIC) {
+                    nb = (nb + nbl) % nbl;
+                  } else {
+                    // float: copy the boundary cell of this block
+                    useSelf = true;
+                    selfIdx[d] = off < 0 ? 1 : nCell[d];
+                    continue;
+                  }
+                }
+                bc[d] = nb;
+                src[d] = idx[d] - off * nCell[d];
+                selfIdx[d] = src[d];
+              }
+            }
+            if (useSelf) {
+              // float BC applied on top of any same-level shift: use the
+              // cell of the neighbour chain that is clamped to the boundary
+              srcBlock = find_block(L, bc[0], bc[1], bc[2]);
+              if (srcBlock < 0) srcBlock = b;
+              for (int d = 0; d < 3; d++) src[d] = selfIdx[d];
+            } else {
+              srcBlock = find_block(L, bc[0], bc[1], bc[2]);
+              if (srcBlock < 0) continue;  // not a single-level neighbour
+            }
+            const double *s = st(srcBlock, src[0], src[1], src[2]);
+            double *t = st(b, i, j, k);
+            for (int v = 0; v < nVar; v++) t[v] = s[v];
+          }
+    }
+  }
+
+  // ------------------------------------------------------------------
+  // calc_primitives (src/ModFaceValue.f90:1530-1621): u = (1/rho)*rhoU
+  void calc_primitives(int b, Scratch &s) {
+    for (int k = MinK; k <= MaxK; k++)
+      for (int j = MinJ; j <= MaxJ; j++)
+        for (int i = MinI; i <= MaxI; i++) {
+          const double *u = st(b, i, j, k);
+          double *p = &s.Prim[nVar * cell(i, j, k)];
+          for (int v = 0; v < nVar; v++) p[v] = u[v];
+          double RhoInv = 1 / p[Rho_];
+          p[RhoUx_] = RhoInv * p[RhoUx_];
+          p[RhoUy_] = RhoInv * p[RhoUy_];
+          p[RhoUz_] = RhoInv * p[RhoUz_];
+        }
+  }
+
+  // limiter (src/ModFaceValue.f90:3689-3791): slopes for a pencil of
+  // primitive values q[l], l = lMin-1 .. lMax (+1 neighbours available)
+  void limiter_pencil(const double *q /* q[l] for l=-1..n+2 via offset */,
+                      int lMin, int lMax, double *dL, double *dR) const {
+    const double Beta = c.limiterBeta;
+    const double cThird = 1. / 3.;
+    for (int l = lMin - 1; l <= lMax; l++) {
+      double d1 = q[l] - q[l - 1];   // left slope dVar1
+      double d2 = q[l + 1] - q[l];   // right slope dVar2
+      double sg = sign25(d1) + sign25(d2);
+      switch (c.typeLimiter) {
+        case ORA_LIM_MINMOD:
+          dR[l] = sg * std::min(std::fabs(d1), std::fabs(d2));
+          dL[l] = dR[l];
+          break;
+        case ORA_LIM_MC:
+          dR[l] = sg * min3(Beta * std::fabs(d1), Beta * std::fabs(d2),
+                            0.5 * std::fabs(d1 + d2));
+          dL[l] = dR[l];
+          break;
+        default:  // mc3 (Koren)
+          dR[l] = sg * min3(Beta * std::fabs(d1), Beta * std::fabs(d2),
+                            cThird * std::fabs(2 * d1 + d2));
+          dL[l] = sg * min3(Beta * std::fabs(d1), Beta * std::fabs(d2),
+                            cThird * std::fabs(d1 + 2 * d2));
+      }
+    }
+  }
+
+  // calc_face_value (src/ModFaceValue.f90:854) with get_facex/y/z_first and
+  // get_facex/y/z_second (:1970-2163) on a single-level block
+  void calc_face_value(int b, Scratch &s) {
+    calc_primitives(b, s);
+    int nCell[3] = {c.nI, c.nJ, c.nK};
+    int nMax = std::max(c.nI, std::max(c.nJ, c.nK));
+    std::vector<double> qbuf(nMax + 6), dLb(nMax + 6), dRb(nMax + 6);
+    double *q = qbuf.data() + 2, *dL = dLb.data() + 2, *dR = dRb.data() + 2;
+    for (int d = 0; d < c.nDim; d++) {
+      int n = nCell[d];
+      // loop over the pencils perpendicular to d
+      int a1 = (d == 0) ? 1 : 0, a2 = (d == 2) ? 1 : 2;  // other two dims
+      for (int p2 = 1; p2 <= nCell[a2]; p2++)
+        for (int p1 = 1; p1 <= nCell[a1]; p1++)
+          for (int v = 0; v < nVar; v++) {
+            for (int l = -1; l <= n + 2; l++) {
+              int idx[3];
+              idx[d] = l; idx[a1] = p1; idx[a2] = p2;
+              q[l] = s.Prim[nVar * cell(idx[0], idx[1], idx[2]) + v];
+            }
+            if (c.nOrder == 2) limiter_pencil(q, 1, n + 1, dL, dR);
+            for (int f = 1; f <= n + 1; f++) {
+              int idx[3];
+              idx[d] = f; idx[a1] = p1; idx[a2] = p2;
+              long fi = face(d, idx[0], idx[1], idx[2]);
+              if (c.nOrder == 1) {
+                s.Left[d][nVar * fi + v] = q[f - 1];
+                s.Right[d][nVar * fi + v] = q[f];
+              } else {
+                s.Left[d][nVar * fi + v] = q[f - 1] + dL[f - 1];
+                s.Right[d][nVar * fi + v] = q[f] - dR[f];
+              }
+            }
+          }
+    }
+  }
+
+  // ------------------------------------------------------------------
+  // get_physical_flux -> get_mhd_flux -> get_magnetic_flux
+  // (src/ModFaceFlux.f90:1166-1410, 1550-1617, 1619-1900), B0 = 0
+  void physical_flux(const double *S, int d, double *Cons, double *F, double &Un) const {
+    const double Rho = S[Rho_], Ux = S[RhoUx_], Uy = S[RhoUy_], Uz = S[RhoUz_];
+    const double Bx = S[Bx_], By = S[By_], Bz = S[Bz_], p = S[P_];
+    const double U[3] = {Ux, Uy, Uz}, B[3] = {Bx, By, Bz};
+    const double Bn = B[d];
+    for (int v = 0; v < nVar; v++) Cons[v] = S[v];
+    Un = U[d];
+    F[Rho_] = Rho * Un;
+    Cons[RhoUx_] = Rho * Ux; Cons[RhoUy_] = Rho * Uy; Cons[RhoUz_] = Rho * Uz;
+    double pn[3] = {0, 0, 0}; pn[d] = p;
+    F[RhoUx_] = Un * Rho * Ux + pn[0];
+    F[RhoUy_] = Un * Rho * Uy + pn[1];
+    F[RhoUz_] = Un * Rho * Uz + pn[2];
+    double e = InvGammaMinus1 * p + 0.5 * Rho * (Ux * Ux + Uy * Uy + Uz * Uz);
+    F[Energy_] = Un * (e + p);
+    F[P_] = Un * p;
+    double B2 = Bx * Bx + By * By + Bz * Bz;
+    double pTotal = 0.5 * B2;
+    double ptn[3] = {0, 0, 0}; ptn[d] = pTotal;
+    // MagneticForce_D = -Bn*FullB + pTotal*Normal
+    double MF[3] = {-Bn * Bx + ptn[0], -Bn * By + ptn[1], -Bn * Bz + ptn[2]};
+    // get_magnetic_flux: UnPlus*FullB - UPlus*FullBn
+    F[Bx_] = Un * Bx - Ux * Bn;
+    F[By_] = Un * By - Uy * Bn;
+    F[Bz_] = Un * Bz - Uz * Bn;
+    F[RhoUx_] = F[RhoUx_] + MF[0];
+    F[RhoUy_] = F[RhoUy_] + MF[1];
+    F[RhoUz_] = F[RhoUz_] + MF[2];
+    Cons[Energy_] = e + 0.5 * B2;
+    F[Energy_] = F[Energy_] + F[Bx_] * Bx + F[By_] * By + F[Bz_] * Bz;
+  }
+
+  // get_speed_max -> get_mhd_speed (src/ModFaceFlux.f90:3545-4250)
+  void speed(const double *S, int d, double &Cmax, double &Cleft, double &Cright) const {
+    const double Rho = S[Rho_];
+    double Sound2 = S[P_] * c.gamma / Rho;
+    double Un = S[RhoUx_ + d];
+    double InvRho = 1.0 / Rho;
+    double Bx = S[Bx_], By = S[By_], Bz = S[Bz_];
+    double Alfven2 = (Bx * Bx + By * By + Bz * Bz) * InvRho;
+    double FullBn = S[Bx_ + d];
+    double Alfven2Normal = InvRho * (FullBn * FullBn);
+    double Fast2 = Sound2 + Alfven2;
+    double Discr = std::sqrt(std::max(0.0, Fast2 * Fast2 - 4 * Sound2 * Alfven2Normal));
+    double Fast = std::sqrt(0.5 * (Fast2 + Discr));
+    Cmax = std::fabs(Un) + Fast;
+    Cleft = Un - Fast;
+    Cright = Un + Fast;
+  }
+
+  // hlld_flux (src/ModFaceFlux.f90:2826-3160) with rotate_state_vectors /
+  // rotate_flux_vector (:4482-4645) for Cartesian faces and B0 = 0.
+  // Returns nonzero where the reference aborts (negative density ratio).
+  int hlld(const double *L, const double *R, int d, double *Flux, double &Cmax, double &UnOut) const {
+    double cmL, clL, crL, cmR, clR, crR;
+    speed(L, d, cmL, clL, crL);
+    speed(R, d, cmR, clR, crR);
+    double sL = std::min(clL, clR);
+    double sR = std::max(crL, crR);
+    Cmax = std::max(sR, -sL);
+    double Cons[nFlux];
+    if (sL >= 0.) { physical_flux(L, d, Cons, Flux, UnOut); return 0; }
+    if (sR <= 0.) { physical_flux(R, d, Cons, Flux, UnOut); return 0; }
+    const int n = d, t1 = (d + 1) % 3, t2 = (d + 2) % 3;
+    double RhoL = L[Rho_], pL = L[P_], RhoR = R[Rho_], pR = R[P_];
+    double UnL = L[RhoUx_ + n], Ut1L = L[RhoUx_ + t1], Ut2L = L[RhoUx_ + t2];
+    double B1nL = L[Bx_ + n], B1t1L = L[Bx_ + t1], B1t2L = L[Bx_ + t2];
+    double UnR = R[RhoUx_ + n], Ut1R = R[RhoUx_ + t1], Ut2R = R[RhoUx_ + t2];
+    double B1nR = R[Bx_ + n], B1t1R = R[Bx_ + t1], B1t2R = R[Bx_ + t2];
+    double B1n = 0.5 * (B1nL + B1nR);
+    double B1n2 = B1n * B1n;
+    double Bn = B1n, Bt1L = B1t1L, Bt2L = B1t2L, Bt1R = B1t1R, Bt2R = B1t2R;
+    double Bn2 = Bn * Bn;
+    double SignBn = std::copysign(1., Bn);
+    double PbL = 0.5 * (B1n2 + B1t1L * B1t1L + B1t2L * B1t2L);
+    double PbR = 0.5 * (B1n2 + B1t1R * B1t1R + B1t2R * B1t2R);
+    double PtotL = pL + PbL;
+    double PtotR = pR + PbR;
+    double DsL = sL - UnL, DsR = sR - UnR;
+    double DsRhoL = DsL * RhoL, DsRhoR = DsR * RhoR;
+    double Tmp = 1. / (DsRhoR - DsRhoL);
+    double Un = (DsRhoR * UnR - DsRhoL * UnL - PtotR + PtotL) * Tmp;
+    double Ptot12 = (DsRhoR * PtotL - DsRhoL * PtotR + DsRhoR * DsRhoL * (UnR - UnL)) * Tmp;
+    double Rho, Ut1, Ut2, B1t1, B1t2, uDotB1, e;
+    double Ut1L1, Ut2L1, B1t1L1, B1t2L1, Ut1R1, Ut2R1, B1t1R1, B1t2R1;
+    if (Un >= 0.) {
+      double InvSLUn = 1.0 / (sL - Un);
+      Rho = DsRhoL * InvSLUn;
+      Tmp = DsRhoL * (sL - Un) - Bn2;
+      if (Tmp < cTiny) {
+        Ut1L1 = Ut1L; Ut2L1 = Ut2L; B1t1L1 = B1t1L; B1t2L1 = B1t2L;
+      } else {
+        Tmp = 1.0 / Tmp;
+        Ut1L1 = Ut1L - Bn * Bt1L * (Un - UnL) * Tmp;
+        Ut2L1 = Ut2L - Bn * Bt2L * (Un - UnL) * Tmp;
+        B1t1L1 = Bt1L * (DsRhoL * DsL - Bn2) * Tmp;
+        B1t2L1 = Bt2L * (DsRhoL * DsL - Bn2) * Tmp;
+      }
+      double eL = InvGammaMinus1 * pL + PbL + 0.5 * RhoL * (UnL * UnL + Ut1L * Ut1L + Ut2L * Ut2L);
+      double uDotB1L = UnL * B1n + Ut1L * B1t1L + Ut2L * B1t2L;
+      double uDotB1L1 = Un * B1n + Ut1L1 * B1t1L1 + Ut2L1 * B1t2L1;
+      e = (DsL * eL - PtotL * UnL + Ptot12 * Un + Bn * (uDotB1L - uDotB1L1)) * InvSLUn;
+      double SqRhoL1 = std::sqrt(Rho);
+      double sL1 = Un - std::fabs(Bn) / SqRhoL1;
+      if (sL1 >= 0.) {
+        Ut1 = Ut1L1; Ut2 = Ut2L1; B1t1 = B1t1L1; B1t2 = B1t2L1; uDotB1 = uDotB1L1;
+      } else {
+        if (DsRhoR / (sR - Un) < 0) return 1;
+        double SqRhoR1 = std::sqrt(DsRhoR / (sR - Un));
+        Tmp = DsRhoR * (sR - Un) - Bn2;
+        if (Tmp < cTiny) {
+          Ut1R1 = Ut1R; Ut2R1 = Ut2R; B1t1R1 = B1t1R; B1t2R1 = B1t2R;
+        } else {
+          Tmp = 1.0 / Tmp;
+          Ut1R1 = Ut1R - Bn * Bt1R * (Un - UnR) * Tmp;
+          Ut2R1 = Ut2R - Bn * Bt2R * (Un - UnR) * Tmp;
+          B1t1R1 = Bt1R * (DsRhoR * DsR - Bn2) * Tmp;
+          B1t2R1 = Bt2R * (DsRhoR * DsR - Bn2) * Tmp;
+        }
+        Tmp = 1. / (SqRhoL1 + SqRhoR1);
+        double SqRhoLR1 = SqRhoL1 * SqRhoR1 * SignBn;
+        Ut1 = (SqRhoL1 * Ut1L1 + SqRhoR1 * Ut1R1 + (B1t1R1 - B1t1L1) * SignBn) * Tmp;
+        Ut2 = (SqRhoL1 * Ut2L1 + SqRhoR1 * Ut2R1 + (B1t2R1 - B1t2L1) * SignBn) * Tmp;
+        B1t1 = (SqRhoL1 * B1t1R1 + SqRhoR1 * B1t1L1 + (Ut1R1 - Ut1L1) * SqRhoLR1) * Tmp;
+        B1t2 = (SqRhoL1 * B1t2R1 + SqRhoR1 * B1t2L1 + (Ut2R1 - Ut2L1) * SqRhoLR1) * Tmp;
+        uDotB1 = Un * B1n + Ut1 * B1t1 + Ut2 * B1t2;
+        e = e - SqRhoL1 * (uDotB1L1 - uDotB1) * SignBn;
+      }
+    } else {
+      double InvSRUn = 1.0 / (sR - Un);
+      Rho = DsRhoR * InvSRUn;
+      Tmp = DsRhoR * (sR - Un) - Bn2;
+      if (Tmp < cTiny) {
+        Ut1R1 = Ut1R; Ut2R1 = Ut2R; B1t1R1 = B1t1R; B1t2R1 = B1t2R;
+      } else {
+        Tmp = 1.0 / Tmp;
+        Ut1R1 = Ut1R - Bn * Bt1R * (Un - UnR) * Tmp;
+        Ut2R1 = Ut2R - Bn * Bt2R * (Un - UnR) * Tmp;
+        B1t1R1 = Bt1R * (DsRhoR * DsR - Bn2) * Tmp;
+        B1t2R1 = Bt2R * (DsRhoR * DsR - Bn2) * Tmp;
+      }
+      double eR = InvGammaMinus1 * pR + PbR + 0.5 * RhoR * (UnR * UnR + Ut1R * Ut1R + Ut2R * Ut2R);
+      double uDotB1R = UnR * B1n + Ut1R * B1t1R + Ut2R * B1t2R;
+      double uDotB1R1 = Un * B1n + Ut1R1 * B1t1R1 + Ut2R1 * B1t2R1;
+      e = (DsR * eR - PtotR * UnR + Ptot12 * Un + Bn * (uDotB1R - uDotB1R1)) * InvSRUn;
+      double SqRhoR1 = std::sqrt(Rho);
+      double sR1 = Un + std::fabs(Bn) / SqRhoR1;
+      if (sR1 <= 0.) {
+        Ut1 = Ut1R1; Ut2 = Ut2R1; B1t1 = B1t1R1; B1t2 = B1t2R1; uDotB1 = uDotB1R1;
+      } else {
+        if (DsRhoL / (sL - Un) < 0) return 1;
+        double SqRhoL1 = std::sqrt(DsRhoL / (sL - Un));
+        Tmp = DsRhoL * (sL - Un) - Bn2;
+        if (Tmp < cTiny) {
+          Ut1L1 = Ut1L; Ut2L1 = Ut2L; B1t1L1 = B1t1L; B1t2L1 = B1t2L;
+        } else {
+          Tmp = 1.0 / Tmp;
+          Ut1L1 = Ut1L - Bn * Bt1L * (Un - UnL) * Tmp;
+          Ut2L1 = Ut2L - Bn * Bt2L * (Un - UnL) * Tmp;
+          B1t1L1 = Bt1L * (DsRhoL * DsL - Bn2) * Tmp;
+          B1t2L1 = Bt2L * (DsRhoL * DsL - Bn2) * Tmp;
+        }
+        Tmp = 1. / (SqRhoL1 + SqRhoR1);
+        double SqRhoLR1 = SqRhoL1 * SqRhoR1 * SignBn;
+        Ut1 = (SqRhoL1 * Ut1L1 + SqRhoR1 * Ut1R1 + (B1t1R1 - B1t1L1) * SignBn) * Tmp;
+        Ut2 = (SqRhoL1 * Ut2L1 + SqRhoR1 * Ut2R1 + (B1t2R1 - B1t2L1) * SignBn) * Tmp;
+        B1t1 = (SqRhoL1 * B1t1R1 + SqRhoR1 * B1t1L1 + (Ut1R1 - Ut1L1) * SqRhoLR1) * Tmp;
+        B1t2 = (SqRhoL1 * B1t2R1 + SqRhoR1 * B1t2L1 + (Ut2R1 - Ut2L1) * SqRhoLR1) * Tmp;
+        uDotB1 = Un * B1n + Ut1 * B1t1 + Ut2 * B1t2;
+        e = e + SqRhoR1 * (uDotB1R1 - uDotB1) * SignBn;
+      }
+    }
+    double RhoUn = Rho * Un;
+    double Bt1 = B1t1, Bt2 = B1t2;
+    double FluxRot[6];  // RhoUn, RhoUt1, RhoUt2, B1n, B1t1, B1t2
+    Flux[Rho_] = RhoUn;
+    FluxRot[0] = RhoUn * Un - B1n * Bn + Ptot12;
+    FluxRot[1] = RhoUn * Ut1 - B1n * Bt1;
+    FluxRot[2] = RhoUn * Ut2 - B1n * Bt2;
+    FluxRot[3] = 0.0;
+    FluxRot[4] = Un * Bt1 - Ut1 * Bn;
+    FluxRot[5] = Un * Bt2 - Ut2 * Bn;
+    Flux[P_] = 0.5 * (sR * UnL * pL - sL * UnR * pR + sR * sL * (pR - pL)) / (sR - sL);
+    Flux[Energy_] = Un * (e + Ptot12) - Bn * uDotB1;
+    Flux[RhoUx_ + n] = FluxRot[0]; Flux[RhoUx_ + t1] = FluxRot[1]; Flux[RhoUx_ + t2] = FluxRot[2];
+    Flux[Bx_ + n] = FluxRot[3]; Flux[Bx_ + t1] = FluxRot[4]; Flux[Bx_ + t2] = FluxRot[5];
+    UnOut = Un;
+    return 0;
+  }
+
+  // get_numerical_flux (src/ModFaceFlux.f90:2130-2473) for one Cartesian
+  // face in direction d with the face Area; writes nFaceValue slots.
+  int numerical_flux(const double *Lin, const double *Rin, int d, double Area, double *Out) const {
+    double L[nVar], R[nVar], S[nVar];
+    for (int v = 0; v < nVar; v++) { L[v] = Lin[v]; R[v] = Rin[v]; }
+    const bool UseLindeFix = c.typeFlux == ORA_FLUX_LINDE || c.typeFlux == ORA_FLUX_HLLD;
+    double DiffBn_D[3] = {0, 0, 0}, DiffE = 0;
+    if (UseLindeFix) {
+      // Sokolov's algorithm: remove the jump in the normal field (:2302-2320)
+      double dBn = 0.5 * (R[Bx_ + d] - L[Bx_ + d]);
+      DiffBn_D[d] = dBn;
+      for (int k = 0; k < 3; k++) { L[Bx_ + k] = L[Bx_ + k] + DiffBn_D[k]; R[Bx_ + k] = R[Bx_ + k] - DiffBn_D[k]; }
+      DiffE = 0.5 * ((R[Bx_] + L[Bx_]) * DiffBn_D[0] + (R[By_] + L[By_]) * DiffBn_D[1] +
+                     (R[Bz_] + L[Bz_]) * DiffBn_D[2]);
+    }
+    for (int v = 0; v < nVar; v++) S[v] = 0.5 * (L[v] + R[v]);
+    double ConsL[nFlux], ConsR[nFlux], FL[nFlux], FR[nFlux], UnL, UnR;
+    double Flux[nFlux];
+    double Cmax, CmaxDt, Un;
+    if (c.typeFlux == ORA_FLUX_RUSANOV) {
+      physical_flux(L, d, ConsL, FL, UnL);
+      physical_flux(R, d, ConsR, FR, UnR);
+      double cl, cr;
+      speed(S, d, Cmax, cl, cr);  // lax_friedrichs_flux (:2513-2559)
+      CmaxDt = Cmax;
+      for (int v = 0; v < nFlux; v++) Flux[v] = 0.5 * (FL[v] + FR[v] - Cmax * (ConsR[v] - ConsL[v]));
+      Un = 0.5 * (UnL + UnR);
+    } else if (c.typeFlux == ORA_FLUX_LINDE) {
+      physical_flux(L, d, ConsL, FL, UnL);
+      physical_flux(R, d, ConsR, FR, UnR);
+      // harten_lax_vanleer_flux (:2561-2645)
+      double ClHat, CrHat, tmp, ClL, CrR;
+      speed(S, d, Cmax, ClHat, CrHat);
+      CmaxDt = Cmax;
+      speed(L, d, tmp, ClL, tmp);
+      speed(R, d, tmp, tmp, CrR);
+      double Cleft = std::min(0.0, std::min(ClL, ClHat));
+      double Cright = std::max(0.0, std::max(CrR, CrHat));
+      double WeightLeft = Cright / (Cright - Cleft);
+      double WeightRight = 1.0 - WeightLeft;
+      double Diffusion = Cright * WeightRight;
+      for (int v = 0; v < nFlux; v++)
+        Flux[v] = (WeightRight * FR[v] + WeightLeft * FL[v] - Diffusion * (ConsR[v] - ConsL[v]));
+      Un = WeightRight * UnR + WeightLeft * UnL;
+    } else {
+      if (hlld(L, R, d, Flux, Cmax, Un)) return 1;
+      CmaxDt = Cmax;
+    }
+    if (UseLindeFix) {
+      // Linde's idea: Lax-Friedrichs flux for Bn (:2403-2418)
+      for (int k = 0; k < 3; k++) Flux[Bx_ + k] = Flux[Bx_ + k] - Cmax * DiffBn_D[k];
+      Flux[Energy_] = Flux[Energy_] - Cmax * DiffE;
+    }
+    for (int v = 0; v < nFlux; v++) Out[v] = Flux[v] * Area;
+    Out[Vdt_] = CmaxDt * Area;
+    Out[Un_] = Un * Area;
+    return 0;
+  }
+
+  // calc_face_flux (src/ModFaceFlux.f90:483-900)
+  int calc_face_flux(int b, Scratch &s) {
+    int nCell[3] = {c.nI, c.nJ, c.nK};
+    int err = 0;
+    for (int d = 0; d < c.nDim; d++) {
+      double Area = cellFace(b, d);
+      long nf = (long)nFace[d][0] * nFace[d][1] * nFace[d][2];
+      for (long f = 0; f < nf; f++)
+        err |= numerical_flux(&s.Left[d][nVar * f], &s.Right[d][nVar * f], d, Area,
+                              &s.Flux[d][nFaceValue * f]);
+    }
+    (void)nCell;
+    return err;
+  }
+
+  // calc_source (src/ModCalcSource.f90:65) with the Powell divB terms
+  // (:862-977) and calc_divb_source (:1694-1891)
+  void calc_source(int b, Scratch &s) {
+    std::fill(s.Source.begin(), s.Source.end(), 0.0);
+    if (!c.useDivbSource) return;
+    double DxInvHalf = 0.5 / dxyz[3 * b], DyInvHalf = 0.5 / dxyz[3 * b + 1], DzInvHalf = 0.5 / dxyz[3 * b + 2];
+    for (int k = 1; k <= c.nK; k++)
+      for (int j = 1; j <= c.nJ; j++)
+        for (int i = 1; i <= c.nI; i++) {
+          auto Lx = [&](int ii) { return s.Left[0][nVar * face(0, ii, j, k) + Bx_]; };
+          auto Rx = [&](int ii) { return s.Right[0][nVar * face(0, ii, j, k) + Bx_]; };
+          double dB1nFace1 = DxInvHalf * (Rx(i) - Lx(i));
+          double dB1nFace2 = DxInvHalf * (Rx(i + 1) - Lx(i + 1));
+          double dB1nFace3 = 0, dB1nFace4 = 0, dB1nFace5 = 0, dB1nFace6 = 0;
+          double DivBInternal = 2 * DxInvHalf * (Lx(i + 1) - Rx(i));
+          if (c.nJ > 1) {
+            auto Ly = [&](int jj) { return s.Left[1][nVar * face(1, i, jj, k) + By_]; };
+            auto Ry = [&](int jj) { return s.Right[1][nVar * face(1, i, jj, k) + By_]; };
+            dB1nFace3 = DyInvHalf * (Ry(j) - Ly(j));
+            dB1nFace4 = DyInvHalf * (Ry(j + 1) - Ly(j + 1));
+            DivBInternal = DivBInternal + 2 * DyInvHalf * (Ly(j + 1) - Ry(j));
+          }
+          if (c.nK > 1) {
+            auto Lz = [&](int kk) { return s.Left[2][nVar * face(2, i, j, kk) + Bz_]; };
+            auto Rz = [&](int kk) { return s.Right[2][nVar * face(2, i, j, kk) + Bz_]; };
+            dB1nFace5 = DzInvHalf * (Rz(k) - Lz(k));
+            dB1nFace6 = DzInvHalf * (Rz(k + 1) - Lz(k + 1));
+            DivBInternal = DivBInternal + 2 * DzInvHalf * (Lz(k + 1) - Rz(k));
+          }
+          double DivB1 = DivBInternal + dB1nFace1 + dB1nFace2;
+          if (c.nJ > 1) DivB1 = DivB1 + dB1nFace3 + dB1nFace4;
+          if (c.nK > 1) DivB1 = DivB1 + dB1nFace5 + dB1nFace6;
+          s.DivB1[icell(i, j, k)] = DivB1;
+          const double *U = st(b, i, j, k);
+          double *Src = &s.Source[(nVar + 1) * icell(i, j, k)];
+          double RhoInv = 1.0 / U[Rho_];
+          double u_D[3] = {RhoInv * U[RhoUx_], RhoInv * U[RhoUy_], RhoInv * U[RhoUz_]};
+          for (int m = 0; m < 3; m++) Src[Bx_ + m] = Src[Bx_ + m] - DivB1 * u_D[m];
+          double SrcMhd[3];
+          for (int m = 0; m < 3; m++) SrcMhd[m] = 0 - DivB1 * U[Bx_ + m];
+          Src[Energy_] = Src[Energy_] - DivB1 * (U[Bx_] * u_D[0] + U[By_] * u_D[1] + U[Bz_] * u_D[2]);
+          for (int m = 0; m < 3; m++) Src[RhoUx_ + m] = Src[RhoUx_ + m] + SrcMhd[m];
+        }
+  }
+
+  // calc_timestep (src/ModTimeStepControl.f90:111-304)
+  void calc_timestep(int b, Scratch &s) {
+    double V = cellVolume(b);
+    double DtBlock = 0;
+    bool first = true;
+    for (int k = 1; k <= c.nK; k++)
+      for (int j = 1; j <= c.nJ; j++)
+        for (int i = 1; i <= c.nI; i++) {
+          double Vdt = std::max(s.Flux[0][nFaceValue * face(0, i, j, k) + Vdt_],
+                                s.Flux[0][nFaceValue * face(0, i + 1, j, k) + Vdt_]);
+          if (c.nJ > 1)
+            Vdt = Vdt + std::max(s.Flux[1][nFaceValue * face(1, i, j, k) + Vdt_],
+                                 s.Flux[1][nFaceValue * face(1, i, j + 1, k) + Vdt_]);
+          if (c.nK > 1)
+            Vdt = Vdt + std::max(s.Flux[2][nFaceValue * face(2, i, j, k) + Vdt_],
+                                 s.Flux[2][nFaceValue * face(2, i, j, k + 1) + Vdt_]);
+          double dt = V / Vdt;
+          DtMax_CB[icell(i, j, k) + (long)c.nI * c.nJ * c.nK * b] = dt;
+          if (first) { DtBlock = dt; first = false; }
+          DtBlock = std::min(DtBlock, dt);
+        }
+    DtMax_B[b] = DtBlock;
+    if (c.useDtFixed)
+      for (long m = 0; m < (long)c.nI * c.nJ * c.nK; m++)
+        DtMax_CB[m + (long)c.nI * c.nJ * c.nK * b] = c.dtFixed;
+  }
+
+  // update_state (src/ModUpdateState.f90:83) -> update_state_normal
+  // (:191-450) -> update_explicit (:453-1160), conservative energy update
+  void update_state(int b, Scratch &s) {
+    if (iStage == 1)
+      std::copy(State.begin() + nVar * nCellG * b, State.begin() + nVar * nCellG * (b + 1),
+                StateOld.begin() + nVar * nCellG * b);
+    if (Dt == 0.0) return;  // IsTimeAccurate .and. Dt == 0
+    double DtFactor = c.useHalfStep ? (c.cfl * iStage) / c.nStage : c.cfl;
+    double V = cellVolume(b);
+    const long nC = (long)c.nI * c.nJ * c.nK;
+    for (int k = 1; k <= c.nK; k++)
+      for (int j = 1; j <= c.nJ; j++)
+        for (int i = 1; i <= c.nI; i++) {
+          double DtLocal = DtFactor * DtMax_CB[icell(i, j, k) + nC * b];
+          double *Src = &s.Source[(nVar + 1) * icell(i, j, k)];
+          const double *fx0 = &s.Flux[0][nFaceValue * face(0, i, j, k)];
+          const double *fx1 = &s.Flux[0][nFaceValue * face(0, i + 1, j, k)];
+          const double *fy0 = c.nJ > 1 ? &s.Flux[1][nFaceValue * face(1, i, j, k)] : nullptr;
+          const double *fy1 = c.nJ > 1 ? &s.Flux[1][nFaceValue * face(1, i, j + 1, k)] : nullptr;
+          const double *fz0 = c.nK > 1 ? &s.Flux[2][nFaceValue * face(2, i, j, k)] : nullptr;
+          const double *fz1 = c.nK > 1 ? &s.Flux[2][nFaceValue * face(2, i, j, k + 1)] : nullptr;
+          for (int v = 0; v < nVar + 1; v++) {
+            double sum = fx0[v] - fx1[v];
+            if (fy0) sum = sum + fy0[v] - fy1[v];
+            if (fz0) sum = sum + fz0[v] - fz1[v];
+            Src[v] = DtLocal * (Src[v] + sum / V);
+          }
+          // pressure_to_energy(StateOld) (src/ModEnergy.f90:47)
+          double *O = so(b, i, j, k);
+          O[P_] = InvGammaMinus1 * O[P_] + 0.5 * (O[RhoUx_] * O[RhoUx_] + O[RhoUy_] * O[RhoUy_] + O[RhoUz_] * O[RhoUz_]) / O[Rho_];
+          O[P_] = O[P_] + 0.5 * (O[Bx_] * O[Bx_] + O[By_] * O[By_] + O[Bz_] * O[Bz_]);
+          Src[P_] = Src[Energy_];
+          double *U = st(b, i, j, k);
+          for (int v = 0; v < nVar; v++) U[v] = O[v] + Src[v];
+          // energy_to_pressure (src/ModEnergy.f90:243) on State and StateOld
+          for (double *X : {U, O}) {
+            X[P_] = X[P_] - 0.5 * (X[Bx_] * X[Bx_] + X[By_] * X[By_] + X[Bz_] * X[Bz_]);
+            X[P_] = GammaMinus1 * (X[P_] - 0.5 * (X[RhoUx_] * X[RhoUx_] + X[RhoUy_] * X[RhoUy_] + X[RhoUz_] * X[RhoUz_]) / X[Rho_]);
+          }
+        }
+  }
+
+  // set_global_timestep (src/ModTimeStepControl.f90:306-524), one process
+  void set_global_timestep(double tLimit) {
+    if (c.useDtFixed) {
+      Dt = c.dtFixed;
+    } else if (nStep < 1 || (nStep == 1 && tLimit > 0.0)) {
+      Dt = 0.0;
+    } else {
+      double DtMin = 1e300;
+      for (int b = 0; b < nBlock; b++) DtMin = std::min(DtMin, DtMax_B[b]);
+      Dt = DtMin;
+    }
+    if (tLimit > 0.0 && tSimulation + c.cfl * Dt > tLimit) Dt = (tLimit - tSimulation) / c.cfl;
+    std::fill(DtMax_CB.begin(), DtMax_CB.end(), Dt);
+    Dt = c.cfl * Dt;
+  }
+
+  // advance_explicit (src/ModAdvanceExplicit.f90:18-325), orig CPU branch
+  int advance_explicit() {
+    int err = 0;
+    for (iStage = 1; iStage <= c.nStage; iStage++) {
+#pragma omp parallel for schedule(dynamic, 4) num_threads((int)scr.size()) reduction(| : err)
+      for (int b = 0; b < nBlock; b++) {
+        int t = 0;
+#ifdef _OPENMP
+        t = omp_get_thread_num();
+#endif
+        Scratch &s = scr[t];
+        calc_face_value(b, s);
+        err |= calc_face_flux(b, s);
+        calc_source(b, s);
+        update_state(b, s);
+        if (iStage == c.nStage && !c.useDtFixed) calc_timestep(b, s);
+      }
+      tSimulation = tSimulation + Dt / c.nStage;
+      if (iStage < c.nStage) exchange_messages();
+    }
+    iStage = c.nStage;
+    return err;
+  }
+
+  // BATS_advance (src/ModBatsrusMethods.f90:493-760), time accurate
+  int advance(double tLimit) {
+    if (tLimit > 0 && tSimulation >= tLimit) return 0;
+    nStep = nStep + 1;
+    set_global_timestep(tLimit);
+    int err = advance_explicit();
+    if (tLimit > 0 && tSimulation < tLimit && tLimit - tSimulation <= 1e-3 * Dt) tSimulation = tLimit;
+    exchange_messages();
+    return err;
+  }
+};
+
+}  // namespace
+
+extern "C" {
+
+void *ora_new(const ora_config *cfg, int nBlock, const int *iLevelCoord) {
+  Oracle *o = new Oracle();
+  o->init(cfg, nBlock, iLevelCoord);
+  return o;
+}
+void ora_free(void *h) { delete (Oracle *)h; }
+long ora_state_size(void *h) { return (long)((Oracle *)h)->State.size(); }
+void ora_set_state(void *h, const double *S) {
+  Oracle *o = (Oracle *)h;
+  std::memcpy(o->State.data(), S, sizeof(double) * o->State.size());
+}
+void ora_get_state(void *h, double *S) {
+  Oracle *o = (Oracle *)h;
+  std::memcpy(S, o->State.data(), sizeof(double) * o->State.size());
+}
+void ora_exchange_messages(void *h) { ((Oracle *)h)->exchange_messages(); }
+int ora_advance(void *h, double tLimit) { return ((Oracle *)h)->advance(tLimit); }
+int ora_advance_n(void *h, int n, double tLimit) {
+  int err = 0;
+  for (int m = 0; m < n; m++) err |= ((Oracle *)h)->advance(tLimit);
+  return err;
+}
+void ora_get_time(void *h, double *t, double *dt, int *n) {
+  Oracle *o = (Oracle *)h;
+  *t = o->tSimulation; *dt = o->Dt; *n = o->nStep;
+}
+void ora_set_time(void *h, double t, int n) {
+  Oracle *o = (Oracle *)h;
+  o->tSimulation = t; o->nStep = n;
+}
+void ora_calc_face_value(void *h, int iBlock) {
+  Oracle *o = (Oracle *)h; o->calc_face_value(iBlock - 1, o->scr[0]);
+}
+void ora_calc_face_flux(void *h, int iBlock) {
+  Oracle *o = (Oracle *)h; o->scr[0].err = o->calc_face_flux(iBlock - 1, o->scr[0]);
+}
+void ora_calc_source(void *h, int iBlock) {
+  Oracle *o = (Oracle *)h; o->calc_source(iBlock - 1, o->scr[0]);
+}
+void ora_calc_timestep(void *h, int iBlock) {
+  Oracle *o = (Oracle *)h; o->calc_timestep(iBlock - 1, o->scr[0]);
+}
+void ora_get_face_values(void *h, int d, double *L, double *R) {
+  Oracle *o = (Oracle *)h;
+  std::memcpy(L, o->scr[0].Left[d].data(), sizeof(double) * o->scr[0].Left[d].size());
+  std::memcpy(R, o->scr[0].Right[d].data(), sizeof(double) * o->scr[0].Right[d].size());
+}
+void ora_get_face_flux(void *h, int d, double *F) {
+  Oracle *o = (Oracle *)h;
+  std::memcpy(F, o->scr[0].Flux[d].data(), sizeof(double) * o->scr[0].Flux[d].size());
+}
+void ora_get_source(void *h, double *S) {
+  Oracle *o = (Oracle *)h;
+  std::memcpy(S, o->scr[0].Source.data(), sizeof(double) * o->scr[0].Source.size());
+}
+void ora_get_dtmax(void *h, double *cb, double *b) {
+  Oracle *o = (Oracle *)h;
+  std::memcpy(cb, o->DtMax_CB.data(), sizeof(double) * o->DtMax_CB.size());
+  std::memcpy(b, o->DtMax_B.data(), sizeof(double) * o->DtMax_B.size());
+}
+
+}  // extern "C"

@@ -1,0 +1,83 @@
+/*
+ * bx_oracle.h -- TEST INFRASTRUCTURE ONLY.
+ *
+ * CPU restatement of the BATS-R-US "orig" explicit MHD path (ModFaceValue,
+ * ModFaceFlux, ModCalcSource, ModUpdateState, ModEnergy, ModTimeStepControl,
+ * ModAdvanceExplicit, ModCellBoundary) used as the parity oracle for the
+ * CUDA kernels in batsrus_b200/csrc.  Only tests/, __graft_entry__.smoke()
+ * and the cpu_baseline leg of bench.py may load it.  The product path never
+ * links or calls it.
+ *
+ * Layout follows the Fortran module arrays: State_VGB(nVar, MinI:MaxI,
+ * MinJ:MaxJ, MinK:MaxK, nBlock), variable index fastest, ghost cells
+ * included (src/ModAdvance.f90:296).
+ */
+#ifndef BX_ORACLE_H
+#define BX_ORACLE_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* flux / limiter selectors (same numbering as include/bx200.h) */
+enum { ORA_FLUX_RUSANOV = 0, ORA_FLUX_LINDE = 1, ORA_FLUX_HLLD = 2 };
+enum { ORA_LIM_MINMOD = 0, ORA_LIM_MC = 1, ORA_LIM_MC3 = 2 };
+enum { ORA_BC_FLOAT = 0, ORA_BC_PERIODIC = 1 };
+
+typedef struct {
+  int nDim;            /* 1, 2 or 3 */
+  int nI, nJ, nK;      /* cells per block (nJ=1 in 1D, nK=1 in 1D/2D) */
+  int nRoot[3];        /* root block counts */
+  double xyzMin[3], xyzMax[3];
+  int typeBc[6];       /* ORA_BC_* for sides x-, x+, y-, y+, z-, z+ */
+  int nOrder;          /* 1 or 2 */
+  int nStage;          /* 1 or 2 */
+  int typeFlux;        /* ORA_FLUX_* */
+  int typeLimiter;     /* ORA_LIM_* */
+  double limiterBeta;
+  double cfl;
+  double gamma;
+  int useDivbSource;   /* Powell source (default nDim>1) */
+  int useDtFixed;
+  double dtFixed;
+  int useHalfStep;     /* #TIMESTEPPING / #SCHEME with nStage<=2 */
+  int nThread;         /* OpenMP threads (0 = default) */
+} ora_config;
+
+/* Create an oracle grid. iLevelCoord holds 4 ints per block: level and the
+ * integer block index (ix,iy,iz) at that level. */
+void *ora_new(const ora_config *cfg, int nBlock, const int *iLevelCoord);
+void ora_free(void *h);
+
+/* full State_VGB including ghost cells */
+long ora_state_size(void *h);
+void ora_set_state(void *h, const double *State_VGB);
+void ora_get_state(void *h, double *State_VGB);
+
+/* ModMessagePass::exchange_messages: ghost fill + outer boundaries */
+void ora_exchange_messages(void *h);
+
+/* One call of BATS_advance (time accurate): set_global_timestep +
+ * advance_explicit + exchange_messages. Returns 0 on success. */
+int ora_advance(void *h, double tSimulationLimit);
+/* nStep calls of ora_advance */
+int ora_advance_n(void *h, int nStep, double tSimulationLimit);
+void ora_get_time(void *h, double *tSimulation, double *Dt, int *nStep);
+void ora_set_time(void *h, double tSimulation, int nStep);
+
+/* per-block orig routines (iBlock is 1-based like the Fortran code) */
+void ora_calc_face_value(void *h, int iBlock);
+void ora_calc_face_flux(void *h, int iBlock);
+void ora_calc_source(void *h, int iBlock);
+void ora_calc_timestep(void *h, int iBlock);
+/* face states (nVar, nI+1, nJ, nK) etc. and fluxes (nFlux+2: fluxes, Vdt, Un)
+ * for direction iDim = 0,1,2 */
+void ora_get_face_values(void *h, int iDim, double *Left, double *Right);
+void ora_get_face_flux(void *h, int iDim, double *Flux);
+void ora_get_source(void *h, double *Source_VC);
+void ora_get_dtmax(void *h, double *DtMax_CB, double *DtMax_B);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,181 @@
+"""ctypes wrapper of the CPU parity oracle (oracle/bx_oracle.cpp).
+
+TEST INFRASTRUCTURE ONLY: imported by tests/, ``__graft_entry__.smoke()`` and
+the ``cpu_baseline`` / ``--impl reference`` legs of ``bench.py``.  The oracle
+restates the BATS-R-US "orig" explicit path (src/ModFaceValue.f90,
+src/ModFaceFlux.f90, src/ModCalcSource.f90, src/ModUpdateState.f90,
+src/ModTimeStepControl.f90, src/ModAdvanceExplicit.f90).
+"""
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB = os.path.join(_HERE, "_build", "liboracle.so")
+
+FLUX = {"rusanov": 0, "linde": 1, "hlld": 2}
+LIMITER = {"minmod": 0, "mc": 1, "mc3": 2, "koren": 2, "no": 0}
+BC = {"float": 0, "periodic": 1}
+
+
+class OraConfig(ctypes.Structure):
+    _fields_ = [
+        ("nDim", ctypes.c_int),
+        ("nI", ctypes.c_int), ("nJ", ctypes.c_int), ("nK", ctypes.c_int),
+        ("nRoot", ctypes.c_int * 3),
+        ("xyzMin", ctypes.c_double * 3), ("xyzMax", ctypes.c_double * 3),
+        ("typeBc", ctypes.c_int * 6),
+        ("nOrder", ctypes.c_int), ("nStage", ctypes.c_int),
+        ("typeFlux", ctypes.c_int), ("typeLimiter", ctypes.c_int),
+        ("limiterBeta", ctypes.c_double),
+        ("cfl", ctypes.c_double), ("gamma", ctypes.c_double),
+        ("useDivbSource", ctypes.c_int),
+        ("useDtFixed", ctypes.c_int), ("dtFixed", ctypes.c_double),
+        ("useHalfStep", ctypes.c_int),
+        ("nThread", ctypes.c_int),
+    ]
+
+
+def build():
+    """Compile the oracle with its Makefile (g++, -ffp-contract=off)."""
+    subprocess.run(["make", "-s", "-C", _HERE], check=True)
+
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(_LIB):
+            build()
+        L = ctypes.CDLL(_LIB)
+        vp, ip, dp = ctypes.c_void_p, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_double)
+        L.ora_new.restype = vp
+        L.ora_new.argtypes = [ctypes.POINTER(OraConfig), ctypes.c_int, ip]
+        L.ora_free.argtypes = [vp]
+        L.ora_state_size.restype = ctypes.c_long
+        L.ora_state_size.argtypes = [vp]
+        for name in ("ora_set_state", "ora_get_state", "ora_get_source"):
+            getattr(L, name).argtypes = [vp, dp]
+        L.ora_exchange_messages.argtypes = [vp]
+        L.ora_advance.restype = ctypes.c_int
+        L.ora_advance.argtypes = [vp, ctypes.c_double]
+        L.ora_advance_n.restype = ctypes.c_int
+        L.ora_advance_n.argtypes = [vp, ctypes.c_int, ctypes.c_double]
+        L.ora_get_time.argtypes = [vp, dp, dp, ip]
+        L.ora_set_time.argtypes = [vp, ctypes.c_double, ctypes.c_int]
+        for name in ("ora_calc_face_value", "ora_calc_face_flux", "ora_calc_source",
+                     "ora_calc_timestep"):
+            getattr(L, name).argtypes = [vp, ctypes.c_int]
+        L.ora_get_face_values.argtypes = [vp, ctypes.c_int, dp, dp]
+        L.ora_get_face_flux.argtypes = [vp, ctypes.c_int, dp]
+        L.ora_get_dtmax.argtypes = [vp, dp, dp]
+        _lib = L
+    return _lib
+
+
+def _dp(a):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+class Oracle:
+    """One oracle grid.  ``scheme`` and ``grid`` use the same keys as
+    :class:`batsrus_b200.session.Scheme` / :class:`batsrus_b200.grid.BlockGrid`."""
+
+    NVAR = 8
+
+    def __init__(self, grid, scheme, n_thread=0):
+        c = OraConfig()
+        c.nDim = grid.nDim
+        c.nI, c.nJ, c.nK = grid.nI, grid.nJ, grid.nK
+        for d in range(3):
+            c.nRoot[d] = grid.nRoot[d]
+            c.xyzMin[d] = grid.xyzMin[d]
+            c.xyzMax[d] = grid.xyzMax[d]
+        for s in range(6):
+            c.typeBc[s] = BC[grid.typeBc[s]]
+        c.nOrder = scheme.nOrder
+        c.nStage = scheme.nStage
+        c.typeFlux = FLUX[scheme.typeFlux.lower()]
+        c.typeLimiter = LIMITER[scheme.typeLimiter.lower()]
+        c.limiterBeta = scheme.limiterBeta
+        c.cfl = scheme.cfl
+        c.gamma = scheme.gamma
+        c.useDivbSource = int(scheme.useDivbSource)
+        c.useDtFixed = int(scheme.useDtFixed)
+        c.dtFixed = scheme.dtFixed
+        c.useHalfStep = int(scheme.useHalfStep)
+        c.nThread = n_thread
+        self.cfg = c
+        self.grid = grid
+        lc = np.ascontiguousarray(grid.iLevelCoord, dtype=np.int32)
+        self.h = lib().ora_new(ctypes.byref(c), grid.nBlock,
+                               lc.ctypes.data_as(ctypes.POINTER(ctypes.c_int)))
+        self.shape = grid.state_shape_fortran()  # (nBlock, nKg, nJg, nIg, nVar)
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            lib().ora_free(self.h)
+            self.h = None
+
+    def set_state(self, State_VGB):
+        a = np.ascontiguousarray(State_VGB, dtype=np.float64)
+        assert a.size == lib().ora_state_size(self.h)
+        lib().ora_set_state(self.h, _dp(a))
+
+    def get_state(self):
+        a = np.empty(self.shape, dtype=np.float64)
+        lib().ora_get_state(self.h, _dp(a))
+        return a
+
+    def exchange_messages(self):
+        lib().ora_exchange_messages(self.h)
+
+    def advance(self, n=1, t_limit=-1.0):
+        err = lib().ora_advance_n(self.h, n, t_limit)
+        if err:
+            raise RuntimeError("oracle advance failed (HLLD negative density ratio)")
+
+    def time(self):
+        t, dt, n = ctypes.c_double(), ctypes.c_double(), ctypes.c_int()
+        lib().ora_get_time(self.h, ctypes.byref(t), ctypes.byref(dt), ctypes.byref(n))
+        return t.value, dt.value, n.value
+
+    def set_time(self, t, n_step):
+        lib().ora_set_time(self.h, t, n_step)
+
+    # per-block orig routines (iBlock 1-based)
+    def calc_face_value(self, iBlock):
+        lib().ora_calc_face_value(self.h, iBlock)
+
+    def calc_face_flux(self, iBlock):
+        lib().ora_calc_face_flux(self.h, iBlock)
+
+    def calc_source(self, iBlock):
+        lib().ora_calc_source(self.h, iBlock)
+
+    def face_values(self, iDim):
+        g = self.grid
+        n = [g.nI, g.nJ, g.nK]
+        n[iDim] += 1
+        L = np.empty((n[2], n[1], n[0], self.NVAR))
+        R = np.empty_like(L)
+        lib().ora_get_face_values(self.h, iDim, _dp(L), _dp(R))
+        return L, R
+
+    def face_flux(self, iDim):
+        g = self.grid
+        n = [g.nI, g.nJ, g.nK]
+        n[iDim] += 1
+        F = np.empty((n[2], n[1], n[0], 11))
+        lib().ora_get_face_flux(self.h, iDim, _dp(F))
+        return F
+
+    def source(self):
+        g = self.grid
+        S = np.empty((g.nK, g.nJ, g.nI, self.NVAR + 1))
+        lib().ora_get_source(self.h, _dp(S))
+        return S
