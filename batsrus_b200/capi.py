@@ -1,0 +1,145 @@
+"""ctypes binding of libbx200.so (include/bx200.h).
+
+The library is the product: it owns the device state and launches the
+sm_100a kernels.  Importing this module fails loudly when the library has
+not been built (``python -m batsrus_b200.build`` or
+``__graft_entry__.build()``); there is no CPU fallback.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "_lib", "libbx200.so")
+
+BX_OK = 0
+STATUS = {0: "BX_OK", 1: "BX_ERR_ARG", 2: "BX_ERR_CUDA", 3: "BX_ERR_STATE", 4: "BX_ERR_NONPHYSICAL",
+          5: "BX_ERR_HLLD", 6: "BX_ERR_KRYLOV", 7: "BX_ERR_TIMEOUT", 8: "BX_ERR_NOMEM"}
+FLUX = {"rusanov": 0, "linde": 1, "hlld": 2}
+LIMITER = {"minmod": 0, "mc": 1, "mc3": 2, "koren": 2, "no": 0}
+BC = {"float": 0, "periodic": 1}
+PRECISION = {"fp64": 0, "fp32": 1, "fp32-bulk": 1}
+
+# every entry point declared in include/bx200.h
+EXPORTS = (
+    "bx_init", "bx_set_scheme", "bx_finalize", "bx_last_error", "bx_upload_state",
+    "bx_download_state", "bx_set_time", "bx_get_time", "bx_calc_face_value", "bx_calc_face_flux",
+    "bx_calc_source", "bx_update_state", "bx_calc_timestep", "bx_get_face_values",
+    "bx_get_face_flux", "bx_get_source", "bx_set_stage", "bx_update_state_fast",
+    "bx_exchange_messages", "bx_set_global_timestep", "bx_advance_explicit", "bx_advance",
+    "bx_synchronize", "bx_timing_enable", "bx_timing_get", "bx_timing_reset",
+    "bx_region_begin", "bx_region_end",
+)
+
+
+class BxError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__("%s: %s" % (STATUS.get(code, code), msg))
+        self.code = code
+
+
+class GridDesc(ctypes.Structure):
+    _fields_ = [
+        ("nDim", ctypes.c_int), ("nI", ctypes.c_int), ("nJ", ctypes.c_int), ("nK", ctypes.c_int),
+        ("nRootBlock", ctypes.c_int * 3),
+        ("CoordMin", ctypes.c_double * 3), ("CoordMax", ctypes.c_double * 3),
+        ("TypeBc", ctypes.c_int * 6),
+        ("nBlock", ctypes.c_int),
+        ("iLevelCoord_IB", ctypes.POINTER(ctypes.c_int)),
+        ("iDevice", ctypes.c_int),
+    ]
+
+
+class SchemeParams(ctypes.Structure):
+    _fields_ = [
+        ("nOrder", ctypes.c_int), ("nStage", ctypes.c_int),
+        ("TypeFlux", ctypes.c_int), ("TypeLimiter", ctypes.c_int),
+        ("LimiterBeta", ctypes.c_double), ("Cfl", ctypes.c_double), ("Gamma", ctypes.c_double),
+        ("UseDivbSource", ctypes.c_int), ("UseHalfStep", ctypes.c_int),
+        ("UseDtFixed", ctypes.c_int), ("DtFixed", ctypes.c_double),
+        ("Precision", ctypes.c_int),
+    ]
+
+
+_lib = None
+
+
+def load():
+    """Load libbx200.so (raises if it has not been built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise ImportError("libbx200.so not found at %s: build it with __graft_entry__.build() "
+                          "(the hot path has no CPU fallback)" % LIB_PATH)
+    L = ctypes.CDLL(LIB_PATH)
+    i, d, p = ctypes.c_int, ctypes.c_double, ctypes.c_void_p
+    dp, ip = ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_int)
+    sig = {
+        "bx_init": [ctypes.POINTER(GridDesc), ctypes.POINTER(SchemeParams)],
+        "bx_set_scheme": [ctypes.POINTER(SchemeParams)],
+        "bx_finalize": [],
+        "bx_upload_state": [dp, i], "bx_download_state": [dp, i],
+        "bx_set_time": [d, i], "bx_get_time": [dp, dp, ip],
+        "bx_calc_face_value": [i, i, i], "bx_calc_face_flux": [i, i],
+        "bx_calc_source": [i], "bx_update_state": [i], "bx_calc_timestep": [i],
+        "bx_get_face_values": [i, dp, dp], "bx_get_face_flux": [i, dp], "bx_get_source": [dp],
+        "bx_set_stage": [i], "bx_update_state_fast": [], "bx_exchange_messages": [i],
+        "bx_set_global_timestep": [d, dp], "bx_advance_explicit": [i], "bx_advance": [i, d],
+        "bx_synchronize": [], "bx_timing_enable": [i], "bx_timing_get": [dp, ip, ip],
+        "bx_timing_reset": [], "bx_region_begin": [], "bx_region_end": [dp],
+    }
+    for name, args in sig.items():
+        f = getattr(L, name)
+        f.argtypes = args
+        f.restype = ctypes.c_int
+    L.bx_last_error.argtypes = []
+    L.bx_last_error.restype = ctypes.c_char_p
+    _lib = L
+    return L
+
+
+def check(code):
+    if code != BX_OK:
+        raise BxError(code, load().bx_last_error().decode())
+    return code
+
+
+def dptr(a):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+def grid_desc(grid, device=0):
+    g = GridDesc()
+    g.nDim = grid.nDim
+    g.nI, g.nJ, g.nK = grid.nI, grid.nJ, grid.nK
+    for d in range(3):
+        g.nRootBlock[d] = grid.nRoot[d]
+        g.CoordMin[d] = grid.xyzMin[d]
+        g.CoordMax[d] = grid.xyzMax[d]
+    for s in range(6):
+        g.TypeBc[s] = BC[grid.typeBc[s]]
+    g.nBlock = grid.nBlock
+    lc = np.ascontiguousarray(grid.iLevelCoord, dtype=np.int32)
+    g.iLevelCoord_IB = lc.ctypes.data_as(ctypes.POINTER(ctypes.c_int))
+    g._keep = lc  # keep the array alive while the struct is used
+    g.iDevice = device
+    return g
+
+
+def scheme_params(s):
+    p = SchemeParams()
+    p.nOrder = s.nOrder
+    p.nStage = s.nStage
+    p.TypeFlux = FLUX[s.typeFlux.lower()]
+    p.TypeLimiter = LIMITER[s.typeLimiter.lower()]
+    p.LimiterBeta = s.limiterBeta
+    p.Cfl = s.cfl
+    p.Gamma = s.gamma
+    p.UseDivbSource = int(s.useDivbSource)
+    p.UseHalfStep = int(s.useHalfStep)
+    p.UseDtFixed = int(s.useDtFixed)
+    p.DtFixed = s.dtFixed
+    p.Precision = PRECISION[s.precision.lower()]
+    return p

@@ -1,0 +1,69 @@
+"""The hot-path workloads: grid, scheme and initial state of each.
+
+* ``shocktube_1d_golden`` -- the reference's own GPU test
+  ``test_shocktube_1d`` (Makefile.test:293-323): 16 blocks of 64 cells on
+  [-128,128], MhdHyp with Hyp = 0 and no hyperbolic cleaning (identical to
+  ideal MHD), gamma 2, first-order Rusanov, 1 stage, Dt fixed at 0.05,
+  512 steps to t = 25.6, float boundaries.
+* ``brio_wu_1d`` -- 256 cells as 32 blocks of 8 on [-0.5,0.5], gamma 2,
+  Rusanov, MC limiter beta 1.5, 2-stage, CFL 0.8, to t = 0.1, float
+  boundaries, no Powell source (nDim = 1).
+* ``orszag_tang_3d`` -- periodic unit cube, (8 nRoot)^3 cells in 8^3 blocks
+  (nRoot = 32 gives 256^3 = 32768 blocks), Linde HLL flux, Koren (mc3)
+  limiter with beta 1.2 (the PARAM.XML default for mc3), CFL 0.8,
+  gamma 5/3, Powell source on.
+"""
+import math
+
+from . import initial
+from .grid import BlockGrid
+from .param import Scheme
+
+
+def shocktube_1d_golden():
+    g = BlockGrid.uniform(1, (64, 1, 1), (16, 1, 1), (-128.0, -0.125, -0.125),
+                          (128.0, 0.125, 0.125), ("float",) * 6)
+    s = Scheme(nOrder=1, nStage=1, typeFlux="Rusanov", typeLimiter="no", cfl=1.0, gamma=2.0,
+               useDivbSource=False, useDtFixed=True, dtFixed=0.05, useHalfStep=True)
+    st = initial.shocktube(g, [1, 0, 0, 0, 0.75, 1, 0, 1], [0.125, 0, 0, 0, 0.75, -1, 0, 0.1])
+    return g, s, st, {"nStep": 512, "tSimulationMax": 25.6}
+
+
+def brio_wu_1d(nBlock=32):
+    g = BlockGrid.uniform(1, (8, 1, 1), (nBlock, 1, 1), (-0.5, -0.5, -0.5), (0.5, 0.5, 0.5),
+                          ("float",) * 6)
+    s = Scheme(nOrder=2, nStage=2, typeFlux="Rusanov", typeLimiter="mc", limiterBeta=1.5, cfl=0.8,
+               gamma=2.0, useDivbSource=False, useHalfStep=True)
+    st = initial.shocktube(g, [1, 0, 0, 0, 0.75, 1, 0, 1], [0.125, 0, 0, 0, 0.75, -1, 0, 0.1])
+    return g, s, st, {"tSimulationMax": 0.1}
+
+
+def orszag_tang_3d(nRoot=32, precision="fp64", flux="Linde", limiter="mc3", beta=1.2,
+                   nCellBlock=(8, 8, 8), order="x"):
+    g = BlockGrid.uniform(3, nCellBlock, (nRoot,) * 3, (0.0, 0.0, 0.0), (1.0, 1.0, 1.0),
+                          ("periodic",) * 6, order=order)
+    s = Scheme(nOrder=2, nStage=2, typeFlux=flux, typeLimiter=limiter, limiterBeta=beta, cfl=0.8,
+               gamma=5.0 / 3.0, useDivbSource=True, useHalfStep=True, precision=precision)
+    st = initial.orszag_tang_3d(g)
+    return g, s, st, {"nStep": 20}
+
+
+def uniform_3d_case(nRoot, flux, limiter="mc3", beta=1.2, precision="fp64", nCellBlock=(8, 8, 8),
+                    state="ot", bc="periodic"):
+    """Small 3D parity case with any flux/limiter."""
+    g = BlockGrid.uniform(3, nCellBlock, tuple(nRoot) if hasattr(nRoot, "__len__") else (nRoot,) * 3,
+                          (0.0, 0.0, 0.0), (1.0, 1.0, 1.0), (bc,) * 6)
+    s = Scheme(nOrder=2, nStage=2, typeFlux=flux, typeLimiter=limiter, limiterBeta=beta, cfl=0.8,
+               gamma=5.0 / 3.0, useDivbSource=True, useHalfStep=True, precision=precision)
+    if state == "ot":
+        st = initial.orszag_tang_3d(g)
+    elif state == "blast":
+        g = BlockGrid.uniform(3, nCellBlock, tuple(nRoot) if hasattr(nRoot, "__len__") else (nRoot,) * 3,
+                              (-0.5, -0.5, -0.5), (0.5, 0.5, 0.5), (bc,) * 6)
+        st = initial.blast(g)
+    else:
+        st = initial.perturbed_ot(g, seed=7, amplitude=0.05, kmax=2)
+    return g, s, st, {}
+
+
+CELLS_PER_STEP_BYTES = {"fp64": 320, "fp32": 256}

@@ -1,0 +1,742 @@
+// bx_capi.cu -- the extern "C" boundary of libbx200 (include/bx200.h).
+//
+// Host side of the explicit hot path: grid bookkeeping (neighbour tables,
+// Morton processing order, block geometry), device state management, the
+// per-block entry points of the orig path, the batched stage launches, the
+// device-side time step and the CUDA-graph time loop.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdint>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <string>
+#include <tuple>
+#include <vector>
+
+#include "../../include/bx200.h"
+#include "bx_device.h"
+
+using namespace bx;
+
+namespace {
+
+struct Ctx {
+  bool ready = false;
+  int dev = 0;
+  int nDim = 3, nI = 8, nJ = 8, nK = 8, shape = kShape888;
+  int nBlock = 0;
+  long nCell = 0;  // cells per block
+  int nRoot[3];
+  double cmin[3], cmax[3];
+  int typeBc[6];
+  bx_scheme_params sch;
+  std::vector<int> lev, ic;  // per block
+  std::vector<int> nbrH, orderH;
+  std::vector<BlockGeom> geomH;
+  // device
+  double *A = nullptr;       // U^n (FP64)
+  double *B = nullptr;       // stage buffer (FP64 or FP32 storage)
+  double *Nx = nullptr, *Ox = nullptr;  // compat next / old (lazy)
+  double *stageAoS = nullptr;  // staging of State_VGB for upload/download
+  size_t stageAoSBytes = 0;
+  int *nbr = nullptr, *order = nullptr;
+  BlockGeom *geom = nullptr;
+  StepState *ts = nullptr;
+  double *dtBlock = nullptr;
+  double *scrL[3] = {}, *scrR[3] = {}, *scrF[3] = {}, *scrSrc = nullptr, *scrDt = nullptr;
+  std::vector<char> touched;
+  bool compatPending = false;
+  int iStage = 1;
+  cudaStream_t st = nullptr;
+  cudaGraphExec_t graph = nullptr;
+  double graphTLimit = 0;
+  // timing
+  bool timing = false;
+  std::vector<cudaEvent_t> evStart, evStop;
+  int nTimed = 0, nLaunchTotal = 0;
+  std::string err;
+};
+
+Ctx g;
+
+int fail(int code, const char *fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof(buf), fmt, ap);
+  va_end(ap);
+  g.err = buf;
+  return code;
+}
+
+#define CK(call)                                                                          \
+  do {                                                                                    \
+    cudaError_t e_ = (call);                                                              \
+    if (e_ != cudaSuccess)                                                                \
+      return fail(BX_ERR_CUDA, "%s failed: %s (%s:%d)", #call, cudaGetErrorString(e_),    \
+                  __FILE__, __LINE__);                                                    \
+  } while (0)
+
+#define NEED_READY() \
+  do { if (!g.ready) return fail(BX_ERR_STATE, "bx_init has not been called"); } while (0)
+
+int shape_of(int nDim, int nI, int nJ, int nK) {
+  if (nDim == 3 && nI == 8 && nJ == 8 && nK == 8) return kShape888;
+  if (nDim == 3 && nI == 4 && nJ == 4 && nK == 4) return kShape444;
+  if (nDim == 2 && nI == 8 && nJ == 8 && nK == 1) return kShape881;
+  if (nDim == 1 && nI == 8 && nJ == 1 && nK == 1) return kShape811;
+  if (nDim == 1 && nI == 64 && nJ == 1 && nK == 1) return kShape6411;
+  return -1;
+}
+
+uint64_t morton3(uint32_t x, uint32_t y, uint32_t z) {
+  uint64_t k = 0;
+  for (int b = 0; b < 21; b++)
+    k |= ((uint64_t)((x >> b) & 1) << (3 * b)) | ((uint64_t)((y >> b) & 1) << (3 * b + 1)) |
+         ((uint64_t)((z >> b) & 1) << (3 * b + 2));
+  return k;
+}
+
+// -------------------------------------------------------------------------
+// kernels of the host boundary
+
+// State_VGB (var fastest, ghost cells) -> SoA interior
+__global__ void aos_to_soa(const double *__restrict__ aos, double *__restrict__ soa, int nBlock,
+                           int nI, int nJ, int nK, int nIg, int nJg, int nKg, int gi, int gj, int gk) {
+  const long nC = (long)nI * nJ * nK;
+  const long total = nC * nBlock;
+  for (long q = blockIdx.x * (long)blockDim.x + threadIdx.x; q < total; q += (long)gridDim.x * blockDim.x) {
+    const long b = q / nC, c = q % nC;
+    const int i = c % nI, j = (c / nI) % nJ, k = c / ((long)nI * nJ);
+    const double *s = aos + 8 * ((i + gi) + (long)nIg * ((j + gj) + (long)nJg * ((k + gk) + (long)nKg * b)));
+    double *t = soa + b * 8 * nC + c;
+#pragma unroll
+    for (int v = 0; v < 8; v++) t[v * nC] = s[v];
+  }
+}
+
+// SoA interior -> State_VGB including ghost cells, filled as
+// exchange_messages does on a single-level grid (neighbour interiors,
+// periodic wrap through the neighbour table, float boundaries copy the
+// boundary cell)
+__global__ void soa_to_aos(const double *__restrict__ soa, double *__restrict__ aos, const int *nbr,
+                           int nBlock, int nDim, int nI, int nJ, int nK, int nIg, int nJg, int nKg, int gi,
+                           int gj, int gk) {
+  const long nC = (long)nI * nJ * nK;
+  const long nG = (long)nIg * nJg * nKg;
+  const long total = nG * nBlock;
+  const int n[3] = {nI, nJ, nK};
+  for (long q = blockIdx.x * (long)blockDim.x + threadIdx.x; q < total; q += (long)gridDim.x * blockDim.x) {
+    const long b = q / nG, c = q % nG;
+    int idx[3] = {(int)(c % nIg) - gi, (int)((c / nIg) % nJg) - gj, (int)(c / ((long)nIg * nJg)) - gk};
+    int sb = (int)b;
+    for (int d = 0; d < nDim; d++) {
+      if (idx[d] < 0 || idx[d] >= n[d]) {
+        const int side = 2 * d + (idx[d] < 0 ? 0 : 1);
+        const int nb = nbr[6 * sb + side];
+        if (nb >= 0) { sb = nb; idx[d] += idx[d] < 0 ? n[d] : -n[d]; }
+        else idx[d] = idx[d] < 0 ? 0 : n[d] - 1;
+      }
+    }
+    const double *s = soa + (long)sb * 8 * nC + idx[0] + (long)nI * (idx[1] + (long)nJ * idx[2]);
+    double *t = aos + 8 * q;
+#pragma unroll
+    for (int v = 0; v < 8; v++) t[v] = s[v * nC];
+  }
+}
+
+// set_global_timestep (src/ModTimeStepControl.f90:306-524) on the device
+__global__ void set_dt_kernel(StepState *ts, double tLimit, int useDtFixed, double dtFixed, double cfl) {
+  ts->nStep = ts->nStep + 1;
+  double dt;
+  // BATS_advance always passes a positive limit (tSimulationMax or
+  // huge(0.0)), so the first time-accurate step has Dt = 0
+  if (useDtFixed) dt = dtFixed;
+  else if (ts->nStep <= 1) dt = 0.0;
+  else dt = __longlong_as_double((long long)ts->DtMinBits);
+  if (tLimit > 0.0 && ts->tSimulation + cfl * dt > tLimit) dt = (tLimit - ts->tSimulation) / cfl;
+  ts->DtNoCfl = dt;
+  ts->Dt = cfl * dt;
+  ts->DtMinBits = 0x7FF0000000000000ull;  // +inf
+}
+
+// end of BATS_advance: tSimulation += Dt/nStage per stage and the final
+// adjustment to the time limit (src/ModBatsrusMethods.f90:606-640)
+__global__ void end_step_kernel(StepState *ts, int nStage, double tLimit) {
+  double t = ts->tSimulation;
+  for (int s = 0; s < nStage; s++) t = t + ts->Dt / nStage;
+  if (tLimit > 0.0 && t < tLimit && tLimit - t <= 1e-3 * ts->Dt) t = tLimit;
+  ts->tSimulation = t;
+}
+
+__global__ void dtmin_from_blocks(StepState *ts, const double *dtBlock, int nBlock) {
+  __shared__ double w[32];
+  double m = 1e300;
+  for (int b = threadIdx.x; b < nBlock; b += blockDim.x) m = fmin(m, dtBlock[b]);
+  for (int off = 16; off > 0; off >>= 1) m = fmin(m, __shfl_xor_sync(0xffffffffu, m, off));
+  if ((threadIdx.x & 31) == 0) w[threadIdx.x >> 5] = m;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double r = w[0];
+    for (int i = 1; i < (int)(blockDim.x >> 5); i++) r = fmin(r, w[i]);
+    ts->DtMinBits = (unsigned long long)__double_as_longlong(r);
+  }
+}
+
+__global__ void copy_blocks(double *dst, const double *src, const int *blocks, int nList, long nPerBlock) {
+  const long total = (long)nList * nPerBlock;
+  for (long q = blockIdx.x * (long)blockDim.x + threadIdx.x; q < total; q += (long)gridDim.x * blockDim.x) {
+    const long b = blocks[q / nPerBlock];
+    dst[b * nPerBlock + q % nPerBlock] = src[b * nPerBlock + q % nPerBlock];
+  }
+}
+
+// -------------------------------------------------------------------------
+void free_all() {
+  if (g.graph) { cudaGraphExecDestroy(g.graph); g.graph = nullptr; }
+  for (double **p : {&g.A, &g.B, &g.Nx, &g.Ox, &g.stageAoS, &g.dtBlock, &g.scrSrc, &g.scrDt}) {
+    if (*p) cudaFree(*p);
+    *p = nullptr;
+  }
+  for (int d = 0; d < 3; d++)
+    for (double **p : {&g.scrL[d], &g.scrR[d], &g.scrF[d]}) {
+      if (*p) cudaFree(*p);
+      *p = nullptr;
+    }
+  if (g.nbr) cudaFree(g.nbr);
+  if (g.order) cudaFree(g.order);
+  if (g.geom) cudaFree(g.geom);
+  if (g.ts) cudaFree(g.ts);
+  g.nbr = g.order = nullptr; g.geom = nullptr; g.ts = nullptr;
+  for (auto e : g.evStart) cudaEventDestroy(e);
+  for (auto e : g.evStop) cudaEventDestroy(e);
+  g.evStart.clear(); g.evStop.clear();
+  if (g.st) cudaStreamDestroy(g.st);
+  g.st = nullptr;
+  g.stageAoSBytes = 0;
+  g.ready = false;
+}
+
+int check_scheme(const bx_scheme_params *s) {
+  if (s->nOrder != 1 && s->nOrder != 2) return fail(BX_ERR_ARG, "nOrder=%d not supported", s->nOrder);
+  if (s->nStage != 1 && s->nStage != 2) return fail(BX_ERR_ARG, "nStage=%d not supported", s->nStage);
+  if (s->TypeFlux < 0 || s->TypeFlux > 2) return fail(BX_ERR_ARG, "TypeFlux=%d unknown", s->TypeFlux);
+  if (s->TypeLimiter < 0 || s->TypeLimiter > 2) return fail(BX_ERR_ARG, "TypeLimiter=%d unknown", s->TypeLimiter);
+  if (s->Gamma <= 1.0) return fail(BX_ERR_ARG, "Gamma must exceed 1");
+  if (s->Cfl <= 0.0) return fail(BX_ERR_ARG, "Cfl must be positive");
+  if (s->Precision == BX_FP32_BULK) {
+    if (g.shape != kShape888 && g.shape != kShape444)
+      return fail(BX_ERR_ARG, "FP32-bulk mode needs 3D 8x8x8 or 4x4x4 blocks");
+    if (s->nStage != 2) return fail(BX_ERR_ARG, "FP32-bulk mode needs the 2-stage scheme");
+  } else if (s->Precision != BX_FP64) {
+    return fail(BX_ERR_ARG, "Precision=%d unknown", s->Precision);
+  }
+  return BX_OK;
+}
+
+StageArgs stage_args(int iStage, bool computeDt) {
+  StageArgs a;
+  a.nbr = g.nbr; a.order = g.order; a.geom = g.geom; a.ts = g.ts; a.dtBlock = g.dtBlock;
+  a.nBlock = g.nBlock;
+  a.iStage = iStage; a.nStage = g.sch.nStage; a.nOrder = g.sch.nOrder; a.limiter = g.sch.TypeLimiter;
+  a.useDivb = g.sch.UseDivbSource; a.useHalfStep = g.sch.UseHalfStep; a.computeDt = computeDt;
+  a.beta = g.sch.LimiterBeta; a.gamma = g.sch.Gamma; a.invGm1 = 1.0 / (g.sch.Gamma - 1.0);
+  a.cfl = g.sch.Cfl;
+  a.old = g.A;
+  if (g.sch.nStage == 1) { a.in = g.A; a.out = g.B; }
+  else if (iStage == 1) { a.in = g.A; a.out = g.B; }
+  else { a.in = g.B; a.out = g.A; }
+  return a;
+}
+
+// one stage of all blocks (update_state_fast)
+int launch_stage(int iStage) {
+  const bool last = iStage == g.sch.nStage;
+  StageArgs a = stage_args(iStage, last);
+  if (g.timing) {
+    if (g.nTimed >= (int)g.evStart.size()) {
+      cudaEvent_t e0, e1;
+      CK(cudaEventCreate(&e0)); CK(cudaEventCreate(&e1));
+      g.evStart.push_back(e0); g.evStop.push_back(e1);
+    }
+    CK(cudaEventRecord(g.evStart[g.nTimed], g.st));
+  }
+  cudaError_t e;
+  if (g.sch.Precision == BX_FP64) e = launch_stage_fp64(g.shape, g.sch.TypeFlux, a, g.st);
+  else e = launch_stage_fp32(g.shape, g.sch.TypeFlux, iStage == 1 ? 0 : 1, a, g.st);
+  if (e != cudaSuccess) return fail(BX_ERR_CUDA, "stage kernel launch: %s", cudaGetErrorString(e));
+  if (g.timing) { CK(cudaEventRecord(g.evStop[g.nTimed], g.st)); g.nTimed++; }
+  g.nLaunchTotal++;
+  if (g.sch.nStage == 1) std::swap(g.A, g.B);  // new state is in B
+  return BX_OK;
+}
+
+int launch_step(double tLimit) {
+  set_dt_kernel<<<1, 1, 0, g.st>>>(g.ts, tLimit, g.sch.UseDtFixed, g.sch.DtFixed, g.sch.Cfl);
+  CK(cudaGetLastError());
+  for (int s = 1; s <= g.sch.nStage; s++) {
+    int r = launch_stage(s);
+    if (r) return r;
+  }
+  end_step_kernel<<<1, 1, 0, g.st>>>(g.ts, g.sch.nStage, tLimit);
+  CK(cudaGetLastError());
+  return BX_OK;
+}
+
+int ensure_compat() {
+  if (g.Nx) return BX_OK;
+  const size_t bytes = sizeof(double) * 8 * g.nCell * g.nBlock;
+  CK(cudaMalloc(&g.Nx, bytes));
+  CK(cudaMalloc(&g.Ox, bytes));
+  CK(cudaMemcpyAsync(g.Nx, g.A, bytes, cudaMemcpyDeviceToDevice, g.st));
+  CK(cudaMemcpyAsync(g.Ox, g.A, bytes, cudaMemcpyDeviceToDevice, g.st));
+  const int nF[3] = {(g.nI + 1) * g.nJ * g.nK, g.nI * (g.nJ + 1) * g.nK, g.nI * g.nJ * (g.nK + 1)};
+  for (int d = 0; d < 3; d++) {
+    CK(cudaMalloc(&g.scrL[d], sizeof(double) * 8 * nF[d]));
+    CK(cudaMalloc(&g.scrR[d], sizeof(double) * 8 * nF[d]));
+    CK(cudaMalloc(&g.scrF[d], sizeof(double) * 9 * nF[d]));
+    CK(cudaMemsetAsync(g.scrL[d], 0, sizeof(double) * 8 * nF[d], g.st));
+    CK(cudaMemsetAsync(g.scrR[d], 0, sizeof(double) * 8 * nF[d], g.st));
+    CK(cudaMemsetAsync(g.scrF[d], 0, sizeof(double) * 9 * nF[d], g.st));
+  }
+  CK(cudaMalloc(&g.scrSrc, sizeof(double) * 9 * g.nCell));
+  CK(cudaMalloc(&g.scrDt, sizeof(double) * g.nCell));
+  g.touched.assign(g.nBlock, 0);
+  return BX_OK;
+}
+
+CompatArgs compat_args() {
+  CompatArgs a;
+  a.state = g.A; a.old = g.Ox; a.next = g.Nx; a.nbr = g.nbr; a.geom = g.geom; a.ts = g.ts;
+  for (int d = 0; d < 3; d++) { a.left[d] = g.scrL[d]; a.right[d] = g.scrR[d]; a.flux[d] = g.scrF[d]; }
+  a.source = g.scrSrc; a.dtCell = g.scrDt; a.dtBlock = g.dtBlock;
+  a.iStage = g.iStage; a.nStage = g.sch.nStage; a.nOrder = g.sch.nOrder; a.limiter = g.sch.TypeLimiter;
+  a.useDivb = g.sch.UseDivbSource; a.useHalfStep = g.sch.UseHalfStep;
+  a.beta = g.sch.LimiterBeta; a.gamma = g.sch.Gamma; a.invGm1 = 1.0 / (g.sch.Gamma - 1.0); a.cfl = g.sch.Cfl;
+  return a;
+}
+
+int compat_phase(int phase, int iBlock) {
+  NEED_READY();
+  if (iBlock < 1 || iBlock > g.nBlock) return fail(BX_ERR_ARG, "iBlock=%d out of range 1..%d", iBlock, g.nBlock);
+  int r = ensure_compat();
+  if (r) return r;
+  cudaError_t e = launch_compat(g.shape, g.sch.TypeFlux, phase, iBlock - 1, compat_args(), g.st);
+  if (e != cudaSuccess) return fail(BX_ERR_CUDA, "per-block kernel: %s", cudaGetErrorString(e));
+  return BX_OK;
+}
+
+int check_err_flag() {
+  int flag = 0;
+  CK(cudaMemcpyAsync(&flag, &g.ts->errFlag, sizeof(int), cudaMemcpyDeviceToHost, g.st));
+  CK(cudaStreamSynchronize(g.st));
+  if (flag) {
+    int zero = 0;
+    CK(cudaMemcpy(&g.ts->errFlag, &zero, sizeof(int), cudaMemcpyHostToDevice));
+    if (flag & kErrHlld) return fail(BX_ERR_HLLD, "hlld_flux: negative density ratio (reference stops)");
+    return fail(BX_ERR_NONPHYSICAL, "non-physical state");
+  }
+  return BX_OK;
+}
+
+}  // namespace
+
+// ===========================================================================
+extern "C" {
+
+const char *bx_last_error(void) { return g.err.c_str(); }
+
+int bx_init(const bx_grid_desc *gd, const bx_scheme_params *sp) {
+  if (!gd || !sp) return fail(BX_ERR_ARG, "null argument");
+  if (g.ready) free_all();
+  const int shape = shape_of(gd->nDim, gd->nI, gd->nJ, gd->nK);
+  if (shape < 0)
+    return fail(BX_ERR_ARG, "block size %dx%dx%d in %dD not supported", gd->nI, gd->nJ, gd->nK, gd->nDim);
+  if (gd->nBlock < 1 || !gd->iLevelCoord_IB) return fail(BX_ERR_ARG, "empty block list");
+  g.shape = shape;
+  g.nDim = gd->nDim; g.nI = gd->nI; g.nJ = gd->nJ; g.nK = gd->nK;
+  g.nBlock = gd->nBlock; g.nCell = (long)gd->nI * gd->nJ * gd->nK;
+  for (int d = 0; d < 3; d++) { g.nRoot[d] = gd->nRootBlock[d]; g.cmin[d] = gd->CoordMin[d]; g.cmax[d] = gd->CoordMax[d]; }
+  for (int s = 0; s < 6; s++) g.typeBc[s] = gd->TypeBc[s];
+  int r = check_scheme(sp);
+  if (r) return r;
+  g.sch = *sp;
+  g.dev = gd->iDevice;
+  CK(cudaSetDevice(g.dev));
+
+  // block bookkeeping (BATL tree of one level: iNode -> neighbours)
+  g.lev.resize(g.nBlock); g.ic.resize(3 * g.nBlock);
+  std::map<std::tuple<int, int, int, int>, int> node;
+  for (int b = 0; b < g.nBlock; b++) {
+    g.lev[b] = gd->iLevelCoord_IB[4 * b];
+    for (int d = 0; d < 3; d++) g.ic[3 * b + d] = gd->iLevelCoord_IB[4 * b + 1 + d];
+    auto key = std::make_tuple(g.lev[b], g.ic[3 * b], g.ic[3 * b + 1], g.ic[3 * b + 2]);
+    if (node.count(key)) return fail(BX_ERR_ARG, "block %d duplicates block %d", b + 1, node[key] + 1);
+    node[key] = b;
+  }
+  g.nbrH.assign(6 * g.nBlock, -1);
+  for (int b = 0; b < g.nBlock; b++) {
+    for (int d = 0; d < g.nDim; d++) {
+      const int nbl = g.nRoot[d] << g.lev[b];
+      for (int side = 0; side < 2; side++) {
+        int c[3] = {g.ic[3 * b], g.ic[3 * b + 1], g.ic[3 * b + 2]};
+        c[d] += side ? 1 : -1;
+        if (c[d] < 0 || c[d] >= nbl) {
+          if (g.typeBc[2 * d + side] == BX_BC_PERIODIC) c[d] = (c[d] + nbl) % nbl;
+          else { g.nbrH[6 * b + 2 * d + side] = -1; continue; }
+        }
+        auto it = node.find(std::make_tuple(g.lev[b], c[0], c[1], c[2]));
+        if (it == node.end())
+          return fail(BX_ERR_ARG, "block %d has no same-level neighbour on side %d: refined grids need the AMR path",
+                      b + 1, 2 * d + side);
+        g.nbrH[6 * b + 2 * d + side] = it->second;
+      }
+    }
+  }
+  // Morton processing order (L2 reuse of the neighbours' interiors)
+  g.orderH.resize(g.nBlock);
+  for (int b = 0; b < g.nBlock; b++) g.orderH[b] = b;
+  std::stable_sort(g.orderH.begin(), g.orderH.end(), [&](int x, int y) {
+    if (g.lev[x] != g.lev[y]) return g.lev[x] < g.lev[y];
+    return morton3(g.ic[3 * x], g.ic[3 * x + 1], g.ic[3 * x + 2]) <
+           morton3(g.ic[3 * y], g.ic[3 * y + 1], g.ic[3 * y + 2]);
+  });
+  // geometry
+  g.geomH.resize(g.nBlock);
+  const int nc[3] = {g.nI, g.nJ, g.nK};
+  for (int b = 0; b < g.nBlock; b++) {
+    BlockGeom &q = g.geomH[b];
+    for (int d = 0; d < 3; d++) {
+      const double ext = g.cmax[d] - g.cmin[d];
+      if (d < g.nDim) {
+        const double bsize = ext / ((double)g.nRoot[d] * (double)(1 << g.lev[b]));
+        q.cellSize[d] = bsize / nc[d];
+      } else {
+        q.cellSize[d] = ext;
+      }
+    }
+    q.volume = q.cellSize[0] * q.cellSize[1] * q.cellSize[2];
+    for (int d = 0; d < 3; d++) {
+      q.area[d] = q.volume / q.cellSize[d];
+      q.invHalf[d] = 0.5 / q.cellSize[d];
+    }
+  }
+
+  CK(cudaStreamCreateWithFlags(&g.st, cudaStreamNonBlocking));
+  const size_t stBytes = sizeof(double) * 8 * g.nCell * g.nBlock;
+  if (cudaMalloc(&g.A, stBytes) != cudaSuccess || cudaMalloc(&g.B, stBytes) != cudaSuccess) {
+    free_all();
+    return fail(BX_ERR_NOMEM, "cannot allocate 2 x %.2f GB of state", stBytes / 1e9);
+  }
+  CK(cudaMemsetAsync(g.A, 0, stBytes, g.st));
+  CK(cudaMemsetAsync(g.B, 0, stBytes, g.st));
+  CK(cudaMalloc(&g.nbr, sizeof(int) * 6 * g.nBlock));
+  CK(cudaMalloc(&g.order, sizeof(int) * g.nBlock));
+  CK(cudaMalloc(&g.geom, sizeof(BlockGeom) * g.nBlock));
+  CK(cudaMalloc(&g.ts, sizeof(StepState)));
+  CK(cudaMalloc(&g.dtBlock, sizeof(double) * g.nBlock));
+  CK(cudaMemcpyAsync(g.nbr, g.nbrH.data(), sizeof(int) * 6 * g.nBlock, cudaMemcpyHostToDevice, g.st));
+  CK(cudaMemcpyAsync(g.order, g.orderH.data(), sizeof(int) * g.nBlock, cudaMemcpyHostToDevice, g.st));
+  CK(cudaMemcpyAsync(g.geom, g.geomH.data(), sizeof(BlockGeom) * g.nBlock, cudaMemcpyHostToDevice, g.st));
+  CK(cudaMemsetAsync(g.dtBlock, 0, sizeof(double) * g.nBlock, g.st));
+  StepState s0;
+  std::memset(&s0, 0, sizeof(s0));
+  s0.DtMinBits = 0x7FF0000000000000ull;
+  CK(cudaMemcpyAsync(g.ts, &s0, sizeof(s0), cudaMemcpyHostToDevice, g.st));
+  CK(cudaStreamSynchronize(g.st));
+  g.iStage = 1;
+  g.ready = true;
+  return BX_OK;
+}
+
+int bx_set_scheme(const bx_scheme_params *sp) {
+  NEED_READY();
+  if (!sp) return fail(BX_ERR_ARG, "null argument");
+  int r = check_scheme(sp);
+  if (r) return r;
+  g.sch = *sp;
+  if (g.graph) { cudaGraphExecDestroy(g.graph); g.graph = nullptr; }
+  return BX_OK;
+}
+
+int bx_finalize(void) {
+  if (g.ready) { cudaStreamSynchronize(g.st); free_all(); }
+  return BX_OK;
+}
+
+static int ensure_stage_aos(size_t bytes) {
+  if (g.stageAoSBytes >= bytes) return BX_OK;
+  if (g.stageAoS) cudaFree(g.stageAoS);
+  g.stageAoS = nullptr;
+  g.stageAoSBytes = 0;
+  if (cudaMalloc(&g.stageAoS, bytes) != cudaSuccess)
+    return fail(BX_ERR_NOMEM, "cannot allocate %.2f GB of State_VGB staging", bytes / 1e9);
+  g.stageAoSBytes = bytes;
+  return BX_OK;
+}
+
+static void ghost_extent(int &nIg, int &nJg, int &nKg, int &gi, int &gj, int &gk) {
+  gi = 2; gj = g.nDim > 1 ? 2 : 0; gk = g.nDim > 2 ? 2 : 0;
+  nIg = g.nI + 2 * gi; nJg = g.nJ + 2 * gj; nKg = g.nK + 2 * gk;
+}
+
+int bx_upload_state(const double *State_VGB, int nBlock) {
+  NEED_READY();
+  if (!State_VGB || nBlock != g.nBlock) return fail(BX_ERR_ARG, "nBlock=%d, expected %d", nBlock, g.nBlock);
+  int nIg, nJg, nKg, gi, gj, gk;
+  ghost_extent(nIg, nJg, nKg, gi, gj, gk);
+  const size_t bytes = sizeof(double) * 8 * (size_t)nIg * nJg * nKg * g.nBlock;
+  int r = ensure_stage_aos(bytes);
+  if (r) return r;
+  CK(cudaMemcpyAsync(g.stageAoS, State_VGB, bytes, cudaMemcpyHostToDevice, g.st));
+  aos_to_soa<<<1184, 256, 0, g.st>>>(g.stageAoS, g.A, g.nBlock, g.nI, g.nJ, g.nK, nIg, nJg, nKg, gi, gj, gk);
+  CK(cudaGetLastError());
+  if (g.Nx) {
+    const size_t sb = sizeof(double) * 8 * g.nCell * g.nBlock;
+    CK(cudaMemcpyAsync(g.Nx, g.A, sb, cudaMemcpyDeviceToDevice, g.st));
+    CK(cudaMemcpyAsync(g.Ox, g.A, sb, cudaMemcpyDeviceToDevice, g.st));
+  }
+  CK(cudaStreamSynchronize(g.st));
+  return BX_OK;
+}
+
+int bx_download_state(double *State_VGB, int nBlock) {
+  NEED_READY();
+  if (!State_VGB || nBlock != g.nBlock) return fail(BX_ERR_ARG, "nBlock=%d, expected %d", nBlock, g.nBlock);
+  int nIg, nJg, nKg, gi, gj, gk;
+  ghost_extent(nIg, nJg, nKg, gi, gj, gk);
+  const size_t bytes = sizeof(double) * 8 * (size_t)nIg * nJg * nKg * g.nBlock;
+  int r = ensure_stage_aos(bytes);
+  if (r) return r;
+  soa_to_aos<<<1184, 256, 0, g.st>>>(g.A, g.stageAoS, g.nbr, g.nBlock, g.nDim, g.nI, g.nJ, g.nK, nIg, nJg, nKg,
+                                     gi, gj, gk);
+  CK(cudaGetLastError());
+  CK(cudaMemcpyAsync(State_VGB, g.stageAoS, bytes, cudaMemcpyDeviceToHost, g.st));
+  CK(cudaStreamSynchronize(g.st));
+  return BX_OK;
+}
+
+int bx_set_time(double tSimulation, int nStep) {
+  NEED_READY();
+  StepState s;
+  CK(cudaMemcpyAsync(&s, g.ts, sizeof(s), cudaMemcpyDeviceToHost, g.st));
+  CK(cudaStreamSynchronize(g.st));
+  s.tSimulation = tSimulation;
+  s.nStep = nStep;
+  CK(cudaMemcpyAsync(g.ts, &s, sizeof(s), cudaMemcpyHostToDevice, g.st));
+  CK(cudaStreamSynchronize(g.st));
+  return BX_OK;
+}
+
+int bx_get_time(double *t, double *dt, int *n) {
+  NEED_READY();
+  StepState s;
+  CK(cudaMemcpyAsync(&s, g.ts, sizeof(s), cudaMemcpyDeviceToHost, g.st));
+  CK(cudaStreamSynchronize(g.st));
+  if (t) *t = s.tSimulation;
+  if (dt) *dt = s.Dt;
+  if (n) *n = s.nStep;
+  return BX_OK;
+}
+
+// ---- per-block entry points ----------------------------------------------
+int bx_calc_face_value(int iBlock, int DoResChangeOnly, int DoMonotoneRestrict) {
+  (void)DoMonotoneRestrict;  // single-level grids have no restricted ghost cells
+  if (DoResChangeOnly) return BX_OK;  // no resolution-change faces on one level
+  return compat_phase(kPhaseFaceValue, iBlock);
+}
+int bx_calc_face_flux(int DoResChangeOnly, int iBlock) {
+  if (DoResChangeOnly) return BX_OK;
+  return compat_phase(kPhaseFaceFlux, iBlock);
+}
+int bx_calc_source(int iBlock) { return compat_phase(kPhaseSource, iBlock); }
+int bx_calc_timestep(int iBlock) { return compat_phase(kPhaseTimestep, iBlock); }
+int bx_update_state(int iBlock) {
+  int r = compat_phase(kPhaseUpdate, iBlock);
+  if (r) return r;
+  g.touched[iBlock - 1] = 1;
+  g.compatPending = true;
+  return BX_OK;
+}
+int bx_get_face_values(int iDim, double *L, double *R) {
+  NEED_READY();
+  if (iDim < 0 || iDim >= g.nDim || !g.scrL[0]) return fail(BX_ERR_ARG, "no face values for iDim=%d", iDim);
+  const int nF[3] = {(g.nI + 1) * g.nJ * g.nK, g.nI * (g.nJ + 1) * g.nK, g.nI * g.nJ * (g.nK + 1)};
+  CK(cudaMemcpyAsync(L, g.scrL[iDim], sizeof(double) * 8 * nF[iDim], cudaMemcpyDeviceToHost, g.st));
+  CK(cudaMemcpyAsync(R, g.scrR[iDim], sizeof(double) * 8 * nF[iDim], cudaMemcpyDeviceToHost, g.st));
+  CK(cudaStreamSynchronize(g.st));
+  return BX_OK;
+}
+int bx_get_face_flux(int iDim, double *F) {
+  NEED_READY();
+  if (iDim < 0 || iDim >= g.nDim || !g.scrF[0]) return fail(BX_ERR_ARG, "no fluxes for iDim=%d", iDim);
+  const int nF[3] = {(g.nI + 1) * g.nJ * g.nK, g.nI * (g.nJ + 1) * g.nK, g.nI * g.nJ * (g.nK + 1)};
+  CK(cudaMemcpyAsync(F, g.scrF[iDim], sizeof(double) * 9 * nF[iDim], cudaMemcpyDeviceToHost, g.st));
+  CK(cudaStreamSynchronize(g.st));
+  return check_err_flag();
+}
+int bx_get_source(double *S) {
+  NEED_READY();
+  if (!g.scrSrc) return fail(BX_ERR_STATE, "bx_calc_source has not been called");
+  CK(cudaMemcpyAsync(S, g.scrSrc, sizeof(double) * 9 * g.nCell, cudaMemcpyDeviceToHost, g.st));
+  CK(cudaStreamSynchronize(g.st));
+  return BX_OK;
+}
+
+// ---- batched entry points --------------------------------------------------
+int bx_set_stage(int iStage) {
+  NEED_READY();
+  if (iStage < 1 || iStage > g.sch.nStage) return fail(BX_ERR_ARG, "iStage=%d", iStage);
+  g.iStage = iStage;
+  return BX_OK;
+}
+
+int bx_update_state_fast(void) {
+  NEED_READY();
+  return launch_stage(g.iStage);
+}
+
+int bx_exchange_messages(int DoResChangeOnly) {
+  NEED_READY();
+  (void)DoResChangeOnly;
+  // The fused stage kernels read neighbour interiors directly, so the ghost
+  // fill needs no separate pass.  Blocks updated through the per-block
+  // entry points become visible here (their ghost copies in the reference).
+  if (g.compatPending) {
+    std::vector<int> list;
+    for (int b = 0; b < g.nBlock; b++)
+      if (g.touched[b]) list.push_back(b);
+    int *dl = nullptr;
+    CK(cudaMalloc(&dl, sizeof(int) * list.size()));
+    CK(cudaMemcpyAsync(dl, list.data(), sizeof(int) * list.size(), cudaMemcpyHostToDevice, g.st));
+    copy_blocks<<<592, 256, 0, g.st>>>(g.A, g.Nx, dl, (int)list.size(), 8 * g.nCell);
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(g.st));
+    cudaFree(dl);
+    std::fill(g.touched.begin(), g.touched.end(), 0);
+    g.compatPending = false;
+  }
+  return BX_OK;
+}
+
+int bx_set_global_timestep(double tLimit, double *Dt) {
+  NEED_READY();
+  // DtMax_B of the blocks whose calc_timestep ran through the per-block path
+  if (g.scrDt) {
+    dtmin_from_blocks<<<1, 1024, 0, g.st>>>(g.ts, g.dtBlock, g.nBlock);
+    CK(cudaGetLastError());
+  }
+  set_dt_kernel<<<1, 1, 0, g.st>>>(g.ts, tLimit, g.sch.UseDtFixed, g.sch.DtFixed, g.sch.Cfl);
+  CK(cudaGetLastError());
+  if (Dt) {
+    StepState s;
+    CK(cudaMemcpyAsync(&s, g.ts, sizeof(s), cudaMemcpyDeviceToHost, g.st));
+    CK(cudaStreamSynchronize(g.st));
+    *Dt = s.Dt;
+  }
+  return BX_OK;
+}
+
+int bx_advance_explicit(int DoCalcTimestep) {
+  NEED_READY();
+  (void)DoCalcTimestep;
+  for (int s = 1; s <= g.sch.nStage; s++) {
+    int r = launch_stage(s);
+    if (r) return r;
+  }
+  return BX_OK;
+}
+
+int bx_advance(int nStep, double tLimit) {
+  NEED_READY();
+  if (nStep < 0) return fail(BX_ERR_ARG, "nStep=%d", nStep);
+  const bool useGraph = !g.timing && g.sch.nStage == 2;
+  if (useGraph && (!g.graph || g.graphTLimit != tLimit) && nStep > 0) {
+    // the first step of a new graph runs uncaptured, so that kernel
+    // attributes are set before capture begins
+    int r0 = launch_step(tLimit);
+    if (r0) return r0;
+    nStep--;
+    if (g.graph) { cudaGraphExecDestroy(g.graph); g.graph = nullptr; }
+    cudaGraph_t gr;
+    CK(cudaStreamBeginCapture(g.st, cudaStreamCaptureModeThreadLocal));
+    int r = launch_step(tLimit);
+    g.nLaunchTotal -= g.sch.nStage;  // captured, not launched
+    cudaError_t e = cudaStreamEndCapture(g.st, &gr);
+    if (r) return r;
+    if (e != cudaSuccess) return fail(BX_ERR_CUDA, "graph capture: %s", cudaGetErrorString(e));
+    CK(cudaGraphInstantiate(&g.graph, gr, 0));
+    cudaGraphDestroy(gr);
+    g.graphTLimit = tLimit;
+  }
+  for (int n = 0; n < nStep; n++) {
+    if (useGraph) {
+      CK(cudaGraphLaunch(g.graph, g.st));
+      g.nLaunchTotal += g.sch.nStage;
+    } else {
+      int r = launch_step(tLimit);
+      if (r) return r;
+    }
+  }
+  return check_err_flag();
+}
+
+int bx_synchronize(void) {
+  NEED_READY();
+  CK(cudaStreamSynchronize(g.st));
+  return BX_OK;
+}
+
+int bx_timing_enable(int on) {
+  NEED_READY();
+  g.timing = on != 0;
+  return BX_OK;
+}
+
+int bx_timing_get(double *msAvg, int *nLaunch, int *nLaunchTotal) {
+  NEED_READY();
+  CK(cudaStreamSynchronize(g.st));
+  double tot = 0;
+  for (int i = 0; i < g.nTimed; i++) {
+    float ms = 0;
+    CK(cudaEventElapsedTime(&ms, g.evStart[i], g.evStop[i]));
+    tot += ms;
+  }
+  if (msAvg) *msAvg = g.nTimed ? tot / g.nTimed : 0.0;
+  if (nLaunch) *nLaunch = g.nTimed;
+  if (nLaunchTotal) *nLaunchTotal = g.nLaunchTotal;
+  return BX_OK;
+}
+
+int bx_timing_reset(void) {
+  NEED_READY();
+  g.nTimed = 0;
+  g.nLaunchTotal = 0;
+  return BX_OK;
+}
+
+static cudaEvent_t g_region[2] = {nullptr, nullptr};
+
+int bx_region_begin(void) {
+  NEED_READY();
+  for (int i = 0; i < 2; i++)
+    if (!g_region[i]) CK(cudaEventCreate(&g_region[i]));
+  CK(cudaEventRecord(g_region[0], g.st));
+  return BX_OK;
+}
+
+int bx_region_end(double *ms) {
+  NEED_READY();
+  if (!g_region[0]) return fail(BX_ERR_STATE, "bx_region_begin has not been called");
+  CK(cudaEventRecord(g_region[1], g.st));
+  CK(cudaEventSynchronize(g_region[1]));
+  float t = 0;
+  CK(cudaEventElapsedTime(&t, g_region[0], g_region[1]));
+  if (ms) *ms = t;
+  return BX_OK;
+}
+
+}  // extern "C"

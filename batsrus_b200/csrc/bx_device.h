@@ -1,0 +1,73 @@
+// bx_device.h -- structures shared by the host side of libbx200 and its
+// kernels (plain C++ / CUDA, no torch types).
+#pragma once
+#include <cuda_runtime.h>
+
+namespace bx {
+
+enum { kErrHlld = 1, kErrNonPhysical = 2 };
+
+// Time-step bookkeeping kept in device memory so that whole steps can be
+// captured in a CUDA graph (set_global_timestep, src/ModTimeStepControl.f90:
+// 306-524, runs on the device).
+struct StepState {
+  double DtNoCfl;                 // DtMax_CB of every cell this step (Dt/Cfl)
+  double Dt;                      // Cfl*DtNoCfl
+  double tSimulation;
+  unsigned long long DtMinBits;   // running min of cell time steps (bits)
+  int nStep;
+  int errFlag;
+};
+
+// per-block Cartesian geometry (BATL CellSize_DB, CellVolume_B,
+// CellFace_DB = CellVolume_B/CellSize_DB)
+struct BlockGeom {
+  double cellSize[3];
+  double volume;
+  double area[3];
+  double invHalf[3];  // 0.5/CellSize (DxInvHalf of calc_divb_source)
+};
+
+struct StageArgs {
+  const void *in;          // gather source (double* or float*)
+  const double *old;       // StateOld: the step's initial state (own cells)
+  void *out;               // stage result (double* or float*)
+  const int *nbr;          // [nBlock][6] neighbour block or -1 (float BC)
+  const int *order;        // processing order (Morton) of the blocks
+  const BlockGeom *geom;   // [nBlock]
+  StepState *ts;
+  double *dtBlock;         // optional DtMax_B per block
+  int nBlock;
+  int iStage, nStage, nOrder, limiter, useDivb, useHalfStep, computeDt;
+  double beta, gamma, invGm1, cfl;
+};
+
+// per-block compatibility kernels (orig-path entry points, FP64)
+struct CompatArgs {
+  const double *state;     // current state (SoA, no ghosts)
+  const double *old;       // StateOld buffer
+  double *next;            // updated block output
+  const int *nbr;
+  const BlockGeom *geom;
+  StepState *ts;
+  double *left[3], *right[3], *flux[3];  // face scratch of one block
+  double *source;          // Source_VC scratch (9 per cell)
+  double *dtCell;          // DtMax_CB of the block (nCell)
+  double *dtBlock;         // DtMax_B
+  int iStage, nStage, nOrder, limiter, useDivb, useHalfStep;
+  double beta, gamma, invGm1, cfl;
+};
+
+// shape ids of the supported block sizes
+enum { kShape888 = 0, kShape444 = 1, kShape881 = 2, kShape811 = 3, kShape6411 = 4, kNumShape = 5 };
+
+// launchers (explicitly instantiated in bx_stage_fp64.cu / bx_stage_fp32.cu
+// / bx_compat.cu)
+cudaError_t launch_stage_fp64(int shape, int flux, const StageArgs &a, cudaStream_t st);
+// kind 0: FP64 in -> FP32 out (stage 1), kind 1: FP32 in -> FP64 out (stage 2)
+cudaError_t launch_stage_fp32(int shape, int flux, int kind, const StageArgs &a, cudaStream_t st);
+cudaError_t launch_compat(int shape, int flux, int phase, int iBlock, const CompatArgs &a,
+                          cudaStream_t st);
+enum { kPhaseFaceValue = 0, kPhaseFaceFlux = 1, kPhaseSource = 2, kPhaseUpdate = 3, kPhaseTimestep = 4 };
+
+}  // namespace bx

@@ -1,0 +1,301 @@
+// bx_physics.cuh -- device functions of the explicit ideal-MHD update.
+//
+// Single-fluid ideal MHD, nVar = 8 (srcEquation/ModEquationMhd.f90:20-35),
+// Cartesian faces, no B0.  Primitive state order in registers:
+//   0 rho, 1 ux, 2 uy, 3 uz, 4 bx, 5 by, 6 bz, 7 p
+// Flux / conservative vectors (8 slots; the reference's p flux slot is not
+// needed by the conservative energy update and is dropped):
+//   0 rho, 1 rho ux, 2 rho uy, 3 rho uz, 4 bx, 5 by, 6 bz, 7 total energy
+//
+// The formulas keep the operation order of the reference "orig" routines so
+// that the FP64 kernels (compiled without FMA contraction) agree with the
+// CPU oracle to rounding level; each function cites the routine it follows.
+#pragma once
+#include <cuda_runtime.h>
+
+namespace bx {
+
+enum { kRho = 0, kUx = 1, kUy = 2, kUz = 3, kBx = 4, kBy = 5, kBz = 6, kP = 7, kE = 7 };
+enum { kFluxRusanov = 0, kFluxLinde = 1, kFluxHlld = 2 };
+enum { kLimMinmod = 0, kLimMc = 1, kLimMc3 = 2 };
+
+template <typename R>
+__device__ __forceinline__ R sign25(R x) { return copysign(R(0.25), x); }
+
+// limiter (src/ModFaceValue.f90:3689-3791) evaluated for one face from the
+// 4-cell stencil q0=P(i-2), q1=P(i-1), q2=P(i), q3=P(i+1):
+//   LeftState  = P(i-1) + dVarLimL(i-1)     (get_facex_second :2021-2027)
+//   RightState = P(i)   - dVarLimR(i)
+template <typename R>
+__device__ __forceinline__ void limited_face(int lim, R beta, R q0, R q1, R q2, R q3,
+                                             R &left, R &right) {
+  const R a = q1 - q0, b = q2 - q1, c = q3 - q2;
+  const R sab = sign25(a) + sign25(b);
+  const R sbc = sign25(b) + sign25(c);
+  R dL, dR;
+  if (lim == kLimMinmod) {
+    dL = sab * fmin(fabs(a), fabs(b));
+    dR = sbc * fmin(fabs(b), fabs(c));
+  } else if (lim == kLimMc) {
+    dL = sab * fmin(fmin(beta * fabs(a), beta * fabs(b)), R(0.5) * fabs(a + b));
+    dR = sbc * fmin(fmin(beta * fabs(b), beta * fabs(c)), R(0.5) * fabs(b + c));
+  } else {  // mc3 (Koren): L uses |d1 + 2 d2|/3, R uses |2 d1 + d2|/3
+    const R cThird = R(1) / R(3);
+    dL = sab * fmin(fmin(beta * fabs(a), beta * fabs(b)), cThird * fabs(a + 2 * b));
+    dR = sbc * fmin(fmin(beta * fabs(b), beta * fabs(c)), cThird * fabs(2 * b + c));
+  }
+  left = q1 + dL;
+  right = q2 - dR;
+}
+
+// get_physical_flux -> get_mhd_flux -> get_magnetic_flux
+// (src/ModFaceFlux.f90:1166-1410, 1550-1617, 1619-1900)
+template <int D, typename R>
+__device__ __forceinline__ void physical_flux(const R (&S)[8], R invGm1, R (&U)[8], R (&F)[8],
+                                              R &un) {
+  const R rho = S[kRho], ux = S[kUx], uy = S[kUy], uz = S[kUz];
+  const R bx = S[kBx], by = S[kBy], bz = S[kBz], p = S[kP];
+  un = D == 0 ? ux : (D == 1 ? uy : uz);
+  const R bn = D == 0 ? bx : (D == 1 ? by : bz);
+  F[kRho] = rho * un;
+  U[kRho] = rho;
+  U[kUx] = rho * ux; U[kUy] = rho * uy; U[kUz] = rho * uz;
+  U[kBx] = bx; U[kBy] = by; U[kBz] = bz;
+  const R e = invGm1 * p + R(0.5) * rho * (ux * ux + uy * uy + uz * uz);
+  const R B2 = bx * bx + by * by + bz * bz;
+  const R pTotal = R(0.5) * B2;
+  // hydro momentum flux (un*rho)*u + p n, then the magnetic force
+  F[kUx] = un * rho * ux; F[kUy] = un * rho * uy; F[kUz] = un * rho * uz;
+  if (D == 0) F[kUx] = F[kUx] + p;
+  if (D == 1) F[kUy] = F[kUy] + p;
+  if (D == 2) F[kUz] = F[kUz] + p;
+  F[kBx] = un * bx - ux * bn;
+  F[kBy] = un * by - uy * bn;
+  F[kBz] = un * bz - uz * bn;
+  R mfx = -bn * bx, mfy = -bn * by, mfz = -bn * bz;
+  if (D == 0) mfx = mfx + pTotal;
+  if (D == 1) mfy = mfy + pTotal;
+  if (D == 2) mfz = mfz + pTotal;
+  F[kUx] = F[kUx] + mfx; F[kUy] = F[kUy] + mfy; F[kUz] = F[kUz] + mfz;
+  U[kE] = e + pTotal;
+  F[kE] = un * (e + p);
+  F[kE] = F[kE] + F[kBx] * bx + F[kBy] * by + F[kBz] * bz;
+}
+
+// get_speed_max -> get_mhd_speed (src/ModFaceFlux.f90:3545-4250): fast
+// magnetosonic speed, cmax = |un| + cf, cleft = un - cf, cright = un + cf
+template <int D, typename R>
+__device__ __forceinline__ void mhd_speed(const R (&S)[8], R gamma, R &cmax, R &cleft, R &cright) {
+  const R rho = S[kRho];
+  const R sound2 = S[kP] * gamma / rho;
+  const R un = S[kUx + D];
+  const R invRho = R(1) / rho;
+  const R alfven2 = (S[kBx] * S[kBx] + S[kBy] * S[kBy] + S[kBz] * S[kBz]) * invRho;
+  const R bn = S[kBx + D];
+  const R alfven2n = invRho * (bn * bn);
+  const R fast2 = sound2 + alfven2;
+  const R discr = sqrt(fmax(R(0), fast2 * fast2 - R(4) * sound2 * alfven2n));
+  const R fast = sqrt(R(0.5) * (fast2 + discr));
+  cmax = fabs(un) + fast;
+  cleft = un - fast;
+  cright = un + fast;
+}
+
+// hlld_flux (src/ModFaceFlux.f90:2826-3160) in the rotated frame
+// (rotate_state_vectors / rotate_flux_vector :4482-4645), B0 = 0.
+// Returns false where the reference stops (negative density ratio).
+template <int D, typename R>
+__device__ __forceinline__ bool hlld_flux(const R (&L)[8], const R (&Rt)[8], R gamma, R invGm1,
+                                          R (&F)[8], R &cmaxOut) {
+  const R cTiny = R(1.0e-6);
+  R cmL, clL, crL, cmR, clR, crR;
+  mhd_speed<D>(L, gamma, cmL, clL, crL);
+  mhd_speed<D>(Rt, gamma, cmR, clR, crR);
+  const R sL = fmin(clL, clR);
+  const R sR = fmax(crL, crR);
+  cmaxOut = fmax(sR, -sL);
+  if (sL >= R(0) || sR <= R(0)) {
+    R U[8], un;
+    physical_flux<D>(sL >= R(0) ? L : Rt, invGm1, U, F, un);
+    return true;
+  }
+  constexpr int n = D, t1 = (D + 1) % 3, t2 = (D + 2) % 3;
+  const R RhoL = L[kRho], pL = L[kP], RhoR = Rt[kRho], pR = Rt[kP];
+  const R UnL = L[kUx + n], Ut1L = L[kUx + t1], Ut2L = L[kUx + t2];
+  const R B1nL = L[kBx + n], B1t1L = L[kBx + t1], B1t2L = L[kBx + t2];
+  const R UnR = Rt[kUx + n], Ut1R = Rt[kUx + t1], Ut2R = Rt[kUx + t2];
+  const R B1nR = Rt[kBx + n], B1t1R = Rt[kBx + t1], B1t2R = Rt[kBx + t2];
+  const R B1n = R(0.5) * (B1nL + B1nR);
+  const R B1n2 = B1n * B1n;
+  const R Bn = B1n, Bn2 = Bn * Bn;
+  const R SignBn = copysign(R(1), Bn);
+  const R PbL = R(0.5) * (B1n2 + B1t1L * B1t1L + B1t2L * B1t2L);
+  const R PbR = R(0.5) * (B1n2 + B1t1R * B1t1R + B1t2R * B1t2R);
+  const R PtotL = pL + PbL, PtotR = pR + PbR;
+  const R DsL = sL - UnL, DsR = sR - UnR;
+  const R DsRhoL = DsL * RhoL, DsRhoR = DsR * RhoR;
+  R Tmp = R(1) / (DsRhoR - DsRhoL);
+  const R Un = (DsRhoR * UnR - DsRhoL * UnL - PtotR + PtotL) * Tmp;
+  const R Ptot12 = (DsRhoR * PtotL - DsRhoL * PtotR + DsRhoR * DsRhoL * (UnR - UnL)) * Tmp;
+  R Rho, Ut1, Ut2, B1t1, B1t2, uDotB1, e;
+  R Ut1L1, Ut2L1, B1t1L1, B1t2L1, Ut1R1, Ut2R1, B1t1R1, B1t2R1;
+  bool ok = true;
+  if (Un >= R(0)) {
+    const R InvSLUn = R(1) / (sL - Un);
+    Rho = DsRhoL * InvSLUn;
+    Tmp = DsRhoL * (sL - Un) - Bn2;
+    if (Tmp < cTiny) {
+      Ut1L1 = Ut1L; Ut2L1 = Ut2L; B1t1L1 = B1t1L; B1t2L1 = B1t2L;
+    } else {
+      Tmp = R(1) / Tmp;
+      Ut1L1 = Ut1L - Bn * B1t1L * (Un - UnL) * Tmp;
+      Ut2L1 = Ut2L - Bn * B1t2L * (Un - UnL) * Tmp;
+      B1t1L1 = B1t1L * (DsRhoL * DsL - Bn2) * Tmp;
+      B1t2L1 = B1t2L * (DsRhoL * DsL - Bn2) * Tmp;
+    }
+    const R eL = invGm1 * pL + PbL + R(0.5) * RhoL * (UnL * UnL + Ut1L * Ut1L + Ut2L * Ut2L);
+    const R uDotB1L = UnL * B1n + Ut1L * B1t1L + Ut2L * B1t2L;
+    const R uDotB1L1 = Un * B1n + Ut1L1 * B1t1L1 + Ut2L1 * B1t2L1;
+    e = (DsL * eL - PtotL * UnL + Ptot12 * Un + Bn * (uDotB1L - uDotB1L1)) * InvSLUn;
+    const R SqRhoL1 = sqrt(Rho);
+    const R sL1 = Un - fabs(Bn) / SqRhoL1;
+    if (sL1 >= R(0)) {
+      Ut1 = Ut1L1; Ut2 = Ut2L1; B1t1 = B1t1L1; B1t2 = B1t2L1; uDotB1 = uDotB1L1;
+    } else {
+      const R ratio = DsRhoR / (sR - Un);
+      if (ratio < R(0)) ok = false;
+      const R SqRhoR1 = sqrt(fabs(ratio));
+      Tmp = DsRhoR * (sR - Un) - Bn2;
+      if (Tmp < cTiny) {
+        Ut1R1 = Ut1R; Ut2R1 = Ut2R; B1t1R1 = B1t1R; B1t2R1 = B1t2R;
+      } else {
+        Tmp = R(1) / Tmp;
+        Ut1R1 = Ut1R - Bn * B1t1R * (Un - UnR) * Tmp;
+        Ut2R1 = Ut2R - Bn * B1t2R * (Un - UnR) * Tmp;
+        B1t1R1 = B1t1R * (DsRhoR * DsR - Bn2) * Tmp;
+        B1t2R1 = B1t2R * (DsRhoR * DsR - Bn2) * Tmp;
+      }
+      Tmp = R(1) / (SqRhoL1 + SqRhoR1);
+      const R SqRhoLR1 = SqRhoL1 * SqRhoR1 * SignBn;
+      Ut1 = (SqRhoL1 * Ut1L1 + SqRhoR1 * Ut1R1 + (B1t1R1 - B1t1L1) * SignBn) * Tmp;
+      Ut2 = (SqRhoL1 * Ut2L1 + SqRhoR1 * Ut2R1 + (B1t2R1 - B1t2L1) * SignBn) * Tmp;
+      B1t1 = (SqRhoL1 * B1t1R1 + SqRhoR1 * B1t1L1 + (Ut1R1 - Ut1L1) * SqRhoLR1) * Tmp;
+      B1t2 = (SqRhoL1 * B1t2R1 + SqRhoR1 * B1t2L1 + (Ut2R1 - Ut2L1) * SqRhoLR1) * Tmp;
+      uDotB1 = Un * B1n + Ut1 * B1t1 + Ut2 * B1t2;
+      e = e - SqRhoL1 * (uDotB1L1 - uDotB1) * SignBn;
+    }
+  } else {
+    const R InvSRUn = R(1) / (sR - Un);
+    Rho = DsRhoR * InvSRUn;
+    Tmp = DsRhoR * (sR - Un) - Bn2;
+    if (Tmp < cTiny) {
+      Ut1R1 = Ut1R; Ut2R1 = Ut2R; B1t1R1 = B1t1R; B1t2R1 = B1t2R;
+    } else {
+      Tmp = R(1) / Tmp;
+      Ut1R1 = Ut1R - Bn * B1t1R * (Un - UnR) * Tmp;
+      Ut2R1 = Ut2R - Bn * B1t2R * (Un - UnR) * Tmp;
+      B1t1R1 = B1t1R * (DsRhoR * DsR - Bn2) * Tmp;
+      B1t2R1 = B1t2R * (DsRhoR * DsR - Bn2) * Tmp;
+    }
+    const R eR = invGm1 * pR + PbR + R(0.5) * RhoR * (UnR * UnR + Ut1R * Ut1R + Ut2R * Ut2R);
+    const R uDotB1R = UnR * B1n + Ut1R * B1t1R + Ut2R * B1t2R;
+    const R uDotB1R1 = Un * B1n + Ut1R1 * B1t1R1 + Ut2R1 * B1t2R1;
+    e = (DsR * eR - PtotR * UnR + Ptot12 * Un + Bn * (uDotB1R - uDotB1R1)) * InvSRUn;
+    const R SqRhoR1 = sqrt(Rho);
+    const R sR1 = Un + fabs(Bn) / SqRhoR1;
+    if (sR1 <= R(0)) {
+      Ut1 = Ut1R1; Ut2 = Ut2R1; B1t1 = B1t1R1; B1t2 = B1t2R1; uDotB1 = uDotB1R1;
+    } else {
+      const R ratio = DsRhoL / (sL - Un);
+      if (ratio < R(0)) ok = false;
+      const R SqRhoL1 = sqrt(fabs(ratio));
+      Tmp = DsRhoL * (sL - Un) - Bn2;
+      if (Tmp < cTiny) {
+        Ut1L1 = Ut1L; Ut2L1 = Ut2L; B1t1L1 = B1t1L; B1t2L1 = B1t2L;
+      } else {
+        Tmp = R(1) / Tmp;
+        Ut1L1 = Ut1L - Bn * B1t1L * (Un - UnL) * Tmp;
+        Ut2L1 = Ut2L - Bn * B1t2L * (Un - UnL) * Tmp;
+        B1t1L1 = B1t1L * (DsRhoL * DsL - Bn2) * Tmp;
+        B1t2L1 = B1t2L * (DsRhoL * DsL - Bn2) * Tmp;
+      }
+      Tmp = R(1) / (SqRhoL1 + SqRhoR1);
+      const R SqRhoLR1 = SqRhoL1 * SqRhoR1 * SignBn;
+      Ut1 = (SqRhoL1 * Ut1L1 + SqRhoR1 * Ut1R1 + (B1t1R1 - B1t1L1) * SignBn) * Tmp;
+      Ut2 = (SqRhoL1 * Ut2L1 + SqRhoR1 * Ut2R1 + (B1t2R1 - B1t2L1) * SignBn) * Tmp;
+      B1t1 = (SqRhoL1 * B1t1R1 + SqRhoR1 * B1t1L1 + (Ut1R1 - Ut1L1) * SqRhoLR1) * Tmp;
+      B1t2 = (SqRhoL1 * B1t2R1 + SqRhoR1 * B1t2L1 + (Ut2R1 - Ut2L1) * SqRhoLR1) * Tmp;
+      uDotB1 = Un * B1n + Ut1 * B1t1 + Ut2 * B1t2;
+      e = e + SqRhoR1 * (uDotB1R1 - uDotB1) * SignBn;
+    }
+  }
+  const R RhoUn = Rho * Un;
+  F[kRho] = RhoUn;
+  F[kUx + n] = RhoUn * Un - B1n * Bn + Ptot12;
+  F[kUx + t1] = RhoUn * Ut1 - B1n * B1t1;
+  F[kUx + t2] = RhoUn * Ut2 - B1n * B1t2;
+  F[kBx + n] = R(0);
+  F[kBx + t1] = Un * B1t1 - Ut1 * Bn;
+  F[kBx + t2] = Un * B1t2 - Ut2 * Bn;
+  F[kE] = Un * (e + Ptot12) - Bn * uDotB1;
+  return ok;
+}
+
+// get_numerical_flux (src/ModFaceFlux.f90:2130-2473) for one face normal
+// to direction D.  Inputs are the reconstructed face states; outputs the
+// 8 fluxes times Area and Vdt = CmaxDt*Area.  Returns false on HLLD abort.
+template <int D, int FLUX, typename R>
+__device__ __forceinline__ bool numerical_flux(R (&L)[8], R (&Rt)[8], R gamma, R invGm1, R area,
+                                               R (&F)[8], R &vdt) {
+  R DiffBn = R(0), DiffE = R(0);
+  if (FLUX != kFluxRusanov) {
+    // UseLindeFix: remove the jump in the normal field (:2302-2320)
+    DiffBn = R(0.5) * (Rt[kBx + D] - L[kBx + D]);
+    L[kBx + D] = L[kBx + D] + DiffBn;
+    Rt[kBx + D] = Rt[kBx + D] - DiffBn;
+    DiffE = R(0.5) * ((Rt[kBx + D] + L[kBx + D]) * DiffBn);
+  }
+  R cmax;
+  bool ok = true;
+  if (FLUX == kFluxHlld) {
+    ok = hlld_flux<D>(L, Rt, gamma, invGm1, F, cmax);
+  } else {
+    R S[8];
+#pragma unroll
+    for (int v = 0; v < 8; v++) S[v] = R(0.5) * (L[v] + Rt[v]);
+    R UL[8], FL[8], UR[8], FR[8], unL, unR;
+    physical_flux<D>(L, invGm1, UL, FL, unL);
+    physical_flux<D>(Rt, invGm1, UR, FR, unR);
+    if (FLUX == kFluxRusanov) {
+      // lax_friedrichs_flux (:2513-2559), Cmax of the averaged state
+      R cl, cr;
+      mhd_speed<D>(S, gamma, cmax, cl, cr);
+#pragma unroll
+      for (int v = 0; v < 8; v++) F[v] = R(0.5) * (FL[v] + FR[v] - cmax * (UR[v] - UL[v]));
+    } else {
+      // harten_lax_vanleer_flux (:2561-2645)
+      R clHat, crHat, tmp, clL, crR;
+      mhd_speed<D>(S, gamma, cmax, clHat, crHat);
+      mhd_speed<D>(L, gamma, tmp, clL, tmp);
+      mhd_speed<D>(Rt, gamma, tmp, tmp, crR);
+      const R cleft = fmin(R(0), fmin(clL, clHat));
+      const R cright = fmax(R(0), fmax(crR, crHat));
+      const R wL = cright / (cright - cleft);
+      const R wR = R(1) - wL;
+      const R diff = cright * wR;
+#pragma unroll
+      for (int v = 0; v < 8; v++) F[v] = wR * FR[v] + wL * FL[v] - diff * (UR[v] - UL[v]);
+    }
+  }
+  if (FLUX != kFluxRusanov) {
+    // Linde's fix: Lax-Friedrichs diffusion of Bn and energy (:2403-2418)
+    F[kBx + D] = F[kBx + D] - cmax * DiffBn;
+    F[kE] = F[kE] - cmax * DiffE;
+  }
+#pragma unroll
+  for (int v = 0; v < 8; v++) F[v] = F[v] * area;
+  vdt = cmax * area;
+  return ok;
+}
+
+}  // namespace bx

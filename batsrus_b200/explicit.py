@@ -1,0 +1,150 @@
+"""Host-side mirror of the reference's explicit-update interface.
+
+``ExplicitSolver`` exposes the entry points a BATS-R-US driver calls on the
+explicit path, with the reference's names and argument meaning, on top of
+the C ABI of libbx200 (include/bx200.h):
+
+* set-up: ``init_mod_advance`` (src/ModAdvance.f90:296) -> ``__init__``;
+* per block (orig path, src/ModAdvanceExplicit.f90:140-226):
+  ``calc_face_value(iBlock, DoResChangeOnly, DoMonotoneRestrict)``,
+  ``calc_face_flux(DoResChangeOnly, iBlock)``, ``calc_source(iBlock)``,
+  ``calc_timestep(iBlock)``, ``update_state(iBlock)``;
+* batched: ``update_state_fast()`` (src/ModUpdateStateFast.f90:190),
+  ``exchange_messages()`` (src/ModMessagePass.f90:27),
+  ``set_global_timestep(TimeSimulationLimit)``
+  (src/ModTimeStepControl.f90:306), ``advance_explicit()``
+  (src/ModAdvanceExplicit.f90:18), ``advance(nStep, TimeSimulationLimit)``
+  (nStep calls of BATS_advance, src/ModBatsrusMethods.f90:493).
+
+Errors come back as :class:`batsrus_b200.capi.BxError` instead of the
+reference's ``stop_mpi`` abort.  One solver is active per process (the
+library keeps one context, like the Fortran module globals).
+"""
+import ctypes
+
+import numpy as np
+
+from . import capi
+from .capi import check, dptr
+
+
+class ExplicitSolver:
+    def __init__(self, grid, scheme, device=0):
+        self.L = capi.load()
+        self.grid = grid
+        self.scheme = scheme
+        self._gd = capi.grid_desc(grid, device)
+        self._sp = capi.scheme_params(scheme)
+        check(self.L.bx_init(ctypes.byref(self._gd), ctypes.byref(self._sp)))
+
+    def set_scheme(self, scheme):
+        """#SCHEME / #TIMESTEPPING of a new session."""
+        self.scheme = scheme
+        self._sp = capi.scheme_params(scheme)
+        check(self.L.bx_set_scheme(ctypes.byref(self._sp)))
+
+    def close(self):
+        self.L.bx_finalize()
+
+    # -- state ---------------------------------------------------------------
+    def set_state(self, State_VGB):
+        a = np.ascontiguousarray(State_VGB, dtype=np.float64)
+        assert a.shape == self.grid.state_shape_fortran(), a.shape
+        check(self.L.bx_upload_state(dptr(a), self.grid.nBlock))
+
+    def get_state(self, out=None):
+        a = out if out is not None else np.empty(self.grid.state_shape_fortran())
+        check(self.L.bx_download_state(dptr(a), self.grid.nBlock))
+        return a
+
+    def set_time(self, tSimulation, nStep):
+        check(self.L.bx_set_time(tSimulation, nStep))
+
+    def time(self):
+        t, dt, n = ctypes.c_double(), ctypes.c_double(), ctypes.c_int()
+        check(self.L.bx_get_time(ctypes.byref(t), ctypes.byref(dt), ctypes.byref(n)))
+        return t.value, dt.value, n.value
+
+    # -- per-block orig path ------------------------------------------------
+    def calc_face_value(self, iBlock, DoResChangeOnly=False, DoMonotoneRestrict=True):
+        check(self.L.bx_calc_face_value(iBlock, int(DoResChangeOnly), int(DoMonotoneRestrict)))
+
+    def calc_face_flux(self, DoResChangeOnly, iBlock):
+        check(self.L.bx_calc_face_flux(int(DoResChangeOnly), iBlock))
+
+    def calc_source(self, iBlock):
+        check(self.L.bx_calc_source(iBlock))
+
+    def calc_timestep(self, iBlock):
+        check(self.L.bx_calc_timestep(iBlock))
+
+    def update_state(self, iBlock):
+        check(self.L.bx_update_state(iBlock))
+
+    def _nface(self, iDim):
+        n = [self.grid.nI, self.grid.nJ, self.grid.nK]
+        n[iDim] += 1
+        return n
+
+    def face_values(self, iDim):
+        n = self._nface(iDim)
+        L = np.empty((n[2], n[1], n[0], 8))
+        R = np.empty_like(L)
+        check(self.L.bx_get_face_values(iDim, dptr(L), dptr(R)))
+        return L, R
+
+    def face_flux(self, iDim):
+        n = self._nface(iDim)
+        F = np.empty((n[2], n[1], n[0], 9))
+        check(self.L.bx_get_face_flux(iDim, dptr(F)))
+        return F
+
+    def source(self):
+        g = self.grid
+        S = np.empty((g.nK, g.nJ, g.nI, 9))
+        check(self.L.bx_get_source(dptr(S)))
+        return S
+
+    # -- batched path --------------------------------------------------------
+    def set_stage(self, iStage):
+        check(self.L.bx_set_stage(iStage))
+
+    def update_state_fast(self):
+        check(self.L.bx_update_state_fast())
+
+    def exchange_messages(self, DoResChangeOnly=False):
+        check(self.L.bx_exchange_messages(int(DoResChangeOnly)))
+
+    def set_global_timestep(self, TimeSimulationLimit=-1.0):
+        dt = ctypes.c_double()
+        check(self.L.bx_set_global_timestep(TimeSimulationLimit, ctypes.byref(dt)))
+        return dt.value
+
+    def advance_explicit(self, DoCalcTimestep=True):
+        check(self.L.bx_advance_explicit(int(DoCalcTimestep)))
+
+    def advance(self, nStep=1, TimeSimulationLimit=-1.0):
+        check(self.L.bx_advance(nStep, TimeSimulationLimit))
+
+    def synchronize(self):
+        check(self.L.bx_synchronize())
+
+    # -- measurement -----------------------------------------------------------
+    def timing(self, on):
+        check(self.L.bx_timing_enable(int(on)))
+
+    def timing_reset(self):
+        check(self.L.bx_timing_reset())
+
+    def region_begin(self):
+        check(self.L.bx_region_begin())
+
+    def region_end(self):
+        ms = ctypes.c_double()
+        check(self.L.bx_region_end(ctypes.byref(ms)))
+        return ms.value
+
+    def timing_get(self):
+        ms, n, ntot = ctypes.c_double(), ctypes.c_int(), ctypes.c_int()
+        check(self.L.bx_timing_get(ctypes.byref(ms), ctypes.byref(n), ctypes.byref(ntot)))
+        return ms.value, n.value, ntot.value

@@ -1,0 +1,288 @@
+"""Benchmark of the explicit MHD hot path: cell-updates/s on the 3D
+Orszag-Tang workload (256^3 cells = 32768 blocks of 8^3, Linde HLL + Koren,
+CFL 0.8, 2-stage), FP64 and FP32-bulk.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+One step = one full time step (2 fused stage launches plus the device-side
+time-step update) over all blocks.  ``value`` is device-resident throughput
+(state in HBM before the timed region, CUDA events on the library's stream,
+max over ranks); ``e2e`` runs the same steps through the C ABI from pinned
+host State_VGB (upload + K steps + download inside the timed region).
+``--impl reference`` times the CPU restatement of the reference's orig path
+(oracle/) on the host cores.  N > 1: one process per GPU, each rank advances
+its own 256^3 Orszag-Tang domain (independent replicas of the workload,
+weak scaling; the single-GPU path has no inter-rank exchange).
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "cell-updates/s FP64 vs FP32 bulk; JFNK s/step learned vs BILU precond at 1e-3"
+UNIT = "cell-updates/s"
+BYTES_PER_CELL_STEP = {"fp64": 320, "fp32": 256}  # algorithmic HBM bytes per cell and step
+WORKLOAD = "orszag_tang_3d_256cubed_linde_koren"
+
+
+def dist_env():
+    r = int(os.environ.get("RANK", "0"))
+    w = int(os.environ.get("WORLD_SIZE", "1"))
+    lr = int(os.environ.get("LOCAL_RANK", "0"))
+    return r, w, lr
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return d["hbm_gbs"], "measured"
+    return 6650.0, "fallback"
+
+
+def profile_traffic():
+    """DRAM bytes per cell and stage launch from the committed ncu summary
+    (profiles/stage_kernel_ot.md, line 'dram_bytes_per_cell_launch: X')."""
+    p = os.path.join(ROOT, "profiles", "stage_kernel_ot.md")
+    if not os.path.exists(p):
+        return None
+    for line in open(p):
+        if line.startswith("dram_bytes_per_cell_launch:"):
+            return float(line.split(":")[1])
+    return None
+
+
+class ClockSampler:
+    def __init__(self, gpu):
+        self.gpu = gpu
+        self.rows = []
+        self.proc = None
+
+    def __enter__(self):
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), "--query-gpu=" + q,
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([x.strip() for x in line.split(",")])
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        sm = [float(r[1]) for r in self.rows if len(r) > 2 and r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if len(r) > 2 and r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = set()
+        for r in self.rows:
+            for i, n in enumerate(names):
+                if len(r) > 5 + i and r[5 + i].lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(self.rows)}
+
+
+def allreduce_max(x, world):
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def run_ours(args):
+    rank, world, lrank = dist_env()
+    if world > 1:
+        import datetime
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(lrank)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    from batsrus_b200 import configs
+    from batsrus_b200.explicit import ExplicitSolver
+
+    hbm_peak, peak_kind = peaks()
+    out = {}
+    for prec in ("fp64", "fp32"):
+        g, s, st, _ = configs.orszag_tang_3d(nRoot=args.nroot, precision=prec)
+        nCell = g.nCell
+        x = ExplicitSolver(g, s, device=lrank)
+        # ---- device-resident throughput ----------------------------------
+        x.set_state(st)
+        x.advance(max(args.warmup, 3))  # includes the first Dt = 0 step
+        x.synchronize()
+        barrier(world)
+        x.timing(True)
+        x.timing_reset()
+        with ClockSampler(lrank) as clk:
+            x.region_begin()
+            x.advance(args.steps)
+            ms = x.region_end()
+        kern_ms, n_launch, n_total = x.timing_get()
+        x.timing(False)
+        barrier(world)
+        ms = allreduce_max(ms, world)
+        value = world * nCell * args.steps / (ms * 1e-3)
+        launch_bytes = BYTES_PER_CELL_STEP[prec] / 2 * nCell  # average over the 2 stages
+        achieved = launch_bytes / (kern_ms * 1e-3) / 1e9
+        t_per_cell = profile_traffic()
+        res = {"value": value, "ms_per_step": ms / args.steps, "kernel_ms": kern_ms,
+               "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": hbm_peak,
+                            "unit": "GB/s", "frac": round(achieved / hbm_peak, 4),
+                            "traffic": (t_per_cell * nCell if t_per_cell else None),
+                            "peak_source": peak_kind},
+               "clocks": clk.summary(), "gpu_launches": 4 * args.steps}
+        # ---- end to end through the C ABI with pinned host buffers ----------
+        if args.e2e:
+            import torch
+            host = torch.empty(g.state_shape_fortran(), dtype=torch.float64).pin_memory()
+            host.numpy()[...] = st
+            back = torch.empty(g.state_shape_fortran(), dtype=torch.float64).pin_memory()
+            x2 = ExplicitSolver(g, s, device=lrank)
+            x2.set_state(host.numpy())
+            x2.advance(1)
+            x2.synchronize()
+            barrier(world)
+            x2.region_begin()
+            x2.set_state(host.numpy())
+            x2.set_time(0.0, 1)  # first Dt = 0 step already taken: time the K full steps
+            x2.advance(args.steps)
+            x2.get_state(back.numpy())
+            ems = x2.region_end()
+            ems = allreduce_max(ems, world)
+            nbytes = host.numel() * 8
+            res["e2e"] = {"value": world * nCell * args.steps / (ems * 1e-3), "unit": UNIT,
+                          "h2d_bytes_per_step": nbytes / args.steps, "d2h_bytes_per_step": nbytes / args.steps,
+                          "ms": ems}
+            x2.close()
+        else:
+            x.close()
+        out[prec] = res
+    return out
+
+
+def cpu_baseline(args, seconds=12.0):
+    """The oracle (C++ restatement of the orig path, OpenMP over blocks) on a
+    64^3 Orszag-Tang sample, on all host cores, timed until ~seconds."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    from batsrus_b200 import configs
+    from oracle import Oracle
+    cores = os.cpu_count()
+    g, s, st, _ = configs.orszag_tang_3d(nRoot=8)
+    o = Oracle(g, s, n_thread=cores)
+    o.set_state(st)
+    o.exchange_messages()
+    o.advance(1)  # Dt = 0 step
+    n, t0 = 0, time.perf_counter()
+    while True:
+        o.advance(1)
+        n += 1
+        el = time.perf_counter() - t0
+        if el > seconds or n >= 40:
+            break
+    return {"value": g.nCell * n / el, "unit": UNIT, "cores": cores, "kind": "port",
+            "sample": "oracle/ C++ restatement, 64^3 Orszag-Tang (512 blocks of 8^3), Linde+Koren, "
+                      "FP64, %d full steps in %.1f s on %d threads" % (n, el, cores)}
+
+
+def run_reference(args):
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    from batsrus_b200 import configs
+    from oracle import Oracle
+    cores = os.cpu_count()
+    g, s, st, _ = configs.orszag_tang_3d(nRoot=8)
+    o = Oracle(g, s, n_thread=cores)
+    o.set_state(st)
+    o.exchange_messages()
+    o.advance(1 + args.warmup)
+    t0 = time.perf_counter()
+    o.advance(args.steps)
+    el = time.perf_counter() - t0
+    v = g.nCell * args.steps / el
+    line = {"metric": METRIC, "value": v, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": el * 1e3 / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "impl": "reference",
+            "config": {"workload": WORKLOAD, "sample": "64^3 of the 256^3 domain per step",
+                       "blocks": "8x8x8", "flux": "Linde", "limiter": "mc3 beta=1.2", "cfl": 0.8},
+            "cpu_baseline": {"value": v, "unit": UNIT, "cores": cores, "kind": "port",
+                             "sample": "oracle/ C++ restatement of the orig path, 64^3 Orszag-Tang, "
+                                       "%d steps, %d threads" % (args.steps, cores)},
+            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--nroot", type=int, default=32, help="root blocks per dimension (32 -> 256^3)")
+    ap.add_argument("--no-e2e", dest="e2e", action="store_false")
+    ap.add_argument("--no-cpu", dest="cpu", action="store_false")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        run_reference(args)
+        return
+    rank, world, _ = dist_env()
+    res = run_ours(args)
+    if rank != 0:
+        return
+    r64, r32 = res["fp64"], res["fp32"]
+    line = {"metric": METRIC, "value": r64["value"], "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": r64["ms_per_step"],
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic",
+            "config": {"workload": WORKLOAD, "cells": (8 * args.nroot) ** 3, "blocks": args.nroot ** 3,
+                       "block_cells": "8x8x8", "flux": "Linde", "limiter": "mc3 beta=1.2", "cfl": 0.8,
+                       "stages": 2, "l2": "inputs larger than L2 (state %.2f GB)" % ((8 * args.nroot) ** 3 * 64 / 1e9),
+                       "parallelism": "one domain per GPU"},
+            "roofline": r64["roofline"], "clocks": r64["clocks"], "gpu_launches": r64["gpu_launches"],
+            "fp32_bulk": {"value": r32["value"], "ms_per_step": r32["ms_per_step"], "dtype": "f32/f64",
+                          "roofline": r32["roofline"], "e2e": r32.get("e2e")}}
+    if "e2e" in r64:
+        line["e2e"] = r64["e2e"]
+    if args.cpu and world == 1:
+        line["cpu_baseline"] = cpu_baseline(args)
+    print(json.dumps(line))
+
+
+if __name__ == "__main__":
+    main()

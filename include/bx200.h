@@ -1,0 +1,165 @@
+/*
+ * bx200.h -- C ABI of the B200-native BATS-R-US hot path (libbx200.so).
+ *
+ * Plain C types only: int, double, pointers and sizes.  Every entry point
+ * returns an int status (BX_OK = 0) and never aborts the caller; the text of
+ * the last error is available from bx_last_error().
+ *
+ * State crosses the boundary in the reference's own layout,
+ * State_VGB(nVar, MinI:MaxI, MinJ:MaxJ, MinK:MaxK, nBlock) with the
+ * variable index fastest (src/ModAdvance.f90:296), ghost cells included.
+ * Inside the library the state lives in HBM as structure-of-arrays
+ * [block][var][k][j][i] without ghost cells.  Block indices are 1-based like
+ * the Fortran iBlock.
+ *
+ * One process drives one GPU; the library keeps one context per process,
+ * like the Fortran module globals it replaces.
+ */
+#ifndef BX200_H
+#define BX200_H
+
+#if defined(__GNUC__)
+#define BX_API __attribute__((visibility("default")))
+#else
+#define BX_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define BX_NVAR 8 /* Rho, RhoUx, RhoUy, RhoUz, Bx, By, Bz, p */
+
+/* status codes */
+enum {
+  BX_OK = 0,
+  BX_ERR_ARG = 1,          /* invalid argument or unsupported configuration */
+  BX_ERR_CUDA = 2,         /* CUDA runtime error (message in bx_last_error) */
+  BX_ERR_STATE = 3,        /* call out of order (e.g. before bx_init) */
+  BX_ERR_NONPHYSICAL = 4,  /* NaN, negative density or pressure found */
+  BX_ERR_HLLD = 5,         /* HLLD negative density ratio (reference aborts) */
+  BX_ERR_KRYLOV = 6,       /* Krylov solver did not converge */
+  BX_ERR_TIMEOUT = 7,      /* a bounded device wait gave up */
+  BX_ERR_NOMEM = 8         /* device allocation failed */
+};
+
+/* TypeFlux (src/ModFaceFlux.f90:396-417) */
+enum { BX_FLUX_RUSANOV = 0, BX_FLUX_LINDE = 1, BX_FLUX_HLLD = 2 };
+/* TypeLimiter (src/ModFaceValue.f90:3689-3791) */
+enum { BX_LIM_MINMOD = 0, BX_LIM_MC = 1, BX_LIM_MC3 = 2 };
+/* outer boundary types (src/ModCellBoundary.f90) */
+enum { BX_BC_FLOAT = 0, BX_BC_PERIODIC = 1 };
+/* arithmetic of the explicit update */
+enum {
+  BX_FP64 = 0,      /* FP64 everywhere, reference operation order */
+  BX_FP32_BULK = 1  /* FP32 reconstruction/fluxes/intermediate stage state,
+                       FP64 conserved-state accumulation and p recovery */
+};
+
+/* Grid: replaces the BATL tree / ModSize / ModGeometry data the Fortran
+ * path reads through module globals (src/ModBatlInterface.f90:99-253). */
+typedef struct {
+  int nDim;              /* 1, 2, 3 */
+  int nI, nJ, nK;        /* cells per block; supported: 8x8x8, 4x4x4, 8x8x1,
+                            8x1x1, 64x1x1 */
+  int nRootBlock[3];
+  double CoordMin[3], CoordMax[3];
+  int TypeBc[6];         /* BX_BC_* for x-, x+, y-, y+, z-, z+ */
+  int nBlock;
+  const int *iLevelCoord_IB; /* 4 ints per block: level, ix, iy, iz */
+  int iDevice;           /* CUDA device ordinal */
+} bx_grid_desc;
+
+/* Scheme: the #SCHEME / #TIMESTEPPING / #FIXEDTIMESTEP / #GAMMA state that
+ * the Fortran path holds in ModMain, ModFaceFlux, ModFaceValue, ModPhysics */
+typedef struct {
+  int nOrder;            /* 1 or 2 */
+  int nStage;            /* 1 or 2 */
+  int TypeFlux;          /* BX_FLUX_* */
+  int TypeLimiter;       /* BX_LIM_* */
+  double LimiterBeta;
+  double Cfl;
+  double Gamma;
+  int UseDivbSource;     /* Powell 8-wave source terms */
+  int UseHalfStep;       /* half-step 2-stage scheme (#TIMESTEPPING) */
+  int UseDtFixed;
+  double DtFixed;
+  int Precision;         /* BX_FP64 or BX_FP32_BULK */
+} bx_scheme_params;
+
+/* ---- set-up ------------------------------------------------------------ */
+/* replaces init_mod_advance + BATL set-up: allocates device state and builds
+ * the neighbour tables (src/ModAdvance.f90:296-342) */
+BX_API int bx_init(const bx_grid_desc *grid, const bx_scheme_params *scheme);
+/* #SCHEME between sessions (src/ModSetParameters.f90:1745-1779) */
+BX_API int bx_set_scheme(const bx_scheme_params *scheme);
+BX_API int bx_finalize(void);
+BX_API const char *bx_last_error(void);
+
+/* host <-> device state in the State_VGB layout; download also fills the
+ * ghost cells as exchange_messages would */
+BX_API int bx_upload_state(const double *State_VGB, int nBlock);
+BX_API int bx_download_state(double *State_VGB, int nBlock);
+BX_API int bx_set_time(double tSimulation, int nStep);
+BX_API int bx_get_time(double *tSimulation, double *Dt, int *nStep);
+
+/* ---- per-block entry points of the orig path (drop-in compatibility) ----
+ * Each works on one block and keeps its result in device scratch arrays that
+ * play the role of the module globals LeftState_V?, Flux_V?I, Source_VC. */
+/* calc_face_value (src/ModFaceValue.f90:854) */
+BX_API int bx_calc_face_value(int iBlock, int DoResChangeOnly, int DoMonotoneRestrict);
+/* calc_face_flux (src/ModFaceFlux.f90:483) */
+BX_API int bx_calc_face_flux(int DoResChangeOnly, int iBlock);
+/* calc_source (src/ModCalcSource.f90:65) */
+BX_API int bx_calc_source(int iBlock);
+/* update_state (src/ModUpdateState.f90:83); the updated block becomes
+ * visible to its neighbours at the next bx_exchange_messages */
+BX_API int bx_update_state(int iBlock);
+/* calc_timestep (src/ModTimeStepControl.f90:111) */
+BX_API int bx_calc_timestep(int iBlock);
+/* read-back of the scratch arrays of the last block processed:
+ * face values (nVar, nFace_i, nFace_j, nFace_k) of direction iDim (0,1,2),
+ * fluxes (BX_NFACEVALUE, nFace_i, nFace_j, nFace_k) and the source
+ * (nVar+1, nI, nJ, nK) with the energy source in the last slot */
+#define BX_NFACEVALUE 9 /* Rho, RhoUx, RhoUy, RhoUz, Bx, By, Bz, Energy
+                           fluxes times Area, then Vdt = CmaxDt*Area */
+BX_API int bx_get_face_values(int iDim, double *LeftState, double *RightState);
+BX_API int bx_get_face_flux(int iDim, double *Flux);
+BX_API int bx_get_source(double *Source_VC);
+
+/* ---- batched entry points ------------------------------------------------ */
+/* stage counter used by the per-block routines and update_state_fast */
+BX_API int bx_set_stage(int iStage);
+/* update_state_fast (src/ModUpdateStateFast.f90:190): one stage of all
+ * blocks in one fused kernel launch (ghost fill, reconstruction, fluxes,
+ * Powell source, update, per-block dt) */
+BX_API int bx_update_state_fast(void);
+/* exchange_messages (src/ModMessagePass.f90:27) */
+BX_API int bx_exchange_messages(int DoResChangeOnly);
+/* set_global_timestep (src/ModTimeStepControl.f90:306) */
+BX_API int bx_set_global_timestep(double TimeSimulationLimit, double *Dt);
+/* advance_explicit (src/ModAdvanceExplicit.f90:18): all stages */
+BX_API int bx_advance_explicit(int DoCalcTimestep);
+/* nStep calls of BATS_advance (src/ModBatsrusMethods.f90:493) for the
+ * explicit scheme, launched as one CUDA graph per step; with
+ * TimeSimulationLimit <= 0 there is no time limit */
+BX_API int bx_advance(int nStep, double TimeSimulationLimit);
+/* wait for the library's stream */
+BX_API int bx_synchronize(void);
+
+/* ---- measurement ----------------------------------------------------------
+ * Kernel timing with CUDA events on the library's stream: when enabled, the
+ * fused stage kernel launches are bracketed by events; the average duration
+ * of the launches since the last reset is returned in milliseconds. */
+BX_API int bx_timing_enable(int on);
+BX_API int bx_timing_get(double *ms_avg_stage_kernel, int *nLaunch, int *nLaunchTotal);
+BX_API int bx_timing_reset(void);
+/* device time of a region of library calls: events recorded on the library's
+ * stream at begin and end; the end call waits and returns milliseconds */
+BX_API int bx_region_begin(void);
+BX_API int bx_region_end(double *ms);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* BX200_H */

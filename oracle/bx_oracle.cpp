@@ -668,7 +668,7 @@ struct Oracle {
   void set_global_timestep(double tLimit) {
     if (c.useDtFixed) {
       Dt = c.dtFixed;
-    } else if (nStep < 1 || (nStep == 1 && tLimit > 0.0)) {
+    } else if (nStep <= 1) {  // TimeSimulationLimit is positive (or huge) in BATS_advance
       Dt = 0.0;
     } else {
       double DtMin = 1e300;

@@ -1,0 +1,34 @@
+"""Regenerate the golden fixtures from the reference's own test outputs.
+
+Reads the IDL ascii golden files of the reference (Param/*/TestOutput) and
+stores the columns the hot path produces as compact .npz fixtures, so that
+the tests never read the reference tree at run time.
+
+    python tests/golden/make_fixtures.py [/path/to/reference]
+"""
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(HERE, "..", ".."))
+from batsrus_b200.idl import read_idl_ascii  # noqa: E402
+
+VARS = ["Rho", "Ux", "Uy", "Uz", "Bx", "By", "Bz", "P"]
+
+
+def main(ref):
+    src = os.path.join(ref, "Param/SHOCKTUBE/TestOutput/mhdhyp_1d_ref.out")
+    d = read_idl_ascii(src)
+    cols = [d["varnames"].index(v) for v in VARS]
+    np.savez_compressed(os.path.join(HERE, "mhdhyp_1d_ref.npz"),
+                        x=d["coord"][:, 0], prim=d["var"][:, cols], names=np.array(VARS),
+                        nStep=d["nStep"], time=d["time"], gamma=d["params"][0],
+                        source="Param/SHOCKTUBE/TestOutput/mhdhyp_1d_ref.out",
+                        tolerance_rel=1e-5, tolerance_abs=1e-11)
+    print("wrote mhdhyp_1d_ref.npz", d["var"].shape)
+
+
+if __name__ == "__main__":
+    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")

@@ -1,0 +1,94 @@
+"""The CPU oracle against the reference's golden output and basic invariants
+(test infrastructure check, no GPU)."""
+import os
+
+import numpy as np
+import pytest
+
+from batsrus_b200 import configs, initial
+from batsrus_b200.grid import BlockGrid
+from batsrus_b200.param import Scheme
+from oracle import Oracle
+
+GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
+
+
+def _prim(state):
+    p = state.copy()
+    p[..., 1:4] /= p[..., 0:1]
+    return p
+
+
+def test_oracle_matches_reference_shocktube_1d_golden():
+    """Param/SHOCKTUBE/TestOutput/mhdhyp_1d_ref.out (Makefile.test:293-323):
+    512 first-order Rusanov steps, DiffNum tolerance -r=1e-5 -a=1e-11."""
+    ref = np.load(os.path.join(GOLDEN, "mhdhyp_1d_ref.npz"))
+    g, s, st, run = configs.shocktube_1d_golden()
+    o = Oracle(g, s)
+    o.set_state(st)
+    o.exchange_messages()
+    o.advance(run["nStep"], run["tSimulationMax"])
+    t, dt, n = o.time()
+    assert n == 512 and abs(t - 25.6) < 1e-9
+    S = o.get_state()[g.interior_slices()].reshape(-1, 8)
+    x = g.cell_centers(with_ghost=False)[..., 0].reshape(-1)
+    order = np.argsort(x)
+    np.testing.assert_allclose(x[order], ref["x"], rtol=0, atol=1e-9)
+    prim = _prim(S[order])
+    d = np.abs(prim - ref["prim"])
+    tol = ref["tolerance_abs"] + ref["tolerance_rel"] * np.abs(ref["prim"])
+    assert (d <= tol).all(), "max violation %g" % (d / tol).max()
+    # the golden file prints 11 significant digits: agreement is at that level
+    assert d.max() < 1e-10
+
+
+def test_oracle_conserves_on_periodic_grid():
+    """Total mass, momentum, B and energy are conserved to rounding on a
+    periodic grid (flux form; the Powell source is not conservative, so it is
+    switched off here)."""
+    g, s, st, _ = configs.uniform_3d_case(2, "Linde", nCellBlock=(4, 4, 4))
+    s.useDivbSource = False
+    o = Oracle(g, s)
+    o.set_state(st)
+    o.exchange_messages()
+
+    def totals():
+        S = o.get_state()[g.interior_slices()]
+        e = S[..., 7] / (s.gamma - 1) + 0.5 * (S[..., 1:4] ** 2).sum(-1) / S[..., 0] + 0.5 * (S[..., 4:7] ** 2).sum(-1)
+        return np.concatenate([S[..., :7].sum(axis=(0, 1, 2, 3)), [e.sum()]])
+
+    t0 = totals()
+    o.advance(4)
+    t1 = totals()
+    scale = np.abs(t0).max()
+    assert np.abs(t1 - t0).max() < 1e-12 * scale * 64
+
+
+@pytest.mark.parametrize("flux", ["Rusanov", "Linde", "HLLD"])
+def test_oracle_uniform_state_is_steady(flux):
+    """A uniform state must stay exactly uniform for every flux."""
+    g = BlockGrid.uniform(3, (4, 4, 4), (2, 2, 2), (0, 0, 0), (1, 1, 1), ("periodic",) * 6)
+    s = Scheme(typeFlux=flux, typeLimiter="mc3", limiterBeta=1.2)
+    st = initial.uniform(g, [1.0, 0.3, -0.2, 0.1, 0.5, 0.2, -0.4, 0.7])
+    o = Oracle(g, s)
+    o.set_state(st)
+    o.exchange_messages()
+    o.advance(3)
+    S = o.get_state()[g.interior_slices()]
+    ref = st[g.interior_slices()]
+    assert np.abs(S - ref).max() < 1e-13
+
+
+def test_oracle_brio_wu_runs_to_time_limit():
+    g, s, st, run = configs.brio_wu_1d()
+    o = Oracle(g, s)
+    o.set_state(st)
+    o.exchange_messages()
+    n = 0
+    while o.time()[0] < run["tSimulationMax"] and n < 10000:
+        o.advance(1, run["tSimulationMax"])
+        n += 1
+    t, dt, nstep = o.time()
+    assert abs(t - 0.1) < 1e-12
+    S = o.get_state()[g.interior_slices()].reshape(-1, 8)
+    assert np.isfinite(S).all() and (S[:, 0] > 0).all() and (S[:, 7] > 0).all()
