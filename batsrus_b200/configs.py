@@ -39,12 +39,12 @@ def brio_wu_1d(nBlock=32):
 
 
 def orszag_tang_3d(nRoot=32, precision="fp64", flux="Linde", limiter="mc3", beta=1.2,
-                   nCellBlock=(8, 8, 8), order="x"):
+                   nCellBlock=(8, 8, 8), order="x", with_state=True):
     g = BlockGrid.uniform(3, nCellBlock, (nRoot,) * 3, (0.0, 0.0, 0.0), (1.0, 1.0, 1.0),
                           ("periodic",) * 6, order=order)
     s = Scheme(nOrder=2, nStage=2, typeFlux=flux, typeLimiter=limiter, limiterBeta=beta, cfl=0.8,
                gamma=5.0 / 3.0, useDivbSource=True, useHalfStep=True, precision=precision)
-    st = initial.orszag_tang_3d(g)
+    st = initial.orszag_tang_3d(g) if with_state else None
     return g, s, st, {"nStep": 20}
 
 

@@ -1,0 +1,157 @@
+! bx200_interface.f90 -- ISO_C_BINDING interface of libbx200 (bx200.h).
+!
+! A BATS-R-US build adds this module and calls the bx_* functions from
+! ModAdvanceExplicit / ModBatsrusMethods in place of the explicit update.
+! Logical flags cross as integers (0/1); iBlock is the Fortran block index;
+! State_VGB is passed as is (real(8), nVar fastest, ghost cells included).
+! Every function returns an integer status (0 = success); the message of a
+! failure is returned by bx_last_error.
+!
+! This file is not compiled in the repository's own build or tests (no
+! Fortran compiler is installed where they run).
+module bx200_interface
+
+  use, intrinsic :: iso_c_binding, only: c_int, c_double, c_ptr, c_char
+
+  implicit none
+
+  integer(c_int), parameter:: BX_FLUX_RUSANOV = 0, BX_FLUX_LINDE = 1, &
+       BX_FLUX_HLLD = 2
+  integer(c_int), parameter:: BX_LIM_MINMOD = 0, BX_LIM_MC = 1, BX_LIM_MC3 = 2
+  integer(c_int), parameter:: BX_BC_FLOAT = 0, BX_BC_PERIODIC = 1
+  integer(c_int), parameter:: BX_FP64 = 0, BX_FP32_BULK = 1
+
+  type, bind(C):: bx_grid_desc
+     integer(c_int):: nDim, nI, nJ, nK
+     integer(c_int):: nRootBlock(3)
+     real(c_double):: CoordMin(3), CoordMax(3)
+     integer(c_int):: TypeBc(6)
+     integer(c_int):: nBlock
+     type(c_ptr)   :: iLevelCoord_IB   ! c_loc of integer(c_int) (4,nBlock)
+     integer(c_int):: iDevice
+  end type bx_grid_desc
+
+  type, bind(C):: bx_scheme_params
+     integer(c_int):: nOrder, nStage, TypeFlux, TypeLimiter
+     real(c_double):: LimiterBeta, Cfl, Gamma
+     integer(c_int):: UseDivbSource, UseHalfStep, UseDtFixed
+     real(c_double):: DtFixed
+     integer(c_int):: Precision
+  end type bx_scheme_params
+
+  interface
+     integer(c_int) function bx_init(Grid, Scheme) bind(C, name='bx_init')
+       import:: c_int, bx_grid_desc, bx_scheme_params
+       type(bx_grid_desc), intent(in):: Grid
+       type(bx_scheme_params), intent(in):: Scheme
+     end function bx_init
+
+     integer(c_int) function bx_set_scheme(Scheme) bind(C, name='bx_set_scheme')
+       import:: c_int, bx_scheme_params
+       type(bx_scheme_params), intent(in):: Scheme
+     end function bx_set_scheme
+
+     integer(c_int) function bx_finalize() bind(C, name='bx_finalize')
+       import:: c_int
+     end function bx_finalize
+
+     type(c_ptr) function bx_last_error() bind(C, name='bx_last_error')
+       import:: c_ptr
+     end function bx_last_error
+
+     integer(c_int) function bx_upload_state(State_VGB, nBlock) &
+          bind(C, name='bx_upload_state')
+       import:: c_int, c_double
+       real(c_double), intent(in):: State_VGB(*)
+       integer(c_int), value:: nBlock
+     end function bx_upload_state
+
+     integer(c_int) function bx_download_state(State_VGB, nBlock) &
+          bind(C, name='bx_download_state')
+       import:: c_int, c_double
+       real(c_double), intent(out):: State_VGB(*)
+       integer(c_int), value:: nBlock
+     end function bx_download_state
+
+     integer(c_int) function bx_calc_face_value(iBlock, DoResChangeOnly, &
+          DoMonotoneRestrict) bind(C, name='bx_calc_face_value')
+       import:: c_int
+       integer(c_int), value:: iBlock, DoResChangeOnly, DoMonotoneRestrict
+     end function bx_calc_face_value
+
+     integer(c_int) function bx_calc_face_flux(DoResChangeOnly, iBlock) &
+          bind(C, name='bx_calc_face_flux')
+       import:: c_int
+       integer(c_int), value:: DoResChangeOnly, iBlock
+     end function bx_calc_face_flux
+
+     integer(c_int) function bx_calc_source(iBlock) &
+          bind(C, name='bx_calc_source')
+       import:: c_int
+       integer(c_int), value:: iBlock
+     end function bx_calc_source
+
+     integer(c_int) function bx_update_state(iBlock) &
+          bind(C, name='bx_update_state')
+       import:: c_int
+       integer(c_int), value:: iBlock
+     end function bx_update_state
+
+     integer(c_int) function bx_calc_timestep(iBlock) &
+          bind(C, name='bx_calc_timestep')
+       import:: c_int
+       integer(c_int), value:: iBlock
+     end function bx_calc_timestep
+
+     integer(c_int) function bx_set_stage(iStage) bind(C, name='bx_set_stage')
+       import:: c_int
+       integer(c_int), value:: iStage
+     end function bx_set_stage
+
+     integer(c_int) function bx_update_state_fast() &
+          bind(C, name='bx_update_state_fast')
+       import:: c_int
+     end function bx_update_state_fast
+
+     integer(c_int) function bx_exchange_messages(DoResChangeOnly) &
+          bind(C, name='bx_exchange_messages')
+       import:: c_int
+       integer(c_int), value:: DoResChangeOnly
+     end function bx_exchange_messages
+
+     integer(c_int) function bx_set_global_timestep(TimeSimulationLimit, Dt) &
+          bind(C, name='bx_set_global_timestep')
+       import:: c_int, c_double
+       real(c_double), value:: TimeSimulationLimit
+       real(c_double), intent(out):: Dt
+     end function bx_set_global_timestep
+
+     integer(c_int) function bx_advance_explicit(DoCalcTimestep) &
+          bind(C, name='bx_advance_explicit')
+       import:: c_int
+       integer(c_int), value:: DoCalcTimestep
+     end function bx_advance_explicit
+
+     integer(c_int) function bx_advance(nStep, TimeSimulationLimit) &
+          bind(C, name='bx_advance')
+       import:: c_int, c_double
+       integer(c_int), value:: nStep
+       real(c_double), value:: TimeSimulationLimit
+     end function bx_advance
+
+     integer(c_int) function bx_get_time(tSimulation, Dt, nStep) &
+          bind(C, name='bx_get_time')
+       import:: c_int, c_double
+       real(c_double), intent(out):: tSimulation, Dt
+       integer(c_int), intent(out):: nStep
+     end function bx_get_time
+
+     integer(c_int) function bx_set_time(tSimulation, nStep) &
+          bind(C, name='bx_set_time')
+       import:: c_int, c_double
+       real(c_double), value:: tSimulation
+       integer(c_int), value:: nStep
+     end function bx_set_time
+  end interface
+
+end module bx200_interface
