@@ -23,9 +23,10 @@ UNITS = [
     ("bx_stage_fp64.cu", ["--fmad=false"]),
     ("bx_compat.cu", ["--fmad=false"]),
     ("bx_stage_fp32.cu", []),
+    ("bx_stage3d.cu", []),
     ("bx_capi.cu", []),
 ]
-HEADERS = ["bx_physics.cuh", "bx_stage.cuh", "bx_device.h"]
+HEADERS = ["bx_physics.cuh", "bx_stage.cuh", "bx_device.h", "bx_stage3d.cuh", "bx_tma.cuh"]
 
 
 def _sources_newer(target, deps):

@@ -53,6 +53,11 @@ struct Ctx {
   cudaStream_t st = nullptr;
   cudaGraphExec_t graph = nullptr;
   double graphTLimit = 0;
+  // TMA tensor maps of the two state buffers (3D shapes)
+  bool use3d = false;
+  int nSM = 148;
+  double *bufX = nullptr, *bufY = nullptr;  // the original A and B allocations
+  TmaMaps mapX64, mapY64, mapY32;
   // timing
   bool timing = false;
   std::vector<cudaEvent_t> evStart, evStop;
@@ -195,6 +200,40 @@ __global__ void copy_blocks(double *dst, const double *src, const int *blocks, i
 }
 
 // -------------------------------------------------------------------------
+// TMA tensor maps: the state [block][var][k][j][i] as a 5D tensor with the
+// interior box and the three ghost-slab boxes of bx_stage3d.cuh
+typedef CUresult (*EncodeTiledFn)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
+                                  const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
+                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+int encode_maps(void *base, bool fp32, int N, int nBlock, TmaMaps &m) {
+  static EncodeTiledFn encode = nullptr;
+  if (!encode) {
+    void *fn = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    CK(cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q));
+    if (!fn || q != cudaDriverEntryPointSuccess) return fail(BX_ERR_CUDA, "cuTensorMapEncodeTiled unavailable");
+    encode = (EncodeTiledFn)fn;
+  }
+  const cuuint64_t e = fp32 ? 4 : 8;
+  const cuuint64_t dims[5] = {(cuuint64_t)N, (cuuint64_t)N, (cuuint64_t)N, 8, (cuuint64_t)nBlock};
+  const cuuint64_t strides[4] = {N * e, N * N * e, (cuuint64_t)N * N * N * e, 8ull * N * N * N * e};
+  const cuuint32_t hx = (cuuint32_t)(16 / e);
+  const cuuint32_t boxes[4][5] = {{(cuuint32_t)N, (cuuint32_t)N, (cuuint32_t)N, 8, 1},
+                                  {hx, (cuuint32_t)N, (cuuint32_t)N, 8, 1},
+                                  {(cuuint32_t)N, 2, (cuuint32_t)N, 8, 1},
+                                  {(cuuint32_t)N, (cuuint32_t)N, 2, 8, 1}};
+  const cuuint32_t estr[5] = {1, 1, 1, 1, 1};
+  CUtensorMap *out[4] = {&m.in, &m.xh, &m.yh, &m.zh};
+  for (int q = 0; q < 4; q++) {
+    CUresult r = encode(out[q], fp32 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 5, base,
+                        dims, strides, boxes[q], estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                        CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) return fail(BX_ERR_CUDA, "cuTensorMapEncodeTiled failed (%d) for box %d", (int)r, q);
+  }
+  return BX_OK;
+}
+
 void free_all() {
   if (g.graph) { cudaGraphExecDestroy(g.graph); g.graph = nullptr; }
   for (double **p : {&g.A, &g.B, &g.Nx, &g.Ox, &g.stageAoS, &g.dtBlock, &g.scrSrc, &g.scrDt}) {
@@ -265,8 +304,25 @@ int launch_stage(int iStage) {
     CK(cudaEventRecord(g.evStart[g.nTimed], g.st));
   }
   cudaError_t e;
-  if (g.sch.Precision == BX_FP64) e = launch_stage_fp64(g.shape, g.sch.TypeFlux, a, g.st);
-  else e = launch_stage_fp32(g.shape, g.sch.TypeFlux, iStage == 1 ? 0 : 1, a, g.st);
+  if (g.use3d) {
+    int kind;
+    const TmaMaps *m;
+    if (g.sch.Precision == BX_FP64) {
+      kind = kKindFp64;
+      m = a.in == g.bufX ? &g.mapX64 : &g.mapY64;
+    } else if (iStage == 1) {
+      kind = kKindFp32In64;
+      m = &g.mapX64;
+    } else {
+      kind = kKindFp32In32;
+      m = &g.mapY32;
+    }
+    e = launch_stage3d(g.shape, g.sch.TypeFlux, kind, *m, a, g.nSM, g.st);
+  } else if (g.sch.Precision == BX_FP64) {
+    e = launch_stage_fp64(g.shape, g.sch.TypeFlux, a, g.st);
+  } else {
+    e = launch_stage_fp32(g.shape, g.sch.TypeFlux, iStage == 1 ? 0 : 1, a, g.st);
+  }
   if (e != cudaSuccess) return fail(BX_ERR_CUDA, "stage kernel launch: %s", cudaGetErrorString(e));
   if (g.timing) { CK(cudaEventRecord(g.evStop[g.nTimed], g.st)); g.nTimed++; }
   g.nLaunchTotal++;
@@ -433,6 +489,16 @@ int bx_init(const bx_grid_desc *gd, const bx_scheme_params *sp) {
   }
   CK(cudaMemsetAsync(g.A, 0, stBytes, g.st));
   CK(cudaMemsetAsync(g.B, 0, stBytes, g.st));
+  g.bufX = g.A;
+  g.bufY = g.B;
+  g.use3d = g.shape == kShape888 || g.shape == kShape444;
+  if (g.use3d) {
+    CK(cudaDeviceGetAttribute(&g.nSM, cudaDevAttrMultiProcessorCount, g.dev));
+    r = encode_maps(g.bufX, false, g.nI, g.nBlock, g.mapX64);
+    if (!r) r = encode_maps(g.bufY, false, g.nI, g.nBlock, g.mapY64);
+    if (!r) r = encode_maps(g.bufY, true, g.nI, g.nBlock, g.mapY32);
+    if (r) { free_all(); return r; }
+  }
   CK(cudaMalloc(&g.nbr, sizeof(int) * 6 * g.nBlock));
   CK(cudaMalloc(&g.order, sizeof(int) * g.nBlock));
   CK(cudaMalloc(&g.geom, sizeof(BlockGeom) * g.nBlock));

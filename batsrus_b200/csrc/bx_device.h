@@ -1,11 +1,12 @@
 // bx_device.h -- structures shared by the host side of libbx200 and its
 // kernels (plain C++ / CUDA, no torch types).
 #pragma once
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 namespace bx {
 
-enum { kErrHlld = 1, kErrNonPhysical = 2 };
+enum { kErrHlld = 1, kErrNonPhysical = 2, kErrTimeout = 4 };
 
 // Time-step bookkeeping kept in device memory so that whole steps can be
 // captured in a CUDA graph (set_global_timestep, src/ModTimeStepControl.f90:
@@ -68,6 +69,14 @@ cudaError_t launch_stage_fp64(int shape, int flux, const StageArgs &a, cudaStrea
 cudaError_t launch_stage_fp32(int shape, int flux, int kind, const StageArgs &a, cudaStream_t st);
 cudaError_t launch_compat(int shape, int flux, int phase, int iBlock, const CompatArgs &a,
                           cudaStream_t st);
+// persistent TMA-staged kernel of 3D shapes (bx_stage3d.cu): tensor maps of
+// the stage input for the interior box and the x, y, z ghost slabs
+struct alignas(64) TmaMaps {
+  CUtensorMap in, xh, yh, zh;
+};
+enum { kKindFp64 = 0, kKindFp32In64 = 1, kKindFp32In32 = 2 };
+cudaError_t launch_stage3d(int shape, int flux, int kind, const TmaMaps &maps, const StageArgs &a, int nSM,
+                           cudaStream_t st);
 enum { kPhaseFaceValue = 0, kPhaseFaceFlux = 1, kPhaseSource = 2, kPhaseUpdate = 3, kPhaseTimestep = 4 };
 
 }  // namespace bx

@@ -298,4 +298,104 @@ __device__ __forceinline__ bool numerical_flux(R (&L)[8], R (&Rt)[8], R gamma, R
   return ok;
 }
 
+// ---------------------------------------------------------------------------
+// Register-light flux for the fused 3D kernel.  Same mathematics as
+// numerical_flux (get_numerical_flux with lax_friedrichs_flux /
+// harten_lax_vanleer_flux and Linde's fix), written component by component
+// so that only the two face states and a few scalars are live, with one
+// division per wave-speed evaluation.  The results agree with the
+// reference-order functions above to rounding level.
+
+// fast magnetosonic speeds of state S normal to D (get_mhd_speed)
+template <int D, typename R>
+__device__ __forceinline__ void mhd_speed_lean(R rho, R un, R bn, R B2, R p, R gamma, R &fast,
+                                               R &unOut) {
+  const R invRho = R(1) / rho;
+  const R sound2 = gamma * p * invRho;
+  const R alfven2 = B2 * invRho;
+  const R alfven2n = invRho * (bn * bn);
+  const R fast2 = sound2 + alfven2;
+  const R discr = sqrt(fmax(R(0), fast2 * fast2 - R(4) * sound2 * alfven2n));
+  fast = sqrt(R(0.5) * (fast2 + discr));
+  unOut = un;
+}
+
+// Writes the 8 fluxes times area to out[v*ostride] and returns Vdt.
+template <int D, int FLUX, typename R>
+__device__ __forceinline__ R flux_lean(R (&L)[8], R (&Rt)[8], R gamma, R invGm1, R area, R *out,
+                                       int ostride) {
+  constexpr int bn = kBx + D, un = kUx + D;
+  R dBn = R(0), dE = R(0);
+  if (FLUX != kFluxRusanov) {
+    dBn = R(0.5) * (Rt[bn] - L[bn]);
+    L[bn] = L[bn] + dBn;
+    Rt[bn] = Rt[bn] - dBn;
+    dE = R(0.5) * ((Rt[bn] + L[bn]) * dBn);
+  }
+  const R B2L = L[kBx] * L[kBx] + L[kBy] * L[kBy] + L[kBz] * L[kBz];
+  const R B2R = Rt[kBx] * Rt[kBx] + Rt[kBy] * Rt[kBy] + Rt[kBz] * Rt[kBz];
+  // averaged state speed (Cmax of lax_friedrichs / hat state of HLL)
+  R cmax, wL, wR, dif;
+  {
+    const R rhoA = R(0.5) * (L[kRho] + Rt[kRho]);
+    const R unA = R(0.5) * (L[un] + Rt[un]);
+    const R bnA = R(0.5) * (L[bn] + Rt[bn]);
+    const R bxA = R(0.5) * (L[kBx] + Rt[kBx]), byA = R(0.5) * (L[kBy] + Rt[kBy]),
+            bzA = R(0.5) * (L[kBz] + Rt[kBz]);
+    const R pA = R(0.5) * (L[kP] + Rt[kP]);
+    R fastA, u;
+    mhd_speed_lean<D>(rhoA, unA, bnA, bxA * bxA + byA * byA + bzA * bzA, pA, gamma, fastA, u);
+    cmax = fabs(unA) + fastA;
+    if (FLUX == kFluxRusanov) {
+      wL = R(0.5); wR = R(0.5); dif = R(0.5) * cmax;
+    } else {
+      R fastL, fastR, uL, uR;
+      mhd_speed_lean<D>(L[kRho], L[un], L[bn], B2L, L[kP], gamma, fastL, uL);
+      mhd_speed_lean<D>(Rt[kRho], Rt[un], Rt[bn], B2R, Rt[kP], gamma, fastR, uR);
+      const R cleft = fmin(R(0), fmin(uL - fastL, unA - fastA));
+      const R cright = fmax(R(0), fmax(uR + fastR, unA + fastA));
+      wL = cright / (cright - cleft);
+      wR = R(1) - wL;
+      dif = cright * wR;
+    }
+  }
+  const R unL = L[un], unR = Rt[un];
+  const R bnL = L[bn], bnR = Rt[bn];
+  const R ptL = R(0.5) * B2L, ptR = R(0.5) * B2R;
+  const R eL = invGm1 * L[kP] + R(0.5) * L[kRho] * (L[kUx] * L[kUx] + L[kUy] * L[kUy] + L[kUz] * L[kUz]);
+  const R eR = invGm1 * Rt[kP] + R(0.5) * Rt[kRho] * (Rt[kUx] * Rt[kUx] + Rt[kUy] * Rt[kUy] + Rt[kUz] * Rt[kUz]);
+  // rho
+  const R mL = L[kRho] * unL, mR = Rt[kRho] * unR;
+  out[0] = area * (wR * mR + wL * mL - dif * (Rt[kRho] - L[kRho]));
+  // momentum
+#pragma unroll
+  for (int c = 0; c < 3; c++) {
+    R fl = mL * L[kUx + c] - bnL * L[kBx + c];
+    R fr = mR * Rt[kUx + c] - bnR * Rt[kBx + c];
+    if (c == D) { fl = fl + L[kP] + ptL; fr = fr + Rt[kP] + ptR; }
+    out[(1 + c) * ostride] =
+        area * (wR * fr + wL * fl - dif * (Rt[kRho] * Rt[kUx + c] - L[kRho] * L[kUx + c]));
+  }
+  // induction and energy (Poynting flux uses the induction fluxes)
+  R poyL = R(0), poyR = R(0);
+#pragma unroll
+  for (int c = 0; c < 3; c++) {
+    const R fl = unL * L[kBx + c] - L[kUx + c] * bnL;
+    const R fr = unR * Rt[kBx + c] - Rt[kUx + c] * bnR;
+    poyL = poyL + fl * L[kBx + c];
+    poyR = poyR + fr * Rt[kBx + c];
+    R f = wR * fr + wL * fl - dif * (Rt[kBx + c] - L[kBx + c]);
+    if (FLUX != kFluxRusanov && c == D) f = f - cmax * dBn;
+    out[(4 + c) * ostride] = area * f;
+  }
+  {
+    const R fl = unL * (eL + L[kP]) + poyL;
+    const R fr = unR * (eR + Rt[kP]) + poyR;
+    R f = wR * fr + wL * fl - dif * ((eR + ptR) - (eL + ptL));
+    if (FLUX != kFluxRusanov) f = f - cmax * dE;
+    out[7 * ostride] = area * f;
+  }
+  return area * cmax;
+}
+
 }  // namespace bx

@@ -1,0 +1,349 @@
+// bx_stage3d.cuh -- persistent, TMA-staged fused stage kernel for 3D blocks.
+//
+// One CUDA block per SM loops over the grid's blocks in Morton order.  While
+// block n is being computed, its successor's halo tile is already streaming
+// into the second shared-memory buffer through TMA bulk-tensor loads
+// (one interior box plus one box per neighbour face, completion counted on
+// an mbarrier).  For each direction every face is handled by one thread:
+// limited reconstruction from the tile, then the flux of
+// flux_lean/hlld_flux written to a shared flux buffer; each thread then sums
+// the flux divergence of its own cell.  The update (Powell source, p<->E,
+// conservative update) and the per-block time step follow as in
+// stage_kernel (bx_stage.cuh).
+//
+// Tile layout per buffer (TileT = stage input type, variables outermost):
+//   IN [8][NK][NJ][NI]   interior (conservative on arrival, primitive after)
+//   XL, XH [8][NK][NJ][HX]  x ghost layers, HX = 16 bytes / sizeof(TileT)
+//   YL, YH [8][NK][2][NI]   y ghost layers
+//   ZL, ZH [8][2][NJ][NI]   z ghost layers
+// A float (outer) boundary has no TMA box; its ghost cells are copies of the
+// boundary cell (src/ModCellBoundary.f90:518-559).
+#pragma once
+#include <cuda.h>
+
+#include "bx_device.h"
+#include "bx_physics.cuh"
+#include "bx_tma.cuh"
+
+namespace bx {
+
+template <int N_, typename TileT>
+struct Tile3 {
+  static constexpr int N = N_;
+  static constexpr int NC = N * N * N;
+  static constexpr int HX = 16 / (int)sizeof(TileT);
+  static constexpr int nIN = 8 * NC;
+  static constexpr int nX = 8 * N * N * HX;
+  static constexpr int nY = 8 * N * 2 * N;
+  static constexpr int nZ = 8 * 2 * N * N;
+  // element offsets of the regions (each a multiple of 128 bytes)
+  static constexpr int oIN = 0, oXL = oIN + nIN, oXH = oXL + nX, oYL = oXH + nX, oYH = oYL + nY,
+                       oZL = oYH + nY, oZH = oZL + nZ, nAll = oZH + nZ;
+  static constexpr int NF = (N + 1) * N * N;             // faces per direction
+  static constexpr int NTHR = ((NF + 31) / 32) * 32;     // one face per thread
+  static constexpr int NHALO_CELLS = (nAll - nIN) / 8;   // ghost cells in the tile
+  static constexpr int NCELLS = NC + NHALO_CELLS;
+  static constexpr int CPT = (NCELLS + NTHR - 1) / NTHR; // conversion cells per thread
+  static constexpr uint32_t bytesIN = sizeof(TileT) * nIN, bytesX = sizeof(TileT) * nX,
+                            bytesY = sizeof(TileT) * nY, bytesZ = sizeof(TileT) * nZ;
+  static constexpr int NSLOT = 10;  // 8 fluxes, Vdt, BnL+BnR
+  template <typename Real>
+  static constexpr size_t smem_bytes() {
+    return 2 * sizeof(TileT) * (size_t)nAll + sizeof(Real) * (size_t)NSLOT * NF + 64;
+  }
+};
+
+// tile element of variable v at cell (i,j,k); at most one coordinate may be
+// outside [0,N) (by 1 or 2 cells)
+template <class T, typename TileT>
+__device__ __forceinline__ int tile_index(int v, int i, int j, int k) {
+  constexpr int N = T::N, HX = T::HX;
+  if (i < 0) return T::oXL + ((v * N + k) * N + j) * HX + (HX + i);
+  if (i >= N) return T::oXH + ((v * N + k) * N + j) * HX + (i - N);
+  if (j < 0) return T::oYL + ((v * N + k) * 2 + (j + 2)) * N + i;
+  if (j >= N) return T::oYH + ((v * N + k) * 2 + (j - N)) * N + i;
+  if (k < 0) return T::oZL + ((v * 2 + (k + 2)) * N + j) * N + i;
+  if (k >= N) return T::oZH + ((v * 2 + (k - N)) * N + j) * N + i;
+  return T::oIN + ((v * N + k) * N + j) * N + i;
+}
+
+// decode the c-th cell of the tile (interior first, then the ghost regions)
+// into its (i,j,k) and the cell whose value it takes: itself, or for a float
+// boundary the boundary cell of the block
+template <class T, typename TileT>
+__device__ __forceinline__ void tile_cell(int c, const int *nb, int &i, int &j, int &k, int &si,
+                                          int &sj, int &sk) {
+  constexpr int N = T::N, HX = T::HX;
+  if (c < T::NC) {
+    i = c % N; j = (c / N) % N; k = c / (N * N);
+    si = i; sj = j; sk = k;
+    return;
+  }
+  c -= T::NC;
+  const int nx = N * N * HX, ny = N * 2 * N, nz = 2 * N * N;
+  int side;
+  if (c < 2 * nx) {
+    side = c / nx; c %= nx;
+    const int h = c % HX; j = (c / HX) % N; k = c / (HX * N);
+    i = side == 0 ? h - HX : N + h;
+  } else if ((c -= 2 * nx) < 2 * ny) {
+    side = 2 + c / ny; c %= ny;
+    i = c % N; const int l = (c / N) % 2; k = c / (2 * N);
+    j = side == 2 ? l - 2 : N + l;
+  } else {
+    c -= 2 * ny;
+    side = 4 + c / nz; c %= nz;
+    i = c % N; j = (c / N) % N; const int l = c / (N * N);
+    k = side == 4 ? l - 2 : N + l;
+  }
+  si = i; sj = j; sk = k;
+  if (nb[side] < 0) {  // float boundary: copy of the boundary cell
+    if (side == 0) si = 0;
+    if (side == 1) si = N - 1;
+    if (side == 2) sj = 0;
+    if (side == 3) sj = N - 1;
+    if (side == 4) sk = 0;
+    if (side == 5) sk = N - 1;
+  }
+}
+
+// issue the TMA loads of block b's tile into buf; returns the byte count
+template <class T, typename TileT>
+__device__ __forceinline__ void issue_tile(const TmaMaps &maps, TileT *buf, uint64_t *bar, const int *nbr,
+                                           int b) {
+  constexpr int N = T::N, HX = T::HX;
+  int nb[6];
+  uint32_t bytes = T::bytesIN;
+#pragma unroll
+  for (int s = 0; s < 6; s++) {
+    nb[s] = nbr[6 * b + s];
+    if (nb[s] >= 0) bytes += s < 2 ? T::bytesX : (s < 4 ? T::bytesY : T::bytesZ);
+  }
+  mbar_arrive_expect_tx(bar, bytes);
+  tma_load_5d(buf + T::oIN, &maps.in, bar, 0, 0, 0, 0, b);
+  if (nb[0] >= 0) tma_load_5d(buf + T::oXL, &maps.xh, bar, N - HX, 0, 0, 0, nb[0]);
+  if (nb[1] >= 0) tma_load_5d(buf + T::oXH, &maps.xh, bar, 0, 0, 0, 0, nb[1]);
+  if (nb[2] >= 0) tma_load_5d(buf + T::oYL, &maps.yh, bar, 0, N - 2, 0, 0, nb[2]);
+  if (nb[3] >= 0) tma_load_5d(buf + T::oYH, &maps.yh, bar, 0, 0, 0, 0, nb[3]);
+  if (nb[4] >= 0) tma_load_5d(buf + T::oZL, &maps.zh, bar, 0, 0, N - 2, 0, nb[4]);
+  if (nb[5] >= 0) tma_load_5d(buf + T::oZH, &maps.zh, bar, 0, 0, 0, 0, nb[5]);
+}
+
+template <class T, int D>
+__device__ __forceinline__ void face_ijk(int f, int &i, int &j, int &k) {
+  constexpr int N = T::N;
+  if (D == 0) { i = f % (N + 1); j = (f / (N + 1)) % N; k = f / ((N + 1) * N); }
+  else if (D == 1) { i = f % N; j = (f / N) % (N + 1); k = f / (N * (N + 1)); }
+  else { i = f % N; j = (f / N) % N; k = f / (N * N); }
+}
+
+template <class T, int D>
+__device__ __forceinline__ int face_id(int i, int j, int k) {
+  constexpr int N = T::N;
+  if (D == 0) return i + (N + 1) * (j + N * k);
+  if (D == 1) return i + N * (j + (N + 1) * k);
+  return i + N * (j + N * k);
+}
+
+// one direction: faces (one per thread) then the cell sums
+template <class T, int D, int FLUX, typename TileT, typename Real>
+__device__ __forceinline__ void sweep3(const StageArgs &a, const BlockGeom &g, const TileT *tile, Real *fbuf,
+                                       double (&chg)[8], double &divB, double &vdt, int &err) {
+  const int t = threadIdx.x;
+  if (t < T::NF) {
+    int i, j, k;
+    face_ijk<T, D>(t, i, j, k);
+    int idx[4];
+#pragma unroll
+    for (int m = 0; m < 4; m++)
+      idx[m] = tile_index<T, TileT>(0, i - (D == 0) * (2 - m), j - (D == 1) * (2 - m), k - (D == 2) * (2 - m));
+    // variable stride of each stencil cell's region
+    int vs[4];
+#pragma unroll
+    for (int m = 0; m < 4; m++)
+      vs[m] = tile_index<T, TileT>(1, i - (D == 0) * (2 - m), j - (D == 1) * (2 - m), k - (D == 2) * (2 - m)) - idx[m];
+    Real L[8], R[8];
+    const Real beta = (Real)a.beta;
+#pragma unroll
+    for (int v = 0; v < 8; v++) {
+      const Real q0 = (Real)tile[idx[0] + v * vs[0]], q1 = (Real)tile[idx[1] + v * vs[1]];
+      const Real q2 = (Real)tile[idx[2] + v * vs[2]], q3 = (Real)tile[idx[3] + v * vs[3]];
+      if (a.nOrder == 1) { L[v] = q1; R[v] = q2; }
+      else limited_face(a.limiter, beta, q0, q1, q2, q3, L[v], R[v]);
+    }
+    fbuf[9 * T::NF + t] = L[kBx + D] + R[kBx + D];
+    const Real area = (Real)g.area[D];
+    if (FLUX == kFluxHlld) {
+      Real F[8], v;
+      if (!numerical_flux<D, FLUX>(L, R, (Real)a.gamma, (Real)a.invGm1, area, F, v)) err = 1;
+#pragma unroll
+      for (int q = 0; q < 8; q++) fbuf[q * T::NF + t] = F[q];
+      fbuf[8 * T::NF + t] = v;
+    } else {
+      fbuf[8 * T::NF + t] = flux_lean<D, FLUX>(L, R, (Real)a.gamma, (Real)a.invGm1, area, fbuf + t, T::NF);
+    }
+  }
+  __syncthreads();
+  if (t < T::NC) {
+    const int i = t % T::N, j = (t / T::N) % T::N, k = t / (T::N * T::N);
+    const int f0 = face_id<T, D>(i, j, k);
+    const int f1 = face_id<T, D>(i + (D == 0), j + (D == 1), k + (D == 2));
+#pragma unroll
+    for (int v = 0; v < 8; v++) {
+      const double d = (double)fbuf[v * T::NF + f0] - (double)fbuf[v * T::NF + f1];
+      chg[v] = D == 0 ? d : chg[v] + d;
+    }
+    // div B from the face normal field, (L+R)/2 differences over the cell
+    const double db = g.invHalf[D] * ((double)fbuf[9 * T::NF + f1] - (double)fbuf[9 * T::NF + f0]);
+    divB = D == 0 ? db : divB + db;
+    const double vm = fmax((double)fbuf[8 * T::NF + f0], (double)fbuf[8 * T::NF + f1]);
+    vdt = D == 0 ? vm : vdt + vm;
+  }
+  __syncthreads();
+}
+
+template <class T, typename TileT, typename Real, typename OutT, int FLUX>
+__global__ void __launch_bounds__(T::NTHR, 1)
+    stage3d_kernel(const __grid_constant__ TmaMaps maps, const StageArgs a) {
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  TileT *buf0 = reinterpret_cast<TileT *>(smem_raw);
+  TileT *buf1 = buf0 + T::nAll;
+  Real *fbuf = reinterpret_cast<Real *>(buf1 + T::nAll);
+  __shared__ uint64_t bar[2];
+  __shared__ double wmin[32];
+  __shared__ int sTimeout;
+  const int t = threadIdx.x;
+  const int nIter = a.nBlock > (int)blockIdx.x ? (a.nBlock - 1 - (int)blockIdx.x) / (int)gridDim.x + 1 : 0;
+  if (t == 0) {
+    mbar_init(&bar[0], 1);
+    mbar_init(&bar[1], 1);
+    fence_mbar_init();
+    sTimeout = 0;
+  }
+  __syncthreads();
+  if (t == 0 && nIter > 0) issue_tile<T, TileT>(maps, buf0, &bar[0], a.nbr, a.order[blockIdx.x]);
+
+  const StepState &ts = *a.ts;
+  const double DtNoCfl = ts.DtNoCfl;
+  const double DtFactor = a.useHalfStep ? (a.cfl * a.iStage) / a.nStage : a.cfl;
+  const double DtLocal = DtFactor * DtNoCfl;
+  const double invGm1 = a.invGm1, gm1 = a.gamma - 1.0;
+  int err = 0;
+
+  for (int it = 0; it < nIter; it++) {
+    const int b = a.order[blockIdx.x + it * gridDim.x];
+    TileT *tile = (it & 1) ? buf1 : buf0;
+    if (!mbar_wait_bounded(&bar[it & 1], (uint32_t)((it >> 1) & 1))) sTimeout = 1;
+    __syncthreads();
+    if (sTimeout) break;  // uniform: every thread read the flag after the barrier
+    // prefetch the next block into the other buffer (freed at the end of the
+    // previous iteration)
+    if (t == 0 && it + 1 < nIter) {
+      fence_proxy_async_smem();
+      issue_tile<T, TileT>(maps, (it & 1) ? buf0 : buf1, &bar[(it + 1) & 1], a.nbr,
+                           a.order[blockIdx.x + (it + 1) * gridDim.x]);
+    }
+    int nb[6];
+#pragma unroll
+    for (int s = 0; s < 6; s++) nb[s] = a.nbr[6 * b + s];
+    const BlockGeom g = a.geom[b];
+
+    // calc_primitives, in two passes (read all, then write) because float
+    // boundary ghosts read interior cells that are converted in place
+    {
+      TileT prim[T::CPT][8];
+#pragma unroll
+      for (int m = 0; m < T::CPT; m++) {
+        const int c = t + m * T::NTHR;
+        if (c < T::NCELLS) {
+          int i, j, k, si, sj, sk;
+          tile_cell<T, TileT>(c, nb, i, j, k, si, sj, sk);
+          const int s0 = tile_index<T, TileT>(0, si, sj, sk);
+          const int sv = tile_index<T, TileT>(1, si, sj, sk) - s0;
+#pragma unroll
+          for (int v = 0; v < 8; v++) prim[m][v] = tile[s0 + v * sv];
+          const TileT rhoInv = TileT(1) / prim[m][kRho];
+          prim[m][kUx] = rhoInv * prim[m][kUx];
+          prim[m][kUy] = rhoInv * prim[m][kUy];
+          prim[m][kUz] = rhoInv * prim[m][kUz];
+        }
+      }
+      __syncthreads();
+#pragma unroll
+      for (int m = 0; m < T::CPT; m++) {
+        const int c = t + m * T::NTHR;
+        if (c < T::NCELLS) {
+          int i, j, k, si, sj, sk;
+          tile_cell<T, TileT>(c, nb, i, j, k, si, sj, sk);
+          const int d0 = tile_index<T, TileT>(0, i, j, k);
+          const int dv = tile_index<T, TileT>(1, i, j, k) - d0;
+#pragma unroll
+          for (int v = 0; v < 8; v++) tile[d0 + v * dv] = prim[m][v];
+        }
+      }
+      __syncthreads();
+    }
+
+    double chg[8], divB = 0, vdt = 0;
+    sweep3<T, 0, FLUX, TileT, Real>(a, g, tile, fbuf, chg, divB, vdt, err);
+    sweep3<T, 1, FLUX, TileT, Real>(a, g, tile, fbuf, chg, divB, vdt, err);
+    sweep3<T, 2, FLUX, TileT, Real>(a, g, tile, fbuf, chg, divB, vdt, err);
+
+    // update_state_normal / update_explicit for the thread's cell
+    double dtmin = 1e300;
+    if (t < T::NC) {
+      const double *old = a.old + (size_t)b * 8 * T::NC;
+      OutT *out = reinterpret_cast<OutT *>(a.out) + (size_t)b * 8 * T::NC;
+      double o[8];
+#pragma unroll
+      for (int v = 0; v < 8; v++) o[v] = old[v * T::NC + t];
+      if (a.computeDt) dtmin = g.volume / vdt;
+      if (DtNoCfl == 0.0) {
+#pragma unroll
+        for (int v = 0; v < 8; v++) out[v * T::NC + t] = (OutT)o[v];
+      } else {
+        double src[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+        if (a.useDivb) {
+          const int ii = t % T::N, jj = (t / T::N) % T::N, kk = t / (T::N * T::N);
+          const int c0 = tile_index<T, TileT>(0, ii, jj, kk);
+          const double ux = tile[c0 + kUx * T::NC], uy = tile[c0 + kUy * T::NC], uz = tile[c0 + kUz * T::NC];
+          const double bx = tile[c0 + kBx * T::NC], by = tile[c0 + kBy * T::NC], bz = tile[c0 + kBz * T::NC];
+          src[kBx] = -divB * ux; src[kBy] = -divB * uy; src[kBz] = -divB * uz;
+          src[kE] = -divB * (bx * ux + by * uy + bz * uz);
+          src[kUx] = -divB * bx; src[kUy] = -divB * by; src[kUz] = -divB * bz;
+        }
+        const double invV = 1.0 / g.volume;
+        double e = invGm1 * o[kP] + 0.5 * (o[kUx] * o[kUx] + o[kUy] * o[kUy] + o[kUz] * o[kUz]) / o[kRho];
+        e = e + 0.5 * (o[kBx] * o[kBx] + o[kBy] * o[kBy] + o[kBz] * o[kBz]);
+        double n[8];
+#pragma unroll
+        for (int v = 0; v < 7; v++) n[v] = o[v] + DtLocal * (src[v] + chg[v] * invV);
+        e = e + DtLocal * (src[kE] + chg[kE] * invV);
+        const double p = e - 0.5 * (n[kBx] * n[kBx] + n[kBy] * n[kBy] + n[kBz] * n[kBz]);
+        n[kP] = gm1 * (p - 0.5 * (n[kUx] * n[kUx] + n[kUy] * n[kUy] + n[kUz] * n[kUz]) / n[kRho]);
+#pragma unroll
+        for (int v = 0; v < 8; v++) out[v * T::NC + t] = (OutT)n[v];
+      }
+    }
+    if (a.computeDt) {
+      for (int off = 16; off > 0; off >>= 1) dtmin = fmin(dtmin, __shfl_xor_sync(0xffffffffu, dtmin, off));
+      if ((t & 31) == 0) wmin[t >> 5] = dtmin;
+      __syncthreads();
+      if (t == 0) {
+        double m = wmin[0];
+        for (int w = 1; w < T::NTHR / 32; w++) m = fmin(m, wmin[w]);
+        if (a.dtBlock) a.dtBlock[b] = m;
+        atomicMin(&a.ts->DtMinBits, (unsigned long long)__double_as_longlong(m));
+      }
+    }
+    __syncthreads();  // the tile buffer is refilled by the next-but-one prefetch
+  }
+  if (err) atomicOr(&a.ts->errFlag, kErrHlld);
+  if (t == 0 && sTimeout) {
+    atomicOr(&a.ts->errFlag, kErrTimeout);
+    // let loads already in flight land before the CTA exits (bounded)
+    for (int q = 0; q < 2; q++) mbar_wait_bounded(&bar[q], 0);
+  }
+}
+
+}  // namespace bx
