@@ -62,6 +62,7 @@ struct Oracle {
   double tSimulation = 0, Dt = 0;
   int nStep = 0, iStage = 1;
   int nFace[3][3];  // face array extents per direction
+  void *implPtr = nullptr;  // Implicit solver state (see below)
 
   long cell(int i, int j, int k) const {
     return (i - MinI) + (long)nIg * ((j - MinJ) + (long)nJg * (k - MinK));
@@ -716,6 +717,569 @@ struct Oracle {
   }
 };
 
+// ---------------------------------------------------------------------
+// Full implicit JFNK step (src/ModPartImplicit.f90:322-814) with BILU-
+// preconditioned restarted GMRES.  The implicit variables are the
+// conservative state with total energy in the pressure slot
+// (UseImplicitEnergy, :29), normalised by Norm_V.  The linear solver of the
+// absent share/Library ModLinearSolver is restated from the standard
+// algorithms: flexible restarted GMRES with modified Gram-Schmidt and right
+// preconditioning, and block ILU(0) on the 8x8 blocks of the 7-point
+// Jacobian of each grid block (block-Jacobi across blocks).
+struct Implicit {
+  Oracle &o;
+  ora_impl_config c;
+  long nCellTot = 0, N = 0;
+  std::vector<double> Impl, ImplOld, ResExpl, ResImpl, Rhs, X, Work, dtCell;
+  std::vector<double> Jac;   // [cell][stencil 7][iVar][jVar]
+  std::vector<double> Dinv;  // [cell][8][8] inverse pivots of BILU
+  double Norm[8];
+  double DtNoCfl = 0, Dt = 0, DtMinNext = 0, DtPrev = 0, ImplCoeff = 1, DtCoeff = 1;
+  int nStepPrev = -100;
+  int nMatvec = 0;
+  double errRel = 0;
+  bool havePrec = false;
+
+  explicit Implicit(Oracle &oo, const ora_impl_config &cc) : o(oo), c(cc) {
+    nCellTot = (long)o.nBlock * o.c.nI * o.c.nJ * o.c.nK;
+    N = nCellTot * nVar;
+    for (auto *v : {&Impl, &ImplOld, &ResExpl, &ResImpl, &Rhs, &X, &Work}) v->assign(N, 0.0);
+    dtCell.assign(nCellTot, 0.0);
+  }
+  long nC() const { return (long)o.c.nI * o.c.nJ * o.c.nK; }
+
+  // explicit2implicit: p -> E (pressure_to_energy)
+  void p2e(const double *S, double *U) const {
+    for (int v = 0; v < nVar; v++) U[v] = S[v];
+    U[P_] = o.InvGammaMinus1 * S[P_] + 0.5 * (S[RhoUx_] * S[RhoUx_] + S[RhoUy_] * S[RhoUy_] + S[RhoUz_] * S[RhoUz_]) / S[Rho_];
+    U[P_] = U[P_] + 0.5 * (S[Bx_] * S[Bx_] + S[By_] * S[By_] + S[Bz_] * S[Bz_]);
+  }
+  // implicit2explicit: E -> p (energy_to_pressure_cell)
+  void e2p(const double *U, double *S) const {
+    for (int v = 0; v < nVar; v++) S[v] = U[v];
+    double p = U[P_] - 0.5 * (U[Bx_] * U[Bx_] + U[By_] * U[By_] + U[Bz_] * U[Bz_]);
+    S[P_] = o.GammaMinus1 * (p - 0.5 * (U[RhoUx_] * U[RhoUx_] + U[RhoUy_] * U[RhoUy_] + U[RhoUz_] * U[RhoUz_]) / U[Rho_]);
+  }
+  void state_to_impl(std::vector<double> &U) {
+    const int nI = o.c.nI, nJ = o.c.nJ, nK = o.c.nK;
+    for (int b = 0; b < o.nBlock; b++)
+      for (int k = 1; k <= nK; k++)
+        for (int j = 1; j <= nJ; j++)
+          for (int i = 1; i <= nI; i++)
+            p2e(o.st(b, i, j, k), &U[nVar * (o.icell(i, j, k) + nC() * b)]);
+  }
+  void impl_to_state(const std::vector<double> &U) {
+    const int nI = o.c.nI, nJ = o.c.nJ, nK = o.c.nK;
+    for (int b = 0; b < o.nBlock; b++)
+      for (int k = 1; k <= nK; k++)
+        for (int j = 1; j <= nJ; j++)
+          for (int i = 1; i <= nI; i++)
+            e2p(&U[nVar * (o.icell(i, j, k) + nC() * b)], o.st(b, i, j, k));
+    o.exchange_messages();
+  }
+
+  // get_residual (src/ModPartImplicit.f90:2064-2162): one explicit stage
+  // with Cfl = 0.5, returned as the increment of the implicit variables.
+  // The high-order call (with the time step) uses DtMax_CB = Dt/Cfl of
+  // set_global_timestep and then leaves the cell time steps of
+  // calc_timestep in DtMax_CB, which the later low-order calls use.
+  void residual(const std::vector<double> &U, bool lowOrder, std::vector<double> &Res) {
+    impl_to_state(U);
+    const int nOrderSave = o.c.nOrder, fluxSave = o.c.typeFlux;
+    if (lowOrder) {
+      o.c.nOrder = c.nOrderImpl;
+      if (c.typeFluxImpl >= 0) o.c.typeFlux = c.typeFluxImpl;
+    }
+    const long nc = nC();
+    double dtmin = 1e300;
+#pragma omp parallel for schedule(dynamic, 4) num_threads((int)o.scr.size()) reduction(min : dtmin)
+    for (int b = 0; b < o.nBlock; b++) {
+      int t = 0;
+#ifdef _OPENMP
+      t = omp_get_thread_num();
+#endif
+      Scratch &s = o.scr[t];
+      o.calc_face_value(b, s);
+      o.calc_face_flux(b, s);
+      o.calc_source(b, s);
+      const double V = o.cellVolume(b);
+      for (int k = 1; k <= o.c.nK; k++)
+        for (int j = 1; j <= o.c.nJ; j++)
+          for (int i = 1; i <= o.c.nI; i++) {
+            const long cc = o.icell(i, j, k) + nc * b;
+            const double DtLocal = 0.5 * (lowOrder ? dtCell[cc] : DtNoCfl);
+            const double *Src = &s.Source[(nVar + 1) * o.icell(i, j, k)];
+            const double *fx0 = &s.Flux[0][nFaceValue * o.face(0, i, j, k)];
+            const double *fx1 = &s.Flux[0][nFaceValue * o.face(0, i + 1, j, k)];
+            const double *fy0 = o.c.nJ > 1 ? &s.Flux[1][nFaceValue * o.face(1, i, j, k)] : nullptr;
+            const double *fy1 = o.c.nJ > 1 ? &s.Flux[1][nFaceValue * o.face(1, i, j + 1, k)] : nullptr;
+            const double *fz0 = o.c.nK > 1 ? &s.Flux[2][nFaceValue * o.face(2, i, j, k)] : nullptr;
+            const double *fz1 = o.c.nK > 1 ? &s.Flux[2][nFaceValue * o.face(2, i, j, k + 1)] : nullptr;
+            double *R = &Res[nVar * cc];
+            for (int v = 0; v < nVar; v++) {
+              const int vf = v == P_ ? Energy_ : v;  // energy in the pressure slot
+              double sum = fx0[vf] - fx1[vf];
+              if (fy0) sum = sum + fy0[vf] - fy1[vf];
+              if (fz0) sum = sum + fz0[vf] - fz1[vf];
+              R[v] = DtLocal * (Src[vf] + sum / V);
+            }
+          }
+      if (!lowOrder) {
+        o.calc_timestep(b, s);
+        for (long m = 0; m < nc; m++) dtCell[m + nc * b] = o.DtMax_CB[m + nc * b];
+        dtmin = std::min(dtmin, o.DtMax_B[b]);
+      }
+    }
+    if (!lowOrder) DtMinNext = dtmin;
+    o.c.nOrder = nOrderSave;
+    o.c.typeFlux = fluxSave;
+  }
+
+  // impl_matvec_free (src/ModPartImplicit.f90:1144-1248):
+  // y = (1 + c) x - c/eps (R(U + eps x Norm) + eps x Norm - ResImpl)/Norm,
+  // eps = sqrt(JacobianEps)/rms(x), c = ImplCoeff*DtCoeff
+  void matvec(const double *x, double *y) {
+    double xn = 0;
+    for (long n = 0; n < N; n++) xn += x[n] * x[n];
+    xn = std::sqrt(xn / N);
+    if (xn < 1e-300) xn = 1.0;  // SmallDouble
+    const double Eps = std::sqrt(c.jacobianEps) / xn;
+    std::vector<double> Ueps(N), Reps(N);
+    for (long n = 0; n < N; n++) Ueps[n] = Impl[n] + Eps * x[n] * Norm[n % nVar];
+    residual(Ueps, true, Reps);
+    // ImplEps = U + eps x Norm + R(U + eps x Norm) (get_residual without subtract)
+    const double Coef1 = 1 + ImplCoeff * DtCoeff;
+    const double Coef2 = ImplCoeff * DtCoeff / Eps;
+    for (long n = 0; n < N; n++) {
+      const double implEps = Ueps[n] + Reps[n];
+      y[n] = Coef1 * x[n] - Coef2 * (implEps - Impl[n] - ResImpl[n]) / Norm[n % nVar];
+    }
+    nMatvec++;
+  }
+
+  // conservative_to_primitive (src/ModPartImplicit.f90:2344-2380)
+  void cons_to_prim(const double *U, double *P) const {
+    for (int v = 0; v < nVar; v++) P[v] = U[v];
+    const double InvRho = 1.0 / U[Rho_];
+    P[P_] = o.GammaMinus1 * (U[P_] - 0.5 * (U[RhoUx_] * U[RhoUx_] + U[RhoUy_] * U[RhoUy_] + U[RhoUz_] * U[RhoUz_]) * InvRho);
+    P[P_] = P[P_] - 0.5 * o.GammaMinus1 * (U[Bx_] * U[Bx_] + U[By_] * U[By_] + U[Bz_] * U[Bz_]);
+    P[RhoUx_] = U[RhoUx_] * InvRho;
+    P[RhoUy_] = U[RhoUy_] * InvRho;
+    P[RhoUz_] = U[RhoUz_] * InvRho;
+  }
+  // get_face_flux (:2206-2280): physical flux of a cell state times Area,
+  // energy flux in the pressure slot
+  void cell_flux(const double *U, int d, double area, double *F8) const {
+    double P[nVar], Cons[nFlux], F[nFlux], un;
+    cons_to_prim(U, P);
+    o.physical_flux(P, d, Cons, F, un);
+    for (int v = 0; v < nVar; v++) F8[v] = (v == P_ ? F[Energy_] : F[v]) * area;
+  }
+
+  // impl_jacobian (src/ModPartImplicit.f90:1250-1860) for block b: the
+  // 7-point stencil of 8x8 blocks of I - dt ImplCoeff Norm_j/Norm_i dR/dU
+  // for the first-order Rusanov residual with frozen face Cmax, plus the
+  // Powell source terms (impl_divbsrc_init / impl_divbsrc_middle).
+  void jacobian(int b) {
+    const int nI = o.c.nI, nJ = o.c.nJ, nK = o.c.nK, nDim = o.c.nDim;
+    const int n[3] = {nI, nJ, nK};
+    const long nc = nC();
+    const double Eps = std::sqrt(c.jacobianEps);
+    const double V = o.cellVolume(b);
+    // implicit state with one ghost layer: p2e of State_VGB
+    auto U = [&](int i, int j, int k, double *out) { p2e(o.st(b, i, j, k), out); };
+    double *J = &Jac[(size_t)nc * b * 7 * 64];
+    std::fill(J, J + nc * 7 * 64, 0.0);
+    auto Jat = [&](long cell, int s, int iv, int jv) -> double & { return J[((cell * 7 + s) * 8 + iv) * 8 + jv]; };
+    std::vector<double> F0((size_t)nc * 8), Feps((size_t)nc * 8), Ucell((size_t)nc * 8);
+    for (int k = 1; k <= nK; k++)
+      for (int j = 1; j <= nJ; j++)
+        for (int i = 1; i <= nI; i++) U(i, j, k, &Ucell[8 * o.icell(i, j, k)]);
+    // DivB_C and sPowell (impl_divbsrc_init, Cartesian)
+    std::vector<double> DivB(nc, 0.0), sPow((size_t)nc * 8, 0.0);
+    if (o.c.useDivbSource) {
+      for (int k = 1; k <= nK; k++)
+        for (int j = 1; j <= nJ; j++)
+          for (int i = 1; i <= nI; i++) {
+            double a[8], bb[8];
+            U(i + 1, j, k, a); U(i - 1, j, k, bb);
+            double dv = (a[Bx_] - bb[Bx_]) / o.dxyz[3 * b];
+            if (nJ > 1) { U(i, j + 1, k, a); U(i, j - 1, k, bb); dv = dv + (a[By_] - bb[By_]) / o.dxyz[3 * b + 1]; }
+            if (nK > 1) { U(i, j, k + 1, a); U(i, j, k - 1, bb); dv = dv + (a[Bz_] - bb[Bz_]) / o.dxyz[3 * b + 2]; }
+            const long cc = o.icell(i, j, k);
+            DivB[cc] = 0.5 * dv;
+            const double *u = &Ucell[8 * cc];
+            double *sp = &sPow[8 * cc];
+            for (int m = 0; m < 3; m++) sp[RhoUx_ + m] = u[Bx_ + m];
+            for (int m = 0; m < 3; m++) sp[Bx_ + m] = u[RhoUx_ + m] / u[Rho_];
+            sp[P_] = (u[Bx_] * u[RhoUx_] + u[By_] * u[RhoUy_] + u[Bz_] * u[RhoUz_]) / u[Rho_];
+          }
+    }
+    // face Cmax of each direction (get_cmax_face), scaled by -0.5
+    std::vector<double> CmaxDF[3];
+    for (int d = 0; d < nDim; d++) {
+      int nf[3] = {nI, nJ, nK};
+      nf[d] += 1;
+      CmaxDF[d].assign((size_t)nf[0] * nf[1] * nf[2], 0.0);
+      for (int k = 1; k <= nf[2]; k++)
+        for (int j = 1; j <= nf[1]; j++)
+          for (int i = 1; i <= nf[0]; i++) {
+            double a[8], bb[8], avg[8], P[8];
+            U(i, j, k, a);
+            U(i - (d == 0), j - (d == 1), k - (d == 2), bb);
+            for (int v = 0; v < 8; v++) avg[v] = 0.5 * (a[v] + bb[v]);
+            cons_to_prim(avg, P);
+            double cm, cl, cr;
+            o.speed(P, d, cm, cl, cr);
+            CmaxDF[d][(i - 1) + (long)nf[0] * ((j - 1) + (long)nf[1] * (k - 1))] = -0.5 * cm;
+          }
+    }
+    auto cmaxAt = [&](int d, int i, int j, int k) {  // face (i,j,k) 1-based of direction d
+      int nf[3] = {nI, nJ, nK};
+      nf[d] += 1;
+      return CmaxDF[d][(i - 1) + (long)nf[0] * ((j - 1) + (long)nf[1] * (k - 1))];
+    };
+    for (int d = 0; d < nDim; d++) {
+      const double area = o.cellFace(b, d);
+      for (long m = 0; m < nc; m++) cell_flux(&Ucell[8 * m], d, area, &F0[8 * m]);
+      for (int jv = 0; jv < 8; jv++) {
+        const double Coeff0 = Eps * Norm[jv];
+        for (long m = 0; m < nc; m++) {
+          double ue[8];
+          for (int v = 0; v < 8; v++) ue[v] = Ucell[8 * m + v];
+          ue[jv] = Ucell[8 * m + jv] + Coeff0;
+          cell_flux(ue, d, area, &Feps[8 * m]);
+        }
+        const double CoeffPow = -0.5 / o.dxyz[3 * b + d];
+        for (int iv = 0; iv < 8; iv++) {
+          const double Coeff = -0.5 / (Eps * Norm[jv]);
+          for (int k = 1; k <= nK; k++)
+            for (int j = 1; j <= nJ; j++)
+              for (int i = 1; i <= nI; i++) {
+                const long cc = o.icell(i, j, k);
+                const double dF = Coeff * (Feps[8 * cc + iv] - F0[8 * cc + iv]);
+                // dFdWLeft at the cell's upper face, dFdWRight at its lower face
+                double left = dF, right = dF;
+                if (iv == jv) {
+                  left = left + cmaxAt(d, i + (d == 0), j + (d == 1), k + (d == 2));
+                  right = right - cmaxAt(d, i, j, k);
+                }
+                left = left / V;
+                right = right / V;
+                Jat(cc, 0, iv, jv) = Jat(cc, 0, iv, jv) - right + left;
+              }
+          // off-diagonal entries need dFdWLeft at face c (from cell c-1) and
+          // dFdWRight at face c+1 (from cell c+1)
+          for (int k = 1; k <= nK; k++)
+            for (int j = 1; j <= nJ; j++)
+              for (int i = 1; i <= nI; i++) {
+                const long cc = o.icell(i, j, k);
+                const int idx[3] = {i, j, k};
+                const bool powRow = o.c.useDivbSource && iv != Rho_ && jv == Bx_ + d;
+                if (idx[d] > 1) {  // lower neighbour: -dFdWLeft(face c)
+                  const int il = i - (d == 0), jl = j - (d == 1), kl = k - (d == 2);
+                  const long cl = o.icell(il, jl, kl);
+                  double left = Coeff * (Feps[8 * cl + iv] - F0[8 * cl + iv]);
+                  if (iv == jv) left = left + cmaxAt(d, i, j, k);
+                  left = left / V;
+                  if (powRow) left = left + CoeffPow * sPow[8 * cc + iv];
+                  Jat(cc, 1 + 2 * d, iv, jv) = -left;
+                }
+                if (idx[d] < n[d]) {  // upper neighbour: +dFdWRight(face c+1)
+                  const int iu = i + (d == 0), ju = j + (d == 1), ku = k + (d == 2);
+                  const long cu = o.icell(iu, ju, ku);
+                  double right = Coeff * (Feps[8 * cu + iv] - F0[8 * cu + iv]);
+                  if (iv == jv) right = right - cmaxAt(d, iu, ju, ku);
+                  right = right / V;
+                  if (powRow) right = right + CoeffPow * sPow[8 * cc + iv];
+                  Jat(cc, 2 + 2 * d, iv, jv) = right;
+                }
+              }
+        }
+      }
+    }
+    // impl_divbsrc_middle: diagonal Powell terms
+    if (o.c.useDivbSource) {
+      for (long m = 0; m < nc; m++) {
+        const double *u = &Ucell[8 * m];
+        const double dB = DivB[m], rho = u[Rho_];
+        for (int q = 0; q < 3; q++) {
+          Jat(m, 0, RhoUx_ + q, Bx_ + q) = Jat(m, 0, RhoUx_ + q, Bx_ + q) - dB;
+          Jat(m, 0, Bx_ + q, Rho_) = Jat(m, 0, Bx_ + q, Rho_) + dB * u[RhoUx_ + q] / (rho * rho);
+          Jat(m, 0, Bx_ + q, RhoUx_ + q) = Jat(m, 0, Bx_ + q, RhoUx_ + q) - dB / rho;
+          Jat(m, 0, P_, RhoUx_ + q) = Jat(m, 0, P_, RhoUx_ + q) - dB * u[Bx_ + q] / rho;
+          Jat(m, 0, P_, Bx_ + q) = Jat(m, 0, P_, Bx_ + q) - dB * u[RhoUx_ + q] / rho;
+        }
+        Jat(m, 0, P_, Rho_) = Jat(m, 0, P_, Rho_) +
+            dB * (u[RhoUx_] * u[Bx_] + u[RhoUy_] * u[By_] + u[RhoUz_] * u[Bz_]) / (rho * rho);
+      }
+    }
+    // time-accurate scaling and the identity
+    for (long m = 0; m < nc; m++)
+      for (int s = 0; s < 7; s++)
+        for (int iv = 0; iv < 8; iv++)
+          for (int jv = 0; jv < 8; jv++)
+            Jat(m, s, iv, jv) = -Jat(m, s, iv, jv) * Dt * ImplCoeff * Norm[jv] / Norm[iv];
+    for (long m = 0; m < nc; m++)
+      for (int iv = 0; iv < 8; iv++) Jat(m, 0, iv, iv) = Jat(m, 0, iv, iv) + 1.0;
+  }
+
+  // ---- block ILU(0) of one grid block (natural order, i fastest) --------
+  static void inv8(const double *A, double *Ainv) {  // Gauss-Jordan, partial pivoting
+    double M[8][16];
+    for (int r = 0; r < 8; r++)
+      for (int q = 0; q < 8; q++) { M[r][q] = A[r * 8 + q]; M[r][8 + q] = r == q ? 1.0 : 0.0; }
+    for (int col = 0; col < 8; col++) {
+      int piv = col;
+      for (int r = col + 1; r < 8; r++)
+        if (std::fabs(M[r][col]) > std::fabs(M[piv][col])) piv = r;
+      if (piv != col)
+        for (int q = 0; q < 16; q++) std::swap(M[col][q], M[piv][q]);
+      const double inv = 1.0 / M[col][col];
+      for (int q = 0; q < 16; q++) M[col][q] *= inv;
+      for (int r = 0; r < 8; r++) {
+        if (r == col) continue;
+        const double f = M[r][col];
+        if (f != 0.0)
+          for (int q = 0; q < 16; q++) M[r][q] -= f * M[col][q];
+      }
+    }
+    for (int r = 0; r < 8; r++)
+      for (int q = 0; q < 8; q++) Ainv[r * 8 + q] = M[r][8 + q];
+  }
+  static void mm8(const double *A, const double *B, double *C) {  // C = A B
+    for (int r = 0; r < 8; r++)
+      for (int q = 0; q < 8; q++) {
+        double s = 0;
+        for (int m = 0; m < 8; m++) s += A[r * 8 + m] * B[m * 8 + q];
+        C[r * 8 + q] = s;
+      }
+  }
+  // D_c = A_cc - sum_{lower n} A_cn D_n^-1 A_nc, stored as Dinv_c
+  void bilu_factor(int b) {
+    const long nc = nC();
+    const int nI = o.c.nI, nJ = o.c.nJ, nK = o.c.nK;
+    const double *J = &Jac[(size_t)nc * b * 7 * 64];
+    double *Di = &Dinv[(size_t)nc * b * 64];
+    for (int k = 1; k <= nK; k++)
+      for (int j = 1; j <= nJ; j++)
+        for (int i = 1; i <= nI; i++) {
+          const long cc = o.icell(i, j, k);
+          double D[64], T1[64], T2[64];
+          for (int q = 0; q < 64; q++) D[q] = J[(cc * 7 + 0) * 64 + q];
+          const int idx[3] = {i, j, k};
+          for (int d = 0; d < o.c.nDim; d++) {
+            if (idx[d] <= 1) continue;
+            const long cl = o.icell(i - (d == 0), j - (d == 1), k - (d == 2));
+            // A_cn = Jac(c, lower d), A_nc = Jac(n, upper d)
+            mm8(&J[(cc * 7 + 1 + 2 * d) * 64], &Di[cl * 64], T1);
+            mm8(T1, &J[(cl * 7 + 2 + 2 * d) * 64], T2);
+            for (int q = 0; q < 64; q++) D[q] -= T2[q];
+          }
+          inv8(D, &Di[cc * 64]);
+        }
+  }
+  // z = M^-1 r with M = (D + L) D^-1 (D + U) for every grid block
+  void bilu_solve(const double *r, double *z) {
+    const long nc = nC();
+    const int nI = o.c.nI, nJ = o.c.nJ, nK = o.c.nK;
+#pragma omp parallel for schedule(static) num_threads((int)o.scr.size())
+    for (int b = 0; b < o.nBlock; b++) {
+      const double *J = &Jac[(size_t)nc * b * 7 * 64];
+      const double *Di = &Dinv[(size_t)nc * b * 64];
+      const double *rb = r + (size_t)nc * b * 8;
+      double *zb = z + (size_t)nc * b * 8;
+      for (int k = 1; k <= nK; k++)  // forward: v_c = D_c^-1 (r_c - sum_lower A_cn v_n)
+        for (int j = 1; j <= nJ; j++)
+          for (int i = 1; i <= nI; i++) {
+            const long cc = o.icell(i, j, k);
+            double w[8];
+            for (int v = 0; v < 8; v++) w[v] = rb[8 * cc + v];
+            const int idx[3] = {i, j, k};
+            for (int d = 0; d < o.c.nDim; d++) {
+              if (idx[d] <= 1) continue;
+              const long cl = o.icell(i - (d == 0), j - (d == 1), k - (d == 2));
+              const double *A = &J[(cc * 7 + 1 + 2 * d) * 64];
+              for (int iv = 0; iv < 8; iv++) {
+                double s = 0;
+                for (int jv = 0; jv < 8; jv++) s += A[iv * 8 + jv] * zb[8 * cl + jv];
+                w[iv] -= s;
+              }
+            }
+            for (int iv = 0; iv < 8; iv++) {
+              double s = 0;
+              for (int jv = 0; jv < 8; jv++) s += Di[cc * 64 + iv * 8 + jv] * w[jv];
+              zb[8 * cc + iv] = s;
+            }
+          }
+      for (int k = nK; k >= 1; k--)  // backward: x_c = v_c - D_c^-1 sum_upper A_cn x_n
+        for (int j = nJ; j >= 1; j--)
+          for (int i = nI; i >= 1; i--) {
+            const long cc = o.icell(i, j, k);
+            double w[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+            const int idx[3] = {i, j, k};
+            bool any = false;
+            for (int d = 0; d < o.c.nDim; d++) {
+              const int nmax = d == 0 ? nI : (d == 1 ? nJ : nK);
+              if (idx[d] >= nmax) continue;
+              any = true;
+              const long cu = o.icell(i + (d == 0), j + (d == 1), k + (d == 2));
+              const double *A = &J[(cc * 7 + 2 + 2 * d) * 64];
+              for (int iv = 0; iv < 8; iv++) {
+                double s = 0;
+                for (int jv = 0; jv < 8; jv++) s += A[iv * 8 + jv] * zb[8 * cu + jv];
+                w[iv] += s;
+              }
+            }
+            if (!any) continue;
+            for (int iv = 0; iv < 8; iv++) {
+              double s = 0;
+              for (int jv = 0; jv < 8; jv++) s += Di[cc * 64 + iv * 8 + jv] * w[jv];
+              zb[8 * cc + iv] -= s;
+            }
+          }
+    }
+  }
+  void precond(const double *r, double *z) {
+    if (c.typePrecond == ORA_PRECOND_BILU && havePrec) bilu_solve(r, z);
+    else std::copy(r, r + N, z);
+  }
+
+  static double dot(const double *a, const double *b, long n) {
+    double s = 0;
+    for (long q = 0; q < n; q++) s += a[q] * b[q];
+    return s;
+  }
+
+  // flexible restarted GMRES(m), right preconditioned, modified
+  // Gram-Schmidt, x0 = 0 (TypeKrylovInit 'nul'); stops when the residual
+  // norm is below errorMax times the initial one ('rel') or after maxMatvec
+  // products.  Returns 0 when converged.
+  int gmres() {
+    const int m = c.nKrylovVector;
+    std::fill(X.begin(), X.end(), 0.0);
+    std::vector<double> r(Rhs);
+    double beta = std::sqrt(dot(r.data(), r.data(), N));
+    const double beta0 = beta;
+    nMatvec = 0;
+    errRel = 0;
+    if (beta0 == 0.0) return 0;
+    std::vector<std::vector<double>> V(m + 1, std::vector<double>(N)), Z(m, std::vector<double>(N));
+    std::vector<double> H((m + 1) * m), cs(m), sn(m), gv(m + 1), w(N);
+    while (true) {
+      for (long q = 0; q < N; q++) V[0][q] = r[q] / beta;
+      std::fill(gv.begin(), gv.end(), 0.0);
+      gv[0] = beta;
+      int kdone = 0;
+      bool conv = false;
+      for (int k = 0; k < m; k++) {
+        precond(V[k].data(), Z[k].data());
+        matvec(Z[k].data(), w.data());
+        for (int q = 0; q <= k; q++) {
+          const double h = dot(V[q].data(), w.data(), N);
+          H[q * m + k] = h;
+          for (long n = 0; n < N; n++) w[n] -= h * V[q][n];
+        }
+        const double hn = std::sqrt(dot(w.data(), w.data(), N));
+        H[(k + 1) * m + k] = hn;
+        if (hn != 0.0)
+          for (long n = 0; n < N; n++) V[k + 1][n] = w[n] / hn;
+        for (int q = 0; q < k; q++) {  // previous Givens rotations
+          const double t0 = H[q * m + k], t1 = H[(q + 1) * m + k];
+          H[q * m + k] = cs[q] * t0 + sn[q] * t1;
+          H[(q + 1) * m + k] = -sn[q] * t0 + cs[q] * t1;
+        }
+        const double a = H[k * m + k], bb = H[(k + 1) * m + k];
+        const double rr = std::sqrt(a * a + bb * bb);
+        cs[k] = a / rr;
+        sn[k] = bb / rr;
+        H[k * m + k] = rr;
+        H[(k + 1) * m + k] = 0.0;
+        gv[k + 1] = -sn[k] * gv[k];
+        gv[k] = cs[k] * gv[k];
+        kdone = k + 1;
+        errRel = std::fabs(gv[k + 1]) / beta0;
+        if (errRel <= c.errorMax || nMatvec >= c.maxMatvec || hn == 0.0) { conv = errRel <= c.errorMax || hn == 0.0; break; }
+      }
+      std::vector<double> y(kdone);
+      for (int q = kdone - 1; q >= 0; q--) {
+        double s = gv[q];
+        for (int p = q + 1; p < kdone; p++) s -= H[q * m + p] * y[p];
+        y[q] = s / H[q * m + q];
+      }
+      for (int q = 0; q < kdone; q++)
+        for (long n = 0; n < N; n++) X[n] += y[q] * Z[q][n];
+      if (conv) return 0;
+      if (nMatvec >= c.maxMatvec) return 1;
+      // restart with the true residual
+      matvec(X.data(), w.data());
+      for (long n = 0; n < N; n++) r[n] = Rhs[n] - w[n];
+      beta = std::sqrt(dot(r.data(), r.data(), N));
+      errRel = beta / beta0;
+      if (errRel <= c.errorMax) return 0;
+    }
+  }
+
+  // BATS_advance with advance_part_impl (full implicit, time accurate)
+  int advance(double tLimit) {
+    if (tLimit <= 0) tLimit = 1e300;
+    if (o.tSimulation >= tLimit) return 0;
+    o.nStep = o.nStep + 1;
+    // set_global_timestep: lagged minimum of the cell time steps, Cfl=CflImpl
+    DtNoCfl = o.nStep <= 1 ? 0.0 : DtMinNext;
+    if (o.tSimulation + c.cflImpl * DtNoCfl > tLimit) DtNoCfl = (tLimit - o.tSimulation) / c.cflImpl;
+    Dt = c.cflImpl * DtNoCfl;
+    o.Dt = Dt;
+    state_to_impl(Impl);
+    // Norm_V: rms of each implicit variable (:454-465)
+    for (int v = 0; v < nVar; v++) {
+      double s = 0;
+      for (long m = 0; m < nCellTot; m++) s += Impl[nVar * m + v] * Impl[nVar * m + v];
+      Norm[v] = std::sqrt(s / nCellTot);
+      if (Norm[v] < 1e-300) Norm[v] = 1.0;
+    }
+    DtCoeff = c.cflImpl / 0.5;
+    // BDF2 needs the previous step (and a nonzero previous time step)
+    const bool bdf2 = c.useBdf2 && o.nStep == nStepPrev + 1 && DtPrev > 0.0;
+    ImplCoeff = bdf2 ? (Dt + DtPrev) / (2 * Dt + DtPrev) : c.implCoeff0;
+    if (!c.useBdf2) ImplOld = Impl;
+    // impl_newton_init (:816-954)
+    residual(Impl, false, ResExpl);
+    residual(Impl, true, ResImpl);
+    for (long n = 0; n < N; n++) {
+      const int v = n % nVar;
+      if (bdf2)
+        Rhs[n] = (ImplCoeff * DtCoeff * ResExpl[n] + (1 - ImplCoeff) * Dt / DtPrev * (Impl[n] - ImplOld[n])) / Norm[v];
+      else
+        Rhs[n] = ResExpl[n] * DtCoeff / Norm[v];
+    }
+    if (c.useBdf2) {
+      nStepPrev = o.nStep;
+      DtPrev = Dt;
+      ImplOld = Impl;
+    }
+    // impl_jacobian + BILU of every implicit block
+    havePrec = false;
+    if (c.typePrecond == ORA_PRECOND_BILU) {
+      Jac.assign((size_t)nCellTot * 7 * 64, 0.0);
+      Dinv.assign((size_t)nCellTot * 64, 0.0);
+      impl_to_state(Impl);  // ghost cells of U^n for the Jacobian
+#pragma omp parallel for schedule(dynamic, 1) num_threads((int)o.scr.size())
+      for (int b = 0; b < o.nBlock; b++) {
+        jacobian(b);
+        bilu_factor(b);
+      }
+      havePrec = true;
+    }
+    const int err = gmres();
+    // impl_newton_update: Impl = Impl + x Norm_V
+    for (long n = 0; n < N; n++) Impl[n] = Impl[n] + X[n] * Norm[n % nVar];
+    impl_to_state(Impl);
+    o.tSimulation = o.tSimulation + Dt;
+    return err;
+  }
+};
+
 }  // namespace
 
 extern "C" {
@@ -725,7 +1289,43 @@ void *ora_new(const ora_config *cfg, int nBlock, const int *iLevelCoord) {
   o->init(cfg, nBlock, iLevelCoord);
   return o;
 }
-void ora_free(void *h) { delete (Oracle *)h; }
+void ora_free(void *h) {
+  Oracle *o = (Oracle *)h;
+  delete (Implicit *)o->implPtr;
+  delete o;
+}
+
+void ora_set_implicit(void *h, const ora_impl_config *cfg) {
+  Oracle *o = (Oracle *)h;
+  delete (Implicit *)o->implPtr;
+  o->implPtr = new Implicit(*o, *cfg);
+}
+int ora_advance_implicit(void *h, double tLimit, int *nMatvec, double *errRel) {
+  Oracle *o = (Oracle *)h;
+  Implicit *im = (Implicit *)o->implPtr;
+  if (!im) return 2;
+  const int r = im->advance(tLimit);
+  if (nMatvec) *nMatvec = im->nMatvec;
+  if (errRel) *errRel = im->errRel;
+  return r;
+}
+void ora_impl_get_rhs(void *h, double *Rhs, double *Norm_V) {
+  Implicit *im = (Implicit *)((Oracle *)h)->implPtr;
+  std::copy(im->Rhs.begin(), im->Rhs.end(), Rhs);
+  std::copy(im->Norm, im->Norm + 8, Norm_V);
+}
+void ora_impl_matvec(void *h, const double *x, double *y) {
+  Implicit *im = (Implicit *)((Oracle *)h)->implPtr;
+  im->matvec(x, y);
+  im->impl_to_state(im->Impl);
+}
+void ora_impl_precond(void *h, const double *r, double *z) {
+  ((Implicit *)((Oracle *)h)->implPtr)->precond(r, z);
+}
+void ora_impl_get_x(void *h, double *x) {
+  Implicit *im = (Implicit *)((Oracle *)h)->implPtr;
+  std::copy(im->X.begin(), im->X.end(), x);
+}
 long ora_state_size(void *h) { return (long)((Oracle *)h)->State.size(); }
 void ora_set_state(void *h, const double *S) {
   Oracle *o = (Oracle *)h;

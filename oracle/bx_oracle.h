@@ -77,6 +77,34 @@ void ora_get_face_flux(void *h, int iDim, double *Flux);
 void ora_get_source(void *h, double *Source_VC);
 void ora_get_dtmax(void *h, double *DtMax_CB, double *DtMax_B);
 
+/* ---- implicit JFNK step (src/ModPartImplicit.f90, full implicit) ---- */
+enum { ORA_PRECOND_NONE = 0, ORA_PRECOND_BILU = 1 };
+typedef struct {
+  double cflImpl;       /* CflImpl of #IMPLICIT */
+  double implCoeff0;    /* ImplCoeff of #IMPLSTEP (1 = backward Euler) */
+  int useBdf2;          /* UseBDF2 of #IMPLSTEP */
+  int nOrderImpl;       /* order of the residual in the matvec (1) */
+  int typeFluxImpl;     /* flux of the matvec residual, -1 = same as explicit */
+  double jacobianEps;   /* JacobianEps of #JACOBIAN (1e-12) */
+  int nKrylovVector;    /* GMRES restart length */
+  int maxMatvec;        /* MaxMatvec of #KRYLOV */
+  double errorMax;      /* relative tolerance of #KRYLOV */
+  int typePrecond;      /* ORA_PRECOND_* */
+} ora_impl_config;
+
+void ora_set_implicit(void *h, const ora_impl_config *cfg);
+/* one BATS_advance call with the full implicit scheme; returns 0 or 1 if
+ * the Krylov solver did not reach the tolerance within maxMatvec */
+int ora_advance_implicit(void *h, double tSimulationLimit, int *nMatvec, double *errorRel);
+/* the normalised Krylov system of the last implicit step:
+ * Rhs (nCell*nVar), Norm_V (nVar), and y = A x for a given x */
+void ora_impl_get_rhs(void *h, double *Rhs, double *Norm_V);
+void ora_impl_matvec(void *h, const double *x, double *y);
+/* apply the BILU preconditioner of the last step: z = M^-1 r */
+void ora_impl_precond(void *h, const double *r, double *z);
+/* the solution x of the last Krylov solve */
+void ora_impl_get_x(void *h, double *x);
+
 #ifdef __cplusplus
 }
 #endif

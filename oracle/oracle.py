@@ -179,3 +179,92 @@ class Oracle:
         S = np.empty((g.nK, g.nJ, g.nI, self.NVAR + 1))
         lib().ora_get_source(self.h, _dp(S))
         return S
+
+
+class OraImplConfig(ctypes.Structure):
+    _fields_ = [
+        ("cflImpl", ctypes.c_double), ("implCoeff0", ctypes.c_double), ("useBdf2", ctypes.c_int),
+        ("nOrderImpl", ctypes.c_int), ("typeFluxImpl", ctypes.c_int), ("jacobianEps", ctypes.c_double),
+        ("nKrylovVector", ctypes.c_int), ("maxMatvec", ctypes.c_int), ("errorMax", ctypes.c_double),
+        ("typePrecond", ctypes.c_int),
+    ]
+
+
+PRECOND = {"none": 0, "bilu": 1}
+
+
+def _impl_lib():
+    L = lib()
+    if not hasattr(L, "_impl_ready"):
+        vp, ip, dp = ctypes.c_void_p, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_double)
+        L.ora_set_implicit.argtypes = [vp, ctypes.POINTER(OraImplConfig)]
+        L.ora_advance_implicit.restype = ctypes.c_int
+        L.ora_advance_implicit.argtypes = [vp, ctypes.c_double, ip, dp]
+        L.ora_impl_get_rhs.argtypes = [vp, dp, dp]
+        L.ora_impl_matvec.argtypes = [vp, dp, dp]
+        L.ora_impl_precond.argtypes = [vp, dp, dp]
+        L.ora_impl_get_x.argtypes = [vp, dp]
+        L._impl_ready = True
+    return L
+
+
+def implicit_config(impl):
+    """``impl`` uses the keys of batsrus_b200.implicit.ImplicitParams"""
+    c = OraImplConfig()
+    c.cflImpl = impl.cflImpl
+    c.implCoeff0 = impl.implCoeff0
+    c.useBdf2 = int(impl.useBdf2)
+    c.nOrderImpl = impl.nOrderImpl
+    c.typeFluxImpl = -1 if impl.typeFluxImpl in (None, "default") else FLUX[impl.typeFluxImpl.lower()]
+    c.jacobianEps = impl.jacobianEps
+    c.nKrylovVector = impl.nKrylovVector
+    c.maxMatvec = impl.maxMatvec
+    c.errorMax = impl.errorMax
+    c.typePrecond = PRECOND[impl.typePrecond.lower()] if impl.typePrecond.lower() in PRECOND else 1
+    return c
+
+
+def _oracle_set_implicit(self, impl):
+    self._icfg = implicit_config(impl)
+    _impl_lib().ora_set_implicit(self.h, ctypes.byref(self._icfg))
+    self.nvec = self.grid.nCell * self.NVAR
+
+
+def _oracle_advance_implicit(self, t_limit=-1.0):
+    n, e = ctypes.c_int(), ctypes.c_double()
+    r = _impl_lib().ora_advance_implicit(self.h, t_limit, ctypes.byref(n), ctypes.byref(e))
+    return r, n.value, e.value
+
+
+def _oracle_impl_rhs(self):
+    rhs, norm = np.empty(self.nvec), np.empty(8)
+    _impl_lib().ora_impl_get_rhs(self.h, _dp(rhs), _dp(norm))
+    return rhs, norm
+
+
+def _oracle_impl_matvec(self, x):
+    x = np.ascontiguousarray(x, dtype=np.float64)
+    y = np.empty_like(x)
+    _impl_lib().ora_impl_matvec(self.h, _dp(x), _dp(y))
+    return y
+
+
+def _oracle_impl_precond(self, r):
+    r = np.ascontiguousarray(r, dtype=np.float64)
+    z = np.empty_like(r)
+    _impl_lib().ora_impl_precond(self.h, _dp(r), _dp(z))
+    return z
+
+
+def _oracle_impl_x(self):
+    x = np.empty(self.nvec)
+    _impl_lib().ora_impl_get_x(self.h, _dp(x))
+    return x
+
+
+Oracle.set_implicit = _oracle_set_implicit
+Oracle.advance_implicit = _oracle_advance_implicit
+Oracle.impl_rhs = _oracle_impl_rhs
+Oracle.impl_matvec = _oracle_impl_matvec
+Oracle.impl_precond = _oracle_impl_precond
+Oracle.impl_x = _oracle_impl_x
