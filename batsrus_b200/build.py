@@ -24,9 +24,11 @@ UNITS = [
     ("bx_compat.cu", ["--fmad=false"]),
     ("bx_stage_fp32.cu", []),
     ("bx_stage3d.cu", []),
+    ("bx_implicit.cu", ["--fmad=false"]),
     ("bx_capi.cu", []),
 ]
-HEADERS = ["bx_physics.cuh", "bx_stage.cuh", "bx_device.h", "bx_stage3d.cuh", "bx_tma.cuh"]
+HEADERS = ["bx_physics.cuh", "bx_stage.cuh", "bx_device.h", "bx_stage3d.cuh", "bx_tma.cuh", "bx_core.h",
+           "bx_impl_kernels.cuh"]
 
 
 def _sources_newer(target, deps):

@@ -30,7 +30,41 @@ EXPORTS = (
     "bx_exchange_messages", "bx_set_global_timestep", "bx_advance_explicit", "bx_advance",
     "bx_synchronize", "bx_timing_enable", "bx_timing_get", "bx_timing_reset",
     "bx_region_begin", "bx_region_end",
+    "bx_implicit_init", "bx_advance_part_impl", "bx_impl_get_rhs", "bx_impl_matvec",
+    "bx_impl_precond", "bx_impl_get_x",
 )
+PRECOND = {"none": 0, "bilu": 1, "learned": 2}
+
+
+class ImplicitParamsC(ctypes.Structure):
+    _fields_ = [
+        ("CflImpl", ctypes.c_double), ("ImplCoeff", ctypes.c_double), ("UseBdf2", ctypes.c_int),
+        ("nOrderImpl", ctypes.c_int), ("TypeFluxImpl", ctypes.c_int), ("JacobianEps", ctypes.c_double),
+        ("nKrylovVector", ctypes.c_int), ("MaxMatvec", ctypes.c_int), ("ErrorMax", ctypes.c_double),
+        ("TypePrecond", ctypes.c_int),
+    ]
+
+
+class KrylovStats(ctypes.Structure):
+    _fields_ = [
+        ("nMatvec", ctypes.c_int), ("iError", ctypes.c_int), ("Error", ctypes.c_double),
+        ("Dt", ctypes.c_double), ("msStep", ctypes.c_double), ("msPrecondSetup", ctypes.c_double),
+    ]
+
+
+def implicit_params(p):
+    c = ImplicitParamsC()
+    c.CflImpl = p.cflImpl
+    c.ImplCoeff = p.implCoeff0
+    c.UseBdf2 = int(p.useBdf2)
+    c.nOrderImpl = p.nOrderImpl
+    c.TypeFluxImpl = -1 if p.typeFluxImpl in (None, "default") else FLUX[p.typeFluxImpl.lower()]
+    c.JacobianEps = p.jacobianEps
+    c.nKrylovVector = p.nKrylovVector
+    c.MaxMatvec = p.maxMatvec
+    c.ErrorMax = p.errorMax
+    c.TypePrecond = PRECOND[p.typePrecond.lower()]
+    return c
 
 
 class BxError(RuntimeError):
@@ -89,6 +123,10 @@ def load():
         "bx_set_global_timestep": [d, dp], "bx_advance_explicit": [i], "bx_advance": [i, d],
         "bx_synchronize": [], "bx_timing_enable": [i], "bx_timing_get": [dp, ip, ip],
         "bx_timing_reset": [], "bx_region_begin": [], "bx_region_end": [dp],
+        "bx_implicit_init": [ctypes.POINTER(ImplicitParamsC)],
+        "bx_advance_part_impl": [d, ctypes.POINTER(KrylovStats)],
+        "bx_impl_get_rhs": [dp, dp], "bx_impl_matvec": [dp, dp], "bx_impl_precond": [dp, dp],
+        "bx_impl_get_x": [dp],
     }
     for name, args in sig.items():
         f = getattr(L, name)

@@ -17,6 +17,7 @@
 #include <vector>
 
 #include "../../include/bx200.h"
+#include "bx_core.h"
 #include "bx_device.h"
 
 using namespace bx;
@@ -393,12 +394,35 @@ int check_err_flag() {
     int zero = 0;
     CK(cudaMemcpy(&g.ts->errFlag, &zero, sizeof(int), cudaMemcpyHostToDevice));
     if (flag & kErrHlld) return fail(BX_ERR_HLLD, "hlld_flux: negative density ratio (reference stops)");
+    if (flag & kErrTimeout) return fail(BX_ERR_TIMEOUT, "a bounded wait for a tile load gave up");
     return fail(BX_ERR_NONPHYSICAL, "non-physical state");
   }
   return BX_OK;
 }
 
 }  // namespace
+
+namespace bx {
+Core core() {
+  Core c;
+  c.ready = g.ready;
+  c.dev = g.dev; c.nDim = g.nDim; c.nI = g.nI; c.nJ = g.nJ; c.nK = g.nK; c.shape = g.shape;
+  c.nBlock = g.nBlock; c.nSM = g.nSM; c.nCell = g.nCell; c.sch = g.sch;
+  c.A = g.A; c.nbr = g.nbr; c.order = g.order; c.geom = g.geom; c.ts = g.ts; c.dtBlock = g.dtBlock;
+  c.st = g.st;
+  return c;
+}
+int core_fail(int code, const char *fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof(buf), fmt, ap);
+  va_end(ap);
+  g.err = buf;
+  return code;
+}
+int core_encode_maps(void *base, bool fp32, TmaMaps &m) { return encode_maps(base, fp32, g.nI, g.nBlock, m); }
+}  // namespace bx
 
 // ===========================================================================
 extern "C" {

@@ -1,0 +1,28 @@
+// bx_core.h -- internal view of the library context shared by the explicit
+// (bx_capi.cu) and implicit (bx_implicit.cu) parts of libbx200.
+#pragma once
+#include <cuda_runtime.h>
+
+#include "../../include/bx200.h"
+#include "bx_device.h"
+
+namespace bx {
+
+struct Core {
+  bool ready;
+  int dev, nDim, nI, nJ, nK, shape, nBlock, nSM;
+  long nCell;  // cells per block
+  bx_scheme_params sch;
+  double *A;   // U^n, pressure form, SoA [block][var][cell]
+  const int *nbr, *order;
+  const BlockGeom *geom;
+  StepState *ts;
+  double *dtBlock;
+  cudaStream_t st;
+};
+
+Core core();
+int core_fail(int code, const char *fmt, ...);
+int core_encode_maps(void *base, bool fp32, TmaMaps &m);
+
+}  // namespace bx

@@ -41,6 +41,14 @@ struct StageArgs {
   int nBlock;
   int iStage, nStage, nOrder, limiter, useDivb, useHalfStep, computeDt;
   double beta, gamma, invGm1, cfl;
+  // residual mode of the 3D kernel (get_residual of the implicit scheme):
+  // the input holds total energy in the pressure slot, the output is the
+  // increment dtScale*DtMax_CB*(S + dF/V) of the implicit variables, with
+  // DtMax_CB per cell (dtCellIn) or the global Dt/Cfl (dtCellIn == nullptr)
+  int inputEnergy = 0, outputResidual = 0;
+  const double *dtCellIn = nullptr;
+  double *dtCellOut = nullptr;  // V/sum(Vdt) per cell when computeDt
+  double dtScale = 0.5;
 };
 
 // per-block compatibility kernels (orig-path entry points, FP64)

@@ -262,6 +262,13 @@ __global__ void __launch_bounds__(T::NTHR, 1)
           const int sv = tile_index<T, TileT>(1, si, sj, sk) - s0;
 #pragma unroll
           for (int v = 0; v < 8; v++) prim[m][v] = tile[s0 + v * sv];
+          if (a.inputEnergy) {  // energy_to_pressure
+            const TileT pb = prim[m][kP] - TileT(0.5) * (prim[m][kBx] * prim[m][kBx] +
+                                                         prim[m][kBy] * prim[m][kBy] + prim[m][kBz] * prim[m][kBz]);
+            prim[m][kP] = (TileT)(a.gamma - 1.0) *
+                          (pb - TileT(0.5) * (prim[m][kUx] * prim[m][kUx] + prim[m][kUy] * prim[m][kUy] +
+                                              prim[m][kUz] * prim[m][kUz]) / prim[m][kRho]);
+          }
           const TileT rhoInv = TileT(1) / prim[m][kRho];
           prim[m][kUx] = rhoInv * prim[m][kUx];
           prim[m][kUy] = rhoInv * prim[m][kUy];
@@ -291,13 +298,38 @@ __global__ void __launch_bounds__(T::NTHR, 1)
 
     // update_state_normal / update_explicit for the thread's cell
     double dtmin = 1e300;
-    if (t < T::NC) {
+    if (t < T::NC && a.outputResidual) {
+      // get_residual: increment of the implicit variables (energy in slot 7)
+      OutT *out = reinterpret_cast<OutT *>(a.out) + (size_t)b * 8 * T::NC;
+      const size_t cell = (size_t)b * T::NC + t;
+      const double dtl = a.dtScale * (a.dtCellIn ? a.dtCellIn[cell] : DtNoCfl);
+      if (a.computeDt) {
+        dtmin = g.volume / vdt;
+        if (a.dtCellOut) a.dtCellOut[cell] = dtmin;
+      }
+      double src[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+      if (a.useDivb) {
+        const int ii = t % T::N, jj = (t / T::N) % T::N, kk = t / (T::N * T::N);
+        const int c0 = tile_index<T, TileT>(0, ii, jj, kk);
+        const double ux = tile[c0 + kUx * T::NC], uy = tile[c0 + kUy * T::NC], uz = tile[c0 + kUz * T::NC];
+        const double bx = tile[c0 + kBx * T::NC], by = tile[c0 + kBy * T::NC], bz = tile[c0 + kBz * T::NC];
+        src[kBx] = -divB * ux; src[kBy] = -divB * uy; src[kBz] = -divB * uz;
+        src[kE] = -divB * (bx * ux + by * uy + bz * uz);
+        src[kUx] = -divB * bx; src[kUy] = -divB * by; src[kUz] = -divB * bz;
+      }
+      const double invV = 1.0 / g.volume;
+#pragma unroll
+      for (int v = 0; v < 8; v++) out[v * T::NC + t] = (OutT)(dtl * (src[v] + chg[v] * invV));
+    } else if (t < T::NC) {
       const double *old = a.old + (size_t)b * 8 * T::NC;
       OutT *out = reinterpret_cast<OutT *>(a.out) + (size_t)b * 8 * T::NC;
       double o[8];
 #pragma unroll
       for (int v = 0; v < 8; v++) o[v] = old[v * T::NC + t];
-      if (a.computeDt) dtmin = g.volume / vdt;
+      if (a.computeDt) {
+        dtmin = g.volume / vdt;
+        if (a.dtCellOut) a.dtCellOut[(size_t)b * T::NC + t] = dtmin;
+      }
       if (DtNoCfl == 0.0) {
 #pragma unroll
         for (int v = 0; v < 8; v++) out[v * T::NC + t] = (OutT)o[v];

@@ -147,6 +147,45 @@ BX_API int bx_advance(int nStep, double TimeSimulationLimit);
 /* wait for the library's stream */
 BX_API int bx_synchronize(void);
 
+/* ---- implicit JFNK step (src/ModPartImplicit.f90, full implicit) --------- */
+enum { BX_PRECOND_NONE = 0, BX_PRECOND_BILU = 1, BX_PRECOND_LEARNED = 2 };
+/* #IMPLICIT, #IMPLSTEP, #IMPLSCHEME, #JACOBIAN, #KRYLOV, #KRYLOVSIZE,
+ * #PRECONDITIONER (read_part_impl_param, src/ModPartImplicit.f90:116-248) */
+typedef struct {
+  double CflImpl;
+  double ImplCoeff;      /* ImplCoeff0: 1 = backward Euler */
+  int UseBdf2;
+  int nOrderImpl;        /* order of the residual in the matvec and Jacobian */
+  int TypeFluxImpl;      /* BX_FLUX_*, or -1 for the explicit flux */
+  double JacobianEps;
+  int nKrylovVector;     /* GMRES restart length */
+  int MaxMatvec;
+  double ErrorMax;       /* relative Krylov tolerance */
+  int TypePrecond;       /* BX_PRECOND_* */
+} bx_implicit_params;
+
+typedef struct {
+  int nMatvec;           /* matrix-vector products of the Krylov solve */
+  int iError;            /* 0 converged, 1 tolerance not reached */
+  double Error;          /* final relative residual */
+  double Dt;             /* implicit time step */
+  double msStep;         /* device time of the whole step */
+  double msPrecondSetup; /* Jacobian + factorisation (BILU) */
+} bx_krylov_stats;
+
+BX_API int bx_implicit_init(const bx_implicit_params *params);
+/* advance_part_impl (src/ModPartImplicit.f90:322): one time step of
+ * BATS_advance with the full implicit scheme */
+BX_API int bx_advance_part_impl(double TimeSimulationLimit, bx_krylov_stats *stats);
+/* the normalised Krylov system of the last implicit step, vectors in the
+ * reference's Rhs_I order (variable fastest, then i, j, k, block):
+ * Rhs_I and Norm_V (impl_newton_init), y = A x (impl_matvec_free), the
+ * preconditioner z = M^-1 r and the Krylov solution x_I */
+BX_API int bx_impl_get_rhs(double *Rhs_I, double *Norm_V);
+BX_API int bx_impl_matvec(const double *x_I, double *y_I);
+BX_API int bx_impl_precond(const double *r_I, double *z_I);
+BX_API int bx_impl_get_x(double *x_I);
+
 /* ---- measurement ----------------------------------------------------------
  * Kernel timing with CUDA events on the library's stream: when enabled, the
  * fused stage kernel launches are bracketed by events; the average duration

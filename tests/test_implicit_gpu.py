@@ -1,0 +1,84 @@
+"""GPU parity of the implicit JFNK step against the CPU oracle through the C
+ABI: the normalised Krylov system (Rhs, Norm_V), the matrix-free product,
+the BILU preconditioner, and whole implicit steps (Krylov iteration count
+and state).
+
+Tolerances: Rhs, Norm_V and the matrix-free product are FP64 evaluations of
+the same formulas (1e-10 relative; the finite-difference product divides a
+residual difference by eps = 1e-6/rms(x), which amplifies rounding by 1e6).
+The preconditioner is compared at 1e-10.  A whole step solves the linear
+system to the Krylov tolerance 1e-3; the GPU and oracle iterates differ
+only by the summation order of the FP64 inner products, so the step results
+agree to 1e-8 relative and the matrix-vector counts agree within one.
+"""
+import numpy as np
+import pytest
+
+from batsrus_b200 import configs
+from batsrus_b200.explicit import ExplicitSolver
+from batsrus_b200.implicit import ImplicitSolver
+from batsrus_b200.implicit_params import ImplicitParams
+from oracle import Oracle
+
+pytestmark = pytest.mark.gpu
+
+
+def rel(a, b):
+    return np.abs(a - b).max() / max(np.abs(b).max(), 1e-300)
+
+
+def pair(prec="BILU", nRoot=2, state="pert", bdf2=True):
+    g, s, st, _ = configs.uniform_3d_case(nRoot, "Linde", "mc3", 1.2, state=state)
+    p = ImplicitParams(typePrecond=prec, useBdf2=bdf2)
+    o = Oracle(g, s)
+    o.set_state(st)
+    o.exchange_messages()
+    o.set_implicit(p)
+    x = ExplicitSolver(g, s)
+    x.set_state(st)
+    im = ImplicitSolver(x, p)
+    return g, o, x, im
+
+
+@pytest.mark.parametrize("prec", ["BILU", "NONE"])
+def test_gpu_jfnk_steps_match_oracle(prec):
+    g, o, x, im = pair(prec)
+    isl = g.interior_slices()
+    for step in range(4):
+        stats = im.advance_part_impl()
+        r, nm, err = o.advance_implicit()
+        assert r == 0 and stats["iError"] == 0
+        assert abs(stats["nMatvec"] - nm) <= 1, (step, stats["nMatvec"], nm)
+        to, dto, no = o.time()
+        tg, _, ng = x.time()
+        assert ng == no and abs(tg - to) <= 1e-12 * max(to, 1.0)
+        assert rel(x.get_state()[isl], o.get_state()[isl]) < 1e-8, step
+
+
+def test_gpu_jfnk_system_matches_oracle():
+    g, o, x, im = pair("BILU")
+    im.advance_part_impl()
+    o.advance_implicit()
+    im.advance_part_impl()
+    o.advance_implicit()
+    rg, ng = im.rhs()
+    ro, no = o.impl_rhs()
+    assert rel(ng, no) < 1e-12
+    assert rel(rg, ro) < 1e-10
+    rng = np.random.default_rng(3)
+    v = rng.normal(size=rg.size)
+    assert rel(im.matvec(v), o.impl_matvec(v)) < 1e-8
+    assert rel(im.precond(v), o.impl_precond(v)) < 1e-10
+    # the Krylov solution satisfies the tolerance on the oracle's operator
+    xs = im.x()
+    res = o.impl_matvec(xs) - ro
+    assert np.linalg.norm(res) <= 1.2e-3 * np.linalg.norm(ro)
+
+
+def test_gpu_jfnk_first_step_only_sets_the_time_step():
+    g, o, x, im = pair("BILU")
+    st0 = x.get_state()
+    stats = im.advance_part_impl()
+    assert stats["Dt"] == 0.0 and stats["nMatvec"] == 0
+    isl = g.interior_slices()
+    assert rel(x.get_state()[isl], st0[isl]) < 1e-14

@@ -92,3 +92,26 @@ def test_oracle_brio_wu_runs_to_time_limit():
     assert abs(t - 0.1) < 1e-12
     S = o.get_state()[g.interior_slices()].reshape(-1, 8)
     assert np.isfinite(S).all() and (S[:, 0] > 0).all() and (S[:, 7] > 0).all()
+
+
+def test_oracle_jfnk_step_solves_its_krylov_system():
+    """One implicit step: the GMRES solution meets the 1e-3 relative
+    tolerance on the matrix-free operator, and BILU needs fewer products
+    than no preconditioner."""
+    from batsrus_b200.implicit_params import ImplicitParams
+    g, s, st, _ = configs.uniform_3d_case(2, "Linde", "mc3", 1.2, state="pert")
+    counts = {}
+    for prec in ("bilu", "none"):
+        o = Oracle(g, s)
+        o.set_state(st)
+        o.exchange_messages()
+        o.set_implicit(ImplicitParams(typePrecond=prec))
+        o.advance_implicit()  # Dt = 0: sets the time step
+        r, nm, err = o.advance_implicit()
+        assert r == 0 and err <= 1e-3
+        rhs, norm = o.impl_rhs()
+        x = o.impl_x()
+        res = o.impl_matvec(x) - rhs
+        assert np.linalg.norm(res) <= 1.05e-3 * np.linalg.norm(rhs)
+        counts[prec] = nm
+    assert counts["bilu"] < counts["none"]
