@@ -433,9 +433,11 @@ int bx_advance_part_impl(double tLimit, bx_krylov_stats *stats) {
   CKI(cudaEventRecord(I.ev[2], c.st));
   int iError = 0;
   if ((r = gmres(iError))) return r;
-  // impl_newton_update and implicit2explicit
-  k_newton_update<<<kG, kT, 0, c.st>>>(I.U, I.X, I.dNorm, I.nCellBlock, I.N);
-  k_impl_to_state<<<kG, kT, 0, c.st>>>(I.U, c.A, I.nCellBlock, I.nCellTot, c.sch.Gamma - 1.0);
+  // impl_newton_update and implicit2explicit; U keeps U^n (the
+  // linearisation point) for bx_impl_matvec after the step
+  CKI(cudaMemcpyAsync(I.Reps, I.U, sizeof(double) * I.N, cudaMemcpyDeviceToDevice, c.st));
+  k_newton_update<<<kG, kT, 0, c.st>>>(I.Reps, I.X, I.dNorm, I.nCellBlock, I.N);
+  k_impl_to_state<<<kG, kT, 0, c.st>>>(I.Reps, c.A, I.nCellBlock, I.nCellTot, c.sch.Gamma - 1.0);
   CKI(cudaGetLastError());
   CKI(cudaEventRecord(I.ev[3], c.st));
   if ((r = read_ts(s))) return r;  // DtMinBits of the high-order residual

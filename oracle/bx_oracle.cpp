@@ -730,7 +730,7 @@ struct Implicit {
   Oracle &o;
   ora_impl_config c;
   long nCellTot = 0, N = 0;
-  std::vector<double> Impl, ImplOld, ResExpl, ResImpl, Rhs, X, Work, dtCell;
+  std::vector<double> Impl, ImplOld, ResExpl, ResImpl, Rhs, X, Work, dtCell, Unew;
   std::vector<double> Jac;   // [cell][stencil 7][iVar][jVar]
   std::vector<double> Dinv;  // [cell][8][8] inverse pivots of BILU
   double Norm[8];
@@ -1272,9 +1272,11 @@ struct Implicit {
       havePrec = true;
     }
     const int err = gmres();
-    // impl_newton_update: Impl = Impl + x Norm_V
-    for (long n = 0; n < N; n++) Impl[n] = Impl[n] + X[n] * Norm[n % nVar];
-    impl_to_state(Impl);
+    // impl_newton_update: U^n+1 = Impl + x Norm_V (Impl keeps U^n, the
+    // linearisation point of the system, for inspection)
+    Unew.resize(N);
+    for (long n = 0; n < N; n++) Unew[n] = Impl[n] + X[n] * Norm[n % nVar];
+    impl_to_state(Unew);
     o.tSimulation = o.tSimulation + Dt;
     return err;
   }
@@ -1317,7 +1319,7 @@ void ora_impl_get_rhs(void *h, double *Rhs, double *Norm_V) {
 void ora_impl_matvec(void *h, const double *x, double *y) {
   Implicit *im = (Implicit *)((Oracle *)h)->implPtr;
   im->matvec(x, y);
-  im->impl_to_state(im->Impl);
+  im->impl_to_state(im->Unew.empty() ? im->Impl : im->Unew);  // restore the current state
 }
 void ora_impl_precond(void *h, const double *r, double *z) {
   ((Implicit *)((Oracle *)h)->implPtr)->precond(r, z);
