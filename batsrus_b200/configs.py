@@ -12,6 +12,11 @@
   (nRoot = 32 gives 256^3 = 32768 blocks), Linde HLL flux, Koren (mc3)
   limiter with beta 1.2 (the PARAM.XML default for mc3), CFL 0.8,
   gamma 5/3, Powell source on.
+* ``jfnk_ot`` -- the implicit workload: periodic unit cube of (8 nRoot)^3
+  cells (nRoot = 16 gives 128^3 = 4096 blocks), Orszag-Tang plus a seeded
+  Gaussian random-phase perturbation (amplitude 1e-2, |k| <= 8), the
+  explicit scheme of ``orszag_tang_3d`` for the high-order residual, and
+  BDF2 with CflImpl 20, GMRES(30) to 1e-3 relative.
 """
 import math
 
@@ -64,6 +69,17 @@ def uniform_3d_case(nRoot, flux, limiter="mc3", beta=1.2, precision="fp64", nCel
     else:
         st = initial.perturbed_ot(g, seed=7, amplitude=0.05, kmax=2)
     return g, s, st, {}
+
+
+def jfnk_ot(nRoot=16, precond="BILU", seed=2024, with_state=True):
+    from .implicit_params import ImplicitParams
+    g = BlockGrid.uniform(3, (8, 8, 8), (nRoot,) * 3, (0.0, 0.0, 0.0), (1.0, 1.0, 1.0), ("periodic",) * 6)
+    s = Scheme(nOrder=2, nStage=2, typeFlux="Linde", typeLimiter="mc3", limiterBeta=1.2, cfl=0.8,
+               gamma=5.0 / 3.0, useDivbSource=True, useHalfStep=True)
+    p = ImplicitParams(cflImpl=20.0, useBdf2=True, nKrylovVector=30, maxMatvec=100, errorMax=1e-3,
+                       typePrecond=precond)
+    st = initial.perturbed_ot(g, seed=seed, amplitude=1e-2, kmax=8) if with_state else None
+    return g, s, p, st
 
 
 CELLS_PER_STEP_BYTES = {"fp64": 320, "fp32": 256}

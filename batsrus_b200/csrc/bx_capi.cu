@@ -236,6 +236,7 @@ int encode_maps(void *base, bool fp32, int N, int nBlock, TmaMaps &m) {
 }
 
 void free_all() {
+  impl_release();
   if (g.graph) { cudaGraphExecDestroy(g.graph); g.graph = nullptr; }
   for (double **p : {&g.A, &g.B, &g.Nx, &g.Ox, &g.stageAoS, &g.dtBlock, &g.scrSrc, &g.scrDt}) {
     if (*p) cudaFree(*p);

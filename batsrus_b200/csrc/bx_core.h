@@ -24,5 +24,7 @@ struct Core {
 Core core();
 int core_fail(int code, const char *fmt, ...);
 int core_encode_maps(void *base, bool fp32, TmaMaps &m);
+// release the implicit context (its buffers are sized for the current grid)
+void impl_release();
 
 }  // namespace bx

@@ -111,6 +111,10 @@ int residual(const double *in, const TmaMaps &map, double *out, bool lowOrder) {
 
 }  // namespace
 
+void bx::impl_release() {
+  if (I.ready) free_impl();
+}
+
 namespace {
 
 int read_ts(StepState &s) {

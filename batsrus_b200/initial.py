@@ -77,6 +77,33 @@ def blast(grid, p_in=10.0, p_out=0.1, r0=0.1, rho=1.0, b=(1 / math.sqrt(2), 1 / 
     return _from_primitive(prim)
 
 
+def _random_phase_field(grid, xyz, ks, amp):
+    """sum_k Re(a_k exp(2 pi i k.x)) at the cell centres xyz (ghosts included).
+
+    On a single-level grid whose domain has unit length in every direction
+    (so that the field is periodic over it) the sum is one inverse FFT of
+    the uniform N^3 mesh, with the half-cell shift of the cell centres in the
+    amplitudes; each cell (ghost cells by their periodic image) then reads
+    its mesh value.  Otherwise the modes are summed directly."""
+    lev = grid.iLevelCoord[:, 0]
+    ext = [grid.xyzMax[d] - grid.xyzMin[d] for d in range(3)]
+    if grid.nDim == 3 and np.all(lev == lev[0]) and all(abs(e - 1.0) < 1e-14 for e in ext):
+        n = [grid.nRoot[d] * (1 << int(lev[0])) * (grid.nI, grid.nJ, grid.nK)[d] for d in range(3)]
+        spec = np.zeros(n, dtype=complex)
+        for (kx, ky, kz), a in zip(ks, amp):
+            x0 = [grid.xyzMin[d] + 0.5 / n[d] for d in range(3)]
+            shift = np.exp(2j * math.pi * (kx * x0[0] + ky * x0[1] + kz * x0[2]))
+            spec[kx % n[0], ky % n[1], kz % n[2]] += a * shift
+        mesh = (np.fft.ifftn(spec) * (n[0] * n[1] * n[2])).real
+        idx = [np.floor((xyz[..., d] - grid.xyzMin[d]) * n[d]).astype(np.int64) % n[d] for d in range(3)]
+        return mesh[idx[0], idx[1], idx[2]]
+    field = np.zeros(xyz.shape[:-1])
+    for (kx, ky, kz), a in zip(ks, amp):
+        ph = 2 * math.pi * (kx * xyz[..., 0] + ky * xyz[..., 1] + kz * xyz[..., 2])
+        field += (a * np.exp(1j * ph)).real
+    return field
+
+
 def perturbed_ot(grid, seed=2024, amplitude=1e-2, kmax=8):
     """Orszag-Tang plus a Gaussian random-phase perturbation of every
     primitive variable: sum over integer wave vectors 0 < |k| <= kmax of
@@ -90,11 +117,8 @@ def perturbed_ot(grid, seed=2024, amplitude=1e-2, kmax=8):
     ks = [(kx, ky, kz) for kx in range(-kmax, kmax + 1) for ky in range(-kmax, kmax + 1)
           for kz in range(0, kmax + 1) if 0 < kx * kx + ky * ky + kz * kz <= kmax * kmax]
     for v in range(NVAR):
-        field = np.zeros(xyz.shape[:-1])
         amp = rng.normal(size=len(ks)) + 1j * rng.normal(size=len(ks))
-        for (kx, ky, kz), a in zip(ks, amp):
-            ph = 2 * math.pi * (kx * xyz[..., 0] + ky * xyz[..., 1] + kz * xyz[..., 2])
-            field += (a * np.exp(1j * ph)).real
+        field = _random_phase_field(grid, xyz, ks, amp)
         field /= max(field.std(), 1e-300)
         if v in (0, 7):
             prim[..., v] *= 1.0 + amplitude * field

@@ -197,6 +197,65 @@ def run_ours(args):
     return out
 
 
+def run_jfnk(args, lrank):
+    """Implicit JFNK steps on the perturbed Orszag-Tang workload, wall time
+    per implicit step (CUDA events around whole steps, the host-side Krylov
+    control included) and Krylov matrix-vector products per step, for each
+    preconditioner."""
+    from batsrus_b200 import configs
+    from batsrus_b200.explicit import ExplicitSolver
+    from batsrus_b200.implicit import ImplicitSolver
+    g, s, _, st = configs.jfnk_ot(nRoot=args.jfnk_nroot)
+    out = {"workload": "perturbed_orszag_tang_%dcubed_bdf2_cfl20_gmres30_1e-3" % (8 * args.jfnk_nroot),
+           "cells": g.nCell, "blocks": g.nBlock, "steps": args.jfnk_steps, "warmup": args.jfnk_warmup,
+           "unit": "s/step", "higher_is_better": False}
+    for prec in args.jfnk_precond.split(","):
+        p = configs.jfnk_ot(nRoot=args.jfnk_nroot, precond=prec, with_state=False)[2]
+        x = ExplicitSolver(g, s, device=lrank)
+        x.set_state(st)
+        im = ImplicitSolver(x, p)
+        for _ in range(1 + args.jfnk_warmup):  # the first step only sets the time step
+            im.advance_part_impl()
+        x.synchronize()
+        x.region_begin()
+        stats = [im.advance_part_impl() for _ in range(args.jfnk_steps)]
+        ms = x.region_end()
+        out[prec.lower()] = {
+            "s_per_step": ms * 1e-3 / args.jfnk_steps,
+            "matvec_per_step": float(np.mean([q["nMatvec"] for q in stats])),
+            "matvec": [q["nMatvec"] for q in stats],
+            "krylov_error": [q["Error"] for q in stats],
+            "ms_precond_setup": float(np.mean([q["msPrecondSetup"] for q in stats])),
+            "converged": all(q["iError"] == 0 for q in stats)}
+        x.close()
+    return out
+
+
+def cpu_baseline_jfnk(args, seconds=20.0):
+    """The oracle's implicit step (BILU) on a 32^3 sample of the JFNK workload."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    from batsrus_b200 import configs
+    from oracle import Oracle
+    cores = os.cpu_count()
+    g, s, p, st = configs.jfnk_ot(nRoot=4)
+    o = Oracle(g, s, n_thread=cores)
+    o.set_state(st)
+    o.exchange_messages()
+    o.set_implicit(p)
+    o.advance_implicit()  # sets the time step
+    n, t0, nm = 0, time.perf_counter(), 0
+    while True:
+        r, m, _ = o.advance_implicit()
+        n, nm = n + 1, nm + m
+        el = time.perf_counter() - t0
+        if el > seconds or n >= 10:
+            break
+    return {"value": el / n, "unit": "s/step", "cores": cores, "kind": "port",
+            "matvec_per_step": nm / n,
+            "sample": "oracle/ C++ restatement of advance_part_impl with BILU, 32^3 (64 blocks) of the "
+                      "perturbed Orszag-Tang workload, %d steps on %d threads" % (n, cores)}
+
+
 def cpu_baseline(args, seconds=12.0):
     """The oracle (C++ restatement of the orig path, OpenMP over blocks) on a
     64^3 Orszag-Tang sample, on all host cores, timed until ~seconds."""
@@ -261,6 +320,10 @@ def main():
     ap.add_argument("--no-e2e", dest="e2e", action="store_false")
     ap.add_argument("--no-cpu", dest="cpu", action="store_false")
     ap.add_argument("--precisions", default="fp64,fp32")
+    ap.add_argument("--jfnk-precond", default="BILU,NONE", help="'' to skip the implicit workload")
+    ap.add_argument("--jfnk-nroot", type=int, default=16, help="16 -> 128^3 cells")
+    ap.add_argument("--jfnk-steps", type=int, default=5)
+    ap.add_argument("--jfnk-warmup", type=int, default=2)
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)
@@ -283,8 +346,12 @@ def main():
                            "roofline": r32["roofline"], "e2e": r32.get("e2e")} if r32 else None)}
     if "e2e" in r64:
         line["e2e"] = r64["e2e"]
+    if args.jfnk_precond:
+        line["jfnk"] = run_jfnk(args, 0)
     if args.cpu and world == 1:
         line["cpu_baseline"] = cpu_baseline(args)
+        if args.jfnk_precond:
+            line["jfnk"]["cpu_baseline"] = cpu_baseline_jfnk(args)
     print(json.dumps(line))
 
 

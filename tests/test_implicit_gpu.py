@@ -9,7 +9,8 @@ residual difference by eps = 1e-6/rms(x), which amplifies rounding by 1e6).
 The preconditioner is compared at 1e-10.  A whole step solves the linear
 system to the Krylov tolerance 1e-3; the GPU and oracle iterates differ
 only by the summation order of the FP64 inner products, so the step results
-agree to 1e-8 relative and the matrix-vector counts agree within one.
+(state and the time, whose next step is taken from the new state) agree to
+1e-8 relative and the matrix-vector counts agree within one.
 """
 import numpy as np
 import pytest
@@ -49,9 +50,11 @@ def test_gpu_jfnk_steps_match_oracle(prec):
         r, nm, err = o.advance_implicit()
         assert r == 0 and stats["iError"] == 0
         assert abs(stats["nMatvec"] - nm) <= 1, (step, stats["nMatvec"], nm)
+        # the next time step is taken from the new state, which agrees with
+        # the oracle's to the Krylov-iterate level, so the time does too
         to, dto, no = o.time()
         tg, _, ng = x.time()
-        assert ng == no and abs(tg - to) <= 1e-12 * max(to, 1.0)
+        assert ng == no and abs(tg - to) <= 1e-8 * max(to, 1.0), (step, tg, to)
         assert rel(x.get_state()[isl], o.get_state()[isl]) < 1e-8, step
 
 
