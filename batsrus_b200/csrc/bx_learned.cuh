@@ -1,0 +1,142 @@
+// bx_learned.cuh -- the learned per-block preconditioner: a 3-layer 3x3x3
+// convolutional network on one 8^3 block (16 -> 32 -> 32 -> 8 channels, ReLU
+// between layers, zero padding at the block faces), BF16 operands with FP32
+// accumulation on the tcgen05 tensor cores, and its training kernels.
+//
+// Each convolution is an implicit GEMM per block: M = cells (tiles of 128),
+// N = output channels, K = 27 taps x input channels, issued as one
+// 128 x N x 16 MMA per (tile, tap, 16-channel step).  Activations live in
+// shared memory in a padded "line" layout chosen so that the operand of a
+// shifted tap is the same layout at another start address:
+//   line(y, z) = (z + 1) * 9 + (y + 1),  y, z in [-1, 8]  (92 lines)
+//   byte(x, y, z, c) = line * LS + (c / 8) * 160 + (x + 1) * 16 + (c % 8) * 2
+// with LS = (C / 8) * 160.  Each line holds x = -1..8 (zero at both ends);
+// the y = -1 line of a plane doubles as the y = 8 line of the plane below,
+// and the planes z = -1 and z = 8 are zero, so every out-of-block neighbour
+// reads zero.  Rows of an M tile are 16 consecutive lines (8 cells each):
+// the K-major core matrices are the 8 cells of a line (16-byte rows) and the
+// tile's row groups are lines (SBO = LS).  The five tiles start at lines 10,
+// 26, 42, 58 and 65 and cover the cell lines 10..80; rows that fall on a
+// padding line are computed and discarded.
+#pragma once
+#include <cuda_bf16.h>
+
+#include "bx_tc.cuh"
+
+namespace bx {
+namespace learned {
+
+constexpr int kLines = 92;
+constexpr int kTiles = 5;
+constexpr int kThreads = 256;
+constexpr int kC0 = 16, kC1 = 32, kC2 = 32, kC3 = 8, kN3 = 16;  // channels (kN3: padded MMA N of layer 3)
+constexpr int kTaps = 27;
+// packed B images (bytes): forward layers, and the transposed images of the
+// backward-data products of layers 3 and 2
+constexpr int kW1Bytes = kTaps * kC1 * kC0 * 2;
+constexpr int kW2Bytes = kTaps * kC2 * kC1 * 2;
+constexpr int kW3Bytes = kTaps * kN3 * kC2 * 2;
+constexpr int kW3tBytes = kTaps * kC2 * kN3 * 2;
+constexpr int kW2tBytes = kTaps * kC1 * kC2 * 2;
+constexpr int kLS16 = 2 * 160, kLS32 = 4 * 160;
+constexpr int kBuf16 = kLines * kLS16, kBuf32 = kLines * kLS32;
+
+__host__ __device__ constexpr int tile_line0(int t) { return t < 4 ? 10 + 16 * t : 65; }
+__host__ __device__ constexpr int line_of(int y, int z) { return (z + 1) * 9 + y + 1; }
+
+// row r of tile t: its cell (or -1 for a padding row, or a row the previous
+// tile already produced)
+__device__ __forceinline__ int tile_row_cell(int t, int r) {
+  const int line = tile_line0(t) + (r >> 3);
+  if (line < 10 || line > 80 || line % 9 == 0) return -1;
+  if (t == 4 && line < 74) return -1;
+  const int y = line % 9 - 1, z = line / 9 - 1, x = r & 7;
+  return x + 8 * (y + 8 * z);
+}
+
+// byte offset of the 16-byte chunk kc of cell c in a buffer with line size LS
+__device__ __forceinline__ int cell_chunk(int c, int kc, int LS) {
+  const int x = c & 7, y = (c >> 3) & 7, z = c >> 6;
+  return line_of(y, z) * LS + kc * 160 + (x + 1) * 16;
+}
+
+// is the 16-byte unit (line, xs) of a buffer a cell (not padding)?
+__device__ __forceinline__ bool unit_is_cell(int line, int xs) {
+  return line >= 10 && line <= 80 && line % 9 != 0 && xs >= 1 && xs <= 8;
+}
+
+__device__ __forceinline__ uint32_t pack_bf16x2(float a, float b) {
+  __nv_bfloat162 h = __floats2bfloat162_rn(a, b);
+  return *reinterpret_cast<uint32_t *>(&h);
+}
+__device__ __forceinline__ float2 unpack_bf16x2(uint32_t u) {
+  __nv_bfloat162 h = *reinterpret_cast<__nv_bfloat162 *>(&u);
+  return __bfloat1622float2(h);
+}
+
+// one thread: the MMAs of one convolution over the five M tiles.
+// KCIN = input chunks of 8 channels (two per K step), N = output channels;
+// flip selects the transposed product (operand read at cell - tap).
+template <int KCIN, int N>
+__device__ __forceinline__ void issue_conv(uint32_t bufIn, uint32_t wImg, uint32_t tmem, bool flip) {
+  constexpr int LS = KCIN * 160;
+  constexpr uint32_t idesc = tc::idesc_bf16(128, N, false, false);
+  constexpr int tapBytes = N * KCIN * 16;
+  tc::fence_after();
+#pragma unroll 1
+  for (int t = 0; t < kTiles; t++) {
+    const int L0 = tile_line0(t);
+#pragma unroll 1
+    for (int tap = 0; tap < kTaps; tap++) {
+      int dz = tap / 9 - 1, dy = (tap / 3) % 3 - 1, dx = tap % 3 - 1;
+      if (flip) { dz = -dz; dy = -dy; dx = -dx; }
+      const uint32_t a0 = bufIn + (uint32_t)((L0 + dz * 9 + dy) * LS + (1 + dx) * 16);
+      const uint32_t b0 = wImg + (uint32_t)(tap * tapBytes);
+#pragma unroll
+      for (int s = 0; s < KCIN / 2; s++) {
+        const uint64_t ad = tc::sdesc(a0 + s * 320, 160, LS);
+        const uint64_t bd = tc::sdesc(b0 + s * 256, 128, KCIN * 128);
+        tc::mma_bf16(tmem + (uint32_t)(t * N), ad, bd, idesc, (tap | s) != 0);
+      }
+    }
+  }
+}
+
+// copy n bytes (multiple of 16) global -> shared with 16-byte loads
+__device__ __forceinline__ void copy_g2s(void *dst, const void *src, int n) {
+  const uint4 *s = reinterpret_cast<const uint4 *>(src);
+  uint4 *d = reinterpret_cast<uint4 *>(dst);
+  for (int i = threadIdx.x; i < n / 16; i += blockDim.x) d[i] = s[i];
+}
+
+__device__ __forceinline__ void zero_smem(void *dst, int n) {
+  uint4 *d = reinterpret_cast<uint4 *>(dst);
+  for (int i = threadIdx.x; i < n / 16; i += blockDim.x) d[i] = make_uint4(0, 0, 0, 0);
+}
+
+// zero the padding units of a buffer with KC chunks per line
+__device__ __forceinline__ void zero_pads(unsigned char *buf, int KC) {
+  const int nUnit = kLines * KC * 10;
+  for (int u = threadIdx.x; u < nUnit; u += blockDim.x) {
+    const int xs = u % 10, line = u / (10 * KC);
+    if (!unit_is_cell(line, xs)) *reinterpret_cast<uint4 *>(buf + u * 16) = make_uint4(0, 0, 0, 0);
+  }
+}
+
+// write a dense [cell][C] BF16 block (C = 8 KC) into the cell units of a buffer
+__device__ __forceinline__ void stage_dense(unsigned char *buf, const __nv_bfloat16 *src, int KC) {
+  const uint4 *s = reinterpret_cast<const uint4 *>(src);
+  for (int u = threadIdx.x; u < 512 * KC; u += blockDim.x) {
+    const int c = u / KC, kc = u % KC;
+    *reinterpret_cast<uint4 *>(buf + cell_chunk(c, kc, KC * 160)) = s[u];
+  }
+}
+
+struct Weights {
+  // packed BF16 images (global)
+  const unsigned char *w1, *w2, *w3, *w3t, *w2t;
+  const float *b1, *b2, *b3;  // biases (FP32)
+};
+
+}  // namespace learned
+}  // namespace bx

@@ -48,14 +48,15 @@ def peaks():
     return 6650.0, "fallback"
 
 
-def profile_traffic():
+def profile_traffic(prec):
     """DRAM bytes per cell and stage launch from the committed ncu summary
-    (profiles/stage_kernel_ot.md, line 'dram_bytes_per_cell_launch: X')."""
+    (profiles/stage_kernel_ot.md, lines 'dram_bytes_per_cell_launch[_fp32]: X')."""
     p = os.path.join(ROOT, "profiles", "stage_kernel_ot.md")
     if not os.path.exists(p):
         return None
+    key = "dram_bytes_per_cell_launch:" if prec == "fp64" else "dram_bytes_per_cell_launch_fp32:"
     for line in open(p):
-        if line.startswith("dram_bytes_per_cell_launch:"):
+        if line.startswith(key):
             return float(line.split(":")[1])
     return None
 
@@ -72,7 +73,7 @@ class ClockSampler:
              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
         try:
             self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), "--query-gpu=" + q,
-                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                          "--format=csv,noheader,nounits", "-lms", "50"],
                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
             self.t.start()
@@ -161,7 +162,7 @@ def run_ours(args):
         value = world * nCell * args.steps / (ms * 1e-3)
         launch_bytes = BYTES_PER_CELL_STEP[prec] / 2 * nCell  # average over the 2 stages
         achieved = launch_bytes / (kern_ms * 1e-3) / 1e9
-        t_per_cell = profile_traffic()
+        t_per_cell = profile_traffic(prec)
         res = {"value": value, "ms_per_step": ms / args.steps, "kernel_ms": kern_ms,
                "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": hbm_peak,
                             "unit": "GB/s", "frac": round(achieved / hbm_peak, 4),
