@@ -32,6 +32,9 @@ EXPORTS = (
     "bx_region_begin", "bx_region_end",
     "bx_implicit_init", "bx_advance_part_impl", "bx_impl_get_rhs", "bx_impl_matvec",
     "bx_impl_precond", "bx_impl_get_x",
+    "bx_learned_init", "bx_learned_finalize", "bx_learned_nparam", "bx_learned_set_params",
+    "bx_learned_get_params", "bx_learned_collect", "bx_learned_num_samples", "bx_learned_set_samples",
+    "bx_learned_gradient", "bx_learned_train", "bx_learned_apply_blocks",
 )
 PRECOND = {"none": 0, "bilu": 1, "learned": 2}
 
@@ -110,6 +113,7 @@ def load():
     L = ctypes.CDLL(LIB_PATH)
     i, d, p = ctypes.c_int, ctypes.c_double, ctypes.c_void_p
     dp, ip = ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_int)
+    fp = ctypes.POINTER(ctypes.c_float)
     sig = {
         "bx_init": [ctypes.POINTER(GridDesc), ctypes.POINTER(SchemeParams)],
         "bx_set_scheme": [ctypes.POINTER(SchemeParams)],
@@ -127,6 +131,13 @@ def load():
         "bx_advance_part_impl": [d, ctypes.POINTER(KrylovStats)],
         "bx_impl_get_rhs": [dp, dp], "bx_impl_matvec": [dp, dp], "bx_impl_precond": [dp, dp],
         "bx_impl_get_x": [dp],
+        "bx_learned_init": [ctypes.c_longlong, ctypes.c_ulonglong], "bx_learned_finalize": [],
+        "bx_learned_nparam": [ip], "bx_learned_set_params": [fp, i], "bx_learned_get_params": [fp, i],
+        "bx_learned_collect": [i], "bx_learned_num_samples": [ctypes.POINTER(ctypes.c_longlong)],
+        "bx_learned_set_samples": [fp, fp, ctypes.c_longlong],
+        "bx_learned_gradient": [ctypes.c_longlong, i, fp, dp],
+        "bx_learned_train": [i, i, d, dp, dp],
+        "bx_learned_apply_blocks": [dp, fp, i, dp],
     }
     for name, args in sig.items():
         f = getattr(L, name)
@@ -146,6 +157,10 @@ def check(code):
 
 def dptr(a):
     return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+def fptr(a):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_float))
 
 
 def grid_desc(grid, device=0):

@@ -27,4 +27,12 @@ int core_encode_maps(void *base, bool fp32, TmaMaps &m);
 // release the implicit context (its buffers are sized for the current grid)
 void impl_release();
 
+// learned preconditioner hooks (bx_learned.cu); vectors in the solver's
+// [block][var][cell] layout of 8^3 blocks
+bool learned_ready();
+bool learned_collecting();
+int learned_features(const double *U, const double *norm, int nBlock, cudaStream_t st);
+int learned_apply(const double *v, double *z, int nBlock, cudaStream_t st);
+int learned_collect(const double *w, const double *z, int nBlock, cudaStream_t st);
+
 }  // namespace bx

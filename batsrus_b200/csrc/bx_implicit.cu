@@ -149,6 +149,10 @@ int matvec(const double *x, double *y) {
 
 int precond(const double *r, double *z) {
   Core c = core();
+  if (I.p.TypePrecond == BX_PRECOND_LEARNED) {
+    if (c.nI != 8) return core_fail(BX_ERR_ARG, "the learned preconditioner works on 8x8x8 blocks");
+    return learned_apply(r, z, c.nBlock, c.st);
+  }
   if (I.p.TypePrecond == BX_PRECOND_BILU && I.havePrec) {
     BiluArgs b;
     b.Jac = I.Jac; b.Dinv = I.Dinv; b.wfCell = I.wfCell; b.wfStart = I.wfStart; b.nWave = I.nWave;
@@ -195,6 +199,7 @@ int gmres(int &iError) {
       double *Vk = I.V + (size_t)k * N, *Zk = I.Z + (size_t)k * N;
       if ((r = precond(Vk, Zk))) return r;
       if ((r = matvec(Zk, I.W))) return r;
+      if (learned_collecting() && c.nI == 8 && (r = learned_collect(I.W, Zk, c.nBlock, c.st))) return r;
       for (int q = 0; q <= k + 1; q++) {
         const double *vq = q > 0 ? I.V + (size_t)(q - 1) * N : nullptr;
         const double *hq = q > 0 ? hdev + q - 1 : nullptr;
@@ -434,6 +439,11 @@ int bx_advance_part_impl(double tLimit, bx_krylov_stats *stats) {
   CKI(cudaEventRecord(I.ev[1], c.st));
   I.havePrec = false;
   if (I.p.TypePrecond == BX_PRECOND_BILU && (r = build_precond())) return r;
+  if (I.p.TypePrecond == BX_PRECOND_LEARNED && !learned_ready())
+    return core_fail(BX_ERR_STATE, "TypePrecond LEARNED needs bx_learned_init (and trained parameters)");
+  if ((I.p.TypePrecond == BX_PRECOND_LEARNED || learned_collecting()) && c.nI == 8 &&
+      (r = learned_features(I.U, I.dNorm, c.nBlock, c.st)))
+    return r;
   CKI(cudaEventRecord(I.ev[2], c.st));
   int iError = 0;
   if ((r = gmres(iError))) return r;

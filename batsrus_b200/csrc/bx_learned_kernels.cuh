@@ -299,3 +299,248 @@ __global__ void __launch_bounds__(kThreads, 1)
   tc::fence_after();
   if ((threadIdx.x >> 5) == 0) tc::tmem_free(tmem, 256);
 }
+
+// ---------------------------------------------------------------------------
+// training backward through layers 3 and 2: dY2 = (dY3 *T W3) . [A2 > 0],
+// dY1 = (dY2 *T W2) . [A1 > 0] (BF16 [sample][cell][32]); accumulates the
+// bias gradients of layers 2 and 1.  W.w3t / W.w2t are the transposed images
+// (N = input channels of the layer, K = its output channels).
+__global__ void __launch_bounds__(kThreads, 1)
+    k_net_bwd_data(Weights W, const __nv_bfloat16 *__restrict__ dY3, const __nv_bfloat16 *__restrict__ A2,
+                   const __nv_bfloat16 *__restrict__ A1, int nSample, __nv_bfloat16 *dY2, __nv_bfloat16 *dY1,
+                   float *gb2, float *gb1, int *err) {
+  extern __shared__ __align__(1024) unsigned char sm[];
+  unsigned char *bufA = sm, *bufB = sm + kBuf32;
+  unsigned char *w3t = bufB + kBuf32, *w2t = w3t + kW3tBytes;
+  Smem &S = *reinterpret_cast<Smem *>(w2t + kW2tBytes);
+  zero_smem(bufA, kBuf32);
+  zero_smem(bufB, kBuf32);
+  copy_g2s(w3t, W.w3t, kW3tBytes);
+  copy_g2s(w2t, W.w2t, kW2tBytes);
+  setup(S, W);
+  if ((threadIdx.x >> 5) == 0) tc::tmem_alloc(&S.tmem, 256);
+  tc::fence_before();
+  __syncthreads();
+  tc::fence_after();
+  const uint32_t tmem = S.tmem;
+  uint32_t phase = 0;
+  bool ok = true;
+  float g2[32], g1[32];
+#pragma unroll
+  for (int m = 0; m < 32; m++) g2[m] = g1[m] = 0.f;
+  for (int n = blockIdx.x; n < nSample && ok; n += gridDim.x) {
+    stage_dense(bufB, dY3 + (size_t)n * 512 * 16, 2);  // 16-channel layout, pads zero throughout
+    fence_proxy_async_smem();
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      issue_conv<2, 32>(smem_u32(bufB), smem_u32(w3t), tmem, true);
+      tc::commit(&S.bar);
+    }
+    if (!(ok = wait_mma(S, phase))) break;
+    const __nv_bfloat16 *a2 = A2 + (size_t)n * 512 * 32, *a1 = A1 + (size_t)n * 512 * 32;
+    __nv_bfloat16 *d2 = dY2 + (size_t)n * 512 * 32, *d1 = dY1 + (size_t)n * 512 * 32;
+    auto masked = [&](int cell, const float(&acc)[32], const __nv_bfloat16 *act, __nv_bfloat16 *gout,
+                      unsigned char *buf, float(&gb)[32]) {
+      const uint4 *am = reinterpret_cast<const uint4 *>(act + (size_t)cell * 32);
+      uint4 q[4];
+      uint32_t *w = reinterpret_cast<uint32_t *>(q);
+#pragma unroll
+      for (int kc = 0; kc < 4; kc++) {
+        const uint4 a4 = am[kc];
+        const uint32_t aw[4] = {a4.x, a4.y, a4.z, a4.w};
+#pragma unroll
+        for (int i = 0; i < 4; i++) {
+          const float2 a = unpack_bf16x2(aw[i]);
+          const int c = 8 * kc + 2 * i;
+          w[4 * kc + i] = pack_bf16x2(a.x > 0.f ? acc[c] : 0.f, a.y > 0.f ? acc[c + 1] : 0.f);
+          const float2 r = unpack_bf16x2(w[4 * kc + i]);
+          gb[c] += r.x;
+          gb[c + 1] += r.y;
+        }
+      }
+      uint4 *g = reinterpret_cast<uint4 *>(gout + (size_t)cell * 32);
+#pragma unroll
+      for (int kc = 0; kc < 4; kc++) {
+        g[kc] = q[kc];
+        if (buf) *reinterpret_cast<uint4 *>(buf + cell_chunk(cell, kc, kLS32)) = q[kc];
+      }
+    };
+    for_tiles<32>(tmem, [&](int, int, int cell, const float(&acc)[32]) {
+      if (cell >= 0) masked(cell, acc, a2, d2, bufA, g2);
+    });
+    tc::fence_before();
+    fence_proxy_async_smem();
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      issue_conv<4, 32>(smem_u32(bufA), smem_u32(w2t), tmem, true);
+      tc::commit(&S.bar);
+    }
+    if (!(ok = wait_mma(S, phase))) break;
+    for_tiles<32>(tmem, [&](int, int, int cell, const float(&acc)[32]) {
+      if (cell >= 0) masked(cell, acc, a1, d1, nullptr, g1);
+    });
+    tc::fence_before();
+    __syncthreads();
+  }
+#pragma unroll
+  for (int m = 0; m < 32; m++)
+    for (int o = 16; o > 0; o >>= 1) {
+      g2[m] += __shfl_xor_sync(0xffffffffu, g2[m], o);
+      g1[m] += __shfl_xor_sync(0xffffffffu, g1[m], o);
+    }
+  if ((threadIdx.x & 31) == 0)
+#pragma unroll
+    for (int m = 0; m < 32; m++) {
+      atomicAdd(gb2 + m, g2[m]);
+      atomicAdd(gb1 + m, g1[m]);
+    }
+  if (!ok && threadIdx.x == 0) atomicOr(err, kErrTimeout);
+  __syncthreads();
+  tc::fence_after();
+  if ((threadIdx.x >> 5) == 0) tc::tmem_free(tmem, 256);
+}
+
+// ---------------------------------------------------------------------------
+// weight gradient of one layer over the taps [tap0, tap0 + nTap):
+//   dW[tap][ci][co] = sum over samples and cells of X[cell + tap][ci] dY[cell][co]
+// One M = 64 MMA per (tap, pair of lines): A = dY^T (MN-major, rows = output
+// channels in 16-byte chunks, K = the 16 cells of two lines), B = X shifted
+// by the tap (MN-major, N = input channels).  Rows of A past the layer's
+// output channels read the following line and are discarded.  TMEM holds
+// nTap * CIN columns; each CTA writes its partial sums to
+// part[cta][tap - tap0][ci][co] (co < CO).
+template <int KCX, int KCD, int CO>
+__global__ void __launch_bounds__(kThreads, 1)
+    k_net_dw(const __nv_bfloat16 *__restrict__ X, const __nv_bfloat16 *__restrict__ dY, int nSample, int tap0,
+             int nTap, float *part, int *err) {
+  constexpr int CIN = 8 * KCX, LSX = KCX * 160, LSD = KCD * 160;
+  extern __shared__ __align__(1024) unsigned char sm[];
+  unsigned char *bufX = sm, *bufD = sm + kLines * LSX;
+  Smem &S = *reinterpret_cast<Smem *>(bufD + kLines * LSD);
+  zero_smem(bufX, kLines * LSX);
+  zero_smem(bufD, kLines * LSD);
+  if (threadIdx.x == 0) {
+    mbar_init(&S.bar, 1);
+    fence_mbar_init();
+  }
+  if ((threadIdx.x >> 5) == 0) tc::tmem_alloc(&S.tmem, 512);
+  tc::fence_before();
+  __syncthreads();
+  tc::fence_after();
+  const uint32_t tmem = S.tmem;
+  constexpr uint32_t idesc = tc::idesc_bf16(64, CIN, true, true);
+  uint32_t phase = 0;
+  bool ok = true, first = true;
+  for (int n = blockIdx.x; n < nSample && ok; n += gridDim.x) {
+    stage_dense(bufX, X + (size_t)n * 512 * CIN, KCX);
+    stage_dense(bufD, dY + (size_t)n * 512 * 8 * KCD, KCD);
+    fence_proxy_async_smem();
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      tc::fence_after();
+      const uint32_t x0 = smem_u32(bufX), d0 = smem_u32(bufD);
+      for (int tl = 0; tl < nTap; tl++) {
+        const int tap = tap0 + tl;
+        const int dz = tap / 9 - 1, dy = (tap / 3) % 3 - 1, dx = tap % 3 - 1;
+        for (int L = 10; L <= 80; L += 2) {
+          const uint64_t ad = tc::sdesc(d0 + (uint32_t)(L * LSD + 16), LSD, 160);
+          const uint64_t bd = tc::sdesc(x0 + (uint32_t)((L + dz * 9 + dy) * LSX + (1 + dx) * 16), LSX, 160);
+          tc::mma_bf16(tmem + (uint32_t)(tl * CIN), ad, bd, idesc, (first && L == 10) ? 0u : 1u);
+        }
+      }
+      tc::commit(&S.bar);
+    }
+    first = false;
+    if (!(ok = wait_mma(S, phase))) break;
+    tc::fence_before();
+    __syncthreads();
+  }
+  if (ok && !first) {
+    // rows co = 16 q + lane (lanes 0..15 of quarters q = 0, 1); columns tl*CIN + ci
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, q = warp & 3;
+    if (q < 2) {
+      const int nChunk = nTap * CIN / 16;
+      for (int j = warp >> 2; j < nChunk; j += kThreads / 128) {
+        float v[16];
+        tc::tmem_ld16(tmem + ((uint32_t)(32 * q) << 16) + (uint32_t)(16 * j), v);
+        const int co = 16 * q + lane;
+        if (lane < 16 && co < CO)
+#pragma unroll
+          for (int i = 0; i < 16; i++) {
+            const int col = 16 * j + i, tl = col / CIN, ci = col % CIN;
+            part[(((size_t)blockIdx.x * nTap + tl) * CIN + ci) * CO + co] = v[i];
+          }
+      }
+    }
+  } else if (first) {
+    // no sample: zero partial sums
+    for (int i = threadIdx.x; i < nTap * CIN * CO; i += kThreads) part[(size_t)blockIdx.x * nTap * CIN * CO + i] = 0.f;
+  }
+  if (!ok && threadIdx.x == 0) atomicOr(err, kErrTimeout);
+  tc::fence_before();
+  __syncthreads();
+  tc::fence_after();
+  if ((threadIdx.x >> 5) == 0) tc::tmem_free(tmem, 512);
+}
+
+// ---------------------------------------------------------------------------
+// parameter vector (FP32): W1[27][16][32] b1[32] W2[27][32][32] b2[32]
+// W3[27][32][8] b3[8]
+constexpr int kOffW1 = 0, kOffB1 = kOffW1 + kTaps * kC0 * kC1, kOffW2 = kOffB1 + kC1,
+              kOffB2 = kOffW2 + kTaps * kC1 * kC2, kOffW3 = kOffB2 + kC2, kOffB3 = kOffW3 + kTaps * kC2 * kC3,
+              kNParam = kOffB3 + kC3;
+
+// image of one K-major B operand: element (n, k) of tap at
+// tap*N*K*2 + (n/8)*(K/8)*128 + (k/8)*128 + (n%8)*16 + (k%8)*2
+__device__ __forceinline__ int bimg_index(int tap, int n, int k, int N, int K) {
+  return (tap * N * K + (n >> 3) * (K >> 3) * 64 + (k >> 3) * 64 + (n & 7) * 8 + (k & 7));
+}
+
+// pack the five BF16 images from the FP32 parameters
+__global__ void k_pack(const float *__restrict__ p, __nv_bfloat16 *w1, __nv_bfloat16 *w2, __nv_bfloat16 *w3,
+                       __nv_bfloat16 *w3t, __nv_bfloat16 *w2t) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  // forward images: n = output channel, k = input channel
+  if (i < kTaps * kC1 * kC0) {  // w1: N 32, K 16
+    const int tap = i / (kC1 * kC0), n = (i / kC0) % kC1, k = i % kC0;
+    w1[bimg_index(tap, n, k, kC1, kC0)] = __float2bfloat16_rn(p[kOffW1 + (tap * kC0 + k) * kC1 + n]);
+  }
+  if (i < kTaps * kC2 * kC1) {  // w2: N 32, K 32; w2t: n = ci, k = co
+    const int tap = i / (kC2 * kC1), n = (i / kC1) % kC2, k = i % kC1;
+    w2[bimg_index(tap, n, k, kC2, kC1)] = __float2bfloat16_rn(p[kOffW2 + (tap * kC1 + k) * kC2 + n]);
+    w2t[bimg_index(tap, n, k, kC1, kC2)] = __float2bfloat16_rn(p[kOffW2 + (tap * kC1 + n) * kC2 + k]);
+  }
+  if (i < kTaps * kN3 * kC2) {  // w3: N 16 (8 used), K 32; w3t: N 32 (ci), K 16 (co, 8 used)
+    const int tap = i / (kN3 * kC2), n = (i / kC2) % kN3, k = i % kC2;
+    w3[bimg_index(tap, n, k, kN3, kC2)] =
+        __float2bfloat16_rn(n < kC3 ? p[kOffW3 + (tap * kC2 + k) * kC3 + n] : 0.f);
+    // transposed: n' = k (ci), k' = n (co)
+    w3t[bimg_index(tap, k, n, kC2, kN3)] =
+        __float2bfloat16_rn(n < kC3 ? p[kOffW3 + (tap * kC2 + k) * kC3 + n] : 0.f);
+  }
+}
+
+// grad[j] = sum over CTAs of part[cta][j] for one layer's weight block
+__global__ void k_sum_parts(const float *__restrict__ part, int nCta, int nPer, float *grad) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= nPer) return;
+  float s = 0.f;
+  for (int c = 0; c < nCta; c++) s += part[(size_t)c * nPer + j];
+  grad[j] = s;
+}
+
+// Adam (bias-corrected), FP32 master parameters
+__global__ void k_adam(float *p, float *m, float *v, const float *g, int n, float lr, float b1, float b2, float eps,
+                       float c1, float c2) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const float gi = g[i];
+  const float mi = b1 * m[i] + (1.f - b1) * gi;
+  const float vi = b2 * v[i] + (1.f - b2) * gi * gi;
+  m[i] = mi;
+  v[i] = vi;
+  p[i] -= lr * (mi / c1) / (sqrtf(vi / c2) + eps);
+}
+
+}  // namespace learned
+}  // namespace bx

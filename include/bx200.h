@@ -186,6 +186,41 @@ BX_API int bx_impl_matvec(const double *x_I, double *y_I);
 BX_API int bx_impl_precond(const double *r_I, double *z_I);
 BX_API int bx_impl_get_x(double *x_I);
 
+/* ---- learned per-block preconditioner -------------------------------------
+ * No counterpart in the reference: a new #PRECONDITIONER value LEARNED for
+ * the FGMRES of advance_part_impl (TypePrecond = BX_PRECOND_LEARNED).  A
+ * 3-layer 3x3x3 convolutional network per 8^3 block (16 -> 32 -> 32 -> 8
+ * channels, ReLU, zero padding at the block faces) maps the block of a
+ * Krylov vector (scaled by its block RMS s) and the block's normalised state
+ * to the correction, z = s N(v / s, U / Norm_V); BF16 operands, FP32
+ * accumulation on the tensor cores.  Training pairs (w = A z, z) are taken
+ * from the BILU-preconditioned FGMRES iterations of implicit steps.  FGMRES
+ * accepts any preconditioner, so the network changes iteration counts, not
+ * the converged answer.  Parameter vector (FP32):
+ *   W1[27][16][32] b1[32] W2[27][32][32] b2[32] W3[27][32][8] b3[8]
+ * with tap = (dz+1)*9 + (dy+1)*3 + (dx+1). */
+BX_API int bx_learned_init(long long nSampleMax, unsigned long long seed);
+BX_API int bx_learned_finalize(void);
+BX_API int bx_learned_nparam(int *nParam);
+BX_API int bx_learned_set_params(const float *params, int nParam);
+BX_API int bx_learned_get_params(float *params, int nParam);
+/* store blocksPerPair randomly chosen blocks of every (w, z) pair of the
+ * following implicit steps' FGMRES iterations (0 stops collecting) */
+BX_API int bx_learned_collect(int blocksPerPair);
+BX_API int bx_learned_num_samples(long long *nSample);
+/* replace the training set: in16 [nSample][512][16] (input / s, then the 8
+ * features), tgt [nSample][512][8] (target / s); cell = i + 8 j + 64 k */
+BX_API int bx_learned_set_samples(const float *in16, const float *tgt, long long nSample);
+/* gradient of the mean squared error over samples [s0, s0 + nS) (nS <= 1024)
+ * without an update; lossSum = sum of squared errors */
+BX_API int bx_learned_gradient(long long s0, int nS, float *grad, double *lossSum);
+/* Adam over the stored samples in mini-batches; mean squared error of the
+ * first and the last epoch */
+BX_API int bx_learned_train(int nEpoch, int batch, double learningRate, double *lossFirst, double *lossLast);
+/* the preconditioner on host blocks: v, z [nBlock][8][512] (solver layout),
+ * feat [nBlock][512][8] */
+BX_API int bx_learned_apply_blocks(const double *v, const float *feat, int nBlock, double *z);
+
 /* ---- measurement ----------------------------------------------------------
  * Kernel timing with CUDA events on the library's stream: when enabled, the
  * fused stage kernel launches are bracketed by events; the average duration

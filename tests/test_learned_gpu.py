@@ -1,0 +1,118 @@
+"""GPU checks of the learned per-block preconditioner (tcgen05 kernels)
+against the numpy reference oracle/learned_ref.py, through the C ABI:
+
+* the inference kernel on random blocks and parameters;
+* the training gradient (forward, backward-data and weight-gradient
+  kernels) on random samples;
+* training lowers the loss on a learnable synthetic target;
+* FGMRES with the trained network: the implicit steps converge to the
+  Krylov tolerance, agree with the BILU steps to that tolerance, and need
+  fewer Krylov iterations than the solver without a preconditioner.
+
+Tolerances: both sides use the same BF16-rounded operands; the GPU sums in
+FP32 (the reference in FP64) and an intermediate activation can round to a
+neighbouring BF16 value, so outputs agree to ~1e-3 relative (test 1e-2) and
+gradients to ~1e-2 (test 3e-2 per parameter group).
+"""
+import numpy as np
+import pytest
+
+import learned_ref as lr
+from batsrus_b200 import configs
+from batsrus_b200.explicit import ExplicitSolver
+from batsrus_b200.implicit import ImplicitSolver
+from batsrus_b200.learned import LearnedPreconditioner
+
+pytestmark = pytest.mark.gpu
+
+
+def relerr(a, b):
+    return np.linalg.norm(np.ravel(a) - np.ravel(b)) / max(np.linalg.norm(np.ravel(b)), 1e-300)
+
+
+@pytest.fixture
+def net():
+    n = LearnedPreconditioner(nSampleMax=4096, seed=11)
+    yield n
+    n.close()
+
+
+def test_apply_matches_reference(net):
+    rng = np.random.default_rng(1)
+    p = lr.init_params(seed=3, out_gain=1.0).astype(np.float32)
+    net.set_params(p)
+    nb = 7
+    v = rng.normal(size=(nb, 8, 512)) * 10.0 ** rng.uniform(-3, 3, size=(nb, 1, 1))
+    v[3] = 0.0  # an all-zero block maps to zero
+    feat = rng.normal(size=(nb, 512, 8)).astype(np.float32)
+    z = net.apply_blocks(v, feat)
+    zr = lr.apply(p, v, feat)
+    assert np.all(z[3] == 0.0)
+    for b in range(nb):
+        if b != 3:
+            assert relerr(z[b], zr[b]) < 1e-2, (b, relerr(z[b], zr[b]))
+
+
+def test_gradient_matches_reference(net):
+    rng = np.random.default_rng(2)
+    p = lr.init_params(seed=4, out_gain=1.0).astype(np.float32)
+    net.set_params(p)
+    n = 5
+    x0 = rng.normal(size=(n, 512, 16)).astype(np.float32)
+    tgt = rng.normal(size=(n, 512, 8)).astype(np.float32)
+    net.set_samples(x0, tgt)
+    loss, g = net.gradient(0, n)
+    lref, gref = lr.loss_and_grad(p, x0.reshape(n, 8, 8, 8, 16), tgt.reshape(n, 8, 8, 8, 8), bf=True)
+    assert abs(loss - lref) <= 1e-3 * lref
+    o = 0
+    for name, shp in lr.SHAPES:
+        k = int(np.prod(shp))
+        assert relerr(g[o:o + k], gref[o:o + k]) < 3e-2, (name, relerr(g[o:o + k], gref[o:o + k]))
+        o += k
+
+
+def test_training_lowers_the_loss(net):
+    # learnable target: a fixed random network of the same shape
+    rng = np.random.default_rng(3)
+    teacher = lr.init_params(seed=9, out_gain=1.0)
+    n = 1024
+    x0 = rng.normal(size=(n, 512, 16)).astype(np.float32)
+    tgt, _, _ = lr.forward(teacher, x0.reshape(n, 8, 8, 8, 16))
+    net.set_samples(x0, tgt.reshape(n, 512, 8).astype(np.float32))
+    first, last = net.train(nEpoch=8, batch=128, lr=3e-3)
+    assert np.isfinite(first) and np.isfinite(last)
+    assert last < 0.5 * first, (first, last)
+
+
+def _jfnk(prec, state, net=None, steps=3):
+    g, s, p, _ = configs.jfnk_ot(nRoot=4, precond=prec, with_state=False)
+    x = ExplicitSolver(g, s)
+    x.set_state(state)
+    im = ImplicitSolver(x, p)
+    out = [im.advance_part_impl() for _ in range(steps)]
+    st = x.get_state()
+    x.close()
+    return out, st, g
+
+
+def test_learned_fgmres_converges_and_gains(net):
+    g, s, p, st = configs.jfnk_ot(nRoot=4)
+    # collect (w = A z, z) pairs from BILU-preconditioned steps, then train
+    net.collect(64)
+    _jfnk("BILU", st, steps=6)
+    net.collect(0)
+    assert net.num_samples() > 1000
+    first, last = net.train(nEpoch=12, batch=128, lr=2e-3)
+    assert last < first
+    bilu, sb, g = _jfnk("BILU", st)
+    none, sn, _ = _jfnk("NONE", st)
+    lrn, sl, _ = _jfnk("LEARNED", st)
+    isl = g.interior_slices()
+    for q in lrn:
+        assert q["iError"] == 0 and q["Error"] <= 1e-3
+    # same answer to the Krylov tolerance
+    du = np.abs(sb[isl] - st[isl]).max()
+    assert np.abs(sl[isl] - sb[isl]).max() <= 2e-2 * du
+    # what the network gains over the solver without a preconditioner
+    assert sum(q["nMatvec"] for q in lrn[1:]) < sum(q["nMatvec"] for q in none[1:]), (
+        [q["nMatvec"] for q in lrn], [q["nMatvec"] for q in none], [q["nMatvec"] for q in bilu])
