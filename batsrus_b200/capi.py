@@ -35,8 +35,10 @@ EXPORTS = (
     "bx_learned_init", "bx_learned_finalize", "bx_learned_nparam", "bx_learned_set_params",
     "bx_learned_get_params", "bx_learned_collect", "bx_learned_num_samples", "bx_learned_set_samples",
     "bx_learned_gradient", "bx_learned_train", "bx_learned_apply_blocks",
+    "bx_impl_norm_noalloc",
 )
 PRECOND = {"none": 0, "bilu": 1, "learned": 2}
+NOALLOC_MAX_BLOCK = 32768  # BX_NOALLOC_MAX_BLOCK
 
 
 class ImplicitParamsC(ctypes.Structure):
@@ -138,6 +140,7 @@ def load():
         "bx_learned_gradient": [ctypes.c_longlong, i, fp, dp],
         "bx_learned_train": [i, i, d, dp, dp],
         "bx_learned_apply_blocks": [dp, fp, i, dp],
+        "bx_impl_norm_noalloc": [p, i, i, p, dp],
     }
     for name, args in sig.items():
         f = getattr(L, name)

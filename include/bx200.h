@@ -186,6 +186,26 @@ BX_API int bx_impl_matvec(const double *x_I, double *y_I);
 BX_API int bx_impl_precond(const double *r_I, double *z_I);
 BX_API int bx_impl_get_x(double *x_I);
 
+/* Norm_V of the implicit scheme (the RMS of each implicit variable over all
+ * cells, as in impl_newton_init) for a vector the CALLER keeps on the device,
+ * with no device allocation.  No counterpart in the reference.
+ *   Impl_dev  device pointer, reference Impl_VGB order (variable fastest,
+ *             then the nCellBlock cells of a block, then the nBlock blocks)
+ *   stream    cudaStream_t to run on (NULL: the default stream)
+ *   Norm_V    host array of 8, written on return (the call synchronizes
+ *             the stream)
+ * For callers that cannot let a library allocate device memory: a host whose
+ * device memory is all reserved by its own pool or OpenACC data regions, or
+ * that cannot afford the device-wide synchronization of cudaMalloc/cudaFree
+ * while other streams run.  It calls no cudaMalloc, cudaFree or allocating
+ * library: the scratch is a static device array for at most
+ * BX_NOALLOC_MAX_BLOCK blocks; larger nBlock is rejected with BX_ERR_ARG.
+ * The first call on a device looks up the scratch address (make it before
+ * any stream capture).  Calls that overlap on the GPU share the scratch and
+ * race: serialize them.  Independent of bx_init. */
+#define BX_NOALLOC_MAX_BLOCK 32768
+BX_API int bx_impl_norm_noalloc(const double *Impl_dev, int nCellBlock, int nBlock, void *stream, double *Norm_V);
+
 /* ---- learned per-block preconditioner -------------------------------------
  * No counterpart in the reference: a new #PRECONDITIONER value LEARNED for
  * the FGMRES of advance_part_impl (TypePrecond = BX_PRECOND_LEARNED).  A
