@@ -132,7 +132,8 @@ __global__ void k_features(const double *__restrict__ U, const double *__restric
 }
 
 // store the picked blocks of the pair (w = A z, z) as training samples
-// base + i: input w / s and the features, target z / s (s = RMS of w)
+// base + i: input w / s and the features, target (z - w) / s (s = RMS of w;
+// the network is the correction to the identity)
 __global__ void k_collect(const double *__restrict__ w, const double *__restrict__ z,
                           const __nv_bfloat16 *__restrict__ feat, const int *__restrict__ pick, long base,
                           __nv_bfloat16 *in16, float *tgt) {
@@ -160,7 +161,7 @@ __global__ void k_collect(const double *__restrict__ w, const double *__restrict
     dst[0] = q[0];
     dst[1] = q[1];
 #pragma unroll
-    for (int m = 0; m < 8; m++) tgt[(n * 512 + c) * 8 + m] = (float)(zb[m * 512 + c] * inv);
+    for (int m = 0; m < 8; m++) tgt[(n * 512 + c) * 8 + m] = (float)((zb[m * 512 + c] - wb[m * 512 + c]) * inv);
   }
 }
 

@@ -210,8 +210,11 @@ def run_jfnk(args, lrank):
     out = {"workload": "perturbed_orszag_tang_%dcubed_bdf2_cfl20_gmres30_1e-3" % (8 * args.jfnk_nroot),
            "cells": g.nCell, "blocks": g.nBlock, "steps": args.jfnk_steps, "warmup": args.jfnk_warmup,
            "unit": "s/step", "higher_is_better": False}
+    net = None
     for prec in args.jfnk_precond.split(","):
         p = configs.jfnk_ot(nRoot=args.jfnk_nroot, precond=prec, with_state=False)[2]
+        if prec.upper() == "LEARNED" and net is None:
+            net, out["learned_training"] = train_learned(args, g, s, lrank)
         x = ExplicitSolver(g, s, device=lrank)
         x.set_state(st)
         im = ImplicitSolver(x, p)
@@ -229,7 +232,40 @@ def run_jfnk(args, lrank):
             "ms_precond_setup": float(np.mean([q["msPrecondSetup"] for q in stats])),
             "converged": all(q["iError"] == 0 for q in stats)}
         x.close()
+    if net is not None:
+        net.close()
     return out
+
+
+def train_learned(args, g, s, lrank, nPair=2000, blocksPerPair=16):
+    """Training data and training of the learned preconditioner: (w = A z, z)
+    pairs from the BILU-preconditioned FGMRES of implicit steps started from
+    a differently seeded perturbation (seed 2025) than the timed steps,
+    blocksPerPair random blocks of each of nPair pairs; then Adam."""
+    from batsrus_b200 import configs
+    from batsrus_b200.explicit import ExplicitSolver
+    from batsrus_b200.implicit import ImplicitSolver
+    from batsrus_b200.learned import LearnedPreconditioner
+    net = LearnedPreconditioner(nSampleMax=nPair * blocksPerPair, seed=2024)
+    _, _, p, st2 = configs.jfnk_ot(nRoot=args.jfnk_nroot, precond="BILU", seed=2025)
+    x = ExplicitSolver(g, s, device=lrank)
+    x.set_state(st2)
+    im = ImplicitSolver(x, p)
+    t0 = time.perf_counter()
+    net.collect(blocksPerPair)
+    nStep = 0
+    while net.num_samples() < nPair * blocksPerPair and nStep < 200:
+        im.advance_part_impl()
+        nStep += 1
+    net.collect(0)
+    x.close()
+    t1 = time.perf_counter()
+    first, last = net.train(nEpoch=args.learned_epochs, batch=256, lr=2e-3)
+    t2 = time.perf_counter()
+    return net, {"pairs": net.num_samples() // blocksPerPair, "block_samples": net.num_samples(),
+                 "collect_steps": nStep, "collect_s": t1 - t0, "epochs": args.learned_epochs,
+                 "train_s": t2 - t1, "mse_first_epoch": first, "mse_last_epoch": last,
+                 "seed_data": 2025, "seed_timed": 2024}
 
 
 def cpu_baseline_jfnk(args, seconds=20.0):
@@ -321,7 +357,8 @@ def main():
     ap.add_argument("--no-e2e", dest="e2e", action="store_false")
     ap.add_argument("--no-cpu", dest="cpu", action="store_false")
     ap.add_argument("--precisions", default="fp64,fp32")
-    ap.add_argument("--jfnk-precond", default="BILU,NONE", help="'' to skip the implicit workload")
+    ap.add_argument("--jfnk-precond", default="BILU,NONE,LEARNED", help="'' to skip the implicit workload")
+    ap.add_argument("--learned-epochs", type=int, default=8)
     ap.add_argument("--jfnk-nroot", type=int, default=16, help="16 -> 128^3 cells")
     ap.add_argument("--jfnk-steps", type=int, default=5)
     ap.add_argument("--jfnk-warmup", type=int, default=2)

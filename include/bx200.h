@@ -212,7 +212,8 @@ BX_API int bx_impl_norm_noalloc(const double *Impl_dev, int nCellBlock, int nBlo
  * 3-layer 3x3x3 convolutional network per 8^3 block (16 -> 32 -> 32 -> 8
  * channels, ReLU, zero padding at the block faces) maps the block of a
  * Krylov vector (scaled by its block RMS s) and the block's normalised state
- * to the correction, z = s N(v / s, U / Norm_V); BF16 operands, FP32
+ * to a correction of the identity, z = v + s N(v / s, U / Norm_V), trained
+ * on the targets (z - w) / s of the pairs below; BF16 operands, FP32
  * accumulation on the tensor cores.  Training pairs (w = A z, z) are taken
  * from the BILU-preconditioned FGMRES iterations of implicit steps.  FGMRES
  * accepts any preconditioner, so the network changes iteration counts, not
