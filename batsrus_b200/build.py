@@ -24,13 +24,14 @@ UNITS = [
     ("bx_compat.cu", ["--fmad=false"]),
     ("bx_stage_fp32.cu", []),
     ("bx_stage3d.cu", []),
+    ("bx_amr.cu", []),
     ("bx_implicit.cu", ["--fmad=false"]),
     ("bx_learned.cu", []),
     ("bx_noalloc.cu", []),
     ("bx_capi.cu", []),
 ]
 HEADERS = ["bx_physics.cuh", "bx_stage.cuh", "bx_device.h", "bx_stage3d.cuh", "bx_tma.cuh", "bx_core.h",
-           "bx_impl_kernels.cuh", "bx_tc.cuh", "bx_learned.cuh", "bx_learned_kernels.cuh"]
+           "bx_impl_kernels.cuh", "bx_tc.cuh", "bx_learned.cuh", "bx_learned_kernels.cuh", "bx_amr.h"]
 
 
 def _sources_newer(target, deps):

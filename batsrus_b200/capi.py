@@ -23,12 +23,12 @@ PRECISION = {"fp64": 0, "fp32": 1, "fp32-bulk": 1}
 
 # every entry point declared in include/bx200.h
 EXPORTS = (
-    "bx_init", "bx_set_scheme", "bx_finalize", "bx_last_error", "bx_upload_state",
+    "bx_init", "bx_set_scheme", "bx_finalize", "bx_last_error", "bx_get_neighbors", "bx_upload_state",
     "bx_download_state", "bx_set_time", "bx_get_time", "bx_calc_face_value", "bx_calc_face_flux",
     "bx_calc_source", "bx_update_state", "bx_calc_timestep", "bx_get_face_values",
     "bx_get_face_flux", "bx_get_source", "bx_set_stage", "bx_update_state_fast",
     "bx_exchange_messages", "bx_set_global_timestep", "bx_advance_explicit", "bx_advance",
-    "bx_synchronize", "bx_timing_enable", "bx_timing_get", "bx_timing_reset",
+    "bx_set_graph_steps", "bx_synchronize", "bx_timing_enable", "bx_timing_get", "bx_timing_reset",
     "bx_region_begin", "bx_region_end",
     "bx_implicit_init", "bx_advance_part_impl", "bx_impl_get_rhs", "bx_impl_matvec",
     "bx_impl_precond", "bx_impl_get_x",
@@ -119,7 +119,7 @@ def load():
     sig = {
         "bx_init": [ctypes.POINTER(GridDesc), ctypes.POINTER(SchemeParams)],
         "bx_set_scheme": [ctypes.POINTER(SchemeParams)],
-        "bx_finalize": [],
+        "bx_finalize": [], "bx_get_neighbors": [ip, ip],
         "bx_upload_state": [dp, i], "bx_download_state": [dp, i],
         "bx_set_time": [d, i], "bx_get_time": [dp, dp, ip],
         "bx_calc_face_value": [i, i, i], "bx_calc_face_flux": [i, i],
@@ -127,7 +127,7 @@ def load():
         "bx_get_face_values": [i, dp, dp], "bx_get_face_flux": [i, dp], "bx_get_source": [dp],
         "bx_set_stage": [i], "bx_update_state_fast": [], "bx_exchange_messages": [i],
         "bx_set_global_timestep": [d, dp], "bx_advance_explicit": [i], "bx_advance": [i, d],
-        "bx_synchronize": [], "bx_timing_enable": [i], "bx_timing_get": [dp, ip, ip],
+        "bx_set_graph_steps": [i], "bx_synchronize": [], "bx_timing_enable": [i], "bx_timing_get": [dp, ip, ip],
         "bx_timing_reset": [], "bx_region_begin": [], "bx_region_end": [dp],
         "bx_implicit_init": [ctypes.POINTER(ImplicitParamsC)],
         "bx_advance_part_impl": [d, ctypes.POINTER(KrylovStats)],

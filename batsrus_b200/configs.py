@@ -17,6 +17,12 @@
   Gaussian random-phase perturbation (amplitude 1e-2, |k| <= 8), the
   explicit scheme of ``orszag_tang_3d`` for the high-order residual, and
   BDF2 with CflImpl 20, GMRES(30) to 1e-3 relative.
+* ``amr_blast`` -- the block-adaptive workload: [-0.5,0.5]^3 (periodic),
+  root blocks of 8^3 cells refined up to maxLevel where |grad p|/p > 0.5 on
+  the initial blast state (rho = 1, p = 10 inside r < 0.1 and 0.1 outside,
+  B = (1,1,0)/sqrt 2), levels balanced 2:1; HLLD flux, MC limiter (beta
+  1.5), CFL 0.8, 2-stage, Powell source, flux correction at resolution
+  changes.
 """
 import math
 
@@ -80,6 +86,37 @@ def jfnk_ot(nRoot=16, precond="BILU", seed=2024, with_state=True):
                        typePrecond=precond)
     st = initial.perturbed_ot(g, seed=seed, amplitude=1e-2, kmax=8) if with_state else None
     return g, s, p, st
+
+
+def _blast_refine(nRoot, pin=10.0, pout=0.1, r0=0.1, crit=0.5):
+    """refine(level, ix, iy, iz): |grad p|/p > crit somewhere in the block,
+    with the gradient by central differences of the initial pressure on the
+    block's own cells (one cell of the block's resolution across)."""
+    import numpy as np
+
+    def refine(lv, i, j, k):
+        n = nRoot << lv
+        bs = 1.0 / n
+        h = bs / 8
+        x = -0.5 + (np.array([i, j, k])[:, None] * bs) + (np.arange(-1, 9)[None, :] + 0.5) * h
+        X, Y, Z = np.meshgrid(x[0], x[1], x[2], indexing="ij")
+        p = np.where(X * X + Y * Y + Z * Z < r0 * r0, pin, pout)
+        gx = (p[2:, 1:-1, 1:-1] - p[:-2, 1:-1, 1:-1]) / (2 * h)
+        gy = (p[1:-1, 2:, 1:-1] - p[1:-1, :-2, 1:-1]) / (2 * h)
+        gz = (p[1:-1, 1:-1, 2:] - p[1:-1, 1:-1, :-2]) / (2 * h)
+        g = np.sqrt(gx * gx + gy * gy + gz * gz) / p[1:-1, 1:-1, 1:-1]
+        return bool((g > crit).any())
+
+    return refine
+
+
+def amr_blast(nRoot=8, maxLevel=3, precision="fp32", flux="HLLD", limiter="mc", beta=1.5, with_state=True):
+    g = BlockGrid.adaptive(3, (8, 8, 8), (nRoot,) * 3, (-0.5,) * 3, (0.5,) * 3, ("periodic",) * 6, maxLevel,
+                           _blast_refine(nRoot))
+    s = Scheme(nOrder=2, nStage=2, typeFlux=flux, typeLimiter=limiter, limiterBeta=beta, cfl=0.8,
+               gamma=5.0 / 3.0, useDivbSource=True, useHalfStep=True, precision=precision)
+    st = initial.blast(g) if with_state else None
+    return g, s, st, {"nStep": 50}
 
 
 CELLS_PER_STEP_BYTES = {"fp64": 320, "fp32": 256}

@@ -17,6 +17,7 @@
 #include <vector>
 
 #include "../../include/bx200.h"
+#include "bx_amr.h"
 #include "bx_core.h"
 #include "bx_device.h"
 
@@ -37,6 +38,14 @@ struct Ctx {
   std::vector<int> lev, ic;  // per block
   std::vector<int> nbrH, orderH;
   std::vector<BlockGeom> geomH;
+  // ModParallel DiLevel_EB / jBlock_IEB (0-based; -1 for none) and the
+  // resolution-change slabs
+  std::vector<int> dilH, jbH, rcTypeH, rcSlabH, lcH;
+  std::vector<RcSlab> slabsH;
+  int nSlab = 0;
+  int *rcType = nullptr, *rcSlab = nullptr, *lcDev = nullptr;
+  RcSlab *slabs = nullptr;
+  double *rcGhost = nullptr, *rcFlux = nullptr;
   // device
   double *A = nullptr;       // U^n (FP64)
   double *B = nullptr;       // stage buffer (FP64 or FP32 storage)
@@ -54,6 +63,7 @@ struct Ctx {
   cudaStream_t st = nullptr;
   cudaGraphExec_t graph = nullptr;
   double graphTLimit = 0;
+  int graphSteps = 1;  // time steps captured in one CUDA graph
   // TMA tensor maps of the two state buffers (3D shapes)
   bool use3d = false;
   int nSM = 148;
@@ -249,6 +259,17 @@ void free_all() {
     }
   if (g.nbr) cudaFree(g.nbr);
   if (g.order) cudaFree(g.order);
+  for (int **p : {&g.rcType, &g.rcSlab, &g.lcDev}) {
+    if (*p) cudaFree(*p);
+    *p = nullptr;
+  }
+  if (g.slabs) cudaFree(g.slabs);
+  g.slabs = nullptr;
+  for (double **p : {&g.rcGhost, &g.rcFlux}) {
+    if (*p) cudaFree(*p);
+    *p = nullptr;
+  }
+  g.nSlab = 0;
   if (g.geom) cudaFree(g.geom);
   if (g.ts) cudaFree(g.ts);
   g.nbr = g.order = nullptr; g.geom = nullptr; g.ts = nullptr;
@@ -287,6 +308,9 @@ StageArgs stage_args(int iStage, bool computeDt) {
   a.beta = g.sch.LimiterBeta; a.gamma = g.sch.Gamma; a.invGm1 = 1.0 / (g.sch.Gamma - 1.0);
   a.cfl = g.sch.Cfl;
   a.old = g.A;
+  if (g.nSlab) {
+    a.rcType = g.rcType; a.rcSlab = g.rcSlab; a.rcGhost = g.rcGhost; a.rcFlux = g.rcFlux;
+  }
   if (g.sch.nStage == 1) { a.in = g.A; a.out = g.B; }
   else if (iStage == 1) { a.in = g.A; a.out = g.B; }
   else { a.in = g.B; a.out = g.A; }
@@ -318,6 +342,11 @@ int launch_stage(int iStage) {
     } else {
       kind = kKindFp32In32;
       m = &g.mapY32;
+    }
+    if (g.nSlab) {
+      e = launch_reschange(g.shape, g.sch.TypeFlux, kind, a, g.slabs, g.nSlab, g.lcDev,
+                           make_int3(g.nRoot[0], g.nRoot[1], g.nRoot[2]), g.rcGhost, g.rcFlux, g.st);
+      if (e != cudaSuccess) return fail(BX_ERR_CUDA, "resolution-change kernels: %s", cudaGetErrorString(e));
     }
     e = launch_stage3d(g.shape, g.sch.TypeFlux, kind, *m, a, g.nSM, g.st);
   } else if (g.sch.Precision == BX_FP64) {
@@ -379,6 +408,7 @@ CompatArgs compat_args() {
 
 int compat_phase(int phase, int iBlock) {
   NEED_READY();
+  if (g.nSlab) return fail(BX_ERR_ARG, "the per-block entry points work on single-level grids");
   if (iBlock < 1 || iBlock > g.nBlock) return fail(BX_ERR_ARG, "iBlock=%d out of range 1..%d", iBlock, g.nBlock);
   int r = ensure_compat();
   if (r) return r;
@@ -409,7 +439,7 @@ Core core() {
   c.ready = g.ready;
   c.dev = g.dev; c.nDim = g.nDim; c.nI = g.nI; c.nJ = g.nJ; c.nK = g.nK; c.shape = g.shape;
   c.nBlock = g.nBlock; c.nSM = g.nSM; c.nCell = g.nCell; c.sch = g.sch;
-  c.A = g.A; c.nbr = g.nbr; c.order = g.order; c.geom = g.geom; c.ts = g.ts; c.dtBlock = g.dtBlock;
+  c.A = g.A; c.nbr = g.nbr; c.order = g.order; c.geom = g.geom; c.ts = g.ts; c.dtBlock = g.dtBlock; c.nSlab = g.nSlab;
   c.st = g.st;
   return c;
 }
@@ -429,6 +459,14 @@ int core_encode_maps(void *base, bool fp32, TmaMaps &m) { return encode_maps(bas
 extern "C" {
 
 const char *bx_last_error(void) { return g.err.c_str(); }
+
+int bx_get_neighbors(int *DiLevel_EB, int *jBlock_IEB) {
+  NEED_READY();
+  if (!DiLevel_EB || !jBlock_IEB) return fail(BX_ERR_ARG, "null argument");
+  for (int i = 0; i < 6 * g.nBlock; i++) DiLevel_EB[i] = g.dilH[i];
+  for (int i = 0; i < 24 * g.nBlock; i++) jBlock_IEB[i] = g.jbH[i] + 1;  // 1-based, 0 = none
+  return BX_OK;
+}
 
 int bx_init(const bx_grid_desc *gd, const bx_scheme_params *sp) {
   if (!gd || !sp) return fail(BX_ERR_ARG, "null argument");
@@ -458,25 +496,69 @@ int bx_init(const bx_grid_desc *gd, const bx_scheme_params *sp) {
     if (node.count(key)) return fail(BX_ERR_ARG, "block %d duplicates block %d", b + 1, node[key] + 1);
     node[key] = b;
   }
-  g.nbrH.assign(6 * g.nBlock, -1);
+  // neighbours (BATL find_neighbor): the block at the same level across the
+  // side, else its parent (coarser), else the 2^(nDim-1) children of that
+  // position touching the side (finer, first transverse direction fastest)
+  auto findb = [&](int L, int x, int y, int z) {
+    auto it = node.find(std::make_tuple(L, x, y, z));
+    return it == node.end() ? -1 : it->second;
+  };
+  g.nbrH.assign(6 * g.nBlock, kNbrFloat);
+  g.dilH.assign(6 * g.nBlock, kDiLevelUnset);
+  g.jbH.assign(24 * g.nBlock, -1);
+  g.rcTypeH.assign(6 * g.nBlock, 0);
+  g.rcSlabH.assign(6 * g.nBlock, -1);
+  g.slabsH.clear();
   for (int b = 0; b < g.nBlock; b++) {
     for (int d = 0; d < g.nDim; d++) {
       const int nbl = g.nRoot[d] << g.lev[b];
       for (int side = 0; side < 2; side++) {
+        const int sd = 2 * d + side;
         int c[3] = {g.ic[3 * b], g.ic[3 * b + 1], g.ic[3 * b + 2]};
         c[d] += side ? 1 : -1;
         if (c[d] < 0 || c[d] >= nbl) {
-          if (g.typeBc[2 * d + side] == BX_BC_PERIODIC) c[d] = (c[d] + nbl) % nbl;
-          else { g.nbrH[6 * b + 2 * d + side] = -1; continue; }
+          if (g.typeBc[sd] == BX_BC_PERIODIC) c[d] = (c[d] + nbl) % nbl;
+          else continue;  // float boundary
         }
-        auto it = node.find(std::make_tuple(g.lev[b], c[0], c[1], c[2]));
-        if (it == node.end())
-          return fail(BX_ERR_ARG, "block %d has no same-level neighbour on side %d: refined grids need the AMR path",
-                      b + 1, 2 * d + side);
-        g.nbrH[6 * b + 2 * d + side] = it->second;
+        int q = findb(g.lev[b], c[0], c[1], c[2]);
+        if (q >= 0) {
+          g.nbrH[6 * b + sd] = q; g.dilH[6 * b + sd] = 0; g.jbH[24 * b + 4 * sd] = q;
+          continue;
+        }
+        RcSlab S;
+        S.block = b; S.side = sd;
+        for (int m = 0; m < 4; m++) S.nb[m] = -1;
+        if (g.lev[b] > 0 && (q = findb(g.lev[b] - 1, c[0] >> 1, c[1] >> 1, c[2] >> 1)) >= 0) {
+          S.type = 1; S.nb[0] = q;
+        } else {
+          S.type = -1;
+          int t[2], nt = 0;
+          for (int e = 0; e < g.nDim; e++) if (e != d) t[nt++] = e;
+          int m = 0;
+          for (int q1 = 0; q1 < (nt > 1 ? 2 : 1); q1++)
+            for (int q0 = 0; q0 < (nt > 0 ? 2 : 1); q0++) {
+              int f[3] = {2 * c[0], g.nDim > 1 ? 2 * c[1] : 0, g.nDim > 2 ? 2 * c[2] : 0};
+              f[d] += side ? 0 : 1;
+              if (nt > 0) f[t[0]] += q0;
+              if (nt > 1) f[t[1]] += q1;
+              S.nb[m] = findb(g.lev[b] + 1, f[0], f[1], f[2]);
+              if (S.nb[m] < 0)
+                return fail(BX_ERR_ARG, "block %d side %d: neighbours differ by more than one level", b + 1, sd);
+              m++;
+            }
+        }
+        g.nbrH[6 * b + sd] = kNbrResChange;
+        g.dilH[6 * b + sd] = S.type;
+        for (int m = 0; m < 4; m++) g.jbH[24 * b + 4 * sd + m] = S.nb[m];
+        g.rcTypeH[6 * b + sd] = S.type;
+        g.rcSlabH[6 * b + sd] = (int)g.slabsH.size();
+        g.slabsH.push_back(S);
       }
     }
   }
+  g.nSlab = (int)g.slabsH.size();
+  if (g.nSlab && g.shape != kShape888 && g.shape != kShape444)
+    return fail(BX_ERR_ARG, "resolution changes need 3D 8x8x8 or 4x4x4 blocks");
   // Morton processing order (L2 reuse of the neighbours' interiors)
   g.orderH.resize(g.nBlock);
   for (int b = 0; b < g.nBlock; b++) g.orderH[b] = b;
@@ -533,6 +615,25 @@ int bx_init(const bx_grid_desc *gd, const bx_scheme_params *sp) {
   CK(cudaMemcpyAsync(g.order, g.orderH.data(), sizeof(int) * g.nBlock, cudaMemcpyHostToDevice, g.st));
   CK(cudaMemcpyAsync(g.geom, g.geomH.data(), sizeof(BlockGeom) * g.nBlock, cudaMemcpyHostToDevice, g.st));
   CK(cudaMemsetAsync(g.dtBlock, 0, sizeof(double) * g.nBlock, g.st));
+  if (g.nSlab) {
+    g.lcH.assign(gd->iLevelCoord_IB, gd->iLevelCoord_IB + 4 * g.nBlock);
+    const size_t nFace = (size_t)g.nI * g.nI;
+    if (cudaMalloc(&g.rcType, sizeof(int) * 6 * g.nBlock) != cudaSuccess ||
+        cudaMalloc(&g.rcSlab, sizeof(int) * 6 * g.nBlock) != cudaSuccess ||
+        cudaMalloc(&g.lcDev, sizeof(int) * 4 * g.nBlock) != cudaSuccess ||
+        cudaMalloc(&g.slabs, sizeof(RcSlab) * g.nSlab) != cudaSuccess ||
+        cudaMalloc(&g.rcGhost, sizeof(double) * 16 * nFace * g.nSlab) != cudaSuccess ||
+        cudaMalloc(&g.rcFlux, sizeof(double) * kRcSlots * nFace * g.nSlab) != cudaSuccess) {
+      free_all();
+      return fail(BX_ERR_NOMEM, "resolution-change buffers (%d slabs)", g.nSlab);
+    }
+    CK(cudaMemcpyAsync(g.rcType, g.rcTypeH.data(), sizeof(int) * 6 * g.nBlock, cudaMemcpyHostToDevice, g.st));
+    CK(cudaMemcpyAsync(g.rcSlab, g.rcSlabH.data(), sizeof(int) * 6 * g.nBlock, cudaMemcpyHostToDevice, g.st));
+    CK(cudaMemcpyAsync(g.lcDev, g.lcH.data(), sizeof(int) * 4 * g.nBlock, cudaMemcpyHostToDevice, g.st));
+    CK(cudaMemcpyAsync(g.slabs, g.slabsH.data(), sizeof(RcSlab) * g.nSlab, cudaMemcpyHostToDevice, g.st));
+    CK(cudaMemsetAsync(g.rcGhost, 0, sizeof(double) * 16 * nFace * g.nSlab, g.st));
+    CK(cudaMemsetAsync(g.rcFlux, 0, sizeof(double) * kRcSlots * nFace * g.nSlab, g.st));
+  }
   StepState s0;
   std::memset(&s0, 0, sizeof(s0));
   s0.DtMinBits = 0x7FF0000000000000ull;
@@ -754,8 +855,11 @@ int bx_advance(int nStep, double tLimit) {
     if (g.graph) { cudaGraphExecDestroy(g.graph); g.graph = nullptr; }
     cudaGraph_t gr;
     CK(cudaStreamBeginCapture(g.st, cudaStreamCaptureModeThreadLocal));
-    int r = launch_step(tLimit);
-    g.nLaunchTotal -= g.sch.nStage;  // captured, not launched
+    int r = 0;
+    for (int q = 0; q < g.graphSteps && !r; q++) {
+      r = launch_step(tLimit);
+      g.nLaunchTotal -= g.sch.nStage;  // captured, not launched
+    }
     cudaError_t e = cudaStreamEndCapture(g.st, &gr);
     if (r) return r;
     if (e != cudaSuccess) return fail(BX_ERR_CUDA, "graph capture: %s", cudaGetErrorString(e));
@@ -763,16 +867,26 @@ int bx_advance(int nStep, double tLimit) {
     cudaGraphDestroy(gr);
     g.graphTLimit = tLimit;
   }
-  for (int n = 0; n < nStep; n++) {
-    if (useGraph) {
+  for (int n = 0; n < nStep;) {
+    if (useGraph && nStep - n >= g.graphSteps) {
       CK(cudaGraphLaunch(g.graph, g.st));
-      g.nLaunchTotal += g.sch.nStage;
+      g.nLaunchTotal += g.sch.nStage * g.graphSteps;
+      n += g.graphSteps;
     } else {
       int r = launch_step(tLimit);
       if (r) return r;
+      n++;
     }
   }
   return check_err_flag();
+}
+
+int bx_set_graph_steps(int nStepPerGraph) {
+  NEED_READY();
+  if (nStepPerGraph < 1 || nStepPerGraph > 1000) return fail(BX_ERR_ARG, "nStepPerGraph=%d", nStepPerGraph);
+  if (nStepPerGraph != g.graphSteps && g.graph) { cudaGraphExecDestroy(g.graph); g.graph = nullptr; }
+  g.graphSteps = nStepPerGraph;
+  return BX_OK;
 }
 
 int bx_synchronize(void) {

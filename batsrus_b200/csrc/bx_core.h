@@ -19,6 +19,7 @@ struct Core {
   StepState *ts;
   double *dtBlock;
   cudaStream_t st;
+  int nSlab;  // resolution-change sides (0 on a single-level grid)
 };
 
 Core core();

@@ -49,7 +49,19 @@ struct StageArgs {
   const double *dtCellIn = nullptr;
   double *dtCellOut = nullptr;  // V/sum(Vdt) per cell when computeDt
   double dtScale = 0.5;
+  // resolution changes (nbr == kNbrResChange): per block and side the level
+  // difference (+1 coarser, -1 finer neighbour, else 0) and the slab holding
+  // its two ghost layers ([slab][var][layer][t1][t0], FP64) and, on the
+  // coarse side, the summed finer fluxes ([slab][t1][t0][10]: 8 fluxes, Vdt,
+  // BnL + BnR)
+  const int *rcType = nullptr;
+  const int *rcSlab = nullptr;
+  const double *rcGhost = nullptr;
+  const double *rcFlux = nullptr;
 };
+
+constexpr int kNbrFloat = -1, kNbrResChange = -2;
+constexpr int kRcSlots = 10;
 
 // per-block compatibility kernels (orig-path entry points, FP64)
 struct CompatArgs {

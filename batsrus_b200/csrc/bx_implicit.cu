@@ -198,8 +198,8 @@ int gmres(int &iError) {
     for (int k = 0; k < m; k++) {
       double *Vk = I.V + (size_t)k * N, *Zk = I.Z + (size_t)k * N;
       if ((r = precond(Vk, Zk))) return r;
+      if (learned_collecting() && c.nI == 8 && (r = learned_collect(Vk, Zk, c.nBlock, c.st))) return r;
       if ((r = matvec(Zk, I.W))) return r;
-      if (learned_collecting() && c.nI == 8 && (r = learned_collect(I.W, Zk, c.nBlock, c.st))) return r;
       for (int q = 0; q <= k + 1; q++) {
         const double *vq = q > 0 ? I.V + (size_t)(q - 1) * N : nullptr;
         const double *hq = q > 0 ? hdev + q - 1 : nullptr;
@@ -340,6 +340,7 @@ int bx_implicit_init(const bx_implicit_params *prm) {
   if (c.shape != kShape888 && c.shape != kShape444)
     return core_fail(BX_ERR_ARG, "the implicit scheme needs 3D 8x8x8 or 4x4x4 blocks");
   if (c.sch.Precision != BX_FP64) return core_fail(BX_ERR_ARG, "the implicit scheme runs in FP64 mode");
+  if (c.nSlab) return core_fail(BX_ERR_ARG, "the implicit scheme works on single-level grids");
   if (prm->nKrylovVector < 1 || prm->nKrylovVector > 32)
     return core_fail(BX_ERR_ARG, "nKrylovVector=%d outside 1..32", prm->nKrylovVector);
   if (prm->TypePrecond < 0 || prm->TypePrecond > 2) return core_fail(BX_ERR_ARG, "TypePrecond=%d", prm->TypePrecond);

@@ -131,9 +131,10 @@ __global__ void k_features(const double *__restrict__ U, const double *__restric
   }
 }
 
-// store the picked blocks of the pair (w = A z, z) as training samples
-// base + i: input w / s and the features, target (z - w) / s (s = RMS of w;
-// the network is the correction to the identity)
+// store the picked blocks of the pair (v, z = P(v)) of a Krylov vector and
+// its preconditioned correction as training samples base + i: input v / s
+// and the features, target z / s (s = RMS of v over the block); a block
+// whose scale is not finite is stored as zeros
 __global__ void k_collect(const double *__restrict__ w, const double *__restrict__ z,
                           const __nv_bfloat16 *__restrict__ feat, const int *__restrict__ pick, long base,
                           __nv_bfloat16 *in16, float *tgt) {
@@ -148,7 +149,7 @@ __global__ void k_collect(const double *__restrict__ w, const double *__restrict
   double tot = 0;
   for (int i = 0; i < (int)(blockDim.x >> 5); i++) tot += red[i];
   const double s = sqrt(tot / 4096.0);
-  const double inv = s > 1e-300 ? 1.0 / s : 0.0;
+  const double inv = (s > 1e-300 && s < 1e300) ? 1.0 / s : 0.0;
   const size_t n = base + blockIdx.x;
   for (int c = threadIdx.x; c < 512; c += blockDim.x) {
     uint4 q[2];
@@ -161,7 +162,10 @@ __global__ void k_collect(const double *__restrict__ w, const double *__restrict
     dst[0] = q[0];
     dst[1] = q[1];
 #pragma unroll
-    for (int m = 0; m < 8; m++) tgt[(n * 512 + c) * 8 + m] = (float)((zb[m * 512 + c] - wb[m * 512 + c]) * inv);
+    for (int m = 0; m < 8; m++) {
+      const double q = zb[m * 512 + c] * inv;
+      tgt[(n * 512 + c) * 8 + m] = isfinite(q) ? (float)q : 0.f;
+    }
   }
 }
 

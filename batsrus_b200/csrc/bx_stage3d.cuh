@@ -97,7 +97,7 @@ __device__ __forceinline__ void tile_cell(int c, const int *nb, int &i, int &j, 
     k = side == 4 ? l - 2 : N + l;
   }
   si = i; sj = j; sk = k;
-  if (nb[side] < 0) {  // float boundary: copy of the boundary cell
+  if (nb[side] == kNbrFloat) {  // float boundary: copy of the boundary cell
     if (side == 0) si = 0;
     if (side == 1) si = N - 1;
     if (side == 2) sj = 0;
@@ -145,14 +145,38 @@ __device__ __forceinline__ int face_id(int i, int j, int k) {
   return i + N * (j + N * k);
 }
 
-// one direction: faces (one per thread) then the cell sums
+// the ten face slots of one face from its left and right primitive states:
+// fluxes times area (0..7), Vdt (8), BnL + BnR (9); false where hlld_flux
+// stops
+template <int D, int FLUX, typename Real>
+__device__ __forceinline__ bool face_slots(Real (&L)[8], Real (&R)[8], Real gamma, Real invGm1, Real area,
+                                           Real *out, int stride) {
+  out[9 * stride] = L[kBx + D] + R[kBx + D];
+  if (FLUX == kFluxHlld) {
+    Real F[8], v;
+    const bool ok = numerical_flux<D, FLUX>(L, R, gamma, invGm1, area, F, v);
+#pragma unroll
+    for (int q = 0; q < 8; q++) out[q * stride] = F[q];
+    out[8 * stride] = v;
+    return ok;
+  }
+  out[8 * stride] = flux_lean<D, FLUX>(L, R, gamma, invGm1, area, out, stride);
+  return true;
+}
+
+// one direction: faces (one per thread) then the cell sums.  rcFine / rcCoarse:
+// bit s set where side s borders a coarser / finer block
 template <class T, int D, int FLUX, typename TileT, typename Real>
 __device__ __forceinline__ void sweep3(const StageArgs &a, const BlockGeom &g, const TileT *tile, Real *fbuf,
-                                       double (&chg)[8], double &divB, double &vdt, int &err) {
+                                       double (&chg)[8], double &divB, double &vdt, int &err, int rcFine,
+                                       int rcCoarse, int b) {
   const int t = threadIdx.x;
   if (t < T::NF) {
     int i, j, k;
     face_ijk<T, D>(t, i, j, k);
+    const int fn = D == 0 ? i : (D == 1 ? j : k);  // face index along D
+    const int side = fn == 0 ? 2 * D : (fn == T::N ? 2 * D + 1 : -1);
+    const bool first = a.nOrder == 1 || (side >= 0 && ((rcFine >> side) & 1));
     int idx[4];
 #pragma unroll
     for (int m = 0; m < 4; m++)
@@ -168,19 +192,16 @@ __device__ __forceinline__ void sweep3(const StageArgs &a, const BlockGeom &g, c
     for (int v = 0; v < 8; v++) {
       const Real q0 = (Real)tile[idx[0] + v * vs[0]], q1 = (Real)tile[idx[1] + v * vs[1]];
       const Real q2 = (Real)tile[idx[2] + v * vs[2]], q3 = (Real)tile[idx[3] + v * vs[3]];
-      if (a.nOrder == 1) { L[v] = q1; R[v] = q2; }
+      if (first) { L[v] = q1; R[v] = q2; }
       else limited_face(a.limiter, beta, q0, q1, q2, q3, L[v], R[v]);
     }
-    fbuf[9 * T::NF + t] = L[kBx + D] + R[kBx + D];
-    const Real area = (Real)g.area[D];
-    if (FLUX == kFluxHlld) {
-      Real F[8], v;
-      if (!numerical_flux<D, FLUX>(L, R, (Real)a.gamma, (Real)a.invGm1, area, F, v)) err = 1;
+    if (!face_slots<D, FLUX, Real>(L, R, (Real)a.gamma, (Real)a.invGm1, (Real)g.area[D], fbuf + t, T::NF)) err = 1;
+    if (side >= 0 && ((rcCoarse >> side) & 1)) {
+      // apply_cons_flux: the summed fluxes of the finer faces
+      const int t0 = D == 0 ? j : i, t1 = D == 2 ? j : k;
+      const double *cf = a.rcFlux + ((size_t)a.rcSlab[6 * b + side] * T::N * T::N + t0 + T::N * t1) * kRcSlots;
 #pragma unroll
-      for (int q = 0; q < 8; q++) fbuf[q * T::NF + t] = F[q];
-      fbuf[8 * T::NF + t] = v;
-    } else {
-      fbuf[8 * T::NF + t] = flux_lean<D, FLUX>(L, R, (Real)a.gamma, (Real)a.invGm1, area, fbuf + t, T::NF);
+      for (int q = 0; q < kRcSlots; q++) fbuf[q * T::NF + t] = (Real)cf[q];
     }
   }
   __syncthreads();
@@ -247,6 +268,33 @@ __global__ void __launch_bounds__(T::NTHR, 1)
 #pragma unroll
     for (int s = 0; s < 6; s++) nb[s] = a.nbr[6 * b + s];
     const BlockGeom g = a.geom[b];
+    int rcFine = 0, rcCoarse = 0;
+#pragma unroll
+    for (int s = 0; s < 6; s++)
+      if (nb[s] == kNbrResChange) {
+        const int rt = a.rcType[6 * b + s];
+        if (rt == 1) rcFine |= 1 << s;
+        if (rt == -1) rcCoarse |= 1 << s;
+      }
+    if (rcFine | rcCoarse) {
+      // ghost layers of the resolution-change sides from their slabs
+      constexpr int N = T::N, nSlab = 8 * 2 * N * N;
+#pragma unroll 1
+      for (int s = 0; s < 6; s++) {
+        if (nb[s] != kNbrResChange) continue;
+        const double *src = a.rcGhost + (size_t)a.rcSlab[6 * b + s] * nSlab;
+        const int d = s >> 1, hi = s & 1;
+        for (int q = t; q < nSlab; q += T::NTHR) {
+          const int t0 = q % N, t1 = (q / N) % N, l = (q / (N * N)) % 2, v = q / (2 * N * N);
+          int c3[3];
+          c3[d] = hi ? N + l : -1 - l;
+          c3[d == 0 ? 1 : 0] = t0;
+          c3[d == 2 ? 1 : 2] = t1;
+          tile[tile_index<T, TileT>(v, c3[0], c3[1], c3[2])] = (TileT)src[q];
+        }
+      }
+      __syncthreads();
+    }
 
     // calc_primitives, in two passes (read all, then write) because float
     // boundary ghosts read interior cells that are converted in place
@@ -292,9 +340,9 @@ __global__ void __launch_bounds__(T::NTHR, 1)
     }
 
     double chg[8], divB = 0, vdt = 0;
-    sweep3<T, 0, FLUX, TileT, Real>(a, g, tile, fbuf, chg, divB, vdt, err);
-    sweep3<T, 1, FLUX, TileT, Real>(a, g, tile, fbuf, chg, divB, vdt, err);
-    sweep3<T, 2, FLUX, TileT, Real>(a, g, tile, fbuf, chg, divB, vdt, err);
+    sweep3<T, 0, FLUX, TileT, Real>(a, g, tile, fbuf, chg, divB, vdt, err, rcFine, rcCoarse, b);
+    sweep3<T, 1, FLUX, TileT, Real>(a, g, tile, fbuf, chg, divB, vdt, err, rcFine, rcCoarse, b);
+    sweep3<T, 2, FLUX, TileT, Real>(a, g, tile, fbuf, chg, divB, vdt, err, rcFine, rcCoarse, b);
 
     // update_state_normal / update_explicit for the thread's cell
     double dtmin = 1e300;

@@ -126,6 +126,10 @@ class ExplicitSolver:
     def advance(self, nStep=1, TimeSimulationLimit=-1.0):
         check(self.L.bx_advance(nStep, TimeSimulationLimit))
 
+    def set_graph_steps(self, n):
+        """time steps captured in one CUDA graph by advance()"""
+        check(self.L.bx_set_graph_steps(int(n)))
+
     def synchronize(self):
         check(self.L.bx_synchronize())
 

@@ -128,3 +128,122 @@ class BlockGrid:
         if not with_ghost:
             xyz = xyz[self.interior_slices()[:4]]
         return xyz
+
+    # -- static block-adaptive grids -------------------------------------------
+    @classmethod
+    def adaptive(cls, nDim, nCellBlock, nRoot, xyzMin, xyzMax, typeBc, maxLevel, refine):
+        """A static refined grid: starting from the root blocks, every block
+        of level L < maxLevel for which ``refine(level, ix, iy, iz)`` is true
+        is split into 2^nDim children; then blocks are split until
+        neighbouring blocks (across faces, edges and corners) differ by at
+        most one level, as BATL keeps its tree.  Blocks are numbered along
+        the Morton curve of the finest level (the order of BATL's
+        space-filling curve over the tree)."""
+        nb0 = [nRoot[d] if d < nDim else 1 for d in range(3)]
+        leaves = {(0, i, j, k) for k in range(nb0[2]) for j in range(nb0[1]) for i in range(nb0[0])}
+        per = [typeBc[2 * d] == "periodic" for d in range(3)]
+        kids = [(a, b, c) for c in range(2 if nDim > 2 else 1) for b in range(2 if nDim > 1 else 1) for a in range(2)]
+
+        def split(key):
+            leaves.discard(key)
+            lv, i, j, k = key
+            for a, b, c in kids:
+                leaves.add((lv + 1, 2 * i + a, 2 * j + b, 2 * k + c))
+
+        def leaf_at(lv, c):
+            """leaf covering the level-lv block index c (wrapped), or None"""
+            n = [nb0[d] << lv if d < nDim else 1 for d in range(3)]
+            c = list(c)
+            for d in range(3):
+                if c[d] < 0 or c[d] >= n[d]:
+                    if d >= nDim or not per[d]:
+                        return None
+                    c[d] %= n[d]
+            for l2 in range(lv, -1, -1):
+                s = lv - l2
+                key = (l2, c[0] >> s, c[1] >> s, c[2] >> s) if nDim == 3 else \
+                    (l2, c[0] >> s, (c[1] >> s) if nDim > 1 else 0, 0)
+                if key in leaves:
+                    return key
+            return None
+
+        offs = [(a, b, c) for c in ((-1, 0, 1) if nDim > 2 else (0,)) for b in ((-1, 0, 1) if nDim > 1 else (0,))
+                for a in (-1, 0, 1) if (a, b, c) != (0, 0, 0)]
+        for lv in range(maxLevel):
+            for key in sorted(k for k in leaves if k[0] == lv):
+                if refine(*key):
+                    split(key)
+            changed = True
+            while changed:
+                changed = False
+                for key in sorted(leaves):
+                    if key not in leaves:
+                        continue
+                    l0, i, j, k = key
+                    for a, b, c in offs:
+                        nk = leaf_at(l0, (i + a, j + b, k + c))
+                        if nk is not None and nk[0] < l0 - 1:
+                            split(nk)
+                            changed = True
+        mx = max(k[0] for k in leaves)
+
+        def order_key(key):
+            s = mx - key[0]
+            return (morton_key(key[1] << s, key[2] << s, key[3] << s), key[0])
+
+        coords = sorted(leaves, key=order_key)
+        return cls(nDim, nCellBlock[0], nCellBlock[1], nCellBlock[2], tuple(nRoot), tuple(map(float, xyzMin)),
+                   tuple(map(float, xyzMax)), tuple(typeBc), np.array(coords, dtype=np.int32))
+
+    def neighbors(self):
+        """DiLevel_EB and jBlock_IEB of ModParallel (0-based block indices):
+        for each block and side (x-, x+, y-, y+, z-, z+) the level
+        difference to the neighbour (0 same level, +1 coarser, -1 finer,
+        -100 (BATL Unset_) at a float boundary or an ignored dimension) and the
+        neighbour blocks: one for 0 and +1; for -1 the 2^(nDim-1) finer
+        blocks touching the face, ordered by their two transverse indices
+        (first transverse direction fastest)."""
+        index = {tuple(int(v) for v in c): b for b, c in enumerate(self.iLevelCoord)}
+        nb0 = [self.nRoot[d] if d < self.nDim else 1 for d in range(3)]
+        per = [self.typeBc[2 * d] == "periodic" for d in range(3)]
+        dil = np.zeros((self.nBlock, 6), dtype=np.int32)
+        jb = -np.ones((self.nBlock, 6, 4), dtype=np.int32)
+        for b, (lv, i, j, k) in enumerate(self.iLevelCoord.tolist()):
+            for d in range(3):
+                for side in range(2):
+                    s = 2 * d + side
+                    if d >= self.nDim:
+                        dil[b, s] = -100
+                        continue
+                    c = [i, j, k]
+                    c[d] += 1 if side else -1
+                    n = nb0[d] << lv
+                    if c[d] < 0 or c[d] >= n:
+                        if not per[d]:
+                            dil[b, s] = -100
+                            continue
+                        c[d] %= n
+                    if (lv, *c) in index:
+                        dil[b, s] = 0
+                        jb[b, s, 0] = index[(lv, *c)]
+                    elif lv > 0 and (lv - 1, c[0] >> 1, c[1] >> 1, c[2] >> 1) in index:
+                        dil[b, s] = 1
+                        jb[b, s, 0] = index[(lv - 1, c[0] >> 1, c[1] >> 1, c[2] >> 1)]
+                    else:
+                        dil[b, s] = -1
+                        t = [e for e in range(3) if e != d and e < self.nDim]
+                        m = 0
+                        for q1 in range(2 if len(t) > 1 else 1):
+                            for q0 in range(2 if len(t) > 0 else 1):
+                                f = [2 * c[0], 2 * c[1] if self.nDim > 1 else 0, 2 * c[2] if self.nDim > 2 else 0]
+                                f[d] += 0 if side else 1  # the child layer touching the face
+                                if len(t) > 0:
+                                    f[t[0]] += q0
+                                if len(t) > 1:
+                                    f[t[1]] += q1
+                                key = (lv + 1, *f)
+                                if key not in index:
+                                    raise ValueError("block %d side %d: unbalanced tree" % (b, s))
+                                jb[b, s, m] = index[key]
+                                m += 1
+        return dil, jb

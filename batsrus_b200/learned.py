@@ -1,7 +1,7 @@
 """Host-side interface of the learned per-block preconditioner
 (include/bx200.h, bx_learned_*): a new #PRECONDITIONER value LEARNED for the
-implicit step's FGMRES, trained on (w = A z, z) pairs that the
-BILU-preconditioned solver generates."""
+implicit step's FGMRES, trained on (Krylov vector, BILU correction) pairs
+that the BILU-preconditioned solver generates."""
 import ctypes
 
 import numpy as np

@@ -238,8 +238,9 @@ def run_jfnk(args, lrank):
 
 
 def train_learned(args, g, s, lrank, nPair=2000, blocksPerPair=16):
-    """Training data and training of the learned preconditioner: (w = A z, z)
-    pairs from the BILU-preconditioned FGMRES of implicit steps started from
+    """Training data and training of the learned preconditioner: (v, BILU(v))
+    pairs of Krylov vectors from the BILU-preconditioned FGMRES of implicit
+    steps started from
     a differently seeded perturbation (seed 2025) than the timed steps,
     blocksPerPair random blocks of each of nPair pairs; then Adam."""
     from batsrus_b200 import configs
@@ -254,8 +255,12 @@ def train_learned(args, g, s, lrank, nPair=2000, blocksPerPair=16):
     t0 = time.perf_counter()
     net.collect(blocksPerPair)
     nStep = 0
+    from batsrus_b200.capi import BxError
     while net.num_samples() < nPair * blocksPerPair and nStep < 200:
-        im.advance_part_impl()
+        try:
+            im.advance_part_impl()
+        except BxError:  # a failed solve ends the collection
+            break
         nStep += 1
     net.collect(0)
     x.close()
@@ -266,6 +271,37 @@ def train_learned(args, g, s, lrank, nPair=2000, blocksPerPair=16):
                  "collect_steps": nStep, "collect_s": t1 - t0, "epochs": args.learned_epochs,
                  "train_s": t2 - t1, "mse_first_epoch": first, "mse_last_epoch": last,
                  "seed_data": 2025, "seed_timed": 2024}
+
+
+def run_amr(args, lrank):
+    """The block-adaptive blast workload: all levels in one persistent stage
+    kernel per stage, resolution-change ghost cells and flux correction,
+    args.amr_steps time steps captured in one CUDA graph; FP32-bulk (the
+    configuration's precision) and FP64, cell-updates/s (cells of all levels
+    x steps / device time of the graph launch)."""
+    from batsrus_b200 import configs
+    from batsrus_b200.explicit import ExplicitSolver
+    out = {}
+    st = None
+    for prec in ("fp32", "fp64"):
+        g, s, st0, _ = configs.amr_blast(nRoot=args.amr_nroot, maxLevel=3, precision=prec, with_state=st is None)
+        st = st0 if st is None else st
+        x = ExplicitSolver(g, s, device=lrank)
+        x.set_state(st)
+        x.advance(1)  # Dt = 0 step
+        x.set_graph_steps(args.amr_steps)
+        x.advance(1 + args.amr_steps)  # one uncaptured step, capture, one graph launch
+        x.synchronize()
+        x.region_begin()
+        x.advance(args.amr_steps)  # one graph launch
+        ms = x.region_end()
+        lev = np.bincount(g.iLevelCoord[:, 0])
+        out[prec] = {"value": g.nCell * args.amr_steps / (ms * 1e-3), "ms_per_step": ms / args.amr_steps}
+        x.close()
+    out.update({"workload": "amr_blast_levels0-3_nroot%d_hlld_mc" % args.amr_nroot, "unit": UNIT,
+                "blocks": int(g.nBlock), "cells": int(g.nCell), "blocks_per_level": [int(v) for v in lev],
+                "steps_per_graph": args.amr_steps, "value_is": "fp32 bulk (FP64 accumulation)"})
+    return out
 
 
 def cpu_baseline_jfnk(args, seconds=20.0):
@@ -359,6 +395,10 @@ def main():
     ap.add_argument("--precisions", default="fp64,fp32")
     ap.add_argument("--jfnk-precond", default="BILU,NONE,LEARNED", help="'' to skip the implicit workload")
     ap.add_argument("--learned-epochs", type=int, default=8)
+    ap.add_argument("--amr", dest="amr", action="store_true", default=True)
+    ap.add_argument("--no-amr", dest="amr", action="store_false")
+    ap.add_argument("--amr-nroot", type=int, default=16, help="root blocks per dimension of the blast grid")
+    ap.add_argument("--amr-steps", type=int, default=50)
     ap.add_argument("--jfnk-nroot", type=int, default=16, help="16 -> 128^3 cells")
     ap.add_argument("--jfnk-steps", type=int, default=5)
     ap.add_argument("--jfnk-warmup", type=int, default=2)
@@ -386,6 +426,8 @@ def main():
         line["e2e"] = r64["e2e"]
     if args.jfnk_precond:
         line["jfnk"] = run_jfnk(args, 0)
+    if args.amr:
+        line["amr"] = run_amr(args, 0)
     if args.cpu and world == 1:
         line["cpu_baseline"] = cpu_baseline(args)
         if args.jfnk_precond:

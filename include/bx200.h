@@ -103,6 +103,15 @@ BX_API int bx_download_state(double *State_VGB, int nBlock);
 BX_API int bx_set_time(double tSimulation, int nStep);
 BX_API int bx_get_time(double *tSimulation, double *Dt, int *nStep);
 
+/* ModParallel DiLevel_EB(iSide, iBlock) and jBlock_IEB(iSub, iSide, iBlock)
+ * (src/ModParallel.f90:10-14) of the grid given to bx_init, sides x-, x+,
+ * y-, y+, z-, z+: level difference 0 (same level), +1 (the neighbour is
+ * coarser), -1 (finer), -100 (BATL Unset_: float boundary or ignored
+ * dimension); 1-based neighbour blocks, 4 for a finer side (first transverse
+ * direction fastest), 0 where there is none.  Arrays of 6*nBlock and
+ * 24*nBlock ints. */
+BX_API int bx_get_neighbors(int *DiLevel_EB, int *jBlock_IEB);
+
 /* ---- per-block entry points of the orig path (drop-in compatibility) ----
  * Each works on one block and keeps its result in device scratch arrays that
  * play the role of the module globals LeftState_V?, Flux_V?I, Source_VC. */
@@ -144,6 +153,8 @@ BX_API int bx_advance_explicit(int DoCalcTimestep);
  * explicit scheme, launched as one CUDA graph per step; with
  * TimeSimulationLimit <= 0 there is no time limit */
 BX_API int bx_advance(int nStep, double TimeSimulationLimit);
+/* time steps that bx_advance captures in one CUDA graph (default 1) */
+BX_API int bx_set_graph_steps(int nStepPerGraph);
 /* wait for the library's stream */
 BX_API int bx_synchronize(void);
 
@@ -212,10 +223,11 @@ BX_API int bx_impl_norm_noalloc(const double *Impl_dev, int nCellBlock, int nBlo
  * 3-layer 3x3x3 convolutional network per 8^3 block (16 -> 32 -> 32 -> 8
  * channels, ReLU, zero padding at the block faces) maps the block of a
  * Krylov vector (scaled by its block RMS s) and the block's normalised state
- * to a correction of the identity, z = v + s N(v / s, U / Norm_V), trained
- * on the targets (z - w) / s of the pairs below; BF16 operands, FP32
- * accumulation on the tensor cores.  Training pairs (w = A z, z) are taken
- * from the BILU-preconditioned FGMRES iterations of implicit steps.  FGMRES
+ * to its correction, z = s N(v / s, U / Norm_V); BF16 operands, FP32
+ * accumulation on the tensor cores.  Training pairs (v, z) are the Krylov
+ * vectors and their BILU corrections of the BILU-preconditioned FGMRES
+ * iterations of implicit steps (BILU is block-Jacobi, so z depends on the
+ * block's v and state only, which a per-block network can represent).  FGMRES
  * accepts any preconditioner, so the network changes iteration counts, not
  * the converged answer.  Parameter vector (FP32):
  *   W1[27][16][32] b1[32] W2[27][32][32] b2[32] W3[27][32][8] b3[8]
@@ -225,7 +237,7 @@ BX_API int bx_learned_finalize(void);
 BX_API int bx_learned_nparam(int *nParam);
 BX_API int bx_learned_set_params(const float *params, int nParam);
 BX_API int bx_learned_get_params(float *params, int nParam);
-/* store blocksPerPair randomly chosen blocks of every (w, z) pair of the
+/* store blocksPerPair randomly chosen blocks of every (v, z) pair of the
  * following implicit steps' FGMRES iterations (0 stops collecting) */
 BX_API int bx_learned_collect(int blocksPerPair);
 BX_API int bx_learned_num_samples(long long *nSample);

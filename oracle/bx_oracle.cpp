@@ -63,6 +63,16 @@ struct Oracle {
   int nStep = 0, iStage = 1;
   int nFace[3][3];  // face array extents per direction
   void *implPtr = nullptr;  // Implicit solver state (see below)
+  // ModParallel DiLevel_EB / jBlock_IEB (src/ModParallel.f90:10-14): per
+  // block and side the level difference to the neighbour (0, +1 coarser,
+  // -1 finer, kNoNei at a float boundary or an ignored dimension) and the
+  // neighbour blocks (4 finer ones, first transverse index fastest)
+  static constexpr int kNoNei = -99;
+  std::vector<int> dil, jbl;
+  bool hasResChange = false;
+  // face values kept per resolution-change face: nFaceValue slots, BnL, BnR
+  static constexpr int nCorr = nFaceValue + 2;
+  std::vector<double> fineFlux, corrFlux;  // [block][side][face][nCorr]
 
   long cell(int i, int j, int k) const {
     return (i - MinI) + (long)nIg * ((j - MinJ) + (long)nJg * (k - MinK));
@@ -135,6 +145,195 @@ struct Oracle {
       s.Source.assign((nVar + 1) * (long)c.nI * c.nJ * c.nK, 0.0);
       s.DivB1.assign((long)c.nI * c.nJ * c.nK, 0.0);
     }
+    build_neighbors();
+  }
+
+  // BATL find_neighbor (srcBATL, absent from the tree): the leaf at the same
+  // level across the side, else its parent (coarser), else the children of
+  // the same-level position that touch the side (finer)
+  void build_neighbors() {
+    dil.assign(6 * nBlock, kNoNei);
+    jbl.assign(24 * nBlock, -1);
+    for (int b = 0; b < nBlock; b++)
+      for (int d = 0; d < 3; d++)
+        for (int side = 0; side < 2; side++) {
+          const int sd = 2 * d + side;
+          if (d >= c.nDim) continue;
+          int cc[3] = {ic[3 * b], ic[3 * b + 1], ic[3 * b + 2]};
+          cc[d] += side ? 1 : -1;
+          const int n = c.nRoot[d] << lev[b];
+          if (cc[d] < 0 || cc[d] >= n) {
+            if (c.typeBc[sd] != ORA_BC_PERIODIC) continue;
+            cc[d] = (cc[d] + n) % n;
+          }
+          int q = find_block(lev[b], cc[0], cc[1], cc[2]);
+          if (q >= 0) { dil[6 * b + sd] = 0; jbl[24 * b + 4 * sd] = q; continue; }
+          if (lev[b] > 0 && (q = find_block(lev[b] - 1, cc[0] >> 1, cc[1] >> 1, cc[2] >> 1)) >= 0) {
+            dil[6 * b + sd] = 1; jbl[24 * b + 4 * sd] = q; hasResChange = true; continue;
+          }
+          int t[2], nt = 0;
+          for (int e = 0; e < c.nDim; e++) if (e != d) t[nt++] = e;
+          int m = 0;
+          for (int q1 = 0; q1 < (nt > 1 ? 2 : 1); q1++)
+            for (int q0 = 0; q0 < (nt > 0 ? 2 : 1); q0++) {
+              int f[3] = {2 * cc[0], c.nDim > 1 ? 2 * cc[1] : 0, c.nDim > 2 ? 2 * cc[2] : 0};
+              f[d] += side ? 0 : 1;
+              if (nt > 0) f[t[0]] += q0;
+              if (nt > 1) f[t[1]] += q1;
+              jbl[24 * b + 4 * sd + m++] = find_block(lev[b] + 1, f[0], f[1], f[2]);
+            }
+          dil[6 * b + sd] = -1;
+          hasResChange = true;
+        }
+    if (hasResChange) {
+      const long nf = (long)std::max(c.nI, c.nJ) * std::max(c.nJ, c.nK);
+      fineFlux.assign(6 * nf * nCorr * nBlock, 0.0);
+      corrFlux = fineFlux;
+    }
+  }
+
+  // ghost cells of the sides with a resolution change (message_pass_cell of
+  // BATL with nProlongOrder = 1, documented in PARAM.XML #RESCHANGE /
+  // Doc/Tex/grid.tex): a coarser neighbour's cell is copied into the fine
+  // ghost cells it covers (injection); a finer neighbour's 2x2x2 cells are
+  // averaged into the coarse ghost cell they fill (restriction)
+  void fill_reschange_ghosts() {
+    const int nCell[3] = {c.nI, c.nJ, c.nK};
+#pragma omp parallel for schedule(static) num_threads((int)scr.size())
+    for (int b = 0; b < nBlock; b++)
+      for (int sd = 0; sd < 2 * c.nDim; sd++) {
+        const int dl = dil[6 * b + sd];
+        if (dl != 1 && dl != -1) continue;
+        const int d = sd / 2, hi = sd % 2;
+        int lo3[3], hi3[3];
+        for (int e = 0; e < 3; e++) { lo3[e] = 1; hi3[e] = e < c.nDim ? nCell[e] : 1; }
+        lo3[d] = hi ? nCell[d] + 1 : 1 - nG;
+        hi3[d] = hi ? nCell[d] + nG : 0;
+        for (int k = lo3[2]; k <= hi3[2]; k++)
+          for (int j = lo3[1]; j <= hi3[1]; j++)
+            for (int i = lo3[0]; i <= hi3[0]; i++) {
+              const int idx[3] = {i, j, k};
+              double *t = st(b, i, j, k);
+              if (dl == 1) {
+                const int C = jbl[24 * b + 4 * sd];
+                int lc[3] = {1, 1, 1};
+                for (int e = 0; e < c.nDim; e++) {
+                  const long tot = (long)nCell[e] * (c.nRoot[e] << lev[b]);
+                  long gf = (long)ic[3 * b + e] * nCell[e] + idx[e] - 1;
+                  gf = (gf + tot) % tot;
+                  lc[e] = (int)((gf >> 1) - (long)ic[3 * C + e] * nCell[e]) + 1;
+                }
+                const double *src = st(C, lc[0], lc[1], lc[2]);
+                for (int v = 0; v < nVar; v++) t[v] = src[v];
+              } else {
+                long gc[3] = {0, 0, 0};
+                for (int e = 0; e < c.nDim; e++) {
+                  const long tot = (long)nCell[e] * (c.nRoot[e] << lev[b]);
+                  gc[e] = ((long)ic[3 * b + e] * nCell[e] + idx[e] - 1 + tot) % tot;
+                }
+                long f0[3] = {2 * gc[0], c.nDim > 1 ? 2 * gc[1] : 0, c.nDim > 2 ? 2 * gc[2] : 0};
+                const int F = find_block(lev[b] + 1, (int)(f0[0] / nCell[0]),
+                                         c.nDim > 1 ? (int)(f0[1] / nCell[1]) : 0,
+                                         c.nDim > 2 ? (int)(f0[2] / nCell[2]) : 0);
+                double sum[nVar] = {0, 0, 0, 0, 0, 0, 0, 0};
+                for (int kk = 0; kk < (c.nDim > 2 ? 2 : 1); kk++)
+                  for (int jj = 0; jj < (c.nDim > 1 ? 2 : 1); jj++)
+                    for (int ii = 0; ii < 2; ii++) {
+                      const long g3[3] = {f0[0] + ii, f0[1] + jj, f0[2] + kk};
+                      int lf[3] = {1, 1, 1};
+                      for (int e = 0; e < c.nDim; e++)
+                        lf[e] = (int)(g3[e] - (long)ic[3 * F + e] * nCell[e]) + 1;
+                      const double *src = st(F, lf[0], lf[1], lf[2]);
+                      for (int v = 0; v < nVar; v++) sum[v] = sum[v] + src[v];
+                    }
+                const double w = c.nDim == 3 ? 0.125 : (c.nDim == 2 ? 0.25 : 0.5);
+                for (int v = 0; v < nVar; v++) t[v] = sum[v] * w;
+              }
+            }
+      }
+  }
+
+  // face index (1-based) of side sd at the transverse position (t0, t1)
+  long side_face(int sd, int t0, int t1) const {
+    const int d = sd / 2, hi = sd % 2;
+    int idx[3];
+    idx[d] = hi ? (d == 0 ? c.nI : d == 1 ? c.nJ : c.nK) + 1 : 1;
+    int e0 = d == 0 ? 1 : 0, e1 = d == 2 ? 1 : 2;
+    idx[e0] = t0; idx[e1] = t1;
+    return face(d, idx[0], idx[1], idx[2]);
+  }
+  int side_extent(int sd, int which) const {
+    const int d = sd / 2;
+    const int e = which == 0 ? (d == 0 ? 1 : 0) : (d == 2 ? 1 : 2);
+    return e == 0 ? c.nI : e == 1 ? c.nJ : c.nK;
+  }
+
+  // save_cons_flux (src/ModConserveFlux.f90:79-265): fluxes 1..Vdt_ and
+  // Bn * FaceRatio at the faces of a finer block next to a coarser one
+  void save_cons_flux(int b, Scratch &s) {
+    const double FaceRatio = 1.0 / (1 << (c.nDim - 1));
+    const long nf = (long)std::max(c.nI, c.nJ) * std::max(c.nJ, c.nK);
+    for (int sd = 0; sd < 2 * c.nDim; sd++) {
+      if (dil[6 * b + sd] != 1) continue;
+      const int d = sd / 2;
+      for (int t1 = 1; t1 <= side_extent(sd, 1); t1++)
+        for (int t0 = 1; t0 <= side_extent(sd, 0); t0++) {
+          const long f = side_face(sd, t0, t1);
+          double *o = &fineFlux[nCorr * ((long)(6 * b + sd) * nf + (t0 - 1) + (long)side_extent(sd, 0) * (t1 - 1))];
+          for (int m = 0; m < nFaceValue; m++) o[m] = s.Flux[d][nFaceValue * f + m];
+          o[nFaceValue] = s.Left[d][nVar * f + Bx_ + d] * FaceRatio;
+          o[nFaceValue + 1] = s.Right[d][nVar * f + Bx_ + d] * FaceRatio;
+        }
+    }
+  }
+
+  // message_pass_face of BATL (absent; DoSubtractIn = .false.): the coarse
+  // side of a resolution change receives the sum of the values of the 2x2
+  // finer faces covering each of its faces
+  void message_pass_face() {
+    const long nf = (long)std::max(c.nI, c.nJ) * std::max(c.nJ, c.nK);
+#pragma omp parallel for schedule(static) num_threads((int)scr.size())
+    for (int b = 0; b < nBlock; b++)
+      for (int sd = 0; sd < 2 * c.nDim; sd++) {
+        if (dil[6 * b + sd] != -1) continue;
+        const int n0 = side_extent(sd, 0), n1 = side_extent(sd, 1);
+        const int h0 = n0 / 2, h1 = c.nDim > 2 ? n1 / 2 : n1;
+        for (int t1 = 1; t1 <= n1; t1++)
+          for (int t0 = 1; t0 <= n0; t0++) {
+            const int q0 = t0 > h0, q1 = c.nDim > 2 ? (t1 > h1) : 0;
+            const int F = jbl[24 * b + 4 * sd + q0 + 2 * q1];
+            const int sf = sd ^ 1;  // the finer block's side facing b
+            const int a0 = 2 * (t0 - 1 - q0 * h0), a1 = c.nDim > 2 ? 2 * (t1 - 1 - q1 * h1) : t1 - 1;
+            double *o = &corrFlux[nCorr * ((long)(6 * b + sd) * nf + (t0 - 1) + (long)n0 * (t1 - 1))];
+            for (int m = 0; m < nCorr; m++) {
+              double sum = 0;
+              for (int u1 = 0; u1 < (c.nDim > 2 ? 2 : 1); u1++)
+                for (int u0 = 0; u0 < 2; u0++) {
+                  const long fi = (a0 + u0) + (long)n0 * (a1 + u1);
+                  sum = sum + fineFlux[nCorr * ((long)(6 * F + sf) * nf + fi) + m];
+                }
+              o[m] = sum;
+            }
+          }
+      }
+  }
+
+  // apply_cons_flux (src/ModConserveFlux.f90:268-445): the coarse side of a
+  // resolution change takes the summed finer fluxes and normal fields
+  void apply_cons_flux(int b, Scratch &s) {
+    const long nf = (long)std::max(c.nI, c.nJ) * std::max(c.nJ, c.nK);
+    for (int sd = 0; sd < 2 * c.nDim; sd++) {
+      if (dil[6 * b + sd] != -1) continue;
+      const int d = sd / 2;
+      for (int t1 = 1; t1 <= side_extent(sd, 1); t1++)
+        for (int t0 = 1; t0 <= side_extent(sd, 0); t0++) {
+          const long f = side_face(sd, t0, t1);
+          const double *o = &corrFlux[nCorr * ((long)(6 * b + sd) * nf + (t0 - 1) + (long)side_extent(sd, 0) * (t1 - 1))];
+          for (int m = 0; m < nFaceValue; m++) s.Flux[d][nFaceValue * f + m] = o[m];
+          s.Left[d][nVar * f + Bx_ + d] = o[nFaceValue];
+          s.Right[d][nVar * f + Bx_ + d] = o[nFaceValue + 1];
+        }
+    }
   }
 
   // ------------------------------------------------------------------
@@ -200,6 +399,7 @@ struct Oracle {
             for (int v = 0; v < nVar; v++) t[v] = s[v];
           }
     }
+    if (hasResChange) fill_reschange_ghosts();
   }
 
   // ------------------------------------------------------------------
@@ -279,6 +479,17 @@ struct Oracle {
                 s.Left[d][nVar * fi + v] = q[f - 1] + dL[f - 1];
                 s.Right[d][nVar * fi + v] = q[f] - dR[f];
               }
+            }
+            // get_faceX_first at a side next to a coarser block
+            // (src/ModFaceValue.f90:1118-1137, UseTvdResChange = F)
+            for (int hi = 0; hi < 2 && hasResChange && c.nOrder == 2; hi++) {
+              if (dil[6 * b + 2 * d + hi] != 1) continue;
+              const int f = hi ? n + 1 : 1;
+              int idx[3];
+              idx[d] = f; idx[a1] = p1; idx[a2] = p2;
+              const long fi = face(d, idx[0], idx[1], idx[2]);
+              s.Left[d][nVar * fi + v] = q[f - 1];
+              s.Right[d][nVar * fi + v] = q[f];
             }
           }
     }
@@ -685,6 +896,25 @@ struct Oracle {
   int advance_explicit() {
     int err = 0;
     for (iStage = 1; iStage <= c.nStage; iStage++) {
+      if (hasResChange) {
+        // DoConserveFlux (src/ModAdvanceExplicit.f90:101-131): fluxes of the
+        // finer blocks at resolution changes, then message_pass_face
+#pragma omp parallel for schedule(dynamic, 4) num_threads((int)scr.size()) reduction(| : err)
+        for (int b = 0; b < nBlock; b++) {
+          bool fine = false;
+          for (int sd = 0; sd < 6; sd++) fine = fine || dil[6 * b + sd] == 1;
+          if (!fine) continue;
+          int t = 0;
+#ifdef _OPENMP
+          t = omp_get_thread_num();
+#endif
+          Scratch &s = scr[t];
+          calc_face_value(b, s);
+          err |= calc_face_flux(b, s);
+          save_cons_flux(b, s);
+        }
+        message_pass_face();
+      }
 #pragma omp parallel for schedule(dynamic, 4) num_threads((int)scr.size()) reduction(| : err)
       for (int b = 0; b < nBlock; b++) {
         int t = 0;
@@ -694,6 +924,7 @@ struct Oracle {
         Scratch &s = scr[t];
         calc_face_value(b, s);
         err |= calc_face_flux(b, s);
+        if (hasResChange) apply_cons_flux(b, s);
         calc_source(b, s);
         update_state(b, s);
         if (iStage == c.nStage && !c.useDtFixed) calc_timestep(b, s);

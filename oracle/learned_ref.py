@@ -107,15 +107,15 @@ def loss_and_grad(p, x0, tgt, bf=True):
 
 def apply(p, v, feat):
     """The preconditioner on blocks: v [nBlock][8][512] (solver layout, cell
-    = x + 8 y + 64 z), feat [nBlock][512][8]; z = v + s N(v / s, feat) with s
-    the RMS of v over the block."""
+    = x + 8 y + 64 z), feat [nBlock][512][8]; z = s N(v / s, feat) with s the
+    RMS of v over the block."""
     nb = v.shape[0]
     s = np.sqrt((v.reshape(nb, -1) ** 2).mean(axis=1))
     inv = np.where(s > 1e-300, 1.0 / np.where(s > 0, s, 1.0), 0.0)
     r = (v * inv[:, None, None]).astype(np.float32)        # [nb][8][512]
     x0 = np.concatenate([r.transpose(0, 2, 1), feat.astype(np.float32)], axis=2)  # [nb][512][16]
     out, _, _ = forward(p, x0.reshape(nb, 8, 8, 8, 16))
-    return v + s[:, None, None] * out.reshape(nb, 512, 8).transpose(0, 2, 1)
+    return s[:, None, None] * out.reshape(nb, 512, 8).transpose(0, 2, 1)
 
 
 def init_params(seed=0, out_gain=0.1):

@@ -97,7 +97,7 @@ def _jfnk(prec, state, net=None, steps=3):
 
 def test_learned_fgmres_converges_and_gains(net):
     g, s, p, st = configs.jfnk_ot(nRoot=4)
-    # collect (w = A z, z) pairs from BILU-preconditioned steps, then train
+    # collect (v, BILU(v)) pairs from BILU-preconditioned steps, then train
     net.collect(64)
     _jfnk("BILU", st, steps=6)
     net.collect(0)
