@@ -35,5 +35,7 @@ bool learned_collecting();
 int learned_features(const double *U, const double *norm, int nBlock, cudaStream_t st);
 int learned_apply(const double *v, double *z, int nBlock, cudaStream_t st);
 int learned_collect(const double *w, const double *z, int nBlock, cudaStream_t st);
+int learned_collect_n(const double *w, const double *z, int nBlock, int perPair, cudaStream_t st);
+bool learned_has_room();
 
 }  // namespace bx

@@ -550,4 +550,36 @@ __global__ void k_sub(double *__restrict__ r, const double *__restrict__ rhs, co
   for (long q = blockIdx.x * (long)blockDim.x + threadIdx.x; q < n; q += (long)gridDim.x * blockDim.x) r[q] = rhs[q] - y[q];
 }
 
+// seeded standard-normal noise (counter-based hash, Box-Muller)
+__device__ __forceinline__ uint64_t mix64(uint64_t x) {
+  x ^= x >> 33; x *= 0xff51afd7ed558ccdull; x ^= x >> 33; x *= 0xc4ceb9fe1a85ec53ull; x ^= x >> 33;
+  return x;
+}
+__global__ void k_probe_noise(double *v, long n, unsigned long long seed) {
+  for (long q = blockIdx.x * (long)blockDim.x + threadIdx.x; q < n; q += (long)gridDim.x * blockDim.x) {
+    const uint64_t h1 = mix64(seed * 0x9E3779B97F4A7C15ull + 2 * (uint64_t)q + 1);
+    const uint64_t h2 = mix64(h1 ^ 0xD1B54A32D192ED03ull);
+    const double u1 = ((h1 >> 11) + 0.5) * 0x1.0p-53, u2 = (h2 >> 11) * 0x1.0p-53;
+    v[q] = sqrt(-2.0 * log(u1)) * cos(6.283185307179586 * u2);
+  }
+}
+// out = average of a cell and its 6 neighbours inside its block (each
+// variable of the [block][var][cell] vector separately)
+__global__ void k_probe_smooth(double *out, const double *in, int N, long n) {
+  const long nc = (long)N * N * N;
+  for (long q = blockIdx.x * (long)blockDim.x + threadIdx.x; q < n; q += (long)gridDim.x * blockDim.x) {
+    const long base = q - q % nc;
+    const int c = (int)(q % nc), i = c % N, j = (c / N) % N, k = c / (N * N);
+    double s = in[q];
+    int m = 1;
+    if (i > 0) { s += in[base + c - 1]; m++; }
+    if (i < N - 1) { s += in[base + c + 1]; m++; }
+    if (j > 0) { s += in[base + c - N]; m++; }
+    if (j < N - 1) { s += in[base + c + N]; m++; }
+    if (k > 0) { s += in[base + c - N * N]; m++; }
+    if (k < N - 1) { s += in[base + c + N * N]; m++; }
+    out[q] = s / m;
+  }
+}
+
 }  // namespace bx

@@ -497,4 +497,30 @@ int bx_impl_get_x(double *x_I) {
   return soa_to_host(I.X, x_I);
 }
 
+int bx_learned_collect_probes(int nProbe, int blocksPerPair, unsigned long long seed) {
+  Core c = core();
+  if (!I.ready || !learned_ready()) return core_fail(BX_ERR_STATE, "needs bx_implicit_init and bx_learned_init");
+  if (I.p.TypePrecond != BX_PRECOND_BILU || !I.havePrec || c.nI != 8)
+    return core_fail(BX_ERR_STATE, "needs the BILU factors of an implicit step on 8x8x8 blocks");
+  if (nProbe < 0 || blocksPerPair < 1 || blocksPerPair > 65536)
+    return core_fail(BX_ERR_ARG, "nProbe=%d blocksPerPair=%d", nProbe, blocksPerPair);
+  int r = learned_features(I.U, I.dNorm, c.nBlock, c.st);
+  if (r) return r;
+  static const int kPasses[4] = {0, 1, 3, 8};
+  for (int p = 0; p < nProbe && learned_has_room(); p++) {
+    // seeded noise, smoothed inside each block by 0, 1, 3 or 8 averaging passes
+    k_probe_noise<<<kG, kT, 0, c.st>>>(I.W, I.N, seed + (unsigned long long)p);
+    double *a = I.W, *b = I.R;
+    for (int q = 0; q < kPasses[p % 4]; q++) {
+      k_probe_smooth<<<kG, kT, 0, c.st>>>(b, a, I.nCellBlock == 512 ? 8 : 4, I.N);
+      std::swap(a, b);
+    }
+    CKI(cudaGetLastError());
+    if ((r = precond(a, I.Z))) return r;
+    if ((r = learned_collect_n(a, I.Z, c.nBlock, blocksPerPair, c.st))) return r;
+  }
+  CKI(cudaStreamSynchronize(c.st));
+  return BX_OK;
+}
+
 }  // extern "C"

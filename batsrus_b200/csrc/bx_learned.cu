@@ -242,8 +242,8 @@ int learned_apply(const double *v, double *z, int nBlock, cudaStream_t st) {
 
 bool learned_collecting() { return Lc.ready && Lc.collectPerPair > 0 && Lc.nSample < Lc.nSampleMax; }
 
-int learned_collect(const double *w, const double *z, int nBlock, cudaStream_t st) {
-  const long nPick = std::min<long>(Lc.collectPerPair, Lc.nSampleMax - Lc.nSample);
+int learned_collect_n(const double *w, const double *z, int nBlock, int perPair, cudaStream_t st) {
+  const long nPick = std::min<long>(perPair, Lc.nSampleMax - Lc.nSample);
   if (nPick <= 0) return BX_OK;
   std::vector<int> pick(nPick);
   std::uniform_int_distribution<int> U(0, nBlock - 1);
@@ -255,6 +255,12 @@ int learned_collect(const double *w, const double *z, int nBlock, cudaStream_t s
   Lc.nSample += nPick;
   return BX_OK;
 }
+
+int learned_collect(const double *w, const double *z, int nBlock, cudaStream_t st) {
+  return learned_collect_n(w, z, nBlock, Lc.collectPerPair, st);
+}
+
+bool learned_has_room() { return Lc.ready && Lc.nSample < Lc.nSampleMax; }
 
 void learned_release() {
   if (Lc.ready) free_learned();

@@ -33,6 +33,11 @@ class LearnedPreconditioner:
     def collect(self, blocksPerPair):
         check(self.L.bx_learned_collect(int(blocksPerPair)))
 
+    def collect_probes(self, nProbe, blocksPerPair, seed=1):
+        """(v, BILU(v)) pairs of seeded probe vectors; call after an implicit
+        step with the BILU preconditioner"""
+        check(self.L.bx_learned_collect_probes(int(nProbe), int(blocksPerPair), int(seed)))
+
     def num_samples(self):
         n = ctypes.c_longlong(0)
         check(self.L.bx_learned_num_samples(ctypes.byref(n)))

@@ -218,12 +218,18 @@ def run_jfnk(args, lrank):
         x = ExplicitSolver(g, s, device=lrank)
         x.set_state(st)
         im = ImplicitSolver(x, p)
-        for _ in range(1 + args.jfnk_warmup):  # the first step only sets the time step
-            im.advance_part_impl()
-        x.synchronize()
-        x.region_begin()
-        stats = [im.advance_part_impl() for _ in range(args.jfnk_steps)]
-        ms = x.region_end()
+        from batsrus_b200.capi import BxError
+        try:
+            for _ in range(1 + args.jfnk_warmup):  # the first step only sets the time step
+                im.advance_part_impl()
+            x.synchronize()
+            x.region_begin()
+            stats = [im.advance_part_impl() for _ in range(args.jfnk_steps)]
+            ms = x.region_end()
+        except BxError as e:
+            out[prec.lower()] = {"failed": str(e)}
+            x.close()
+            continue
         out[prec.lower()] = {
             "s_per_step": ms * 1e-3 / args.jfnk_steps,
             "matvec_per_step": float(np.mean([q["nMatvec"] for q in stats])),
@@ -239,8 +245,9 @@ def run_jfnk(args, lrank):
 
 def train_learned(args, g, s, lrank, nPair=2000, blocksPerPair=16):
     """Training data and training of the learned preconditioner: (v, BILU(v))
-    pairs of Krylov vectors from the BILU-preconditioned FGMRES of implicit
-    steps started from
+    pairs, half of them the Krylov vectors of the BILU-preconditioned FGMRES
+    of implicit steps, half seeded probe vectors (noise smoothed inside the
+    blocks to several degrees) at the last step's state; the steps start from
     a differently seeded perturbation (seed 2025) than the timed steps,
     blocksPerPair random blocks of each of nPair pairs; then Adam."""
     from batsrus_b200 import configs
@@ -253,21 +260,26 @@ def train_learned(args, g, s, lrank, nPair=2000, blocksPerPair=16):
     x.set_state(st2)
     im = ImplicitSolver(x, p)
     t0 = time.perf_counter()
+    # half of the pairs from the Krylov vectors of BILU-preconditioned
+    # implicit steps, half from seeded probe vectors at the last step's state
     net.collect(blocksPerPair)
     nStep = 0
     from batsrus_b200.capi import BxError
-    while net.num_samples() < nPair * blocksPerPair and nStep < 200:
+    while net.num_samples() < (nPair // 2) * blocksPerPair and nStep < 100:
         try:
             im.advance_part_impl()
         except BxError:  # a failed solve ends the collection
             break
         nStep += 1
     net.collect(0)
+    nKrylov = net.num_samples() // blocksPerPair
+    net.collect_probes(nPair - nKrylov, blocksPerPair, seed=2025)
     x.close()
     t1 = time.perf_counter()
     first, last = net.train(nEpoch=args.learned_epochs, batch=256, lr=2e-3)
     t2 = time.perf_counter()
-    return net, {"pairs": net.num_samples() // blocksPerPair, "block_samples": net.num_samples(),
+    return net, {"pairs": net.num_samples() // blocksPerPair, "krylov_pairs": nKrylov,
+                 "probe_pairs": net.num_samples() // blocksPerPair - nKrylov, "block_samples": net.num_samples(),
                  "collect_steps": nStep, "collect_s": t1 - t0, "epochs": args.learned_epochs,
                  "train_s": t2 - t1, "mse_first_epoch": first, "mse_last_epoch": last,
                  "seed_data": 2025, "seed_timed": 2024}

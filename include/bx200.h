@@ -240,6 +240,12 @@ BX_API int bx_learned_get_params(float *params, int nParam);
 /* store blocksPerPair randomly chosen blocks of every (v, z) pair of the
  * following implicit steps' FGMRES iterations (0 stops collecting) */
 BX_API int bx_learned_collect(int blocksPerPair);
+/* after an implicit step with BX_PRECOND_BILU: store blocksPerPair random
+ * blocks of each of nProbe pairs (v, BILU(v)) for seeded probe vectors v
+ * (normal noise, smoothed inside each block by 0, 1, 3 or 8 averaging
+ * passes in turn), so that the training inputs span smooth and rough
+ * vectors as well as the Krylov vectors */
+BX_API int bx_learned_collect_probes(int nProbe, int blocksPerPair, unsigned long long seed);
 BX_API int bx_learned_num_samples(long long *nSample);
 /* replace the training set: in16 [nSample][512][16] (input / s, then the 8
  * features), tgt [nSample][512][8] (target / s); cell = i + 8 j + 64 k */

@@ -97,11 +97,19 @@ def _jfnk(prec, state, net=None, steps=3):
 
 def test_learned_fgmres_converges_and_gains(net):
     g, s, p, st = configs.jfnk_ot(nRoot=4)
-    # collect (v, BILU(v)) pairs from BILU-preconditioned steps, then train
-    net.collect(64)
-    _jfnk("BILU", st, steps=6)
+    _, _, _, st2 = configs.jfnk_ot(nRoot=4, seed=2025)
+    # (v, BILU(v)) pairs: Krylov vectors of BILU-preconditioned steps from
+    # another seed, then probe vectors at the last state; then train
+    x = ExplicitSolver(g, s)
+    x.set_state(st2)
+    im = ImplicitSolver(x, p)
+    net.collect(8)
+    for _ in range(4):
+        im.advance_part_impl()
     net.collect(0)
-    assert net.num_samples() > 1000
+    net.collect_probes(64, 32, seed=5)
+    x.close()
+    assert net.num_samples() > 2000
     first, last = net.train(nEpoch=12, batch=128, lr=2e-3)
     assert last < first
     bilu, sb, g = _jfnk("BILU", st)
