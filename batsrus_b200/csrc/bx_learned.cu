@@ -40,6 +40,7 @@ struct LCtx {
   float *scal = nullptr;  // loss, gb3[8], gb2[32], gb1[32]
   int *err = nullptr, *pick = nullptr;
   int adamStep = 0;
+  int relu = 0;  // 0: linear in the Krylov vector; 1: ReLU network with features
   cudaStream_t st = nullptr;
 };
 
@@ -88,6 +89,7 @@ Weights weights() {
   W.b1 = Lc.p + kOffB1;
   W.b2 = Lc.p + kOffB2;
   W.b3 = Lc.p + kOffB3;
+  W.relu = Lc.relu;
   return W;
 }
 
@@ -204,6 +206,7 @@ int gradient(long s0, int nS, cudaStream_t st) {
   CKL(cudaMemcpyAsync(Lc.g + kOffB3, Lc.scal + 1, sizeof(float) * kC3, cudaMemcpyDeviceToDevice, st));
   CKL(cudaMemcpyAsync(Lc.g + kOffB2, Lc.scal + 9, sizeof(float) * kC2, cudaMemcpyDeviceToDevice, st));
   CKL(cudaMemcpyAsync(Lc.g + kOffB1, Lc.scal + 41, sizeof(float) * kC1, cudaMemcpyDeviceToDevice, st));
+  if (!Lc.relu) k_mask_linear<<<(kTaps * kC0 * kC1 + 255) / 256, 256, 0, st>>>(Lc.g);
   CKL(cudaGetLastError());
   return BX_OK;
 }
@@ -308,7 +311,7 @@ int bx_learned_init(long long nSampleMax, unsigned long long seed) {
   std::vector<float> h(kNParam, 0.f);
   std::normal_distribution<float> N01(0.f, 1.f);
   auto fill = [&](int off, int cin, int cout, float gain) {
-    const float sd = gain * std::sqrt(2.f / (27.f * cin));
+    const float sd = gain * std::sqrt((Lc.relu ? 2.f : 1.f) / (27.f * cin));
     for (int i = 0; i < kTaps * cin * cout; i++) h[off + i] = sd * N01(Lc.rng);
   };
   fill(kOffW1, kC0, kC1, 1.f);
@@ -318,9 +321,25 @@ int bx_learned_init(long long nSampleMax, unsigned long long seed) {
   CKL(cudaMemsetAsync(Lc.m, 0, sizeof(float) * kNParam, Lc.st));
   CKL(cudaMemsetAsync(Lc.v, 0, sizeof(float) * kNParam, Lc.st));
   CKL(cudaMemsetAsync(Lc.err, 0, sizeof(int), Lc.st));
+  if (!Lc.relu) k_mask_linear<<<(kTaps * kC0 * kC1 + 255) / 256, 256, 0, Lc.st>>>(Lc.p);
   if ((r = pack(Lc.st))) { free_learned(); return r; }
   CKL(cudaStreamSynchronize(Lc.st));
   Lc.ready = true;
+  return BX_OK;
+}
+
+int bx_learned_set_activation(int relu) {
+  int r = require_ready();
+  if (r) return r;
+  if (relu != 0 && relu != 1) return core_fail(BX_ERR_ARG, "relu=%d", relu);
+  Lc.relu = relu;
+  if (!relu) {
+    for (float *x : {Lc.p, Lc.m, Lc.v})
+      k_mask_linear<<<(kTaps * kC0 * kC1 + 255) / 256, 256, 0, Lc.st>>>(x);
+    CKL(cudaGetLastError());
+  }
+  if ((r = pack(Lc.st))) return r;
+  CKL(cudaStreamSynchronize(Lc.st));
   return BX_OK;
 }
 

@@ -136,6 +136,8 @@ struct Weights {
   // packed BF16 images (global)
   const unsigned char *w1, *w2, *w3, *w3t, *w2t;
   const float *b1, *b2, *b3;  // biases (FP32)
+  int relu;  // 1: ReLU between the layers and the cell features as input;
+             // 0: linear in the Krylov vector (no activation, features off)
 };
 
 }  // namespace learned

@@ -74,14 +74,15 @@ __device__ __forceinline__ void for_tiles(uint32_t tmem, F &&f) {
   }
 }
 
-// bias + ReLU, BF16 into the 32-channel buffer (and optionally global)
+// bias (+ ReLU), BF16 into the 32-channel buffer (and optionally global)
 __device__ __forceinline__ void relu_store32(unsigned char *buf, const float *bias, int cell, const float (&acc)[32],
-                                             __nv_bfloat16 *gout) {
+                                             __nv_bfloat16 *gout, int relu) {
   uint4 q[4];
   uint32_t *w = reinterpret_cast<uint32_t *>(q);
+  const float lo = relu ? 0.f : -INFINITY;
 #pragma unroll
   for (int i = 0; i < 16; i++)
-    w[i] = pack_bf16x2(fmaxf(acc[2 * i] + bias[2 * i], 0.f), fmaxf(acc[2 * i + 1] + bias[2 * i + 1], 0.f));
+    w[i] = pack_bf16x2(fmaxf(acc[2 * i] + bias[2 * i], lo), fmaxf(acc[2 * i + 1] + bias[2 * i + 1], lo));
 #pragma unroll
   for (int kc = 0; kc < 4; kc++) *reinterpret_cast<uint4 *>(buf + cell_chunk(cell, kc, kLS32)) = q[kc];
   if (gout) {
@@ -142,7 +143,7 @@ __global__ void __launch_bounds__(kThreads, 1)
 #pragma unroll
           for (int m = 0; m < 4; m++)
             w[m] = pack_bf16x2((float)vb[(2 * m) * 512 + c] * inv, (float)vb[(2 * m + 1) * 512 + c] * inv);
-        } else {
+        } else if (W.relu) {
           q = fb[c];
         }
       }
@@ -157,7 +158,7 @@ __global__ void __launch_bounds__(kThreads, 1)
     if (!(ok = wait_mma(S, phase))) break;
     zero_pads(bufB, 4);
     for_tiles<32>(tmem, [&](int, int, int cell, const float(&acc)[32]) {
-      if (cell >= 0) relu_store32(bufA, S.bias, cell, acc, nullptr);
+      if (cell >= 0) relu_store32(bufA, S.bias, cell, acc, nullptr, W.relu);
     });
     tc::fence_before();
     fence_proxy_async_smem();
@@ -168,7 +169,7 @@ __global__ void __launch_bounds__(kThreads, 1)
     }
     if (!(ok = wait_mma(S, phase))) break;
     for_tiles<32>(tmem, [&](int, int, int cell, const float(&acc)[32]) {
-      if (cell >= 0) relu_store32(bufB, S.bias + 32, cell, acc, nullptr);
+      if (cell >= 0) relu_store32(bufB, S.bias + 32, cell, acc, nullptr, W.relu);
     });
     tc::fence_before();
     fence_proxy_async_smem();
@@ -234,7 +235,7 @@ __global__ void __launch_bounds__(kThreads, 1)
     zero_pads(bufB, 4);
     __nv_bfloat16 *a1 = A1 + (size_t)n * 512 * 32, *a2 = A2 + (size_t)n * 512 * 32;
     for_tiles<32>(tmem, [&](int, int, int cell, const float(&acc)[32]) {
-      if (cell >= 0) relu_store32(bufA, S.bias, cell, acc, a1);
+      if (cell >= 0) relu_store32(bufA, S.bias, cell, acc, a1, W.relu);
     });
     tc::fence_before();
     fence_proxy_async_smem();
@@ -245,7 +246,7 @@ __global__ void __launch_bounds__(kThreads, 1)
     }
     if (!(ok = wait_mma(S, phase))) break;
     for_tiles<32>(tmem, [&](int, int, int cell, const float(&acc)[32]) {
-      if (cell >= 0) relu_store32(bufB, S.bias + 32, cell, acc, a2);
+      if (cell >= 0) relu_store32(bufB, S.bias + 32, cell, acc, a2, W.relu);
     });
     tc::fence_before();
     fence_proxy_async_smem();
@@ -352,7 +353,7 @@ __global__ void __launch_bounds__(kThreads, 1)
         for (int i = 0; i < 4; i++) {
           const float2 a = unpack_bf16x2(aw[i]);
           const int c = 8 * kc + 2 * i;
-          w[4 * kc + i] = pack_bf16x2(a.x > 0.f ? acc[c] : 0.f, a.y > 0.f ? acc[c + 1] : 0.f);
+          w[4 * kc + i] = pack_bf16x2(!W.relu || a.x > 0.f ? acc[c] : 0.f, !W.relu || a.y > 0.f ? acc[c + 1] : 0.f);
           const float2 r = unpack_bf16x2(w[4 * kc + i]);
           gb[c] += r.x;
           gb[c + 1] += r.y;
@@ -518,6 +519,19 @@ __global__ void k_pack(const float *__restrict__ p, __nv_bfloat16 *w1, __nv_bflo
     w3t[bimg_index(tap, k, n, kC2, kN3)] =
         __float2bfloat16_rn(n < kC3 ? p[kOffW3 + (tap * kC2 + k) * kC3 + n] : 0.f);
   }
+}
+
+// linear mode: the biases and the feature inputs of layer 1 stay zero (their
+// entries of x are cleared)
+__global__ void k_mask_linear(float *x) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < kTaps * kC0 * kC1) {
+    const int ci = (i / kC1) % kC0;
+    if (ci >= 8) x[kOffW1 + i] = 0.f;
+  }
+  if (i < kC1) x[kOffB1 + i] = 0.f;
+  if (i < kC2) x[kOffB2 + i] = 0.f;
+  if (i < kC3) x[kOffB3 + i] = 0.f;
 }
 
 // grad[j] = sum over CTAs of part[cta][j] for one layer's weight block

@@ -11,9 +11,11 @@ from .capi import check, dptr, fptr
 
 
 class LearnedPreconditioner:
-    def __init__(self, nSampleMax=32768, seed=2024):
+    def __init__(self, nSampleMax=32768, seed=2024, relu=False):
         self.L = capi.load()
         check(self.L.bx_learned_init(int(nSampleMax), int(seed)))
+        if relu:
+            check(self.L.bx_learned_set_activation(1))
         n = ctypes.c_int(0)
         check(self.L.bx_learned_nparam(ctypes.byref(n)))
         self.nparam = n.value

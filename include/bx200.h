@@ -233,6 +233,11 @@ BX_API int bx_impl_norm_noalloc(const double *Impl_dev, int nCellBlock, int nBlo
  *   W1[27][16][32] b1[32] W2[27][32][32] b2[32] W3[27][32][8] b3[8]
  * with tap = (dz+1)*9 + (dy+1)*3 + (dx+1). */
 BX_API int bx_learned_init(long long nSampleMax, unsigned long long seed);
+/* relu = 0 (the default after bx_learned_init): the network is linear in the
+ * Krylov vector (no activation, zero biases, feature inputs off), a learned
+ * per-block stencil that FGMRES sees as a linear preconditioner; relu = 1:
+ * ReLU between the layers and the cell features as inputs */
+BX_API int bx_learned_set_activation(int relu);
 BX_API int bx_learned_finalize(void);
 BX_API int bx_learned_nparam(int *nParam);
 BX_API int bx_learned_set_params(const float *params, int nParam);

@@ -76,36 +76,43 @@ def _round(a, on):
     return bf16(a).astype(np.float64) if on else np.asarray(a, dtype=np.float64)
 
 
-def forward(p, x0, bf=True):
-    """x0: [n, 8, 8, 8, 16] network input; returns (out, a1, a2)."""
+def forward(p, x0, bf=True, relu=True):
+    """x0: [n, 8, 8, 8, 16] network input; returns (out, a1, a2).  relu=False
+    is the linear mode (no activation)."""
     P = unpack(p)
     W1, W2, W3 = (_round(P[k], bf) for k in ("W1", "W2", "W3"))
     x0 = _round(x0, bf)
-    a1 = _round(np.maximum(conv(x0, W1) + P["b1"], 0.0), bf)
-    a2 = _round(np.maximum(conv(a1, W2) + P["b2"], 0.0), bf)
+    act = (lambda a: np.maximum(a, 0.0)) if relu else (lambda a: a)
+    a1 = _round(act(conv(x0, W1) + P["b1"]), bf)
+    a2 = _round(act(conv(a1, W2) + P["b2"]), bf)
     out = conv(a2, W3) + P["b3"]
     return out, a1, a2
 
 
-def loss_and_grad(p, x0, tgt, bf=True):
+def loss_and_grad(p, x0, tgt, bf=True, relu=True):
     """Sum of squares of (out - tgt) and the gradient of its mean over all
-    output elements (the GPU's scaling of dL/dY3)."""
+    output elements (the GPU's scaling of dL/dY3).  In the linear mode the
+    biases and the feature inputs of layer 1 get zero gradients."""
     P = unpack(p)
     W2, W3 = _round(P["W2"], bf), _round(P["W3"], bf)
     x0r = _round(x0, bf)
-    out, a1, a2 = forward(p, x0, bf)
+    out, a1, a2 = forward(p, x0, bf, relu)
     d = out - tgt
     gscale = 2.0 / d.size
     g3 = _round(gscale * d, bf)
-    g2 = _round(conv_t(g3, W3) * (a2 > 0), bf)
-    g1 = _round(conv_t(g2, W2) * (a1 > 0), bf)
+    g2 = _round(conv_t(g3, W3) * ((a2 > 0) if relu else 1.0), bf)
+    g1 = _round(conv_t(g2, W2) * ((a1 > 0) if relu else 1.0), bf)
     G = {"W3": weight_grad(a2, g3), "b3": g3.sum(axis=(0, 1, 2, 3)),
          "W2": weight_grad(a1, g2), "b2": g2.sum(axis=(0, 1, 2, 3)),
          "W1": weight_grad(x0r, g1), "b1": g1.sum(axis=(0, 1, 2, 3))}
+    if not relu:
+        G["W1"][:, 8:, :] = 0.0
+        for k in ("b1", "b2", "b3"):
+            G[k] = 0.0 * G[k]
     return float((d * d).sum()), pack(G)
 
 
-def apply(p, v, feat):
+def apply(p, v, feat, relu=True):
     """The preconditioner on blocks: v [nBlock][8][512] (solver layout, cell
     = x + 8 y + 64 z), feat [nBlock][512][8]; z = s N(v / s, feat) with s the
     RMS of v over the block."""
@@ -113,8 +120,9 @@ def apply(p, v, feat):
     s = np.sqrt((v.reshape(nb, -1) ** 2).mean(axis=1))
     inv = np.where(s > 1e-300, 1.0 / np.where(s > 0, s, 1.0), 0.0)
     r = (v * inv[:, None, None]).astype(np.float32)        # [nb][8][512]
-    x0 = np.concatenate([r.transpose(0, 2, 1), feat.astype(np.float32)], axis=2)  # [nb][512][16]
-    out, _, _ = forward(p, x0.reshape(nb, 8, 8, 8, 16))
+    f = feat.astype(np.float32) if relu else np.zeros_like(feat, dtype=np.float32)
+    x0 = np.concatenate([r.transpose(0, 2, 1), f], axis=2)  # [nb][512][16]
+    out, _, _ = forward(p, x0.reshape(nb, 8, 8, 8, 16), relu=relu)
     return s[:, None, None] * out.reshape(nb, 512, 8).transpose(0, 2, 1)
 
 

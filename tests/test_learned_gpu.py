@@ -37,23 +37,44 @@ def net():
     n.close()
 
 
-def test_apply_matches_reference(net):
+@pytest.fixture
+def net_relu():
+    n = LearnedPreconditioner(nSampleMax=4096, seed=11, relu=True)
+    yield n
+    n.close()
+
+
+@pytest.mark.parametrize("relu", [True, False])
+def test_apply_matches_reference(relu):
+    net = LearnedPreconditioner(nSampleMax=64, seed=11, relu=relu)
     rng = np.random.default_rng(1)
     p = lr.init_params(seed=3, out_gain=1.0).astype(np.float32)
+    if not relu:
+        P = lr.unpack(p)
+        P["W1"][:, 8:, :] = 0.0
+        for k in ("b1", "b2", "b3"):
+            P[k][:] = 0.0
+        p = lr.pack(P)
     net.set_params(p)
     nb = 7
     v = rng.normal(size=(nb, 8, 512)) * 10.0 ** rng.uniform(-3, 3, size=(nb, 1, 1))
     v[3] = 0.0  # an all-zero block maps to zero
     feat = rng.normal(size=(nb, 512, 8)).astype(np.float32)
     z = net.apply_blocks(v, feat)
-    zr = lr.apply(p, v, feat)
+    zr = lr.apply(p, v, feat, relu=relu)
+    net.close()
     assert np.all(z[3] == 0.0)
     for b in range(nb):
         if b != 3:
             assert relerr(z[b], zr[b]) < 1e-2, (b, relerr(z[b], zr[b]))
+    if not relu:  # the linear mode is linear in v
+        z2 = 2.0 * z[0]
+        assert relerr(z2, 2.0 * zr[0]) < 1e-2
 
 
-def test_gradient_matches_reference(net):
+@pytest.mark.parametrize("relu", [True, False])
+def test_gradient_matches_reference(relu):
+    net = LearnedPreconditioner(nSampleMax=64, seed=11, relu=relu)
     rng = np.random.default_rng(2)
     p = lr.init_params(seed=4, out_gain=1.0).astype(np.float32)
     net.set_params(p)
@@ -62,16 +83,21 @@ def test_gradient_matches_reference(net):
     tgt = rng.normal(size=(n, 512, 8)).astype(np.float32)
     net.set_samples(x0, tgt)
     loss, g = net.gradient(0, n)
-    lref, gref = lr.loss_and_grad(p, x0.reshape(n, 8, 8, 8, 16), tgt.reshape(n, 8, 8, 8, 8), bf=True)
+    net.close()
+    lref, gref = lr.loss_and_grad(p, x0.reshape(n, 8, 8, 8, 16), tgt.reshape(n, 8, 8, 8, 8), bf=True, relu=relu)
     assert abs(loss - lref) <= 1e-3 * lref
     o = 0
     for name, shp in lr.SHAPES:
         k = int(np.prod(shp))
-        assert relerr(g[o:o + k], gref[o:o + k]) < 3e-2, (name, relerr(g[o:o + k], gref[o:o + k]))
+        if np.linalg.norm(gref[o:o + k]) == 0.0:
+            assert np.all(g[o:o + k] == 0.0), name
+        else:
+            assert relerr(g[o:o + k], gref[o:o + k]) < 3e-2, (name, relerr(g[o:o + k], gref[o:o + k]))
         o += k
 
 
-def test_training_lowers_the_loss(net):
+def test_training_lowers_the_loss(net_relu):
+    net = net_relu
     # learnable target: a fixed random network of the same shape
     rng = np.random.default_rng(3)
     teacher = lr.init_params(seed=9, out_gain=1.0)
