@@ -41,6 +41,10 @@ struct LCtx {
   int *err = nullptr, *pick = nullptr;
   int adamStep = 0;
   int relu = 0;  // 0: linear in the Krylov vector; 1: ReLU network with features
+  // the network predicts targets divided by their RMS over the training set
+  // (fixed at the first training call); inference multiplies by it
+  double outScale = 1.0;
+  bool scaleSet = false;
   cudaStream_t st = nullptr;
 };
 
@@ -90,6 +94,7 @@ Weights weights() {
   W.b2 = Lc.p + kOffB2;
   W.b3 = Lc.p + kOffB3;
   W.relu = Lc.relu;
+  W.outScale = Lc.outScale;
   return W;
 }
 
@@ -171,16 +176,25 @@ __global__ void k_collect(const double *__restrict__ w, const double *__restrict
   }
 }
 
+// *out += sum of x^2 (FP32 partial sums per warp)
+__global__ void k_sumsq(const float *__restrict__ x, long n, float *out) {
+  float s = 0.f;
+  for (long q = blockIdx.x * (long)blockDim.x + threadIdx.x; q < n; q += (long)gridDim.x * blockDim.x)
+    s += x[q] * x[q];
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+  if ((threadIdx.x & 31) == 0) atomicAdd(out, s);
+}
+
 // one gradient evaluation over samples [s0, s0 + nS) of the training set:
 // Lc.g = d(loss)/d(params) with loss = mean of (out - tgt)^2 over the samples'
 // elements, and Lc.scal[0] = the sum of squares
-int gradient(long s0, int nS, cudaStream_t st) {
+int gradient(long s0, int nS, cudaStream_t st, float tgtMul) {
   const Weights W = weights();
   const int grid = std::min(nS, Lc.nSM);
   const float gscale = 2.0f / (4096.0f * (float)nS);
   CKL(cudaMemsetAsync(Lc.scal, 0, sizeof(float) * 80, st));
   const __nv_bfloat16 *in = Lc.in16 + (size_t)s0 * 512 * 16;
-  k_net_fwd_train<<<grid, kThreads, kSmemFwd, st>>>(W, in, Lc.tgt + (size_t)s0 * 512 * 8, nS, gscale, Lc.A1, Lc.A2,
+  k_net_fwd_train<<<grid, kThreads, kSmemFwd, st>>>(W, in, Lc.tgt + (size_t)s0 * 512 * 8, nS, gscale, tgtMul, Lc.A1, Lc.A2,
                                                     Lc.dY3, Lc.scal, Lc.scal + 1, Lc.err);
   CKL(cudaGetLastError());
   k_net_bwd_data<<<grid, kThreads, kSmemBwd, st>>>(W, Lc.dY3, Lc.A2, Lc.A1, nS, Lc.dY2, Lc.dY1, Lc.scal + 9,
@@ -287,6 +301,9 @@ int bx_learned_init(long long nSampleMax, unsigned long long seed) {
   Lc.collectPerPair = 0;
   Lc.rng.seed(seed);
   Lc.adamStep = 0;
+  Lc.relu = 0;
+  Lc.outScale = 1.0;
+  Lc.scaleSet = false;
   bool okAlloc = true;
   for (float **q : {&Lc.p, &Lc.m, &Lc.v, &Lc.g}) okAlloc = okAlloc && cudaMalloc(q, sizeof(float) * kNParam) == cudaSuccess;
   okAlloc = okAlloc && cudaMalloc(&Lc.w1, kW1Bytes) == cudaSuccess && cudaMalloc(&Lc.w2, kW2Bytes) == cudaSuccess &&
@@ -362,6 +379,8 @@ int bx_learned_set_params(const float *params, int n) {
   if (r) return r;
   if (!params || n != kNParam) return core_fail(BX_ERR_ARG, "expected %d parameters, got %d", kNParam, n);
   CKL(cudaMemcpyAsync(Lc.p, params, sizeof(float) * kNParam, cudaMemcpyHostToDevice, Lc.st));
+  Lc.outScale = 1.0;
+  Lc.scaleSet = false;
   if ((r = pack(Lc.st))) return r;
   CKL(cudaStreamSynchronize(Lc.st));
   return BX_OK;
@@ -412,7 +431,7 @@ int bx_learned_gradient(long long s0, int nS, float *grad, double *lossSum) {
   if (s0 < 0 || nS < 1 || nS > kBatchMax || s0 + nS > Lc.nSample)
     return core_fail(BX_ERR_ARG, "samples [%lld, %lld) outside the %ld stored (batch <= %d)", s0, s0 + nS, Lc.nSample,
                      kBatchMax);
-  if ((r = gradient(s0, nS, Lc.st))) return r;
+  if ((r = gradient(s0, nS, Lc.st, 1.0f))) return r;
   float l = 0;
   CKL(cudaMemcpyAsync(&l, Lc.scal, sizeof(float), cudaMemcpyDeviceToHost, Lc.st));
   if (grad) CKL(cudaMemcpyAsync(grad, Lc.g, sizeof(float) * kNParam, cudaMemcpyDeviceToHost, Lc.st));
@@ -427,6 +446,19 @@ int bx_learned_train(int nEpoch, int batch, double lr, double *lossFirst, double
   if (nEpoch < 1 || batch < 1 || batch > kBatchMax || !(lr > 0))
     return core_fail(BX_ERR_ARG, "nEpoch=%d batch=%d lr=%g", nEpoch, batch, lr);
   if (Lc.nSample < 1) return core_fail(BX_ERR_STATE, "no training samples collected");
+  if (!Lc.scaleSet) {
+    // RMS of the stored targets
+    CKL(cudaMemsetAsync(Lc.scal, 0, sizeof(float) * 2, Lc.st));
+    const long n = Lc.nSample * 512L * 8;
+    k_sumsq<<<4 * Lc.nSM, 256, 0, Lc.st>>>(Lc.tgt, n, Lc.scal);
+    CKL(cudaGetLastError());
+    float ss = 0;
+    CKL(cudaMemcpyAsync(&ss, Lc.scal, sizeof(float), cudaMemcpyDeviceToHost, Lc.st));
+    CKL(cudaStreamSynchronize(Lc.st));
+    const double rms = std::sqrt((double)ss / (double)n);
+    Lc.outScale = rms > 0 && std::isfinite(rms) ? rms : 1.0;
+    Lc.scaleSet = true;
+  }
   const long nB = (Lc.nSample + batch - 1) / batch;
   std::vector<long> order(nB);
   for (long i = 0; i < nB; i++) order[i] = i;
@@ -439,7 +471,7 @@ int bx_learned_train(int nEpoch, int batch, double lr, double *lossFirst, double
     for (long i = 0; i < nB; i++) {
       const long s0 = order[i] * batch;
       const int nS = (int)std::min<long>(batch, Lc.nSample - s0);
-      if ((r = gradient(s0, nS, Lc.st))) return r;
+      if ((r = gradient(s0, nS, Lc.st, (float)(1.0 / Lc.outScale)))) return r;
       Lc.adamStep++;
       const float b1 = 0.9f, b2 = 0.999f;
       const float c1 = 1.f - std::pow(b1, (float)Lc.adamStep), c2 = 1.f - std::pow(b2, (float)Lc.adamStep);

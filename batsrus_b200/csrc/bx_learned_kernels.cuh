@@ -103,7 +103,7 @@ __device__ __forceinline__ void setup(Smem &S, const Weights &W) {
 }
 
 // ---------------------------------------------------------------------------
-// inference: z[b] = s N(v[b]/s, feat[b]) for every block; v, z are FP64
+// inference: z[b] = s outScale N(v[b]/s, feat[b]) for every block; v, z are FP64
 // [block][var][cell] (512 cells), feat BF16 [block][cell][8]
 __global__ void __launch_bounds__(kThreads, 1)
     k_net_apply(Weights W, const double *__restrict__ v, double *__restrict__ z,
@@ -183,7 +183,7 @@ __global__ void __launch_bounds__(kThreads, 1)
     for_tiles<kN3>(tmem, [&](int, int, int cell, const float(&acc)[kN3]) {
       if (cell >= 0)
 #pragma unroll
-        for (int m = 0; m < kC3; m++) zb[m * 512 + cell] = s * (double)(acc[m] + S.bias[64 + m]);
+        for (int m = 0; m < kC3; m++) zb[m * 512 + cell] = s * W.outScale * (double)(acc[m] + S.bias[64 + m]);
     });
     tc::fence_before();
     __syncthreads();
@@ -196,13 +196,14 @@ __global__ void __launch_bounds__(kThreads, 1)
 
 // ---------------------------------------------------------------------------
 // training forward pass.  in16: BF16 [sample][cell][16] (input / s and the
-// features), tgt: FP32 [sample][cell][8] (target / s).  Stores A1, A2 (BF16
+// features), tgt: FP32 [sample][cell][8] (target / s, compared after
+// multiplication by tgtMul).  Stores A1, A2 (BF16
 // [sample][cell][32]) and dY3 = gscale (out - tgt) (BF16 [sample][cell][16],
 // channels 8..15 zero); accumulates sum (out - tgt)^2 into loss[0] and the
 // bias gradient of layer 3 into gb3[0..7].
 __global__ void __launch_bounds__(kThreads, 1)
     k_net_fwd_train(Weights W, const __nv_bfloat16 *__restrict__ in16, const float *__restrict__ tgt, int nSample,
-                    float gscale, __nv_bfloat16 *A1, __nv_bfloat16 *A2, __nv_bfloat16 *dY3, float *loss, float *gb3,
+                    float gscale, float tgtMul, __nv_bfloat16 *A1, __nv_bfloat16 *A2, __nv_bfloat16 *dY3, float *loss, float *gb3,
                     int *err) {
   extern __shared__ __align__(1024) unsigned char sm[];
   unsigned char *bufA = sm, *bufB = sm + kBuf32;
@@ -265,7 +266,7 @@ __global__ void __launch_bounds__(kThreads, 1)
         float g[kC3];
 #pragma unroll
         for (int m = 0; m < kC3; m++) {
-          const float d = acc[m] + S.bias[64 + m] - tg[cell * 8 + m];
+          const float d = acc[m] + S.bias[64 + m] - tgtMul * tg[cell * 8 + m];
           lossAcc += d * d;
           g[m] = gscale * d;
         }

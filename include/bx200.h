@@ -259,7 +259,9 @@ BX_API int bx_learned_set_samples(const float *in16, const float *tgt, long long
  * without an update; lossSum = sum of squared errors */
 BX_API int bx_learned_gradient(long long s0, int nS, float *grad, double *lossSum);
 /* Adam over the stored samples in mini-batches; mean squared error of the
- * first and the last epoch */
+ * first and the last epoch, in units of the targets divided by their RMS
+ * over the training set (fixed at the first call after bx_learned_init or
+ * bx_learned_set_params; the preconditioner multiplies its output by it) */
 BX_API int bx_learned_train(int nEpoch, int batch, double learningRate, double *lossFirst, double *lossLast);
 /* the preconditioner on host blocks: v, z [nBlock][8][512] (solver layout),
  * feat [nBlock][512][8] */
