@@ -45,6 +45,10 @@ struct LCtx {
   // (fixed at the first training call); inference multiplies by it
   double outScale = 1.0;
   bool scaleSet = false;
+  // identity part of the preconditioner: the least-squares coefficient of
+  // the targets on the inputs; the network learns the remainder
+  double identCoef = 0.0;
+  long nResidual = 0;  // samples whose targets hold the remainder
   cudaStream_t st = nullptr;
 };
 
@@ -95,6 +99,7 @@ Weights weights() {
   W.b3 = Lc.p + kOffB3;
   W.relu = Lc.relu;
   W.outScale = Lc.outScale;
+  W.identCoef = Lc.identCoef;
   return W;
 }
 
@@ -174,6 +179,34 @@ __global__ void k_collect(const double *__restrict__ w, const double *__restrict
       tgt[(n * 512 + c) * 8 + m] = isfinite(q) ? (float)q : 0.f;
     }
   }
+}
+
+// out[0] += sum tgt . x, out[1] += sum x . x over cells [0, nCell) (x = the
+// first 8 input channels)
+__global__ void k_ident_fit(const __nv_bfloat16 *__restrict__ in16, const float *__restrict__ tgt, long nCell,
+                            float *out) {
+  float a = 0.f, b = 0.f;
+  for (long q = blockIdx.x * (long)blockDim.x + threadIdx.x; q < nCell; q += (long)gridDim.x * blockDim.x)
+#pragma unroll
+    for (int m = 0; m < 8; m++) {
+      const float x = __bfloat162float(in16[q * 16 + m]);
+      a += tgt[q * 8 + m] * x;
+      b += x * x;
+    }
+  for (int o = 16; o > 0; o >>= 1) {
+    a += __shfl_xor_sync(0xffffffffu, a, o);
+    b += __shfl_xor_sync(0xffffffffu, b, o);
+  }
+  if ((threadIdx.x & 31) == 0) {
+    atomicAdd(out, a);
+    atomicAdd(out + 1, b);
+  }
+}
+// tgt -= c x over cells [c0, c1)
+__global__ void k_ident_sub(const __nv_bfloat16 *__restrict__ in16, float *tgt, long c0, long c1, float c) {
+  for (long q = c0 + blockIdx.x * (long)blockDim.x + threadIdx.x; q < c1; q += (long)gridDim.x * blockDim.x)
+#pragma unroll
+    for (int m = 0; m < 8; m++) tgt[q * 8 + m] -= c * __bfloat162float(in16[q * 16 + m]);
 }
 
 // *out += sum of x^2 (FP32 partial sums per warp)
@@ -304,6 +337,8 @@ int bx_learned_init(long long nSampleMax, unsigned long long seed) {
   Lc.relu = 0;
   Lc.outScale = 1.0;
   Lc.scaleSet = false;
+  Lc.identCoef = 0.0;
+  Lc.nResidual = 0;
   bool okAlloc = true;
   for (float **q : {&Lc.p, &Lc.m, &Lc.v, &Lc.g}) okAlloc = okAlloc && cudaMalloc(q, sizeof(float) * kNParam) == cudaSuccess;
   okAlloc = okAlloc && cudaMalloc(&Lc.w1, kW1Bytes) == cudaSuccess && cudaMalloc(&Lc.w2, kW2Bytes) == cudaSuccess &&
@@ -381,6 +416,8 @@ int bx_learned_set_params(const float *params, int n) {
   CKL(cudaMemcpyAsync(Lc.p, params, sizeof(float) * kNParam, cudaMemcpyHostToDevice, Lc.st));
   Lc.outScale = 1.0;
   Lc.scaleSet = false;
+  Lc.identCoef = 0.0;
+  Lc.nResidual = Lc.nSample;
   if ((r = pack(Lc.st))) return r;
   CKL(cudaStreamSynchronize(Lc.st));
   return BX_OK;
@@ -422,6 +459,7 @@ int bx_learned_set_samples(const float *in16, const float *tgt, long long nSampl
   CKL(cudaMemcpyAsync(Lc.tgt, tgt, sizeof(float) * 512 * 8 * (size_t)nSample, cudaMemcpyHostToDevice, Lc.st));
   CKL(cudaStreamSynchronize(Lc.st));
   Lc.nSample = nSample;
+  Lc.nResidual = nSample;  // targets taken as given
   return BX_OK;
 }
 
@@ -446,6 +484,22 @@ int bx_learned_train(int nEpoch, int batch, double lr, double *lossFirst, double
   if (nEpoch < 1 || batch < 1 || batch > kBatchMax || !(lr > 0))
     return core_fail(BX_ERR_ARG, "nEpoch=%d batch=%d lr=%g", nEpoch, batch, lr);
   if (Lc.nSample < 1) return core_fail(BX_ERR_STATE, "no training samples collected");
+  if (!Lc.scaleSet && Lc.nResidual < Lc.nSample) {
+    // identity coefficient a = <tgt, x> / <x, x> over the collected samples
+    CKL(cudaMemsetAsync(Lc.scal, 0, sizeof(float) * 2, Lc.st));
+    k_ident_fit<<<4 * Lc.nSM, 256, 0, Lc.st>>>(Lc.in16, Lc.tgt, Lc.nSample * 512L, Lc.scal);
+    CKL(cudaGetLastError());
+    float ab[2] = {0, 0};
+    CKL(cudaMemcpyAsync(ab, Lc.scal, sizeof(ab), cudaMemcpyDeviceToHost, Lc.st));
+    CKL(cudaStreamSynchronize(Lc.st));
+    Lc.identCoef = ab[1] > 0 ? (double)ab[0] / (double)ab[1] : 0.0;
+  }
+  if (Lc.nResidual < Lc.nSample) {  // targets -> remainder after the identity part
+    k_ident_sub<<<4 * Lc.nSM, 256, 0, Lc.st>>>(Lc.in16, Lc.tgt, Lc.nResidual * 512L, Lc.nSample * 512L,
+                                               (float)Lc.identCoef);
+    CKL(cudaGetLastError());
+    Lc.nResidual = Lc.nSample;
+  }
   if (!Lc.scaleSet) {
     // RMS of the stored targets
     CKL(cudaMemsetAsync(Lc.scal, 0, sizeof(float) * 2, Lc.st));

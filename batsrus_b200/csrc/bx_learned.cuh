@@ -138,7 +138,8 @@ struct Weights {
   const float *b1, *b2, *b3;  // biases (FP32)
   int relu;  // 1: ReLU between the layers and the cell features as input;
              // 0: linear in the Krylov vector (no activation, features off)
-  double outScale;  // output scale: the RMS of the training targets
+  double outScale;   // output scale: the RMS of the training targets
+  double identCoef;  // z = identCoef v + s outScale N(v / s)
 };
 
 }  // namespace learned

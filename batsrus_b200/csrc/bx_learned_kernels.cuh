@@ -1,8 +1,8 @@
 // bx_learned_kernels.cuh -- kernels of the learned preconditioner (layout and
 // MMA scheme in bx_learned.cuh).
 //
-//   k_net_apply     z = s N(v / s, features) per block (s = RMS of v over the
-//                   block), the preconditioner inside FGMRES
+//   k_net_apply     z = a v + s N(v / s, features) per block (s = RMS of v
+//                   over the block), the preconditioner inside FGMRES
 //   k_net_fwd_train forward pass of training samples: stores the layer
 //                   activations, the loss and dL/dY3
 //   k_net_bwd_data  dL/dY2 and dL/dY1 (transposed convolutions and the ReLU
@@ -103,7 +103,8 @@ __device__ __forceinline__ void setup(Smem &S, const Weights &W) {
 }
 
 // ---------------------------------------------------------------------------
-// inference: z[b] = s outScale N(v[b]/s, feat[b]) for every block; v, z are FP64
+// inference: z[b] = identCoef v[b] + s outScale N(v[b]/s, feat[b]) for every
+// block; v, z are FP64
 // [block][var][cell] (512 cells), feat BF16 [block][cell][8]
 __global__ void __launch_bounds__(kThreads, 1)
     k_net_apply(Weights W, const double *__restrict__ v, double *__restrict__ z,
@@ -183,7 +184,8 @@ __global__ void __launch_bounds__(kThreads, 1)
     for_tiles<kN3>(tmem, [&](int, int, int cell, const float(&acc)[kN3]) {
       if (cell >= 0)
 #pragma unroll
-        for (int m = 0; m < kC3; m++) zb[m * 512 + cell] = s * W.outScale * (double)(acc[m] + S.bias[64 + m]);
+        for (int m = 0; m < kC3; m++)
+          zb[m * 512 + cell] = W.identCoef * vb[m * 512 + cell] + s * W.outScale * (double)(acc[m] + S.bias[64 + m]);
     });
     tc::fence_before();
     __syncthreads();

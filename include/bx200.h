@@ -223,7 +223,9 @@ BX_API int bx_impl_norm_noalloc(const double *Impl_dev, int nCellBlock, int nBlo
  * 3-layer 3x3x3 convolutional network per 8^3 block (16 -> 32 -> 32 -> 8
  * channels, ReLU, zero padding at the block faces) maps the block of a
  * Krylov vector (scaled by its block RMS s) and the block's normalised state
- * to its correction, z = s N(v / s, U / Norm_V); BF16 operands, FP32
+ * to its correction, z = a v + s N(v / s, U / Norm_V), where a is the
+ * least-squares identity coefficient of the training targets and the network
+ * learns the remainder; BF16 operands, FP32
  * accumulation on the tensor cores.  Training pairs (v, z) are the Krylov
  * vectors and their BILU corrections of the BILU-preconditioned FGMRES
  * iterations of implicit steps (BILU is block-Jacobi, so z depends on the
