@@ -32,7 +32,7 @@ EXPORTS = (
     "bx_region_begin", "bx_region_end",
     "bx_implicit_init", "bx_advance_part_impl", "bx_impl_get_rhs", "bx_impl_matvec",
     "bx_impl_precond", "bx_impl_get_x",
-    "bx_learned_init", "bx_learned_set_activation", "bx_learned_finalize", "bx_learned_nparam", "bx_learned_set_params",
+    "bx_learned_init", "bx_learned_set_activation", "bx_learned_set_blend", "bx_learned_finalize", "bx_learned_nparam", "bx_learned_set_params",
     "bx_learned_get_params", "bx_learned_collect", "bx_learned_collect_probes", "bx_learned_num_samples", "bx_learned_set_samples",
     "bx_learned_gradient", "bx_learned_train", "bx_learned_apply_blocks",
     "bx_impl_norm_noalloc",
@@ -134,7 +134,7 @@ def load():
         "bx_impl_get_rhs": [dp, dp], "bx_impl_matvec": [dp, dp], "bx_impl_precond": [dp, dp],
         "bx_impl_get_x": [dp],
         "bx_learned_init": [ctypes.c_longlong, ctypes.c_ulonglong], "bx_learned_finalize": [],
-        "bx_learned_set_activation": [i],
+        "bx_learned_set_activation": [i], "bx_learned_set_blend": [d],
         "bx_learned_nparam": [ip], "bx_learned_set_params": [fp, i], "bx_learned_get_params": [fp, i],
         "bx_learned_collect": [i], "bx_learned_collect_probes": [i, i, ctypes.c_ulonglong], "bx_learned_num_samples": [ctypes.POINTER(ctypes.c_longlong)],
         "bx_learned_set_samples": [fp, fp, ctypes.c_longlong],

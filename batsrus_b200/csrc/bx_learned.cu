@@ -49,6 +49,7 @@ struct LCtx {
   // the targets on the inputs; the network learns the remainder
   double identCoef = 0.0;
   long nResidual = 0;  // samples whose targets hold the remainder
+  double blend = 1.0;  // weight of the learned remainder at inference
   cudaStream_t st = nullptr;
 };
 
@@ -98,7 +99,7 @@ Weights weights() {
   W.b2 = Lc.p + kOffB2;
   W.b3 = Lc.p + kOffB3;
   W.relu = Lc.relu;
-  W.outScale = Lc.outScale;
+  W.outScale = Lc.outScale * Lc.blend;
   W.identCoef = Lc.identCoef;
   return W;
 }
@@ -339,6 +340,7 @@ int bx_learned_init(long long nSampleMax, unsigned long long seed) {
   Lc.scaleSet = false;
   Lc.identCoef = 0.0;
   Lc.nResidual = 0;
+  Lc.blend = 1.0;
   bool okAlloc = true;
   for (float **q : {&Lc.p, &Lc.m, &Lc.v, &Lc.g}) okAlloc = okAlloc && cudaMalloc(q, sizeof(float) * kNParam) == cudaSuccess;
   okAlloc = okAlloc && cudaMalloc(&Lc.w1, kW1Bytes) == cudaSuccess && cudaMalloc(&Lc.w2, kW2Bytes) == cudaSuccess &&
@@ -392,6 +394,14 @@ int bx_learned_set_activation(int relu) {
   }
   if ((r = pack(Lc.st))) return r;
   CKL(cudaStreamSynchronize(Lc.st));
+  return BX_OK;
+}
+
+int bx_learned_set_blend(double blend) {
+  int r = require_ready();
+  if (r) return r;
+  if (!(blend >= 0.0 && blend <= 1.0)) return core_fail(BX_ERR_ARG, "blend=%g outside [0, 1]", blend);
+  Lc.blend = blend;
   return BX_OK;
 }
 

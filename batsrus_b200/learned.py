@@ -20,6 +20,10 @@ class LearnedPreconditioner:
         check(self.L.bx_learned_nparam(ctypes.byref(n)))
         self.nparam = n.value
 
+    def set_blend(self, blend):
+        """weight of the learned remainder at inference (0: identity part only)"""
+        check(self.L.bx_learned_set_blend(float(blend)))
+
     def close(self):
         self.L.bx_learned_finalize()
 

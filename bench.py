@@ -276,13 +276,15 @@ def train_learned(args, g, s, lrank, nPair=2000, blocksPerPair=16):
     net.collect_probes(nPair - nKrylov, blocksPerPair, seed=2025)
     x.close()
     t1 = time.perf_counter()
-    first, last = net.train(nEpoch=args.learned_epochs, batch=256, lr=2e-3)
+    first, last = net.train(nEpoch=args.learned_epochs, batch=256, lr=1e-3)
+    net.set_blend(args.learned_blend)
     t2 = time.perf_counter()
     return net, {"pairs": net.num_samples() // blocksPerPair, "krylov_pairs": nKrylov,
                  "probe_pairs": net.num_samples() // blocksPerPair - nKrylov, "block_samples": net.num_samples(),
                  "collect_steps": nStep, "collect_s": t1 - t0, "epochs": args.learned_epochs,
                  "train_s": t2 - t1, "mse_first_epoch": first, "mse_last_epoch": last,
-                 "seed_data": 2025, "seed_timed": 2024}
+                 "seed_data": 2025, "seed_timed": 2024, "mode": "linear, identity part + learned remainder",
+                 "blend": args.learned_blend}
 
 
 def run_amr(args, lrank):
@@ -407,6 +409,7 @@ def main():
     ap.add_argument("--precisions", default="fp64,fp32")
     ap.add_argument("--jfnk-precond", default="BILU,NONE,LEARNED", help="'' to skip the implicit workload")
     ap.add_argument("--learned-epochs", type=int, default=8)
+    ap.add_argument("--learned-blend", type=float, default=0.25)
     ap.add_argument("--amr", dest="amr", action="store_true", default=True)
     ap.add_argument("--no-amr", dest="amr", action="store_false")
     ap.add_argument("--amr-nroot", type=int, default=16, help="root blocks per dimension of the blast grid")

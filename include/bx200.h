@@ -240,6 +240,9 @@ BX_API int bx_learned_init(long long nSampleMax, unsigned long long seed);
  * per-block stencil that FGMRES sees as a linear preconditioner; relu = 1:
  * ReLU between the layers and the cell features as inputs */
 BX_API int bx_learned_set_activation(int relu);
+/* weight in [0, 1] of the learned remainder at inference, z = a v + blend s
+ * N(v / s) (default 1; 0 leaves the identity part alone) */
+BX_API int bx_learned_set_blend(double blend);
 BX_API int bx_learned_finalize(void);
 BX_API int bx_learned_nparam(int *nParam);
 BX_API int bx_learned_set_params(const float *params, int nParam);
