@@ -31,6 +31,23 @@ module bx200_interface
      integer(c_int):: iDevice
   end type bx_grid_desc
 
+  integer(c_int), parameter:: BX_PRECOND_NONE = 0, BX_PRECOND_BILU = 1, &
+       BX_PRECOND_LEARNED = 2
+
+  type, bind(C):: bx_implicit_params
+     real(c_double):: CflImpl, ImplCoeff
+     integer(c_int):: UseBdf2, nOrderImpl, TypeFluxImpl
+     real(c_double):: JacobianEps
+     integer(c_int):: nKrylovVector, MaxMatvec
+     real(c_double):: ErrorMax
+     integer(c_int):: TypePrecond
+  end type bx_implicit_params
+
+  type, bind(C):: bx_krylov_stats
+     integer(c_int):: nMatvec, iError
+     real(c_double):: Error, Dt, msStep, msPrecondSetup
+  end type bx_krylov_stats
+
   type, bind(C):: bx_scheme_params
      integer(c_int):: nOrder, nStage, TypeFlux, TypeLimiter
      real(c_double):: LimiterBeta, Cfl, Gamma
@@ -152,6 +169,33 @@ module bx200_interface
        real(c_double), value:: tSimulation
        integer(c_int), value:: nStep
      end function bx_set_time
+  end interface
+
+  interface
+     integer(c_int) function bx_get_neighbors(DiLevel_EB, jBlock_IEB) &
+          bind(C, name='bx_get_neighbors')
+       import:: c_int
+       integer(c_int), intent(out):: DiLevel_EB(*), jBlock_IEB(*)
+     end function bx_get_neighbors
+
+     integer(c_int) function bx_set_graph_steps(nStepPerGraph) &
+          bind(C, name='bx_set_graph_steps')
+       import:: c_int
+       integer(c_int), value:: nStepPerGraph
+     end function bx_set_graph_steps
+
+     integer(c_int) function bx_implicit_init(Params) &
+          bind(C, name='bx_implicit_init')
+       import:: c_int, bx_implicit_params
+       type(bx_implicit_params), intent(in):: Params
+     end function bx_implicit_init
+
+     integer(c_int) function bx_advance_part_impl(TimeSimulationLimit, Stats) &
+          bind(C, name='bx_advance_part_impl')
+       import:: c_int, c_double, bx_krylov_stats
+       real(c_double), value:: TimeSimulationLimit
+       type(bx_krylov_stats), intent(out):: Stats
+     end function bx_advance_part_impl
   end interface
 
 end module bx200_interface
