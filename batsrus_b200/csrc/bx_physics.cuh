@@ -48,6 +48,28 @@ __device__ __forceinline__ void limited_face(int lim, R beta, R q0, R q1, R q2, 
   right = q2 - dR;
 }
 
+// limited_face with the limiter fixed at compile time (same arithmetic)
+template <int LIM, typename R>
+__device__ __forceinline__ void limited_face_t(R beta, R q0, R q1, R q2, R q3, R &left, R &right) {
+  const R a = q1 - q0, b = q2 - q1, c = q3 - q2;
+  const R sab = sign25(a) + sign25(b);
+  const R sbc = sign25(b) + sign25(c);
+  R dL, dR;
+  if (LIM == kLimMinmod) {
+    dL = sab * fmin(fabs(a), fabs(b));
+    dR = sbc * fmin(fabs(b), fabs(c));
+  } else if (LIM == kLimMc) {
+    dL = sab * fmin(fmin(beta * fabs(a), beta * fabs(b)), R(0.5) * fabs(a + b));
+    dR = sbc * fmin(fmin(beta * fabs(b), beta * fabs(c)), R(0.5) * fabs(b + c));
+  } else {
+    const R cThird = R(1) / R(3);
+    dL = sab * fmin(fmin(beta * fabs(a), beta * fabs(b)), cThird * fabs(a + 2 * b));
+    dR = sbc * fmin(fmin(beta * fabs(b), beta * fabs(c)), cThird * fabs(2 * b + c));
+  }
+  left = q1 + dL;
+  right = q2 - dR;
+}
+
 // get_physical_flux -> get_mhd_flux -> get_magnetic_flux
 // (src/ModFaceFlux.f90:1166-1410, 1550-1617, 1619-1900)
 template <int D, typename R>

@@ -8,10 +8,10 @@
 
 namespace bx {
 
-template <int N, typename TileT, typename Real, typename OutT, int FLUX>
-static cudaError_t launch_one(const TmaMaps &maps, const StageArgs &a, int nSM, cudaStream_t st) {
+template <int N, typename TileT, typename Real, typename OutT, int FLUX, int LIM>
+static cudaError_t launch_lim(const TmaMaps &maps, const StageArgs &a, int nSM, cudaStream_t st) {
   using T = Tile3<N, TileT>;
-  auto k = stage3d_kernel<T, TileT, Real, OutT, FLUX>;
+  auto k = stage3d_kernel<T, TileT, Real, OutT, FLUX, LIM>;
   constexpr size_t sm = T::template smem_bytes<Real>();
   static bool attr = false;
   if (!attr) {
@@ -22,6 +22,17 @@ static cudaError_t launch_one(const TmaMaps &maps, const StageArgs &a, int nSM, 
   const int grid = a.nBlock < nSM ? a.nBlock : nSM;
   k<<<grid, T::NTHR, sm, st>>>(maps, a);
   return cudaGetLastError();
+}
+
+// the limiter is a template parameter of the kernel (no per-variable switch)
+template <int N, typename TileT, typename Real, typename OutT, int FLUX>
+static cudaError_t launch_one(const TmaMaps &maps, const StageArgs &a, int nSM, cudaStream_t st) {
+  switch (a.limiter) {
+    case kLimMinmod: return launch_lim<N, TileT, Real, OutT, FLUX, kLimMinmod>(maps, a, nSM, st);
+    case kLimMc: return launch_lim<N, TileT, Real, OutT, FLUX, kLimMc>(maps, a, nSM, st);
+    case kLimMc3: return launch_lim<N, TileT, Real, OutT, FLUX, kLimMc3>(maps, a, nSM, st);
+  }
+  return cudaErrorInvalidValue;
 }
 
 template <int N, typename TileT, typename Real, typename OutT>

@@ -166,7 +166,7 @@ __device__ __forceinline__ bool face_slots(Real (&L)[8], Real (&R)[8], Real gamm
 
 // one direction: faces (one per thread) then the cell sums.  rcFine / rcCoarse:
 // bit s set where side s borders a coarser / finer block
-template <class T, int D, int FLUX, typename TileT, typename Real>
+template <class T, int D, int FLUX, int LIM, typename TileT, typename Real>
 __device__ __forceinline__ void sweep3(const StageArgs &a, const BlockGeom &g, const TileT *tile, Real *fbuf,
                                        double (&chg)[8], double &divB, double &vdt, int &err, int rcFine,
                                        int rcCoarse, int b) {
@@ -193,7 +193,7 @@ __device__ __forceinline__ void sweep3(const StageArgs &a, const BlockGeom &g, c
       const Real q0 = (Real)tile[idx[0] + v * vs[0]], q1 = (Real)tile[idx[1] + v * vs[1]];
       const Real q2 = (Real)tile[idx[2] + v * vs[2]], q3 = (Real)tile[idx[3] + v * vs[3]];
       if (first) { L[v] = q1; R[v] = q2; }
-      else limited_face(a.limiter, beta, q0, q1, q2, q3, L[v], R[v]);
+      else limited_face_t<LIM>(beta, q0, q1, q2, q3, L[v], R[v]);
     }
     if (!face_slots<D, FLUX, Real>(L, R, (Real)a.gamma, (Real)a.invGm1, (Real)g.area[D], fbuf + t, T::NF)) err = 1;
     if (side >= 0 && ((rcCoarse >> side) & 1)) {
@@ -223,7 +223,7 @@ __device__ __forceinline__ void sweep3(const StageArgs &a, const BlockGeom &g, c
   __syncthreads();
 }
 
-template <class T, typename TileT, typename Real, typename OutT, int FLUX>
+template <class T, typename TileT, typename Real, typename OutT, int FLUX, int LIM>
 __global__ void __launch_bounds__(T::NTHR, 1)
     stage3d_kernel(const __grid_constant__ TmaMaps maps, const StageArgs a) {
   extern __shared__ __align__(128) unsigned char smem_raw[];
@@ -340,9 +340,9 @@ __global__ void __launch_bounds__(T::NTHR, 1)
     }
 
     double chg[8], divB = 0, vdt = 0;
-    sweep3<T, 0, FLUX, TileT, Real>(a, g, tile, fbuf, chg, divB, vdt, err, rcFine, rcCoarse, b);
-    sweep3<T, 1, FLUX, TileT, Real>(a, g, tile, fbuf, chg, divB, vdt, err, rcFine, rcCoarse, b);
-    sweep3<T, 2, FLUX, TileT, Real>(a, g, tile, fbuf, chg, divB, vdt, err, rcFine, rcCoarse, b);
+    sweep3<T, 0, FLUX, LIM, TileT, Real>(a, g, tile, fbuf, chg, divB, vdt, err, rcFine, rcCoarse, b);
+    sweep3<T, 1, FLUX, LIM, TileT, Real>(a, g, tile, fbuf, chg, divB, vdt, err, rcFine, rcCoarse, b);
+    sweep3<T, 2, FLUX, LIM, TileT, Real>(a, g, tile, fbuf, chg, divB, vdt, err, rcFine, rcCoarse, b);
 
     // update_state_normal / update_explicit for the thread's cell
     double dtmin = 1e300;

@@ -4,7 +4,7 @@ static two- or three-level blast grid: the neighbour bookkeeping
 for each flux (resolution-change ghost cells by injection / restriction,
 first-order faces next to coarser blocks, flux correction on the coarse
 side), conservation of mass and momentum through the flux correction, and
-the FP32-bulk mode within 1e-5 relative L1 of the FP64 oracle."""
+the FP32-bulk mode within 1e-6 relative L1 of the FP64 oracle."""
 import numpy as np
 import pytest
 
@@ -111,4 +111,4 @@ def test_amr_fp32_bulk_l1():
     a, b = x.get_state()[isl], o.get_state()[isl]
     l1 = np.abs(a - b).sum() / np.abs(b).sum()
     x.close()
-    assert l1 < 1e-5, l1
+    assert l1 < 1e-6, l1

@@ -200,7 +200,8 @@ def test_gpu_per_block_update_loop_equals_fused_stage():
 
 def test_gpu_fp32_bulk_error_vs_fp64():
     """FP32 reconstruction/fluxes with FP64 accumulation: relative L1 error
-    of the conserved state against the FP64 mode after 20 steps."""
+    of the conserved state against the FP64 mode after 20 steps, at most
+    1e-6 (measured: 5e-8 overall)."""
     g, s, st, _ = configs.orszag_tang_3d(nRoot=4)
     x = ExplicitSolver(g, s)
     x.set_state(st)
@@ -211,10 +212,14 @@ def test_gpu_fp32_bulk_error_vs_fp64():
     x.set_state(st)
     x.advance(21)
     got = x.get_state()[g.interior_slices()]
-    l1 = np.abs(got - ref).sum(axis=(0, 1, 2, 3)) / np.abs(ref).sum(axis=(0, 1, 2, 3))
-    # Bz starts at 0 and stays small: measure it against the field scale
-    l1[6] = np.abs(got[..., 6] - ref[..., 6]).sum() / np.abs(ref[..., 4:7]).sum()
-    assert l1.max() < 1e-5, l1
+    # per variable, the momentum and field components against the L1 norm of
+    # their vector (uz and Bz are small in this state); the bound is 1e-6
+    den = np.abs(ref).sum(axis=(0, 1, 2, 3))
+    den[1:4] = np.sqrt((ref[..., 1:4] ** 2).sum(-1)).sum()
+    den[4:7] = np.sqrt((ref[..., 4:7] ** 2).sum(-1)).sum()
+    l1 = np.abs(got - ref).sum(axis=(0, 1, 2, 3)) / den
+    assert l1.max() < 1e-6, l1
+    assert np.abs(got - ref).sum() / np.abs(ref).sum() < 1e-6
 
 
 def test_gpu_hlld_error_status_is_reported_not_aborted():
