@@ -36,6 +36,8 @@ EXPORTS = (
     "bx_learned_get_params", "bx_learned_collect", "bx_learned_collect_probes", "bx_learned_num_samples", "bx_learned_set_samples",
     "bx_learned_gradient", "bx_learned_train", "bx_learned_apply_blocks",
     "bx_impl_norm_noalloc",
+    "bx_heat_init", "bx_advance_semi_impl", "bx_heat_get_te", "bx_heat_get_rhs", "bx_heat_matvec",
+    "bx_heat_precond",
 )
 PRECOND = {"none": 0, "bilu": 1, "learned": 2}
 NOALLOC_MAX_BLOCK = 32768  # BX_NOALLOC_MAX_BLOCK
@@ -55,6 +57,19 @@ class KrylovStats(ctypes.Structure):
         ("nMatvec", ctypes.c_int), ("iError", ctypes.c_int), ("Error", ctypes.c_double),
         ("Dt", ctypes.c_double), ("msStep", ctypes.c_double), ("msPrecondSetup", ctypes.c_double),
     ]
+
+
+class HeatParamsC(ctypes.Structure):
+    _fields_ = [
+        ("HeatCondPar", ctypes.c_double), ("FractionFieldAligned", ctypes.c_double), ("Cv", ctypes.c_double),
+        ("Dt", ctypes.c_double), ("SemiImplCoeff", ctypes.c_double), ("nKrylovVector", ctypes.c_int),
+        ("MaxMatvec", ctypes.c_int), ("ErrorMax", ctypes.c_double), ("TypePrecond", ctypes.c_int),
+    ]
+
+
+def heat_params(p):
+    return HeatParamsC(p.heatCondPar, p.fieldAligned, p.cv, p.dt, p.semiImplCoeff, p.nKrylovVector,
+                       p.maxMatvec, p.errorMax, PRECOND[p.typePrecond.lower()])
 
 
 def implicit_params(p):
@@ -142,6 +157,9 @@ def load():
         "bx_learned_train": [i, i, d, dp, dp],
         "bx_learned_apply_blocks": [dp, fp, i, dp],
         "bx_impl_norm_noalloc": [p, i, i, p, dp],
+        "bx_heat_init": [ctypes.POINTER(HeatParamsC), dp, dp, ctypes.POINTER(ctypes.c_ubyte)],
+        "bx_advance_semi_impl": [ctypes.POINTER(KrylovStats)],
+        "bx_heat_get_te": [dp], "bx_heat_get_rhs": [dp], "bx_heat_matvec": [dp, dp], "bx_heat_precond": [dp, dp],
     }
     for name, args in sig.items():
         f = getattr(L, name)

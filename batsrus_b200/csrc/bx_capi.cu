@@ -247,6 +247,7 @@ int encode_maps(void *base, bool fp32, int N, int nBlock, TmaMaps &m) {
 
 void free_all() {
   impl_release();
+  heat_release();
   if (g.graph) { cudaGraphExecDestroy(g.graph); g.graph = nullptr; }
   for (double **p : {&g.A, &g.B, &g.Nx, &g.Ox, &g.stageAoS, &g.dtBlock, &g.scrSrc, &g.scrDt}) {
     if (*p) cudaFree(*p);
@@ -442,6 +443,14 @@ Core core() {
   c.A = g.A; c.nbr = g.nbr; c.order = g.order; c.geom = g.geom; c.ts = g.ts; c.dtBlock = g.dtBlock; c.nSlab = g.nSlab;
   c.st = g.st;
   return c;
+}
+CoreGrid core_grid() {
+  CoreGrid r;
+  for (int d = 0; d < 3; d++) { r.nRoot[d] = g.nRoot[d]; r.cmin[d] = g.cmin[d]; r.cmax[d] = g.cmax[d]; }
+  for (int s = 0; s < 6; s++) r.typeBc[s] = g.typeBc[s];
+  r.lev = g.lev.data();
+  r.ic = g.ic.data();
+  return r;
 }
 int core_fail(int code, const char *fmt, ...) {
   char buf[512];

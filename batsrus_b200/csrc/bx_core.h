@@ -23,10 +23,20 @@ struct Core {
 };
 
 Core core();
+// the block list of the grid given to bx_init (host copies)
+struct CoreGrid {
+  int nRoot[3];
+  double cmin[3], cmax[3];
+  int typeBc[6];
+  const int *lev, *ic;  // per block: level; ix, iy, iz
+};
+CoreGrid core_grid();
 int core_fail(int code, const char *fmt, ...);
 int core_encode_maps(void *base, bool fp32, TmaMaps &m);
 // release the implicit context (its buffers are sized for the current grid)
 void impl_release();
+// release the heat conduction context (bx_heat.cu)
+void heat_release();
 
 // learned preconditioner hooks (bx_learned.cu); vectors in the solver's
 // [block][var][cell] layout of 8^3 blocks

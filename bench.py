@@ -318,6 +318,69 @@ def run_amr(args, lrank):
     return out
 
 
+def run_heat(args, lrank):
+    """Semi-implicit field-aligned heat conduction on the dipole workload:
+    device time per solve (CUDA events around bx_advance_semi_impl, the
+    host-side Krylov control included) and matrix-vector products per solve,
+    for each preconditioner; every solve advances the temperature."""
+    from batsrus_b200.capi import BxError
+    from batsrus_b200.explicit import ExplicitSolver
+    from batsrus_b200.heat import HeatSolver
+    from batsrus_b200.heat_params import HeatParams, heat_dipole, global_to_blocks
+    from batsrus_b200.param import Scheme
+    nR = args.heat_nroot
+    n = 8 * nR
+    g, Te, b, used, dx = heat_dipole(nRoot=nR)
+    tb = lambda a: global_to_blocks(a.reshape((n, n, n) + a.shape[1:]), nR)
+    Te, b, used = tb(Te), tb(b), tb(used)
+    out = {"workload": "dipole_heat_conduction_%dcubed_kpar_kperp_1e6_gmres30_1e-6" % n, "cells": g.nCell,
+           "blocks": g.nBlock, "used_fraction": float(used.mean()), "solves": args.heat_steps,
+           "warmup": args.heat_warmup, "unit": "s/solve", "higher_is_better": False}
+    for prec in args.heat_precond.split(","):
+        x = ExplicitSolver(g, Scheme(), device=lrank)
+        h = HeatSolver(x, HeatParams(typePrecond=prec), Te, b, used)
+        try:
+            for _ in range(args.heat_warmup):
+                h.advance_semi_impl()
+            x.synchronize()
+            x.region_begin()
+            stats = [h.advance_semi_impl() for _ in range(args.heat_steps)]
+            ms = x.region_end()
+        except BxError as e:
+            out[prec.lower()] = {"failed": str(e)}
+            x.close()
+            continue
+        out[prec.lower()] = {"s_per_solve": ms * 1e-3 / args.heat_steps,
+                             "matvec_per_solve": float(np.mean([q["nMatvec"] for q in stats])),
+                             "matvec": [q["nMatvec"] for q in stats],
+                             "krylov_error": [q["Error"] for q in stats]}
+        x.close()
+    return out
+
+
+def cpu_baseline_heat(args, seconds=20.0):
+    """The oracle's heat conduction solve (BILU) on a 64^3 sample of the
+    dipole workload."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    from batsrus_b200.heat_params import HeatParams, heat_dipole
+    from oracle import HeatOracle
+    nR = 8
+    _, Te, b, used, dx = heat_dipole(nRoot=nR)
+    o = HeatOracle(8 * nR, dx, Te, b, used, HeatParams())
+    n, t0, nm = 0, time.perf_counter(), 0
+    while True:
+        r, _, m, _ = o.solve()
+        n, nm = n + 1, nm + m
+        el = time.perf_counter() - t0
+        if el > seconds or n >= 5:
+            break
+    o.close()
+    return {"value": el / n, "unit": "s/solve", "cores": os.cpu_count(), "kind": "port",
+            "matvec_per_solve": nm / n,
+            "sample": "oracle/ C++ restatement of advance_semi_impl with BILU, 64^3 (512 blocks) of the "
+                      "dipole workload, %d solves (residual on all threads, Krylov and ILU on one)" % n}
+
+
 def cpu_baseline_jfnk(args, seconds=20.0):
     """The oracle's implicit step (BILU) on a 32^3 sample of the JFNK workload."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
@@ -417,6 +480,10 @@ def main():
     ap.add_argument("--jfnk-nroot", type=int, default=16, help="16 -> 128^3 cells")
     ap.add_argument("--jfnk-steps", type=int, default=5)
     ap.add_argument("--jfnk-warmup", type=int, default=2)
+    ap.add_argument("--heat-precond", default="BILU,NONE", help="'' to skip the heat conduction workload")
+    ap.add_argument("--heat-nroot", type=int, default=32, help="32 -> 256^3 cells")
+    ap.add_argument("--heat-steps", type=int, default=3)
+    ap.add_argument("--heat-warmup", type=int, default=1)
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)
@@ -443,10 +510,14 @@ def main():
         line["jfnk"] = run_jfnk(args, 0)
     if args.amr:
         line["amr"] = run_amr(args, 0)
+    if args.heat_precond:
+        line["heat"] = run_heat(args, 0)
     if args.cpu and world == 1:
         line["cpu_baseline"] = cpu_baseline(args)
         if args.jfnk_precond:
             line["jfnk"]["cpu_baseline"] = cpu_baseline_jfnk(args)
+        if args.heat_precond:
+            line["heat"]["cpu_baseline"] = cpu_baseline_heat(args)
     print(json.dumps(line))
 
 

@@ -272,6 +272,47 @@ BX_API int bx_learned_train(int nEpoch, int batch, double learningRate, double *
  * feat [nBlock][512][8] */
 BX_API int bx_learned_apply_blocks(const double *v, const float *feat, int nBlock, double *z);
 
+/* ---- semi-implicit field-aligned heat conduction ---------------------------
+ * TypeSemiImplicit = 'parcond' of src/ModSemiImplicit.f90 on the grid given
+ * to bx_init (all blocks of 8^3 at one level, float outer boundaries): one
+ * linear solve per call, the electron temperature as the semi-implicit
+ * variable, HeatCoef = HeatCondPar Te^2.5 and the tensor
+ * FractionFieldAligned b b + (1 - FractionFieldAligned) I of
+ * get_heat_cond_tensor (src/ModHeatConduction.f90:923-1093). */
+typedef struct {
+  double HeatCondPar;          /* HeatCondPar of #HEATCONDUCTION (normalised) */
+  double FractionFieldAligned; /* kappa_perp / kappa_par = 1 - this */
+  double Cv;                   /* DconsDsemi: heat capacity per volume */
+  double Dt;                   /* time step of the solve */
+  double SemiImplCoeff;        /* #SEMICOEFF: 1 = backward Euler */
+  int nKrylovVector;           /* #SEMIKRYLOVSIZE: GMRES restart length, <= 64 */
+  int MaxMatvec;               /* #SEMIKRYLOV MaxMatvecSemi */
+  double ErrorMax;             /* #SEMIKRYLOV ErrorMaxSemi (relative, preconditioned) */
+  int TypePrecond;             /* #SEMIPRECOND: BX_PRECOND_BILU or BX_PRECOND_NONE */
+} bx_heat_params;
+
+/* init_mod_semi_impl (src/ModSemiImplicit.f90:110) and the state the solve
+ * reads: Te (nI, nJ, nK, nBlock), the unit field direction bhat
+ * (3, nI, nJ, nK, nBlock) and used (nI, nJ, nK, nBlock): 1 for cells of the
+ * solve, 0 for cells whose temperature is held (Used_GB of the body).
+ * Rejected on multi-level grids and periodic boundaries. */
+BX_API int bx_heat_init(const bx_heat_params *params, const double *Te, const double *bhat,
+                        const unsigned char *used);
+/* advance_semi_impl (src/ModSemiImplicit.f90:240): the right-hand side
+ * (get_semi_impl_rhs :469), the block ILU of get_semi_impl_jacobian (:984,
+ * add_jacobian_heat_cond src/ModHeatConduction.f90:1547), left-preconditioned
+ * GMRES with semi_impl_matvec (:578), then Te += x on used cells.  Returns
+ * BX_ERR_KRYLOV when MaxMatvec is reached before ErrorMax. */
+BX_API int bx_advance_semi_impl(bx_krylov_stats *stats);
+/* Te after the solves, (nI, nJ, nK, nBlock) */
+BX_API int bx_heat_get_te(double *Te);
+/* the linear system of the next solve, vectors (nI, nJ, nK, nBlock):
+ * b = V Res(Te) (get_heat_conduction_rhs :1434), y = A x
+ * (semi_impl_matvec), z = M^-1 r (semi_precond :783) */
+BX_API int bx_heat_get_rhs(double *b);
+BX_API int bx_heat_matvec(const double *x, double *y);
+BX_API int bx_heat_precond(const double *r, double *z);
+
 /* ---- measurement ----------------------------------------------------------
  * Kernel timing with CUDA events on the library's stream: when enabled, the
  * fused stage kernel launches are bracketed by events; the average duration

@@ -1615,3 +1615,325 @@ void ora_get_dtmax(void *h, double *cb, double *b) {
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------
+// Semi-implicit field-aligned heat conduction on a uniform Cartesian grid
+// (TypeSemiImplicit = 'parcond'): get_impl_heat_cond_state and
+// get_heat_cond_tensor (src/ModHeatConduction.f90:923-1432),
+// get_face_gradient (src/ModFaceGradient.f90:933-1140),
+// get_heat_conduction_rhs (:1434-1545), add_jacobian_heat_cond
+// (:1547-1638), semi_impl_matvec / get_semi_impl_jacobian
+// (src/ModSemiImplicit.f90:578-811).  Cells that are not used (inside the
+// excluded sphere) keep their temperature: their update is 0 and the linear
+// operator is V Cv/Dt there.  The linear solver of the absent share library
+// is restated as left-preconditioned restarted GMRES with modified
+// Gram-Schmidt; the preconditioner is ILU(0) of the 7-point Jacobian inside
+// each block (block Jacobi across blocks).
+namespace {
+
+struct Heat {
+  int n[3], nB;
+  double dx[3], V, area[3];
+  ora_heat_config c;
+  std::vector<double> Te, b3;       // Te per cell, unit field (3 per cell)
+  std::vector<unsigned char> used;
+  std::vector<double> HC;            // HeatCoef per cell
+  std::vector<double> diag, off;     // 7-point preconditioner matrix, block ILU diagonal
+  std::vector<double> dIlu;
+
+  long id(int i, int j, int k) const { return i + (long)n[0] * (j + (long)n[1] * k); }
+  long idc(int i, int j, int k) const {  // float boundary: clamp into the domain
+    i = std::min(std::max(i, 0), n[0] - 1);
+    j = std::min(std::max(j, 0), n[1] - 1);
+    k = std::min(std::max(k, 0), n[2] - 1);
+    return id(i, j, k);
+  }
+  long nCell() const { return (long)n[0] * n[1] * n[2]; }
+
+  void init(const int *nc, int nb, const double *d, const double *te, const double *bh, const unsigned char *u,
+            const ora_heat_config *cfg) {
+    for (int q = 0; q < 3; q++) { n[q] = nc[q]; dx[q] = d[q]; }
+    nB = nb;
+    c = *cfg;
+    V = dx[0] * dx[1] * dx[2];
+    for (int q = 0; q < 3; q++) area[q] = V / dx[q];
+    Te.assign(te, te + nCell());
+    b3.assign(bh, bh + 3 * nCell());
+    used.assign(u, u + nCell());
+    set_coef();
+  }
+
+  // HeatCoef = HeatCondPar Te^2.5 (get_heat_cond_tensor, Spitzer form)
+  void set_coef() {
+    HC.resize(nCell());
+    for (long q = 0; q < nCell(); q++) HC[q] = c.heatCondPar * std::pow(Te[q], 2.5);
+  }
+  double Bb(long q, int d1, int d2) const {
+    return c.fieldAligned * b3[3 * q + d1] * b3[3 * q + d2] + (1.0 - c.fieldAligned) * (d1 == d2 ? 1.0 : 0.0);
+  }
+  // HeatCond_DFDB(dir) of the face between cells L and R in dimension d
+  double heat_cond(long L, long R, int d, int dir) const {
+    const double BbF = 0.5 * (Bb(R, d, dir) + Bb(L, d, dir));
+    const double HeatCoef = 0.5 * (HC[R] + HC[L]);
+    return area[d] * HeatCoef * BbF;
+  }
+
+  // -HeatCond . FaceGrad at the face below cell (i,j,k) in dimension d, for
+  // the scalar S (values of out-of-domain cells are those of the clamped cell)
+  double face_flux(const std::vector<double> &S, int i, int j, int k, int d) const {
+    int iL = i, jL = j, kL = k;
+    if (d == 0) iL--; else if (d == 1) jL--; else kL--;
+    const long L = idc(iL, jL, kL), R = idc(i, j, k);
+    const double inv[3] = {1.0 / dx[0], 1.0 / dx[1], 1.0 / dx[2]};
+    double g[3];
+    g[d] = inv[d] * (S[R] - S[L]);
+    for (int e = 0; e < 3; e++) {
+      if (e == d) continue;
+      const double Ae = -0.25 * inv[e], Be = 0.0, Ce = 0.25 * inv[e];
+      int o[3] = {0, 0, 0};
+      o[e] = 1;
+      auto s2 = [&](int sh) {  // S(iD) + S(iU) shifted by sh along e
+        return S[idc(iL + sh * o[0], jL + sh * o[1], kL + sh * o[2])] +
+               S[idc(i + sh * o[0], j + sh * o[1], k + sh * o[2])];
+      };
+      g[e] = Ae * s2(-1) + Be * s2(0) + Ce * s2(1);
+    }
+    double f = 0;
+    for (int dir = 0; dir < 3; dir++) f = f + heat_cond(L, R, d, dir) * g[dir];
+    return -f;
+  }
+
+  // Res = -sum_d (F(i+1/2) - F(i-1/2)) / V per cell
+  void residual(const std::vector<double> &S, std::vector<double> &Res) const {
+    Res.assign(nCell(), 0.0);
+#pragma omp parallel for schedule(static)
+    for (int k = 0; k < n[2]; k++)
+      for (int j = 0; j < n[1]; j++)
+        for (int i = 0; i < n[0]; i++) {
+          double r = 0.0;
+          for (int d = 0; d < 3; d++) {
+            int o[3] = {0, 0, 0};
+            o[d] = 1;
+            r = r - (face_flux(S, i + o[0], j + o[1], k + o[2], d) - face_flux(S, i, j, k, d)) / V;
+          }
+          Res[id(i, j, k)] = r;
+        }
+  }
+
+  void rhs(double *b) const {
+    std::vector<double> Res;
+    residual(Te, Res);
+    for (long q = 0; q < nCell(); q++) b[q] = used[q] ? V * Res[q] : 0.0;
+  }
+
+  void matvec(const double *x, double *y) const {
+    std::vector<double> S(x, x + nCell()), Res;
+    for (long q = 0; q < nCell(); q++)
+      if (!used[q]) S[q] = 0.0;
+    residual(S, Res);
+    for (long q = 0; q < nCell(); q++)
+      y[q] = used[q] ? V * (S[q] * c.cv / c.dt - c.semiImplCoeff * Res[q]) : V * (x[q] * c.cv / c.dt);
+  }
+
+  // 7-point matrix of the preconditioner: off[7*q + s], s = 1..6 for
+  // -x, +x, -y, +y, -z, +z; diag in off[7*q]
+  void jacobian() {
+    off.assign(7 * nCell(), 0.0);
+    for (int k = 0; k < n[2]; k++)
+      for (int j = 0; j < n[1]; j++)
+        for (int i = 0; i < n[0]; i++) {
+          const long q = id(i, j, k);
+          off[7 * q] = V * c.cv / c.dt;
+          if (!used[q]) continue;
+          double sumJ = 0.0;
+          double J[7] = {0, 0, 0, 0, 0, 0, 0};
+          for (int d = 0; d < 3; d++) {
+            int o[3] = {0, 0, 0};
+            o[d] = 1;
+            const double Coeff = (1.0 / dx[d]) / V;
+            const double DiffLeft = Coeff * heat_cond(idc(i - o[0], j - o[1], k - o[2]), q, d, d);
+            const double DiffRight = Coeff * heat_cond(q, idc(i + o[0], j + o[1], k + o[2]), d, d);
+            sumJ = sumJ - (DiffLeft + DiffRight);
+            J[1 + 2 * d] = DiffLeft;
+            J[2 + 2 * d] = DiffRight;
+          }
+          const double Coeff = -c.semiImplCoeff * V;
+          off[7 * q] = Coeff * sumJ + V * c.cv / c.dt;
+          for (int s = 1; s < 7; s++) off[7 * q + s] = Coeff * J[s];
+        }
+  }
+  // neighbour of q on side s inside the same nB^3 block and used, else -1
+  long nb_in_block(int i, int j, int k, int s) const {
+    int c3[3] = {i, j, k};
+    const int d = (s - 1) / 2, hi = (s - 1) % 2;
+    c3[d] += hi ? 1 : -1;
+    if (c3[d] < 0 || c3[d] >= n[d]) return -1;
+    if (c3[d] / nB != (d == 0 ? i : d == 1 ? j : k) / nB) return -1;
+    const long m = id(c3[0], c3[1], c3[2]);
+    return used[m] ? m : -1;
+  }
+  void bilu_factor() {
+    jacobian();
+    dIlu.assign(nCell(), 0.0);
+    // natural order inside each block: lower neighbours are -x, -y, -z
+    for (int k = 0; k < n[2]; k++)
+      for (int j = 0; j < n[1]; j++)
+        for (int i = 0; i < n[0]; i++) {
+          const long q = id(i, j, k);
+          double d = off[7 * q];
+          if (used[q])
+            for (int s = 1; s <= 5; s += 2) {
+              const long m = nb_in_block(i, j, k, s);
+              if (m < 0) continue;
+              d = d - off[7 * q + s] * off[7 * m + s + 1] / dIlu[m];
+            }
+          dIlu[q] = d;
+        }
+  }
+  void precond(const double *r, double *z) const {
+    if (c.typePrecond == 0) {
+      std::copy(r, r + nCell(), z);
+      return;
+    }
+    std::vector<double> y(nCell());
+    for (int k = 0; k < n[2]; k++)
+      for (int j = 0; j < n[1]; j++)
+        for (int i = 0; i < n[0]; i++) {
+          const long q = id(i, j, k);
+          double s = r[q];
+          if (used[q])
+            for (int t = 1; t <= 5; t += 2) {
+              const long m = nb_in_block(i, j, k, t);
+              if (m >= 0) s = s - off[7 * q + t] * y[m];
+            }
+          y[q] = s / dIlu[q];
+        }
+    for (int k = n[2] - 1; k >= 0; k--)
+      for (int j = n[1] - 1; j >= 0; j--)
+        for (int i = n[0] - 1; i >= 0; i--) {
+          const long q = id(i, j, k);
+          double s = 0.0;
+          if (used[q])
+            for (int t = 2; t <= 6; t += 2) {
+              const long m = nb_in_block(i, j, k, t);
+              if (m >= 0) s = s + off[7 * q + t] * z[m];
+            }
+          z[q] = y[q] - s / dIlu[q];
+        }
+  }
+
+  static double dot(const std::vector<double> &a, const std::vector<double> &b) {
+    double s = 0.0;
+    for (size_t q = 0; q < a.size(); q++) s += a[q] * b[q];
+    return s;
+  }
+
+  // left-preconditioned restarted GMRES(m), modified Gram-Schmidt, x0 = 0;
+  // converged when |M^-1 (b - A x)| <= errorMax |M^-1 b|
+  int solve(double *xOut, int &nMatvec, double &errRel) {
+    if (c.typePrecond == 1) bilu_factor();
+    const long N = nCell();
+    const int m = c.nKrylovVector;
+    std::vector<double> b(N), x(N, 0.0), r(N), w(N), tmp(N);
+    rhs(b.data());
+    precond(b.data(), r.data());
+    const double beta0 = std::sqrt(dot(r, r));
+    nMatvec = 0;
+    errRel = 0.0;
+    if (beta0 == 0.0) { std::copy(x.begin(), x.end(), xOut); return 0; }
+    double beta = beta0;
+    std::vector<std::vector<double>> Vb(m + 1, std::vector<double>(N));
+    std::vector<double> H((m + 1) * m), cs(m), sn(m), g(m + 1), y(m);
+    while (true) {
+      for (long q = 0; q < N; q++) Vb[0][q] = r[q] / beta;
+      std::fill(g.begin(), g.end(), 0.0);
+      g[0] = beta;
+      int kdone = 0;
+      bool conv = false;
+      for (int k = 0; k < m; k++) {
+        matvec(Vb[k].data(), tmp.data());
+        nMatvec++;
+        precond(tmp.data(), w.data());
+        for (int q = 0; q <= k; q++) {
+          const double h = dot(w, Vb[q]);
+          H[q * m + k] = h;
+          for (long p = 0; p < N; p++) w[p] = w[p] - h * Vb[q][p];
+        }
+        const double hn = std::sqrt(dot(w, w));
+        H[(k + 1) * m + k] = hn;
+        if (hn != 0.0)
+          for (long p = 0; p < N; p++) Vb[k + 1][p] = w[p] / hn;
+        for (int q = 0; q < k; q++) {
+          const double t0 = H[q * m + k], t1 = H[(q + 1) * m + k];
+          H[q * m + k] = cs[q] * t0 + sn[q] * t1;
+          H[(q + 1) * m + k] = -sn[q] * t0 + cs[q] * t1;
+        }
+        const double a0 = H[k * m + k], b0 = H[(k + 1) * m + k];
+        const double rr = std::sqrt(a0 * a0 + b0 * b0);
+        cs[k] = a0 / rr;
+        sn[k] = b0 / rr;
+        H[k * m + k] = rr;
+        H[(k + 1) * m + k] = 0.0;
+        g[k + 1] = -sn[k] * g[k];
+        g[k] = cs[k] * g[k];
+        kdone = k + 1;
+        errRel = std::fabs(g[k + 1]) / beta0;
+        if (errRel <= c.errorMax || nMatvec >= c.maxMatvec || hn == 0.0) {
+          conv = errRel <= c.errorMax || hn == 0.0;
+          break;
+        }
+      }
+      for (int q = kdone - 1; q >= 0; q--) {
+        double s = g[q];
+        for (int p = q + 1; p < kdone; p++) s -= H[q * m + p] * y[p];
+        y[q] = s / H[q * m + q];
+      }
+      for (int q = 0; q < kdone; q++)
+        for (long p = 0; p < N; p++) x[p] = x[p] + y[q] * Vb[q][p];
+      if (conv) break;
+      if (nMatvec >= c.maxMatvec) { std::copy(x.begin(), x.end(), xOut); return 1; }
+      matvec(x.data(), tmp.data());
+      for (long p = 0; p < N; p++) tmp[p] = b[p] - tmp[p];
+      precond(tmp.data(), r.data());
+      beta = std::sqrt(dot(r, r));
+      errRel = beta / beta0;
+      if (errRel <= c.errorMax) break;
+    }
+    for (long q = 0; q < N; q++)
+      if (used[q]) Te[q] = Te[q] + x[q];
+    set_coef();
+    std::copy(x.begin(), x.end(), xOut);
+    return 0;
+  }
+};
+
+}  // namespace
+
+extern "C" {
+void *ora_heat_new(const int nCell[3], int nB, const double dx[3], const double *Te, const double *bhat,
+                   const unsigned char *used, const ora_heat_config *cfg) {
+  Heat *h = new Heat();
+  h->init(nCell, nB, dx, Te, bhat, used, cfg);
+  return h;
+}
+void ora_heat_free(void *h) { delete (Heat *)h; }
+void ora_heat_rhs(void *h, double *b) { ((Heat *)h)->rhs(b); }
+void ora_heat_matvec(void *h, const double *x, double *y) { ((Heat *)h)->matvec(x, y); }
+void ora_heat_precond(void *h, const double *r, double *z) {
+  Heat *H = (Heat *)h;
+  if (H->dIlu.empty() && H->c.typePrecond == 1) H->bilu_factor();
+  H->precond(r, z);
+}
+int ora_heat_solve(void *h, double *x, int *nMatvec, double *errorRel) {
+  int nm = 0;
+  double e = 0;
+  const int r = ((Heat *)h)->solve(x, nm, e);
+  if (nMatvec) *nMatvec = nm;
+  if (errorRel) *errorRel = e;
+  return r;
+}
+void ora_heat_get_te(void *h, double *Te) {
+  Heat *H = (Heat *)h;
+  std::copy(H->Te.begin(), H->Te.end(), Te);
+}
+}  // extern "C"

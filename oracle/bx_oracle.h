@@ -105,6 +105,36 @@ void ora_impl_precond(void *h, const double *r, double *z);
 /* the solution x of the last Krylov solve */
 void ora_impl_get_x(void *h, double *x);
 
+/* ---- semi-implicit field-aligned heat conduction (ModSemiImplicit with
+ * TypeSemiImplicit = 'parcond', ModHeatConduction) on a uniform Cartesian
+ * grid of nCell[0] x nCell[1] x nCell[2] cells (x fastest), float outer
+ * boundaries, blocks of nB^3 cells for the block ILU */
+typedef struct {
+  double heatCondPar;     /* HeatCondPar: HeatCoef = HeatCondPar * Te^2.5 */
+  double fieldAligned;    /* FractionFieldAligned: Bb = f bb + (1 - f) I */
+  double cv;              /* DconsDsemi (energy per volume per unit Te) */
+  double dt;              /* Dt of the semi-implicit step */
+  double semiImplCoeff;   /* SemiImplCoeff (1 = backward Euler) */
+  int nKrylovVector;      /* GMRES restart length */
+  int maxMatvec;
+  double errorMax;        /* relative tolerance on the preconditioned residual */
+  int typePrecond;        /* 0 none, 1 block ILU(0) */
+} ora_heat_config;
+
+void *ora_heat_new(const int nCell[3], int nB, const double dx[3], const double *Te, const double *bhat,
+                   const unsigned char *used, const ora_heat_config *cfg);
+void ora_heat_free(void *h);
+/* b = V Res(Te) on used cells, 0 elsewhere */
+void ora_heat_rhs(void *h, double *b);
+/* y = A x of the semi-implicit step */
+void ora_heat_matvec(void *h, const double *x, double *y);
+/* z = M^-1 r (block ILU(0) of the 7-point Jacobian) */
+void ora_heat_precond(void *h, const double *r, double *z);
+/* solve A x = b by left-preconditioned restarted GMRES from x = 0, update
+ * Te += x on used cells; returns 0 when converged */
+int ora_heat_solve(void *h, double *x, int *nMatvec, double *errorRel);
+void ora_heat_get_te(void *h, double *Te);
+
 #ifdef __cplusplus
 }
 #endif

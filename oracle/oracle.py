@@ -268,3 +268,69 @@ Oracle.impl_rhs = _oracle_impl_rhs
 Oracle.impl_matvec = _oracle_impl_matvec
 Oracle.impl_precond = _oracle_impl_precond
 Oracle.impl_x = _oracle_impl_x
+
+
+class HeatConfig(ctypes.Structure):
+    _fields_ = [("heatCondPar", ctypes.c_double), ("fieldAligned", ctypes.c_double), ("cv", ctypes.c_double),
+                ("dt", ctypes.c_double), ("semiImplCoeff", ctypes.c_double), ("nKrylovVector", ctypes.c_int),
+                ("maxMatvec", ctypes.c_int), ("errorMax", ctypes.c_double), ("typePrecond", ctypes.c_int)]
+
+
+class HeatOracle:
+    """Semi-implicit heat conduction restated on the CPU (global arrays,
+    x fastest; blocks of 8^3 for the block ILU)."""
+
+    def __init__(self, n, dx, Te, bhat, used, params):
+        L = lib()
+        for name, res in (("ora_heat_new", ctypes.c_void_p), ("ora_heat_solve", ctypes.c_int)):
+            getattr(L, name).restype = res
+        L.ora_heat_new.argtypes = [ctypes.POINTER(ctypes.c_int), ctypes.c_int, ctypes.POINTER(ctypes.c_double),
+                                   ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.POINTER(HeatConfig)]
+        for name in ("ora_heat_free", "ora_heat_rhs", "ora_heat_matvec", "ora_heat_precond", "ora_heat_solve",
+                     "ora_heat_get_te"):
+            getattr(L, name).argtypes = None
+        c = HeatConfig(params.heatCondPar, params.fieldAligned, params.cv, params.dt, params.semiImplCoeff,
+                       params.nKrylovVector, params.maxMatvec, params.errorMax,
+                       {"none": 0, "bilu": 1}[params.typePrecond.lower()])
+        self.N = n ** 3
+        self._keep = [np.ascontiguousarray(Te, dtype=np.float64), np.ascontiguousarray(bhat, dtype=np.float64),
+                      np.ascontiguousarray(used, dtype=np.uint8)]
+        nc = (ctypes.c_int * 3)(n, n, n)
+        d3 = (ctypes.c_double * 3)(dx, dx, dx)
+        self.h = ctypes.c_void_p(L.ora_heat_new(nc, 8, d3, self._keep[0].ctypes.data, self._keep[1].ctypes.data,
+                                                self._keep[2].ctypes.data, ctypes.byref(c)))
+        self.L = L
+
+    def close(self):
+        self.L.ora_heat_free(self.h)
+
+    def _vec(self):
+        return np.zeros(self.N)
+
+    def rhs(self):
+        b = self._vec()
+        self.L.ora_heat_rhs(self.h, b.ctypes.data_as(ctypes.c_void_p))
+        return b
+
+    def matvec(self, x):
+        x = np.ascontiguousarray(x, dtype=np.float64)
+        y = self._vec()
+        self.L.ora_heat_matvec(self.h, x.ctypes.data_as(ctypes.c_void_p), y.ctypes.data_as(ctypes.c_void_p))
+        return y
+
+    def precond(self, r):
+        r = np.ascontiguousarray(r, dtype=np.float64)
+        z = self._vec()
+        self.L.ora_heat_precond(self.h, r.ctypes.data_as(ctypes.c_void_p), z.ctypes.data_as(ctypes.c_void_p))
+        return z
+
+    def solve(self):
+        x = self._vec()
+        nm, err = ctypes.c_int(0), ctypes.c_double(0)
+        r = self.L.ora_heat_solve(self.h, x.ctypes.data_as(ctypes.c_void_p), ctypes.byref(nm), ctypes.byref(err))
+        return r, x, nm.value, err.value
+
+    def te(self):
+        t = self._vec()
+        self.L.ora_heat_get_te(self.h, t.ctypes.data_as(ctypes.c_void_p))
+        return t

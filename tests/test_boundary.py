@@ -30,7 +30,9 @@ def test_library_exports_every_declared_symbol():
 
 def test_structs_match_header_field_order():
     txt = open(HEADER).read()
-    for cname, pystruct in (("bx_grid_desc", capi.GridDesc), ("bx_scheme_params", capi.SchemeParams)):
+    for cname, pystruct in (("bx_grid_desc", capi.GridDesc), ("bx_scheme_params", capi.SchemeParams),
+                            ("bx_implicit_params", capi.ImplicitParamsC), ("bx_krylov_stats", capi.KrylovStats),
+                            ("bx_heat_params", capi.HeatParamsC)):
         body = re.search(r"typedef struct \{([^{}]*)\}\s*%s;" % cname, txt).group(1)
         body = re.sub(r"/\*.*?\*/", "", body, flags=re.S)
         names = []
