@@ -14,10 +14,10 @@
 //                  :1434-1545); mode RHS writes b = V Res(Te), mode MATVEC
 //                  y = V (x Cv/Dt - SemiImplCoeff Res(x)) (semi_impl_matvec,
 //                  src/ModSemiImplicit.f90:578-762)
-//   k_heat_jac     7-point matrix of the preconditioner (add_jacobian_heat_cond
-//                  :1547-1638, get_semi_impl_jacobian)
-//   k_heat_ilu_*   ILU(0) of that matrix inside each block, factor and solve
-//                  by i+j+k wavefronts
+//   k_heat_factor  7-point matrix of the preconditioner (add_jacobian_heat_cond
+//                  :1547-1638, get_semi_impl_jacobian) and its ILU(0) inside
+//                  each block
+//   k_heat_ilu     the triangular solves of that ILU(0)
 // The linear solver is left-preconditioned restarted GMRES with modified
 // Gram-Schmidt and deterministic FP64 inner products; the Givens rotations
 // run on the host.  Cells that are not used keep their temperature.
@@ -29,18 +29,19 @@
 #include <vector>
 
 #include "bx_core.h"
+#include "bx_krylov.cuh"
 
 using namespace bx;
 
 namespace {
 
 constexpr int kNB = 8, kNC = 512, kTile = 10;
-constexpr int kRedBlk = 592, kRedThr = 256;
 
 struct HeatArgs {
   int n[3];        // global cells per dimension
   int nbx[3];      // blocks per dimension
   double dx[3], V, area[3];
+  double invDx[3], gA[3], gC[3];  // 1/dx and the transverse gradient weights -0.25/dx, +0.25/dx
   double f, cv, dt, sic;
   const int *blkAt;   // [nbx[2]][nbx[1]][nbx[0]] -> block index
   const int *blkXYZ;  // per block: its block coordinates
@@ -56,7 +57,14 @@ struct HeatCtx {
   unsigned char *used = nullptr;
   int *blkAt = nullptr, *blkXYZ = nullptr;
   double *b = nullptr, *x = nullptr, *w = nullptr, *t = nullptr, *r = nullptr, *V = nullptr;
-  double *off = nullptr, *dIlu = nullptr;
+  double *K = nullptr;  // face conduction tensor [block][dim][dir][face]
+  double4 *coef = nullptr;   // forward and backward sweep coefficients, interleaved by 32 blocks
+  double *yI = nullptr;      // forward-sweep scratch, interleaved
+  unsigned *usedM = nullptr; // used masks [group][cell]
+  int nGroup = 0;            // groups of 32 blocks
+  long nIl = 0;              // cells of the interleaved arrays (nGroup x 32 x 512)
+  struct WaveTable *wtab = nullptr;
+  unsigned *cnt = nullptr;
   double *partial = nullptr, *scal = nullptr;
   int nMatvec = 0;
   double errRel = 0;
@@ -94,216 +102,377 @@ __global__ void k_heat_coef(const double *__restrict__ Te, double *HC, double he
 
 enum { kModeRhs = 0, kModeMatvec = 1 };
 
-// face flux below tile cell (i,j,k) (tile coordinates 0..9) in dimension d
-__device__ __forceinline__ double face_flux(const HeatArgs &a, const double *S, const double *hc, const double *b3,
-                                            int i, int j, int k, int d) {
-  auto T = [](int ii, int jj, int kk) { return ii + kTile * (jj + kTile * kk); };
-  int iL = i, jL = j, kL = k;
-  if (d == 0) iL--; else if (d == 1) jL--; else kL--;
-  const int L = T(iL, jL, kL), R = T(i, j, k);
-  const double inv[3] = {1.0 / a.dx[0], 1.0 / a.dx[1], 1.0 / a.dx[2]};
+// faces of one dimension of a block: 9 along the dimension x 8 x 8, x
+// fastest (so that neighbouring threads read neighbouring tile cells):
+// r = a + 9 (j + 8 k) for x faces, i + 8 (a + 9 k) for y faces and
+// i + 8 (j + 8 a) for z faces, with a the face index along the dimension
+// (the right cell at tile coordinate a + 1)
+constexpr int kFacesDim = (kNB + 1) * kNB * kNB;
+constexpr int kKBlock = 9 * kFacesDim;  // doubles of K per block
+
+// tile coordinates (1..9 along d) of the right cell of face r of dimension D
+template <int D>
+__device__ __forceinline__ void face_cell(int r, int &i, int &j, int &k) {
+  if (D == 0) { i = r % 9 + 1; j = (r / 9) % 8 + 1; k = r / 72 + 1; }
+  else if (D == 1) { i = r % 8 + 1; j = (r / 8) % 9 + 1; k = r / 72 + 1; }
+  else { i = r % 8 + 1; j = (r / 8) % 8 + 1; k = r / 64 + 1; }
+}
+// r of the lower face of block cell (i, j, k) (0..7) in dimension d
+__device__ __forceinline__ int lower_face(int d, int i, int j, int k) {
+  return d == 0 ? i + 9 * (j + 8 * k) : (d == 1 ? i + 8 * (j + 9 * k) : i + 8 * (j + 8 * k));
+}
+
+__device__ __forceinline__ int tidx(int i, int j, int k) { return i + kTile * (j + kTile * k); }
+
+// HeatCond_DFDB(dir, face, D) = Area HeatCoef_f BbF(D, dir) with the face
+// averages of HeatCoef and of the tensor (get_impl_heat_cond_state,
+// src/ModHeatConduction.f90:1096-1432)
+template <int D>
+__device__ __forceinline__ void face_tensor(const HeatArgs &a, const double *hc, const double *b3, int r, double *Kd) {
+  int i, j, k;
+  face_cell<D>(r, i, j, k);
+  const int R = tidx(i, j, k), L = tidx(i - (D == 0), j - (D == 1), k - (D == 2));
+#pragma unroll
+  for (int dir = 0; dir < 3; dir++) {
+    const double BbF = 0.5 * (bb(b3 + 3 * R, a.f, D, dir) + bb(b3 + 3 * L, a.f, D, dir));
+    const double HeatCoef = 0.5 * (hc[R] + hc[L]);
+    Kd[dir * kFacesDim + r] = a.area[D] * HeatCoef * BbF;
+  }
+}
+
+// -HeatCond . FaceGrad of face r of dimension D (get_face_gradient,
+// src/ModFaceGradient.f90:933-1140, uniform Cartesian grid; the flux of
+// get_heat_conduction_rhs, src/ModHeatConduction.f90:1466-1477)
+template <int D>
+__device__ __forceinline__ double face_flux(const HeatArgs &a, const double *S, const double *__restrict__ Kd, int r) {
+  int i, j, k;
+  face_cell<D>(r, i, j, k);
+  const int R = tidx(i, j, k), L = tidx(i - (D == 0), j - (D == 1), k - (D == 2));
   double g[3];
-  g[d] = inv[d] * (S[R] - S[L]);
+  g[D] = a.invDx[D] * (S[R] - S[L]);
 #pragma unroll
   for (int e = 0; e < 3; e++) {
-    if (e == d) continue;
-    const double Ae = -0.25 * inv[e], Be = 0.0, Ce = 0.25 * inv[e];
+    if (e == D) continue;
+    const double Be = 0.0;
     const int o = e == 0 ? 1 : (e == 1 ? kTile : kTile * kTile);
     const double sm = S[L - o] + S[R - o], s0 = S[L] + S[R], sp = S[L + o] + S[R + o];
-    g[e] = Ae * sm + Be * s0 + Ce * sp;
+    g[e] = a.gA[e] * sm + Be * s0 + a.gC[e] * sp;
   }
   double f = 0.0;
 #pragma unroll
-  for (int dir = 0; dir < 3; dir++) {
-    const double BbF = 0.5 * (bb(b3 + 3 * R, a.f, d, dir) + bb(b3 + 3 * L, a.f, d, dir));
-    const double HeatCoef = 0.5 * (hc[R] + hc[L]);
-    f = f + a.area[d] * HeatCoef * BbF * g[dir];
-  }
+  for (int dir = 0; dir < 3; dir++) f = f + Kd[dir * kFacesDim + r] * g[dir];
   return -f;
 }
 
-// one CTA per block, 512 threads
-__global__ void __launch_bounds__(512) k_heat_apply(HeatArgs a, const double *__restrict__ S,
-                                                    const double *__restrict__ HC, const double *__restrict__ B3,
-                                                    const unsigned char *__restrict__ used, double *out, int mode) {
-  __shared__ double sS[kTile * kTile * kTile], sH[kTile * kTile * kTile], sB[3 * kTile * kTile * kTile];
-  const int blk = blockIdx.x;
+// the tile of the block and its ghost layer, clamped into the domain
+template <typename F>
+__device__ __forceinline__ void for_tile(const HeatArgs &a, int blk, F &&fn) {
   const int bx = a.blkXYZ[3 * blk], by = a.blkXYZ[3 * blk + 1], bz = a.blkXYZ[3 * blk + 2];
   for (int q = threadIdx.x; q < kTile * kTile * kTile; q += blockDim.x) {
     const int ti = q % kTile, tj = (q / kTile) % kTile, tk = q / (kTile * kTile);
-    const long g = gidx(a, bx * kNB + ti - 1, by * kNB + tj - 1, bz * kNB + tk - 1);
-    double s = S[g];
-    if (mode == kModeMatvec && !used[g]) s = 0.0;  // unused cells keep their value
-    sS[q] = s;
+    fn(q, gidx(a, bx * kNB + ti - 1, by * kNB + tj - 1, bz * kNB + tk - 1));
+  }
+}
+
+// K of every face of a block (one CTA per block); run whenever HeatCoef changes
+__global__ void __launch_bounds__(512) k_heat_faces(HeatArgs a, const double *__restrict__ HC,
+                                                    const double *__restrict__ B3, double *K) {
+  __shared__ double sH[kTile * kTile * kTile], sB[3 * kTile * kTile * kTile];
+  const int blk = blockIdx.x;
+  for_tile(a, blk, [&](int q, long g) {
     sH[q] = HC[g];
     sB[3 * q] = B3[3 * g];
     sB[3 * q + 1] = B3[3 * g + 1];
     sB[3 * q + 2] = B3[3 * g + 2];
+  });
+  __syncthreads();
+  double *Kb = K + (size_t)blk * kKBlock;
+  for (int f = threadIdx.x; f < 3 * kFacesDim; f += blockDim.x) {
+    const int d = f / kFacesDim, r = f % kFacesDim;  // d is warp-uniform (576 = 18 x 32)
+    if (d == 0) face_tensor<0>(a, sH, sB, r, Kb);
+    else if (d == 1) face_tensor<1>(a, sH, sB, r, Kb + 3 * kFacesDim);
+    else face_tensor<2>(a, sH, sB, r, Kb + 6 * kFacesDim);
+  }
+}
+
+// one CTA per block, 512 threads: the 10^3 tile of the scalar, each of the
+// block's 3 x 576 face fluxes once, then per cell Res = -sum (F+ - F-)/V
+// (get_heat_conduction_rhs :1434-1545); mode RHS writes b = V Res(Te), mode
+// MATVEC y = V (x Cv/Dt - SemiImplCoeff Res(x)) (semi_impl_matvec,
+// src/ModSemiImplicit.f90:578-762)
+__global__ void __launch_bounds__(512) k_heat_apply(HeatArgs a, const double *__restrict__ S,
+                                                    const double *__restrict__ K,
+                                                    const unsigned char *__restrict__ used, double *out, int mode) {
+  __shared__ double sS[kTile * kTile * kTile], sF[3 * kFacesDim];
+  const int blk = blockIdx.x;
+  for_tile(a, blk, [&](int q, long g) {
+    double s = S[g];
+    if (mode == kModeMatvec && !used[g]) s = 0.0;  // unused cells keep their value
+    sS[q] = s;
+  });
+  __syncthreads();
+  const double *Kb = K + (size_t)blk * kKBlock;
+  for (int f = threadIdx.x; f < 3 * kFacesDim; f += blockDim.x) {
+    const int d = f / kFacesDim, r = f % kFacesDim;
+    double v;
+    if (d == 0) v = face_flux<0>(a, sS, Kb, r);
+    else if (d == 1) v = face_flux<1>(a, sS, Kb + 3 * kFacesDim, r);
+    else v = face_flux<2>(a, sS, Kb + 6 * kFacesDim, r);
+    sF[f] = v;
   }
   __syncthreads();
   const int c = threadIdx.x;
-  const int i = c % kNB + 1, j = (c / kNB) % kNB + 1, k = c / (kNB * kNB) + 1;
+  const int i = c % kNB, j = (c / kNB) % kNB, k = c / (kNB * kNB);
+  const double *F0 = sF, *F1 = sF + kFacesDim, *F2 = sF + 2 * kFacesDim;
+  const int r0 = lower_face(0, i, j, k), r1 = lower_face(1, i, j, k), r2 = lower_face(2, i, j, k);
   double res = 0.0;
-#pragma unroll
-  for (int d = 0; d < 3; d++) {
-    const double fUp = face_flux(a, sS, sH, sB, i + (d == 0), j + (d == 1), k + (d == 2), d);
-    const double fDn = face_flux(a, sS, sH, sB, i, j, k, d);
-    res = res - (fUp - fDn) / a.V;
-  }
+  res = res - (F0[r0 + 1] - F0[r0]) / a.V;
+  res = res - (F1[r1 + kNB] - F1[r1]) / a.V;
+  res = res - (F2[r2 + kNB * kNB] - F2[r2]) / a.V;
   const long q = (long)blk * kNC + c;
-  const int tc = i + kTile * (j + kTile * k);
+  const int tc = tidx(i + 1, j + 1, k + 1);
   if (mode == kModeRhs) out[q] = used[q] ? a.V * res : 0.0;
   else out[q] = used[q] ? a.V * (sS[tc] * a.cv / a.dt - a.sic * res) : a.V * (S[q] * a.cv / a.dt);
 }
 
-// 7-point preconditioner matrix off[7q + s]: s = 0 diagonal, 1..6 the -x,
-// +x, -y, +y, -z, +z neighbours
-__global__ void k_heat_jac(HeatArgs a, const double *__restrict__ HC, const double *__restrict__ B3,
-                           const unsigned char *__restrict__ used, double *off, long nCell) {
-  for (long q = blockIdx.x * (long)blockDim.x + threadIdx.x; q < nCell; q += (long)gridDim.x * blockDim.x) {
-    const int blk = (int)(q / kNC), c = (int)(q % kNC);
-    const int bx = a.blkXYZ[3 * blk], by = a.blkXYZ[3 * blk + 1], bz = a.blkXYZ[3 * blk + 2];
-    const int gi = bx * kNB + c % kNB, gj = by * kNB + (c / kNB) % kNB, gk = bz * kNB + c / (kNB * kNB);
-    double *o = off + 7 * q;
-    o[0] = a.V * a.cv / a.dt;
-    for (int s = 1; s < 7; s++) o[s] = 0.0;
-    if (!used[q]) continue;
-    double sumJ = 0.0, J[7] = {0, 0, 0, 0, 0, 0, 0};
-    for (int d = 0; d < 3; d++) {
-      const int e0 = d == 0, e1 = d == 1, e2 = d == 2;
-      const long Lq = gidx(a, gi - e0, gj - e1, gk - e2), Rq = gidx(a, gi + e0, gj + e1, gk + e2);
-      const double Coeff = (1.0 / a.dx[d]) / a.V;
-      const double hl = a.area[d] * (0.5 * (HC[q] + HC[Lq])) *
-                        (0.5 * (bb(B3 + 3 * q, a.f, d, d) + bb(B3 + 3 * Lq, a.f, d, d)));
-      const double hr = a.area[d] * (0.5 * (HC[Rq] + HC[q])) *
-                        (0.5 * (bb(B3 + 3 * Rq, a.f, d, d) + bb(B3 + 3 * q, a.f, d, d)));
-      const double DiffLeft = Coeff * hl, DiffRight = Coeff * hr;
-      sumJ = sumJ - (DiffLeft + DiffRight);
-      J[1 + 2 * d] = DiffLeft;
-      J[2 + 2 * d] = DiffRight;
-    }
-    const double Coeff = -a.sic * a.V;
-    o[0] = Coeff * sumJ + a.V * a.cv / a.dt;
-    for (int s = 1; s < 7; s++) o[s] = Coeff * J[s];
-  }
+// ---- block ILU(0) of the 7-point preconditioner matrix --------------------
+// The matrix (add_jacobian_heat_cond, src/ModHeatConduction.f90:1547-1638;
+// get_semi_impl_jacobian, src/ModSemiImplicit.f90:984) is symmetric: the
+// coupling of a cell to its +d neighbour and that of the neighbour to the
+// cell are the same product of the same face values.  One double4 per cell
+// holds the couplings to the -x, -y, -z neighbours and the diagonal, which
+// the factorisation replaces by the ILU(0) pivot.  Couplings across block
+// faces and to unused cells are dropped (BILU on 8^3 blocks).  The sweeps
+// multiply by the pivot reciprocals that the factorisation stores.  Per
+// cell the factorisation writes two double4: {lower x, lower y, lower z,
+// 1/pivot} for the forward sweep and {upper x, upper y, upper z, 1/pivot}
+// (the lower couplings of the +x, +y, +z neighbours) for the backward one.
+//
+// The factorisation runs one warp per block over the 22 planes i+j+k =
+// const (every lower neighbour lies on the previous plane).  The sweeps run
+// one lane per block in the natural order of the oracle, 32 blocks per warp
+// with no barrier between cells: the coefficients and the used flags are
+// stored interleaved by groups of 32 blocks (a warp's load of one cell of its
+// 32 blocks is one contiguous 1 KB), and the right-hand side and the result
+// pass through a shared-memory transpose one 8x8 plane at a time.
+constexpr int kWarpsPerCta = 2, kNumWave = 3 * (kNB - 1) + 1;
+
+struct WaveTable {
+  short cell[kNC];       // cells ordered by i+j+k, then natural order
+  short off[kNumWave + 1];
+};
+
+struct IluSmem {
+  double cf[kWarpsPerCta][4][kNC];  // lower x, lower y, lower z, pivot (reciprocal)
+  double y[kWarpsPerCta][kNC];
+  unsigned char u[kWarpsPerCta][kNC];
+  WaveTable wt;
+};
+
+__device__ __forceinline__ void load_wave_table(const WaveTable *g, WaveTable &s) {
+  const short *src = reinterpret_cast<const short *>(g);
+  short *dst = reinterpret_cast<short *>(&s);
+  for (int q = threadIdx.x; q < (int)(sizeof(WaveTable) / sizeof(short)); q += blockDim.x) dst[q] = src[q];
 }
 
-// block neighbour of cell c on side s (1..6) if inside the block and used
-__device__ __forceinline__ int nb_in(int c, int s, const unsigned char *usedB) {
-  const int i = c % kNB, j = (c / kNB) % kNB, k = c / (kNB * kNB);
-  const int d = (s - 1) / 2, hi = (s - 1) % 2;
-  int i3[3] = {i, j, k};
-  i3[d] += hi ? 1 : -1;
-  if (i3[d] < 0 || i3[d] >= kNB) return -1;
-  const int m = i3[0] + kNB * (i3[1] + kNB * i3[2]);
-  return usedB[m] ? m : -1;
-}
-
-// ILU(0) diagonal, one CTA per block, wavefronts i+j+k = w
-__global__ void __launch_bounds__(512) k_heat_ilu_factor(const double *__restrict__ off,
-                                                         const unsigned char *__restrict__ used, double *dIlu) {
-  __shared__ double sd[kNC];
-  const int blk = blockIdx.x, c = threadIdx.x;
-  const long q = (long)blk * kNC + c;
-  const int w0 = c % kNB + (c / kNB) % kNB + c / (kNB * kNB);
-  const unsigned char *u = used + (long)blk * kNC;
-  for (int w = 0; w <= 3 * (kNB - 1); w++) {
-    if (w0 == w) {
-      double d = off[7 * q];
-      if (u[c])
-        for (int s = 1; s <= 5; s += 2) {
-          const int m = nb_in(c, s, u);
-          if (m < 0) continue;
-          d = d - off[7 * q + s] * off[7 * ((long)blk * kNC + m) + s + 1] / sd[m];
-        }
-      sd[c] = d;
-    }
-    __syncthreads();
-  }
-  dIlu[q] = sd[c];
-}
-
-__global__ void __launch_bounds__(512) k_heat_ilu_solve(const double *__restrict__ off,
-                                                        const unsigned char *__restrict__ used,
-                                                        const double *__restrict__ dIlu, const double *__restrict__ r,
-                                                        double *z) {
-  __shared__ double sy[kNC], sz[kNC];
-  const int blk = blockIdx.x, c = threadIdx.x;
-  const long q = (long)blk * kNC + c;
-  const int w0 = c % kNB + (c / kNB) % kNB + c / (kNB * kNB);
-  const unsigned char *u = used + (long)blk * kNC;
-  const double dq = dIlu[q], rq = r[q];
-  for (int w = 0; w <= 3 * (kNB - 1); w++) {
-    if (w0 == w) {
-      double s = rq;
-      if (u[c])
-        for (int t = 1; t <= 5; t += 2) {
-          const int m = nb_in(c, t, u);
-          if (m >= 0) s = s - off[7 * q + t] * sy[m];
-        }
-      sy[c] = s / dq;
-    }
-    __syncthreads();
-  }
-  for (int w = 3 * (kNB - 1); w >= 0; w--) {
-    if (w0 == w) {
-      double s = 0.0;
-      if (u[c])
-        for (int t = 2; t <= 6; t += 2) {
-          const int m = nb_in(c, t, u);
-          if (m >= 0) s = s + off[7 * q + t] * sz[m];
-        }
-      sz[c] = sy[c] - s / dq;
-    }
-    __syncthreads();
-  }
-  z[q] = sz[c];
-}
-
-// ---- vector kernels (deterministic reductions) --------------------------
-__device__ __forceinline__ double blk_sum(double v) {
-  __shared__ double sh[32];
-  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-  if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = v;
+// matrix + factorisation; coef[q] = {lower x, lower y, lower z, 1 / pivot}
+__global__ void __launch_bounds__(32 * kWarpsPerCta) k_heat_factor(HeatArgs a, const double *__restrict__ K,
+                                                                 const unsigned char *__restrict__ used,
+                                                                 const WaveTable *__restrict__ wtab, double4 *coefL,
+                                                                 double4 *coefU, int nBlock) {
+  __shared__ IluSmem sm;
+  load_wave_table(wtab, sm.wt);
   __syncthreads();
-  double r = 0;
-  if (threadIdx.x == 0)
-    for (int w = 0; w < (int)(blockDim.x >> 5); w++) r += sh[w];
-  __syncthreads();
-  return r;
-}
-// w -= h vq (h from device memory), then partial sums of w . vn (or w . w)
-__global__ void k_h_axpy_dot(double *__restrict__ w, const double *__restrict__ vq, const double *hq,
-                             const double *__restrict__ vn, long n, double *partial) {
-  const double h = hq ? *hq : 0.0;
-  double s = 0;
-  for (long q = blockIdx.x * (long)blockDim.x + threadIdx.x; q < n; q += (long)gridDim.x * blockDim.x) {
-    double x = w[q];
-    if (vq) { x = x - h * vq[q]; w[q] = x; }
-    s += vn ? x * vn[q] : x * x;
+  const int wp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int blk = blockIdx.x * kWarpsPerCta + wp;
+  if (blk >= nBlock) return;
+  double *lx = sm.cf[wp][0], *ly = sm.cf[wp][1], *lz = sm.cf[wp][2], *dp = sm.cf[wp][3];
+  unsigned char *u = sm.u[wp];
+  const double Cs = -a.sic * a.V, D0 = a.V * a.cv / a.dt;
+  const double *Kb = K + (size_t)blk * kKBlock;
+  for (int c = lane; c < kNC; c += 32) {
+    const long q = (long)blk * kNC + c;
+    const int i = c & 7, j = (c >> 3) & 7, k = c >> 6;
+    u[c] = used[q];
+    double lo[3] = {0.0, 0.0, 0.0}, dg = D0;
+    if (used[q]) {
+      double sumJ = 0.0;
+      const int r[3] = {lower_face(0, i, j, k), lower_face(1, i, j, k), lower_face(2, i, j, k)};
+#pragma unroll
+      for (int d = 0; d < 3; d++) {
+        const double *Kdd = Kb + (3 * d + d) * kFacesDim;  // HeatCond_DFDB(d, face, d)
+        const double Coeff = (1.0 / a.dx[d]) / a.V;
+        const double DiffLeft = Coeff * Kdd[r[d]], DiffRight = Coeff * Kdd[r[d] + (d == 0 ? 1 : (d == 1 ? kNB : kNB * kNB))];
+        sumJ = sumJ - (DiffLeft + DiffRight);
+        lo[d] = Cs * DiffLeft;
+      }
+      dg = Cs * sumJ + D0;
+    }
+    lx[c] = lo[0];
+    ly[c] = lo[1];
+    lz[c] = lo[2];
+    dp[c] = dg;
   }
-  s = blk_sum(s);
-  if (threadIdx.x == 0) partial[blockIdx.x] = s;
-}
-__global__ void k_h_sum(const double *partial, int nPart, double *out) {
-  double s = 0;
-  for (int i = threadIdx.x; i < nPart; i += blockDim.x) s += partial[i];
-  s = blk_sum(s);
-  if (threadIdx.x == 0) *out = s;
-}
-// y = x / sqrt(*a2) (invert) or y = x * (*a)
-__global__ void k_h_scale(double *y, const double *x, const double *a, int invert, long n) {
-  const double s = invert ? 1.0 / sqrt(*a) : *a;
-  for (long q = blockIdx.x * (long)blockDim.x + threadIdx.x; q < n; q += (long)gridDim.x * blockDim.x) y[q] = s * x[q];
-}
-// x += sum_q y_q V_q
-__global__ void k_h_update(double *x, const double *Vb, const double *y, int k, long n) {
-  for (long q = blockIdx.x * (long)blockDim.x + threadIdx.x; q < n; q += (long)gridDim.x * blockDim.x) {
-    double s = x[q];
-    for (int m = 0; m < k; m++) s = s + y[m] * Vb[(size_t)m * n + q];
-    x[q] = s;
+  __syncwarp();
+  // pivots: d_c = A_cc - sum over used lower neighbours m of A_cm A_mc / d_m
+  for (int w = 0; w < kNumWave; w++) {
+    for (int e = sm.wt.off[w] + lane; e < sm.wt.off[w + 1]; e += 32) {
+      const int c = sm.wt.cell[e];
+      double d = dp[c];
+      if (u[c]) {
+        if ((c & 7) && u[c - 1]) d = d - lx[c] * lx[c] / dp[c - 1];
+        if (((c >> 3) & 7) && u[c - 8]) d = d - ly[c] * ly[c] / dp[c - 8];
+        if ((c >> 6) && u[c - 64]) d = d - lz[c] * lz[c] / dp[c - 64];
+      }
+      dp[c] = d;
+    }
+    __syncwarp();
+  }
+  for (int c = lane; c < kNC; c += 32) {
+    const double iv = 1.0 / dp[c];
+    const long o = ((long)(blk >> 5) * kNC + c) * 32 + (blk & 31);  // interleaved by 32 blocks
+    coefL[o] = make_double4(lx[c], ly[c], lz[c], iv);
+    coefU[o] = make_double4((c & 7) != 7 ? lx[c + 1] : 0.0, ((c >> 3) & 7) != 7 ? ly[c + 8] : 0.0,
+                            (c >> 6) != 7 ? lz[c + 64] : 0.0, iv);
   }
 }
+
+// z = M^-1 r: forward sweep (L + D) y = r, backward (D + U) z = D y, one
+// lane per block (blocks 32 g .. 32 g + 31 in warp g); usedM[g][c] has bit
+// l set when cell c of block 32 g + l is used; yI is the interleaved
+// scratch of the forward result.  Plane buffers hold element (p, l) at
+// p * 32 + (l ^ (p & 31)): rows and columns are free of bank conflicts.
+__device__ __forceinline__ int swz(int p, int l) { return p * 32 + (l ^ (p & 31)); }
+
+struct IluRow {
+  double4 v[kNB];
+  unsigned m[kNB];
+};
+
+// the coefficients and used masks of one x row (8 cells from c0), loaded
+// ahead of the row's arithmetic
+__device__ __forceinline__ void load_row(IluRow &row, const double4 *__restrict__ cf, const unsigned *__restrict__ um,
+                                         int c0) {
+#pragma unroll
+  for (int i = 0; i < kNB; i++) {
+    const double2 *p2 = reinterpret_cast<const double2 *>(cf + (long)(c0 + i) * 32);
+    const double2 lo = __ldg(p2), hi = __ldg(p2 + 1);
+    row.v[i] = make_double4(lo.x, lo.y, hi.x, hi.y);
+    row.m[i] = __ldg(um + c0 + i);
+  }
+}
+
+__global__ void __launch_bounds__(32) k_heat_ilu(const double4 *__restrict__ coefL, const double4 *__restrict__ coefU,
+                                                 const unsigned *__restrict__ usedM, const double *__restrict__ r,
+                                                 double *__restrict__ yI, double *__restrict__ z, int nBlock) {
+  __shared__ double plane[2][64 * 32];
+  const int g = blockIdx.x, lane = threadIdx.x;
+  const long gb = (long)g * 32;  // first block of the group
+  const unsigned *um = usedM + (long)g * kNC;
+  const double4 *cL = coefL + (long)g * kNC * 32 + lane, *cU = coefU + (long)g * kNC * 32 + lane;
+  double *yl = yI + (long)g * kNC * 32 + lane;
+  double *cur = plane[0], *prv = plane[1];
+  IluRow A, B;
+  // forward, rows (j, k) in natural order
+  load_row(A, cL, um, 0);
+  for (int k = 0; k < kNB; k++) {
+#pragma unroll 8
+    for (int bb = 0; bb < 32; bb++) {
+      const long blk = gb + bb;
+      double v0 = 0.0, v1 = 0.0;
+      if (blk < nBlock) {
+        v0 = __ldg(r + blk * kNC + 64 * k + lane);
+        v1 = __ldg(r + blk * kNC + 64 * k + 32 + lane);
+      }
+      cur[swz(lane, bb)] = v0;
+      cur[swz(32 + lane, bb)] = v1;
+    }
+    __syncwarp();
+    unsigned mDn[kNB] = {0, 0, 0, 0, 0, 0, 0, 0};  // masks of the row below
+    for (int j = 0; j < kNB; j++) {
+      const int c0 = 64 * k + 8 * j;
+      if (c0 + 8 < kNC) load_row(B, cL, um, c0 + 8);
+      double ym = 0.0;  // y of the cell at x - 1
+#pragma unroll
+      for (int i = 0; i < kNB; i++) {
+        const int p = i + 8 * j, c = c0 + i;
+        const unsigned m = A.m[i];
+        const double4 v = A.v[i];
+        double s = cur[swz(p, lane)];
+        if ((m >> lane) & 1) {
+          if (i > 0 && ((A.m[i - 1] >> lane) & 1)) s = s - v.x * ym;
+          if (j > 0 && ((mDn[i] >> lane) & 1)) s = s - v.y * cur[swz(p - 8, lane)];
+          if (k > 0 && ((__ldg(um + c - 64) >> lane) & 1)) s = s - v.z * prv[swz(p, lane)];
+        }
+        const double y = s * v.w;
+        cur[swz(p, lane)] = y;
+        yl[(long)c * 32] = y;
+        ym = y;
+      }
+#pragma unroll
+      for (int i = 0; i < kNB; i++) mDn[i] = A.m[i];
+      A = B;
+    }
+    __syncwarp();
+    double *t = cur; cur = prv; prv = t;
+  }
+  __syncwarp();
+  // backward, rows in reverse order
+  load_row(A, cU, um, kNC - 8);
+  for (int k = kNB - 1; k >= 0; k--) {
+    unsigned mUp[kNB] = {0, 0, 0, 0, 0, 0, 0, 0};  // masks of the row above
+    for (int j = kNB - 1; j >= 0; j--) {
+      const int c0 = 64 * k + 8 * j;
+      if (c0 > 0) load_row(B, cU, um, c0 - 8);
+      double yv[kNB];
+#pragma unroll
+      for (int i = 0; i < kNB; i++) yv[i] = yl[(long)(c0 + i) * 32];
+      double zp = 0.0;  // z of the cell at x + 1
+#pragma unroll
+      for (int i = kNB - 1; i >= 0; i--) {
+        const int p = i + 8 * j, c = c0 + i;
+        const unsigned m = A.m[i];
+        const double4 v = A.v[i];
+        double s = 0.0;
+        if ((m >> lane) & 1) {
+          if (i < kNB - 1 && ((A.m[i + 1] >> lane) & 1)) s = s + v.x * zp;
+          if (j < kNB - 1 && ((mUp[i] >> lane) & 1)) s = s + v.y * cur[swz(p + 8, lane)];
+          if (k < kNB - 1 && ((__ldg(um + c + 64) >> lane) & 1)) s = s + v.z * prv[swz(p, lane)];
+        }
+        const double zc = yv[i] - s * v.w;
+        cur[swz(p, lane)] = zc;
+        zp = zc;
+      }
+#pragma unroll
+      for (int i = 0; i < kNB; i++) mUp[i] = A.m[i];
+      A = B;
+    }
+    __syncwarp();
+#pragma unroll 8
+    for (int bb = 0; bb < 32; bb++) {
+      const long blk = gb + bb;
+      if (blk < nBlock) {
+        z[blk * kNC + 64 * k + lane] = cur[swz(lane, bb)];
+        z[blk * kNC + 64 * k + 32 + lane] = cur[swz(32 + lane, bb)];
+      }
+    }
+    __syncwarp();
+    double *t = cur; cur = prv; prv = t;
+  }
+}
+
+WaveTable make_wave_table() {
+  WaveTable t;
+  int n = 0;
+  for (int w = 0; w < kNumWave; w++) {
+    t.off[w] = (short)n;
+    for (int c = 0; c < kNC; c++)
+      if ((c & 7) + ((c >> 3) & 7) + (c >> 6) == w) t.cell[n++] = (short)c;
+  }
+  t.off[kNumWave] = (short)n;
+  return t;
+}
+
 __global__ void k_h_sub(double *y, const double *b, const double *ax, long n) {
   for (long q = blockIdx.x * (long)blockDim.x + threadIdx.x; q < n; q += (long)gridDim.x * blockDim.x) y[q] = b[q] - ax[q];
 }
@@ -313,7 +482,7 @@ __global__ void k_h_te_update(double *Te, const double *x, const unsigned char *
 }
 
 void free_heat() {
-  for (double **p : {&H.Te, &H.HC, &H.B3, &H.b, &H.x, &H.w, &H.t, &H.r, &H.V, &H.off, &H.dIlu, &H.partial, &H.scal}) {
+  for (double **p : {&H.Te, &H.HC, &H.B3, &H.b, &H.x, &H.w, &H.t, &H.r, &H.V, &H.partial, &H.scal}) {
     if (*p) cudaFree(*p);
     *p = nullptr;
   }
@@ -323,20 +492,31 @@ void free_heat() {
     if (*p) cudaFree(*p);
     *p = nullptr;
   }
+  if (H.K) cudaFree(H.K);
+  H.K = nullptr;
+  if (H.yI) cudaFree(H.yI);
+  if (H.usedM) cudaFree(H.usedM);
+  H.yI = nullptr;
+  H.usedM = nullptr;
+  if (H.coef) cudaFree(H.coef);
+  if (H.wtab) cudaFree(H.wtab);
+  if (H.cnt) cudaFree(H.cnt);
+  H.coef = nullptr;
+  H.wtab = nullptr;
+  H.cnt = nullptr;
   for (auto &e : H.ev)
     if (e) { cudaEventDestroy(e); e = nullptr; }
   H.ready = false;
 }
 
 int dotd(const double *x, const double *y, double *out, cudaStream_t st) {
-  k_h_axpy_dot<<<kRedBlk, kRedThr, 0, st>>>(const_cast<double *>(x), nullptr, nullptr, y, H.nCell, H.partial);
-  k_h_sum<<<1, kRedThr, 0, st>>>(H.partial, kRedBlk, out);
+  kry_mgs(const_cast<double *>(x), nullptr, nullptr, y, H.nCell, H.partial, H.cnt, out, st);
   CKH(cudaGetLastError());
   return BX_OK;
 }
 
 int matvec(const double *x, double *y, cudaStream_t st) {
-  k_heat_apply<<<H.nBlock, 512, 0, st>>>(H.a, x, H.HC, H.B3, H.used, y, kModeMatvec);
+  k_heat_apply<<<H.nBlock, 512, 0, st>>>(H.a, x, H.K, H.used, y, kModeMatvec);
   CKH(cudaGetLastError());
   H.nMatvec++;
   return BX_OK;
@@ -344,7 +524,7 @@ int matvec(const double *x, double *y, cudaStream_t st) {
 
 int precond(const double *r, double *z, cudaStream_t st) {
   if (H.p.TypePrecond == BX_PRECOND_BILU) {
-    k_heat_ilu_solve<<<H.nBlock, 512, 0, st>>>(H.off, H.used, H.dIlu, r, z);
+    k_heat_ilu<<<H.nGroup, 32, 0, st>>>(H.coef, H.coef + H.nIl, H.usedM, r, H.yI, z, H.nBlock);
   } else if (H.p.TypePrecond == BX_PRECOND_NONE) {
     CKH(cudaMemcpyAsync(z, r, sizeof(double) * H.nCell, cudaMemcpyDeviceToDevice, st));
   } else {
@@ -375,7 +555,7 @@ int gmres(int &iError, cudaStream_t st) {
   double beta = beta0;
   std::vector<double> Hm((m + 1) * m), cs(m), sn(m), g(m + 1), y(m), hb(m + 2);
   while (true) {
-    k_h_scale<<<1184, 256, 0, st>>>(Vb, H.r, H.scal + 2, 1, N);
+    k_kry_scale<<<kKryBlocks, kKryThreads, 0, st>>>(Vb, H.r, H.scal + 2, 1, N);
     CKH(cudaGetLastError());
     std::fill(g.begin(), g.end(), 0.0);
     g[0] = beta;
@@ -389,15 +569,14 @@ int gmres(int &iError, cudaStream_t st) {
         const double *vq = q > 0 ? Vb + (size_t)(q - 1) * N : nullptr;
         const double *hq = q > 0 ? hdev + q - 1 : nullptr;
         const double *vn = q <= k ? Vb + (size_t)q * N : nullptr;
-        k_h_axpy_dot<<<kRedBlk, kRedThr, 0, st>>>(H.w, vq, hq, vn, N, H.partial);
-        k_h_sum<<<1, kRedThr, 0, st>>>(H.partial, kRedBlk, hdev + q);
+        kry_mgs(H.w, vq, hq, vn, N, H.partial, H.cnt, hdev + q, st);
       }
       CKH(cudaGetLastError());
       CKH(cudaMemcpyAsync(hb.data(), hdev, sizeof(double) * (k + 2), cudaMemcpyDeviceToHost, st));
       CKH(cudaStreamSynchronize(st));
       const double hn = std::sqrt(hb[k + 1]);
       if (hn != 0.0) {
-        k_h_scale<<<1184, 256, 0, st>>>(Vb + (size_t)(k + 1) * N, H.w, hdev + k + 1, 1, N);
+        k_kry_scale<<<kKryBlocks, kKryThreads, 0, st>>>(Vb + (size_t)(k + 1) * N, H.w, hdev + k + 1, 1, N);
         CKH(cudaGetLastError());
       }
       for (int q = 0; q <= k; q++) Hm[q * m + k] = hb[q];
@@ -428,7 +607,7 @@ int gmres(int &iError, cudaStream_t st) {
       y[q] = s / Hm[q * m + q];
     }
     CKH(cudaMemcpyAsync(H.scal + 80, y.data(), sizeof(double) * kdone, cudaMemcpyHostToDevice, st));
-    k_h_update<<<1184, 256, 0, st>>>(H.x, Vb, H.scal + 80, kdone, N);
+    k_kry_update<<<kKryBlocks, kKryThreads, 0, st>>>(H.x, Vb, H.scal + 80, kdone, N);
     CKH(cudaGetLastError());
     if (conv) return BX_OK;
     if (H.nMatvec >= H.p.MaxMatvec) { iError = 1; return BX_OK; }
@@ -477,6 +656,14 @@ int grid_tables(const Core &c, std::vector<int> &at, std::vector<int> &xyz) {
   return BX_OK;
 }
 
+// HeatCoef and the face tensor K from the current Te
+int update_coef(cudaStream_t st) {
+  k_heat_coef<<<1184, 256, 0, st>>>(H.Te, H.HC, H.p.HeatCondPar, H.nCell);
+  k_heat_faces<<<H.nBlock, 512, 0, st>>>(H.a, H.HC, H.B3, H.K);
+  CKH(cudaGetLastError());
+  return BX_OK;
+}
+
 int need_heat() {
   if (!H.ready) return core_fail(BX_ERR_STATE, "bx_heat_init has not been called");
   return BX_OK;
@@ -519,20 +706,32 @@ int bx_heat_init(const bx_heat_params *prm, const double *Te, const double *bhat
   H.nCell = (long)c.nBlock * kNC;
   for (int d = 0; d < 3; d++) H.a.n[d] = H.a.nbx[d] * kNB;
   H.a.V = H.a.dx[0] * H.a.dx[1] * H.a.dx[2];
-  for (int d = 0; d < 3; d++) H.a.area[d] = H.a.V / H.a.dx[d];
+  for (int d = 0; d < 3; d++) {
+    H.a.area[d] = H.a.V / H.a.dx[d];
+    H.a.invDx[d] = 1.0 / H.a.dx[d];
+    H.a.gA[d] = -0.25 * H.a.invDx[d];
+    H.a.gC[d] = 0.25 * H.a.invDx[d];
+  }
   H.a.f = prm->FractionFieldAligned;
   H.a.cv = prm->Cv;
   H.a.dt = prm->Dt;
   H.a.sic = prm->SemiImplCoeff;
   const size_t vb = sizeof(double) * H.nCell;
   bool ok = true;
-  for (double **p : {&H.Te, &H.HC, &H.b, &H.x, &H.w, &H.t, &H.r, &H.dIlu}) ok = ok && cudaMalloc(p, vb) == cudaSuccess;
-  ok = ok && cudaMalloc(&H.B3, 3 * vb) == cudaSuccess && cudaMalloc(&H.off, 7 * vb) == cudaSuccess &&
+  for (double **p : {&H.Te, &H.HC, &H.b, &H.x, &H.w, &H.t, &H.r}) ok = ok && cudaMalloc(p, vb) == cudaSuccess;
+  H.nGroup = (H.nBlock + 31) / 32;
+  H.nIl = (long)H.nGroup * 32 * kNC;
+  ok = ok && cudaMalloc(&H.B3, 3 * vb) == cudaSuccess &&
+       cudaMalloc(&H.coef, 2 * sizeof(double4) * H.nIl) == cudaSuccess &&
+       cudaMalloc(&H.yI, sizeof(double) * H.nIl) == cudaSuccess &&
+       cudaMalloc(&H.usedM, sizeof(unsigned) * H.nGroup * kNC) == cudaSuccess &&
+       cudaMalloc(&H.K, sizeof(double) * kKBlock * H.nBlock) == cudaSuccess &&
+       cudaMalloc(&H.wtab, sizeof(WaveTable)) == cudaSuccess && cudaMalloc(&H.cnt, sizeof(unsigned)) == cudaSuccess &&
        cudaMalloc(&H.V, vb * (prm->nKrylovVector + 1)) == cudaSuccess &&
        cudaMalloc(&H.used, H.nCell) == cudaSuccess &&
        cudaMalloc(&H.blkAt, sizeof(int) * atH.size()) == cudaSuccess &&
        cudaMalloc(&H.blkXYZ, sizeof(int) * xyzH.size()) == cudaSuccess &&
-       cudaMalloc(&H.partial, sizeof(double) * kRedBlk) == cudaSuccess &&
+       cudaMalloc(&H.partial, sizeof(double) * kKryBlocks) == cudaSuccess &&
        cudaMalloc(&H.scal, sizeof(double) * 160) == cudaSuccess;
   if (!ok) {
     free_heat();
@@ -547,7 +746,18 @@ int bx_heat_init(const bx_heat_params *prm, const double *Te, const double *bhat
   CKH(cudaMemcpyAsync(H.blkXYZ, xyzH.data(), sizeof(int) * xyzH.size(), cudaMemcpyHostToDevice, c.st));
   H.a.blkAt = H.blkAt;
   H.a.blkXYZ = H.blkXYZ;
-  k_heat_coef<<<1184, 256, 0, c.st>>>(H.Te, H.HC, prm->HeatCondPar, H.nCell);
+  static const WaveTable wt = make_wave_table();
+  CKH(cudaMemcpyAsync(H.wtab, &wt, sizeof(WaveTable), cudaMemcpyHostToDevice, c.st));
+  CKH(cudaMemsetAsync(H.cnt, 0, sizeof(unsigned), c.st));
+  CKH(cudaMemsetAsync(H.coef, 0, 2 * sizeof(double4) * H.nIl, c.st));
+  {
+    std::vector<unsigned> um((size_t)H.nGroup * kNC, 0u);
+    for (long b = 0; b < H.nBlock; b++)
+      for (int q = 0; q < kNC; q++)
+        if (used[b * kNC + q]) um[(size_t)(b >> 5) * kNC + q] |= 1u << (b & 31);
+    CKH(cudaMemcpy(H.usedM, um.data(), sizeof(unsigned) * um.size(), cudaMemcpyHostToDevice));
+  }
+  if (const int e = update_coef(c.st)) return e;
   CKH(cudaGetLastError());
   CKH(cudaStreamSynchronize(c.st));
   H.ready = true;
@@ -559,16 +769,16 @@ int bx_advance_semi_impl(bx_krylov_stats *stats) {
   if (r) return r;
   Core c = core();
   CKH(cudaEventRecord(H.ev[0], c.st));
-  k_heat_apply<<<H.nBlock, 512, 0, c.st>>>(H.a, H.Te, H.HC, H.B3, H.used, H.b, kModeRhs);
+  k_heat_apply<<<H.nBlock, 512, 0, c.st>>>(H.a, H.Te, H.K, H.used, H.b, kModeRhs);
   if (H.p.TypePrecond == BX_PRECOND_BILU) {
-    k_heat_jac<<<1184, 256, 0, c.st>>>(H.a, H.HC, H.B3, H.used, H.off, H.nCell);
-    k_heat_ilu_factor<<<H.nBlock, 512, 0, c.st>>>(H.off, H.used, H.dIlu);
+    k_heat_factor<<<(H.nBlock + kWarpsPerCta - 1) / kWarpsPerCta, 32 * kWarpsPerCta, 0, c.st>>>(
+        H.a, H.K, H.used, H.wtab, H.coef, H.coef + H.nIl, H.nBlock);
   }
   CKH(cudaGetLastError());
   int iError = 0;
   if ((r = gmres(iError, c.st))) return r;
   k_h_te_update<<<1184, 256, 0, c.st>>>(H.Te, H.x, H.used, H.nCell);
-  k_heat_coef<<<1184, 256, 0, c.st>>>(H.Te, H.HC, H.p.HeatCondPar, H.nCell);
+  if ((r = update_coef(c.st))) return r;
   CKH(cudaGetLastError());
   CKH(cudaEventRecord(H.ev[1], c.st));
   CKH(cudaEventSynchronize(H.ev[1]));
@@ -598,7 +808,7 @@ int bx_heat_get_rhs(double *b) {
   if (r) return r;
   if (!b) return core_fail(BX_ERR_ARG, "null argument");
   Core c = core();
-  k_heat_apply<<<H.nBlock, 512, 0, c.st>>>(H.a, H.Te, H.HC, H.B3, H.used, H.b, kModeRhs);
+  k_heat_apply<<<H.nBlock, 512, 0, c.st>>>(H.a, H.Te, H.K, H.used, H.b, kModeRhs);
   CKH(cudaGetLastError());
   return copy_out(b, H.b);
 }
@@ -621,8 +831,8 @@ int bx_heat_precond(const double *rv, double *z) {
   if (!rv || !z) return core_fail(BX_ERR_ARG, "null argument");
   Core c = core();
   if (H.p.TypePrecond == BX_PRECOND_BILU) {
-    k_heat_jac<<<1184, 256, 0, c.st>>>(H.a, H.HC, H.B3, H.used, H.off, H.nCell);
-    k_heat_ilu_factor<<<H.nBlock, 512, 0, c.st>>>(H.off, H.used, H.dIlu);
+    k_heat_factor<<<(H.nBlock + kWarpsPerCta - 1) / kWarpsPerCta, 32 * kWarpsPerCta, 0, c.st>>>(
+        H.a, H.K, H.used, H.wtab, H.coef, H.coef + H.nIl, H.nBlock);
     CKH(cudaGetLastError());
   }
   if ((r = copy_in(H.r, rv))) return r;

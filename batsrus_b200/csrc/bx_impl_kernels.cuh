@@ -61,15 +61,6 @@ __device__ __forceinline__ double block_sum(double v, double *sh) {
   return r;
 }
 
-// partial[blockIdx] = sum a*b
-__global__ void k_dot_partial(const double *__restrict__ a, const double *__restrict__ b, long n, double *partial) {
-  __shared__ double sh[32];
-  double s = 0;
-  for (long q = blockIdx.x * (long)blockDim.x + threadIdx.x; q < n; q += (long)gridDim.x * blockDim.x) s += a[q] * b[q];
-  s = block_sum(s, sh);
-  if (threadIdx.x == 0) partial[blockIdx.x] = s;
-}
-
 // per-variable sums of squares: partial[blockIdx*8 + v]
 __global__ void k_varsq_partial(const double *__restrict__ a, long nCellBlock, long nCell, double *partial) {
   __shared__ double sh[32];
@@ -97,29 +88,6 @@ __global__ void k_sum_partials(const double *partial, int nPart, int stride, int
     s = block_sum(s, sh);
     if (threadIdx.x == 0) out[j] = s;
   }
-}
-
-// MGS step of the Arnoldi process, fused: w -= h_q v_q (with h_q read from
-// device memory), then partial dot of the updated w with v_next
-__global__ void k_mgs_axpy_dot(double *__restrict__ w, const double *__restrict__ vq, const double *hq,
-                               const double *__restrict__ vnext, long n, double *partial) {
-  __shared__ double sh[32];
-  const double h = hq ? *hq : 0.0;
-  double s = 0;
-  for (long q = blockIdx.x * (long)blockDim.x + threadIdx.x; q < n; q += (long)gridDim.x * blockDim.x) {
-    double x = w[q];
-    if (vq) x = x - h * vq[q];
-    if (vq) w[q] = x;
-    s += vnext ? x * vnext[q] : x * x;
-  }
-  s = block_sum(s, sh);
-  if (threadIdx.x == 0) partial[blockIdx.x] = s;
-}
-
-// y = a*x (a from device memory, optionally its inverse)
-__global__ void k_scale(double *__restrict__ y, const double *__restrict__ x, const double *a, int invert, long n) {
-  const double s = invert ? 1.0 / sqrt(*a) : *a;
-  for (long q = blockIdx.x * (long)blockDim.x + threadIdx.x; q < n; q += (long)gridDim.x * blockDim.x) y[q] = s * x[q];
 }
 
 // Ueps = U + eps x Norm_V (eps = sqrt(JacobianEps)/rms(x), rms from xx)
@@ -157,15 +125,6 @@ __global__ void k_rhs(double *__restrict__ rhs, const double *__restrict__ resEx
     const int v = (int)((q / nCellBlock) % 8);
     if (bdf2) rhs[q] = (c1 * resExpl[q] + c2 * (U[q] - Uold[q])) / norm[v];
     else rhs[q] = resExpl[q] * c1 / norm[v];
-  }
-}
-
-// x += sum_q y_q z_q (y on the device)
-__global__ void k_update_x(double *__restrict__ x, const double *__restrict__ Z, const double *y, int k, long n) {
-  for (long q = blockIdx.x * (long)blockDim.x + threadIdx.x; q < n; q += (long)gridDim.x * blockDim.x) {
-    double s = x[q];
-    for (int p = 0; p < k; p++) s += y[p] * Z[(size_t)p * n + q];
-    x[q] = s;
   }
 }
 

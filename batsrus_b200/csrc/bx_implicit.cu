@@ -23,6 +23,7 @@
 
 #include "bx_core.h"
 #include "bx_impl_kernels.cuh"
+#include "bx_krylov.cuh"
 
 using namespace bx;
 
@@ -39,6 +40,7 @@ struct ImplCtx {
   double *dtCell = nullptr;                    // DtMax_CB left by calc_timestep
   double *Jac = nullptr, *Dinv = nullptr;
   double *partial = nullptr, *scal = nullptr;  // reduction scratch, device scalars
+  unsigned *cnt = nullptr;                     // CTA counter of the one-launch reductions
   double *dNorm = nullptr;
   int *wfCell = nullptr, *wfStart = nullptr;
   int nWave = 0, maxWave = 0;
@@ -70,6 +72,8 @@ void free_impl() {
     if (*p) cudaFree(*p);
     *p = nullptr;
   }
+  if (I.cnt) cudaFree(I.cnt);
+  I.cnt = nullptr;
   if (I.wfCell) cudaFree(I.wfCell);
   if (I.wfStart) cudaFree(I.wfStart);
   I.wfCell = I.wfStart = nullptr;
@@ -78,8 +82,7 @@ void free_impl() {
 
 // deterministic dot product into device scalar *out
 int ddot(const double *a, const double *b, double *out, cudaStream_t st) {
-  k_dot_partial<<<kRedBlocks, kRedThreads, 0, st>>>(a, b, I.N, I.partial);
-  k_sum_partials<<<1, kRedThreads, 0, st>>>(I.partial, kRedBlocks, 1, 1, out);
+  kry_mgs(const_cast<double *>(a), nullptr, nullptr, a == b ? nullptr : b, I.N, I.partial, I.cnt, out, st);
   CKI(cudaGetLastError());
   return BX_OK;
 }
@@ -189,7 +192,7 @@ int gmres(int &iError) {
   std::vector<double> H((m + 1) * m), cs(m), sn(m), gv(m + 1), hb(m + 2), y(m);
   double *hdev = I.scal + 8;  // h_0 .. h_{k+1}
   while (true) {
-    k_scale<<<kG, kT, 0, c.st>>>(I.V, rvec, I.scal + 2, 1, N);  // V0 = r/||r||
+    k_kry_scale<<<kKryBlocks, kKryThreads, 0, c.st>>>(I.V, rvec, I.scal + 2, 1, N);  // V0 = r/||r||
     CKI(cudaGetLastError());
     std::fill(gv.begin(), gv.end(), 0.0);
     gv[0] = beta;
@@ -204,15 +207,14 @@ int gmres(int &iError) {
         const double *vq = q > 0 ? I.V + (size_t)(q - 1) * N : nullptr;
         const double *hq = q > 0 ? hdev + q - 1 : nullptr;
         const double *vn = q <= k ? I.V + (size_t)q * N : nullptr;
-        k_mgs_axpy_dot<<<kRedBlocks, kRedThreads, 0, c.st>>>(I.W, vq, hq, vn, N, I.partial);
-        k_sum_partials<<<1, kRedThreads, 0, c.st>>>(I.partial, kRedBlocks, 1, 1, hdev + q);
+        kry_mgs(I.W, vq, hq, vn, N, I.partial, I.cnt, hdev + q, c.st);
       }
       CKI(cudaGetLastError());
       CKI(cudaMemcpyAsync(hb.data(), hdev, sizeof(double) * (k + 2), cudaMemcpyDeviceToHost, c.st));
       CKI(cudaStreamSynchronize(c.st));
       const double hn = std::sqrt(hb[k + 1]);
       if (hn != 0.0) {
-        k_scale<<<kG, kT, 0, c.st>>>(I.V + (size_t)(k + 1) * N, I.W, hdev + k + 1, 1, N);
+        k_kry_scale<<<kKryBlocks, kKryThreads, 0, c.st>>>(I.V + (size_t)(k + 1) * N, I.W, hdev + k + 1, 1, N);
         CKI(cudaGetLastError());
       }
       for (int q = 0; q <= k; q++) H[q * m + k] = hb[q];
@@ -243,7 +245,7 @@ int gmres(int &iError) {
       y[q] = s / H[q * m + q];
     }
     CKI(cudaMemcpyAsync(I.scal + 48, y.data(), sizeof(double) * kdone, cudaMemcpyHostToDevice, c.st));
-    k_update_x<<<kG, kT, 0, c.st>>>(I.X, I.Z, I.scal + 48, kdone, N);
+    k_kry_update<<<kKryBlocks, kKryThreads, 0, c.st>>>(I.X, I.Z, I.scal + 48, kdone, N);
     CKI(cudaGetLastError());
     if (conv) return BX_OK;
     if (I.nMatvec >= I.p.MaxMatvec) { iError = 1; return BX_OK; }
@@ -356,7 +358,8 @@ int bx_implicit_init(const bx_implicit_params *prm) {
   if (cudaMalloc(&I.V, vb * (I.m + 1)) != cudaSuccess || cudaMalloc(&I.Z, vb * I.m) != cudaSuccess ||
       cudaMalloc(&I.dtCell, sizeof(double) * I.nCellTot) != cudaSuccess ||
       cudaMalloc(&I.partial, sizeof(double) * kRedBlocks * 8) != cudaSuccess ||
-      cudaMalloc(&I.scal, sizeof(double) * 128) != cudaSuccess || cudaMalloc(&I.dNorm, sizeof(double) * 8) != cudaSuccess) {
+      cudaMalloc(&I.scal, sizeof(double) * 128) != cudaSuccess || cudaMalloc(&I.dNorm, sizeof(double) * 8) != cudaSuccess ||
+      cudaMalloc(&I.cnt, sizeof(unsigned)) != cudaSuccess || cudaMemset(I.cnt, 0, sizeof(unsigned)) != cudaSuccess) {
     free_impl();
     return core_fail(BX_ERR_NOMEM, "Krylov bases");
   }
