@@ -28,7 +28,7 @@ UNITS = [
     ("bx_implicit.cu", ["--fmad=false"]),
     ("bx_learned.cu", []),
     ("bx_noalloc.cu", []),
-    ("bx_heat.cu", ["--fmad=false"]),
+    ("bx_heat.cu", []),
     ("bx_capi.cu", []),
 ]
 HEADERS = ["bx_physics.cuh", "bx_stage.cuh", "bx_device.h", "bx_stage3d.cuh", "bx_tma.cuh", "bx_core.h",

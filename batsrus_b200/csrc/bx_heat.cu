@@ -22,7 +22,10 @@
 // Gram-Schmidt and deterministic FP64 inner products; the Givens rotations
 // run on the host.  Cells that are not used keep their temperature.
 //
-// Compiled with --fmad=false: the formulas keep the oracle's operation order.
+// The formulas follow the oracle's operation order; multiply-adds are
+// contracted, products by 1/V and 1/Dt replace the divisions and the zero
+// weight of the central term of the transverse gradient is dropped, so the
+// results agree with the oracle to rounding (1e-12 relative), not bitwise.
 #include <cuda_runtime.h>
 
 #include <cmath>
@@ -30,6 +33,7 @@
 
 #include "bx_core.h"
 #include "bx_krylov.cuh"
+#include "bx_tma.cuh"
 
 using namespace bx;
 
@@ -42,9 +46,11 @@ struct HeatArgs {
   int nbx[3];      // blocks per dimension
   double dx[3], V, area[3];
   double invDx[3], gA[3], gC[3];  // 1/dx and the transverse gradient weights -0.25/dx, +0.25/dx
+  double invV, cvDt;              // 1/V and Cv/Dt
   double f, cv, dt, sic;
   const int *blkAt;   // [nbx[2]][nbx[1]][nbx[0]] -> block index
   const int *blkXYZ;  // per block: its block coordinates
+  int *err;           // set when a bounded wait gives up
 };
 
 struct HeatCtx {
@@ -65,6 +71,7 @@ struct HeatCtx {
   long nIl = 0;              // cells of the interleaved arrays (nGroup x 32 x 512)
   struct WaveTable *wtab = nullptr;
   unsigned *cnt = nullptr;
+  int *errDev = nullptr;  // device error flag of the bounded waits
   double *partial = nullptr, *scal = nullptr;
   int nMatvec = 0;
   double errRel = 0;
@@ -110,13 +117,6 @@ enum { kModeRhs = 0, kModeMatvec = 1 };
 constexpr int kFacesDim = (kNB + 1) * kNB * kNB;
 constexpr int kKBlock = 9 * kFacesDim;  // doubles of K per block
 
-// tile coordinates (1..9 along d) of the right cell of face r of dimension D
-template <int D>
-__device__ __forceinline__ void face_cell(int r, int &i, int &j, int &k) {
-  if (D == 0) { i = r % 9 + 1; j = (r / 9) % 8 + 1; k = r / 72 + 1; }
-  else if (D == 1) { i = r % 8 + 1; j = (r / 8) % 9 + 1; k = r / 72 + 1; }
-  else { i = r % 8 + 1; j = (r / 8) % 8 + 1; k = r / 64 + 1; }
-}
 // r of the lower face of block cell (i, j, k) (0..7) in dimension d
 __device__ __forceinline__ int lower_face(int d, int i, int j, int k) {
   return d == 0 ? i + 9 * (j + 8 * k) : (d == 1 ? i + 8 * (j + 9 * k) : i + 8 * (j + 8 * k));
@@ -126,42 +126,51 @@ __device__ __forceinline__ int tidx(int i, int j, int k) { return i + kTile * (j
 
 // HeatCond_DFDB(dir, face, D) = Area HeatCoef_f BbF(D, dir) with the face
 // averages of HeatCoef and of the tensor (get_impl_heat_cond_state,
-// src/ModHeatConduction.f90:1096-1432)
+// src/ModHeatConduction.f90:1096-1432).  K stores the faces of dimension D
+// row-major: index u + 8 v + 64 a for the face at position a (0..8) along D
+// whose transverse block coordinates (0..7, dimension order) are u, v
 template <int D>
-__device__ __forceinline__ void face_tensor(const HeatArgs &a, const double *hc, const double *b3, int r, double *Kd) {
-  int i, j, k;
-  face_cell<D>(r, i, j, k);
-  const int R = tidx(i, j, k), L = tidx(i - (D == 0), j - (D == 1), k - (D == 2));
+__device__ __forceinline__ void face_tensor(const HeatArgs &a, const double *hc, const double *b3, int rk, double *Kd) {
+  constexpr int E1 = D == 0 ? 1 : 0, E2 = D == 2 ? 1 : 2;
+  int x[3];
+  x[D] = rk / 64 + 1;
+  x[E1] = rk % 8 + 1;
+  x[E2] = (rk / 8) % 8 + 1;
+  const int R = tidx(x[0], x[1], x[2]);
+  x[D]--;
+  const int L = tidx(x[0], x[1], x[2]);
 #pragma unroll
   for (int dir = 0; dir < 3; dir++) {
     const double BbF = 0.5 * (bb(b3 + 3 * R, a.f, D, dir) + bb(b3 + 3 * L, a.f, D, dir));
     const double HeatCoef = 0.5 * (hc[R] + hc[L]);
-    Kd[dir * kFacesDim + r] = a.area[D] * HeatCoef * BbF;
+    Kd[dir * kFacesDim + rk] = a.area[D] * HeatCoef * BbF;
   }
 }
 
-// -HeatCond . FaceGrad of face r of dimension D (get_face_gradient,
-// src/ModFaceGradient.f90:933-1140, uniform Cartesian grid; the flux of
-// get_heat_conduction_rhs, src/ModHeatConduction.f90:1466-1477)
+// -HeatCond . FaceGrad of the face with K index rk of dimension D
+// (get_face_gradient, src/ModFaceGradient.f90:933-1140, uniform Cartesian
+// grid; the flux of get_heat_conduction_rhs, src/ModHeatConduction.f90:
+// 1466-1477), stored at its x-fastest index in F
 template <int D>
-__device__ __forceinline__ double face_flux(const HeatArgs &a, const double *S, const double *__restrict__ Kd, int r) {
-  int i, j, k;
-  face_cell<D>(r, i, j, k);
-  const int R = tidx(i, j, k), L = tidx(i - (D == 0), j - (D == 1), k - (D == 2));
+__device__ __forceinline__ void face_flux(const HeatArgs &a, const double *S, const double *Kd, double *F, int rk) {
+  constexpr int E1 = D == 0 ? 1 : 0, E2 = D == 2 ? 1 : 2;
+  constexpr int O1 = E1 == 0 ? 1 : kTile, O2 = E2 == 1 ? kTile : kTile * kTile;
+  const int an = rk / 64, u = rk % 8, v = (rk / 8) % 8;
+  int x[3];
+  x[D] = an + 1;
+  x[E1] = u + 1;
+  x[E2] = v + 1;
+  const int R = tidx(x[0], x[1], x[2]);
+  const int L = R - (D == 0 ? 1 : (D == 1 ? kTile : kTile * kTile));
   double g[3];
   g[D] = a.invDx[D] * (S[R] - S[L]);
-#pragma unroll
-  for (int e = 0; e < 3; e++) {
-    if (e == D) continue;
-    const double Be = 0.0;
-    const int o = e == 0 ? 1 : (e == 1 ? kTile : kTile * kTile);
-    const double sm = S[L - o] + S[R - o], s0 = S[L] + S[R], sp = S[L + o] + S[R + o];
-    g[e] = a.gA[e] * sm + Be * s0 + a.gC[e] * sp;
-  }
+  g[E1] = a.gA[E1] * (S[L - O1] + S[R - O1]) + a.gC[E1] * (S[L + O1] + S[R + O1]);
+  g[E2] = a.gA[E2] * (S[L - O2] + S[R - O2]) + a.gC[E2] * (S[L + O2] + S[R + O2]);
   double f = 0.0;
 #pragma unroll
-  for (int dir = 0; dir < 3; dir++) f = f + Kd[dir * kFacesDim + r] * g[dir];
-  return -f;
+  for (int dir = 0; dir < 3; dir++) f = f + Kd[dir * kFacesDim + rk] * g[dir];
+  const int rF = D == 0 ? an + 9 * (u + 8 * v) : (D == 1 ? u + 8 * (an + 9 * v) : u + 8 * (v + 8 * an));
+  F[rF] = -f;
 }
 
 // the tile of the block and its ghost layer, clamped into the domain
@@ -195,30 +204,46 @@ __global__ void __launch_bounds__(512) k_heat_faces(HeatArgs a, const double *__
   }
 }
 
-// one CTA per block, 512 threads: the 10^3 tile of the scalar, each of the
-// block's 3 x 576 face fluxes once, then per cell Res = -sum (F+ - F-)/V
-// (get_heat_conduction_rhs :1434-1545); mode RHS writes b = V Res(Te), mode
-// MATVEC y = V (x Cv/Dt - SemiImplCoeff Res(x)) (semi_impl_matvec,
-// src/ModSemiImplicit.f90:578-762)
+// one CTA per block, 512 threads: the block's face tensor (41.5 KB,
+// contiguous) arrives by one bulk copy while the threads gather the 10^3
+// tile of the scalar; then each of the block's 3 x 576 face fluxes once, and
+// per cell Res = -sum (F+ - F-)/V (get_heat_conduction_rhs :1434-1545);
+// mode RHS writes b = V Res(Te), mode MATVEC y = V (x Cv/Dt - SemiImplCoeff
+// Res(x)) (semi_impl_matvec, src/ModSemiImplicit.f90:578-762)
+constexpr size_t kApplySmem = sizeof(double) * (kKBlock + kTile * kTile * kTile + 3 * kFacesDim);
+
 __global__ void __launch_bounds__(512) k_heat_apply(HeatArgs a, const double *__restrict__ S,
                                                     const double *__restrict__ K,
                                                     const unsigned char *__restrict__ used, double *out, int mode) {
-  __shared__ double sS[kTile * kTile * kTile], sF[3 * kFacesDim];
+  extern __shared__ __align__(128) double dsm[];
+  double *sK = dsm, *sS = sK + kKBlock, *sF = sS + kTile * kTile * kTile;
+  __shared__ uint64_t bar;
   const int blk = blockIdx.x;
+  if (threadIdx.x == 0) {
+    mbar_init(&bar, 1);
+    fence_mbar_init();
+  }
+  __syncthreads();  // the barrier is initialised before any thread waits on it
+  if (threadIdx.x == 0) {
+    mbar_arrive_expect_tx(&bar, sizeof(double) * kKBlock);
+    bulk_load(sK, K + (size_t)blk * kKBlock, sizeof(double) * kKBlock, &bar);
+  }
   for_tile(a, blk, [&](int q, long g) {
     double s = S[g];
     if (mode == kModeMatvec && !used[g]) s = 0.0;  // unused cells keep their value
     sS[q] = s;
   });
-  __syncthreads();
-  const double *Kb = K + (size_t)blk * kKBlock;
+  const bool ok = mbar_wait_bounded(&bar, 0);
+  if (!__syncthreads_and(ok)) {  // also the barrier of the tile
+    if (threadIdx.x == 0) atomicExch(a.err, 1);
+    if (!ok) mbar_wait_bounded(&bar, 0);  // the copy into this CTA's shared memory must end before the CTA does
+    return;
+  }
   for (int f = threadIdx.x; f < 3 * kFacesDim; f += blockDim.x) {
-    const int d = f / kFacesDim, r = f % kFacesDim;
-    double v;
-    if (d == 0) v = face_flux<0>(a, sS, Kb, r);
-    else if (d == 1) v = face_flux<1>(a, sS, Kb + 3 * kFacesDim, r);
-    else v = face_flux<2>(a, sS, Kb + 6 * kFacesDim, r);
-    sF[f] = v;
+    const int d = f / kFacesDim, rk = f % kFacesDim;  // d is warp-uniform (576 = 18 x 32)
+    if (d == 0) face_flux<0>(a, sS, sK, sF, rk);
+    else if (d == 1) face_flux<1>(a, sS, sK + 3 * kFacesDim, sF + kFacesDim, rk);
+    else face_flux<2>(a, sS, sK + 6 * kFacesDim, sF + 2 * kFacesDim, rk);
   }
   __syncthreads();
   const int c = threadIdx.x;
@@ -226,13 +251,13 @@ __global__ void __launch_bounds__(512) k_heat_apply(HeatArgs a, const double *__
   const double *F0 = sF, *F1 = sF + kFacesDim, *F2 = sF + 2 * kFacesDim;
   const int r0 = lower_face(0, i, j, k), r1 = lower_face(1, i, j, k), r2 = lower_face(2, i, j, k);
   double res = 0.0;
-  res = res - (F0[r0 + 1] - F0[r0]) / a.V;
-  res = res - (F1[r1 + kNB] - F1[r1]) / a.V;
-  res = res - (F2[r2 + kNB * kNB] - F2[r2]) / a.V;
+  res = res - (F0[r0 + 1] - F0[r0]) * a.invV;
+  res = res - (F1[r1 + kNB] - F1[r1]) * a.invV;
+  res = res - (F2[r2 + kNB * kNB] - F2[r2]) * a.invV;
   const long q = (long)blk * kNC + c;
   const int tc = tidx(i + 1, j + 1, k + 1);
   if (mode == kModeRhs) out[q] = used[q] ? a.V * res : 0.0;
-  else out[q] = used[q] ? a.V * (sS[tc] * a.cv / a.dt - a.sic * res) : a.V * (S[q] * a.cv / a.dt);
+  else out[q] = used[q] ? a.V * (sS[tc] * a.cvDt - a.sic * res) : a.V * (S[q] * a.cvDt);
 }
 
 // ---- block ILU(0) of the 7-point preconditioner matrix --------------------
@@ -297,12 +322,12 @@ __global__ void __launch_bounds__(32 * kWarpsPerCta) k_heat_factor(HeatArgs a, c
     double lo[3] = {0.0, 0.0, 0.0}, dg = D0;
     if (used[q]) {
       double sumJ = 0.0;
-      const int r[3] = {lower_face(0, i, j, k), lower_face(1, i, j, k), lower_face(2, i, j, k)};
+      const int r[3] = {j + 8 * k + 64 * i, i + 8 * k + 64 * j, i + 8 * j + 64 * k};  // K index of the lower faces
 #pragma unroll
       for (int d = 0; d < 3; d++) {
         const double *Kdd = Kb + (3 * d + d) * kFacesDim;  // HeatCond_DFDB(d, face, d)
         const double Coeff = (1.0 / a.dx[d]) / a.V;
-        const double DiffLeft = Coeff * Kdd[r[d]], DiffRight = Coeff * Kdd[r[d] + (d == 0 ? 1 : (d == 1 ? kNB : kNB * kNB))];
+        const double DiffLeft = Coeff * Kdd[r[d]], DiffRight = Coeff * Kdd[r[d] + 64];
         sumJ = sumJ - (DiffLeft + DiffRight);
         lo[d] = Cs * DiffLeft;
       }
@@ -501,6 +526,8 @@ void free_heat() {
   if (H.coef) cudaFree(H.coef);
   if (H.wtab) cudaFree(H.wtab);
   if (H.cnt) cudaFree(H.cnt);
+  if (H.errDev) cudaFree(H.errDev);
+  H.errDev = nullptr;
   H.coef = nullptr;
   H.wtab = nullptr;
   H.cnt = nullptr;
@@ -516,7 +543,7 @@ int dotd(const double *x, const double *y, double *out, cudaStream_t st) {
 }
 
 int matvec(const double *x, double *y, cudaStream_t st) {
-  k_heat_apply<<<H.nBlock, 512, 0, st>>>(H.a, x, H.K, H.used, y, kModeMatvec);
+  k_heat_apply<<<H.nBlock, 512, kApplySmem, st>>>(H.a, x, H.K, H.used, y, kModeMatvec);
   CKH(cudaGetLastError());
   H.nMatvec++;
   return BX_OK;
@@ -664,6 +691,18 @@ int update_coef(cudaStream_t st) {
   return BX_OK;
 }
 
+// BX_ERR_TIMEOUT when a kernel's bounded wait gave up (the flag is cleared)
+int check_device_error(cudaStream_t st) {
+  int e = 0;
+  CKH(cudaMemcpyAsync(&e, H.errDev, sizeof(int), cudaMemcpyDeviceToHost, st));
+  CKH(cudaStreamSynchronize(st));
+  if (e) {
+    CKH(cudaMemsetAsync(H.errDev, 0, sizeof(int), st));
+    return core_fail(BX_ERR_TIMEOUT, "a bounded wait for a bulk copy gave up in the heat conduction kernels");
+  }
+  return BX_OK;
+}
+
 int need_heat() {
   if (!H.ready) return core_fail(BX_ERR_STATE, "bx_heat_init has not been called");
   return BX_OK;
@@ -678,7 +717,7 @@ int copy_out(double *h, const double *d) {
   Core c = core();
   CKH(cudaMemcpyAsync(h, d, sizeof(double) * H.nCell, cudaMemcpyDeviceToHost, c.st));
   CKH(cudaStreamSynchronize(c.st));
-  return BX_OK;
+  return check_device_error(c.st);
 }
 
 }  // namespace
@@ -712,6 +751,8 @@ int bx_heat_init(const bx_heat_params *prm, const double *Te, const double *bhat
     H.a.gA[d] = -0.25 * H.a.invDx[d];
     H.a.gC[d] = 0.25 * H.a.invDx[d];
   }
+  H.a.invV = 1.0 / H.a.V;
+  H.a.cvDt = prm->Cv / prm->Dt;
   H.a.f = prm->FractionFieldAligned;
   H.a.cv = prm->Cv;
   H.a.dt = prm->Dt;
@@ -727,6 +768,7 @@ int bx_heat_init(const bx_heat_params *prm, const double *Te, const double *bhat
        cudaMalloc(&H.usedM, sizeof(unsigned) * H.nGroup * kNC) == cudaSuccess &&
        cudaMalloc(&H.K, sizeof(double) * kKBlock * H.nBlock) == cudaSuccess &&
        cudaMalloc(&H.wtab, sizeof(WaveTable)) == cudaSuccess && cudaMalloc(&H.cnt, sizeof(unsigned)) == cudaSuccess &&
+       cudaMalloc(&H.errDev, sizeof(int)) == cudaSuccess &&
        cudaMalloc(&H.V, vb * (prm->nKrylovVector + 1)) == cudaSuccess &&
        cudaMalloc(&H.used, H.nCell) == cudaSuccess &&
        cudaMalloc(&H.blkAt, sizeof(int) * atH.size()) == cudaSuccess &&
@@ -749,6 +791,9 @@ int bx_heat_init(const bx_heat_params *prm, const double *Te, const double *bhat
   static const WaveTable wt = make_wave_table();
   CKH(cudaMemcpyAsync(H.wtab, &wt, sizeof(WaveTable), cudaMemcpyHostToDevice, c.st));
   CKH(cudaMemsetAsync(H.cnt, 0, sizeof(unsigned), c.st));
+  CKH(cudaMemsetAsync(H.errDev, 0, sizeof(int), c.st));
+  H.a.err = H.errDev;
+  CKH(cudaFuncSetAttribute(k_heat_apply, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kApplySmem));
   CKH(cudaMemsetAsync(H.coef, 0, 2 * sizeof(double4) * H.nIl, c.st));
   {
     std::vector<unsigned> um((size_t)H.nGroup * kNC, 0u);
@@ -769,7 +814,7 @@ int bx_advance_semi_impl(bx_krylov_stats *stats) {
   if (r) return r;
   Core c = core();
   CKH(cudaEventRecord(H.ev[0], c.st));
-  k_heat_apply<<<H.nBlock, 512, 0, c.st>>>(H.a, H.Te, H.K, H.used, H.b, kModeRhs);
+  k_heat_apply<<<H.nBlock, 512, kApplySmem, c.st>>>(H.a, H.Te, H.K, H.used, H.b, kModeRhs);
   if (H.p.TypePrecond == BX_PRECOND_BILU) {
     k_heat_factor<<<(H.nBlock + kWarpsPerCta - 1) / kWarpsPerCta, 32 * kWarpsPerCta, 0, c.st>>>(
         H.a, H.K, H.used, H.wtab, H.coef, H.coef + H.nIl, H.nBlock);
@@ -782,6 +827,7 @@ int bx_advance_semi_impl(bx_krylov_stats *stats) {
   CKH(cudaGetLastError());
   CKH(cudaEventRecord(H.ev[1], c.st));
   CKH(cudaEventSynchronize(H.ev[1]));
+  if ((r = check_device_error(c.st))) return r;
   if (stats) {
     float ms = 0;
     cudaEventElapsedTime(&ms, H.ev[0], H.ev[1]);
@@ -808,7 +854,7 @@ int bx_heat_get_rhs(double *b) {
   if (r) return r;
   if (!b) return core_fail(BX_ERR_ARG, "null argument");
   Core c = core();
-  k_heat_apply<<<H.nBlock, 512, 0, c.st>>>(H.a, H.Te, H.K, H.used, H.b, kModeRhs);
+  k_heat_apply<<<H.nBlock, 512, kApplySmem, c.st>>>(H.a, H.Te, H.K, H.used, H.b, kModeRhs);
   CKH(cudaGetLastError());
   return copy_out(b, H.b);
 }

@@ -65,4 +65,14 @@ __device__ __forceinline__ void tma_load_5d(void *dst, const CUtensorMap *map, u
       : "memory");
 }
 
+// untiled bulk copy of bytes (a multiple of 16, both addresses 16-byte
+// aligned) from this GPU's global memory into shared memory, completion
+// counted on bar
+__device__ __forceinline__ void bulk_load(void *dst, const void *src, uint32_t bytes, uint64_t *bar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(smem_u32(dst)),
+      "l"(reinterpret_cast<uint64_t>(src)), "r"(bytes), "r"(smem_u32(bar))
+      : "memory");
+}
+
 }  // namespace bx

@@ -337,9 +337,10 @@ def run_heat(args, lrank):
            "blocks": g.nBlock, "used_fraction": float(used.mean()), "solves": args.heat_steps,
            "warmup": args.heat_warmup, "unit": "s/solve", "higher_is_better": False}
     for prec in args.heat_precond.split(","):
-        x = ExplicitSolver(g, Scheme(), device=lrank)
-        h = HeatSolver(x, HeatParams(typePrecond=prec), Te, b, used)
+        x = None
         try:
+            x = ExplicitSolver(g, Scheme(), device=lrank)
+            h = HeatSolver(x, HeatParams(typePrecond=prec), Te, b, used)
             for _ in range(args.heat_warmup):
                 h.advance_semi_impl()
             x.synchronize()
@@ -348,7 +349,8 @@ def run_heat(args, lrank):
             ms = x.region_end()
         except BxError as e:
             out[prec.lower()] = {"failed": str(e)}
-            x.close()
+            if x is not None:
+                x.close()
             continue
         out[prec.lower()] = {"s_per_solve": ms * 1e-3 / args.heat_steps,
                              "matvec_per_solve": float(np.mean([q["nMatvec"] for q in stats])),
