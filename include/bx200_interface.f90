@@ -11,7 +11,7 @@
 ! Fortran compiler is installed where they run).
 module bx200_interface
 
-  use, intrinsic :: iso_c_binding, only: c_int, c_double, c_ptr, c_char
+  use, intrinsic :: iso_c_binding, only: c_int, c_double, c_ptr, c_char, c_signed_char
 
   implicit none
 
@@ -47,6 +47,13 @@ module bx200_interface
      integer(c_int):: nMatvec, iError
      real(c_double):: Error, Dt, msStep, msPrecondSetup
   end type bx_krylov_stats
+
+  type, bind(C):: bx_heat_params
+     real(c_double):: HeatCondPar, FractionFieldAligned, Cv, Dt, SemiImplCoeff
+     integer(c_int):: nKrylovVector, MaxMatvec
+     real(c_double):: ErrorMax
+     integer(c_int):: TypePrecond
+  end type bx_heat_params
 
   type, bind(C):: bx_scheme_params
      integer(c_int):: nOrder, nStage, TypeFlux, TypeLimiter
@@ -196,6 +203,22 @@ module bx200_interface
        real(c_double), value:: TimeSimulationLimit
        type(bx_krylov_stats), intent(out):: Stats
      end function bx_advance_part_impl
+
+     ! advance_semi_impl (src/ModSemiImplicit.f90:240), TypeSemiImplicit = parcond
+     integer(c_int) function bx_heat_init(Params, Te, Bhat, Used) bind(C, name='bx_heat_init')
+       import:: c_int, c_double, c_signed_char, bx_heat_params
+       type(bx_heat_params), intent(in):: Params
+       real(c_double), intent(in):: Te(*), Bhat(*)
+       integer(c_signed_char), intent(in):: Used(*)
+     end function bx_heat_init
+     integer(c_int) function bx_advance_semi_impl(Stats) bind(C, name='bx_advance_semi_impl')
+       import:: c_int, bx_krylov_stats
+       type(bx_krylov_stats), intent(out):: Stats
+     end function bx_advance_semi_impl
+     integer(c_int) function bx_heat_get_te(Te) bind(C, name='bx_heat_get_te')
+       import:: c_int, c_double
+       real(c_double), intent(out):: Te(*)
+     end function bx_heat_get_te
   end interface
 
 end module bx200_interface
