@@ -204,6 +204,9 @@ def grid_desc(grid, device=0):
 
 
 def scheme_params(s):
+    if getattr(s, "useNonConservative", False):
+        raise ValueError("#NONCONSERVATIVE (the pressure equation) is not on the GPU path: "
+                         "bx_update_state_fast solves for the energy")
     p = SchemeParams()
     p.nOrder = s.nOrder
     p.nStage = s.nStage

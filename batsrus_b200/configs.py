@@ -40,6 +40,37 @@ def shocktube_1d_golden():
     return g, s, st, {"nStep": 512, "tSimulationMax": 25.6}
 
 
+def fast_wave_golden():
+    """Param/SHOCKTUBE/PARAM.in.fast_wave (Makefile.test:439-459) on its
+    root grid: 5 x 5 x 20 blocks of 10^3 cells, [-45.255, 45.255]^2 x
+    [-181.02, 181.02], periodic; the uniform state rho = 1, u = (0, 0,
+    0.005), B = (0, 0.04, 0), p = 4.5e-4 with the fast-wave perturbations
+    (lambda = 32) rotated by 45 degrees (ShockSlope = 1); fixed time step 0.5
+    (Cfl = 1 with a fixed step), the pressure equation (#NONCONSERVATIVE),
+    Powell source; three sessions: Rusanov first order to t = 25, Rusanov
+    second order mc3 (beta 1.2) to t = 50, Linde mc3 to t = 75.  The
+    reference run also refines the two root blocks that touch the box
+    [-1, 1]^3; this grid has no refinement, so a comparison excludes the
+    refined patch and its surroundings."""
+    g = BlockGrid.uniform(3, (10, 10, 10), (5, 5, 20), (-45.255, -45.255, -181.02),
+                          (45.255, 45.255, 181.02), ("periodic",) * 6)
+    base = dict(cfl=1.0, gamma=5.0 / 3.0, useDivbSource=True, useDtFixed=True, dtFixed=0.5,
+                useHalfStep=True, useNonConservative=True)
+    sessions = [
+        (Scheme(nOrder=1, nStage=1, typeFlux="Rusanov", typeLimiter="no", **base), 25.0),
+        (Scheme(nOrder=2, nStage=2, typeFlux="Rusanov", typeLimiter="mc3", limiterBeta=1.2, **base), 50.0),
+        (Scheme(nOrder=2, nStage=2, typeFlux="Linde", typeLimiter="mc3", limiterBeta=1.2, **base), 75.0),
+    ]
+    waves = [("Rho", 1000.0, 0.1, 32.0, -1.0, -1.0, 0.0),
+             ("Ux", 1000.0, 0.005, 32.0, -1.0, -1.0, 0.0),
+             ("Uz", 1000.0, 0.0001, -1.0, -1.0, 32.0, 0.0),
+             ("Bx", 1000.0, 0.0004, 32.0, -1.0, -1.0, 0.0),
+             ("By", 1000.0, 0.004, 32.0, -1.0, -1.0, 0.0),
+             ("p", 10000.0, 7.5e-5, 32.0, -1.0, -1.0, 0.0)]
+    st = initial.uniform_waves(g, [1.0, 0.0, 0.0, 0.005, 0.0, 0.04, 0.0, 4.5e-4], waves, shock_slope=1.0)
+    return g, sessions, st
+
+
 def brio_wu_1d(nBlock=32):
     g = BlockGrid.uniform(1, (8, 1, 1), (nBlock, 1, 1), (-0.5, -0.5, -0.5), (0.5, 0.5, 0.5),
                           ("float",) * 6)

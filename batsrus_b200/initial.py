@@ -125,3 +125,69 @@ def perturbed_ot(grid, seed=2024, amplitude=1e-2, kmax=8):
         else:
             prim[..., v] += amplitude * field
     return _from_primitive(prim)
+
+
+# primitive variable order of the wave tables below
+_PRIM = {"rho": 0, "ux": 1, "uy": 2, "uz": 3, "bx": 4, "by": 5, "bz": 6, "p": 7}
+
+
+def uniform_waves(grid, state, waves, shock_slope=0.0):
+    """#UNIFORMSTATE + #WAVE perturbations with #SHOCKPOSITION's slope
+    (set_initial_condition, apply_wave and rotate_wave of
+    src/ModSetInitialCondition.f90:195-528).
+
+    ``state`` is the primitive uniform state; each wave is (name, width,
+    amplitude, lambda_x, lambda_y, lambda_z, phase in degrees), a negative
+    wavelength meaning no variation along that axis.  With a nonzero slope
+    the vector variables of the uniform state, the wave amplitudes of the
+    vector pairs (x, y) and all wave vectors are rotated by atan(slope) in
+    the x-y plane; a vector pair with a wave on one component only copies
+    that wave's width, wave vector, phase and power to the other component
+    first (copy_wave)."""
+    nV = 8
+    width = np.zeros(nV)
+    ampl = np.zeros(nV)
+    kx = np.zeros(nV)
+    ky = np.zeros(nV)
+    kz = np.zeros(nV)
+    phase = np.zeros(nV)
+    for name, w, a, lx, ly, lz, ph in waves:
+        v = _PRIM[name.lower()]
+        width[v], ampl[v], phase[v] = w, a, ph * math.pi / 180.0
+        kx[v] = max(0.0, 2.0 * math.pi / lx)
+        ky[v] = max(0.0, 2.0 * math.pi / ly)
+        kz[v] = max(0.0, 2.0 * math.pi / lz)
+    prim0 = np.array(state, dtype=np.float64)
+    if shock_slope != 0.0:
+        c = 1.0 / math.sqrt(1.0 + shock_slope ** 2)
+        s = shock_slope * c
+        for vx in (1, 4):  # (Ux, Uy) and (Bx, By)
+            vy = vx + 1
+            for src, dst in ((vx, vy), (vy, vx)):
+                if width[src] > 0.0 and width[dst] == 0.0:
+                    width[dst], kx[dst], ky[dst], kz[dst], phase[dst] = \
+                        width[src], kx[src], ky[src], kz[src], phase[src]
+            x, y = ampl[vx], ampl[vy]
+            ampl[vx], ampl[vy] = c * x - s * y, s * x + c * y
+            x, y = prim0[vx], prim0[vy]
+            prim0[vx], prim0[vy] = c * x - s * y, s * x + c * y
+        x, y = kx.copy(), ky.copy()
+        kx, ky = c * x - s * y, s * x + c * y
+    xyz = grid.cell_centers()
+    X, Y, Z = xyz[..., 0], xyz[..., 1], xyz[..., 2]
+    prim = np.empty(grid.state_shape_fortran())
+    prim[...] = prim0
+    for v in range(nV):
+        if ampl[v] == 0.0:
+            continue
+        inside = np.ones(X.shape, dtype=bool)
+        if width[v] > 0.0:
+            if kx[v] > 0.0:
+                inside = np.abs(X + shock_slope * Y) <= width[v]
+            elif ky[v] > 0.0:
+                inside = np.abs(Y) <= width[v]
+            elif kz[v] > 0.0:
+                inside = np.abs(Z) <= width[v]
+        wave = ampl[v] * np.cos(phase[v] + kx[v] * X + ky[v] * Y + kz[v] * Z)
+        prim[..., v] = np.where(inside, prim[..., v] + wave, prim[..., v])
+    return _from_primitive(prim)

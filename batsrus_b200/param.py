@@ -90,6 +90,7 @@ class Scheme:
     useHalfStep: bool = True
     isTimeAccurate: bool = True
     precision: str = "fp64"  # 'fp64' | 'fp32'
+    useNonConservative: bool = False  # #NONCONSERVATIVE (oracle only; the GPU path solves for energy)
 
 
 @dataclass

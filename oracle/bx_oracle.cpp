@@ -766,6 +766,7 @@ struct Oracle {
   // (:862-977) and calc_divb_source (:1694-1891)
   void calc_source(int b, Scratch &s) {
     std::fill(s.Source.begin(), s.Source.end(), 0.0);
+    if (c.useNonConservative) adiabatic_source(b, s);
     if (!c.useDivbSource) return;
     double DxInvHalf = 0.5 / dxyz[3 * b], DyInvHalf = 0.5 / dxyz[3 * b + 1], DzInvHalf = 0.5 / dxyz[3 * b + 2];
     for (int k = 1; k <= c.nK; k++)
@@ -804,6 +805,25 @@ struct Oracle {
           for (int m = 0; m < 3; m++) SrcMhd[m] = 0 - DivB1 * U[Bx_ + m];
           Src[Energy_] = Src[Energy_] - DivB1 * (U[Bx_] * u_D[0] + U[By_] * u_D[1] + U[Bz_] * u_D[2]);
           for (int m = 0; m < 3; m++) Src[RhoUx_ + m] = Src[RhoUx_ + m] + SrcMhd[m];
+        }
+  }
+
+  // Adiabatic heating -(g-1) p div(u) of the pressure equation
+  // (#NONCONSERVATIVE; src/ModCalcSource.f90:367-378 with div_u, the
+  // difference of the face normal velocities times Area over the volume)
+  void adiabatic_source(int b, Scratch &s) {
+    const double V = cellVolume(b);
+    for (int k = 1; k <= c.nK; k++)
+      for (int j = 1; j <= c.nJ; j++)
+        for (int i = 1; i <= c.nI; i++) {
+          double DivU = s.Flux[0][nFaceValue * face(0, i + 1, j, k) + Un_] - s.Flux[0][nFaceValue * face(0, i, j, k) + Un_];
+          if (c.nJ > 1)
+            DivU = DivU + s.Flux[1][nFaceValue * face(1, i, j + 1, k) + Un_] - s.Flux[1][nFaceValue * face(1, i, j, k) + Un_];
+          if (c.nK > 1)
+            DivU = DivU + s.Flux[2][nFaceValue * face(2, i, j, k + 1) + Un_] - s.Flux[2][nFaceValue * face(2, i, j, k) + Un_];
+          DivU = DivU / V;
+          double *Src = &s.Source[(nVar + 1) * icell(i, j, k)];
+          Src[P_] = Src[P_] - GammaMinus1 * st(b, i, j, k)[P_] * DivU;
         }
   }
 
@@ -861,8 +881,13 @@ struct Oracle {
             if (fz0) sum = sum + fz0[v] - fz1[v];
             Src[v] = DtLocal * (Src[v] + sum / V);
           }
-          // pressure_to_energy(StateOld) (src/ModEnergy.f90:47)
           double *O = so(b, i, j, k);
+          if (c.useNonConservative) {  // pressure equation: no energy conversion
+            double *U = st(b, i, j, k);
+            for (int v = 0; v < nVar; v++) U[v] = O[v] + Src[v];
+            continue;
+          }
+          // pressure_to_energy(StateOld) (src/ModEnergy.f90:47)
           O[P_] = InvGammaMinus1 * O[P_] + 0.5 * (O[RhoUx_] * O[RhoUx_] + O[RhoUy_] * O[RhoUy_] + O[RhoUz_] * O[RhoUz_]) / O[Rho_];
           O[P_] = O[P_] + 0.5 * (O[Bx_] * O[Bx_] + O[By_] * O[By_] + O[Bz_] * O[Bz_]);
           Src[P_] = Src[Energy_];

@@ -42,6 +42,7 @@ typedef struct {
   double dtFixed;
   int useHalfStep;     /* #TIMESTEPPING / #SCHEME with nStage<=2 */
   int nThread;         /* OpenMP threads (0 = default) */
+  int useNonConservative; /* #NONCONSERVATIVE: pressure equation instead of energy */
 } ora_config;
 
 /* Create an oracle grid. iLevelCoord holds 4 ints per block: level and the

@@ -35,6 +35,7 @@ class OraConfig(ctypes.Structure):
         ("useDtFixed", ctypes.c_int), ("dtFixed", ctypes.c_double),
         ("useHalfStep", ctypes.c_int),
         ("nThread", ctypes.c_int),
+        ("useNonConservative", ctypes.c_int),
     ]
 
 
@@ -109,6 +110,7 @@ class Oracle:
         c.dtFixed = scheme.dtFixed
         c.useHalfStep = int(scheme.useHalfStep)
         c.nThread = n_thread
+        c.useNonConservative = int(getattr(scheme, "useNonConservative", False))
         self.cfg = c
         self.grid = grid
         lc = np.ascontiguousarray(grid.iLevelCoord, dtype=np.int32)

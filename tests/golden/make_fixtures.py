@@ -29,6 +29,18 @@ def main(ref):
                         tolerance_rel=1e-5, tolerance_abs=1e-11)
     print("wrote mhdhyp_1d_ref.npz", d["var"].shape)
 
+    # Param/SHOCKTUBE/PARAM.in.fast_wave (Makefile.test:439-459): the z=0 cut
+    # at step 150, t = 75; DiffNum tolerances -r=1e-3 -a=1e-6
+    src = os.path.join(ref, "Param/SHOCKTUBE/TestOutput/fast_wave_ref.out")
+    d = read_idl_ascii(src)
+    cols = [d["varnames"].index(v) for v in VARS]
+    np.savez_compressed(os.path.join(HERE, "fast_wave_ref.npz"),
+                        xy=d["coord"][:, :2], prim=d["var"][:, cols], names=np.array(VARS),
+                        nStep=d["nStep"], time=d["time"], gamma=d["params"][0],
+                        source="Param/SHOCKTUBE/TestOutput/fast_wave_ref.out",
+                        tolerance_rel=1e-3, tolerance_abs=1e-6)
+    print("wrote fast_wave_ref.npz", d["var"].shape)
+
 
 if __name__ == "__main__":
     main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")

@@ -115,3 +115,63 @@ def test_oracle_jfnk_step_solves_its_krylov_system():
         assert np.linalg.norm(res) <= 1.05e-3 * np.linalg.norm(rhs)
         counts[prec] = nm
     assert counts["bilu"] < counts["none"]
+
+
+def test_oracle_matches_reference_fast_wave_golden():
+    """Param/SHOCKTUBE/TestOutput/fast_wave_ref.out (Makefile.test:439-459):
+    the 3D fast-wave test of the fast path, 150 steps in three sessions
+    (Rusanov first order, Rusanov second order with the Koren limiter mc3
+    beta = 1.2, Linde with mc3), Powell source, pressure equation, fixed
+    time step, 10^3-cell blocks, periodic.  The reference's z=0 cut is the
+    mean of the two cell layers next to z = 0.  The reference refines the
+    two root blocks at the origin; this grid does not, so the comparison
+    covers the cells farther than 30 from the origin in x or y (1344 of
+    the 2400 coarse points, away from the refined patch's influence):
+    there the oracle matches the golden's printed digits (relative 1e-8),
+    and the DiffNum tolerances (-r=1e-3 -a=1e-6) hold beyond 20."""
+    ref = np.load(os.path.join(GOLDEN, "fast_wave_ref.npz"))
+    g, sessions, st = configs.fast_wave_golden()
+    t, n = 0.0, 0
+    state = st
+    for s, tEnd in sessions:
+        o = Oracle(g, s)
+        o.set_state(state)
+        o.set_time(t, n)
+        o.exchange_messages()
+        o.advance(int(round((tEnd - t) / s.dtFixed)), tEnd)
+        t, _, n = o.time()
+        state = o.get_state()
+    assert n == int(ref["nStep"]) == 150 and abs(t - float(ref["time"])) < 1e-9
+    prim = _prim(state[g.interior_slices()])
+    xyz = g.cell_centers(with_ghost=False)
+    dz = 1.8102
+    layers = []
+    for zc in (-0.5 * dz, 0.5 * dz):
+        m = np.abs(xyz[..., 2] - zc) < 0.1 * dz
+        X, P = xyz[m][:, :2], prim[m]
+        o_ = np.lexsort((X[:, 0], X[:, 1]))
+        layers.append((X[o_], P[o_]))
+    X = layers[0][0]
+    P = 0.5 * (layers[0][1] + layers[1][1])
+    # golden points on the coarse grid
+    cell = np.round((ref["xy"] + 45.255) / dz - 0.5).astype(int)
+    mine = np.round((X + 45.255) / dz - 0.5).astype(int)
+    lut = -np.ones((50, 50), dtype=int)
+    lut[mine[:, 0], mine[:, 1]] = np.arange(len(X))
+    k = lut[cell[:, 0], cell[:, 1]]
+    coarse = np.abs(X[k] - ref["xy"]).max(1) < 1e-3
+    assert coarse.sum() == 2400
+    R, G, XY = ref["prim"][coarse], P[k[coarse]], ref["xy"][coarse]
+    dist = np.maximum(np.abs(XY[:, 0]), np.abs(XY[:, 1]))
+    d = np.abs(G - R)
+    far = dist > 30.0
+    assert far.sum() == 1344
+    # per variable; u and B components against the largest vector magnitude
+    # (Bz stays at round-off level in this problem)
+    scale = np.abs(R[far]).max(0)
+    scale[1:4] = np.sqrt((R[far][:, 1:4] ** 2).sum(1)).max()
+    scale[4:7] = np.sqrt((R[far][:, 4:7] ** 2).sum(1)).max()
+    assert (d[far] / scale).max() < 1e-8, (d[far] / scale).max(0)
+    mid = dist > 20.0
+    bad = (d[mid] > float(ref["tolerance_abs"])) & (d[mid] > float(ref["tolerance_rel"]) * np.abs(R[mid]))
+    assert not bad.any(), bad.sum(0)
