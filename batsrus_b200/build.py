@@ -29,10 +29,11 @@ UNITS = [
     ("bx_learned.cu", []),
     ("bx_noalloc.cu", []),
     ("bx_heat.cu", []),
+    ("bx_tune.cu", []),
     ("bx_capi.cu", []),
 ]
 HEADERS = ["bx_physics.cuh", "bx_stage.cuh", "bx_device.h", "bx_stage3d.cuh", "bx_tma.cuh", "bx_core.h",
-           "bx_impl_kernels.cuh", "bx_krylov.cuh", "bx_tc.cuh", "bx_learned.cuh", "bx_learned_kernels.cuh", "bx_amr.h"]
+           "bx_impl_kernels.cuh", "bx_krylov.cuh", "bx_tune.h", "bx_tc.cuh", "bx_learned.cuh", "bx_learned_kernels.cuh", "bx_amr.h"]
 
 
 def _sources_newer(target, deps):

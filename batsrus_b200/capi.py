@@ -38,6 +38,7 @@ EXPORTS = (
     "bx_impl_norm_noalloc",
     "bx_heat_init", "bx_advance_semi_impl", "bx_heat_get_te", "bx_heat_get_rhs", "bx_heat_matvec",
     "bx_heat_precond",
+    "bx_autotune", "bx_tune_info", "bx_tune_set", "bx_tune_reset",
 )
 PRECOND = {"none": 0, "bilu": 1, "learned": 2}
 NOALLOC_MAX_BLOCK = 32768  # BX_NOALLOC_MAX_BLOCK
@@ -159,6 +160,8 @@ def load():
         "bx_impl_norm_noalloc": [p, i, i, p, dp],
         "bx_heat_init": [ctypes.POINTER(HeatParamsC), dp, dp, ctypes.POINTER(ctypes.c_ubyte)],
         "bx_advance_semi_impl": [ctypes.POINTER(KrylovStats)],
+        "bx_autotune": [], "bx_tune_set": [ctypes.c_char_p, i], "bx_tune_reset": [],
+        "bx_tune_info": [i, ctypes.c_char_p, i, ip, ip, ip, ip, fp],
         "bx_heat_get_te": [dp], "bx_heat_get_rhs": [dp], "bx_heat_matvec": [dp, dp], "bx_heat_precond": [dp, dp],
     }
     for name, args in sig.items():
@@ -221,3 +224,34 @@ def scheme_params(s):
     p.DtFixed = s.dtFixed
     p.Precision = PRECISION[s.precision.lower()]
     return p
+
+
+def tune_info():
+    """The autotuner's knobs: {name: {"value", "tuned", "candidates", "ms"}}."""
+    L = load()
+    out = {}
+    i = 0
+    while True:
+        name = ctypes.create_string_buffer(64)
+        v, t, n = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        cand = (ctypes.c_int * 8)()
+        ms = (ctypes.c_float * 8)()
+        if L.bx_tune_info(i, name, 64, ctypes.byref(v), ctypes.byref(t), ctypes.byref(n), cand, ms) != BX_OK:
+            break
+        out[name.value.decode()] = {"value": v.value, "tuned": t.value, "candidates": list(cand[:n.value]),
+                                    "ms": [round(float(x), 4) for x in ms[:n.value]]}
+        i += 1
+    return out
+
+
+def tune_set(name, value):
+    check(load().bx_tune_set(name.encode(), int(value)))
+
+
+def tune_reset():
+    check(load().bx_tune_reset())
+
+
+def autotune():
+    check(load().bx_autotune())
+    return tune_info()

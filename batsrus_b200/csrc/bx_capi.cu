@@ -19,6 +19,7 @@
 #include "../../include/bx200.h"
 #include "bx_amr.h"
 #include "bx_core.h"
+#include "bx_tune.h"
 #include "bx_device.h"
 
 using namespace bx;
@@ -362,6 +363,59 @@ int launch_stage(int iStage) {
   return BX_OK;
 }
 
+// autotune the persistent grid of the stage kernel: time stage-1 launches
+// (they write only the stage buffer, the block time steps and the step
+// state, which are restored) for each candidate number of CTAs per SM
+int tune_stage_impl() {
+  TuneKnobInfo &k = tune_knob(kTuneStageGrid);
+  if (!g.ready || !g.use3d || k.tuned == 2) return BX_OK;
+  StepState saved;
+  std::vector<double> dtSaved(g.nBlock);
+  CK(cudaMemcpyAsync(&saved, g.ts, sizeof(StepState), cudaMemcpyDeviceToHost, g.st));
+  CK(cudaMemcpyAsync(dtSaved.data(), g.dtBlock, sizeof(double) * g.nBlock, cudaMemcpyDeviceToHost, g.st));
+  CK(cudaStreamSynchronize(g.st));
+  const int v0 = k.value;
+  float best = 1e30f;
+  int bestV = v0;
+  cudaEvent_t e0, e1;
+  CK(cudaEventCreate(&e0));
+  CK(cudaEventCreate(&e1));
+  int r = BX_OK;
+  for (int i = 0; i < k.nCand && !r; i++) {
+    k.value = k.cand[i];
+    StageArgs a = stage_args(1, g.sch.nStage == 1);
+    const int kind = g.sch.Precision == BX_FP64 ? kKindFp64 : kKindFp32In64;
+    const TmaMaps *m = g.sch.Precision == BX_FP64 ? (a.in == g.bufX ? &g.mapX64 : &g.mapY64) : &g.mapX64;
+    cudaError_t e = cudaSuccess;
+    for (int rep = 0; rep < 4 && e == cudaSuccess; rep++) {
+      if (rep == 1) e = cudaEventRecord(e0, g.st);
+      if (e == cudaSuccess && g.nSlab)
+        e = launch_reschange(g.shape, g.sch.TypeFlux, kind, a, g.slabs, g.nSlab, g.lcDev,
+                             make_int3(g.nRoot[0], g.nRoot[1], g.nRoot[2]), g.rcGhost, g.rcFlux, g.st);
+      if (e == cudaSuccess) e = launch_stage3d(g.shape, g.sch.TypeFlux, kind, *m, a, g.nSM, g.st);
+    }
+    if (e == cudaSuccess) e = cudaEventRecord(e1, g.st);
+    if (e == cudaSuccess) e = cudaEventSynchronize(e1);
+    float ms = 0;
+    if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, e0, e1);
+    if (e != cudaSuccess) {
+      r = fail(BX_ERR_CUDA, "autotune of the stage kernel: %s", cudaGetErrorString(e));
+      break;
+    }
+    k.ms[i] = ms / 3;
+    if (k.ms[i] < best) { best = k.ms[i]; bestV = k.cand[i]; }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  k.value = r ? v0 : bestV;
+  if (!r) k.tuned = 1;
+  CK(cudaMemcpyAsync(g.ts, &saved, sizeof(StepState), cudaMemcpyHostToDevice, g.st));
+  CK(cudaMemcpyAsync(g.dtBlock, dtSaved.data(), sizeof(double) * g.nBlock, cudaMemcpyHostToDevice, g.st));
+  CK(cudaStreamSynchronize(g.st));
+  if (g.graph) { cudaGraphExecDestroy(g.graph); g.graph = nullptr; }  // captured with the old grid
+  return r;
+}
+
 int launch_step(double tLimit) {
   set_dt_kernel<<<1, 1, 0, g.st>>>(g.ts, tLimit, g.sch.UseDtFixed, g.sch.DtFixed, g.sch.Cfl);
   CK(cudaGetLastError());
@@ -462,6 +516,7 @@ int core_fail(int code, const char *fmt, ...) {
   return code;
 }
 int core_encode_maps(void *base, bool fp32, TmaMaps &m) { return encode_maps(base, fp32, g.nI, g.nBlock, m); }
+int tune_stage() { return tune_stage_impl(); }
 }  // namespace bx
 
 // ===========================================================================

@@ -34,6 +34,7 @@
 #include "bx_core.h"
 #include "bx_krylov.cuh"
 #include "bx_tma.cuh"
+#include "bx_tune.h"
 
 using namespace bx;
 
@@ -387,11 +388,19 @@ __device__ __forceinline__ void load_row(IluRow &row, const double4 *__restrict_
   }
 }
 
-__global__ void __launch_bounds__(32) k_heat_ilu(const double4 *__restrict__ coefL, const double4 *__restrict__ coefU,
-                                                 const unsigned *__restrict__ usedM, const double *__restrict__ r,
-                                                 double *__restrict__ yI, double *__restrict__ z, int nBlock) {
-  __shared__ double plane[2][64 * 32];
-  const int g = blockIdx.x, lane = threadIdx.x;
+// W warps per CTA (autotuned), each with its own group of 32 blocks and
+// its two plane buffers (32 KB) in dynamic shared memory
+template <int W>
+__global__ void __launch_bounds__(32 * W) k_heat_ilu(const double4 *__restrict__ coefL,
+                                                     const double4 *__restrict__ coefU,
+                                                     const unsigned *__restrict__ usedM,
+                                                     const double *__restrict__ r, double *__restrict__ yI,
+                                                     double *__restrict__ z, int nBlock, int nGroup) {
+  extern __shared__ double dyn[];
+  const int wp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int g = blockIdx.x * W + wp;
+  if (g >= nGroup) return;  // the warps work independently (no CTA barrier)
+  double(*plane)[64 * 32] = reinterpret_cast<double(*)[64 * 32]>(dyn + (size_t)wp * 2 * 64 * 32);
   const long gb = (long)g * 32;  // first block of the group
   const unsigned *um = usedM + (long)g * kNC;
   const double4 *cL = coefL + (long)g * kNC * 32 + lane, *cU = coefU + (long)g * kNC * 32 + lane;
@@ -506,6 +515,28 @@ __global__ void k_h_te_update(double *Te, const double *x, const unsigned char *
     if (used[q]) Te[q] = Te[q] + x[q];
 }
 
+template <int W>
+cudaError_t launch_ilu_w(const double *r, double *z, cudaStream_t st) {
+  constexpr size_t smem = sizeof(double) * W * 2 * 64 * 32;
+  static bool attr = false;
+  if (!attr) {
+    const cudaError_t e = cudaFuncSetAttribute(k_heat_ilu<W>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    attr = true;
+  }
+  k_heat_ilu<W><<<(H.nGroup + W - 1) / W, 32 * W, smem, st>>>(H.coef, H.coef + H.nIl, H.usedM, r, H.yI, z,
+                                                               H.nBlock, H.nGroup);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_ilu(int w, const double *r, double *z, cudaStream_t st) {
+  switch (w) {
+    case 2: return launch_ilu_w<2>(r, z, st);
+    case 4: return launch_ilu_w<4>(r, z, st);
+    default: return launch_ilu_w<1>(r, z, st);
+  }
+}
+
 void free_heat() {
   for (double **p : {&H.Te, &H.HC, &H.B3, &H.b, &H.x, &H.w, &H.t, &H.r, &H.V, &H.partial, &H.scal}) {
     if (*p) cudaFree(*p);
@@ -551,7 +582,8 @@ int matvec(const double *x, double *y, cudaStream_t st) {
 
 int precond(const double *r, double *z, cudaStream_t st) {
   if (H.p.TypePrecond == BX_PRECOND_BILU) {
-    k_heat_ilu<<<H.nGroup, 32, 0, st>>>(H.coef, H.coef + H.nIl, H.usedM, r, H.yI, z, H.nBlock);
+    const cudaError_t e = launch_ilu(tune_value(kTuneHeatIluWarps), r, z, st);
+    if (e != cudaSuccess) return core_fail(BX_ERR_CUDA, "heat ILU launch: %s", cudaGetErrorString(e));
   } else if (H.p.TypePrecond == BX_PRECOND_NONE) {
     CKH(cudaMemcpyAsync(z, r, sizeof(double) * H.nCell, cudaMemcpyDeviceToDevice, st));
   } else {
@@ -582,7 +614,7 @@ int gmres(int &iError, cudaStream_t st) {
   double beta = beta0;
   std::vector<double> Hm((m + 1) * m), cs(m), sn(m), g(m + 1), y(m), hb(m + 2);
   while (true) {
-    k_kry_scale<<<kKryBlocks, kKryThreads, 0, st>>>(Vb, H.r, H.scal + 2, 1, N);
+    k_kry_scale<<<kry_grid(), kKryThreads, 0, st>>>(Vb, H.r, H.scal + 2, 1, N);
     CKH(cudaGetLastError());
     std::fill(g.begin(), g.end(), 0.0);
     g[0] = beta;
@@ -603,7 +635,7 @@ int gmres(int &iError, cudaStream_t st) {
       CKH(cudaStreamSynchronize(st));
       const double hn = std::sqrt(hb[k + 1]);
       if (hn != 0.0) {
-        k_kry_scale<<<kKryBlocks, kKryThreads, 0, st>>>(Vb + (size_t)(k + 1) * N, H.w, hdev + k + 1, 1, N);
+        k_kry_scale<<<kry_grid(), kKryThreads, 0, st>>>(Vb + (size_t)(k + 1) * N, H.w, hdev + k + 1, 1, N);
         CKH(cudaGetLastError());
       }
       for (int q = 0; q <= k; q++) Hm[q * m + k] = hb[q];
@@ -634,7 +666,7 @@ int gmres(int &iError, cudaStream_t st) {
       y[q] = s / Hm[q * m + q];
     }
     CKH(cudaMemcpyAsync(H.scal + 80, y.data(), sizeof(double) * kdone, cudaMemcpyHostToDevice, st));
-    k_kry_update<<<kKryBlocks, kKryThreads, 0, st>>>(H.x, Vb, H.scal + 80, kdone, N);
+    k_kry_update<<<kry_grid(), kKryThreads, 0, st>>>(H.x, Vb, H.scal + 80, kdone, N);
     CKH(cudaGetLastError());
     if (conv) return BX_OK;
     if (H.nMatvec >= H.p.MaxMatvec) { iError = 1; return BX_OK; }
@@ -726,6 +758,35 @@ void bx::heat_release() {
   if (H.ready) free_heat();
 }
 
+// autotune the warps per CTA of the ILU sweeps on the current system
+int bx::tune_heat() {
+  TuneKnobInfo &k = tune_knob(kTuneHeatIluWarps);
+  if (!H.ready || H.p.TypePrecond != BX_PRECOND_BILU || k.tuned == 2) return BX_OK;
+  Core c = core();
+  k_heat_apply<<<H.nBlock, 512, kApplySmem, c.st>>>(H.a, H.Te, H.K, H.used, H.b, kModeRhs);
+  k_heat_factor<<<(H.nBlock + kWarpsPerCta - 1) / kWarpsPerCta, 32 * kWarpsPerCta, 0, c.st>>>(
+      H.a, H.K, H.used, H.wtab, H.coef, H.coef + H.nIl, H.nBlock);
+  CKH(cudaGetLastError());
+  cudaEvent_t e0 = H.ev[0], e1 = H.ev[1];
+  float best = 1e30f;
+  int bestV = k.value;
+  for (int i = 0; i < k.nCand; i++) {
+    cudaError_t e = launch_ilu(k.cand[i], H.b, H.t, c.st);
+    if (e == cudaSuccess) e = cudaEventRecord(e0, c.st);
+    for (int rep = 0; rep < 3 && e == cudaSuccess; rep++) e = launch_ilu(k.cand[i], H.b, H.t, c.st);
+    if (e == cudaSuccess) e = cudaEventRecord(e1, c.st);
+    if (e == cudaSuccess) e = cudaEventSynchronize(e1);
+    float ms = 0;
+    if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, e0, e1);
+    if (e != cudaSuccess) return core_fail(BX_ERR_CUDA, "autotune of the heat ILU: %s", cudaGetErrorString(e));
+    k.ms[i] = ms / 3;
+    if (k.ms[i] < best) { best = k.ms[i]; bestV = k.cand[i]; }
+  }
+  k.value = bestV;
+  k.tuned = 1;
+  return check_device_error(c.st);
+}
+
 extern "C" {
 
 int bx_heat_init(const bx_heat_params *prm, const double *Te, const double *bhat, const unsigned char *used) {
@@ -773,7 +834,7 @@ int bx_heat_init(const bx_heat_params *prm, const double *Te, const double *bhat
        cudaMalloc(&H.used, H.nCell) == cudaSuccess &&
        cudaMalloc(&H.blkAt, sizeof(int) * atH.size()) == cudaSuccess &&
        cudaMalloc(&H.blkXYZ, sizeof(int) * xyzH.size()) == cudaSuccess &&
-       cudaMalloc(&H.partial, sizeof(double) * kKryBlocks) == cudaSuccess &&
+       cudaMalloc(&H.partial, sizeof(double) * kKryMaxBlocks) == cudaSuccess &&
        cudaMalloc(&H.scal, sizeof(double) * 160) == cudaSuccess;
   if (!ok) {
     free_heat();

@@ -24,6 +24,7 @@
 #include "bx_core.h"
 #include "bx_impl_kernels.cuh"
 #include "bx_krylov.cuh"
+#include "bx_tune.h"
 
 using namespace bx;
 
@@ -160,7 +161,8 @@ int precond(const double *r, double *z) {
     BiluArgs b;
     b.Jac = I.Jac; b.Dinv = I.Dinv; b.wfCell = I.wfCell; b.wfStart = I.wfStart; b.nWave = I.nWave;
     b.nBlock = c.nBlock; b.r = r; b.z = z;
-    const int thr = ((8 * I.maxWave + 31) / 32) * 32;
+    const int tv = tune_value(kTuneBiluThreads);  // 0: 8 x the widest wavefront
+    const int thr = tv > 0 ? tv : ((8 * I.maxWave + 31) / 32) * 32;
     if (c.nI == 8) k_bilu_solve<8><<<c.nBlock, thr, 0, c.st>>>(b);
     else k_bilu_solve<4><<<c.nBlock, thr, 0, c.st>>>(b);
     CKI(cudaGetLastError());
@@ -192,7 +194,7 @@ int gmres(int &iError) {
   std::vector<double> H((m + 1) * m), cs(m), sn(m), gv(m + 1), hb(m + 2), y(m);
   double *hdev = I.scal + 8;  // h_0 .. h_{k+1}
   while (true) {
-    k_kry_scale<<<kKryBlocks, kKryThreads, 0, c.st>>>(I.V, rvec, I.scal + 2, 1, N);  // V0 = r/||r||
+    k_kry_scale<<<kry_grid(), kKryThreads, 0, c.st>>>(I.V, rvec, I.scal + 2, 1, N);  // V0 = r/||r||
     CKI(cudaGetLastError());
     std::fill(gv.begin(), gv.end(), 0.0);
     gv[0] = beta;
@@ -214,7 +216,7 @@ int gmres(int &iError) {
       CKI(cudaStreamSynchronize(c.st));
       const double hn = std::sqrt(hb[k + 1]);
       if (hn != 0.0) {
-        k_kry_scale<<<kKryBlocks, kKryThreads, 0, c.st>>>(I.V + (size_t)(k + 1) * N, I.W, hdev + k + 1, 1, N);
+        k_kry_scale<<<kry_grid(), kKryThreads, 0, c.st>>>(I.V + (size_t)(k + 1) * N, I.W, hdev + k + 1, 1, N);
         CKI(cudaGetLastError());
       }
       for (int q = 0; q <= k; q++) H[q * m + k] = hb[q];
@@ -245,7 +247,7 @@ int gmres(int &iError) {
       y[q] = s / H[q * m + q];
     }
     CKI(cudaMemcpyAsync(I.scal + 48, y.data(), sizeof(double) * kdone, cudaMemcpyHostToDevice, c.st));
-    k_kry_update<<<kKryBlocks, kKryThreads, 0, c.st>>>(I.X, I.Z, I.scal + 48, kdone, N);
+    k_kry_update<<<kry_grid(), kKryThreads, 0, c.st>>>(I.X, I.Z, I.scal + 48, kdone, N);
     CKI(cudaGetLastError());
     if (conv) return BX_OK;
     if (I.nMatvec >= I.p.MaxMatvec) { iError = 1; return BX_OK; }
@@ -527,3 +529,36 @@ int bx_learned_collect_probes(int nProbe, int blocksPerPair, unsigned long long 
 }
 
 }  // extern "C"
+
+// autotune the threads per block CTA of the BILU sweeps, on the Jacobian of
+// the last implicit step (the scratch vectors R and W carry the data)
+int bx::tune_bilu() {
+  TuneKnobInfo &k = tune_knob(kTuneBiluThreads);
+  if (!I.ready || I.p.TypePrecond != BX_PRECOND_BILU || !I.havePrec || k.tuned == 2) return BX_OK;
+  Core c = core();
+  cudaEvent_t e0, e1;
+  CKI(cudaEventCreate(&e0));
+  CKI(cudaEventCreate(&e1));
+  const int v0 = k.value;
+  float best = 1e30f;
+  int bestV = v0, r = BX_OK;
+  CKI(cudaMemsetAsync(I.R, 0, sizeof(double) * I.N, c.st));
+  for (int i = 0; i < k.nCand && !r; i++) {
+    k.value = k.cand[i];
+    r = precond(I.R, I.W);
+    if (!r && cudaEventRecord(e0, c.st) != cudaSuccess) r = core_fail(BX_ERR_CUDA, "cudaEventRecord");
+    for (int rep = 0; rep < 3 && !r; rep++) r = precond(I.R, I.W);
+    if (r) break;
+    float ms = 0;
+    if (cudaEventRecord(e1, c.st) != cudaSuccess || cudaEventSynchronize(e1) != cudaSuccess ||
+        cudaEventElapsedTime(&ms, e0, e1) != cudaSuccess)
+      r = core_fail(BX_ERR_CUDA, "autotune of the BILU sweeps");
+    k.ms[i] = ms / 3;
+    if (!r && k.ms[i] < best) { best = k.ms[i]; bestV = k.cand[i]; }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  k.value = r ? v0 : bestV;
+  if (!r) k.tuned = 1;
+  return r;
+}

@@ -7,9 +7,24 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include "bx_tune.h"
+
 namespace bx {
 
-constexpr int kKryBlocks = 148 * 4, kKryThreads = 256;
+// the grid is kTuneKryCtas CTAs per SM (autotuned); partial-sum buffers are
+// sized for the largest candidate
+constexpr int kKryThreads = 256, kKryMaxBlocks = 8 * 160;
+
+inline int kry_grid() {
+  static int nsm = 0;
+  if (!nsm) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || nsm <= 0) nsm = 148;
+  }
+  const int g = tune_value(kTuneKryCtas) * nsm;
+  return g < kKryMaxBlocks ? g : kKryMaxBlocks;
+}
 
 __device__ __forceinline__ double kry_block_sum(double v, double *sh) {
   for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
@@ -47,11 +62,11 @@ __device__ __forceinline__ void kry_finish(double s, double *partial, unsigned *
 }
 
 // modified Gram-Schmidt step: w -= (*hq) vq when VQ, then *out = w . vn
-// (VN) or w . w
-template <bool VQ, bool VN>
-__global__ void __launch_bounds__(kKryThreads, 4) k_kry_mgs_t(double *__restrict__ w, const double *__restrict__ vq,
-                                                              const double *hq, const double *__restrict__ vn, long n,
-                                                              double *partial, unsigned *cnt, double *out) {
+// (VN) or w . w; U independent 16-byte loads per vector in flight per thread
+template <bool VQ, bool VN, int U>
+__global__ void __launch_bounds__(kKryThreads) k_kry_mgs_t(double *__restrict__ w, const double *__restrict__ vq,
+                                                           const double *hq, const double *__restrict__ vn, long n,
+                                                           double *partial, unsigned *cnt, double *out) {
   __shared__ double sh[32];
   const double h = VQ ? *hq : 0.0;
   const long n2 = n >> 1;
@@ -59,24 +74,34 @@ __global__ void __launch_bounds__(kKryThreads, 4) k_kry_mgs_t(double *__restrict
   double2 *w2 = reinterpret_cast<double2 *>(w);
   const double2 *v2 = reinterpret_cast<const double2 *>(vq);
   const double2 *c2 = reinterpret_cast<const double2 *>(vn);
-  double s0 = 0, s1 = 0;
+  double s[U];
+#pragma unroll
+  for (int u = 0; u < U; u++) s[u] = 0.0;
   long q = blockIdx.x * (long)blockDim.x + threadIdx.x;
-  for (; q + stride < n2; q += 2 * stride) {
-    double2 a = w2[q], b = w2[q + stride];
+  for (; q + (U - 1) * stride < n2; q += U * stride) {
+    double2 a[U];
+#pragma unroll
+    for (int u = 0; u < U; u++) a[u] = w2[q + u * stride];
     if (VQ) {
-      const double2 va = __ldcs(v2 + q), vb = __ldcs(v2 + q + stride);
-      a.x = a.x - h * va.x; a.y = a.y - h * va.y;
-      b.x = b.x - h * vb.x; b.y = b.y - h * vb.y;
-      w2[q] = a;
-      w2[q + stride] = b;
+      double2 va[U];
+#pragma unroll
+      for (int u = 0; u < U; u++) va[u] = __ldcs(v2 + q + u * stride);
+#pragma unroll
+      for (int u = 0; u < U; u++) {
+        a[u].x = a[u].x - h * va[u].x;
+        a[u].y = a[u].y - h * va[u].y;
+        w2[q + u * stride] = a[u];
+      }
     }
     if (VN) {
-      const double2 ca = c2[q], cb = c2[q + stride];
-      s0 += a.x * ca.x + a.y * ca.y;
-      s1 += b.x * cb.x + b.y * cb.y;
+      double2 ca[U];
+#pragma unroll
+      for (int u = 0; u < U; u++) ca[u] = c2[q + u * stride];
+#pragma unroll
+      for (int u = 0; u < U; u++) s[u] += a[u].x * ca[u].x + a[u].y * ca[u].y;
     } else {
-      s0 += a.x * a.x + a.y * a.y;
-      s1 += b.x * b.x + b.y * b.y;
+#pragma unroll
+      for (int u = 0; u < U; u++) s[u] += a[u].x * a[u].x + a[u].y * a[u].y;
     }
   }
   for (; q < n2; q += stride) {
@@ -88,21 +113,36 @@ __global__ void __launch_bounds__(kKryThreads, 4) k_kry_mgs_t(double *__restrict
     }
     if (VN) {
       const double2 ca = c2[q];
-      s0 += a.x * ca.x + a.y * ca.y;
+      s[0] += a.x * ca.x + a.y * ca.y;
     } else {
-      s0 += a.x * a.x + a.y * a.y;
+      s[0] += a.x * a.x + a.y * a.y;
     }
   }
-  kry_finish(s0 + s1, partial, cnt, out, sh);
+  double t = 0.0;
+#pragma unroll
+  for (int u = 0; u < U; u++) t += s[u];
+  kry_finish(t, partial, cnt, out, sh);
 }
 
-// one MGS step on stream st (vq / vn may be null, as above)
+template <int U>
+inline void kry_mgs_u(double *w, const double *vq, const double *hq, const double *vn, long n, double *partial,
+                      unsigned *cnt, double *out, cudaStream_t st) {
+  const int g = kry_grid();
+  if (vq && vn) k_kry_mgs_t<true, true, U><<<g, kKryThreads, 0, st>>>(w, vq, hq, vn, n, partial, cnt, out);
+  else if (vq) k_kry_mgs_t<true, false, U><<<g, kKryThreads, 0, st>>>(w, vq, hq, vn, n, partial, cnt, out);
+  else if (vn) k_kry_mgs_t<false, true, U><<<g, kKryThreads, 0, st>>>(w, vq, hq, vn, n, partial, cnt, out);
+  else k_kry_mgs_t<false, false, U><<<g, kKryThreads, 0, st>>>(w, vq, hq, vn, n, partial, cnt, out);
+}
+
+// one MGS step on stream st (vq / vn may be null, as above); the unroll
+// depth is the autotuned kTuneKryUnroll
 inline void kry_mgs(double *w, const double *vq, const double *hq, const double *vn, long n, double *partial,
                     unsigned *cnt, double *out, cudaStream_t st) {
-  if (vq && vn) k_kry_mgs_t<true, true><<<kKryBlocks, kKryThreads, 0, st>>>(w, vq, hq, vn, n, partial, cnt, out);
-  else if (vq) k_kry_mgs_t<true, false><<<kKryBlocks, kKryThreads, 0, st>>>(w, vq, hq, vn, n, partial, cnt, out);
-  else if (vn) k_kry_mgs_t<false, true><<<kKryBlocks, kKryThreads, 0, st>>>(w, vq, hq, vn, n, partial, cnt, out);
-  else k_kry_mgs_t<false, false><<<kKryBlocks, kKryThreads, 0, st>>>(w, vq, hq, vn, n, partial, cnt, out);
+  switch (tune_value(kTuneKryUnroll)) {
+    case 1: kry_mgs_u<1>(w, vq, hq, vn, n, partial, cnt, out, st); break;
+    case 4: kry_mgs_u<4>(w, vq, hq, vn, n, partial, cnt, out, st); break;
+    default: kry_mgs_u<2>(w, vq, hq, vn, n, partial, cnt, out, st); break;
+  }
 }
 
 // y = x / sqrt(*a2) (invert) or y = x * (*a2)

@@ -5,6 +5,7 @@
 // reconstruction and fluxes run in FP32, the flux-divergence sums, the
 // conserved-state update and the pressure recovery in FP64.
 #include "bx_stage3d.cuh"
+#include "bx_tune.h"
 
 namespace bx {
 
@@ -19,7 +20,10 @@ static cudaError_t launch_lim(const TmaMaps &maps, const StageArgs &a, int nSM, 
     if (e != cudaSuccess) return e;
     attr = true;
   }
-  const int grid = a.nBlock < nSM ? a.nBlock : nSM;
+  // persistent grid: the autotuned number of CTAs per SM (several fit for
+  // the small tiles of 4^3 blocks)
+  const int want = nSM * tune_value(kTuneStageGrid);
+  const int grid = a.nBlock < want ? a.nBlock : want;
   k<<<grid, T::NTHR, sm, st>>>(maps, a);
   return cudaGetLastError();
 }

@@ -134,6 +134,11 @@ class ExplicitSolver:
         check(self.L.bx_synchronize())
 
     # -- measurement -----------------------------------------------------------
+    def autotune(self):
+        """bx_autotune: time the candidate launch shapes of every kernel whose
+        context is ready and keep the fastest; returns the knob table."""
+        return capi.autotune()
+
     def timing(self, on):
         check(self.L.bx_timing_enable(int(on)))
 

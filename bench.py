@@ -147,6 +147,7 @@ def run_ours(args):
         # ---- device-resident throughput ----------------------------------
         x.set_state(st)
         x.advance(max(args.warmup, 3))  # includes the first Dt = 0 step
+        tuned = x.autotune() if args.autotune else None
         x.synchronize()
         barrier(world)
         x.timing(True)
@@ -168,7 +169,8 @@ def run_ours(args):
                             "unit": "GB/s", "frac": round(achieved / hbm_peak, 4),
                             "traffic": (t_per_cell * nCell if t_per_cell else None),
                             "peak_source": peak_kind},
-               "clocks": clk.summary(), "gpu_launches": 4 * args.steps}
+               "clocks": clk.summary(), "gpu_launches": 4 * args.steps,
+               "autotune": ({k: v["value"] for k, v in tuned.items()} if tuned else None)}
         # ---- end to end through the C ABI with pinned host buffers ----------
         if args.e2e:
             import torch
@@ -222,6 +224,8 @@ def run_jfnk(args, lrank):
         try:
             for _ in range(1 + args.jfnk_warmup):  # the first step only sets the time step
                 im.advance_part_impl()
+            if args.autotune:
+                x.autotune()
             x.synchronize()
             x.region_begin()
             stats = [im.advance_part_impl() for _ in range(args.jfnk_steps)]
@@ -341,6 +345,8 @@ def run_heat(args, lrank):
         try:
             x = ExplicitSolver(g, Scheme(), device=lrank)
             h = HeatSolver(x, HeatParams(typePrecond=prec), Te, b, used)
+            if args.autotune:
+                x.autotune()
             for _ in range(args.heat_warmup):
                 h.advance_semi_impl()
             x.synchronize()
@@ -482,6 +488,8 @@ def main():
     ap.add_argument("--jfnk-nroot", type=int, default=16, help="16 -> 128^3 cells")
     ap.add_argument("--jfnk-steps", type=int, default=5)
     ap.add_argument("--jfnk-warmup", type=int, default=2)
+    ap.add_argument("--no-autotune", dest="autotune", action="store_false",
+                    help="keep the default launch shapes instead of bx_autotune")
     ap.add_argument("--heat-precond", default="BILU,NONE", help="'' to skip the heat conduction workload")
     ap.add_argument("--heat-nroot", type=int, default=32, help="32 -> 256^3 cells")
     ap.add_argument("--heat-steps", type=int, default=3)
@@ -504,6 +512,7 @@ def main():
                        "stages": 2, "l2": "inputs larger than L2 (state %.2f GB)" % ((8 * args.nroot) ** 3 * 64 / 1e9),
                        "parallelism": "one domain per GPU"},
             "roofline": r64["roofline"], "clocks": r64["clocks"], "gpu_launches": r64["gpu_launches"],
+            "autotune": r64.get("autotune"),
             "fp32_bulk": ({"value": r32["value"], "ms_per_step": r32["ms_per_step"], "dtype": "f32/f64",
                            "roofline": r32["roofline"], "e2e": r32.get("e2e")} if r32 else None)}
     if "e2e" in r64:

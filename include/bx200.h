@@ -313,6 +313,27 @@ BX_API int bx_heat_get_rhs(double *b);
 BX_API int bx_heat_matvec(const double *x, double *y);
 BX_API int bx_heat_precond(const double *r, double *z);
 
+/* ---- autotuner ----------------------------------------------------------------
+ * No counterpart in the reference (its launch shapes are fixed by OpenACC
+ * directives).  Launch-shape knobs (threads per CTA, CTAs per SM, unroll
+ * depth) with candidate values: bx_autotune times every candidate of every
+ * knob whose context is ready (the explicit stage after bx_init, the heat
+ * ILU after bx_heat_init, the BILU sweeps after an implicit BILU step, the
+ * Krylov vector kernels always) with CUDA events on the live data and keeps
+ * the fastest.  Knobs set by bx_tune_set are kept.  The candidates of a knob
+ * compute the same result, except the Krylov grid, which sets the summation
+ * order of the GMRES inner products. */
+BX_API int bx_autotune(void);
+/* knob iKnob (0-based; BX_ERR_ARG past the last): name (nameLen bytes),
+ * current value, tuned (0 default, 1 autotuned, 2 set by the caller), the
+ * candidates (at most 8) and their times in ms from the last autotune */
+BX_API int bx_tune_info(int iKnob, char *name, int nameLen, int *value, int *tuned, int *nCand, int *cand,
+                        float *ms);
+/* force a knob to one of its candidates */
+BX_API int bx_tune_set(const char *name, int value);
+/* every knob back to its default, none tuned */
+BX_API int bx_tune_reset(void);
+
 /* ---- measurement ----------------------------------------------------------
  * Kernel timing with CUDA events on the library's stream: when enabled, the
  * fused stage kernel launches are bracketed by events; the average duration

@@ -51,6 +51,17 @@ def test_argument_errors_without_gpu():
     # calls before bx_init are refused
     assert L.bx_advance(1, -1.0) == 3
     assert b"bx_init" in L.bx_last_error()
+    assert L.bx_autotune() == 3
+    # the autotuner's table needs no device
+    knobs = capi.tune_info()
+    assert set(knobs) == {"stage_ctas_per_sm", "krylov_ctas_per_sm", "krylov_unroll", "heat_ilu_warps",
+                          "bilu_threads"}
+    assert all(k["value"] in k["candidates"] and k["tuned"] == 0 for k in knobs.values())
+    assert L.bx_tune_set(b"krylov_unroll", 3) == 1 and L.bx_tune_set(b"no_such_knob", 1) == 1
+    capi.tune_set("krylov_unroll", 4)
+    assert capi.tune_info()["krylov_unroll"] == dict(knobs["krylov_unroll"], value=4, tuned=2)
+    capi.tune_reset()
+    assert capi.tune_info() == knobs
     # unsupported block size is rejected before any device call
     g, s, _, _ = configs.brio_wu_1d()
     gd = capi.grid_desc(g)
