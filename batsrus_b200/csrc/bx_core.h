@@ -47,5 +47,13 @@ int learned_apply(const double *v, double *z, int nBlock, cudaStream_t st);
 int learned_collect(const double *w, const double *z, int nBlock, cudaStream_t st);
 int learned_collect_n(const double *w, const double *z, int nBlock, int perPair, cudaStream_t st);
 bool learned_has_room();
+// zero features and a channel-0 identity part for a scalar solve embedded in
+// the 8 channels (bx_heat.cu)
+int learned_scalar_setup(int nBlock, cudaStream_t st);
+// store block pairs of a scalar solve with the picked blocks' ILU factors
+// (coefL: {lower x, lower y, lower z, 1/pivot} interleaved by 32 blocks):
+// the network is then trained on the residual-space loss |M z - t|^2
+int learned_collect_scalar(const double *w, const double *z, const double4 *coefL, const unsigned char *used,
+                           int nBlock, cudaStream_t st);
 
 }  // namespace bx

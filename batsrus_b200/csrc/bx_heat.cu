@@ -67,6 +67,8 @@ struct HeatCtx {
   double *K = nullptr;  // face conduction tensor [block][dim][dir][face]
   double4 *coef = nullptr;   // forward and backward sweep coefficients, interleaved by 32 blocks
   double *yI = nullptr;      // forward-sweep scratch, interleaved
+  double *V8 = nullptr, *Z8 = nullptr;  // learned preconditioner: embedded input and output [block][8][512]
+  double *Zb = nullptr;                 // flexible GMRES: preconditioned basis (m vectors)
   unsigned *usedM = nullptr; // used masks [group][cell]
   int nGroup = 0;            // groups of 32 blocks
   long nIl = 0;              // cells of the interleaved arrays (nGroup x 32 x 512)
@@ -537,6 +539,44 @@ cudaError_t launch_ilu(int w, const double *r, double *z, cudaStream_t st) {
   }
 }
 
+// ---- learned preconditioner (BX_PRECOND_LEARNED) --------------------------
+// The per-block network of the implicit solver works on 8-channel block
+// vectors and is linear in them.  The scalar vector v enters as v and seven
+// copies of v weighted by the local conduction tensor (bx^2, by^2, bz^2,
+// bx by, bx bz, by bz, HeatCoef / HeatCondPar / 2^2.5): still linear in v,
+// with the anisotropy the preconditioner has to follow.  z is output
+// channel 0.
+__global__ void k_heat_embed(const double *__restrict__ v, const double *__restrict__ B3,
+                             const double *__restrict__ HC, double hcScale, double *V8, long n) {
+  for (long q = blockIdx.x * (long)blockDim.x + threadIdx.x; q < n; q += (long)gridDim.x * blockDim.x) {
+    const long b = q / kNC, c = q % kNC;
+    const double x = v[q], bx = B3[3 * q], by = B3[3 * q + 1], bz = B3[3 * q + 2];
+    double *o = V8 + b * 8 * kNC + c;
+    o[0] = x;
+    o[kNC] = x * bx * bx;
+    o[2 * kNC] = x * by * by;
+    o[3 * kNC] = x * bz * bz;
+    o[4 * kNC] = x * bx * by;
+    o[5 * kNC] = x * bx * bz;
+    o[6 * kNC] = x * by * bz;
+    o[7 * kNC] = x * HC[q] * hcScale;
+  }
+}
+// Z8 = (z, 0, ..., 0): a training target
+__global__ void k_heat_target(const double *__restrict__ z, double *Z8, long n) {
+  for (long q = blockIdx.x * (long)blockDim.x + threadIdx.x; q < n; q += (long)gridDim.x * blockDim.x) {
+    const long b = q / kNC, c = q % kNC;
+    double *o = Z8 + b * 8 * kNC + c;
+    o[0] = z[q];
+#pragma unroll
+    for (int m = 1; m < 8; m++) o[m * kNC] = 0.0;
+  }
+}
+__global__ void k_heat_take0(const double *__restrict__ Z8, double *z, long n) {
+  for (long q = blockIdx.x * (long)blockDim.x + threadIdx.x; q < n; q += (long)gridDim.x * blockDim.x)
+    z[q] = Z8[(q / kNC) * 8 * kNC + q % kNC];
+}
+
 void free_heat() {
   for (double **p : {&H.Te, &H.HC, &H.B3, &H.b, &H.x, &H.w, &H.t, &H.r, &H.V, &H.partial, &H.scal}) {
     if (*p) cudaFree(*p);
@@ -550,6 +590,10 @@ void free_heat() {
   }
   if (H.K) cudaFree(H.K);
   H.K = nullptr;
+  for (double **p : {&H.V8, &H.Z8, &H.Zb}) {
+    if (*p) cudaFree(*p);
+    *p = nullptr;
+  }
   if (H.yI) cudaFree(H.yI);
   if (H.usedM) cudaFree(H.usedM);
   H.yI = nullptr;
@@ -580,7 +624,40 @@ int matvec(const double *x, double *y, cudaStream_t st) {
   return BX_OK;
 }
 
+int need_learned_buffers(bool basis) {
+  const size_t v8 = sizeof(double) * 8 * H.nCell;
+  if (!H.V8 && (cudaMalloc(&H.V8, v8) != cudaSuccess || cudaMalloc(&H.Z8, v8) != cudaSuccess))
+    return core_fail(BX_ERR_NOMEM, "learned preconditioner buffers (%.2f GB)", 2e-9 * v8);
+  if (basis && !H.Zb && cudaMalloc(&H.Zb, sizeof(double) * H.nCell * H.p.nKrylovVector) != cudaSuccess)
+    return core_fail(BX_ERR_NOMEM, "flexible GMRES basis");
+  return BX_OK;
+}
+
+void embed(const double *v, cudaStream_t st) {
+  k_heat_embed<<<1184, 256, 0, st>>>(v, H.B3, H.HC, 1.0 / (H.p.HeatCondPar * 5.656854249492381), H.V8, H.nCell);
+}
+
+// store (t, BILU(t)) block pairs for the learned preconditioner
+int collect_pair(const double *t, const double *z, cudaStream_t st) {
+  int r = need_learned_buffers(false);
+  if (r) return r;
+  embed(t, st);
+  k_heat_target<<<1184, 256, 0, st>>>(z, H.Z8, H.nCell);
+  CKH(cudaGetLastError());
+  return learned_collect_scalar(H.V8, H.Z8, H.coef, H.used, H.nBlock, st);
+}
+
 int precond(const double *r, double *z, cudaStream_t st) {
+  if (H.p.TypePrecond == BX_PRECOND_LEARNED) {
+    if (!learned_ready()) return core_fail(BX_ERR_STATE, "the learned preconditioner is not initialised");
+    int e = need_learned_buffers(false);
+    if (e) return e;
+    embed(r, st);
+    if ((e = learned_apply(H.V8, H.Z8, H.nBlock, st))) return e;
+    k_heat_take0<<<1184, 256, 0, st>>>(H.Z8, z, H.nCell);
+    CKH(cudaGetLastError());
+    return BX_OK;
+  }
   if (H.p.TypePrecond == BX_PRECOND_BILU) {
     const cudaError_t e = launch_ilu(tune_value(kTuneHeatIluWarps), r, z, st);
     if (e != cudaSuccess) return core_fail(BX_ERR_CUDA, "heat ILU launch: %s", cudaGetErrorString(e));
@@ -624,6 +701,7 @@ int gmres(int &iError, cudaStream_t st) {
       double *Vk = Vb + (size_t)k * N;
       if ((r = matvec(Vk, H.t, st))) return r;
       if ((r = precond(H.t, H.w, st))) return r;
+      if (H.p.TypePrecond == BX_PRECOND_BILU && learned_collecting() && (r = collect_pair(H.t, H.w, st))) return r;
       for (int q = 0; q <= k + 1; q++) {
         const double *vq = q > 0 ? Vb + (size_t)(q - 1) * N : nullptr;
         const double *hq = q > 0 ? hdev + q - 1 : nullptr;
@@ -679,6 +757,96 @@ int gmres(int &iError, cudaStream_t st) {
     beta = std::sqrt(b2);
     H.errRel = beta / beta0;
     if (H.errRel <= H.p.ErrorMax) return BX_OK;
+  }
+}
+
+// flexible restarted GMRES(m), right preconditioned (the learned
+// preconditioner is linear only up to its BF16 rounding), modified
+// Gram-Schmidt, x0 = 0; converged when |b - A x| <= ErrorMax |b|
+int fgmres(int &iError, cudaStream_t st) {
+  const int m = H.p.nKrylovVector;
+  const long N = H.nCell;
+  double *Vb = H.V, *Zb = H.Zb, *hdev = H.scal + 8;
+  CKH(cudaMemsetAsync(H.x, 0, sizeof(double) * N, st));
+  H.nMatvec = 0;
+  H.errRel = 0;
+  iError = 0;
+  int r = dotd(H.b, H.b, H.scal + 2, st);
+  if (r) return r;
+  double b2;
+  CKH(cudaMemcpyAsync(&b2, H.scal + 2, sizeof(double), cudaMemcpyDeviceToHost, st));
+  CKH(cudaStreamSynchronize(st));
+  const double beta0 = std::sqrt(b2);
+  if (beta0 == 0.0) return BX_OK;
+  double beta = beta0;
+  const double *rvec = H.b;
+  std::vector<double> Hm((m + 1) * m), cs(m), sn(m), g(m + 1), y(m), hb(m + 2);
+  while (true) {
+    k_kry_scale<<<kry_grid(), kKryThreads, 0, st>>>(Vb, rvec, H.scal + 2, 1, N);
+    CKH(cudaGetLastError());
+    std::fill(g.begin(), g.end(), 0.0);
+    g[0] = beta;
+    int kdone = 0;
+    bool conv = false;
+    for (int k = 0; k < m; k++) {
+      double *Vk = Vb + (size_t)k * N, *Zk = Zb + (size_t)k * N;
+      if ((r = precond(Vk, Zk, st))) return r;
+      if ((r = matvec(Zk, H.w, st))) return r;
+      for (int q = 0; q <= k + 1; q++) {
+        const double *vq = q > 0 ? Vb + (size_t)(q - 1) * N : nullptr;
+        const double *hq = q > 0 ? hdev + q - 1 : nullptr;
+        const double *vn = q <= k ? Vb + (size_t)q * N : nullptr;
+        kry_mgs(H.w, vq, hq, vn, N, H.partial, H.cnt, hdev + q, st);
+      }
+      CKH(cudaGetLastError());
+      CKH(cudaMemcpyAsync(hb.data(), hdev, sizeof(double) * (k + 2), cudaMemcpyDeviceToHost, st));
+      CKH(cudaStreamSynchronize(st));
+      const double hn = std::sqrt(hb[k + 1]);
+      if (hn != 0.0) {
+        k_kry_scale<<<kry_grid(), kKryThreads, 0, st>>>(Vb + (size_t)(k + 1) * N, H.w, hdev + k + 1, 1, N);
+        CKH(cudaGetLastError());
+      }
+      for (int q = 0; q <= k; q++) Hm[q * m + k] = hb[q];
+      Hm[(k + 1) * m + k] = hn;
+      for (int q = 0; q < k; q++) {
+        const double t0 = Hm[q * m + k], t1 = Hm[(q + 1) * m + k];
+        Hm[q * m + k] = cs[q] * t0 + sn[q] * t1;
+        Hm[(q + 1) * m + k] = -sn[q] * t0 + cs[q] * t1;
+      }
+      const double a0 = Hm[k * m + k], b0 = Hm[(k + 1) * m + k];
+      const double rr = std::sqrt(a0 * a0 + b0 * b0);
+      cs[k] = a0 / rr;
+      sn[k] = b0 / rr;
+      Hm[k * m + k] = rr;
+      Hm[(k + 1) * m + k] = 0.0;
+      g[k + 1] = -sn[k] * g[k];
+      g[k] = cs[k] * g[k];
+      kdone = k + 1;
+      H.errRel = std::fabs(g[k + 1]) / beta0;
+      if (H.errRel <= H.p.ErrorMax || H.nMatvec >= H.p.MaxMatvec || hn == 0.0) {
+        conv = H.errRel <= H.p.ErrorMax || hn == 0.0;
+        break;
+      }
+    }
+    for (int q = kdone - 1; q >= 0; q--) {
+      double s = g[q];
+      for (int p = q + 1; p < kdone; p++) s -= Hm[q * m + p] * y[p];
+      y[q] = s / Hm[q * m + q];
+    }
+    CKH(cudaMemcpyAsync(H.scal + 80, y.data(), sizeof(double) * kdone, cudaMemcpyHostToDevice, st));
+    k_kry_update<<<kry_grid(), kKryThreads, 0, st>>>(H.x, Zb, H.scal + 80, kdone, N);
+    CKH(cudaGetLastError());
+    if (conv) return BX_OK;
+    if (H.nMatvec >= H.p.MaxMatvec) { iError = 1; return BX_OK; }
+    if ((r = matvec(H.x, H.t, st))) return r;  // restart with the true residual
+    k_h_sub<<<1184, 256, 0, st>>>(H.r, H.b, H.t, N);
+    if ((r = dotd(H.r, H.r, H.scal + 2, st))) return r;
+    CKH(cudaMemcpyAsync(&b2, H.scal + 2, sizeof(double), cudaMemcpyDeviceToHost, st));
+    CKH(cudaStreamSynchronize(st));
+    beta = std::sqrt(b2);
+    H.errRel = beta / beta0;
+    if (H.errRel <= H.p.ErrorMax) return BX_OK;
+    rvec = H.r;
   }
 }
 
@@ -795,8 +963,10 @@ int bx_heat_init(const bx_heat_params *prm, const double *Te, const double *bhat
   if (!prm || !Te || !bhat || !used) return core_fail(BX_ERR_ARG, "null argument");
   if (prm->nKrylovVector < 1 || prm->nKrylovVector > 64 || prm->MaxMatvec < 1 || !(prm->Dt > 0) || !(prm->Cv > 0))
     return core_fail(BX_ERR_ARG, "bad heat conduction parameters");
-  if (prm->TypePrecond != BX_PRECOND_NONE && prm->TypePrecond != BX_PRECOND_BILU)
-    return core_fail(BX_ERR_ARG, "TypePrecond=%d: the heat conduction solve takes NONE or BILU", prm->TypePrecond);
+  if (prm->TypePrecond != BX_PRECOND_NONE && prm->TypePrecond != BX_PRECOND_BILU &&
+      prm->TypePrecond != BX_PRECOND_LEARNED)
+    return core_fail(BX_ERR_ARG, "TypePrecond=%d: the heat conduction solve takes NONE, BILU or LEARNED",
+                     prm->TypePrecond);
   if (H.ready) free_heat();
   std::vector<int> atH, xyzH;
   const int r0 = grid_tables(c, atH, xyzH);
@@ -882,7 +1052,14 @@ int bx_advance_semi_impl(bx_krylov_stats *stats) {
   }
   CKH(cudaGetLastError());
   int iError = 0;
-  if ((r = gmres(iError, c.st))) return r;
+  const bool learned = H.p.TypePrecond == BX_PRECOND_LEARNED;
+  if ((learned || learned_collecting()) && (r = learned_scalar_setup(H.nBlock, c.st))) return r;
+  if (learned) {
+    if ((r = need_learned_buffers(true))) return r;
+    if ((r = fgmres(iError, c.st))) return r;
+  } else if ((r = gmres(iError, c.st))) {
+    return r;
+  }
   k_h_te_update<<<1184, 256, 0, c.st>>>(H.Te, H.x, H.used, H.nCell);
   if ((r = update_coef(c.st))) return r;
   CKH(cudaGetLastError());
@@ -942,6 +1119,7 @@ int bx_heat_precond(const double *rv, double *z) {
         H.a, H.K, H.used, H.wtab, H.coef, H.coef + H.nIl, H.nBlock);
     CKH(cudaGetLastError());
   }
+  if (H.p.TypePrecond == BX_PRECOND_LEARNED && (r = learned_scalar_setup(H.nBlock, c.st))) return r;
   if ((r = copy_in(H.r, rv))) return r;
   if ((r = precond(H.r, H.t, c.st))) return r;
   return copy_out(z, H.t);

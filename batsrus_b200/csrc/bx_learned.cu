@@ -50,6 +50,16 @@ struct LCtx {
   double identCoef = 0.0;
   long nResidual = 0;  // samples whose targets hold the remainder
   double blend = 1.0;  // weight of the learned remainder at inference
+  // channels of the identity part: 8 for the MHD vectors; 1 for a scalar
+  // solve (the heat conduction embeds its vector in channel 0 and seven
+  // weighted copies of it in the others, which carry no identity part)
+  int identChannels = 8;
+  // residual-space training of a scalar solve: the loss is |M z - t|^2 with
+  // each sample block's ILU factors M (mcoef [sample][512]: pivot and the
+  // three lower couplings) instead of the MSE against the ILU correction
+  bool residMode = false;
+  float4 *mcoef = nullptr;
+  float *outRaw = nullptr;  // [batch][512]
   cudaStream_t st = nullptr;
 };
 
@@ -70,7 +80,9 @@ constexpr size_t kSmemBwd = 2 * (size_t)kBuf32 + kW3tBytes + kW2tBytes + sizeof(
 constexpr size_t kSmemDw = 2 * (size_t)kBuf32 + sizeof(Smem);
 
 void free_learned() {
-  for (float **q : {&Lc.p, &Lc.m, &Lc.v, &Lc.g, &Lc.tgt, &Lc.part, &Lc.scal}) {
+  if (Lc.mcoef) cudaFree(Lc.mcoef);
+  Lc.mcoef = nullptr;
+  for (float **q : {&Lc.p, &Lc.m, &Lc.v, &Lc.g, &Lc.tgt, &Lc.part, &Lc.scal, &Lc.outRaw}) {
     if (*q) cudaFree(*q);
     *q = nullptr;
   }
@@ -182,14 +194,29 @@ __global__ void k_collect(const double *__restrict__ w, const double *__restrict
   }
 }
 
+// the ILU factors of the picked blocks of a scalar solve: coefL is the
+// forward-sweep double4 {lower x, lower y, lower z, 1/pivot} per cell,
+// interleaved by groups of 32 blocks; the couplings are kept where the cell
+// and its neighbour are both used
+__global__ void k_collect_mc(const double4 *__restrict__ coefL, const unsigned char *__restrict__ used,
+                             const int *__restrict__ pick, long base, float4 *mcoef) {
+  const int b = pick[blockIdx.x], c = threadIdx.x;
+  const double4 v = coefL[((size_t)(b >> 5) * 512 + c) * 32 + (b & 31)];
+  const unsigned char *u = used + (size_t)b * 512;
+  const int i = c & 7, j = (c >> 3) & 7, k = c >> 6;
+  const bool uc = u[c];
+  mcoef[(base + blockIdx.x) * 512 + c] =
+      make_float4((float)(1.0 / v.w), (uc && i > 0 && u[c - 1]) ? (float)v.x : 0.f,
+                  (uc && j > 0 && u[c - 8]) ? (float)v.y : 0.f, (uc && k > 0 && u[c - 64]) ? (float)v.z : 0.f);
+}
+
 // out[0] += sum tgt . x, out[1] += sum x . x over cells [0, nCell) (x = the
 // first 8 input channels)
 __global__ void k_ident_fit(const __nv_bfloat16 *__restrict__ in16, const float *__restrict__ tgt, long nCell,
-                            float *out) {
+                            int nCh, float *out) {
   float a = 0.f, b = 0.f;
   for (long q = blockIdx.x * (long)blockDim.x + threadIdx.x; q < nCell; q += (long)gridDim.x * blockDim.x)
-#pragma unroll
-    for (int m = 0; m < 8; m++) {
+    for (int m = 0; m < nCh; m++) {
       const float x = __bfloat162float(in16[q * 16 + m]);
       a += tgt[q * 8 + m] * x;
       b += x * x;
@@ -203,11 +230,10 @@ __global__ void k_ident_fit(const __nv_bfloat16 *__restrict__ in16, const float 
     atomicAdd(out + 1, b);
   }
 }
-// tgt -= c x over cells [c0, c1)
-__global__ void k_ident_sub(const __nv_bfloat16 *__restrict__ in16, float *tgt, long c0, long c1, float c) {
+// tgt -= c x over cells [c0, c1), channels [0, nCh)
+__global__ void k_ident_sub(const __nv_bfloat16 *__restrict__ in16, float *tgt, long c0, long c1, int nCh, float c) {
   for (long q = c0 + blockIdx.x * (long)blockDim.x + threadIdx.x; q < c1; q += (long)gridDim.x * blockDim.x)
-#pragma unroll
-    for (int m = 0; m < 8; m++) tgt[q * 8 + m] -= c * __bfloat162float(in16[q * 16 + m]);
+    for (int m = 0; m < nCh; m++) tgt[q * 8 + m] -= c * __bfloat162float(in16[q * 16 + m]);
 }
 
 // *out += sum of x^2 (FP32 partial sums per warp)
@@ -228,9 +254,17 @@ int gradient(long s0, int nS, cudaStream_t st, float tgtMul) {
   const float gscale = 2.0f / (4096.0f * (float)nS);
   CKL(cudaMemsetAsync(Lc.scal, 0, sizeof(float) * 80, st));
   const __nv_bfloat16 *in = Lc.in16 + (size_t)s0 * 512 * 16;
+  if (Lc.residMode && !Lc.outRaw && cudaMalloc(&Lc.outRaw, sizeof(float) * 512 * kBatchMax) != cudaSuccess)
+    return core_fail(BX_ERR_NOMEM, "learned preconditioner training buffers");
   k_net_fwd_train<<<grid, kThreads, kSmemFwd, st>>>(W, in, Lc.tgt + (size_t)s0 * 512 * 8, nS, gscale, tgtMul, Lc.A1, Lc.A2,
-                                                    Lc.dY3, Lc.scal, Lc.scal + 1, Lc.err);
+                                                    Lc.dY3, Lc.scal, Lc.scal + 1, Lc.err,
+                                                    Lc.residMode ? Lc.outRaw : nullptr);
   CKL(cudaGetLastError());
+  if (Lc.residMode) {
+    k_resid_grad<<<nS, 512, 0, st>>>(in, Lc.mcoef + (size_t)s0 * 512, Lc.outRaw, (float)Lc.identCoef,
+                                     (float)Lc.outScale, 2.0f / (512.0f * (float)nS), Lc.dY3, Lc.scal, Lc.scal + 1);
+    CKL(cudaGetLastError());
+  }
   k_net_bwd_data<<<grid, kThreads, kSmemBwd, st>>>(W, Lc.dY3, Lc.A2, Lc.A1, nS, Lc.dY2, Lc.dY1, Lc.scal + 9,
                                                    Lc.scal + 41, Lc.err);
   CKL(cudaGetLastError());
@@ -282,12 +316,29 @@ int learned_features(const double *U, const double *norm, int nBlock, cudaStream
   }
   k_features<<<4 * Lc.nSM, 256, 0, st>>>(U, norm, 512L * nBlock, Lc.feat);
   CKL(cudaGetLastError());
+  Lc.identChannels = 8;
   return BX_OK;
 }
 
 int learned_apply(const double *v, double *z, int nBlock, cudaStream_t st) {
   k_net_apply<<<std::min(nBlock, Lc.nSM), kThreads, kSmemFwd, st>>>(weights(), v, z, Lc.feat, nBlock, Lc.err);
   CKL(cudaGetLastError());
+  return BX_OK;
+}
+
+// zero cell features for nBlock blocks (a solve without state features) and
+// the identity part on channel 0 only
+int learned_scalar_setup(int nBlock, cudaStream_t st) {
+  if (Lc.featBlocks < nBlock) {
+    if (Lc.feat) cudaFree(Lc.feat);
+    Lc.feat = nullptr;
+    Lc.featBlocks = 0;
+    if (cudaMalloc(&Lc.feat, sizeof(__nv_bfloat16) * 512 * 8 * (size_t)nBlock) != cudaSuccess)
+      return core_fail(BX_ERR_NOMEM, "learned preconditioner features");
+    Lc.featBlocks = nBlock;
+  }
+  CKL(cudaMemsetAsync(Lc.feat, 0, sizeof(__nv_bfloat16) * 512 * 8 * (size_t)nBlock, st));
+  Lc.identChannels = 1;
   return BX_OK;
 }
 
@@ -304,6 +355,20 @@ int learned_collect_n(const double *w, const double *z, int nBlock, int perPair,
   CKL(cudaGetLastError());
   CKL(cudaStreamSynchronize(st));  // the pick list is reused by the next call
   Lc.nSample += nPick;
+  return BX_OK;
+}
+
+int learned_collect_scalar(const double *w, const double *z, const double4 *coefL, const unsigned char *used,
+                           int nBlock, cudaStream_t st) {
+  if (!Lc.mcoef && cudaMalloc(&Lc.mcoef, sizeof(float4) * 512 * (size_t)Lc.nSampleMax) != cudaSuccess)
+    return core_fail(BX_ERR_NOMEM, "learned preconditioner factors (%.2f GB)", 8.2e-6 * Lc.nSampleMax);
+  const long base = Lc.nSample;
+  int r = learned_collect_n(w, z, nBlock, Lc.collectPerPair, st);
+  if (r || Lc.nSample == base) return r;
+  // the pick list of that call is still on the device (the call synchronised)
+  k_collect_mc<<<(int)(Lc.nSample - base), 512, 0, st>>>(coefL, used, Lc.pick, base, Lc.mcoef);
+  CKL(cudaGetLastError());
+  Lc.residMode = true;
   return BX_OK;
 }
 
@@ -339,6 +404,8 @@ int bx_learned_init(long long nSampleMax, unsigned long long seed) {
   Lc.outScale = 1.0;
   Lc.scaleSet = false;
   Lc.identCoef = 0.0;
+  Lc.identChannels = 8;
+  Lc.residMode = false;
   Lc.nResidual = 0;
   Lc.blend = 1.0;
   bool okAlloc = true;
@@ -497,7 +564,7 @@ int bx_learned_train(int nEpoch, int batch, double lr, double *lossFirst, double
   if (!Lc.scaleSet && Lc.nResidual < Lc.nSample) {
     // identity coefficient a = <tgt, x> / <x, x> over the collected samples
     CKL(cudaMemsetAsync(Lc.scal, 0, sizeof(float) * 2, Lc.st));
-    k_ident_fit<<<4 * Lc.nSM, 256, 0, Lc.st>>>(Lc.in16, Lc.tgt, Lc.nSample * 512L, Lc.scal);
+    k_ident_fit<<<4 * Lc.nSM, 256, 0, Lc.st>>>(Lc.in16, Lc.tgt, Lc.nSample * 512L, Lc.identChannels, Lc.scal);
     CKL(cudaGetLastError());
     float ab[2] = {0, 0};
     CKL(cudaMemcpyAsync(ab, Lc.scal, sizeof(ab), cudaMemcpyDeviceToHost, Lc.st));
@@ -506,7 +573,7 @@ int bx_learned_train(int nEpoch, int batch, double lr, double *lossFirst, double
   }
   if (Lc.nResidual < Lc.nSample) {  // targets -> remainder after the identity part
     k_ident_sub<<<4 * Lc.nSM, 256, 0, Lc.st>>>(Lc.in16, Lc.tgt, Lc.nResidual * 512L, Lc.nSample * 512L,
-                                               (float)Lc.identCoef);
+                                               Lc.identChannels, (float)Lc.identCoef);
     CKL(cudaGetLastError());
     Lc.nResidual = Lc.nSample;
   }

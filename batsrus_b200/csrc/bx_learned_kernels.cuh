@@ -203,10 +203,13 @@ __global__ void __launch_bounds__(kThreads, 1)
 // [sample][cell][32]) and dY3 = gscale (out - tgt) (BF16 [sample][cell][16],
 // channels 8..15 zero); accumulates sum (out - tgt)^2 into loss[0] and the
 // bias gradient of layer 3 into gb3[0..7].
+// With outRaw set, the epilogue stores the raw output of channel 0 (FP32
+// [sample][cell]) instead of the MSE gradient: the residual-space loss of a
+// scalar solve forms its gradient in k_resid_grad.
 __global__ void __launch_bounds__(kThreads, 1)
     k_net_fwd_train(Weights W, const __nv_bfloat16 *__restrict__ in16, const float *__restrict__ tgt, int nSample,
                     float gscale, float tgtMul, __nv_bfloat16 *A1, __nv_bfloat16 *A2, __nv_bfloat16 *dY3, float *loss, float *gb3,
-                    int *err) {
+                    int *err, float *outRaw) {
   extern __shared__ __align__(1024) unsigned char sm[];
   unsigned char *bufA = sm, *bufB = sm + kBuf32;
   unsigned char *w1 = bufB + kBuf32, *w2 = w1 + kW1Bytes, *w3 = w2 + kW2Bytes;
@@ -261,8 +264,11 @@ __global__ void __launch_bounds__(kThreads, 1)
     if (!(ok = wait_mma(S, phase))) break;
     const float *tg = tgt + (size_t)n * 512 * 8;
     __nv_bfloat16 *dy = dY3 + (size_t)n * 512 * 16;
+    float *orw = outRaw ? outRaw + (size_t)n * 512 : nullptr;
     for_tiles<kN3>(tmem, [&](int, int, int cell, const float(&acc)[kN3]) {
-      if (cell >= 0) {
+      if (cell >= 0 && orw) {
+        orw[cell] = acc[0] + S.bias[64];
+      } else if (cell >= 0) {
         uint4 q[2];
         uint32_t *w = reinterpret_cast<uint32_t *>(q);
         float g[kC3];
@@ -535,6 +541,75 @@ __global__ void k_mask_linear(float *x) {
   if (i < kC1) x[kOffB1 + i] = 0.f;
   if (i < kC2) x[kOffB2 + i] = 0.f;
   if (i < kC3) x[kOffB3 + i] = 0.f;
+}
+
+// Residual-space loss of a scalar solve (one CTA of 512 threads per sample
+// block): with the block's ILU factors M = (L + D) D^-1 (D + U) (mc: pivot
+// and the couplings to the -x, -y, -z neighbours, zero where a cell or its
+// neighbour is not used; M is symmetric), the preconditioner output in
+// training units z = a t + outScale out (t = input channel 0) and
+// r = M z - t: loss += |r|^2, dY3 channel 0 = gscale outScale M r (the
+// other channels 0), gb3[0] += its sum.
+__device__ __forceinline__ void ilu_product(const float4 *mc, const float *x, float *y, float *tmp, int c) {
+  // y = (L + D) D^-1 (D + U) x; tmp holds D^-1 (D + U) x
+  const int i = c & 7, j = (c >> 3) & 7, k = c >> 6;
+  const float4 m = mc[c];
+  float s = m.x * x[c];
+  if (i < 7) s += mc[c + 1].y * x[c + 1];
+  if (j < 7) s += mc[c + 8].z * x[c + 8];
+  if (k < 7) s += mc[c + 64].w * x[c + 64];
+  tmp[c] = s / m.x;
+  __syncthreads();
+  float t = m.x * tmp[c];
+  if (i > 0) t += m.y * tmp[c - 1];
+  if (j > 0) t += m.z * tmp[c - 8];
+  if (k > 0) t += m.w * tmp[c - 64];
+  y[c] = t;
+  __syncthreads();
+}
+
+__global__ void __launch_bounds__(512) k_resid_grad(const __nv_bfloat16 *__restrict__ in16, const float4 *__restrict__ mcoef,
+                                                    const float *__restrict__ outRaw, float a, float outScale,
+                                                    float gscale, __nv_bfloat16 *dY3, float *loss, float *gb3) {
+  __shared__ float4 mc[512];
+  __shared__ float z[512], r[512], tmp[512], red[16][2];
+  const int n = blockIdx.x, c = threadIdx.x;
+  mc[c] = mcoef[(size_t)n * 512 + c];
+  const float t = __bfloat162float(in16[((size_t)n * 512 + c) * 16]);
+  z[c] = a * t + outScale * outRaw[(size_t)n * 512 + c];
+  __syncthreads();
+  ilu_product(mc, z, r, tmp, c);
+  const float rc = r[c] - t;
+  __syncthreads();
+  r[c] = rc;
+  __syncthreads();
+  ilu_product(mc, r, z, tmp, c);  // z = M r
+  const float g = gscale * outScale * z[c];
+  const __nv_bfloat16 gb = __float2bfloat16(g);
+  __nv_bfloat16 *dy = dY3 + ((size_t)n * 512 + c) * 16;
+  uint4 q0 = make_uint4(0, 0, 0, 0), q1 = make_uint4(0, 0, 0, 0);
+  reinterpret_cast<__nv_bfloat16 *>(&q0)[0] = gb;
+  reinterpret_cast<uint4 *>(dy)[0] = q0;
+  reinterpret_cast<uint4 *>(dy)[1] = q1;
+  float l = rc * rc, gs = __bfloat162float(gb);
+  for (int o = 16; o > 0; o >>= 1) {
+    l += __shfl_xor_sync(0xffffffffu, l, o);
+    gs += __shfl_xor_sync(0xffffffffu, gs, o);
+  }
+  if ((c & 31) == 0) {
+    red[c >> 5][0] = l;
+    red[c >> 5][1] = gs;
+  }
+  __syncthreads();
+  if (c == 0) {
+    float L = 0, G = 0;
+    for (int w = 0; w < 16; w++) {
+      L += red[w][0];
+      G += red[w][1];
+    }
+    atomicAdd(loss, L);
+    atomicAdd(gb3, G);
+  }
 }
 
 // grad[j] = sum over CTAs of part[cta][j] for one layer's weight block

@@ -340,9 +340,12 @@ def run_heat(args, lrank):
     out = {"workload": "dipole_heat_conduction_%dcubed_kpar_kperp_1e6_gmres30_1e-6" % n, "cells": g.nCell,
            "blocks": g.nBlock, "used_fraction": float(used.mean()), "solves": args.heat_steps,
            "warmup": args.heat_warmup, "unit": "s/solve", "higher_is_better": False}
+    net = None
     for prec in args.heat_precond.split(","):
         x = None
         try:
+            if prec.upper() == "LEARNED" and net is None:
+                net, out["learned_training"] = train_learned_heat(args, g, lrank)
             x = ExplicitSolver(g, Scheme(), device=lrank)
             h = HeatSolver(x, HeatParams(typePrecond=prec), Te, b, used)
             if args.autotune:
@@ -361,9 +364,49 @@ def run_heat(args, lrank):
         out[prec.lower()] = {"s_per_solve": ms * 1e-3 / args.heat_steps,
                              "matvec_per_solve": float(np.mean([q["nMatvec"] for q in stats])),
                              "matvec": [q["nMatvec"] for q in stats],
-                             "krylov_error": [q["Error"] for q in stats]}
+                             "krylov_error": [q["Error"] for q in stats],
+                             "criterion": ("true residual (flexible GMRES)" if prec.upper() in ("LEARNED", "NONE")
+                                           else "preconditioned residual (left GMRES)")}
         x.close()
+    if net is not None:
+        net.close()
     return out
+
+
+def train_learned_heat(args, g, lrank, nPair=2000, blocksPerPair=16):
+    """The learned preconditioner of the heat solve: (t, BILU(t)) block pairs
+    with the blocks' ILU factors from BILU solves of a differently seeded
+    field (seed 2025), training on the residual-space loss, blend 0.05 (the
+    largest weight of the learned remainder that keeps flexible GMRES
+    convergent at 256^3)."""
+    from batsrus_b200.explicit import ExplicitSolver
+    from batsrus_b200.heat import HeatSolver
+    from batsrus_b200.heat_params import HeatParams, heat_dipole, global_to_blocks
+    from batsrus_b200.learned import LearnedPreconditioner
+    from batsrus_b200.param import Scheme
+    nR = args.heat_nroot
+    n = 8 * nR
+    _, Te, b, used, _ = heat_dipole(nRoot=nR, seed=2025)
+    tb = lambda a: global_to_blocks(a.reshape((n, n, n) + a.shape[1:]), nR)
+    net = LearnedPreconditioner(nSampleMax=nPair * blocksPerPair, seed=2024)
+    x = ExplicitSolver(g, Scheme(), device=lrank)
+    h = HeatSolver(x, HeatParams(), tb(Te), tb(b), tb(used))
+    t0 = time.perf_counter()
+    net.collect(blocksPerPair)
+    nSolve = 0
+    while net.num_samples() < nPair * blocksPerPair and nSolve < 60:
+        h.advance_semi_impl()
+        nSolve += 1
+    net.collect(0)
+    x.close()
+    t1 = time.perf_counter()
+    first, last = net.train(nEpoch=12, batch=256, lr=1e-3)
+    net.set_blend(0.05)
+    t2 = time.perf_counter()
+    return net, {"pairs": net.num_samples() // blocksPerPair, "collect_solves": nSolve, "collect_s": t1 - t0,
+                 "train_s": t2 - t1, "loss_first_epoch": first, "loss_last_epoch": last,
+                 "loss": "residual space |M N(t) - t|^2 with the blocks' ILU factors", "seed_data": 2025,
+                 "seed_timed": 2024, "blend": 0.05}
 
 
 def cpu_baseline_heat(args, seconds=20.0):
@@ -490,7 +533,7 @@ def main():
     ap.add_argument("--jfnk-warmup", type=int, default=2)
     ap.add_argument("--no-autotune", dest="autotune", action="store_false",
                     help="keep the default launch shapes instead of bx_autotune")
-    ap.add_argument("--heat-precond", default="BILU,NONE", help="'' to skip the heat conduction workload")
+    ap.add_argument("--heat-precond", default="BILU,NONE,LEARNED", help="'' to skip the heat conduction workload")
     ap.add_argument("--heat-nroot", type=int, default=32, help="32 -> 256^3 cells")
     ap.add_argument("--heat-steps", type=int, default=3)
     ap.add_argument("--heat-warmup", type=int, default=1)

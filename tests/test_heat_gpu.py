@@ -133,3 +133,52 @@ def test_full_size_solve_reaches_tolerance():
     rel = np.linalg.norm(res) / np.linalg.norm(Mb)
     assert rel <= 1.5e-6, rel
     x.close()
+
+
+def test_learned_preconditioner_trains_and_gains_over_none():
+    """The learned per-block preconditioner in the heat solve: (t, BILU(t))
+    block pairs from the BILU-preconditioned solves of a differently seeded
+    field, training on the residual-space loss |M N(t) - t|^2 with each
+    block's ILU factors M, then flexible GMRES with the network.  It
+    converges to the tolerance, agrees with the BILU answer to it, and needs
+    fewer matvecs than no preconditioner on this 64^3 case."""
+    from batsrus_b200.learned import LearnedPreconditioner
+    nRoot, n = 8, 64
+
+    def fields(seed):
+        g, Te, b, used, dx = heat_dipole(nRoot=nRoot, seed=seed)
+        tb = lambda a: global_to_blocks(a.reshape((n, n, n) + a.shape[1:]), nRoot)
+        return g, (tb(Te), tb(b), tb(used))
+
+    g, ftrain = fields(10)
+    _, ftest = fields(9)
+    x = ExplicitSolver(g, Scheme())
+    net = LearnedPreconditioner(nSampleMax=2000 * 16, seed=2024)
+    net.collect(16)
+    h = HeatSolver(x, HeatParams(), *ftrain)
+    for _ in range(60):
+        if net.num_samples() >= 2000 * 16:
+            break
+        h.advance_semi_impl()
+    net.collect(0)
+    first, last = net.train(nEpoch=12, batch=256, lr=1e-3)
+    assert last < 0.5 * first
+    net.set_blend(0.25)
+    res = {}
+    for prec in ("NONE", "BILU", "LEARNED"):
+        hh = HeatSolver(x, HeatParams(typePrecond=prec), *ftest)
+        bvec = hh.rhs()
+        s = hh.advance_semi_impl()
+        res[prec] = (s["nMatvec"], s["Error"], hh.te(), bvec)
+    Te0 = ftest[0]
+    # flexible GMRES stops on the true residual: check it through the C ABI
+    nM, err, te, bvec = res["LEARNED"]
+    assert err <= 1e-6
+    hh = HeatSolver(x, HeatParams(), *ftest)
+    rel = np.linalg.norm(bvec - hh.matvec(te - Te0)) / np.linalg.norm(bvec)
+    assert rel <= 1.5e-6, rel
+    dT = np.abs(res["BILU"][2] - Te0).max()
+    assert np.abs(te - res["BILU"][2]).max() <= 1e-2 * dT
+    assert nM < res["NONE"][0], {k: v[0] for k, v in res.items()}
+    net.close()
+    x.close()
