@@ -24,6 +24,7 @@ UNITS = [
     ("bx_compat.cu", ["--fmad=false"]),
     ("bx_stage_fp32.cu", []),
     ("bx_stage3d.cu", []),
+    ("bx_stage3d_fpt2.cu", []),
     ("bx_amr.cu", []),
     ("bx_implicit.cu", ["--fmad=false"]),
     ("bx_learned.cu", []),
@@ -32,7 +33,7 @@ UNITS = [
     ("bx_tune.cu", []),
     ("bx_capi.cu", []),
 ]
-HEADERS = ["bx_physics.cuh", "bx_stage.cuh", "bx_device.h", "bx_stage3d.cuh", "bx_tma.cuh", "bx_core.h",
+HEADERS = ["bx_physics.cuh", "bx_stage.cuh", "bx_device.h", "bx_stage3d.cuh", "bx_stage3d_launch.cuh", "bx_tma.cuh", "bx_core.h",
            "bx_impl_kernels.cuh", "bx_krylov.cuh", "bx_tune.h", "bx_tc.cuh", "bx_learned.cuh", "bx_learned_kernels.cuh", "bx_amr.h"]
 
 

@@ -367,52 +367,67 @@ int launch_stage(int iStage) {
 // (they write only the stage buffer, the block time steps and the step
 // state, which are restored) for each candidate number of CTAs per SM
 int tune_stage_impl() {
-  TuneKnobInfo &k = tune_knob(kTuneStageGrid);
-  if (!g.ready || !g.use3d || k.tuned == 2) return BX_OK;
+  TuneKnobInfo &k = tune_knob(kTuneStageGrid), &kf = tune_knob(kTuneStageFpt);
+  if (!g.ready || !g.use3d || (k.tuned == 2 && kf.tuned == 2)) return BX_OK;
   StepState saved;
   std::vector<double> dtSaved(g.nBlock);
   CK(cudaMemcpyAsync(&saved, g.ts, sizeof(StepState), cudaMemcpyDeviceToHost, g.st));
   CK(cudaMemcpyAsync(dtSaved.data(), g.dtBlock, sizeof(double) * g.nBlock, cudaMemcpyDeviceToHost, g.st));
   CK(cudaStreamSynchronize(g.st));
-  const int v0 = k.value;
+  const int v0 = k.value, f0 = kf.value;
+  const bool fixG = k.tuned == 2, fixF = kf.tuned == 2 || g.shape != kShape888;  // faces per thread: 8^3 only
   float best = 1e30f;
-  int bestV = v0;
+  int bestV = v0, bestF = f0;
   cudaEvent_t e0, e1;
   CK(cudaEventCreate(&e0));
   CK(cudaEventCreate(&e1));
   int r = BX_OK;
-  for (int i = 0; i < k.nCand && !r; i++) {
-    k.value = k.cand[i];
-    StageArgs a = stage_args(1, g.sch.nStage == 1);
-    const int kind = g.sch.Precision == BX_FP64 ? kKindFp64 : kKindFp32In64;
-    const TmaMaps *m = g.sch.Precision == BX_FP64 ? (a.in == g.bufX ? &g.mapX64 : &g.mapY64) : &g.mapX64;
-    cudaError_t e = cudaSuccess;
-    for (int rep = 0; rep < 4 && e == cudaSuccess; rep++) {
-      if (rep == 1) e = cudaEventRecord(e0, g.st);
-      if (e == cudaSuccess && g.nSlab)
-        e = launch_reschange(g.shape, g.sch.TypeFlux, kind, a, g.slabs, g.nSlab, g.lcDev,
-                             make_int3(g.nRoot[0], g.nRoot[1], g.nRoot[2]), g.rcGhost, g.rcFlux, g.st);
-      if (e == cudaSuccess) e = launch_stage3d(g.shape, g.sch.TypeFlux, kind, *m, a, g.nSM, g.st);
+  for (int i = 0; i < k.nCand; i++) k.ms[i] = 1e30f;
+  for (int i = 0; i < kf.nCand; i++) kf.ms[i] = 1e30f;
+  for (int jf = 0; jf < kf.nCand && !r; jf++) {
+    if (fixF && kf.cand[jf] != f0) continue;
+    for (int i = 0; i < k.nCand && !r; i++) {
+      if (fixG && k.cand[i] != v0) continue;
+      k.value = k.cand[i];
+      kf.value = kf.cand[jf];
+      StageArgs a = stage_args(1, g.sch.nStage == 1);
+      const int kind = g.sch.Precision == BX_FP64 ? kKindFp64 : kKindFp32In64;
+      const TmaMaps *m = g.sch.Precision == BX_FP64 ? (a.in == g.bufX ? &g.mapX64 : &g.mapY64) : &g.mapX64;
+      cudaError_t e = cudaSuccess;
+      for (int rep = 0; rep < 4 && e == cudaSuccess; rep++) {
+        if (rep == 1) e = cudaEventRecord(e0, g.st);
+        if (e == cudaSuccess && g.nSlab)
+          e = launch_reschange(g.shape, g.sch.TypeFlux, kind, a, g.slabs, g.nSlab, g.lcDev,
+                               make_int3(g.nRoot[0], g.nRoot[1], g.nRoot[2]), g.rcGhost, g.rcFlux, g.st);
+        if (e == cudaSuccess) e = launch_stage3d(g.shape, g.sch.TypeFlux, kind, *m, a, g.nSM, g.st);
+      }
+      if (e == cudaSuccess) e = cudaEventRecord(e1, g.st);
+      if (e == cudaSuccess) e = cudaEventSynchronize(e1);
+      float ms = 0;
+      if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, e0, e1);
+      if (e != cudaSuccess) {
+        r = fail(BX_ERR_CUDA, "autotune of the stage kernel: %s", cudaGetErrorString(e));
+        break;
+      }
+      ms /= 3;
+      // each knob records its best time over the other knob's candidates
+      if (ms < k.ms[i]) k.ms[i] = ms;
+      if (ms < kf.ms[jf]) kf.ms[jf] = ms;
+      if (ms < best) { best = ms; bestV = k.cand[i]; bestF = kf.cand[jf]; }
     }
-    if (e == cudaSuccess) e = cudaEventRecord(e1, g.st);
-    if (e == cudaSuccess) e = cudaEventSynchronize(e1);
-    float ms = 0;
-    if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, e0, e1);
-    if (e != cudaSuccess) {
-      r = fail(BX_ERR_CUDA, "autotune of the stage kernel: %s", cudaGetErrorString(e));
-      break;
-    }
-    k.ms[i] = ms / 3;
-    if (k.ms[i] < best) { best = k.ms[i]; bestV = k.cand[i]; }
   }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   k.value = r ? v0 : bestV;
-  if (!r) k.tuned = 1;
+  kf.value = r ? f0 : bestF;
+  if (!r) {
+    if (!fixG) k.tuned = 1;
+    if (!fixF) kf.tuned = 1;
+  }
   CK(cudaMemcpyAsync(g.ts, &saved, sizeof(StepState), cudaMemcpyHostToDevice, g.st));
   CK(cudaMemcpyAsync(g.dtBlock, dtSaved.data(), sizeof(double) * g.nBlock, cudaMemcpyHostToDevice, g.st));
   CK(cudaStreamSynchronize(g.st));
-  if (g.graph) { cudaGraphExecDestroy(g.graph); g.graph = nullptr; }  // captured with the old grid
+  if (g.graph) { cudaGraphExecDestroy(g.graph); g.graph = nullptr; }  // captured with the old shapes
   return r;
 }
 

@@ -27,9 +27,14 @@
 
 namespace bx {
 
-template <int N_, typename TileT>
+// FPT_: faces per thread in a sweep.  One face per thread gives 576
+// threads for 8^3 blocks (96 registers each); two faces per thread give 288
+// threads with two independent face computations each (168 registers, no
+// spills) and two cells per thread in the update.
+template <int N_, typename TileT, int FPT_ = 1>
 struct Tile3 {
   static constexpr int N = N_;
+  static constexpr int FPT = FPT_;
   static constexpr int NC = N * N * N;
   static constexpr int HX = 16 / (int)sizeof(TileT);
   static constexpr int nIN = 8 * NC;
@@ -40,7 +45,8 @@ struct Tile3 {
   static constexpr int oIN = 0, oXL = oIN + nIN, oXH = oXL + nX, oYL = oXH + nX, oYH = oYL + nY,
                        oZL = oYH + nY, oZH = oZL + nZ, nAll = oZH + nZ;
   static constexpr int NF = (N + 1) * N * N;             // faces per direction
-  static constexpr int NTHR = ((NF + 31) / 32) * 32;     // one face per thread
+  static constexpr int NTHR = (((NF + FPT - 1) / FPT + 31) / 32) * 32;  // FPT faces per thread
+  static constexpr int CPC = (NC + NTHR - 1) / NTHR;      // update cells per thread
   static constexpr int NHALO_CELLS = (nAll - nIN) / 8;   // ghost cells in the tile
   static constexpr int NCELLS = NC + NHALO_CELLS;
   static constexpr int CPT = (NCELLS + NTHR - 1) / NTHR; // conversion cells per thread
@@ -168,12 +174,15 @@ __device__ __forceinline__ bool face_slots(Real (&L)[8], Real (&R)[8], Real gamm
 // bit s set where side s borders a coarser / finer block
 template <class T, int D, int FLUX, int LIM, typename TileT, typename Real>
 __device__ __forceinline__ void sweep3(const StageArgs &a, const BlockGeom &g, const TileT *tile, Real *fbuf,
-                                       double (&chg)[8], double &divB, double &vdt, int &err, int rcFine,
-                                       int rcCoarse, int b) {
+                                       double (&chg)[T::CPC][8], double (&divB)[T::CPC], double (&vdt)[T::CPC],
+                                       int &err, int rcFine, int rcCoarse, int b) {
   const int t = threadIdx.x;
-  if (t < T::NF) {
+#pragma unroll
+  for (int r = 0; r < T::FPT; r++) {
+    const int f = t + r * T::NTHR;
+    if (f >= T::NF) continue;
     int i, j, k;
-    face_ijk<T, D>(t, i, j, k);
+    face_ijk<T, D>(f, i, j, k);
     const int fn = D == 0 ? i : (D == 1 ? j : k);  // face index along D
     const int side = fn == 0 ? 2 * D : (fn == T::N ? 2 * D + 1 : -1);
     const bool first = a.nOrder == 1 || (side >= 0 && ((rcFine >> side) & 1));
@@ -195,30 +204,33 @@ __device__ __forceinline__ void sweep3(const StageArgs &a, const BlockGeom &g, c
       if (first) { L[v] = q1; R[v] = q2; }
       else limited_face_t<LIM>(beta, q0, q1, q2, q3, L[v], R[v]);
     }
-    if (!face_slots<D, FLUX, Real>(L, R, (Real)a.gamma, (Real)a.invGm1, (Real)g.area[D], fbuf + t, T::NF)) err = 1;
+    if (!face_slots<D, FLUX, Real>(L, R, (Real)a.gamma, (Real)a.invGm1, (Real)g.area[D], fbuf + f, T::NF)) err = 1;
     if (side >= 0 && ((rcCoarse >> side) & 1)) {
       // apply_cons_flux: the summed fluxes of the finer faces
       const int t0 = D == 0 ? j : i, t1 = D == 2 ? j : k;
       const double *cf = a.rcFlux + ((size_t)a.rcSlab[6 * b + side] * T::N * T::N + t0 + T::N * t1) * kRcSlots;
 #pragma unroll
-      for (int q = 0; q < kRcSlots; q++) fbuf[q * T::NF + t] = (Real)cf[q];
+      for (int q = 0; q < kRcSlots; q++) fbuf[q * T::NF + f] = (Real)cf[q];
     }
   }
   __syncthreads();
-  if (t < T::NC) {
-    const int i = t % T::N, j = (t / T::N) % T::N, k = t / (T::N * T::N);
+#pragma unroll
+  for (int r = 0; r < T::CPC; r++) {
+    const int c = t + r * T::NTHR;
+    if (c >= T::NC) continue;
+    const int i = c % T::N, j = (c / T::N) % T::N, k = c / (T::N * T::N);
     const int f0 = face_id<T, D>(i, j, k);
     const int f1 = face_id<T, D>(i + (D == 0), j + (D == 1), k + (D == 2));
 #pragma unroll
     for (int v = 0; v < 8; v++) {
       const double d = (double)fbuf[v * T::NF + f0] - (double)fbuf[v * T::NF + f1];
-      chg[v] = D == 0 ? d : chg[v] + d;
+      chg[r][v] = D == 0 ? d : chg[r][v] + d;
     }
     // div B from the face normal field, (L+R)/2 differences over the cell
     const double db = g.invHalf[D] * ((double)fbuf[9 * T::NF + f1] - (double)fbuf[9 * T::NF + f0]);
-    divB = D == 0 ? db : divB + db;
+    divB[r] = D == 0 ? db : divB[r] + db;
     const double vm = fmax((double)fbuf[8 * T::NF + f0], (double)fbuf[8 * T::NF + f1]);
-    vdt = D == 0 ? vm : vdt + vm;
+    vdt[r] = D == 0 ? vm : vdt[r] + vm;
   }
   __syncthreads();
 }
@@ -339,70 +351,77 @@ __global__ void __launch_bounds__(T::NTHR, 1)
       __syncthreads();
     }
 
-    double chg[8], divB = 0, vdt = 0;
+    double chg[T::CPC][8], divB[T::CPC], vdt[T::CPC];
     sweep3<T, 0, FLUX, LIM, TileT, Real>(a, g, tile, fbuf, chg, divB, vdt, err, rcFine, rcCoarse, b);
     sweep3<T, 1, FLUX, LIM, TileT, Real>(a, g, tile, fbuf, chg, divB, vdt, err, rcFine, rcCoarse, b);
     sweep3<T, 2, FLUX, LIM, TileT, Real>(a, g, tile, fbuf, chg, divB, vdt, err, rcFine, rcCoarse, b);
 
-    // update_state_normal / update_explicit for the thread's cell
+    // update_state_normal / update_explicit for the thread's cells
     double dtmin = 1e300;
-    if (t < T::NC && a.outputResidual) {
-      // get_residual: increment of the implicit variables (energy in slot 7)
-      OutT *out = reinterpret_cast<OutT *>(a.out) + (size_t)b * 8 * T::NC;
-      const size_t cell = (size_t)b * T::NC + t;
-      const double dtl = a.dtScale * (a.dtCellIn ? a.dtCellIn[cell] : DtNoCfl);
-      if (a.computeDt) {
-        dtmin = g.volume / vdt;
-        if (a.dtCellOut) a.dtCellOut[cell] = dtmin;
-      }
-      double src[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-      if (a.useDivb) {
-        const int ii = t % T::N, jj = (t / T::N) % T::N, kk = t / (T::N * T::N);
-        const int c0 = tile_index<T, TileT>(0, ii, jj, kk);
-        const double ux = tile[c0 + kUx * T::NC], uy = tile[c0 + kUy * T::NC], uz = tile[c0 + kUz * T::NC];
-        const double bx = tile[c0 + kBx * T::NC], by = tile[c0 + kBy * T::NC], bz = tile[c0 + kBz * T::NC];
-        src[kBx] = -divB * ux; src[kBy] = -divB * uy; src[kBz] = -divB * uz;
-        src[kE] = -divB * (bx * ux + by * uy + bz * uz);
-        src[kUx] = -divB * bx; src[kUy] = -divB * by; src[kUz] = -divB * bz;
-      }
-      const double invV = 1.0 / g.volume;
 #pragma unroll
-      for (int v = 0; v < 8; v++) out[v * T::NC + t] = (OutT)(dtl * (src[v] + chg[v] * invV));
-    } else if (t < T::NC) {
-      const double *old = a.old + (size_t)b * 8 * T::NC;
-      OutT *out = reinterpret_cast<OutT *>(a.out) + (size_t)b * 8 * T::NC;
-      double o[8];
-#pragma unroll
-      for (int v = 0; v < 8; v++) o[v] = old[v * T::NC + t];
-      if (a.computeDt) {
-        dtmin = g.volume / vdt;
-        if (a.dtCellOut) a.dtCellOut[(size_t)b * T::NC + t] = dtmin;
-      }
-      if (DtNoCfl == 0.0) {
-#pragma unroll
-        for (int v = 0; v < 8; v++) out[v * T::NC + t] = (OutT)o[v];
-      } else {
+    for (int r = 0; r < T::CPC; r++) {
+      const int cc = t + r * T::NTHR;
+      if (cc >= T::NC) continue;
+      if (a.outputResidual) {
+        // get_residual: increment of the implicit variables (energy in slot 7)
+        OutT *out = reinterpret_cast<OutT *>(a.out) + (size_t)b * 8 * T::NC;
+        const size_t cell = (size_t)b * T::NC + cc;
+        const double dtl = a.dtScale * (a.dtCellIn ? a.dtCellIn[cell] : DtNoCfl);
+        if (a.computeDt) {
+          const double dtc = g.volume / vdt[r];
+          dtmin = fmin(dtmin, dtc);
+          if (a.dtCellOut) a.dtCellOut[cell] = dtc;
+        }
         double src[8] = {0, 0, 0, 0, 0, 0, 0, 0};
         if (a.useDivb) {
-          const int ii = t % T::N, jj = (t / T::N) % T::N, kk = t / (T::N * T::N);
+          const int ii = cc % T::N, jj = (cc / T::N) % T::N, kk = cc / (T::N * T::N);
           const int c0 = tile_index<T, TileT>(0, ii, jj, kk);
           const double ux = tile[c0 + kUx * T::NC], uy = tile[c0 + kUy * T::NC], uz = tile[c0 + kUz * T::NC];
           const double bx = tile[c0 + kBx * T::NC], by = tile[c0 + kBy * T::NC], bz = tile[c0 + kBz * T::NC];
-          src[kBx] = -divB * ux; src[kBy] = -divB * uy; src[kBz] = -divB * uz;
-          src[kE] = -divB * (bx * ux + by * uy + bz * uz);
-          src[kUx] = -divB * bx; src[kUy] = -divB * by; src[kUz] = -divB * bz;
+          src[kBx] = -divB[r] * ux; src[kBy] = -divB[r] * uy; src[kBz] = -divB[r] * uz;
+          src[kE] = -divB[r] * (bx * ux + by * uy + bz * uz);
+          src[kUx] = -divB[r] * bx; src[kUy] = -divB[r] * by; src[kUz] = -divB[r] * bz;
         }
         const double invV = 1.0 / g.volume;
-        double e = invGm1 * o[kP] + 0.5 * (o[kUx] * o[kUx] + o[kUy] * o[kUy] + o[kUz] * o[kUz]) / o[kRho];
-        e = e + 0.5 * (o[kBx] * o[kBx] + o[kBy] * o[kBy] + o[kBz] * o[kBz]);
-        double n[8];
 #pragma unroll
-        for (int v = 0; v < 7; v++) n[v] = o[v] + DtLocal * (src[v] + chg[v] * invV);
-        e = e + DtLocal * (src[kE] + chg[kE] * invV);
-        const double p = e - 0.5 * (n[kBx] * n[kBx] + n[kBy] * n[kBy] + n[kBz] * n[kBz]);
-        n[kP] = gm1 * (p - 0.5 * (n[kUx] * n[kUx] + n[kUy] * n[kUy] + n[kUz] * n[kUz]) / n[kRho]);
+        for (int v = 0; v < 8; v++) out[v * T::NC + cc] = (OutT)(dtl * (src[v] + chg[r][v] * invV));
+      } else {
+        const double *old = a.old + (size_t)b * 8 * T::NC;
+        OutT *out = reinterpret_cast<OutT *>(a.out) + (size_t)b * 8 * T::NC;
+        double o[8];
 #pragma unroll
-        for (int v = 0; v < 8; v++) out[v * T::NC + t] = (OutT)n[v];
+        for (int v = 0; v < 8; v++) o[v] = old[v * T::NC + cc];
+        if (a.computeDt) {
+          const double dtc = g.volume / vdt[r];
+          dtmin = fmin(dtmin, dtc);
+          if (a.dtCellOut) a.dtCellOut[(size_t)b * T::NC + cc] = dtc;
+        }
+        if (DtNoCfl == 0.0) {
+#pragma unroll
+          for (int v = 0; v < 8; v++) out[v * T::NC + cc] = (OutT)o[v];
+        } else {
+          double src[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+          if (a.useDivb) {
+            const int ii = cc % T::N, jj = (cc / T::N) % T::N, kk = cc / (T::N * T::N);
+            const int c0 = tile_index<T, TileT>(0, ii, jj, kk);
+            const double ux = tile[c0 + kUx * T::NC], uy = tile[c0 + kUy * T::NC], uz = tile[c0 + kUz * T::NC];
+            const double bx = tile[c0 + kBx * T::NC], by = tile[c0 + kBy * T::NC], bz = tile[c0 + kBz * T::NC];
+            src[kBx] = -divB[r] * ux; src[kBy] = -divB[r] * uy; src[kBz] = -divB[r] * uz;
+            src[kE] = -divB[r] * (bx * ux + by * uy + bz * uz);
+            src[kUx] = -divB[r] * bx; src[kUy] = -divB[r] * by; src[kUz] = -divB[r] * bz;
+          }
+          const double invV = 1.0 / g.volume;
+          double e = invGm1 * o[kP] + 0.5 * (o[kUx] * o[kUx] + o[kUy] * o[kUy] + o[kUz] * o[kUz]) / o[kRho];
+          e = e + 0.5 * (o[kBx] * o[kBx] + o[kBy] * o[kBy] + o[kBz] * o[kBz]);
+          double n[8];
+#pragma unroll
+          for (int v = 0; v < 7; v++) n[v] = o[v] + DtLocal * (src[v] + chg[r][v] * invV);
+          e = e + DtLocal * (src[kE] + chg[r][kE] * invV);
+          const double p = e - 0.5 * (n[kBx] * n[kBx] + n[kBy] * n[kBy] + n[kBz] * n[kBz]);
+          n[kP] = gm1 * (p - 0.5 * (n[kUx] * n[kUx] + n[kUy] * n[kUy] + n[kUz] * n[kUz]) / n[kRho]);
+#pragma unroll
+          for (int v = 0; v < 8; v++) out[v * T::NC + cc] = (OutT)n[v];
+        }
       }
     }
     if (a.computeDt) {

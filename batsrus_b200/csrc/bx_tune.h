@@ -16,6 +16,7 @@ enum TuneKnob {
   kTuneKryUnroll,      // Krylov MGS step: independent 16-byte loads in flight per thread and vector
   kTuneHeatIluWarps,   // heat ILU sweeps: warps (groups of 32 blocks) per CTA
   kTuneBiluThreads,    // JFNK BILU sweeps: threads per block CTA (8 per cell of a wavefront)
+  kTuneStageFpt,       // stage kernel, 8^3 blocks: faces per thread (1: 576 threads, 2: 288)
   kNumTune
 };
 

@@ -1,7 +1,8 @@
 """The autotuner (bx_autotune, bx_tune_set): every candidate launch shape of
-a knob computes the same result (bit for bit where the knob does not touch a
-reduction order), and bx_autotune picks a candidate of every knob whose
-context is ready, times it, and keeps knobs that the caller set."""
+a knob computes the same result (bit for bit where neither a reduction order
+nor a separate instantiation of a kernel is involved, to rounding
+otherwise), and bx_autotune picks a candidate of every knob whose context is
+ready, times it, and keeps knobs that the caller set."""
 import numpy as np
 import pytest
 
@@ -37,6 +38,27 @@ def test_stage_grid_candidates_bit_identical():
     ref = out[1]
     for v, a in out.items():
         assert np.array_equal(a, ref), v
+
+
+@pytest.mark.parametrize("prec", ["fp64", "fp32"])
+def test_stage_faces_per_thread_bit_identical(prec):
+    # 8^3 blocks, HLLD and Linde with the Koren limiter, a blast state
+    out = {}
+    for flux in ("Linde", "HLLD"):
+        g, s, st, _ = configs.uniform_3d_case(2, flux, "mc3", 1.2, precision=prec, state="blast")
+        for f in capi.tune_info()["stage_faces_per_thread"]["candidates"]:
+            capi.tune_set("stage_faces_per_thread", f)
+            x = ExplicitSolver(g, s)
+            x.set_state(st)
+            x.advance(3)
+            out[(flux, f)] = (x.get_state(), x.time())
+            x.close()
+        # the instantiations may contract multiply-adds differently, so the
+        # variants agree to rounding (FP64 came out identical here)
+        a, b = out[(flux, 2)][0], out[(flux, 1)][0]
+        rel = np.abs(a - b).max() / np.abs(b).max()
+        assert rel <= (1e-13 if prec == "fp64" else 1e-5), (flux, rel)
+        assert abs(out[(flux, 2)][1][0] - out[(flux, 1)][1][0]) <= 1e-12 * abs(out[(flux, 1)][1][0])
 
 
 def heat_case(nRoot=2, prec="BILU"):
@@ -99,7 +121,7 @@ def test_autotune_picks_candidates_and_keeps_caller_choice():
     x, h, _ = heat_case(nRoot=4)
     capi.tune_set("krylov_unroll", 1)
     knobs = x.autotune()
-    for name in ("stage_ctas_per_sm", "krylov_ctas_per_sm", "heat_ilu_warps"):
+    for name in ("stage_ctas_per_sm", "stage_faces_per_thread", "krylov_ctas_per_sm", "heat_ilu_warps"):
         k = knobs[name]
         assert k["tuned"] == 1 and k["value"] in k["candidates"], (name, k)
         assert all(m > 0 for m in k["ms"]), (name, k)
