@@ -76,30 +76,59 @@ __device__ __forceinline__ float2 unpack_bf16x2(uint32_t u) {
 
 // one thread: the MMAs of one convolution over the five M tiles.
 // KCIN = input chunks of 8 channels (two per K step), N = output channels;
-// flip selects the transposed product (operand read at cell - tap).
-template <int KCIN, int N>
-__device__ __forceinline__ void issue_conv(uint32_t bufIn, uint32_t wImg, uint32_t tmem, bool flip) {
+// FLIP selects the transposed product (operand read at cell - tap).
+// The two shared-memory descriptors are built once: the address field counts
+// 16-byte units and every operand lies inside the CTA's shared window (below
+// 256 KB), so the operand of a tap and K step is the base descriptor plus a
+// compile-time offset, and the fully unrolled loop issues one MMA per add.
+template <int KCIN, int N, bool FLIP>
+__device__ __forceinline__ void issue_conv(uint32_t bufIn, uint32_t wImg, uint32_t tmem) {
   constexpr int LS = KCIN * 160;
   constexpr uint32_t idesc = tc::idesc_bf16(128, N, false, false);
-  constexpr int tapBytes = N * KCIN * 16;
+  constexpr int tapUnits = N * KCIN;  // tap stride of the weight image, 16-byte units
+  const uint64_t a00 = tc::sdesc(bufIn, 160, LS), b00 = tc::sdesc(wImg, 128, KCIN * 128);
   tc::fence_after();
 #pragma unroll 1
   for (int t = 0; t < kTiles; t++) {
-    const int L0 = tile_line0(t);
-#pragma unroll 1
-    for (int tap = 0; tap < kTaps; tap++) {
-      int dz = tap / 9 - 1, dy = (tap / 3) % 3 - 1, dx = tap % 3 - 1;
-      if (flip) { dz = -dz; dy = -dy; dx = -dx; }
-      const uint32_t a0 = bufIn + (uint32_t)((L0 + dz * 9 + dy) * LS + (1 + dx) * 16);
-      const uint32_t b0 = wImg + (uint32_t)(tap * tapBytes);
+    const uint64_t aT = a00 + (uint64_t)((tile_line0(t) * LS + 16) >> 4);
+    const uint32_t d = tmem + (uint32_t)(t * N);
 #pragma unroll
-      for (int s = 0; s < KCIN / 2; s++) {
-        const uint64_t ad = tc::sdesc(a0 + s * 320, 160, LS);
-        const uint64_t bd = tc::sdesc(b0 + s * 256, 128, KCIN * 128);
-        tc::mma_bf16(tmem + (uint32_t)(t * N), ad, bd, idesc, (tap | s) != 0);
-      }
+    for (int tap = 0; tap < kTaps; tap++) {
+      const int sg = FLIP ? -1 : 1;
+      const int dz = sg * (tap / 9 - 1), dy = sg * ((tap / 3) % 3 - 1), dx = sg * (tap % 3 - 1);
+      const int aoff = (dz * 9 + dy) * (LS / 16) + dx;
+#pragma unroll
+      for (int s = 0; s < KCIN / 2; s++)
+        tc::mma_bf16(d, aT + (uint64_t)(int64_t)(aoff + s * 20), b00 + (uint64_t)(tap * tapUnits + s * 16), idesc,
+                     (tap | s) != 0);
     }
   }
+}
+
+// one thread: the MMAs of M tile t of a convolution (the same operands as
+// issue_conv), committed to bar.  Several warps may issue different tiles at
+// once: the tiles accumulate into disjoint TMEM columns, and a commit tracks
+// the MMAs of the thread that issues it.
+template <int KCIN, int N, bool FLIP>
+__device__ __forceinline__ void issue_conv_tile(int t, uint32_t bufIn, uint32_t wImg, uint32_t tmem, uint64_t *bar) {
+  constexpr int LS = KCIN * 160;
+  constexpr uint32_t idesc = tc::idesc_bf16(128, N, false, false);
+  constexpr int tapUnits = N * KCIN;
+  const uint64_t aT = tc::sdesc(bufIn + (uint32_t)(tile_line0(t) * LS + 16), 160, LS);
+  const uint64_t b00 = tc::sdesc(wImg, 128, KCIN * 128);
+  const uint32_t d = tmem + (uint32_t)(t * N);
+  tc::fence_after();
+#pragma unroll
+  for (int tap = 0; tap < kTaps; tap++) {
+    const int sg = FLIP ? -1 : 1;
+    const int dz = sg * (tap / 9 - 1), dy = sg * ((tap / 3) % 3 - 1), dx = sg * (tap % 3 - 1);
+    const int aoff = (dz * 9 + dy) * (LS / 16) + dx;
+#pragma unroll
+    for (int s = 0; s < KCIN / 2; s++)
+      tc::mma_bf16(d, aT + (uint64_t)(int64_t)(aoff + s * 20), b00 + (uint64_t)(tap * tapUnits + s * 16), idesc,
+                   (tap | s) != 0);
+  }
+  tc::commit(bar);
 }
 
 // copy n bytes (multiple of 16) global -> shared with 16-byte loads

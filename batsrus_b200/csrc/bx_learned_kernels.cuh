@@ -24,6 +24,7 @@ constexpr int kErrTimeout = 1;
 
 struct Smem {
   uint64_t bar;
+  uint64_t tileBar[kTiles];  // per M tile completion (inference)
   uint32_t tmem;
   int ok;
   double red[8];
@@ -74,6 +75,33 @@ __device__ __forceinline__ void for_tiles(uint32_t tmem, F &&f) {
   }
 }
 
+// the same over the tiles of a convolution whose MMAs were committed tile by
+// tile: each warp waits (bounded) for its tile's barrier before reading its
+// accumulator; a wait that gives up clears S.ok and skips the unit
+template <int N, class F>
+__device__ __forceinline__ void for_tiles_wait(uint32_t tmem, Smem &S, uint32_t phase, F &&f) {
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  for (int u = warp; u < 4 * kTiles; u += kThreads / 32) {
+    const int tile = u >> 2, q = u & 3;
+    const bool ready = __all_sync(0xffffffffu, mbar_wait_bounded(&S.tileBar[tile], phase));
+    if (!ready) {
+      if (lane == 0) S.ok = 0;
+      continue;
+    }
+    tc::fence_after();
+    const int row = 32 * q + lane;
+    float acc[N];
+#pragma unroll
+    for (int h = 0; h < N / 16; h++) {
+      float v[16];
+      tc::tmem_ld16(tmem + ((uint32_t)(32 * q) << 16) + (uint32_t)(tile * N + 16 * h), v);
+#pragma unroll
+      for (int i = 0; i < 16; i++) acc[16 * h + i] = v[i];
+    }
+    f(tile, row, tile_row_cell(tile, row), acc);
+  }
+}
+
 // bias (+ ReLU), BF16 into the 32-channel buffer (and optionally global)
 __device__ __forceinline__ void relu_store32(unsigned char *buf, const float *bias, int cell, const float (&acc)[32],
                                              __nv_bfloat16 *gout, int relu) {
@@ -104,11 +132,17 @@ __device__ __forceinline__ void setup(Smem &S, const Weights &W) {
 
 // ---------------------------------------------------------------------------
 // inference: z[b] = identCoef v[b] + s outScale N(v[b]/s, feat[b]) for every
-// block; v, z are FP64
-// [block][var][cell] (512 cells), feat BF16 [block][cell][8]
+// block; v, z are FP64 [block][var][cell] (512 cells), feat BF16
+// [block][cell][8].
+// Per block: the three convolutions, the MMAs of M tile t issued by lane 0
+// of warp t and committed to the tile's mbarrier, and each tile's epilogue as
+// soon as its tile is done.  Thread t holds cells t and t + 256 of the next block's input in
+// registers: their loads are issued before the last layer's epilogue, so
+// that they arrive while this block finishes.
 __global__ void __launch_bounds__(kThreads, 1)
     k_net_apply(Weights W, const double *__restrict__ v, double *__restrict__ z,
                 const __nv_bfloat16 *__restrict__ feat, int nBlock, int *err) {
+  static_assert(kThreads * 2 == 512, "two cells of the input per thread");
   extern __shared__ __align__(1024) unsigned char sm[];
   unsigned char *bufA = sm, *bufB = sm + kBuf32;
   unsigned char *w1 = bufB + kBuf32, *w2 = w1 + kW1Bytes, *w3 = w2 + kW2Bytes;
@@ -119,78 +153,100 @@ __global__ void __launch_bounds__(kThreads, 1)
   copy_g2s(w2, W.w2, kW2Bytes);
   copy_g2s(w3, W.w3, kW3Bytes);
   setup(S, W);
+  if (threadIdx.x == 0) {
+    for (int t = 0; t < kTiles; t++) mbar_init(&S.tileBar[t], 1);
+    S.ok = 1;
+    fence_mbar_init();
+  }
   if ((threadIdx.x >> 5) == 0) tc::tmem_alloc(&S.tmem, 256);
   tc::fence_before();
   __syncthreads();
   tc::fence_after();
   const uint32_t tmem = S.tmem;
+  const int c0 = threadIdx.x, c1 = threadIdx.x + 256;
+  double vin[2][8];  // this thread's two cells of the block's input
+  auto load_input = [&](int b) {
+    if (b >= nBlock) return;
+    const double *vb = v + (size_t)b * 4096;
+#pragma unroll
+    for (int m = 0; m < 8; m++) {
+      vin[0][m] = vb[m * 512 + c0];
+      vin[1][m] = vb[m * 512 + c1];
+    }
+  };
+  load_input(blockIdx.x);
   uint32_t phase = 0;
   bool ok = true;
-  for (int b = blockIdx.x; b < nBlock && ok; b += gridDim.x) {
-    const double *vb = v + (size_t)b * 4096;
+  for (int b = blockIdx.x; b < nBlock; b += gridDim.x) {
     double ss = 0;
-    for (int i = threadIdx.x; i < 4096; i += kThreads) ss += vb[i] * vb[i];
+#pragma unroll
+    for (int m = 0; m < 8; m++) ss += vin[0][m] * vin[0][m] + vin[1][m] * vin[1][m];
     const double s = sqrt(block_sum_d(ss, S) / 4096.0);
     const float inv = s > 1e-300 ? (float)(1.0 / s) : 0.f;
-    // 16-channel input (aliases bufB): residual / s, then the cell features
+    // 16-channel input (aliases bufB): channels 0..7 the input / s of the
+    // cell units, channels 8..15 the cell features (ReLU mode) or zero, and
+    // zero padding units
     const uint4 *fb = reinterpret_cast<const uint4 *>(feat + (size_t)b * 512 * 8);
     for (int u = threadIdx.x; u < kLines * 20; u += kThreads) {
       const int line = u / 20, kc = (u / 10) & 1, xs = u % 10;
       uint4 q = make_uint4(0, 0, 0, 0);
-      if (unit_is_cell(line, xs)) {
-        const int c = (xs - 1) + 8 * ((line % 9 - 1) + 8 * (line / 9 - 1));
-        if (kc == 0) {
-          uint32_t *w = reinterpret_cast<uint32_t *>(&q);
+      if (kc == 1 && W.relu && unit_is_cell(line, xs))
+        q = fb[(xs - 1) + 8 * ((line % 9 - 1) + 8 * (line / 9 - 1))];
+      if (kc == 1 || !unit_is_cell(line, xs)) *reinterpret_cast<uint4 *>(bufB + u * 16) = q;
+    }
 #pragma unroll
-          for (int m = 0; m < 4; m++)
-            w[m] = pack_bf16x2((float)vb[(2 * m) * 512 + c] * inv, (float)vb[(2 * m + 1) * 512 + c] * inv);
-        } else if (W.relu) {
-          q = fb[c];
-        }
-      }
-      *reinterpret_cast<uint4 *>(bufB + u * 16) = q;
+    for (int j = 0; j < 2; j++) {
+      uint4 q;
+      uint32_t *w = reinterpret_cast<uint32_t *>(&q);
+#pragma unroll
+      for (int m = 0; m < 4; m++) w[m] = pack_bf16x2((float)vin[j][2 * m] * inv, (float)vin[j][2 * m + 1] * inv);
+      *reinterpret_cast<uint4 *>(bufB + cell_chunk(j ? c1 : c0, 0, kLS16)) = q;
     }
     fence_proxy_async_smem();
     __syncthreads();
-    if (threadIdx.x == 0) {
-      issue_conv<2, 32>(smem_u32(bufB), smem_u32(w1), tmem, false);
-      tc::commit(&S.bar);
-    }
-    if (!(ok = wait_mma(S, phase))) break;
-    zero_pads(bufB, 4);
-    for_tiles<32>(tmem, [&](int, int, int cell, const float(&acc)[32]) {
+    if ((threadIdx.x & 31) == 0 && threadIdx.x < 32 * kTiles)
+      issue_conv_tile<2, 32, false>(threadIdx.x >> 5, smem_u32(bufB), smem_u32(w1), tmem, &S.tileBar[threadIdx.x >> 5]);
+    for_tiles_wait<32>(tmem, S, phase, [&](int, int, int cell, const float(&acc)[32]) {
       if (cell >= 0) relu_store32(bufA, S.bias, cell, acc, nullptr, W.relu);
     });
+    phase ^= 1u;
+    __syncthreads();  // every tile of layer 1 is done: bufB is free
+    if (!(ok = S.ok != 0)) break;
+    zero_pads(bufB, 4);
     tc::fence_before();
     fence_proxy_async_smem();
     __syncthreads();
-    if (threadIdx.x == 0) {
-      issue_conv<4, 32>(smem_u32(bufA), smem_u32(w2), tmem, false);
-      tc::commit(&S.bar);
-    }
-    if (!(ok = wait_mma(S, phase))) break;
-    for_tiles<32>(tmem, [&](int, int, int cell, const float(&acc)[32]) {
+    if ((threadIdx.x & 31) == 0 && threadIdx.x < 32 * kTiles)
+      issue_conv_tile<4, 32, false>(threadIdx.x >> 5, smem_u32(bufA), smem_u32(w2), tmem, &S.tileBar[threadIdx.x >> 5]);
+    for_tiles_wait<32>(tmem, S, phase, [&](int, int, int cell, const float(&acc)[32]) {
       if (cell >= 0) relu_store32(bufB, S.bias + 32, cell, acc, nullptr, W.relu);
     });
+    phase ^= 1u;
     tc::fence_before();
     fence_proxy_async_smem();
     __syncthreads();
-    if (threadIdx.x == 0) {
-      issue_conv<4, kN3>(smem_u32(bufB), smem_u32(w3), tmem, false);
-      tc::commit(&S.bar);
-    }
-    if (!(ok = wait_mma(S, phase))) break;
+    if (!(ok = S.ok != 0)) break;
+    if ((threadIdx.x & 31) == 0 && threadIdx.x < 32 * kTiles)
+      issue_conv_tile<4, kN3, false>(threadIdx.x >> 5, smem_u32(bufB), smem_u32(w3), tmem, &S.tileBar[threadIdx.x >> 5]);
+    const double *vb = v + (size_t)b * 4096;
     double *zb = z + (size_t)b * 4096;
-    for_tiles<kN3>(tmem, [&](int, int, int cell, const float(&acc)[kN3]) {
+    load_input(b + gridDim.x);
+    for_tiles_wait<kN3>(tmem, S, phase, [&](int, int, int cell, const float(&acc)[kN3]) {
       if (cell >= 0)
 #pragma unroll
         for (int m = 0; m < kC3; m++)
           zb[m * 512 + cell] = W.identCoef * vb[m * 512 + cell] + s * W.outScale * (double)(acc[m] + S.bias[64 + m]);
     });
+    phase ^= 1u;
     tc::fence_before();
     __syncthreads();
+    if (!(ok = S.ok != 0)) break;
   }
-  if (!ok && threadIdx.x == 0) atomicOr(err, kErrTimeout);
+  if (!ok && threadIdx.x == 0) {
+    atomicOr(err, kErrTimeout);
+    // the MMAs in flight finish before the tensor memory is freed
+    for (int t = 0; t < kTiles; t++) mbar_wait_bounded(&S.tileBar[t], phase ^ 1u);
+  }
   __syncthreads();
   tc::fence_after();
   if ((threadIdx.x >> 5) == 0) tc::tmem_free(tmem, 256);
@@ -234,7 +290,7 @@ __global__ void __launch_bounds__(kThreads, 1)
     fence_proxy_async_smem();
     __syncthreads();
     if (threadIdx.x == 0) {
-      issue_conv<2, 32>(smem_u32(bufB), smem_u32(w1), tmem, false);
+      issue_conv<2, 32, false>(smem_u32(bufB), smem_u32(w1), tmem);
       tc::commit(&S.bar);
     }
     if (!(ok = wait_mma(S, phase))) break;
@@ -247,7 +303,7 @@ __global__ void __launch_bounds__(kThreads, 1)
     fence_proxy_async_smem();
     __syncthreads();
     if (threadIdx.x == 0) {
-      issue_conv<4, 32>(smem_u32(bufA), smem_u32(w2), tmem, false);
+      issue_conv<4, 32, false>(smem_u32(bufA), smem_u32(w2), tmem);
       tc::commit(&S.bar);
     }
     if (!(ok = wait_mma(S, phase))) break;
@@ -258,7 +314,7 @@ __global__ void __launch_bounds__(kThreads, 1)
     fence_proxy_async_smem();
     __syncthreads();
     if (threadIdx.x == 0) {
-      issue_conv<4, kN3>(smem_u32(bufB), smem_u32(w3), tmem, false);
+      issue_conv<4, kN3, false>(smem_u32(bufB), smem_u32(w3), tmem);
       tc::commit(&S.bar);
     }
     if (!(ok = wait_mma(S, phase))) break;
@@ -343,7 +399,7 @@ __global__ void __launch_bounds__(kThreads, 1)
     fence_proxy_async_smem();
     __syncthreads();
     if (threadIdx.x == 0) {
-      issue_conv<2, 32>(smem_u32(bufB), smem_u32(w3t), tmem, true);
+      issue_conv<2, 32, true>(smem_u32(bufB), smem_u32(w3t), tmem);
       tc::commit(&S.bar);
     }
     if (!(ok = wait_mma(S, phase))) break;
@@ -382,7 +438,7 @@ __global__ void __launch_bounds__(kThreads, 1)
     fence_proxy_async_smem();
     __syncthreads();
     if (threadIdx.x == 0) {
-      issue_conv<4, 32>(smem_u32(bufA), smem_u32(w2t), tmem, true);
+      issue_conv<4, 32, true>(smem_u32(bufA), smem_u32(w2t), tmem);
       tc::commit(&S.bar);
     }
     if (!(ok = wait_mma(S, phase))) break;
@@ -449,14 +505,17 @@ __global__ void __launch_bounds__(kThreads, 1)
     if (threadIdx.x == 0) {
       tc::fence_after();
       const uint32_t x0 = smem_u32(bufX), d0 = smem_u32(bufD);
+      // descriptors advance by two lines (2 LS / 16 address units) per MMA
+      const uint64_t ad0 = tc::sdesc(d0 + (uint32_t)(10 * LSD + 16), LSD, 160);
       for (int tl = 0; tl < nTap; tl++) {
         const int tap = tap0 + tl;
         const int dz = tap / 9 - 1, dy = (tap / 3) % 3 - 1, dx = tap % 3 - 1;
-        for (int L = 10; L <= 80; L += 2) {
-          const uint64_t ad = tc::sdesc(d0 + (uint32_t)(L * LSD + 16), LSD, 160);
-          const uint64_t bd = tc::sdesc(x0 + (uint32_t)((L + dz * 9 + dy) * LSX + (1 + dx) * 16), LSX, 160);
-          tc::mma_bf16(tmem + (uint32_t)(tl * CIN), ad, bd, idesc, (first && L == 10) ? 0u : 1u);
-        }
+        const uint64_t bd0 = tc::sdesc(x0 + (uint32_t)((10 + dz * 9 + dy) * LSX + (1 + dx) * 16), LSX, 160);
+        const uint32_t d = tmem + (uint32_t)(tl * CIN);
+#pragma unroll
+        for (int j = 0; j < 36; j++)  // lines L = 10 + 2 j, 10..80
+          tc::mma_bf16(d, ad0 + (uint64_t)(j * (2 * LSD / 16)), bd0 + (uint64_t)(j * (2 * LSX / 16)), idesc,
+                       (first && j == 0) ? 0u : 1u);
       }
       tc::commit(&S.bar);
     }
