@@ -39,7 +39,10 @@ EXPORTS = (
     "bx_heat_init", "bx_advance_semi_impl", "bx_heat_get_te", "bx_heat_get_rhs", "bx_heat_matvec",
     "bx_heat_precond",
     "bx_autotune", "bx_tune_info", "bx_tune_set", "bx_tune_reset",
+    "bx_amr_criteria", "bx_regrid",
 )
+# #AMRCRITERIA TypeRefine -> BX_AMR_*
+AMR_CRIT = {"gradt": 1, "gradlogrho": 2, "gradlogp": 3, "gradp": 4, "pjumpratio": 5}
 PRECOND = {"none": 0, "bilu": 1, "learned": 2}
 NOALLOC_MAX_BLOCK = 32768  # BX_NOALLOC_MAX_BLOCK
 
@@ -163,6 +166,7 @@ def load():
         "bx_autotune": [], "bx_tune_set": [ctypes.c_char_p, i], "bx_tune_reset": [],
         "bx_tune_info": [i, ctypes.c_char_p, i, ip, ip, ip, ip, fp],
         "bx_heat_get_te": [dp], "bx_heat_get_rhs": [dp], "bx_heat_matvec": [dp, dp], "bx_heat_precond": [dp, dp],
+        "bx_amr_criteria": [i, ip, dp], "bx_regrid": [ctypes.POINTER(GridDesc), ip],
     }
     for name, args in sig.items():
         f = getattr(L, name)

@@ -28,6 +28,44 @@ __device__ __forceinline__ long gidx(const int *lc, int blk, int e, int N, int x
   return (long)lc[4 * blk + 1 + e] * N + x;
 }
 
+// state value (variable v) of the ghost cell x3 (block-local coordinates,
+// x3[d] = -1 - l or N + l) across the resolution-change side S: a coarser
+// neighbour's cell copied into the finer ghost cells it covers (injection),
+// or the mean of the 2x2x2 finer cells in a fixed order (restriction)
+template <int N, typename InT>
+__device__ __forceinline__ double rc_ghost_value(const InT *in, const RcSlab &S, const int *lc, const int nr[3],
+                                                 const int x3[3], int v) {
+  constexpr int NC = N * N * N;
+  const int d = S.side >> 1;
+  const int e0 = d == 0 ? 1 : 0, e1 = d == 2 ? 1 : 2;
+  const int lev = lc[4 * S.block];
+  if (S.type == 1) {
+    const int C = S.nb[0];
+    int c3[3];
+    for (int e = 0; e < 3; e++) {
+      const long tot = (long)N * ((long)nr[e] << lev);
+      long gf = gidx(lc, S.block, e, N, x3[e]);
+      gf = (gf + tot) % tot;
+      c3[e] = (int)((gf >> 1) - (long)lc[4 * C + 1 + e] * N);
+    }
+    return (double)in[((size_t)C * 8 + v) * NC + c3[0] + N * (c3[1] + N * c3[2])];
+  }
+  // the finer neighbour covering this transverse quadrant
+  const int F = S.nb[(x3[e0] >= N / 2) + 2 * (x3[e1] >= N / 2)];
+  long f0[3];
+  for (int e = 0; e < 3; e++) {
+    const long tot = (long)N * ((long)nr[e] << lev);
+    const long gc = (gidx(lc, S.block, e, N, x3[e]) + tot) % tot;
+    f0[e] = 2 * gc - (long)lc[4 * F + 1 + e] * N;
+  }
+  double sum = 0.0;
+  for (int kk = 0; kk < 2; kk++)
+    for (int jj = 0; jj < 2; jj++)
+      for (int ii = 0; ii < 2; ii++)
+        sum = sum + (double)in[((size_t)F * 8 + v) * NC + (f0[0] + ii) + N * ((f0[1] + jj) + N * (f0[2] + kk))];
+  return sum * 0.125;
+}
+
 template <int N, typename InT>
 __global__ void k_rc_ghost(const InT *__restrict__ in, const RcSlab *__restrict__ slabs, const int *__restrict__ lc,
                            int3 nRoot, double *ghost) {
@@ -35,8 +73,7 @@ __global__ void k_rc_ghost(const InT *__restrict__ in, const RcSlab *__restrict_
   const int d = S.side >> 1, hi = S.side & 1;
   const int e0 = d == 0 ? 1 : 0, e1 = d == 2 ? 1 : 2;
   const int nr[3] = {nRoot.x, nRoot.y, nRoot.z};
-  const int lev = lc[4 * S.block];
-  constexpr int NC = N * N * N, nSlab = 8 * 2 * N * N;
+  constexpr int nSlab = 8 * 2 * N * N;
   double *out = ghost + (size_t)blockIdx.x * nSlab;
   for (int q = threadIdx.x; q < nSlab; q += blockDim.x) {
     const int t0 = q % N, t1 = (q / N) % N, l = (q / (N * N)) % 2, v = q / (2 * N * N);
@@ -44,33 +81,7 @@ __global__ void k_rc_ghost(const InT *__restrict__ in, const RcSlab *__restrict_
     x3[d] = hi ? N + l : -1 - l;
     x3[e0] = t0;
     x3[e1] = t1;
-    if (S.type == 1) {
-      // injection from the coarser neighbour
-      const int C = S.nb[0];
-      int c3[3];
-      for (int e = 0; e < 3; e++) {
-        const long tot = (long)N * ((long)nr[e] << lev);
-        long gf = gidx(lc, S.block, e, N, x3[e]);
-        gf = (gf + tot) % tot;
-        c3[e] = (int)((gf >> 1) - (long)lc[4 * C + 1 + e] * N);
-      }
-      out[q] = (double)in[((size_t)C * 8 + v) * NC + c3[0] + N * (c3[1] + N * c3[2])];
-    } else {
-      // restriction from the finer neighbour covering this transverse quadrant
-      const int F = S.nb[(t0 >= N / 2) + 2 * (t1 >= N / 2)];
-      long f0[3];
-      for (int e = 0; e < 3; e++) {
-        const long tot = (long)N * ((long)nr[e] << lev);
-        const long gc = (gidx(lc, S.block, e, N, x3[e]) + tot) % tot;
-        f0[e] = 2 * gc - (long)lc[4 * F + 1 + e] * N;
-      }
-      double sum = 0.0;
-      for (int kk = 0; kk < 2; kk++)
-        for (int jj = 0; jj < 2; jj++)
-          for (int ii = 0; ii < 2; ii++)
-            sum = sum + (double)in[((size_t)F * 8 + v) * NC + (f0[0] + ii) + N * ((f0[1] + jj) + N * (f0[2] + kk))];
-      out[q] = sum * 0.125;
-    }
+    out[q] = rc_ghost_value<N>(in, S, lc, nr, x3, v);
   }
 }
 
@@ -174,6 +185,151 @@ cudaError_t launch_reschange(int shape, int flux, int kind, const StageArgs &a, 
                 : rc_launch<4, float, float>(flux, a, slabs, nSlab, lc, nRoot, ghost, fluxBuf, st);
   }
   return cudaErrorInvalidValue;
+}
+
+// ---------------------------------------------------------------------------
+// dynamic AMR: prepare_amr -> amr_criteria and do_amr -> regrid_batl
+// (src/ModAMR.f90:171-386, 388-723)
+
+// per block, the maximum over its cells of each criterion.  The gradient
+// criteria follow calc_gradient3 on a Cartesian block
+// (src/ModCellGradient.f90:345-380): Grad_d = CellFace_d (V(+1) - V(-1))
+// 0.5 / CellVolume, criterion sqrt(max |Grad|^2); pjumpratio is the largest
+// max/min of p over the three cells along each direction
+// (src/ModAMR.f90:483-495).  The ghost cells across the block sides are the
+// neighbour's cells at the same level, the boundary cell itself at a float
+// boundary, and the injection / restriction of rc_ghost_value at a
+// resolution change.  The arithmetic avoids contraction so that it can be
+// restated exactly on the CPU (log10 aside).
+template <int N>
+__global__ void __launch_bounds__(N * N * N) k_amr_crit(AmrCritArgs a) {
+  constexpr int NC = N * N * N;
+  __shared__ double red[NC / 32 > 0 ? NC / 32 : 1];
+  const int b = blockIdx.x, c = threadIdx.x;
+  const int ijk[3] = {c % N, (c / N) % N, c / (N * N)};
+  const int nr[3] = {a.nRoot.x, a.nRoot.y, a.nRoot.z};
+  const BlockGeom g = a.geom[b];
+  // rho and p of the cell (0) and of its neighbours: 1 + 2 d + side
+  double rho[7], p[7];
+  rho[0] = a.in[((size_t)b * 8 + kRho) * NC + c];
+  p[0] = a.in[((size_t)b * 8 + kP) * NC + c];
+#pragma unroll
+  for (int d = 0; d < 3; d++)
+#pragma unroll
+    for (int side = 0; side < 2; side++) {
+      int x3[3] = {ijk[0], ijk[1], ijk[2]};
+      x3[d] += side ? 1 : -1;
+      int blk = b;
+      const int s = 2 * d + side, m = 1 + s;
+      if (x3[d] < 0 || x3[d] >= N) {
+        const int nb = a.nbr[6 * b + s];
+        if (nb >= 0) {
+          blk = nb;
+          x3[d] = side ? 0 : N - 1;
+        } else if (nb == kNbrFloat) {
+          x3[d] = side ? N - 1 : 0;
+        } else {
+          const RcSlab S = a.slabs[a.rcSlab[6 * b + s]];
+          rho[m] = rc_ghost_value<N>(a.in, S, a.lc, nr, x3, kRho);
+          p[m] = rc_ghost_value<N>(a.in, S, a.lc, nr, x3, kP);
+          continue;
+        }
+      }
+      const int cc = x3[0] + N * (x3[1] + N * x3[2]);
+      rho[m] = a.in[((size_t)blk * 8 + kRho) * NC + cc];
+      p[m] = a.in[((size_t)blk * 8 + kP) * NC + cc];
+    }
+  const double vInvHalf = 0.5 / g.volume;
+  for (int q = 0; q < a.nCrit; q++) {
+    const int type = a.type[q];
+    double val;
+    if (type == kAmrPJumpRatio) {
+      val = 0.0;
+#pragma unroll
+      for (int d = 0; d < 3; d++) {
+        const double mx = fmax(fmax(p[1 + 2 * d], p[0]), p[2 + 2 * d]);
+        const double mn = fmin(fmin(p[1 + 2 * d], p[0]), p[2 + 2 * d]);
+        val = fmax(val, __ddiv_rn(mx, mn));
+      }
+    } else {
+      double f[7];
+#pragma unroll
+      for (int m = 0; m < 7; m++) {
+        if (type == kAmrGradT) f[m] = __ddiv_rn(p[m], rho[m]);
+        else if (type == kAmrGradLogRho) f[m] = log10(rho[m]);
+        else if (type == kAmrGradLogP) f[m] = log10(p[m]);
+        else f[m] = p[m];
+      }
+      double g2 = 0.0;
+#pragma unroll
+      for (int d = 0; d < 3; d++) {
+        const double gd = __dmul_rn(__dmul_rn(g.area[d], __dsub_rn(f[2 + 2 * d], f[1 + 2 * d])), vInvHalf);
+        g2 = d == 0 ? __dmul_rn(gd, gd) : __dadd_rn(g2, __dmul_rn(gd, gd));
+      }
+      val = g2;
+    }
+    // block maximum
+    for (int o = 16; o > 0; o >>= 1) val = fmax(val, __shfl_xor_sync(0xffffffffu, val, o));
+    if (NC >= 32) {
+      __syncthreads();
+      if ((c & 31) == 0) red[c >> 5] = val;
+      __syncthreads();
+      if (c == 0) {
+        double m = red[0];
+        for (int w = 1; w < NC / 32; w++) m = fmax(m, red[w]);
+        a.crit[(size_t)b * a.nCrit + q] = type == kAmrPJumpRatio ? m : __dsqrt_rn(m);
+      }
+    }
+  }
+}
+
+// new block b from the old state: a copy, the injection from its parent
+// (octant a + 2 b + 4 c of the parent), or the mean of the 2x2x2 cells of
+// its eight children (in the order of rc_ghost_value)
+template <int N>
+__global__ void k_amr_remap(const double *__restrict__ in, double *__restrict__ out, const int *__restrict__ remap) {
+  constexpr int NC = N * N * N;
+  const int b = blockIdx.x;
+  const int *R = remap + kRemapInts * (size_t)b;
+  const int op = R[0];
+  for (int q = threadIdx.x; q < 8 * NC; q += blockDim.x) {
+    const int v = q / NC, c = q % NC;
+    const int i = c % N, j = (c / N) % N, k = c / (N * N);
+    double val;
+    if (op == kRemapCopy) {
+      val = in[((size_t)R[1] * 8 + v) * NC + c];
+    } else if (op == kRemapProlong) {
+      const int o = R[2];
+      const int pi = (i + (o & 1) * N) >> 1, pj = (j + ((o >> 1) & 1) * N) >> 1, pk = (k + (o >> 2) * N) >> 1;
+      val = in[((size_t)R[1] * 8 + v) * NC + pi + N * (pj + N * pk)];
+    } else {
+      const int ox = i >= N / 2, oy = j >= N / 2, oz = k >= N / 2;
+      const int ch = R[1 + ox + 2 * oy + 4 * oz];
+      const int f0 = 2 * (i - ox * (N / 2)), f1 = 2 * (j - oy * (N / 2)), f2 = 2 * (k - oz * (N / 2));
+      double sum = 0.0;
+      for (int kk = 0; kk < 2; kk++)
+        for (int jj = 0; jj < 2; jj++)
+          for (int ii = 0; ii < 2; ii++)
+            sum = sum + in[((size_t)ch * 8 + v) * NC + (f0 + ii) + N * ((f1 + jj) + N * (f2 + kk))];
+      val = sum * 0.125;
+    }
+    out[((size_t)b * 8 + v) * NC + c] = val;
+  }
+}
+
+cudaError_t launch_amr_crit(int shape, const AmrCritArgs &a, int nBlock, cudaStream_t st) {
+  if (shape == kShape888) k_amr_crit<8><<<nBlock, 512, 0, st>>>(a);
+  else if (shape == kShape444) k_amr_crit<4><<<nBlock, 64, 0, st>>>(a);
+  else return cudaErrorInvalidValue;
+  return cudaGetLastError();
+}
+
+cudaError_t launch_amr_remap(int shape, const double *in, double *out, const int *remap, int nBlockNew,
+                             cudaStream_t st) {
+  if (shape == kShape888) k_amr_remap<8><<<nBlockNew, 256, 0, st>>>(in, out, remap);
+  else if (shape == kShape444) k_amr_remap<4><<<nBlockNew, 256, 0, st>>>(in, out, remap);
+  else return cudaErrorInvalidValue;
+  return cudaGetLastError();
 }
 
 }  // namespace bx

@@ -19,6 +19,30 @@ struct RcSlab {
               // direction fastest)
 };
 
+// dynamic AMR criteria (amr_criteria, src/ModAMR.f90:388-723)
+constexpr int kAmrGradT = 1, kAmrGradLogRho = 2, kAmrGradLogP = 3, kAmrGradP = 4, kAmrPJumpRatio = 5;
+
+struct AmrCritArgs {
+  const double *in;  // U^n [block][var][cell]
+  const int *nbr, *rcSlab, *lc;
+  const RcSlab *slabs;
+  const BlockGeom *geom;
+  int3 nRoot;
+  int nCrit;
+  int type[3];
+  double *crit;  // [block][nCrit]
+};
+
+// regrid remap table: kRemapInts ints per new block: op, then the old block
+// (copy), the old parent and the octant (prolong), or the eight old children
+// by octant a + 2 b + 4 c (restrict); 0-based block indices
+constexpr int kRemapInts = 10;
+constexpr int kRemapCopy = 0, kRemapProlong = 1, kRemapRestrict = 2;
+
+cudaError_t launch_amr_crit(int shape, const AmrCritArgs &a, int nBlock, cudaStream_t st);
+cudaError_t launch_amr_remap(int shape, const double *in, double *out, const int *remap, int nBlockNew,
+                             cudaStream_t st);
+
 // ghost slabs of all resolution-change sides and, for the coarse sides, the
 // summed finer fluxes; lc = level, ix, iy, iz per block
 cudaError_t launch_reschange(int shape, int flux, int kind, const StageArgs &a, const RcSlab *slabs, int nSlab,

@@ -319,10 +319,10 @@ StageArgs stage_args(int iStage, bool computeDt) {
   return a;
 }
 
-// one stage of all blocks (update_state_fast)
-int launch_stage(int iStage) {
-  const bool last = iStage == g.sch.nStage;
-  StageArgs a = stage_args(iStage, last);
+// one stage of all blocks (update_state_fast); the cell time steps are
+// computed in the last stage, or where computeDt asks for them
+int launch_stage_dt(int iStage, bool computeDt) {
+  StageArgs a = stage_args(iStage, computeDt);
   if (g.timing) {
     if (g.nTimed >= (int)g.evStart.size()) {
       cudaEvent_t e0, e1;
@@ -362,6 +362,8 @@ int launch_stage(int iStage) {
   if (g.sch.nStage == 1) std::swap(g.A, g.B);  // new state is in B
   return BX_OK;
 }
+
+int launch_stage(int iStage) { return launch_stage_dt(iStage, iStage == g.sch.nStage); }
 
 // autotune the persistent grid of the stage kernel: time stage-1 launches
 // (they write only the stage buffer, the block time steps and the step
@@ -957,6 +959,106 @@ int bx_advance(int nStep, double tLimit) {
       n++;
     }
   }
+  return check_err_flag();
+}
+
+int bx_amr_criteria(int nCrit, const int *iTypeCrit_I, double *Crit_IB) {
+  NEED_READY();
+  if (nCrit < 1 || nCrit > 3 || !iTypeCrit_I || !Crit_IB) return fail(BX_ERR_ARG, "nCrit=%d (1..3)", nCrit);
+  if (!g.use3d) return fail(BX_ERR_ARG, "AMR criteria need 3D 8x8x8 or 4x4x4 blocks");
+  AmrCritArgs a;
+  a.in = g.A; a.nbr = g.nbr; a.rcSlab = g.rcSlab; a.lc = g.lcDev; a.slabs = g.slabs; a.geom = g.geom;
+  a.nRoot = make_int3(g.nRoot[0], g.nRoot[1], g.nRoot[2]);
+  a.nCrit = nCrit;
+  for (int q = 0; q < nCrit; q++) {
+    if (iTypeCrit_I[q] < BX_AMR_GRADT || iTypeCrit_I[q] > BX_AMR_PJUMPRATIO)
+      return fail(BX_ERR_ARG, "criterion %d: type %d", q + 1, iTypeCrit_I[q]);
+    a.type[q] = iTypeCrit_I[q];
+  }
+  double *dCrit = nullptr;
+  CK(cudaMallocAsync(&dCrit, sizeof(double) * nCrit * g.nBlock, g.st));
+  a.crit = dCrit;
+  cudaError_t e = launch_amr_crit(g.shape, a, g.nBlock, g.st);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(Crit_IB, dCrit, sizeof(double) * nCrit * g.nBlock, cudaMemcpyDeviceToHost, g.st);
+  cudaFreeAsync(dCrit, g.st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(g.st);
+  if (e != cudaSuccess) return fail(BX_ERR_CUDA, "AMR criteria: %s", cudaGetErrorString(e));
+  return BX_OK;
+}
+
+int bx_regrid(const bx_grid_desc *gd, const int *iRemap_IB) {
+  NEED_READY();
+  if (!gd || !iRemap_IB) return fail(BX_ERR_ARG, "null argument");
+  if (!g.use3d) return fail(BX_ERR_ARG, "regrid needs 3D 8x8x8 or 4x4x4 blocks");
+  if (gd->nDim != g.nDim || gd->nI != g.nI || gd->nJ != g.nJ || gd->nK != g.nK)
+    return fail(BX_ERR_ARG, "regrid cannot change the block size");
+  for (int d = 0; d < 3; d++)
+    if (gd->nRootBlock[d] != g.nRoot[d] || gd->CoordMin[d] != g.cmin[d] || gd->CoordMax[d] != g.cmax[d])
+      return fail(BX_ERR_ARG, "regrid cannot change the root grid or the domain");
+  for (int s = 0; s < 6; s++)
+    if (gd->TypeBc[s] != g.typeBc[s]) return fail(BX_ERR_ARG, "regrid cannot change the outer boundaries");
+  const int nOld = g.nBlock, nNew = gd->nBlock;
+  if (nNew < 1 || !gd->iLevelCoord_IB) return fail(BX_ERR_ARG, "empty block list");
+  // the remap table against the old and new trees (1-based blocks at the
+  // boundary, 0-based on the device)
+  std::vector<int> R((size_t)kRemapInts * nNew, -1);
+  for (int b = 0; b < nNew; b++) {
+    const int *in = iRemap_IB + (size_t)kRemapInts * b;
+    const int *lcN = gd->iLevelCoord_IB + 4 * b;
+    int *out = R.data() + (size_t)kRemapInts * b;
+    out[0] = in[0];
+    auto old_ok = [&](int ib) { return ib >= 1 && ib <= nOld; };
+    auto lev = [&](int ib) { return g.lev[ib - 1]; };
+    auto ic = [&](int ib, int d) { return g.ic[3 * (ib - 1) + d]; };
+    bool ok = true;
+    if (in[0] == kRemapCopy) {
+      ok = old_ok(in[1]) && lev(in[1]) == lcN[0];
+      for (int d = 0; ok && d < 3; d++) ok = ic(in[1], d) == lcN[1 + d];
+      if (ok) out[1] = in[1] - 1;
+    } else if (in[0] == kRemapProlong) {
+      ok = old_ok(in[1]) && in[2] >= 0 && in[2] < 8 && lev(in[1]) + 1 == lcN[0];
+      for (int d = 0; ok && d < 3; d++)
+        ok = ic(in[1], d) == (lcN[1 + d] >> 1) && ((in[2] >> d) & 1) == (lcN[1 + d] & 1);
+      if (ok) { out[1] = in[1] - 1; out[2] = in[2]; }
+    } else if (in[0] == kRemapRestrict) {
+      for (int o = 0; ok && o < 8; o++) {
+        ok = old_ok(in[1 + o]) && lev(in[1 + o]) == lcN[0] + 1;
+        for (int d = 0; ok && d < 3; d++) ok = ic(in[1 + o], d) == 2 * lcN[1 + d] + ((o >> d) & 1);
+        if (ok) out[1 + o] = in[1 + o] - 1;
+      }
+    } else {
+      ok = false;
+    }
+    if (!ok) return fail(BX_ERR_ARG, "remap entry of new block %d does not match the old and new trees", b + 1);
+  }
+  // the old state survives the rebuild of the context
+  CK(cudaStreamSynchronize(g.st));
+  StepState ts;
+  CK(cudaMemcpy(&ts, g.ts, sizeof(ts), cudaMemcpyDeviceToHost));
+  double *oldA = g.A;
+  g.A = nullptr;
+  const bx_scheme_params sch = g.sch;
+  int r = bx_init(gd, &sch);
+  if (r) { cudaFree(oldA); return r; }
+  int *dR = nullptr;
+  cudaError_t e = cudaMalloc(&dR, sizeof(int) * R.size());
+  if (e == cudaSuccess) e = cudaMemcpyAsync(dR, R.data(), sizeof(int) * R.size(), cudaMemcpyHostToDevice, g.st);
+  if (e == cudaSuccess) e = launch_amr_remap(g.shape, oldA, g.A, dR, nNew, g.st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(g.st);
+  cudaFree(dR);
+  cudaFree(oldA);
+  if (e != cudaSuccess) return fail(BX_ERR_CUDA, "regrid remap: %s", cudaGetErrorString(e));
+  // time and step count carry over; the next time step is the minimum cell
+  // time step of the new grid: a stage with Dt = 0 copies U into the stage
+  // buffer and computes V / sum(Vdt) of every cell
+  ts.DtNoCfl = 0.0;
+  ts.Dt = 0.0;
+  ts.DtMinBits = 0x7FF0000000000000ull;
+  ts.errFlag = 0;
+  CK(cudaMemcpyAsync(g.ts, &ts, sizeof(ts), cudaMemcpyHostToDevice, g.st));
+  r = launch_stage_dt(1, true);
+  if (r) return r;
+  CK(cudaStreamSynchronize(g.st));
   return check_err_flag();
 }
 

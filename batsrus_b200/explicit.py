@@ -133,6 +133,56 @@ class ExplicitSolver:
     def synchronize(self):
         check(self.L.bx_synchronize())
 
+    # -- dynamic AMR (src/ModAMR.f90) ----------------------------------------
+    def amr_criteria(self, names):
+        """amr_criteria (src/ModAMR.f90:388-723) on the GPU: Crit_IB as an
+        (nBlock, len(names)) array, names from #AMRCRITERIA."""
+        n = len(names)
+        try:
+            codes = (ctypes.c_int * n)(*[capi.AMR_CRIT[str(t).lower()] for t in names])
+        except KeyError as e:
+            raise ValueError("AMR criterion %s is not built (built: %s)" % (e, ", ".join(capi.AMR_CRIT)))
+        out = np.empty((self.grid.nBlock, n))
+        check(self.L.bx_amr_criteria(n, codes, dptr(out)))
+        return out
+
+    def regrid(self, grid, remap):
+        """bx_regrid: replace the grid and move the state onto it."""
+        gd = capi.grid_desc(grid, self._gd.iDevice)
+        R = np.ascontiguousarray(remap, dtype=np.int32)
+        assert R.shape == (grid.nBlock, 10), R.shape
+        check(self.L.bx_regrid(ctypes.byref(gd), R.ctypes.data_as(ctypes.POINTER(ctypes.c_int))))
+        self.grid, self._gd = grid, gd
+
+    def do_amr(self, params):
+        """prepare_amr + do_amr (src/ModAMR.f90:171-386): criteria on the
+        GPU, the new tree on the host (batsrus_b200.amr), the state moved on
+        the GPU.  Returns True if the grid changed."""
+        from . import amr
+        crit = self.amr_criteria([c.name for c in params.criteria])
+        grid, remap, changed = amr.regrid(self.grid, crit, params)
+        if changed:
+            self.regrid(grid, remap)
+        return changed
+
+    def advance_amr(self, nStep, params, TimeSimulationLimit=-1.0):
+        """nStep steps of BATS_advance with do_amr after every step whose
+        number is a multiple of DnRefine (src/ModBatsrusMethods.f90:493-760).
+        Returns the number of regrids that changed the grid."""
+        if params.dnRefine <= 0:
+            self.advance(nStep, TimeSimulationLimit)
+            return 0
+        nRegrid = 0
+        done = 0
+        while done < nStep:
+            n0 = self.time()[2]
+            k = min(nStep - done, params.dnRefine - n0 % params.dnRefine)
+            self.advance(k, TimeSimulationLimit)
+            done += k
+            if self.time()[2] % params.dnRefine == 0:
+                nRegrid += self.do_amr(params)
+        return nRegrid
+
     # -- measurement -----------------------------------------------------------
     def autotune(self):
         """bx_autotune: time the candidate launch shapes of every kernel whose

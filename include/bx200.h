@@ -158,6 +158,30 @@ BX_API int bx_set_graph_steps(int nStepPerGraph);
 /* wait for the library's stream */
 BX_API int bx_synchronize(void);
 
+/* ---- dynamic AMR (src/ModAMR.f90) ---------------------------------------- */
+/* #AMRCRITERIA TypeRefine values (PARAM.XML:6814-6843) that are built */
+enum { BX_AMR_GRADT = 1, BX_AMR_GRADLOGRHO = 2, BX_AMR_GRADLOGP = 3, BX_AMR_GRADP = 4, BX_AMR_PJUMPRATIO = 5 };
+/* prepare_amr -> amr_criteria (src/ModAMR.f90:171-229, 388-723) on the
+ * current state: Crit_IB(nCrit, nBlock), the maximum over each block's cells
+ * of criteria iTypeCrit_I(1:nCrit) (nCrit <= 3), in normalised units. The
+ * ghost cells are filled as by exchange_messages with first-order
+ * prolongation. 3D grids of 8x8x8 or 4x4x4 blocks. */
+BX_API int bx_amr_criteria(int nCrit, const int *iTypeCrit_I, double *Crit_IB);
+/* do_amr -> regrid_batl (src/ModAMR.f90:231-386): replace the grid by gd
+ * (same root grid, domain, boundaries and block size) and move the state
+ * onto it. iRemap_IB(10, gd->nBlock) gives, for each new block: op, then
+ *   op 0 (unchanged):  the old block;
+ *   op 1 (refined):    the old parent block and the octant a + 2b + 4c of
+ *                      the new block in it (injection: each new cell takes
+ *                      the parent cell that covers it);
+ *   op 2 (coarsened):  the eight old children by octant (each new cell is
+ *                      the mean of the 2x2x2 child cells it covers).
+ * Block indices are 1-based; every entry is checked against both trees
+ * (BX_ERR_ARG). The time and step count carry over, and the next time step
+ * is the minimum cell time step of the new grid. Implicit and heat
+ * conduction contexts are released. */
+BX_API int bx_regrid(const bx_grid_desc *gd, const int *iRemap_IB);
+
 /* ---- implicit JFNK step (src/ModPartImplicit.f90, full implicit) --------- */
 enum { BX_PRECOND_NONE = 0, BX_PRECOND_BILU = 1, BX_PRECOND_LEARNED = 2 };
 /* #IMPLICIT, #IMPLSTEP, #IMPLSCHEME, #JACOBIAN, #KRYLOV, #KRYLOVSIZE,

@@ -961,6 +961,44 @@ struct Oracle {
     return err;
   }
 
+  // The cell time steps of the current state without an update: the faces
+  // of every block as in a stage (the finer fluxes at resolution changes
+  // included) and calc_timestep.  After a regrid this gives the time step of
+  // the next step on the new grid (bx_regrid does the same on the GPU).
+  int recompute_timestep() {
+    int err = 0;
+    if (hasResChange) {
+#pragma omp parallel for schedule(dynamic, 4) num_threads((int)scr.size()) reduction(| : err)
+      for (int b = 0; b < nBlock; b++) {
+        bool fine = false;
+        for (int sd = 0; sd < 6; sd++) fine = fine || dil[6 * b + sd] == 1;
+        if (!fine) continue;
+        int t = 0;
+#ifdef _OPENMP
+        t = omp_get_thread_num();
+#endif
+        Scratch &s = scr[t];
+        calc_face_value(b, s);
+        err |= calc_face_flux(b, s);
+        save_cons_flux(b, s);
+      }
+      message_pass_face();
+    }
+#pragma omp parallel for schedule(dynamic, 4) num_threads((int)scr.size()) reduction(| : err)
+    for (int b = 0; b < nBlock; b++) {
+      int t = 0;
+#ifdef _OPENMP
+      t = omp_get_thread_num();
+#endif
+      Scratch &s = scr[t];
+      calc_face_value(b, s);
+      err |= calc_face_flux(b, s);
+      if (hasResChange) apply_cons_flux(b, s);
+      calc_timestep(b, s);
+    }
+    return err;
+  }
+
   // BATS_advance (src/ModBatsrusMethods.f90:493-760), time accurate
   int advance(double tLimit) {
     if (tLimit > 0 && tSimulation >= tLimit) return 0;
@@ -1617,6 +1655,7 @@ void ora_calc_face_flux(void *h, int iBlock) {
 void ora_calc_source(void *h, int iBlock) {
   Oracle *o = (Oracle *)h; o->calc_source(iBlock - 1, o->scr[0]);
 }
+int ora_recompute_timestep(void *h) { return ((Oracle *)h)->recompute_timestep(); }
 void ora_calc_timestep(void *h, int iBlock) {
   Oracle *o = (Oracle *)h; o->calc_timestep(iBlock - 1, o->scr[0]);
 }

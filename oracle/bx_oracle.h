@@ -71,6 +71,9 @@ void ora_calc_face_value(void *h, int iBlock);
 void ora_calc_face_flux(void *h, int iBlock);
 void ora_calc_source(void *h, int iBlock);
 void ora_calc_timestep(void *h, int iBlock);
+/* the cell time steps of the current state without an update (DtMax_B for
+   the next step; used after a regrid) */
+int ora_recompute_timestep(void *h);
 /* face states (nVar, nI+1, nJ, nK) etc. and fluxes (nFlux+2: fluxes, Vdt, Un)
  * for direction iDim = 0,1,2 */
 void ora_get_face_values(void *h, int iDim, double *Left, double *Right);

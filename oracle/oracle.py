@@ -50,7 +50,8 @@ _lib = None
 def lib():
     global _lib
     if _lib is None:
-        if not os.path.exists(_LIB):
+        srcs = [os.path.join(_HERE, f) for f in ("bx_oracle.cpp", "bx_oracle.h")]
+        if not os.path.exists(_LIB) or any(os.path.getmtime(f) > os.path.getmtime(_LIB) for f in srcs):
             build()
         L = ctypes.CDLL(_LIB)
         vp, ip, dp = ctypes.c_void_p, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_double)
@@ -74,6 +75,8 @@ def lib():
         L.ora_get_face_values.argtypes = [vp, ctypes.c_int, dp, dp]
         L.ora_get_face_flux.argtypes = [vp, ctypes.c_int, dp]
         L.ora_get_dtmax.argtypes = [vp, dp, dp]
+        L.ora_recompute_timestep.restype = ctypes.c_int
+        L.ora_recompute_timestep.argtypes = [vp]
         _lib = L
     return _lib
 
@@ -140,6 +143,11 @@ class Oracle:
         err = lib().ora_advance_n(self.h, n, t_limit)
         if err:
             raise RuntimeError("oracle advance failed (HLLD negative density ratio)")
+
+    def recompute_timestep(self):
+        """cell time steps of the current state, no update (after a regrid)"""
+        if lib().ora_recompute_timestep(self.h):
+            raise RuntimeError("oracle time step failed (HLLD negative density ratio)")
 
     def time(self):
         t, dt, n = ctypes.c_double(), ctypes.c_double(), ctypes.c_int()

@@ -1,0 +1,185 @@
+"""Host side of the dynamic AMR (batsrus_b200.amr, the BATL regrid rules
+restated from PARAM.XML's #AMR / #AMRCRITERIA / #AMRLEVELS): refinement with
+the splits that keep neighbouring levels within one, coarsening of whole
+sibling groups only, the level and block-count limits, the remap table of
+bx_regrid, the PARAM.in commands, and the conservation of the oracle's
+restated remap (injection and 2x2x2 means).  CPU only."""
+import numpy as np
+import pytest
+
+from batsrus_b200 import amr, configs
+from batsrus_b200.grid import BlockGrid
+from batsrus_b200.param import apply_commands, read_param, Scheme
+from amr_ref import block_geometry, remap_state
+
+
+def uniform(n=2, level=0, bc="periodic"):
+    return BlockGrid.uniform(3, (8, 8, 8), (n,) * 3, (-0.5,) * 3, (0.5,) * 3, (bc,) * 6, level=level, order="morton")
+
+
+def params(coarsen=0.2, refine=1.0, **kw):
+    return amr.AmrParams(dnRefine=1, criteria=[amr.AmrCriterion("gradlogp", coarsen, refine)], **kw)
+
+
+def crit_for(grid, refine_keys=(), coarsen_all=False, value=0.5):
+    c = np.full((grid.nBlock, 1), 0.0 if coarsen_all else value)
+    keys = [tuple(int(v) for v in k) for k in grid.iLevelCoord]
+    for b, k in enumerate(keys):
+        if k in refine_keys:
+            c[b, 0] = 10.0
+    return c
+
+
+def keyset(grid):
+    return {tuple(int(v) for v in k) for k in grid.iLevelCoord}
+
+
+def test_refine_one_block_of_a_uniform_grid():
+    g = uniform(2)
+    new, R, changed = amr.regrid(g, crit_for(g, {(0, 0, 0, 0)}), params())
+    assert changed and new.nBlock == g.nBlock + 7
+    assert amr.is_balanced(new)
+    ops = R[:, 0]
+    assert (ops == amr.PROLONG).sum() == 8 and (ops == amr.COPY).sum() == 7
+    kids = R[ops == amr.PROLONG]
+    assert set(kids[:, 1]) == {1 + [tuple(k) for k in g.iLevelCoord.tolist()].index((0, 0, 0, 0))}
+    assert sorted(kids[:, 2]) == list(range(8))
+
+
+def test_refinement_splits_coarser_neighbours():
+    g = uniform(2)
+    g1, _, _ = amr.regrid(g, crit_for(g, {(0, 0, 0, 0)}), params())
+    # refine a level-1 child at the corner of the refined region: the level-0
+    # blocks across its faces, edges and corners (periodic) must split too
+    new, R, _ = amr.regrid(g1, crit_for(g1, {(1, 0, 0, 0)}), params())
+    assert amr.is_balanced(new)
+    levels = np.bincount(new.iLevelCoord[:, 0])
+    assert levels[2] == 8 and new.nBlock > g1.nBlock + 7
+    # every new block is kept, refined once or coarsened once
+    assert set(np.unique(R[:, 0])) <= {amr.COPY, amr.PROLONG}
+
+
+def test_no_criterion_fired_keeps_the_grid():
+    g = configs.amr_blast(nRoot=2, maxLevel=2, with_state=False)[0]
+    new, R, changed = amr.regrid(g, crit_for(g), params())
+    assert not changed and np.array_equal(new.iLevelCoord, g.iLevelCoord)
+    assert (R[:, 0] == amr.COPY).all() and np.array_equal(R[:, 1], np.arange(1, g.nBlock + 1))
+
+
+def test_coarsening_merges_whole_sibling_groups_away_from_finer_blocks():
+    g = configs.amr_blast(nRoot=2, maxLevel=2, with_state=False)[0]
+    new, R, changed = amr.regrid(g, crit_for(g, coarsen_all=True), params())
+    assert changed and new.nBlock < g.nBlock and amr.is_balanced(new)
+    old = keyset(g)
+    for b in np.flatnonzero(R[:, 0] == amr.RESTRICT):
+        lv, i, j, k = new.iLevelCoord[b]
+        for o in range(8):
+            assert (lv + 1, 2 * i + (o & 1), 2 * j + ((o >> 1) & 1), 2 * k + (o >> 2)) in old
+    # the finest level cannot coarsen where a level-2 block touches level-1
+    # siblings, so one pass coarsens by at most one level everywhere
+    assert new.iLevelCoord[:, 0].max() >= g.iLevelCoord[:, 0].max() - 1
+
+
+def test_refine_then_coarsen_restores_a_uniform_grid():
+    g = uniform(2)
+    up, _, _ = amr.regrid(g, np.full((g.nBlock, 1), 10.0), params())
+    assert up.nBlock == 8 * g.nBlock and (up.iLevelCoord[:, 0] == 1).all()
+    down, R, _ = amr.regrid(up, crit_for(up, coarsen_all=True), params())
+    assert keyset(down) == keyset(g) and (R[:, 0] == amr.RESTRICT).all()
+
+
+def test_level_limits():
+    g = uniform(2, level=1)
+    p = params(minBlockLevel=1, maxBlockLevel=2)
+    down, _, changed = amr.regrid(g, crit_for(g, coarsen_all=True), p)
+    assert not changed  # MinBlockLevel = 1: no coarsening below level 1
+    up, _, _ = amr.regrid(g, np.full((g.nBlock, 1), 10.0), p)
+    assert (up.iLevelCoord[:, 0] == 2).all()
+    again, _, changed = amr.regrid(up, np.full((up.nBlock, 1), 10.0), p)
+    assert not changed  # MaxBlockLevel = 2: level-2 blocks neither refine nor coarsen
+    again, _, changed = amr.regrid(up, crit_for(up, coarsen_all=True), p)
+    assert not changed
+
+
+def test_max_total_blocks():
+    g = uniform(2)
+    c = np.arange(g.nBlock, dtype=float)[:, None] + 2.0  # every block asks, largest last
+    new, _, _ = amr.regrid(g, c, params(maxTotalBlocks=g.nBlock + 2 * 7))
+    assert new.nBlock <= g.nBlock + 14 and amr.is_balanced(new)
+    # the two largest criteria were refined
+    lv1 = {(int(k[1]) >> 1, int(k[2]) >> 1, int(k[3]) >> 1) for k in new.iLevelCoord if k[0] == 1}
+    keys = [tuple(int(v) for v in k[1:]) for k in g.iLevelCoord]
+    assert lv1 >= {keys[-1]} and len(lv1) >= 1
+
+
+@pytest.mark.parametrize("seed", range(6))
+def test_random_regrids_stay_balanced_and_remap_covers_every_cell(seed):
+    rng = np.random.default_rng(seed)
+    g = configs.amr_blast(nRoot=2, maxLevel=2, with_state=False)[0]
+    for _ in range(3):
+        c = rng.uniform(0.0, 2.0, size=(g.nBlock, 1))
+        new, R, _ = amr.regrid(g, c, params(coarsen=0.5, refine=1.5, maxBlockLevel=4))
+        assert amr.is_balanced(new)
+        # volume: kept + refined + coarsened blocks tile the old domain
+        _, vold, _ = block_geometry(g)
+        _, vnew, _ = block_geometry(new)
+        assert np.isclose(vold.sum() * 512, vnew.sum() * 512)
+        old_keys = [tuple(int(v) for v in k) for k in g.iLevelCoord]
+        used = np.zeros(g.nBlock, int)
+        for b in range(new.nBlock):
+            if R[b, 0] == amr.COPY:
+                used[R[b, 1] - 1] += 8
+            elif R[b, 0] == amr.PROLONG:
+                used[R[b, 1] - 1] += 1
+            else:
+                used[R[b, 1:9] - 1] += 8
+        assert (used == 8).all()  # every old block's volume goes exactly once
+        g = new
+
+
+def test_oracle_remap_conserves_mass_and_is_exact_for_copies():
+    g = configs.amr_blast(nRoot=2, maxLevel=2, with_state=False)[0]
+    from batsrus_b200 import initial
+    st = initial.blast(g)
+    # refine the coarsest blocks, coarsen everything else
+    lev = g.iLevelCoord[:, :1]
+    c = np.where(lev == lev.min(), 10.0, 0.0)
+    new, R, _ = amr.regrid(g, c, params(maxBlockLevel=4))
+    assert (R[:, 0] == amr.PROLONG).any() and (R[:, 0] == amr.RESTRICT).any()
+    s2 = remap_state(st, R, new)
+    isl = g.interior_slices()
+    _, vo, _ = block_geometry(g)
+    _, vn, _ = block_geometry(new)
+    m0 = (st[isl][..., 0].reshape(g.nBlock, -1).sum(1) * vo).sum()
+    m1 = (s2[new.interior_slices()][..., 0].reshape(new.nBlock, -1).sum(1) * vn).sum()
+    assert abs(m1 - m0) <= 1e-13 * m0
+    for b in np.flatnonzero(R[:, 0] == amr.COPY):
+        assert np.array_equal(s2[new.interior_slices()][b], st[isl][R[b, 1] - 1])
+
+
+def test_param_commands():
+    text = """
+#DOAMR
+T			DoAmr
+4			DnAmr
+-1.0			DtAmr
+T			IsStrictAmr
+
+#AMRCRITERIA
+2			nRefineCrit
+gradlogP		TypeRefine
+0.3			CoarsenLimit
+1.2			RefineLimit
+pjumpratio		TypeRefine
+1.1			CoarsenLimit
+1.6			RefineLimit
+
+#AMRLEVELS
+0			MinBlockLevel
+3			MaxBlockLevel
+"""
+    info = apply_commands(read_param(text)[0], Scheme())
+    p = amr.read_amr_params(info)
+    assert p.dnRefine == 4 and p.minBlockLevel == 0 and p.maxBlockLevel == 3
+    assert [(c.name, c.coarsenLimit, c.refineLimit) for c in p.criteria] == [
+        ("gradlogp", 0.3, 1.2), ("pjumpratio", 1.1, 1.6)]
