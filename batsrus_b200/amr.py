@@ -218,6 +218,27 @@ def regrid(grid, crit, params):
     return new, remap_table(grid, new), changed
 
 
+def plan_native(grid, crit, params):
+    """the same decisions made by the library (bx_amr_plan, host code, no
+    device needed): (new_grid, remap, changed)"""
+    import ctypes
+    from . import capi
+    L = capi.load()
+    crit = np.ascontiguousarray(crit, dtype=np.float64).reshape(grid.nBlock, -1)
+    gd = capi.grid_desc(grid)
+    cp = capi.amr_params(params)
+    ip = ctypes.POINTER(ctypes.c_int)
+    nMax = max(8 * grid.nBlock, 64)
+    lc = np.empty((nMax, 4), dtype=np.int32)
+    R = np.empty((nMax, REMAP_INTS), dtype=np.int32)
+    n, ch = ctypes.c_int(), ctypes.c_int()
+    capi.check(L.bx_amr_plan(ctypes.byref(gd), ctypes.byref(cp), capi.dptr(crit), nMax, ctypes.byref(n),
+                             lc.ctypes.data_as(ip), R.ctypes.data_as(ip), ctypes.byref(ch)))
+    new = BlockGrid(grid.nDim, grid.nI, grid.nJ, grid.nK, grid.nRoot, grid.xyzMin, grid.xyzMax, grid.typeBc,
+                    lc[:n.value].copy())
+    return new, R[:n.value].copy(), bool(ch.value)
+
+
 def remap_table(old, new):
     """iRemap_IB of bx_regrid: per new block the operation and the old
     blocks (1-based) it is made from."""

@@ -26,6 +26,7 @@ UNITS = [
     ("bx_stage3d.cu", []),
     ("bx_stage3d_fpt2.cu", []),
     ("bx_amr.cu", []),
+    ("bx_amr_plan.cu", []),
     ("bx_implicit.cu", ["--fmad=false"]),
     ("bx_learned.cu", []),
     ("bx_noalloc.cu", []),

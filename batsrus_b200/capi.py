@@ -39,7 +39,7 @@ EXPORTS = (
     "bx_heat_init", "bx_advance_semi_impl", "bx_heat_get_te", "bx_heat_get_rhs", "bx_heat_matvec",
     "bx_heat_precond",
     "bx_autotune", "bx_tune_info", "bx_tune_set", "bx_tune_reset",
-    "bx_amr_criteria", "bx_regrid",
+    "bx_amr_criteria", "bx_regrid", "bx_amr_plan", "bx_do_amr", "bx_get_grid",
 )
 # #AMRCRITERIA TypeRefine -> BX_AMR_*
 AMR_CRIT = {"gradt": 1, "gradlogrho": 2, "gradlogp": 3, "gradp": 4, "pjumpratio": 5}
@@ -61,6 +61,31 @@ class KrylovStats(ctypes.Structure):
         ("nMatvec", ctypes.c_int), ("iError", ctypes.c_int), ("Error", ctypes.c_double),
         ("Dt", ctypes.c_double), ("msStep", ctypes.c_double), ("msPrecondSetup", ctypes.c_double),
     ]
+
+
+class AmrParamsC(ctypes.Structure):
+    _fields_ = [
+        ("nCrit", ctypes.c_int), ("iTypeCrit", ctypes.c_int * 3), ("CoarsenLimit", ctypes.c_double * 3),
+        ("RefineLimit", ctypes.c_double * 3), ("MinBlockLevel", ctypes.c_int), ("MaxBlockLevel", ctypes.c_int),
+        ("MaxTotalBlocks", ctypes.c_int),
+    ]
+
+
+def amr_params(p):
+    """bx_amr_params from batsrus_b200.amr.AmrParams"""
+    c = AmrParamsC()
+    if not 1 <= len(p.criteria) <= 3:
+        raise ValueError("1 to 3 AMR criteria, got %d" % len(p.criteria))
+    c.nCrit = len(p.criteria)
+    for q, cr in enumerate(p.criteria):
+        try:
+            c.iTypeCrit[q] = AMR_CRIT[cr.name.lower()]
+        except KeyError:
+            raise ValueError("AMR criterion %s is not built (built: %s)" % (cr.name, ", ".join(AMR_CRIT)))
+        c.CoarsenLimit[q] = cr.coarsenLimit
+        c.RefineLimit[q] = cr.refineLimit
+    c.MinBlockLevel, c.MaxBlockLevel, c.MaxTotalBlocks = p.minBlockLevel, p.maxBlockLevel, p.maxTotalBlocks
+    return c
 
 
 class HeatParamsC(ctypes.Structure):
@@ -167,6 +192,8 @@ def load():
         "bx_tune_info": [i, ctypes.c_char_p, i, ip, ip, ip, ip, fp],
         "bx_heat_get_te": [dp], "bx_heat_get_rhs": [dp], "bx_heat_matvec": [dp, dp], "bx_heat_precond": [dp, dp],
         "bx_amr_criteria": [i, ip, dp], "bx_regrid": [ctypes.POINTER(GridDesc), ip],
+        "bx_amr_plan": [ctypes.POINTER(GridDesc), ctypes.POINTER(AmrParamsC), dp, i, ip, ip, ip, ip],
+        "bx_do_amr": [ctypes.POINTER(AmrParamsC), ip, ip], "bx_get_grid": [ip],
     }
     for name, args in sig.items():
         f = getattr(L, name)

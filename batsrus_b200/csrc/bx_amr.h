@@ -3,6 +3,10 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include <vector>
+
+#include "../../include/bx200.h"
+
 #include "bx_device.h"
 
 namespace bx {
@@ -38,6 +42,10 @@ struct AmrCritArgs {
 // by octant a + 2 b + 4 c (restrict); 0-based block indices
 constexpr int kRemapInts = 10;
 constexpr int kRemapCopy = 0, kRemapProlong = 1, kRemapRestrict = 2;
+
+// bx_amr_plan.cu: the new tree and remap table (block indices 1-based)
+int amr_plan(const bx_grid_desc *gd, const bx_amr_params *p, const double *Crit_IB, std::vector<int> &lcNew,
+             std::vector<int> &remap, bool &changed);
 
 cudaError_t launch_amr_crit(int shape, const AmrCritArgs &a, int nBlock, cudaStream_t st);
 cudaError_t launch_amr_remap(int shape, const double *in, double *out, const int *remap, int nBlockNew,

@@ -1062,6 +1062,47 @@ int bx_regrid(const bx_grid_desc *gd, const int *iRemap_IB) {
   return check_err_flag();
 }
 
+int bx_get_grid(int *iLevelCoord_IB) {
+  NEED_READY();
+  if (!iLevelCoord_IB) return fail(BX_ERR_ARG, "null argument");
+  for (int b = 0; b < g.nBlock; b++) {
+    iLevelCoord_IB[4 * b] = g.lev[b];
+    for (int d = 0; d < 3; d++) iLevelCoord_IB[4 * b + 1 + d] = g.ic[3 * b + d];
+  }
+  return BX_OK;
+}
+
+int bx_do_amr(const bx_amr_params *p, int *nBlockNew, int *IsChanged) {
+  NEED_READY();
+  if (!p) return fail(BX_ERR_ARG, "null argument");
+  if (p->nCrit < 1 || p->nCrit > 3) return fail(BX_ERR_ARG, "nCrit=%d (1..3)", p->nCrit);
+  std::vector<double> crit((size_t)p->nCrit * g.nBlock);
+  int r = bx_amr_criteria(p->nCrit, p->iTypeCrit, crit.data());
+  if (r) return r;
+  std::vector<int> lc(4 * (size_t)g.nBlock);
+  bx_get_grid(lc.data());
+  bx_grid_desc gd;
+  gd.nDim = g.nDim; gd.nI = g.nI; gd.nJ = g.nJ; gd.nK = g.nK;
+  for (int d = 0; d < 3; d++) { gd.nRootBlock[d] = g.nRoot[d]; gd.CoordMin[d] = g.cmin[d]; gd.CoordMax[d] = g.cmax[d]; }
+  for (int s = 0; s < 6; s++) gd.TypeBc[s] = g.typeBc[s];
+  gd.nBlock = g.nBlock;
+  gd.iLevelCoord_IB = lc.data();
+  gd.iDevice = g.dev;
+  std::vector<int> lcNew, R;
+  bool changed = false;
+  r = amr_plan(&gd, p, crit.data(), lcNew, R, changed);
+  if (r) return r;
+  if (changed) {
+    gd.nBlock = (int)(lcNew.size() / 4);
+    gd.iLevelCoord_IB = lcNew.data();
+    r = bx_regrid(&gd, R.data());
+    if (r) return r;
+  }
+  if (nBlockNew) *nBlockNew = g.nBlock;
+  if (IsChanged) *IsChanged = changed ? 1 : 0;
+  return BX_OK;
+}
+
 int bx_set_graph_steps(int nStepPerGraph) {
   NEED_READY();
   if (nStepPerGraph < 1 || nStepPerGraph > 1000) return fail(BX_ERR_ARG, "nStepPerGraph=%d", nStepPerGraph);

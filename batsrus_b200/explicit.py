@@ -155,15 +155,20 @@ class ExplicitSolver:
         self.grid, self._gd = grid, gd
 
     def do_amr(self, params):
-        """prepare_amr + do_amr (src/ModAMR.f90:171-386): criteria on the
-        GPU, the new tree on the host (batsrus_b200.amr), the state moved on
-        the GPU.  Returns True if the grid changed."""
-        from . import amr
-        crit = self.amr_criteria([c.name for c in params.criteria])
-        grid, remap, changed = amr.regrid(self.grid, crit, params)
-        if changed:
-            self.regrid(grid, remap)
-        return changed
+        """prepare_amr + do_amr (src/ModAMR.f90:171-386) in one library call
+        (bx_do_amr): criteria on the GPU, the new tree in the library's host
+        code, the state moved on the GPU.  Returns True if the grid changed."""
+        from .grid import BlockGrid
+        cp = capi.amr_params(params)
+        n, ch = ctypes.c_int(), ctypes.c_int()
+        check(self.L.bx_do_amr(ctypes.byref(cp), ctypes.byref(n), ctypes.byref(ch)))
+        if ch.value:
+            lc = np.empty((n.value, 4), dtype=np.int32)
+            check(self.L.bx_get_grid(lc.ctypes.data_as(ctypes.POINTER(ctypes.c_int))))
+            g = self.grid
+            self.grid = BlockGrid(g.nDim, g.nI, g.nJ, g.nK, g.nRoot, g.xyzMin, g.xyzMax, g.typeBc, lc)
+            self._gd = capi.grid_desc(self.grid, self._gd.iDevice)
+        return bool(ch.value)
 
     def advance_amr(self, nStep, params, TimeSimulationLimit=-1.0):
         """nStep steps of BATS_advance with do_amr after every step whose

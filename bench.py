@@ -322,6 +322,49 @@ def run_amr(args, lrank):
     return out
 
 
+def run_amr_dynamic(args, lrank):
+    """The blast with dynamic AMR (#DOAMR every args.amr_dyn_dn steps,
+    #AMRCRITERIA pjumpratio refining above 1.3 and coarsening below 1.02,
+    #AMRLEVELS 0..4, MaxTotalBlocks 3x the initial grid): FP32-bulk steps plus the regrids
+    (criteria on the GPU, the tree in the library's host code, the state
+    remapped on the GPU, tables and graph rebuilt).  Reports the steps'
+    cell-updates/s without and with the regrid time, and the time per regrid
+    (host wall clock around bx_do_amr, synchronised)."""
+    from batsrus_b200 import amr, configs
+    from batsrus_b200.explicit import ExplicitSolver
+    g, s, st, _ = configs.amr_blast(nRoot=args.amr_nroot, maxLevel=3, precision="fp32")
+    x = ExplicitSolver(g, s, device=lrank)
+    x.set_state(st)
+    x.advance(2)  # Dt = 0 step, then one step
+    p = amr.AmrParams(dnRefine=args.amr_dyn_dn, criteria=[amr.AmrCriterion("pjumpratio", 1.02, 1.3)],
+                      minBlockLevel=0, maxBlockLevel=4, maxTotalBlocks=3 * g.nBlock)
+    blocks0 = g.nBlock
+    stepMs, cellSteps, regridMs, blocks = 0.0, 0, [], [g.nBlock]
+    done = 0
+    while done < args.amr_dyn_steps:
+        k = min(args.amr_dyn_dn, args.amr_dyn_steps - done)
+        x.synchronize()
+        x.region_begin()
+        x.advance(k)
+        stepMs += x.region_end()
+        cellSteps += x.grid.nCell * k
+        done += k
+        t0 = time.perf_counter()
+        x.do_amr(p)
+        x.synchronize()
+        regridMs.append(1e3 * (time.perf_counter() - t0))
+        blocks.append(x.grid.nBlock)
+    x.close()
+    tot = stepMs + sum(regridMs)
+    return {"workload": "amr_blast_dynamic_nroot%d_levels0-4_doamr%d_pjumpratio" % (args.amr_nroot, args.amr_dyn_dn),
+            "unit": UNIT, "precision": "fp32", "steps": args.amr_dyn_steps, "regrids": len(regridMs),
+            "blocks_initial": blocks0, "blocks_after_each_regrid": blocks,
+            "steps_value": cellSteps / (stepMs * 1e-3), "value_with_regrids": cellSteps / (tot * 1e-3),
+            "ms_per_regrid": regridMs, "steps_ms": stepMs,
+            "criteria": "pjumpratio coarsen < 1.02, refine > 1.3",
+            "regrid_timing": "host wall clock around bx_do_amr, synchronised"}
+
+
 def run_heat(args, lrank):
     """Semi-implicit field-aligned heat conduction on the dipole workload:
     device time per solve (CUDA events around bx_advance_semi_impl, the
@@ -528,6 +571,8 @@ def main():
     ap.add_argument("--no-amr", dest="amr", action="store_false")
     ap.add_argument("--amr-nroot", type=int, default=16, help="root blocks per dimension of the blast grid")
     ap.add_argument("--amr-steps", type=int, default=50)
+    ap.add_argument("--amr-dyn-steps", type=int, default=50, help="steps of the dynamic-AMR blast (0: skip)")
+    ap.add_argument("--amr-dyn-dn", type=int, default=10, help="steps between regrids (#DOAMR DnAmr)")
     ap.add_argument("--jfnk-nroot", type=int, default=16, help="16 -> 128^3 cells")
     ap.add_argument("--jfnk-steps", type=int, default=5)
     ap.add_argument("--jfnk-warmup", type=int, default=2)
@@ -564,6 +609,8 @@ def main():
         line["jfnk"] = run_jfnk(args, 0)
     if args.amr:
         line["amr"] = run_amr(args, 0)
+        if args.amr_dyn_steps > 0:
+            line["amr"]["dynamic"] = run_amr_dynamic(args, 0)
     if args.heat_precond:
         line["heat"] = run_heat(args, 0)
     if args.cpu and world == 1:

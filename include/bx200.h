@@ -167,6 +167,36 @@ enum { BX_AMR_GRADT = 1, BX_AMR_GRADLOGRHO = 2, BX_AMR_GRADLOGP = 3, BX_AMR_GRAD
  * ghost cells are filled as by exchange_messages with first-order
  * prolongation. 3D grids of 8x8x8 or 4x4x4 blocks. */
 BX_API int bx_amr_criteria(int nCrit, const int *iTypeCrit_I, double *Crit_IB);
+/* #AMRCRITERIA (TypeRefine, CoarsenLimit, RefineLimit for up to 3 criteria),
+ * #AMRLEVELS, #AMR MaxTotalBlocks (PARAM.XML:6658-6910) */
+typedef struct {
+  int nCrit;
+  int iTypeCrit[3];      /* BX_AMR_* */
+  double CoarsenLimit[3];
+  double RefineLimit[3];
+  int MinBlockLevel;
+  int MaxBlockLevel;
+  int MaxTotalBlocks;
+} bx_amr_params;
+/* The tree decisions of BATL's set_amr_criteria / regrid_batl (absent from
+ * the reference tree, restated from PARAM.XML:6658-6910), host only: from
+ * the grid gd and its Crit_IB(nCrit, nBlock), the new block list
+ * (iLevelCoordNew_IB, 4 ints per block, Morton order of the finest level)
+ * and the iRemap_IB table of bx_regrid. A block refines if any criterion
+ * exceeds its RefineLimit (below MaxBlockLevel); 2^nDim siblings coarsen if
+ * all their criteria are below the CoarsenLimits (above MinBlockLevel,
+ * below MaxBlockLevel) and no block next to their parent is finer;
+ * neighbouring levels (faces, edges, corners) differ by at most one; the
+ * block count stays within MaxTotalBlocks. The output arrays hold
+ * nBlockNewMax blocks; BX_ERR_ARG with *nBlockNew set if more are needed. */
+BX_API int bx_amr_plan(const bx_grid_desc *gd, const bx_amr_params *p, const double *Crit_IB, int nBlockNewMax,
+                       int *nBlockNew, int *iLevelCoordNew_IB, int *iRemap_IB, int *IsChanged);
+/* prepare_amr + do_amr (src/ModAMR.f90:171-386) on the current grid:
+ * bx_amr_criteria, bx_amr_plan and, if the tree changed, bx_regrid.
+ * *nBlockNew is the block count afterwards (bx_get_grid gives the list). */
+BX_API int bx_do_amr(const bx_amr_params *p, int *nBlockNew, int *IsChanged);
+/* the current block list: 4 ints per block (level, ix, iy, iz) */
+BX_API int bx_get_grid(int *iLevelCoord_IB);
 /* do_amr -> regrid_batl (src/ModAMR.f90:231-386): replace the grid by gd
  * (same root grid, domain, boundaries and block size) and move the state
  * onto it. iRemap_IB(10, gd->nBlock) gives, for each new block: op, then

@@ -202,3 +202,22 @@ def test_inconsistent_remap_is_rejected():
     assert x.grid is g
     x.advance(1)
     x.close()
+
+
+def test_do_amr_in_the_library_matches_the_host_restatement():
+    """bx_do_amr (criteria, the library's tree code, regrid in one call)
+    gives the grid of the Python restatement and the same remapped state"""
+    g, s, x, o = setup()
+    x.advance(2)
+    c = x.amr_criteria(["gradlogp"])
+    p = amr.AmrParams(criteria=[amr.AmrCriterion("gradlogp", gap_limit(c[:, 0], 50), gap_limit(c[:, 0], 85))],
+                      maxBlockLevel=3)
+    new, R, changed = amr.regrid(g, c, p)
+    before = x.get_state()
+    assert x.do_amr(p) == changed and changed
+    assert np.array_equal(x.grid.iLevelCoord, new.iLevelCoord)
+    isl = new.interior_slices()
+    assert np.array_equal(x.get_state()[isl], remap_state(before, R, new)[isl])
+    x.advance(1)
+    assert np.isfinite(x.get_state()[isl]).all()
+    x.close()

@@ -183,3 +183,35 @@ pjumpratio		TypeRefine
     assert p.dnRefine == 4 and p.minBlockLevel == 0 and p.maxBlockLevel == 3
     assert [(c.name, c.coarsenLimit, c.refineLimit) for c in p.criteria] == [
         ("gradlogp", 0.3, 1.2), ("pjumpratio", 1.1, 1.6)]
+
+
+def crit_patterns(g, rng):
+    """criteria that refine, coarsen, both, or hit the block limit"""
+    lev = g.iLevelCoord[:, :1]
+    yield rng.uniform(0.0, 2.0, size=(g.nBlock, 1)), params(coarsen=0.5, refine=1.5, maxBlockLevel=4)
+    yield np.zeros((g.nBlock, 1)), params()
+    yield np.where(lev == lev.min(), 10.0, 0.0), params(maxBlockLevel=4)
+    yield np.where(lev == lev.max(), 0.0, 0.5), params(maxBlockLevel=4)
+    yield rng.uniform(0.0, 20.0, size=(g.nBlock, 1)), params(maxTotalBlocks=g.nBlock + 40, maxBlockLevel=5)
+    yield rng.uniform(0.0, 2.0, size=(g.nBlock, 1)), params(coarsen=0.9, refine=1.8, minBlockLevel=1, maxBlockLevel=3)
+
+
+@pytest.mark.parametrize("nRoot,maxLevel", [(2, 2), (4, 2), (3, 3)])
+def test_native_plan_matches_restatement(nRoot, maxLevel):
+    """bx_amr_plan (the library's C++ tree code, host only) makes the same
+    decisions as the Python restatement: same blocks in the same order, same
+    remap table"""
+    g = configs.amr_blast(nRoot=nRoot, maxLevel=maxLevel, with_state=False)[0]
+    rng = np.random.default_rng(nRoot + 10 * maxLevel)
+    seen = set()
+    for c, p in crit_patterns(g, rng):
+        a = amr.regrid(g, c, p)
+        b = amr.plan_native(g, c, p)
+        assert np.array_equal(a[0].iLevelCoord, b[0].iLevelCoord) and np.array_equal(a[1], b[1]) and a[2] == b[2]
+        seen.update(np.unique(a[1][:, 0]).tolist())
+        # a second pass from the new grid
+        c2 = rng.uniform(0.0, 2.0, size=(a[0].nBlock, 1))
+        p2 = params(coarsen=0.7, refine=1.7, maxBlockLevel=maxLevel + 2)
+        a2, b2 = amr.regrid(a[0], c2, p2), amr.plan_native(a[0], c2, p2)
+        assert np.array_equal(a2[0].iLevelCoord, b2[0].iLevelCoord) and np.array_equal(a2[1], b2[1])
+    assert seen == {amr.COPY, amr.PROLONG, amr.RESTRICT}
