@@ -48,6 +48,17 @@ module bx200_interface
      real(c_double):: Error, Dt, msStep, msPrecondSetup
   end type bx_krylov_stats
 
+  integer(c_int), parameter:: BX_AMR_GRADT = 1, BX_AMR_GRADLOGRHO = 2, &
+       BX_AMR_GRADLOGP = 3, BX_AMR_GRADP = 4, BX_AMR_PJUMPRATIO = 5
+
+  ! #AMRCRITERIA, #AMRLEVELS, #AMR MaxTotalBlocks
+  type, bind(C):: bx_amr_params
+     integer(c_int):: nCrit
+     integer(c_int):: iTypeCrit(3)
+     real(c_double):: CoarsenLimit(3), RefineLimit(3)
+     integer(c_int):: MinBlockLevel, MaxBlockLevel, MaxTotalBlocks
+  end type bx_amr_params
+
   type, bind(C):: bx_heat_params
      real(c_double):: HeatCondPar, FractionFieldAligned, Cv, Dt, SemiImplCoeff
      integer(c_int):: nKrylovVector, MaxMatvec
@@ -203,6 +214,31 @@ module bx200_interface
        real(c_double), value:: TimeSimulationLimit
        type(bx_krylov_stats), intent(out):: Stats
      end function bx_advance_part_impl
+
+     ! prepare_amr + do_amr (src/ModAMR.f90:171-386): criteria, new tree,
+     ! state moved onto it; the new block list comes from bx_get_grid
+     integer(c_int) function bx_do_amr(Params, nBlockNew, IsChanged) bind(C, name='bx_do_amr')
+       import:: c_int, bx_amr_params
+       type(bx_amr_params), intent(in):: Params
+       integer(c_int), intent(out):: nBlockNew, IsChanged
+     end function bx_do_amr
+     integer(c_int) function bx_get_grid(iLevelCoord_IB) bind(C, name='bx_get_grid')
+       import:: c_int
+       integer(c_int), intent(out):: iLevelCoord_IB(*)
+     end function bx_get_grid
+     ! amr_criteria (src/ModAMR.f90:388-723): Crit_IB(nCrit, nBlock)
+     integer(c_int) function bx_amr_criteria(nCrit, iTypeCrit_I, Crit_IB) bind(C, name='bx_amr_criteria')
+       import:: c_int, c_double
+       integer(c_int), value:: nCrit
+       integer(c_int), intent(in):: iTypeCrit_I(*)
+       real(c_double), intent(out):: Crit_IB(*)
+     end function bx_amr_criteria
+     ! regrid_batl with a caller-made tree: iRemap_IB(10, nBlockNew)
+     integer(c_int) function bx_regrid(Grid, iRemap_IB) bind(C, name='bx_regrid')
+       import:: c_int, bx_grid_desc
+       type(bx_grid_desc), intent(in):: Grid
+       integer(c_int), intent(in):: iRemap_IB(*)
+     end function bx_regrid
 
      ! advance_semi_impl (src/ModSemiImplicit.f90:240), TypeSemiImplicit = parcond
      integer(c_int) function bx_heat_init(Params, Te, Bhat, Used) bind(C, name='bx_heat_init')

@@ -32,7 +32,7 @@ def test_structs_match_header_field_order():
     txt = open(HEADER).read()
     for cname, pystruct in (("bx_grid_desc", capi.GridDesc), ("bx_scheme_params", capi.SchemeParams),
                             ("bx_implicit_params", capi.ImplicitParamsC), ("bx_krylov_stats", capi.KrylovStats),
-                            ("bx_heat_params", capi.HeatParamsC)):
+                            ("bx_heat_params", capi.HeatParamsC), ("bx_amr_params", capi.AmrParamsC)):
         body = re.search(r"typedef struct \{([^{}]*)\}\s*%s;" % cname, txt).group(1)
         body = re.sub(r"/\*.*?\*/", "", body, flags=re.S)
         names = []
@@ -62,6 +62,8 @@ def test_argument_errors_without_gpu():
     assert capi.tune_info()["krylov_unroll"] == dict(knobs["krylov_unroll"], value=4, tuned=2)
     capi.tune_reset()
     assert capi.tune_info() == knobs
+    # dynamic AMR entry points need a grid
+    assert L.bx_do_amr(None, None, None) == 3 and L.bx_get_grid(None) == 3
     # unsupported block size is rejected before any device call
     g, s, _, _ = configs.brio_wu_1d()
     gd = capi.grid_desc(g)
