@@ -12,6 +12,7 @@
 #include <cstdio>
 #include <cstring>
 #include <map>
+#include <unordered_map>
 #include <string>
 #include <tuple>
 #include <vector>
@@ -69,6 +70,7 @@ struct Ctx {
   bool use3d = false;
   int nSM = 148;
   double *bufX = nullptr, *bufY = nullptr;  // the original A and B allocations
+  size_t stateCap = 0;                       // bytes of each of them
   TmaMaps mapX64, mapY64, mapY32;
   // timing
   bool timing = false;
@@ -78,6 +80,13 @@ struct Ctx {
 };
 
 Ctx g;
+
+// the two state buffers a regrid passes to bx_init (each cap bytes)
+struct StateHandoff {
+  double *A = nullptr, *B = nullptr;
+  size_t cap = 0;
+};
+StateHandoff g_hand;
 
 int fail(int code, const char *fmt, ...) {
   char buf[512];
@@ -569,19 +578,31 @@ int bx_init(const bx_grid_desc *gd, const bx_scheme_params *sp) {
 
   // block bookkeeping (BATL tree of one level: iNode -> neighbours)
   g.lev.resize(g.nBlock); g.ic.resize(3 * g.nBlock);
-  std::map<std::tuple<int, int, int, int>, int> node;
+  // level (5 bits) and three 19-bit block indices
+  auto nodeKey = [](int L, int x, int y, int z) {
+    return ((uint64_t)L << 57) | ((uint64_t)(uint32_t)x << 38) | ((uint64_t)(uint32_t)y << 19) | (uint64_t)(uint32_t)z;
+  };
+  std::unordered_map<uint64_t, int> node;
+  node.reserve(2 * (size_t)g.nBlock);
   for (int b = 0; b < g.nBlock; b++) {
     g.lev[b] = gd->iLevelCoord_IB[4 * b];
     for (int d = 0; d < 3; d++) g.ic[3 * b + d] = gd->iLevelCoord_IB[4 * b + 1 + d];
-    auto key = std::make_tuple(g.lev[b], g.ic[3 * b], g.ic[3 * b + 1], g.ic[3 * b + 2]);
-    if (node.count(key)) return fail(BX_ERR_ARG, "block %d duplicates block %d", b + 1, node[key] + 1);
-    node[key] = b;
+    if (g.lev[b] < 0 || g.lev[b] > 30)
+      return fail(BX_ERR_ARG, "block %d: level %d", b + 1, g.lev[b]);
+    for (int d = 0; d < 3; d++) {
+      const int n = d < gd->nDim ? gd->nRootBlock[d] << g.lev[b] : 1;
+      if (g.ic[3 * b + d] < 0 || g.ic[3 * b + d] >= n || n > (1 << 19))
+        return fail(BX_ERR_ARG, "block %d: index %d outside 0..%d in dimension %d", b + 1, g.ic[3 * b + d], n - 1,
+                    d + 1);
+    }
+    auto ins = node.emplace(nodeKey(g.lev[b], g.ic[3 * b], g.ic[3 * b + 1], g.ic[3 * b + 2]), b);
+    if (!ins.second) return fail(BX_ERR_ARG, "block %d duplicates block %d", b + 1, ins.first->second + 1);
   }
   // neighbours (BATL find_neighbor): the block at the same level across the
   // side, else its parent (coarser), else the 2^(nDim-1) children of that
   // position touching the side (finer, first transverse direction fastest)
   auto findb = [&](int L, int x, int y, int z) {
-    auto it = node.find(std::make_tuple(L, x, y, z));
+    auto it = node.find(nodeKey(L, x, y, z));
     return it == node.end() ? -1 : it->second;
   };
   g.nbrH.assign(6 * g.nBlock, kNbrFloat);
@@ -671,12 +692,20 @@ int bx_init(const bx_grid_desc *gd, const bx_scheme_params *sp) {
 
   CK(cudaStreamCreateWithFlags(&g.st, cudaStreamNonBlocking));
   const size_t stBytes = sizeof(double) * 8 * g.nCell * g.nBlock;
-  if (cudaMalloc(&g.A, stBytes) != cudaSuccess || cudaMalloc(&g.B, stBytes) != cudaSuccess) {
-    free_all();
-    return fail(BX_ERR_NOMEM, "cannot allocate 2 x %.2f GB of state", stBytes / 1e9);
+  if (g_hand.A && g_hand.cap >= stBytes) {
+    // a regrid hands over two buffers; it fills U, the first stage fills
+    // the stage buffer
+    g.A = g_hand.A; g.B = g_hand.B; g.stateCap = g_hand.cap;
+    g_hand = StateHandoff();
+  } else {
+    if (cudaMalloc(&g.A, stBytes) != cudaSuccess || cudaMalloc(&g.B, stBytes) != cudaSuccess) {
+      free_all();
+      return fail(BX_ERR_NOMEM, "cannot allocate 2 x %.2f GB of state", stBytes / 1e9);
+    }
+    g.stateCap = stBytes;
+    CK(cudaMemsetAsync(g.A, 0, stBytes, g.st));
+    CK(cudaMemsetAsync(g.B, 0, stBytes, g.st));
   }
-  CK(cudaMemsetAsync(g.A, 0, stBytes, g.st));
-  CK(cudaMemsetAsync(g.B, 0, stBytes, g.st));
   g.bufX = g.A;
   g.bufY = g.B;
   g.use3d = g.shape == kShape888 || g.shape == kShape444;
@@ -1031,22 +1060,47 @@ int bx_regrid(const bx_grid_desc *gd, const int *iRemap_IB) {
     }
     if (!ok) return fail(BX_ERR_ARG, "remap entry of new block %d does not match the old and new trees", b + 1);
   }
-  // the old state survives the rebuild of the context
+  // the old state survives the rebuild of the context.  If the buffers are
+  // large enough the stage buffer (dead here) becomes the new U and, after
+  // the remap, the old U the new stage buffer; otherwise a new pair is
+  // allocated with a quarter of headroom for later regrids
   CK(cudaStreamSynchronize(g.st));
   StepState ts;
   CK(cudaMemcpy(&ts, g.ts, sizeof(ts), cudaMemcpyDeviceToHost));
-  double *oldA = g.A;
-  g.A = nullptr;
+  double *oldA = g.A, *oldB = g.B;
+  const size_t cap = g.stateCap, newBytes = sizeof(double) * 8 * g.nCell * (size_t)nNew;
+  g.A = g.B = nullptr;
+  const bool reuse = cap >= newBytes;
+  if (reuse) {
+    g_hand.A = oldB; g_hand.B = oldA; g_hand.cap = cap;
+  } else {
+    const size_t newCap = newBytes + newBytes / 4;
+    if (cudaMalloc(&g_hand.A, newCap) != cudaSuccess || cudaMalloc(&g_hand.B, newCap) != cudaSuccess) {
+      if (g_hand.A) cudaFree(g_hand.A);
+      g_hand = StateHandoff();
+      cudaFree(oldA); cudaFree(oldB);
+      free_all();
+      return fail(BX_ERR_NOMEM, "regrid: cannot allocate 2 x %.2f GB of state", newCap / 1e9);
+    }
+    g_hand.cap = newCap;
+  }
   const bx_scheme_params sch = g.sch;
   int r = bx_init(gd, &sch);
-  if (r) { cudaFree(oldA); return r; }
+  if (g_hand.A) {  // not taken over (bx_init failed before the state)
+    cudaFree(g_hand.A); cudaFree(g_hand.B);
+    g_hand = StateHandoff();
+  }
+  if (r) {
+    if (!reuse) { cudaFree(oldA); cudaFree(oldB); }
+    return r;
+  }
   int *dR = nullptr;
   cudaError_t e = cudaMalloc(&dR, sizeof(int) * R.size());
   if (e == cudaSuccess) e = cudaMemcpyAsync(dR, R.data(), sizeof(int) * R.size(), cudaMemcpyHostToDevice, g.st);
   if (e == cudaSuccess) e = launch_amr_remap(g.shape, oldA, g.A, dR, nNew, g.st);
   if (e == cudaSuccess) e = cudaStreamSynchronize(g.st);
   cudaFree(dR);
-  cudaFree(oldA);
+  if (!reuse) { cudaFree(oldA); cudaFree(oldB); }
   if (e != cudaSuccess) return fail(BX_ERR_CUDA, "regrid remap: %s", cudaGetErrorString(e));
   // time and step count carry over; the next time step is the minimum cell
   // time step of the new grid: a stage with Dt = 0 copies U into the stage
