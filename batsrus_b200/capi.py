@@ -40,6 +40,7 @@ EXPORTS = (
     "bx_heat_precond",
     "bx_autotune", "bx_tune_info", "bx_tune_set", "bx_tune_reset",
     "bx_amr_criteria", "bx_regrid", "bx_amr_plan", "bx_do_amr", "bx_get_grid",
+    "bx_get_block_dt", "bx_set_block_dt",
 )
 # #AMRCRITERIA TypeRefine -> BX_AMR_*
 AMR_CRIT = {"gradt": 1, "gradlogrho": 2, "gradlogp": 3, "gradp": 4, "pjumpratio": 5}
@@ -194,6 +195,7 @@ def load():
         "bx_amr_criteria": [i, ip, dp], "bx_regrid": [ctypes.POINTER(GridDesc), ip],
         "bx_amr_plan": [ctypes.POINTER(GridDesc), ctypes.POINTER(AmrParamsC), dp, i, ip, ip, ip, ip],
         "bx_do_amr": [ctypes.POINTER(AmrParamsC), ip, ip], "bx_get_grid": [ip],
+        "bx_get_block_dt": [dp], "bx_set_block_dt": [dp],
     }
     for name, args in sig.items():
         f = getattr(L, name)

@@ -833,6 +833,34 @@ int bx_set_time(double tSimulation, int nStep) {
   return BX_OK;
 }
 
+int bx_get_block_dt(double *DtMax_B) {
+  NEED_READY();
+  if (!DtMax_B) return fail(BX_ERR_ARG, "null argument");
+  CK(cudaMemcpyAsync(DtMax_B, g.dtBlock, sizeof(double) * g.nBlock, cudaMemcpyDeviceToHost, g.st));
+  CK(cudaStreamSynchronize(g.st));
+  return BX_OK;
+}
+
+int bx_set_block_dt(const double *DtMax_B) {
+  NEED_READY();
+  if (!DtMax_B) return fail(BX_ERR_ARG, "null argument");
+  double m = 1e300;
+  for (int b = 0; b < g.nBlock; b++) {
+    if (!(DtMax_B[b] > 0.0)) return fail(BX_ERR_ARG, "DtMax_B(%d) = %g", b + 1, DtMax_B[b]);
+    m = std::min(m, DtMax_B[b]);
+  }
+  CK(cudaMemcpyAsync(g.dtBlock, DtMax_B, sizeof(double) * g.nBlock, cudaMemcpyHostToDevice, g.st));
+  StepState s;
+  CK(cudaMemcpyAsync(&s, g.ts, sizeof(s), cudaMemcpyDeviceToHost, g.st));
+  CK(cudaStreamSynchronize(g.st));
+  uint64_t bits;
+  std::memcpy(&bits, &m, sizeof(bits));
+  s.DtMinBits = bits;
+  CK(cudaMemcpyAsync(g.ts, &s, sizeof(s), cudaMemcpyHostToDevice, g.st));
+  CK(cudaStreamSynchronize(g.st));
+  return BX_OK;
+}
+
 int bx_get_time(double *t, double *dt, int *n) {
   NEED_READY();
   StepState s;

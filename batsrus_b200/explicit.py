@@ -65,6 +65,18 @@ class ExplicitSolver:
         check(self.L.bx_get_time(ctypes.byref(t), ctypes.byref(dt), ctypes.byref(n)))
         return t.value, dt.value, n.value
 
+    def block_dt(self):
+        """DtMax_B of every block from the last step (bx_get_block_dt)"""
+        out = np.empty(self.grid.nBlock)
+        check(self.L.bx_get_block_dt(dptr(out)))
+        return out
+
+    def set_block_dt(self, DtMax_B):
+        """DtMax_B from a restart: the next step's time step (bx_set_block_dt)"""
+        a = np.ascontiguousarray(DtMax_B, dtype=np.float64)
+        assert a.shape == (self.grid.nBlock,), a.shape
+        check(self.L.bx_set_block_dt(dptr(a)))
+
     # -- per-block orig path ------------------------------------------------
     def calc_face_value(self, iBlock, DoResChangeOnly=False, DoMonotoneRestrict=True):
         check(self.L.bx_calc_face_value(iBlock, int(DoResChangeOnly), int(DoMonotoneRestrict)))

@@ -102,6 +102,14 @@ BX_API int bx_upload_state(const double *State_VGB, int nBlock);
 BX_API int bx_download_state(double *State_VGB, int nBlock);
 BX_API int bx_set_time(double tSimulation, int nStep);
 BX_API int bx_get_time(double *tSimulation, double *Dt, int *nStep);
+/* DtMax_B(nBlock): each block's largest stable time step (the minimum of
+ * its cells' V / sum(Vdt)), from the last step; write_restart_file
+ * (src/ModRestartFile.f90:795-833) stores it */
+BX_API int bx_get_block_dt(double *DtMax_B);
+/* DtMax_B from a restart (read_restart_file, src/ModRestartFile.f90:682):
+ * the next step's time step is their minimum, as set_global_timestep
+ * takes it after a restart */
+BX_API int bx_set_block_dt(const double *DtMax_B);
 
 /* ModParallel DiLevel_EB(iSide, iBlock) and jBlock_IEB(iSub, iSide, iBlock)
  * (src/ModParallel.f90:10-14) of the grid given to bx_init, sides x-, x+,

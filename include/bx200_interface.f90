@@ -215,6 +215,17 @@ module bx200_interface
        type(bx_krylov_stats), intent(out):: Stats
      end function bx_advance_part_impl
 
+     ! DtMax_B for write_restart_file / from read_restart_file
+     ! (src/ModRestartFile.f90:682-833)
+     integer(c_int) function bx_get_block_dt(DtMax_B) bind(C, name='bx_get_block_dt')
+       import:: c_int, c_double
+       real(c_double), intent(out):: DtMax_B(*)
+     end function bx_get_block_dt
+     integer(c_int) function bx_set_block_dt(DtMax_B) bind(C, name='bx_set_block_dt')
+       import:: c_int, c_double
+       real(c_double), intent(in):: DtMax_B(*)
+     end function bx_set_block_dt
+
      ! prepare_amr + do_amr (src/ModAMR.f90:171-386): criteria, new tree,
      ! state moved onto it; the new block list comes from bx_get_grid
      integer(c_int) function bx_do_amr(Params, nBlockNew, IsChanged) bind(C, name='bx_do_amr')
