@@ -109,11 +109,13 @@ class ClockSampler:
 
 
 def allreduce_max(x, world):
+    """the maximum of x over the ranks (NCCL on the GPUs, or gloo)"""
     if world == 1:
         return x
     import torch
     import torch.distributed as dist
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([x], dtype=torch.float64, device=dev)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
 
@@ -122,6 +124,18 @@ def barrier(world):
     if world > 1:
         import torch.distributed as dist
         dist.barrier()
+
+
+def replica_rate(timed, units, world):
+    """One timed region of replicas: a barrier, this rank's timed() (it
+    returns milliseconds measured on its device), a barrier, the maximum over
+    the ranks.  Returns (whole-job units per second = world x units / the
+    slowest rank's time, that time in ms)."""
+    barrier(world)
+    ms = timed()
+    barrier(world)
+    ms = allreduce_max(ms, world)
+    return world * units / (ms * 1e-3), ms
 
 
 def run_ours(args):
@@ -149,18 +163,18 @@ def run_ours(args):
         x.advance(max(args.warmup, 3))  # includes the first Dt = 0 step
         tuned = x.autotune() if args.autotune else None
         x.synchronize()
-        barrier(world)
         x.timing(True)
         x.timing_reset()
-        with ClockSampler(lrank) as clk:
-            x.region_begin()
-            x.advance(args.steps)
-            ms = x.region_end()
+        clk = ClockSampler(lrank)
+
+        def timed():
+            with clk:
+                x.region_begin()
+                x.advance(args.steps)
+                return x.region_end()
+        value, ms = replica_rate(timed, nCell * args.steps, world)
         kern_ms, n_launch, n_total = x.timing_get()
         x.timing(False)
-        barrier(world)
-        ms = allreduce_max(ms, world)
-        value = world * nCell * args.steps / (ms * 1e-3)
         launch_bytes = BYTES_PER_CELL_STEP[prec] / 2 * nCell  # average over the 2 stages
         achieved = launch_bytes / (kern_ms * 1e-3) / 1e9
         t_per_cell = profile_traffic(prec)
@@ -181,16 +195,17 @@ def run_ours(args):
             x2.set_state(host.numpy())
             x2.advance(1)
             x2.synchronize()
-            barrier(world)
-            x2.region_begin()
-            x2.set_state(host.numpy())
-            x2.set_time(0.0, 1)  # first Dt = 0 step already taken: time the K full steps
-            x2.advance(args.steps)
-            x2.get_state(back.numpy())
-            ems = x2.region_end()
-            ems = allreduce_max(ems, world)
+
+            def timed_e2e():
+                x2.region_begin()
+                x2.set_state(host.numpy())
+                x2.set_time(0.0, 1)  # first Dt = 0 step already taken: time the K full steps
+                x2.advance(args.steps)
+                x2.get_state(back.numpy())
+                return x2.region_end()
+            evalue, ems = replica_rate(timed_e2e, nCell * args.steps, world)
             nbytes = host.numel() * 8
-            res["e2e"] = {"value": world * nCell * args.steps / (ems * 1e-3), "unit": UNIT,
+            res["e2e"] = {"value": evalue, "unit": UNIT,
                           "h2d_bytes_per_step": nbytes / args.steps, "d2h_bytes_per_step": nbytes / args.steps,
                           "ms": ems}
             x2.close()
