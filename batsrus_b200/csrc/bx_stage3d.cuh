@@ -214,6 +214,7 @@ __device__ __forceinline__ void sweep3(const StageArgs &a, const BlockGeom &g, c
     }
   }
   __syncthreads();
+  constexpr bool kFloatFlux = sizeof(Real) == sizeof(float);
 #pragma unroll
   for (int r = 0; r < T::CPC; r++) {
     const int c = t + r * T::NTHR;
@@ -223,13 +224,17 @@ __device__ __forceinline__ void sweep3(const StageArgs &a, const BlockGeom &g, c
     const int f1 = face_id<T, D>(i + (D == 0), j + (D == 1), k + (D == 2));
 #pragma unroll
     for (int v = 0; v < 8; v++) {
-      const double d = (double)fbuf[v * T::NF + f0] - (double)fbuf[v * T::NF + f1];
+      // FP32 fluxes: the difference of neighbouring faces in FP32 (exact
+      // when they are within a factor of two) and one conversion
+      const double d = kFloatFlux ? (double)(fbuf[v * T::NF + f0] - fbuf[v * T::NF + f1])
+                                  : (double)fbuf[v * T::NF + f0] - (double)fbuf[v * T::NF + f1];
       chg[r][v] = D == 0 ? d : chg[r][v] + d;
     }
     // div B from the face normal field, (L+R)/2 differences over the cell
-    const double db = g.invHalf[D] * ((double)fbuf[9 * T::NF + f1] - (double)fbuf[9 * T::NF + f0]);
+    const double db = g.invHalf[D] * (kFloatFlux ? (double)(fbuf[9 * T::NF + f1] - fbuf[9 * T::NF + f0])
+                                                 : (double)fbuf[9 * T::NF + f1] - (double)fbuf[9 * T::NF + f0]);
     divB[r] = D == 0 ? db : divB[r] + db;
-    const double vm = fmax((double)fbuf[8 * T::NF + f0], (double)fbuf[8 * T::NF + f1]);
+    const double vm = (double)fmax(fbuf[8 * T::NF + f0], fbuf[8 * T::NF + f1]);
     vdt[r] = D == 0 ? vm : vdt[r] + vm;
   }
   __syncthreads();
@@ -309,7 +314,12 @@ __global__ void __launch_bounds__(T::NTHR, 1)
     }
 
     // calc_primitives, in two passes (read all, then write) because float
-    // boundary ghosts read interior cells that are converted in place
+    // boundary ghosts read interior cells that are converted in place.  The
+    // primitives are written in the arithmetic type of the sweeps: for an
+    // FP64 tile and FP32 fluxes (the first stage of FP32-bulk) into an FP32
+    // view of the same buffer (same element indices, first half of the
+    // bytes), so that the sweeps read it without conversions
+    Real *tv = reinterpret_cast<Real *>(tile);
     {
       TileT prim[T::CPT][8];
 #pragma unroll
@@ -345,16 +355,16 @@ __global__ void __launch_bounds__(T::NTHR, 1)
           const int d0 = tile_index<T, TileT>(0, i, j, k);
           const int dv = tile_index<T, TileT>(1, i, j, k) - d0;
 #pragma unroll
-          for (int v = 0; v < 8; v++) tile[d0 + v * dv] = prim[m][v];
+          for (int v = 0; v < 8; v++) tv[d0 + v * dv] = (Real)prim[m][v];
         }
       }
       __syncthreads();
     }
 
     double chg[T::CPC][8], divB[T::CPC], vdt[T::CPC];
-    sweep3<T, 0, FLUX, LIM, TileT, Real>(a, g, tile, fbuf, chg, divB, vdt, err, rcFine, rcCoarse, b);
-    sweep3<T, 1, FLUX, LIM, TileT, Real>(a, g, tile, fbuf, chg, divB, vdt, err, rcFine, rcCoarse, b);
-    sweep3<T, 2, FLUX, LIM, TileT, Real>(a, g, tile, fbuf, chg, divB, vdt, err, rcFine, rcCoarse, b);
+    sweep3<T, 0, FLUX, LIM, Real, Real>(a, g, tv, fbuf, chg, divB, vdt, err, rcFine, rcCoarse, b);
+    sweep3<T, 1, FLUX, LIM, Real, Real>(a, g, tv, fbuf, chg, divB, vdt, err, rcFine, rcCoarse, b);
+    sweep3<T, 2, FLUX, LIM, Real, Real>(a, g, tv, fbuf, chg, divB, vdt, err, rcFine, rcCoarse, b);
 
     // update_state_normal / update_explicit for the thread's cells
     double dtmin = 1e300;
@@ -376,8 +386,8 @@ __global__ void __launch_bounds__(T::NTHR, 1)
         if (a.useDivb) {
           const int ii = cc % T::N, jj = (cc / T::N) % T::N, kk = cc / (T::N * T::N);
           const int c0 = tile_index<T, TileT>(0, ii, jj, kk);
-          const double ux = tile[c0 + kUx * T::NC], uy = tile[c0 + kUy * T::NC], uz = tile[c0 + kUz * T::NC];
-          const double bx = tile[c0 + kBx * T::NC], by = tile[c0 + kBy * T::NC], bz = tile[c0 + kBz * T::NC];
+          const double ux = tv[c0 + kUx * T::NC], uy = tv[c0 + kUy * T::NC], uz = tv[c0 + kUz * T::NC];
+          const double bx = tv[c0 + kBx * T::NC], by = tv[c0 + kBy * T::NC], bz = tv[c0 + kBz * T::NC];
           src[kBx] = -divB[r] * ux; src[kBy] = -divB[r] * uy; src[kBz] = -divB[r] * uz;
           src[kE] = -divB[r] * (bx * ux + by * uy + bz * uz);
           src[kUx] = -divB[r] * bx; src[kUy] = -divB[r] * by; src[kUz] = -divB[r] * bz;
@@ -404,8 +414,8 @@ __global__ void __launch_bounds__(T::NTHR, 1)
           if (a.useDivb) {
             const int ii = cc % T::N, jj = (cc / T::N) % T::N, kk = cc / (T::N * T::N);
             const int c0 = tile_index<T, TileT>(0, ii, jj, kk);
-            const double ux = tile[c0 + kUx * T::NC], uy = tile[c0 + kUy * T::NC], uz = tile[c0 + kUz * T::NC];
-            const double bx = tile[c0 + kBx * T::NC], by = tile[c0 + kBy * T::NC], bz = tile[c0 + kBz * T::NC];
+            const double ux = tv[c0 + kUx * T::NC], uy = tv[c0 + kUy * T::NC], uz = tv[c0 + kUz * T::NC];
+            const double bx = tv[c0 + kBx * T::NC], by = tv[c0 + kBy * T::NC], bz = tv[c0 + kBz * T::NC];
             src[kBx] = -divB[r] * ux; src[kBy] = -divB[r] * uy; src[kBz] = -divB[r] * uz;
             src[kE] = -divB[r] * (bx * ux + by * uy + bz * uz);
             src[kUx] = -divB[r] * bx; src[kUy] = -divB[r] * by; src[kUz] = -divB[r] * bz;
