@@ -124,24 +124,36 @@ def _jfnk(prec, state, net=None, steps=3):
     return out, st, g
 
 
-def test_learned_fgmres_converges_and_gains(net):
+def test_learned_fgmres_converges_and_gains():
+    """The trained network in the FGMRES of advance_part_impl at 32^3: it
+    converges to the tolerance with the BILU answer, and needs fewer Krylov
+    matvecs than the same solver without a preconditioner.  Training as in
+    the benchmark: (v, BILU(v)) pairs of 16 blocks each, half from the Krylov
+    vectors of BILU-preconditioned steps of a differently seeded state, half
+    from probe vectors at its last state, then 8 epochs of Adam."""
+    from batsrus_b200.capi import BxError
     g, s, p, st = configs.jfnk_ot(nRoot=4)
     _, _, _, st2 = configs.jfnk_ot(nRoot=4, seed=2025)
-    # (v, BILU(v)) pairs: Krylov vectors of BILU-preconditioned steps from
-    # another seed, then probe vectors at the last state; then train
+    nPair, bpp = 2000, 16
+    net = LearnedPreconditioner(nSampleMax=nPair * bpp, seed=2024)
     x = ExplicitSolver(g, s)
     x.set_state(st2)
     im = ImplicitSolver(x, p)
-    net.collect(8)
-    for _ in range(4):
-        im.advance_part_impl()
+    net.collect(bpp)
+    for _ in range(100):
+        if net.num_samples() >= (nPair // 2) * bpp:
+            break
+        try:
+            im.advance_part_impl()
+        except BxError:  # a failed solve ends the collection
+            break
     net.collect(0)
-    net.collect_probes(64, 32, seed=5)
+    net.collect_probes(nPair - net.num_samples() // bpp, bpp, seed=2025)
     x.close()
-    assert net.num_samples() > 2000
-    first, last = net.train(nEpoch=8, batch=128, lr=1e-3)
+    assert net.num_samples() == nPair * bpp
+    first, last = net.train(nEpoch=8, batch=256, lr=1e-3)
     assert last < first
-    net.set_blend(0.25)
+    net.set_blend(0.5)
     bilu, sb, g = _jfnk("BILU", st)
     none, sn, _ = _jfnk("NONE", st)
     lrn, sl, _ = _jfnk("LEARNED", st)
@@ -154,4 +166,6 @@ def test_learned_fgmres_converges_and_gains(net):
     # the Krylov counts with and without the network
     nl, nn = sum(q["nMatvec"] for q in lrn[1:]), sum(q["nMatvec"] for q in none[1:])
     print("matvecs learned %d, none %d, bilu %d" % (nl, nn, sum(q["nMatvec"] for q in bilu[1:])))
-    assert nl <= 1.2 * nn, ([q["nMatvec"] for q in lrn], [q["nMatvec"] for q in none])
+    # the gain of the trained network over the same solver without it
+    assert nl < nn, ([q["nMatvec"] for q in lrn], [q["nMatvec"] for q in none])
+    net.close()
