@@ -580,8 +580,8 @@ def main():
     ap.add_argument("--no-cpu", dest="cpu", action="store_false")
     ap.add_argument("--precisions", default="fp64,fp32")
     ap.add_argument("--jfnk-precond", default="BILU,NONE,LEARNED", help="'' to skip the implicit workload")
-    ap.add_argument("--learned-epochs", type=int, default=8)
-    ap.add_argument("--learned-blend", type=float, default=0.25)
+    ap.add_argument("--learned-epochs", type=int, default=64)
+    ap.add_argument("--learned-blend", type=float, default=0.6)
     ap.add_argument("--amr", dest="amr", action="store_true", default=True)
     ap.add_argument("--no-amr", dest="amr", action="store_false")
     ap.add_argument("--amr-nroot", type=int, default=16, help="root blocks per dimension of the blast grid")
