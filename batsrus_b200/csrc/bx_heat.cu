@@ -702,12 +702,7 @@ int gmres(int &iError, cudaStream_t st) {
       if ((r = matvec(Vk, H.t, st))) return r;
       if ((r = precond(H.t, H.w, st))) return r;
       if (H.p.TypePrecond == BX_PRECOND_BILU && learned_collecting() && (r = collect_pair(H.t, H.w, st))) return r;
-      for (int q = 0; q <= k + 1; q++) {
-        const double *vq = q > 0 ? Vb + (size_t)(q - 1) * N : nullptr;
-        const double *hq = q > 0 ? hdev + q - 1 : nullptr;
-        const double *vn = q <= k ? Vb + (size_t)q * N : nullptr;
-        kry_mgs(H.w, vq, hq, vn, N, H.partial, H.cnt, hdev + q, st);
-      }
+      kry_orth(H.w, Vb, k, N, hdev, H.scal + 150, H.partial, H.cnt, st);
       CKH(cudaGetLastError());
       CKH(cudaMemcpyAsync(hb.data(), hdev, sizeof(double) * (k + 2), cudaMemcpyDeviceToHost, st));
       CKH(cudaStreamSynchronize(st));
@@ -792,12 +787,7 @@ int fgmres(int &iError, cudaStream_t st) {
       double *Vk = Vb + (size_t)k * N, *Zk = Zb + (size_t)k * N;
       if ((r = precond(Vk, Zk, st))) return r;
       if ((r = matvec(Zk, H.w, st))) return r;
-      for (int q = 0; q <= k + 1; q++) {
-        const double *vq = q > 0 ? Vb + (size_t)(q - 1) * N : nullptr;
-        const double *hq = q > 0 ? hdev + q - 1 : nullptr;
-        const double *vn = q <= k ? Vb + (size_t)q * N : nullptr;
-        kry_mgs(H.w, vq, hq, vn, N, H.partial, H.cnt, hdev + q, st);
-      }
+      kry_orth(H.w, Vb, k, N, hdev, H.scal + 150, H.partial, H.cnt, st);
       CKH(cudaGetLastError());
       CKH(cudaMemcpyAsync(hb.data(), hdev, sizeof(double) * (k + 2), cudaMemcpyDeviceToHost, st));
       CKH(cudaStreamSynchronize(st));
@@ -1004,7 +994,7 @@ int bx_heat_init(const bx_heat_params *prm, const double *Te, const double *bhat
        cudaMalloc(&H.used, H.nCell) == cudaSuccess &&
        cudaMalloc(&H.blkAt, sizeof(int) * atH.size()) == cudaSuccess &&
        cudaMalloc(&H.blkXYZ, sizeof(int) * xyzH.size()) == cudaSuccess &&
-       cudaMalloc(&H.partial, sizeof(double) * kKryMaxBlocks) == cudaSuccess &&
+       cudaMalloc(&H.partial, sizeof(double) * 3 * kKryMaxBlocks) == cudaSuccess &&
        cudaMalloc(&H.scal, sizeof(double) * 160) == cudaSuccess;
   if (!ok) {
     free_heat();

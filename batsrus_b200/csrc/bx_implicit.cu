@@ -205,12 +205,7 @@ int gmres(int &iError) {
       if ((r = precond(Vk, Zk))) return r;
       if (learned_collecting() && c.nI == 8 && (r = learned_collect(Vk, Zk, c.nBlock, c.st))) return r;
       if ((r = matvec(Zk, I.W))) return r;
-      for (int q = 0; q <= k + 1; q++) {
-        const double *vq = q > 0 ? I.V + (size_t)(q - 1) * N : nullptr;
-        const double *hq = q > 0 ? hdev + q - 1 : nullptr;
-        const double *vn = q <= k ? I.V + (size_t)q * N : nullptr;
-        kry_mgs(I.W, vq, hq, vn, N, I.partial, I.cnt, hdev + q, c.st);
-      }
+      kry_orth(I.W, I.V, k, N, hdev, I.scal + 112, I.partial, I.cnt, c.st);
       CKI(cudaGetLastError());
       CKI(cudaMemcpyAsync(hb.data(), hdev, sizeof(double) * (k + 2), cudaMemcpyDeviceToHost, c.st));
       CKI(cudaStreamSynchronize(c.st));
