@@ -702,7 +702,7 @@ int gmres(int &iError, cudaStream_t st) {
       if ((r = matvec(Vk, H.t, st))) return r;
       if ((r = precond(H.t, H.w, st))) return r;
       if (H.p.TypePrecond == BX_PRECOND_BILU && learned_collecting() && (r = collect_pair(H.t, H.w, st))) return r;
-      kry_orth(H.w, Vb, k, N, hdev, H.scal + 150, H.partial, H.cnt, st);
+      kry_orth(H.w, Vb, k, N, hdev, H.scal + 160, H.partial, H.cnt, st);  // scal 160..177
       CKH(cudaGetLastError());
       CKH(cudaMemcpyAsync(hb.data(), hdev, sizeof(double) * (k + 2), cudaMemcpyDeviceToHost, st));
       CKH(cudaStreamSynchronize(st));
@@ -787,7 +787,7 @@ int fgmres(int &iError, cudaStream_t st) {
       double *Vk = Vb + (size_t)k * N, *Zk = Zb + (size_t)k * N;
       if ((r = precond(Vk, Zk, st))) return r;
       if ((r = matvec(Zk, H.w, st))) return r;
-      kry_orth(H.w, Vb, k, N, hdev, H.scal + 150, H.partial, H.cnt, st);
+      kry_orth(H.w, Vb, k, N, hdev, H.scal + 160, H.partial, H.cnt, st);  // scal 160..177
       CKH(cudaGetLastError());
       CKH(cudaMemcpyAsync(hb.data(), hdev, sizeof(double) * (k + 2), cudaMemcpyDeviceToHost, st));
       CKH(cudaStreamSynchronize(st));
@@ -994,8 +994,8 @@ int bx_heat_init(const bx_heat_params *prm, const double *Te, const double *bhat
        cudaMalloc(&H.used, H.nCell) == cudaSuccess &&
        cudaMalloc(&H.blkAt, sizeof(int) * atH.size()) == cudaSuccess &&
        cudaMalloc(&H.blkXYZ, sizeof(int) * xyzH.size()) == cudaSuccess &&
-       cudaMalloc(&H.partial, sizeof(double) * 3 * kKryMaxBlocks) == cudaSuccess &&
-       cudaMalloc(&H.scal, sizeof(double) * 160) == cudaSuccess;
+       cudaMalloc(&H.partial, sizeof(double) * 10 * kKryMaxBlocks) == cudaSuccess &&
+       cudaMalloc(&H.scal, sizeof(double) * 192) == cudaSuccess;
   if (!ok) {
     free_heat();
     return core_fail(BX_ERR_NOMEM, "heat conduction buffers");

@@ -205,7 +205,7 @@ int gmres(int &iError) {
       if ((r = precond(Vk, Zk))) return r;
       if (learned_collecting() && c.nI == 8 && (r = learned_collect(Vk, Zk, c.nBlock, c.st))) return r;
       if ((r = matvec(Zk, I.W))) return r;
-      kry_orth(I.W, I.V, k, N, hdev, I.scal + 112, I.partial, I.cnt, c.st);
+      kry_orth(I.W, I.V, k, N, hdev, I.scal + 104, I.partial, I.cnt, c.st);  // scal 104..121
       CKI(cudaGetLastError());
       CKI(cudaMemcpyAsync(hb.data(), hdev, sizeof(double) * (k + 2), cudaMemcpyDeviceToHost, c.st));
       CKI(cudaStreamSynchronize(c.st));
@@ -354,7 +354,7 @@ int bx_implicit_init(const bx_implicit_params *prm) {
     if (cudaMalloc(p, vb) != cudaSuccess) { free_impl(); return core_fail(BX_ERR_NOMEM, "implicit vectors"); }
   if (cudaMalloc(&I.V, vb * (I.m + 1)) != cudaSuccess || cudaMalloc(&I.Z, vb * I.m) != cudaSuccess ||
       cudaMalloc(&I.dtCell, sizeof(double) * I.nCellTot) != cudaSuccess ||
-      cudaMalloc(&I.partial, sizeof(double) * kRedBlocks * 8) != cudaSuccess ||
+      cudaMalloc(&I.partial, sizeof(double) * (kRedBlocks * 8 > 10 * kKryMaxBlocks ? kRedBlocks * 8 : 10 * kKryMaxBlocks)) != cudaSuccess ||
       cudaMalloc(&I.scal, sizeof(double) * 128) != cudaSuccess || cudaMalloc(&I.dNorm, sizeof(double) * 8) != cudaSuccess ||
       cudaMalloc(&I.cnt, sizeof(unsigned)) != cudaSuccess || cudaMemset(I.cnt, 0, sizeof(unsigned)) != cudaSuccess) {
     free_impl();

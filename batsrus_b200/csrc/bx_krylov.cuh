@@ -152,112 +152,6 @@ __device__ __forceinline__ void kry_finish_n(const double (&v)[NS], double *part
   if (threadIdx.x == 0) *cnt = 0;
 }
 
-// two Gram-Schmidt steps in one pass over w:
-//   w -= a va + b vb,  a = *ha,  b = *d1 - a * *g   (stored in *hb)
-// (b is the modified Gram-Schmidt coefficient (w - a va) . vb, from w . vb
-// and va . vb of the previous pass), then the inner products of the updated
-// w with vc and vd and vc . vd for the next pass, or w . w without VC.
-// VB, VD false: one step; one inner product.  The main loop issues all
-// loads of its U elements before any arithmetic.
-template <bool VB, bool VC, bool VD, int U>
-__global__ void __launch_bounds__(kKryThreads) k_kry_gs2(double *__restrict__ w, const double *__restrict__ va,
-                                                         const double *__restrict__ vb, const double *ha,
-                                                         const double *d1, const double *g, double *hb,
-                                                         const double *__restrict__ vc, const double *__restrict__ vd,
-                                                         long n, double *partial, unsigned *cnt, double *oc,
-                                                         double *od, double *ocd) {
-  __shared__ double sh[32];
-  const double a = *ha;
-  const double b = VB ? *d1 - a * *g : 0.0;
-  if (VB && blockIdx.x == 0 && threadIdx.x == 0) *hb = b;
-  const long n2 = n >> 1;
-  const long stride = (long)gridDim.x * blockDim.x;
-  double2 *w2 = reinterpret_cast<double2 *>(w);
-  const double2 *a2 = reinterpret_cast<const double2 *>(va), *b2 = reinterpret_cast<const double2 *>(vb);
-  const double2 *c2 = reinterpret_cast<const double2 *>(vc), *e2 = reinterpret_cast<const double2 *>(vd);
-  double sc = 0.0, sd = 0.0, scd = 0.0;
-  auto step = [&](double2 x, double2 pa, double2 pb, double2 c, double2 e, long q) {
-    x.x = x.x - a * pa.x;
-    x.y = x.y - a * pa.y;
-    if (VB) {
-      x.x = x.x - b * pb.x;
-      x.y = x.y - b * pb.y;
-    }
-    w2[q] = x;
-    if (VC) {
-      sc += x.x * c.x + x.y * c.y;
-      if (VD) {
-        sd += x.x * e.x + x.y * e.y;
-        scd += c.x * e.x + c.y * e.y;
-      }
-    } else {
-      sc += x.x * x.x + x.y * x.y;
-    }
-  };
-  const double2 z = make_double2(0.0, 0.0);
-  long q = blockIdx.x * (long)blockDim.x + threadIdx.x;
-  for (; q + (U - 1) * stride < n2; q += U * stride) {
-    double2 x[U], pa[U], pb[U], c[U], e[U];
-#pragma unroll
-    for (int u = 0; u < U; u++) {
-      x[u] = w2[q + u * stride];
-      pa[u] = __ldcs(a2 + q + u * stride);
-      pb[u] = VB ? __ldcs(b2 + q + u * stride) : z;
-      c[u] = VC ? c2[q + u * stride] : z;
-      e[u] = VD ? e2[q + u * stride] : z;
-    }
-#pragma unroll
-    for (int u = 0; u < U; u++) step(x[u], pa[u], pb[u], c[u], e[u], q + u * stride);
-  }
-  for (; q < n2; q += stride)
-    step(w2[q], a2[q], VB ? b2[q] : z, VC ? c2[q] : z, VD ? e2[q] : z, q);
-  if (VD) {
-    double *const outs[3] = {oc, od, ocd};
-    kry_finish_n<3>({sc, sd, scd}, partial, cnt, outs, sh);
-  } else {
-    double *const outs[1] = {oc};
-    kry_finish_n<1>({sc}, partial, cnt, outs, sh);
-  }
-}
-
-template <int U>
-inline void kry_gs2_u(double *w, const double *va, const double *vb, const double *ha, const double *d1,
-                      const double *g, double *hb, const double *vc, const double *vd, long n, double *partial,
-                      unsigned *cnt, double *oc, double *od, double *ocd, cudaStream_t st) {
-  const int gr = kry_grid();
-#define BX_GS2(B, C, D)                                                                                        \
-  k_kry_gs2<B, C, D, U><<<gr, kKryThreads, 0, st>>>(w, va, vb, ha, d1, g, hb, vc, vd, n, partial, cnt, oc, od, \
-                                                    ocd)
-  if (vb && vc && vd) BX_GS2(true, true, true);
-  else if (vb && vc) BX_GS2(true, true, false);
-  else if (vb) BX_GS2(true, false, false);
-  else if (vc && vd) BX_GS2(false, true, true);
-  else if (vc) BX_GS2(false, true, false);
-  else BX_GS2(false, false, false);
-#undef BX_GS2
-}
-
-// the first pass of kry_orth: w . c, w . d and c . d
-static __global__ void __launch_bounds__(kKryThreads) k_kry_gs2_first(const double *__restrict__ w,
-                                                               const double *__restrict__ c,
-                                                               const double *__restrict__ d, long n, double *partial,
-                                                               unsigned *cnt, double *oc, double *od, double *ocd) {
-  __shared__ double sh[32];
-  const long n2 = n >> 1;
-  const long stride = (long)gridDim.x * blockDim.x;
-  const double2 *w2 = reinterpret_cast<const double2 *>(w), *c2 = reinterpret_cast<const double2 *>(c),
-                *d2 = reinterpret_cast<const double2 *>(d);
-  double sc = 0.0, sd = 0.0, scd = 0.0;
-  for (long q = blockIdx.x * (long)blockDim.x + threadIdx.x; q < n2; q += stride) {
-    const double2 x = w2[q], cc = c2[q], dd = d2[q];
-    sc += x.x * cc.x + x.y * cc.y;
-    sd += x.x * dd.x + x.y * dd.y;
-    scd += cc.x * dd.x + cc.y * dd.y;
-  }
-  double *const outs[3] = {oc, od, ocd};
-  kry_finish_n<3>({sc, sd, scd}, partial, cnt, outs, sh);
-}
-
 template <int U>
 inline void kry_mgs_u(double *w, const double *vq, const double *hq, const double *vn, long n, double *partial,
                       unsigned *cnt, double *out, cudaStream_t st) {
@@ -309,13 +203,129 @@ static __global__ void __launch_bounds__(kKryThreads) k_kry_update(double *__res
   }
 }
 
+// up to four Gram-Schmidt steps in one pass over w.  NA vectors va[] are
+// subtracted with the coefficients of modified Gram-Schmidt:
+//   c_0 = *h0 (the inner product w . va[0] of the previous pass),
+//   c_j = d_j - sum_{i<j} c_i G_ij  (d_j = w . va[j] and the Gram entries
+//   G_ij = va[i] . va[j] of the previous pass, in din), stored in hout[j-1];
+// then the NC inner products of the updated w with vc[] and the Gram entries
+// among vc[] for the next pass (or w . w when NC = 0) go to outs[].  With
+// NA = 0 nothing is subtracted and w is only read.  Gram entries are ordered
+// (0,1), (0,2), (0,3), (1,2), (1,3), (2,3) (those that exist).
+struct GsArgs {
+  double *w;
+  const double *va[4], *vc[4];
+  const double *h0, *din;  // din: d_1 .. d_3 then the Gram entries
+  double *hout;
+  double *outs[10];
+  long n;
+  double *partial;
+  unsigned *cnt;
+};
+
+__host__ __device__ constexpr int gs_pair(int i, int j, int m) {
+  // index of (i, j), i < j, among the pairs of m vectors in the order above
+  return i * m - i * (i + 1) / 2 + (j - i - 1);
+}
+
+template <int NA, int NC, int U>
+__global__ void __launch_bounds__(kKryThreads) k_kry_gs(GsArgs g) {
+  constexpr int NS = NC > 0 ? NC + NC * (NC - 1) / 2 : 1;
+  __shared__ double sh[32];
+  double c[NA > 0 ? NA : 1];
+  if (NA > 0) {
+    c[0] = *g.h0;
+#pragma unroll
+    for (int j = 1; j < NA; j++) {
+      double t = g.din[j - 1];
+#pragma unroll
+      for (int i = 0; i < j; i++) t = t - c[i] * g.din[3 + gs_pair(i, j, NA)];
+      c[j] = t;
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0)
+#pragma unroll
+      for (int j = 1; j < NA; j++) g.hout[j - 1] = c[j];
+  }
+  const long n2 = g.n >> 1;
+  const long stride = (long)gridDim.x * blockDim.x;
+  double2 *w2 = reinterpret_cast<double2 *>(g.w);
+  double acc[NS];
+#pragma unroll
+  for (int k = 0; k < NS; k++) acc[k] = 0.0;
+  auto step = [&](double2 x, const double2 (&pa)[NA > 0 ? NA : 1], const double2 (&pc)[NC > 0 ? NC : 1], long q) {
+    if (NA > 0) {
+#pragma unroll
+      for (int j = 0; j < NA; j++) {
+        x.x = x.x - c[j] * pa[j].x;
+        x.y = x.y - c[j] * pa[j].y;
+      }
+      w2[q] = x;
+    }
+    if (NC > 0) {
+#pragma unroll
+      for (int i = 0; i < NC; i++) acc[i] += x.x * pc[i].x + x.y * pc[i].y;
+#pragma unroll
+      for (int i = 0; i < NC; i++)
+#pragma unroll
+        for (int j = i + 1; j < NC; j++) acc[NC + gs_pair(i, j, NC)] += pc[i].x * pc[j].x + pc[i].y * pc[j].y;
+    } else {
+      acc[0] += x.x * x.x + x.y * x.y;
+    }
+  };
+  long q = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  for (; q + (U - 1) * stride < n2; q += U * stride) {
+    double2 x[U], pa[U][NA > 0 ? NA : 1], pc[U][NC > 0 ? NC : 1];
+#pragma unroll
+    for (int u = 0; u < U; u++) {
+      x[u] = w2[q + u * stride];
+#pragma unroll
+      for (int j = 0; j < NA; j++) pa[u][j] = __ldcs(reinterpret_cast<const double2 *>(g.va[j]) + q + u * stride);
+#pragma unroll
+      for (int j = 0; j < NC; j++) pc[u][j] = reinterpret_cast<const double2 *>(g.vc[j])[q + u * stride];
+    }
+#pragma unroll
+    for (int u = 0; u < U; u++) step(x[u], pa[u], pc[u], q + u * stride);
+  }
+  for (; q < n2; q += stride) {
+    double2 pa[NA > 0 ? NA : 1], pc[NC > 0 ? NC : 1];
+#pragma unroll
+    for (int j = 0; j < NA; j++) pa[j] = reinterpret_cast<const double2 *>(g.va[j])[q];
+#pragma unroll
+    for (int j = 0; j < NC; j++) pc[j] = reinterpret_cast<const double2 *>(g.vc[j])[q];
+    step(w2[q], pa, pc, q);
+  }
+  kry_finish_n<NS>(acc, g.partial, g.cnt, *reinterpret_cast<double *const(*)[NS]>(g.outs), sh);
+}
+
+template <int NA>
+inline void kry_gs_na(const GsArgs &a, int nc, cudaStream_t st) {
+  const int gr = kry_grid();
+  switch (nc) {
+    case 0: k_kry_gs<NA, 0, 2><<<gr, kKryThreads, 0, st>>>(a); break;
+    case 1: k_kry_gs<NA, 1, 2><<<gr, kKryThreads, 0, st>>>(a); break;
+    case 2: k_kry_gs<NA, 2, 2><<<gr, kKryThreads, 0, st>>>(a); break;
+    case 3: k_kry_gs<NA, 3, 2><<<gr, kKryThreads, 0, st>>>(a); break;
+    default: k_kry_gs<NA, 4, 2><<<gr, kKryThreads, 0, st>>>(a); break;
+  }
+}
+
+inline void kry_gs(const GsArgs &a, int na, int nc, cudaStream_t st) {
+  switch (na) {
+    case 0: kry_gs_na<0>(a, nc, st); break;
+    case 1: kry_gs_na<1>(a, nc, st); break;
+    case 2: kry_gs_na<2>(a, nc, st); break;
+    case 3: kry_gs_na<3>(a, nc, st); break;
+    default: kry_gs_na<4>(a, nc, st); break;
+  }
+}
+
 // Orthogonalisation of w against the Krylov vectors V_0..V_k (V_q at
 // V + q n), the Hessenberg column into h[0..k+1] (h[k+1] = |w|^2 before the
 // normalisation), as modified Gram-Schmidt.  With the knob
-// kTuneKryGsSteps = 1, one pass per step (k_kry_mgs_t); with 2, one pass per
-// two steps (k_kry_gs2), which reads four vectors and w and writes w per two
-// steps instead of six and two: the same coefficients in exact arithmetic,
-// rounded differently.  tmp: 4 device doubles; partial: 3 x kKryMaxBlocks.
+// kTuneKryGsSteps = 1, one pass per step (k_kry_mgs_t); with S = 2..4, one
+// pass per S steps (k_kry_gs), which reads 2S vectors and w and writes w per
+// S steps instead of 3S and S: the same coefficients in exact arithmetic,
+// rounded differently.  tmp: 18 device doubles; partial: 10 x kKryMaxBlocks.
 inline void kry_orth(double *w, const double *V, int k, long n, double *h, double *tmp, double *partial,
                      unsigned *cnt, cudaStream_t st) {
   if (tune_value(kTuneKryGsSteps) < 2) {
@@ -327,28 +337,37 @@ inline void kry_orth(double *w, const double *V, int k, long n, double *h, doubl
     }
     return;
   }
-  const int g = kry_grid();
-  auto vec = [&](int q) { return q <= k ? V + (size_t)q * n : nullptr; };
-  // the first pass: w . V_0, w . V_1 and V_0 . V_1 (w . w when k < 0)
-  {
-    const double *c = vec(0), *d = vec(1);
-    if (c && d) {
-      k_kry_gs2_first<<<g, kKryThreads, 0, st>>>(w, c, d, n, partial, cnt, h, tmp, tmp + 1);
-    } else {
-      kry_mgs(w, nullptr, nullptr, c, n, partial, cnt, h, st);
+  // groups of S vectors: a pass subtracts one group and takes the inner
+  // products (and Gram entries) of the next; tmp holds two sets of 9
+  const int S = tune_value(kTuneKryGsSteps);
+  auto count = [&](int q0) { return q0 > k ? 0 : (k + 1 - q0 < S ? k + 1 - q0 : S); };
+  auto fill = [&](GsArgs &a, int q0, int nc, double *to, int slotNorm) {
+    for (int j = 0; j < nc; j++) a.vc[j] = V + (size_t)(q0 + j) * n;
+    if (nc == 0) {
+      a.outs[0] = h + slotNorm;
+      return;
     }
-  }
+    a.outs[0] = h + q0;                         // the next pass's c_0
+    for (int j = 1; j < nc; j++) a.outs[j] = to + (j - 1);       // d_1 .. d_3
+    for (int i = 0; i < nc; i++)
+      for (int j = i + 1; j < nc; j++) a.outs[nc + gs_pair(i, j, nc)] = to + 3 + gs_pair(i, j, nc);
+  };
+  GsArgs a;
+  a.w = w; a.n = n; a.partial = partial; a.cnt = cnt;
+  // the first pass: inner products and Gram entries of the first group
+  int nc = count(0);
+  fill(a, 0, nc, tmp, k + 1);
+  kry_gs(a, 0, nc, st);
   int buf = 0;
-  for (int q = 0; q <= k; q += 2) {
-    const double *va = vec(q), *vb = q + 1 <= k ? vec(q + 1) : nullptr;
-    const double *vc = vec(q + 2), *vd = q + 3 <= k ? vec(q + 3) : nullptr;
-    double *in = tmp + 2 * buf, *out = tmp + 2 * (1 - buf);
-    double *oc = vc ? h + q + 2 : h + (vb ? q + 2 : q + 1);
-    switch (tune_value(kTuneKryUnroll)) {
-      case 1: kry_gs2_u<1>(w, va, vb, h + q, in, in + 1, h + q + 1, vc, vd, n, partial, cnt, oc, out, out + 1, st); break;
-      case 4: kry_gs2_u<4>(w, va, vb, h + q, in, in + 1, h + q + 1, vc, vd, n, partial, cnt, oc, out, out + 1, st); break;
-      default: kry_gs2_u<2>(w, va, vb, h + q, in, in + 1, h + q + 1, vc, vd, n, partial, cnt, oc, out, out + 1, st);
-    }
+  for (int q = 0; q <= k; q += S) {
+    const int na = count(q);
+    nc = count(q + S);
+    for (int j = 0; j < na; j++) a.va[j] = V + (size_t)(q + j) * n;
+    a.h0 = h + q;
+    a.din = tmp + 9 * buf;
+    a.hout = h + q + 1;
+    fill(a, q + S, nc, tmp + 9 * (1 - buf), k + 1);
+    kry_gs(a, na, nc, st);
     buf = 1 - buf;
   }
 }

@@ -30,7 +30,7 @@ struct LCtx {
   int collectPerPair = 0;  // blocks stored per collected pair (0: not collecting)
   std::mt19937_64 rng;
   float *p = nullptr, *m = nullptr, *v = nullptr, *g = nullptr;
-  __nv_bfloat16 *w1 = nullptr, *w2 = nullptr, *w3 = nullptr, *w3t = nullptr, *w2t = nullptr;
+  __nv_bfloat16 *w1 = nullptr, *w2 = nullptr, *w3 = nullptr, *w3t = nullptr, *w2t = nullptr, *w1p = nullptr;
   __nv_bfloat16 *feat = nullptr;
   long featBlocks = 0;
   __nv_bfloat16 *in16 = nullptr;  // [nSampleMax][512][16]
@@ -86,7 +86,7 @@ void free_learned() {
     if (*q) cudaFree(*q);
     *q = nullptr;
   }
-  for (__nv_bfloat16 **q : {&Lc.w1, &Lc.w2, &Lc.w3, &Lc.w3t, &Lc.w2t, &Lc.feat, &Lc.in16, &Lc.A1, &Lc.A2, &Lc.dY1,
+  for (__nv_bfloat16 **q : {&Lc.w1, &Lc.w1p, &Lc.w2, &Lc.w3, &Lc.w3t, &Lc.w2t, &Lc.feat, &Lc.in16, &Lc.A1, &Lc.A2, &Lc.dY1,
                             &Lc.dY2, &Lc.dY3}) {
     if (*q) cudaFree(*q);
     *q = nullptr;
@@ -103,6 +103,7 @@ void free_learned() {
 Weights weights() {
   Weights W;
   W.w1 = reinterpret_cast<const unsigned char *>(Lc.w1);
+  W.w1p = reinterpret_cast<const unsigned char *>(Lc.w1p);
   W.w2 = reinterpret_cast<const unsigned char *>(Lc.w2);
   W.w3 = reinterpret_cast<const unsigned char *>(Lc.w3);
   W.w3t = reinterpret_cast<const unsigned char *>(Lc.w3t);
@@ -118,7 +119,7 @@ Weights weights() {
 
 int pack(cudaStream_t st) {
   const int n = kTaps * kC2 * kC1;
-  k_pack<<<(n + 255) / 256, 256, 0, st>>>(Lc.p, Lc.w1, Lc.w2, Lc.w3, Lc.w3t, Lc.w2t);
+  k_pack<<<(n + 255) / 256, 256, 0, st>>>(Lc.p, Lc.w1, Lc.w2, Lc.w3, Lc.w3t, Lc.w2t, Lc.w1p);
   CKL(cudaGetLastError());
   return BX_OK;
 }
@@ -410,7 +411,7 @@ int bx_learned_init(long long nSampleMax, unsigned long long seed) {
   Lc.blend = 1.0;
   bool okAlloc = true;
   for (float **q : {&Lc.p, &Lc.m, &Lc.v, &Lc.g}) okAlloc = okAlloc && cudaMalloc(q, sizeof(float) * kNParam) == cudaSuccess;
-  okAlloc = okAlloc && cudaMalloc(&Lc.w1, kW1Bytes) == cudaSuccess && cudaMalloc(&Lc.w2, kW2Bytes) == cudaSuccess &&
+  okAlloc = okAlloc && cudaMalloc(&Lc.w1, kW1Bytes) == cudaSuccess && cudaMalloc(&Lc.w1p, kW1pBytes) == cudaSuccess && cudaMalloc(&Lc.w2, kW2Bytes) == cudaSuccess &&
             cudaMalloc(&Lc.w3, kW3Bytes) == cudaSuccess && cudaMalloc(&Lc.w3t, kW3tBytes) == cudaSuccess &&
             cudaMalloc(&Lc.w2t, kW2tBytes) == cudaSuccess;
   okAlloc = okAlloc && cudaMalloc(&Lc.in16, sizeof(__nv_bfloat16) * 512 * 16 * (size_t)nSampleMax) == cudaSuccess &&

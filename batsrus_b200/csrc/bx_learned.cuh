@@ -39,6 +39,16 @@ constexpr int kW3Bytes = kTaps * kN3 * kC2 * 2;
 constexpr int kW3tBytes = kTaps * kC2 * kN3 * 2;
 constexpr int kW2tBytes = kTaps * kC1 * kC2 * 2;
 constexpr int kLS16 = 2 * 160, kLS32 = 4 * 160;
+// layer 1 in linear mode: input channels 8..15 are zero, so two taps share a
+// K = 16 MMA (14 MMAs instead of 27 per tile): MMAs 0..8 pair dx = -1 with
+// dx = 0 of the (dz, dy) row m, MMAs 9..13 pair the dx = +1 taps of rows
+// 2s and 2s + 1 (row 8 alone, its second chunk on the zero channels)
+constexpr int kPack1 = 14;
+constexpr int kW1pBytes = kPack1 * 32 * 16 * 2;
+__host__ __device__ constexpr int pack1_tap(int m, int half) {  // -1: none
+  return m < 9 ? 9 * (m / 3) + 3 * (m % 3) + half
+               : (2 * (m - 9) + half > 8 ? -1 : 9 * ((2 * (m - 9) + half) / 3) + 3 * ((2 * (m - 9) + half) % 3) + 2);
+}
 constexpr int kBuf16 = kLines * kLS16, kBuf32 = kLines * kLS32;
 
 __host__ __device__ constexpr int tile_line0(int t) { return t < 4 ? 10 + 16 * t : 65; }
@@ -131,6 +141,36 @@ __device__ __forceinline__ void issue_conv_tile(int t, uint32_t bufIn, uint32_t 
   tc::commit(bar);
 }
 
+// layer 1 of M tile t in linear mode with two taps per MMA (kPack1 MMAs; the
+// packed weight image w1p holds kPack1 K-major 32 x 16 images), committed to
+// bar.  The A operand of a pair is the first tap's cells; its second K chunk
+// (the second tap) lies LBO bytes further: one cell (16 bytes) for dx = -1 /
+// 0, the distance between the two rows for dx = +1, or the zero channels
+// (160 bytes) for the last tap alone.
+__device__ __forceinline__ void issue_conv1_packed_tile(int t, uint32_t bufIn, uint32_t w1p, uint32_t tmem,
+                                                        uint64_t *bar) {
+  constexpr int LS = kLS16;
+  constexpr uint32_t idesc = tc::idesc_bf16(128, 32, false, false);
+  const uint32_t base = bufIn + (uint32_t)(tile_line0(t) * LS);
+  const uint32_t d = tmem + (uint32_t)(t * 32);
+  tc::fence_after();
+#pragma unroll
+  for (int m = 0; m < kPack1; m++) {
+    const int ta = pack1_tap(m, 0), tb = pack1_tap(m, 1);
+    const int dza = ta / 9 - 1, dya = (ta / 3) % 3 - 1, dxa = ta % 3 - 1;
+    const int offA = (dza * 9 + dya) * LS + (1 + dxa) * 16;
+    int lbo = 160;
+    if (tb >= 0) {
+      const int dzb = tb / 9 - 1, dyb = (tb / 3) % 3 - 1, dxb = tb % 3 - 1;
+      lbo = ((dzb * 9 + dyb) * LS + (1 + dxb) * 16) - offA;
+    }
+    const uint64_t ad = tc::sdesc(base + (uint32_t)offA, (uint32_t)lbo, LS);
+    const uint64_t bd = tc::sdesc(w1p + (uint32_t)(m * 1024), 128, 256);
+    tc::mma_bf16(d, ad, bd, idesc, m != 0);
+  }
+  tc::commit(bar);
+}
+
 // copy n bytes (multiple of 16) global -> shared with 16-byte loads
 __device__ __forceinline__ void copy_g2s(void *dst, const void *src, int n) {
   const uint4 *s = reinterpret_cast<const uint4 *>(src);
@@ -164,6 +204,7 @@ __device__ __forceinline__ void stage_dense(unsigned char *buf, const __nv_bfloa
 struct Weights {
   // packed BF16 images (global)
   const unsigned char *w1, *w2, *w3, *w3t, *w2t;
+  const unsigned char *w1p;  // layer 1, two taps per MMA (linear mode)
   const float *b1, *b2, *b3;  // biases (FP32)
   int relu;  // 1: ReLU between the layers and the cell features as input;
              // 0: linear in the Krylov vector (no activation, features off)

@@ -149,7 +149,8 @@ __global__ void __launch_bounds__(kThreads, 1)
   Smem &S = *reinterpret_cast<Smem *>(w3 + kW3Bytes);
   zero_smem(bufA, kBuf32);
   zero_smem(bufB, kBuf32);
-  copy_g2s(w1, W.w1, kW1Bytes);
+  if (W.relu) copy_g2s(w1, W.w1, kW1Bytes);
+  else copy_g2s(w1, W.w1p, kW1pBytes);  // the packed image in the layer-1 slot
   copy_g2s(w2, W.w2, kW2Bytes);
   copy_g2s(w3, W.w3, kW3Bytes);
   setup(S, W);
@@ -204,8 +205,12 @@ __global__ void __launch_bounds__(kThreads, 1)
     }
     fence_proxy_async_smem();
     __syncthreads();
-    if ((threadIdx.x & 31) == 0 && threadIdx.x < 32 * kTiles)
-      issue_conv_tile<2, 32, false>(threadIdx.x >> 5, smem_u32(bufB), smem_u32(w1), tmem, &S.tileBar[threadIdx.x >> 5]);
+    if ((threadIdx.x & 31) == 0 && threadIdx.x < 32 * kTiles) {
+      if (W.relu)
+        issue_conv_tile<2, 32, false>(threadIdx.x >> 5, smem_u32(bufB), smem_u32(w1), tmem, &S.tileBar[threadIdx.x >> 5]);
+      else
+        issue_conv1_packed_tile(threadIdx.x >> 5, smem_u32(bufB), smem_u32(w1), tmem, &S.tileBar[threadIdx.x >> 5]);
+    }
     for_tiles_wait<32>(tmem, S, phase, [&](int, int, int cell, const float(&acc)[32]) {
       if (cell >= 0) relu_store32(bufA, S.bias, cell, acc, nullptr, W.relu);
     });
@@ -567,8 +572,14 @@ __device__ __forceinline__ int bimg_index(int tap, int n, int k, int N, int K) {
 
 // pack the five BF16 images from the FP32 parameters
 __global__ void k_pack(const float *__restrict__ p, __nv_bfloat16 *w1, __nv_bfloat16 *w2, __nv_bfloat16 *w3,
-                       __nv_bfloat16 *w3t, __nv_bfloat16 *w2t) {
+                       __nv_bfloat16 *w3t, __nv_bfloat16 *w2t, __nv_bfloat16 *w1p) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < kPack1 * kC1 * 16) {  // w1p: N 32, K 16 = channels 0..7 of two taps
+    const int m = i / (kC1 * 16), n = (i / 16) % kC1, k = i % 16;
+    const int tap = pack1_tap(m, k >> 3);
+    w1p[bimg_index(m, n, k, kC1, 16)] =
+        __float2bfloat16_rn(tap >= 0 ? p[kOffW1 + (tap * kC0 + (k & 7)) * kC1 + n] : 0.f);
+  }
   // forward images: n = output channel, k = input channel
   if (i < kTaps * kC1 * kC0) {  // w1: N 32, K 16
     const int tap = i / (kC1 * kC0), n = (i / kC0) % kC1, k = i % kC0;

@@ -17,7 +17,7 @@ enum TuneKnob {
   kTuneHeatIluWarps,   // heat ILU sweeps: warps (groups of 32 blocks) per CTA
   kTuneBiluThreads,    // JFNK BILU sweeps: threads per block CTA (8 per cell of a wavefront)
   kTuneStageFpt,       // stage kernel, 8^3 blocks: faces per thread (1: 576 threads, 2: 288)
-  kTuneKryGsSteps,     // Gram-Schmidt steps per pass over w (1: one per step, 2: two); set, not timed
+  kTuneKryGsSteps,     // Gram-Schmidt steps per pass over w (1 to 4); set, not timed
   kNumTune
 };
 

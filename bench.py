@@ -262,7 +262,7 @@ def run_jfnk(args, lrank):
     return out
 
 
-def train_learned(args, g, s, lrank, nPair=2000, blocksPerPair=16):
+def train_learned(args, g, s, lrank, nPair=2000, blocksPerPair=32):
     """Training data and training of the learned preconditioner: (v, BILU(v))
     pairs, half of them the Krylov vectors of the BILU-preconditioned FGMRES
     of implicit steps, half seeded probe vectors (noise smoothed inside the

@@ -98,18 +98,18 @@ def test_gpu_jfnk_first_step_only_sets_the_time_step():
     assert rel(x.get_state()[isl], st0[isl]) < 1e-14
 
 
-@pytest.mark.parametrize("prec", ["BILU", "NONE"])
-def test_two_step_gram_schmidt_steps_agree_with_one_step(prec):
-    """the default krylov_gs_steps = 2 against 1: the same implicit steps to
-    1e-6 relative and the matrix-vector counts within one per step"""
+@pytest.mark.parametrize("prec,steps_per_pass", [("BILU", 2), ("NONE", 2), ("BILU", 3), ("NONE", 4)])
+def test_multi_step_gram_schmidt_steps_agree_with_one_step(prec, steps_per_pass):
+    """krylov_gs_steps = 2..4 against 1: the same implicit steps to 1e-6
+    relative and the matrix-vector counts within one per step"""
     out = {}
-    for steps in (1, 2):
+    for steps in (1, steps_per_pass):
         capi.tune_set("krylov_gs_steps", steps)
         g, o, x, im = pair(prec)
         stats = [im.advance_part_impl() for _ in range(4)]
         out[steps] = ([q["nMatvec"] for q in stats], x.get_state()[g.interior_slices()])
         x.close()
     capi.tune_reset()
-    (n1, s1), (n2, s2) = out[1], out[2]
+    (n1, s1), (n2, s2) = out[1], out[steps_per_pass]
     assert all(abs(a - b) <= 1 for a, b in zip(n1, n2)), (n1, n2)
     assert rel(s2, s1) < 1e-6
