@@ -149,10 +149,11 @@ __global__ void k_features(const double *__restrict__ U, const double *__restric
     const long b = q / 512, c = q % 512;
     uint4 o;
     uint32_t *w = reinterpret_cast<uint32_t *>(&o);
+    auto fin = [](double x) { return isfinite(x) ? (float)x : 0.f; };  // a state that is not finite: no feature
 #pragma unroll
     for (int m = 0; m < 4; m++)
-      w[m] = pack_bf16x2((float)(U[(b * 8 + 2 * m) * 512 + c] / norm[2 * m]),
-                         (float)(U[(b * 8 + 2 * m + 1) * 512 + c] / norm[2 * m + 1]));
+      w[m] = pack_bf16x2(fin(U[(b * 8 + 2 * m) * 512 + c] / norm[2 * m]),
+                         fin(U[(b * 8 + 2 * m + 1) * 512 + c] / norm[2 * m + 1]));
     reinterpret_cast<uint4 *>(feat)[q] = o;
   }
 }
@@ -180,9 +181,13 @@ __global__ void k_collect(const double *__restrict__ w, const double *__restrict
   for (int c = threadIdx.x; c < 512; c += blockDim.x) {
     uint4 q[2];
     uint32_t *u = reinterpret_cast<uint32_t *>(q);
+    // a vector that is not finite (a solve that diverged while its pairs
+    // were collected) gives a zero input and a zero target: no loss, no
+    // gradient
+    auto fin = [](double x) { return isfinite(x) ? (float)x : 0.f; };
 #pragma unroll
     for (int m = 0; m < 4; m++)
-      u[m] = pack_bf16x2((float)(wb[(2 * m) * 512 + c] * inv), (float)(wb[(2 * m + 1) * 512 + c] * inv));
+      u[m] = pack_bf16x2(fin(wb[(2 * m) * 512 + c] * inv), fin(wb[(2 * m + 1) * 512 + c] * inv));
     q[1] = reinterpret_cast<const uint4 *>(feat)[(size_t)b * 512 + c];
     uint4 *dst = reinterpret_cast<uint4 *>(in16 + (n * 512 + c) * 16);
     dst[0] = q[0];
