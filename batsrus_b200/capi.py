@@ -16,7 +16,7 @@ LIB_PATH = os.path.join(_HERE, "_lib", "libbx200.so")
 BX_OK = 0
 STATUS = {0: "BX_OK", 1: "BX_ERR_ARG", 2: "BX_ERR_CUDA", 3: "BX_ERR_STATE", 4: "BX_ERR_NONPHYSICAL",
           5: "BX_ERR_HLLD", 6: "BX_ERR_KRYLOV", 7: "BX_ERR_TIMEOUT", 8: "BX_ERR_NOMEM"}
-FLUX = {"rusanov": 0, "linde": 1, "hlld": 2}
+FLUX = {"rusanov": 0, "linde": 1, "hlld": 2, "roe": 3}
 LIMITER = {"minmod": 0, "mc": 1, "mc3": 2, "koren": 2, "no": 0}
 BC = {"float": 0, "periodic": 1}
 PRECISION = {"fp64": 0, "fp32": 1, "fp32-bulk": 1}

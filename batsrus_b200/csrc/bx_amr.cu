@@ -129,7 +129,9 @@ __device__ __forceinline__ void rc_face_sum(const StageArgs &a, const RcSlab &S,
         L[v] = hi ? Pc[v] : Pf[v];
         R[v] = hi ? Pf[v] : Pc[v];
       }
-      ok = face_slots<D, FLUX, Real>(L, R, (Real)a.gamma, (Real)a.invGm1, area, o, 1) && ok;
+      // first-order faces: the face states are the cell values
+      ok = face_slots<D, FLUX, Real>(L, R, (Real)a.gamma, (Real)a.invGm1, area, o, 1, L[kBx + D], R[kBx + D],
+                                     L[kUx + D], R[kUx + D]) && ok;
 #pragma unroll
       for (int m = 0; m < 9; m++) sum[m] = sum[m] + (double)o[m];
       bnL = bnL + (double)L[kBx + D] * 0.25;
@@ -163,6 +165,7 @@ static cudaError_t rc_launch(int flux, const StageArgs &a, const RcSlab *slabs, 
   switch (flux) {
     case kFluxRusanov: k_rc_flux<N, TileT, Real, kFluxRusanov><<<nSlab, N * N, 0, st>>>(a, slabs, fluxBuf); break;
     case kFluxLinde: k_rc_flux<N, TileT, Real, kFluxLinde><<<nSlab, N * N, 0, st>>>(a, slabs, fluxBuf); break;
+    case kFluxRoe: k_rc_flux<N, TileT, Real, kFluxRoe><<<nSlab, N * N, 0, st>>>(a, slabs, fluxBuf); break;
     default: k_rc_flux<N, TileT, Real, kFluxHlld><<<nSlab, N * N, 0, st>>>(a, slabs, fluxBuf); break;
   }
   return cudaGetLastError();

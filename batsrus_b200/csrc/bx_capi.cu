@@ -296,7 +296,7 @@ void free_all() {
 int check_scheme(const bx_scheme_params *s) {
   if (s->nOrder != 1 && s->nOrder != 2) return fail(BX_ERR_ARG, "nOrder=%d not supported", s->nOrder);
   if (s->nStage != 1 && s->nStage != 2) return fail(BX_ERR_ARG, "nStage=%d not supported", s->nStage);
-  if (s->TypeFlux < 0 || s->TypeFlux > 2) return fail(BX_ERR_ARG, "TypeFlux=%d unknown", s->TypeFlux);
+  if (s->TypeFlux < 0 || s->TypeFlux > 3) return fail(BX_ERR_ARG, "TypeFlux=%d unknown", s->TypeFlux);
   if (s->TypeLimiter < 0 || s->TypeLimiter > 2) return fail(BX_ERR_ARG, "TypeLimiter=%d unknown", s->TypeLimiter);
   if (s->Gamma <= 1.0) return fail(BX_ERR_ARG, "Gamma must exceed 1");
   if (s->Cfl <= 0.0) return fail(BX_ERR_ARG, "Cfl must be positive");
@@ -491,6 +491,7 @@ int compat_phase(int phase, int iBlock) {
   NEED_READY();
   if (g.nSlab) return fail(BX_ERR_ARG, "the per-block entry points work on single-level grids");
   if (iBlock < 1 || iBlock > g.nBlock) return fail(BX_ERR_ARG, "iBlock=%d out of range 1..%d", iBlock, g.nBlock);
+  if (g.sch.TypeFlux == BX_FLUX_ROE) return fail(BX_ERR_ARG, "the per-block entry points have no Roe flux");
   int r = ensure_compat();
   if (r) return r;
   cudaError_t e = launch_compat(g.shape, g.sch.TypeFlux, phase, iBlock - 1, compat_args(), g.st);
@@ -565,6 +566,8 @@ int bx_init(const bx_grid_desc *gd, const bx_scheme_params *sp) {
   if (shape < 0)
     return fail(BX_ERR_ARG, "block size %dx%dx%d in %dD not supported", gd->nI, gd->nJ, gd->nK, gd->nDim);
   if (gd->nBlock < 1 || !gd->iLevelCoord_IB) return fail(BX_ERR_ARG, "empty block list");
+  if (sp->TypeFlux == BX_FLUX_ROE && shape != kShape888 && shape != kShape444)
+    return fail(BX_ERR_ARG, "the Roe flux is built for 3D blocks of 8^3 or 4^3 cells");
   g.shape = shape;
   g.nDim = gd->nDim; g.nI = gd->nI; g.nJ = gd->nJ; g.nK = gd->nK;
   g.nBlock = gd->nBlock; g.nCell = (long)gd->nI * gd->nJ * gd->nK;

@@ -16,7 +16,7 @@
 namespace bx {
 
 enum { kRho = 0, kUx = 1, kUy = 2, kUz = 3, kBx = 4, kBy = 5, kBz = 6, kP = 7, kE = 7 };
-enum { kFluxRusanov = 0, kFluxLinde = 1, kFluxHlld = 2 };
+enum { kFluxRusanov = 0, kFluxLinde = 1, kFluxHlld = 2, kFluxRoe = 3 };
 enum { kLimMinmod = 0, kLimMc = 1, kLimMc3 = 2 };
 
 template <typename R>
@@ -418,6 +418,201 @@ __device__ __forceinline__ R flux_lean(R (&L)[8], R (&Rt)[8], R gamma, R invGm1,
     out[7 * ostride] = area * f;
   }
   return area * cmax;
+}
+
+// ---------------------------------------------------------------------------
+// Roe flux (TypeFlux = 'Roe', roe_solver_new, src/ModFaceFlux.f90:2490-2500)
+// for a Cartesian face normal to D with B0 = 0, Climit < 0 and no body faces.
+//
+// L, Rt: the face primitives after the RS7 change (src/ModFaceFlux.f90:
+// 600-625), whose normal field is that of the cell on each side; uLn, uRn:
+// the normal velocity of those cells; dBnL, dBnR: the face-minus-cell normal
+// field the change removed.  The dissipation is get_dissipation_flux_mhd
+// (src/ModCharacteristic.f90:451-516): the 7-wave decomposition of the
+// jump about the Roe-type average (decompose_state, :96-413), absolute
+// eigenvalues with the entropy fix of get_fixed_abs_eigenvalue (:416-448),
+// and the div B wave carried with the cell velocities.  Then the jump of the
+// normal field is split between the two states (:2302-2320), and both
+// physical fluxes get the DiffBb terms of modify_flux (:2477-2488).
+//
+// The products keep the reference's association; eigenvector entries that
+// are zero for an axis normal are left out, which does not change the sums.
+// Writes the 8 fluxes times area to out[v*ostride] (7: energy) and returns
+// Vdt = Cmax*area.
+
+// get_characteristic_speeds (src/ModCharacteristic.f90:387-410): A comes in
+// as the squared sound speed and leaves as the sound speed
+template <typename R>
+__device__ __forceinline__ void char_speeds(R &A, R rhoInv, R rhoSqrt, R bn, R bt0, R bt1, R &btang2, R &cs,
+                                            R &ca, R &cf) {
+  A = sqrt(A);
+  btang2 = bt0 * bt0 + bt1 * bt1;
+  const R tmp = btang2 * rhoInv;
+  ca = fabs(bn) / rhoSqrt;
+  cf = R(0.5) * (sqrt((A - ca) * (A - ca) + tmp) + sqrt((A + ca) * (A + ca) + tmp));
+  cs = ca * A / cf;
+}
+
+template <int D, typename R>
+__device__ __forceinline__ R roe_flux(R (&L)[8], R (&Rt)[8], R uLn, R uRn, R dBnL, R dBnR, R gamma, R invGm1,
+                                      R area, R *out, int ostride) {
+  constexpr int T0 = D == 0 ? 1 : 0, T1 = D == 2 ? 1 : 2;  // tangential axes, T0 < T1
+  constexpr int bn = kBx + D, un = kUx + D;
+  const R gm1 = gamma - R(1);
+  const R tol2 = R(1e-10) * R(1e-10);  // ModNumConst::cTolerance squared
+  R dS[8];
+#pragma unroll
+  for (int v = 0; v < 8; v++) dS[v] = L[v] - Rt[v];
+  const R rhoInvL = R(1) / L[kRho];
+  R aL = gamma * L[kP] * rhoInvL;
+  const R rhoInvR = R(1) / Rt[kRho];
+  R aR = gamma * Rt[kP] * rhoInvR;
+  const R sqL = sqrt(L[kRho]), sqR = sqrt(Rt[kRho]);
+  const R rhoH = sqL * sqR, rhoInvH = R(1) / rhoH, sqH = sqrt(rhoH);
+  const R wInv = R(1) / (sqL + sqR);
+  R uH[3], b1H[3];
+#pragma unroll
+  for (int m = 0; m < 3; m++) uH[m] = wInv * (sqL * L[kUx + m] + sqR * Rt[kUx + m]);
+  const R bnL = L[bn], bnR = Rt[bn];
+  b1H[T0] = wInv * (sqL * Rt[kBx + T0] + sqR * L[kBx + T0]);
+  b1H[T1] = wInv * (sqL * Rt[kBx + T1] + sqR * L[kBx + T1]);
+  b1H[D] = R(0.5) * (bnL + bnR);
+  const R dbn = bnR - bnL;
+  const R xnH = R(0.25) * rhoInvH * (dbn * dbn);
+  const R dt0 = L[kBx + T0] - Rt[kBx + T0], dt1 = L[kBx + T1] - Rt[kBx + T1];
+  const R xH = R(0.5) * (wInv * wInv) * (dt0 * dt0 + dt1 * dt1);
+  const R du2 = dS[kUx] * dS[kUx] + dS[kUy] * dS[kUy] + dS[kUz] * dS[kUz];
+  R aH = wInv * (sqL * aL + sqR * aR) + gamma * xH + gm1 * (xnH + R(0.5) * du2 * rhoH * (wInv * wInv));
+  const R bnH = b1H[D];
+  R bt2H, csH, caH, cfH;
+  char_speeds(aH, rhoInvH, sqH, bnH, b1H[T0], b1H[T1], bt2H, csH, caH, cfH);
+  const R sgn = copysign(R(1), bnH);
+  R alphaF, alphaS;
+  const R tmp = cfH * cfH - csH * csH;
+  if (tmp > tol2) {
+    alphaF = sqrt(fmax(R(0), (aH * aH - csH * csH) / tmp));
+    alphaS = sqrt(fmax(R(0), (cfH * cfH - aH * aH) / tmp));
+  } else if (bnH * bnH * rhoInvH <= aH * aH) {
+    alphaF = R(1); alphaS = R(0);
+  } else {
+    alphaF = R(0); alphaS = R(1);
+  }
+  // Tangent1 along the averaged tangential field, Tangent2 = e_D x Tangent1
+  // (generate_tangent12, :31-49, where that field vanishes)
+  R t1[3] = {R(0), R(0), R(0)}, t2[3] = {R(0), R(0), R(0)};
+  if (bt2H < tol2) {
+    if (D == 0) { t1[2] = R(-1); t2[1] = R(1); }
+    else if (D == 1) { t1[2] = R(1); t2[0] = R(1); }
+    else { t1[1] = R(-1); t2[0] = R(1); }
+  } else {
+    const R sq = sqrt(bt2H);
+    t1[T0] = b1H[T0] / sq;
+    t1[T1] = b1H[T1] / sq;
+    t2[(D + 1) % 3] = -t1[(D + 2) % 3];
+    t2[(D + 2) % 3] = t1[(D + 1) % 3];
+  }
+  const R dRho = dS[kRho];
+  const R dUnRho = dS[un] * rhoH;
+  const R dUt1Rho = (t1[T0] * dS[kUx + T0] + t1[T1] * dS[kUx + T1]) * rhoH;
+  const R dUt2Rho = (t2[T0] * dS[kUx + T0] + t2[T1] * dS[kUx + T1]) * rhoH;
+  const R dBn = dS[bn];
+  const R dBt1 = t1[T0] * dS[kBx + T0] + t1[T1] * dS[kBx + T1];
+  const R dBt2 = t2[T0] * dS[kBx + T0] + t2[T1] * dS[kBx + T1];
+  const R dP = dS[kP] + xH * dRho;
+  // wave amplitudes: entropy, Alfven+, Alfven-, slow+, fast+, slow-, fast-
+  const R normCoef = R(0.5) / (rhoH * aH * aH);
+  const R sa = sgn * sqH * aH;
+  R dw[7];
+  dw[0] = dRho * rhoInvH - dP * R(2) * normCoef;
+  dw[1] = normCoef * (-aH * dUt2Rho + sa * dBt2);
+  dw[2] = normCoef * (aH * dUt2Rho + sa * dBt2);
+  dw[3] = normCoef * (alphaS * (dP + csH * dUnRho) + alphaF * (cfH * dUt1Rho * sgn - sqH * aH * dBt1));
+  dw[4] = normCoef * (alphaF * (dP + cfH * dUnRho) + alphaS * (-csH * dUt1Rho * sgn + sqH * aH * dBt1));
+  dw[5] = normCoef * (alphaS * (dP - csH * dUnRho) + alphaF * (-cfH * dUt1Rho * sgn - sqH * aH * dBt1));
+  dw[6] = normCoef * (alphaF * (dP - cfH * dUnRho) + alphaS * (csH * dUt1Rho * sgn + sqH * aH * dBt1));
+  // absolute eigenvalues; the left and right speeds use the averaged Bn
+  R bt2, csL, caL, cfL, csR, caR, cfR;
+  char_speeds(aL, rhoInvL, sqL, bnH, L[kBx + T0], L[kBx + T1], bt2, csL, caL, cfL);
+  char_speeds(aR, rhoInvR, sqR, bnH, Rt[kBx + T0], Rt[kBx + T1], bt2, csR, caR, cfR);
+  const R u0 = uH[D], uL0 = L[un], uR0 = Rt[un];
+  const R eps0 = fmax(R(0), fabs((u0 + cfH) - (u0 - cfH)) * R(0.05));
+  auto fixed = [eps0](R lam, R lamL, R lamR) { return fmax(fabs(lam), fmax(fmax(lamR - lam, lam - lamL), eps0)); };
+  R fx[7];
+  fx[0] = fixed(u0, uL0, uR0);
+  fx[1] = fixed(u0 + caH, uL0 + caL, uR0 + caR);
+  fx[2] = fixed(u0 - caH, uL0 - caL, uR0 - caR);
+  fx[3] = fixed(u0 + csH, uL0 + csL, uR0 + csR);
+  fx[4] = fixed(u0 + cfH, uL0 + cfL, uR0 + cfR);
+  fx[5] = fixed(u0 - csH, uL0 - csL, uR0 - csR);
+  fx[6] = fixed(u0 - cfH, uL0 - cfL, uR0 - cfR);
+  R cmax = fmax(fx[4], fx[6]);
+  const R fx7 = fmax(fabs(uLn), fabs(uRn));
+  cmax = fmax(cmax, fx7);
+  // sum over the waves of eigenvector * |eigenvalue| * amplitude
+  const R aS = alphaS * csH, aF = alphaF * cfH;
+  const R pS = rhoH * alphaS * (aH * aH), pF = rhoH * alphaF * (aH * aH);
+  R pc0 = rhoH * fx[0] * dw[0];
+  pc0 = pc0 + rhoH * alphaS * fx[3] * dw[3];
+  pc0 = pc0 + rhoH * alphaF * fx[4] * dw[4];
+  pc0 = pc0 + rhoH * alphaS * fx[5] * dw[5];
+  pc0 = pc0 + rhoH * alphaF * fx[6] * dw[6];
+  R pcP = pS * fx[3] * dw[3];
+  pcP = pcP + pF * fx[4] * dw[4];
+  pcP = pcP + pS * fx[5] * dw[5];
+  pcP = pcP + pF * fx[6] * dw[6];
+  R pcM[3], pcB[3];
+#pragma unroll
+  for (int m = 0; m < 3; m++) {
+    if (m == D) {
+      R x = rhoH * aS * fx[3] * dw[3];
+      x = x + rhoH * aF * fx[4] * dw[4];
+      x = x + rhoH * (-aS) * fx[5] * dw[5];
+      x = x + rhoH * (-aF) * fx[6] * dw[6];
+      pcM[m] = x;
+      pcB[m] = uLn * dBnR + uRn * dBnL + fx7 * (dBn + dBnL - dBnR);
+    } else {
+      R x = -rhoH * aH * t2[m] * fx[1] * dw[1];
+      x = x + rhoH * aH * t2[m] * fx[2] * dw[2];
+      x = x + rhoH * (aF * sgn * t1[m]) * fx[3] * dw[3];
+      x = x + rhoH * (-(alphaS * csH * sgn * t1[m])) * fx[4] * dw[4];
+      x = x + rhoH * (-(aF * sgn * t1[m])) * fx[5] * dw[5];
+      x = x + rhoH * (alphaS * csH * sgn * t1[m]) * fx[6] * dw[6];
+      pcM[m] = x;
+      R y = sa * t2[m] * fx[1] * dw[1];
+      y = y + sa * t2[m] * fx[2] * dw[2];
+      y = y + -sqH * alphaF * aH * t1[m] * fx[3] * dw[3];
+      y = y + sqH * alphaS * aH * t1[m] * fx[4] * dw[4];
+      y = y + -sqH * alphaF * aH * t1[m] * fx[5] * dw[5];
+      y = y + sqH * alphaS * aH * t1[m] * fx[6] * dw[6];
+      pcB[m] = y;
+    }
+  }
+  // flux_from_pseudochar (:70-93), halved
+  R diss[8];
+  diss[kRho] = R(0.5) * pc0;
+#pragma unroll
+  for (int m = 0; m < 3; m++) {
+    diss[kUx + m] = R(0.5) * (pcM[m] + pc0 * uH[m]);
+    diss[kBx + m] = R(0.5) * pcB[m];
+  }
+  diss[kE] = R(0.5) * (pcP * invGm1 + (pcM[0] * uH[0] + pcM[1] * uH[1] + pcM[2] * uH[2]) +
+                       (pcB[0] * b1H[0] + pcB[1] * b1H[1] + pcB[2] * b1H[2]) +
+                       pc0 * (R(0.5) * (uH[0] * uH[0] + uH[1] * uH[1] + uH[2] * uH[2]) + (R(1) - invGm1) * xH));
+  // the jump of the normal field split between the states, DiffBb terms
+  const R dBnJ = R(0.5) * (Rt[bn] - L[bn]);
+  L[bn] = L[bn] + dBnJ;
+  Rt[bn] = Rt[bn] - dBnJ;
+  const R diffBb = dBnJ * dBnJ;
+  R UL[8], FL[8], UR[8], FR[8], unL, unR;
+  physical_flux<D>(L, invGm1, UL, FL, unL);
+  physical_flux<D>(Rt, invGm1, UR, FR, unR);
+  FL[un] = FL[un] + R(0.5) * diffBb;
+  FL[kE] = FL[kE] + unL * diffBb;
+  FR[un] = FR[un] + R(0.5) * diffBb;
+  FR[kE] = FR[kE] + unR * diffBb;
+#pragma unroll
+  for (int v = 0; v < 8; v++) out[v * ostride] = (R(0.5) * (FL[v] + FR[v]) + diss[v]) * area;
+  return cmax * area;
 }
 
 }  // namespace bx

@@ -153,10 +153,22 @@ __device__ __forceinline__ int face_id(int i, int j, int k) {
 
 // the ten face slots of one face from its left and right primitive states:
 // fluxes times area (0..7), Vdt (8), BnL + BnR (9); false where hlld_flux
-// stops
+// stops.  cbL, cbR, cuL, cuR: the normal field and normal velocity of the
+// cells either side, used by the Roe flux, whose RS7 change gives each face
+// state its cell's normal field before the div B slot is formed
+// (src/ModFaceFlux.f90:600-625)
 template <int D, int FLUX, typename Real>
 __device__ __forceinline__ bool face_slots(Real (&L)[8], Real (&R)[8], Real gamma, Real invGm1, Real area,
-                                           Real *out, int stride) {
+                                           Real *out, int stride, Real cbL, Real cbR, Real cuL, Real cuR) {
+  if (FLUX == kFluxRoe) {
+    const Real dBnR = R[kBx + D] - cbR;
+    R[kBx + D] = R[kBx + D] - dBnR;
+    const Real dBnL = L[kBx + D] - cbL;
+    L[kBx + D] = L[kBx + D] - dBnL;
+    out[9 * stride] = L[kBx + D] + R[kBx + D];
+    out[8 * stride] = roe_flux<D>(L, R, cuL, cuR, dBnL, dBnR, gamma, invGm1, area, out, stride);
+    return true;
+  }
   out[9 * stride] = L[kBx + D] + R[kBx + D];
   if (FLUX == kFluxHlld) {
     Real F[8], v;
@@ -195,7 +207,7 @@ __device__ __forceinline__ void sweep3(const StageArgs &a, const BlockGeom &g, c
 #pragma unroll
     for (int m = 0; m < 4; m++)
       vs[m] = tile_index<T, TileT>(1, i - (D == 0) * (2 - m), j - (D == 1) * (2 - m), k - (D == 2) * (2 - m)) - idx[m];
-    Real L[8], R[8];
+    Real L[8], R[8], cbL = Real(0), cbR = Real(0), cuL = Real(0), cuR = Real(0);
     const Real beta = (Real)a.beta;
 #pragma unroll
     for (int v = 0; v < 8; v++) {
@@ -203,8 +215,12 @@ __device__ __forceinline__ void sweep3(const StageArgs &a, const BlockGeom &g, c
       const Real q2 = (Real)tile[idx[2] + v * vs[2]], q3 = (Real)tile[idx[3] + v * vs[3]];
       if (first) { L[v] = q1; R[v] = q2; }
       else limited_face_t<LIM>(beta, q0, q1, q2, q3, L[v], R[v]);
+      if (FLUX == kFluxRoe && v == kBx + D) { cbL = q1; cbR = q2; }
+      if (FLUX == kFluxRoe && v == kUx + D) { cuL = q1; cuR = q2; }
     }
-    if (!face_slots<D, FLUX, Real>(L, R, (Real)a.gamma, (Real)a.invGm1, (Real)g.area[D], fbuf + f, T::NF)) err = 1;
+    if (!face_slots<D, FLUX, Real>(L, R, (Real)a.gamma, (Real)a.invGm1, (Real)g.area[D], fbuf + f, T::NF, cbL,
+                                   cbR, cuL, cuR))
+      err = 1;
     if (side >= 0 && ((rcCoarse >> side) & 1)) {
       // apply_cons_flux: the summed fluxes of the finer faces
       const int t0 = D == 0 ? j : i, t1 = D == 2 ? j : k;

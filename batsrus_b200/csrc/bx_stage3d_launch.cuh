@@ -44,6 +44,7 @@ static cudaError_t launch_flux(int flux, const TmaMaps &maps, const StageArgs &a
     case kFluxRusanov: return launch_one<N, FPT, TileT, Real, OutT, kFluxRusanov>(maps, a, nSM, st);
     case kFluxLinde: return launch_one<N, FPT, TileT, Real, OutT, kFluxLinde>(maps, a, nSM, st);
     case kFluxHlld: return launch_one<N, FPT, TileT, Real, OutT, kFluxHlld>(maps, a, nSM, st);
+    case kFluxRoe: return launch_one<N, FPT, TileT, Real, OutT, kFluxRoe>(maps, a, nSM, st);
   }
   return cudaErrorInvalidValue;
 }

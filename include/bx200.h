@@ -44,7 +44,10 @@ enum {
 };
 
 /* TypeFlux (src/ModFaceFlux.f90:396-417) */
-enum { BX_FLUX_RUSANOV = 0, BX_FLUX_LINDE = 1, BX_FLUX_HLLD = 2 };
+enum { BX_FLUX_RUSANOV = 0, BX_FLUX_LINDE = 1, BX_FLUX_HLLD = 2,
+       /* 'Roe': roe_solver_new (src/ModFaceFlux.f90:2490) with the
+          7-wave solver of src/ModCharacteristic.f90; 3D blocks only */
+       BX_FLUX_ROE = 3 };
 /* TypeLimiter (src/ModFaceValue.f90:3689-3791) */
 enum { BX_LIM_MINMOD = 0, BX_LIM_MC = 1, BX_LIM_MC3 = 2 };
 /* outer boundary types (src/ModCellBoundary.f90) */

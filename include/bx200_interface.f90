@@ -16,7 +16,7 @@ module bx200_interface
   implicit none
 
   integer(c_int), parameter:: BX_FLUX_RUSANOV = 0, BX_FLUX_LINDE = 1, &
-       BX_FLUX_HLLD = 2
+       BX_FLUX_HLLD = 2, BX_FLUX_ROE = 3
   integer(c_int), parameter:: BX_LIM_MINMOD = 0, BX_LIM_MC = 1, BX_LIM_MC3 = 2
   integer(c_int), parameter:: BX_BC_FLOAT = 0, BX_BC_PERIODIC = 1
   integer(c_int), parameter:: BX_FP64 = 0, BX_FP32_BULK = 1

@@ -33,6 +33,9 @@ enum { Vdt_ = 9, Un_ = 10, nFaceValue = 11 };
 // share/Library ModNumConst::cTiny (library absent from the tree; the
 // published SWMF value 1e-6 is assumed, used only by the HLLD guards)
 const double cTiny = 1.0e-6;
+// ModNumConst::cTolerance (same library; the published value 1e-10 is
+// assumed), used only by the degenerate-case tests of the Roe solver
+const double cTolerance = 1.0e-10;
 
 inline double sign25(double x) { return std::copysign(0.25, x); }
 inline double min3(double a, double b, double c) { return std::min(std::min(a, b), c); }
@@ -688,9 +691,170 @@ struct Oracle {
     return 0;
   }
 
+  // get_dissipation_flux_mhd (src/ModCharacteristic.f90:451-516) with
+  // decompose_state (:96-413) and get_fixed_abs_eigenvalue (:416-448) for
+  // the Cartesian normal e_d, B0 = 0, Climit < 0 and no body faces.  L, R:
+  // the face primitives after the RS7 change; uLn, uRn: the normal velocity
+  // of the cells either side; dBnL, dBnR: DeltaBnL, DeltaBnR.  Diss holds
+  // the nVar dissipation fluxes and the energy one (DissipationFlux_V).
+  void roe_dissipation(const double *L, const double *R, int d, double uLn, double uRn, double dBnL,
+                       double dBnR, double *Diss, double &cMax, double &Un) const {
+    const int t0 = d == 0 ? 1 : 0, t1 = d == 2 ? 1 : 2;  // tangential axes, lo < hi
+    double dS[nVar];
+    for (int v = 0; v < nVar; v++) dS[v] = L[v] - R[v];
+    const double RhoL = L[Rho_], RhoInvL = 1.0 / RhoL;
+    double aL = c.gamma * L[P_] * RhoInvL;
+    const double RhoR = R[Rho_], RhoInvR = 1.0 / RhoR;
+    double aR = c.gamma * R[P_] * RhoInvR;
+    const double RhoSqrtL = std::sqrt(RhoL), RhoSqrtR = std::sqrt(RhoR);
+    const double RhoH = RhoSqrtL * RhoSqrtR, RhoInvH = 1.0 / RhoH, RhoSqrtH = std::sqrt(RhoH);
+    const double WeightInv = 1.0 / (RhoSqrtL + RhoSqrtR);
+    double UH[3], B1H[3], BLt[3] = {0, 0, 0}, BRt[3] = {0, 0, 0};
+    for (int m = 0; m < 3; m++) UH[m] = WeightInv * (RhoSqrtL * L[RhoUx_ + m] + RhoSqrtR * R[RhoUx_ + m]);
+    const double BnL = L[Bx_ + d], BnR = R[Bx_ + d];
+    // tangential parts of the face fields
+    BLt[t0] = L[Bx_ + t0]; BLt[t1] = L[Bx_ + t1];
+    BRt[t0] = R[Bx_ + t0]; BRt[t1] = R[Bx_ + t1];
+    B1H[t0] = WeightInv * (RhoSqrtL * BRt[t0] + RhoSqrtR * BLt[t0]);
+    B1H[t1] = WeightInv * (RhoSqrtL * BRt[t1] + RhoSqrtR * BLt[t1]);
+    B1H[d] = 0.5 * (BnL + BnR);
+    const double dBnLR = BnR - BnL;
+    const double XnH = 0.25 * RhoInvH * (dBnLR * dBnLR);
+    const double dt0 = BLt[t0] - BRt[t0], dt1 = BLt[t1] - BRt[t1];
+    const double XH = 0.5 * (WeightInv * WeightInv) * (dt0 * dt0 + dt1 * dt1);
+    const double du2 = dS[RhoUx_] * dS[RhoUx_] + dS[RhoUy_] * dS[RhoUy_] + dS[RhoUz_] * dS[RhoUz_];
+    double aH = WeightInv * (RhoSqrtL * aL + RhoSqrtR * aR) + c.gamma * XH +
+                GammaMinus1 * (XnH + 0.5 * du2 * RhoH * (WeightInv * WeightInv));
+    const double BnH = B1H[d];
+    const double BHt[3] = {d == 0 ? 0.0 : B1H[0], d == 1 ? 0.0 : B1H[1], d == 2 ? 0.0 : B1H[2]};
+    // get_characteristic_speeds (:387-410): A becomes the sound speed
+    auto speeds = [](double &A, double RhoInv, double RhoSqrt, double Bn, double bt0, double bt1, double &BTang2,
+                     double &Cs, double &Ca, double &Cf) {
+      A = std::sqrt(A);
+      BTang2 = bt0 * bt0 + bt1 * bt1;
+      const double Tmp = BTang2 * RhoInv;
+      Ca = std::fabs(Bn) / RhoSqrt;
+      Cf = 0.5 * (std::sqrt((A - Ca) * (A - Ca) + Tmp) + std::sqrt((A + Ca) * (A + Ca) + Tmp));
+      Cs = Ca * A / Cf;
+    };
+    double BTang2, CsH, CaH, CfH;
+    speeds(aH, RhoInvH, RhoSqrtH, BnH, BHt[t0], BHt[t1], BTang2, CsH, CaH, CfH);
+    const double SignBnH = std::copysign(1.0, BnH);
+    double AlphaF, AlphaS;
+    const double cTolerance2 = cTolerance * cTolerance;
+    double Tmp = CfH * CfH - CsH * CsH;
+    if (Tmp > cTolerance2) {
+      AlphaF = std::sqrt(std::max(0.0, (aH * aH - CsH * CsH) / Tmp));
+      AlphaS = std::sqrt(std::max(0.0, (CfH * CfH - aH * aH) / Tmp));
+    } else if (BnH * BnH * RhoInvH <= aH * aH) {
+      AlphaF = 1.0; AlphaS = 0.0;
+    } else {
+      AlphaF = 0.0; AlphaS = 1.0;
+    }
+    double T1[3] = {0, 0, 0}, T2[3] = {0, 0, 0};
+    if (BTang2 < cTolerance2) {
+      // generate_tangent12 (:31-49) for the axis normals
+      if (d == 0) { T1[2] = -1.0; T2[1] = 1.0; }
+      else if (d == 1) { T1[2] = 1.0; T2[0] = 1.0; }
+      else { T1[1] = -1.0; T2[0] = 1.0; }
+    } else {
+      const double s = std::sqrt(BTang2);
+      T1[t0] = BHt[t0] / s; T1[t1] = BHt[t1] / s;
+      // Normal x Tangent1 for the axis normal e_d
+      T2[(d + 1) % 3] = -T1[(d + 2) % 3];
+      T2[(d + 2) % 3] = T1[(d + 1) % 3];
+    }
+    auto dot_t = [&](const double *T, int off) { return T[t0] * dS[off + t0] + T[t1] * dS[off + t1]; };
+    const double dRho = dS[Rho_];
+    const double dUnRho = dS[RhoUx_ + d] * RhoH;
+    const double dUt1Rho = dot_t(T1, RhoUx_) * RhoH;
+    const double dUt2Rho = dot_t(T2, RhoUx_) * RhoH;
+    const double dBn = dS[Bx_ + d];
+    const double dBt1 = dot_t(T1, Bx_), dBt2 = dot_t(T2, Bx_);
+    const double dP = dS[P_] + XH * dRho;
+    // wave amplitudes and right eigenvectors (columns), waves 0..7 =
+    // entropy, Alfven+, Alfven-, slow+, fast+, slow-, fast-, div B
+    double DW[nVar], EV[nVar][nVar] = {};
+    const double NormCoef = 0.5 / (RhoH * aH * aH);
+    const double SA = SignBnH * RhoSqrtH * aH;
+    DW[0] = dRho * RhoInvH - dP * 2 * NormCoef;
+    EV[Rho_][0] = RhoH;
+    DW[1] = NormCoef * (-aH * dUt2Rho + SA * dBt2);
+    DW[2] = NormCoef * (aH * dUt2Rho + SA * dBt2);
+    for (int m = 0; m < 3; m++) {
+      EV[RhoUx_ + m][1] = -RhoH * aH * T2[m];
+      EV[Bx_ + m][1] = SA * T2[m];
+      EV[RhoUx_ + m][2] = RhoH * aH * T2[m];
+      EV[Bx_ + m][2] = SA * T2[m];
+    }
+    const double N[3] = {d == 0 ? 1.0 : 0.0, d == 1 ? 1.0 : 0.0, d == 2 ? 1.0 : 0.0};
+    DW[3] = NormCoef * (AlphaS * (dP + CsH * dUnRho) + AlphaF * (CfH * dUt1Rho * SignBnH - RhoSqrtH * aH * dBt1));
+    DW[4] = NormCoef * (AlphaF * (dP + CfH * dUnRho) + AlphaS * (-CsH * dUt1Rho * SignBnH + RhoSqrtH * aH * dBt1));
+    DW[5] = NormCoef * (AlphaS * (dP - CsH * dUnRho) + AlphaF * (-CfH * dUt1Rho * SignBnH - RhoSqrtH * aH * dBt1));
+    DW[6] = NormCoef * (AlphaF * (dP - CfH * dUnRho) + AlphaS * (CsH * dUt1Rho * SignBnH + RhoSqrtH * aH * dBt1));
+    EV[Rho_][3] = RhoH * AlphaS;
+    EV[Rho_][4] = RhoH * AlphaF;
+    EV[Rho_][5] = RhoH * AlphaS;
+    EV[Rho_][6] = RhoH * AlphaF;
+    for (int m = 0; m < 3; m++) {
+      EV[RhoUx_ + m][3] = RhoH * (AlphaS * CsH * N[m] + AlphaF * CfH * SignBnH * T1[m]);
+      EV[Bx_ + m][3] = -RhoSqrtH * AlphaF * aH * T1[m];
+      EV[RhoUx_ + m][4] = RhoH * (AlphaF * CfH * N[m] - AlphaS * CsH * SignBnH * T1[m]);
+      EV[Bx_ + m][4] = RhoSqrtH * AlphaS * aH * T1[m];
+      EV[RhoUx_ + m][5] = RhoH * (-AlphaS * CsH * N[m] - AlphaF * CfH * SignBnH * T1[m]);
+      EV[Bx_ + m][5] = -RhoSqrtH * AlphaF * aH * T1[m];
+      EV[RhoUx_ + m][6] = RhoH * (-AlphaF * CfH * N[m] + AlphaS * CsH * SignBnH * T1[m]);
+      EV[Bx_ + m][6] = RhoSqrtH * AlphaS * aH * T1[m];
+    }
+    EV[P_][3] = RhoH * AlphaS * (aH * aH);
+    EV[P_][4] = RhoH * AlphaF * (aH * aH);
+    EV[P_][5] = RhoH * AlphaS * (aH * aH);
+    EV[P_][6] = RhoH * AlphaF * (aH * aH);
+    DW[7] = dBn;
+    // eigenvalues of the averaged, left and right states (set_eigenvalues);
+    // the left and right speeds use the averaged normal field BnH
+    double CsL, CaL, CfL, CsR, CaR, CfR, bt2;
+    speeds(aL, RhoInvL, RhoSqrtL, BnH, BLt[t0], BLt[t1], bt2, CsL, CaL, CfL);
+    speeds(aR, RhoInvR, RhoSqrtR, BnH, BRt[t0], BRt[t1], bt2, CsR, CaR, CfR);
+    auto eig = [](double u, double Cs, double Ca, double Cf, double *E) {
+      E[0] = u; E[1] = u + Ca; E[2] = u - Ca; E[3] = u + Cs; E[4] = u + Cf; E[5] = u - Cs; E[6] = u - Cf;
+    };
+    double Ev[7], EvL[7], EvR[7], Fix[nVar];
+    eig(UH[d], CsH, CaH, CfH, Ev);
+    eig(L[RhoUx_ + d], CsL, CaL, CfL, EvL);
+    eig(R[RhoUx_ + d], CsR, CaR, CfR, EvR);
+    const double Eps0 = std::max(0.0, std::fabs(Ev[4] - Ev[6]) * 0.05);  // LambdaB0 = 0
+    for (int w = 0; w < 7; w++) {
+      const double Lambda = Ev[w];
+      const double Eps = std::max(std::max(EvR[w] - Lambda, Lambda - EvL[w]), Eps0);
+      Fix[w] = std::max(std::fabs(Lambda), Eps);
+    }
+    cMax = std::max(Fix[4], Fix[6]);
+    Fix[7] = std::max(std::fabs(uLn), std::fabs(uRn));
+    cMax = std::max(cMax, Fix[7]);
+    double FPC[nVar] = {0, 0, 0, 0, 0, 0, 0, 0};
+    for (int w = 0; w < 7; w++)
+      for (int v = 0; v < nVar; v++) FPC[v] = FPC[v] + EV[v][w] * Fix[w] * DW[w];
+    FPC[Bx_ + d] = FPC[Bx_ + d] + (uLn * dBnR + uRn * dBnL + Fix[7] * (DW[7] + dBnL - dBnR));
+    // flux_from_pseudochar (:70-93), halved
+    double F[nFlux];
+    for (int v = 0; v < nVar; v++) F[v] = FPC[v];
+    for (int m = 0; m < 3; m++) F[RhoUx_ + m] = FPC[RhoUx_ + m] + FPC[Rho_] * UH[m];
+    F[Energy_] = FPC[P_] * InvGammaMinus1 +
+                 (FPC[RhoUx_] * UH[0] + FPC[RhoUy_] * UH[1] + FPC[RhoUz_] * UH[2]) +
+                 (FPC[Bx_] * B1H[0] + FPC[By_] * B1H[1] + FPC[Bz_] * B1H[2]) +
+                 FPC[Rho_] * (0.5 * (UH[0] * UH[0] + UH[1] * UH[1] + UH[2] * UH[2]) + (1 - InvGammaMinus1) * XH);
+    F[P_] = FPC[P_] - XH * FPC[Rho_];
+    for (int v = 0; v < nFlux; v++) Diss[v] = 0.5 * F[v];
+    Un = UH[d];
+  }
+
   // get_numerical_flux (src/ModFaceFlux.f90:2130-2473) for one Cartesian
-  // face in direction d with the face Area; writes nFaceValue slots.
-  int numerical_flux(const double *Lin, const double *Rin, int d, double Area, double *Out) const {
+  // face in direction d with the face Area; writes nFaceValue slots.  rs7
+  // (Roe only): the cell normal velocities left and right, DeltaBnL and
+  // DeltaBnR of the RS7 change made by the caller.
+  int numerical_flux(const double *Lin, const double *Rin, int d, double Area, double *Out,
+                     const double *rs7 = nullptr) const {
     double L[nVar], R[nVar], S[nVar];
     for (int v = 0; v < nVar; v++) { L[v] = Lin[v]; R[v] = Rin[v]; }
     const bool UseLindeFix = c.typeFlux == ORA_FLUX_LINDE || c.typeFlux == ORA_FLUX_HLLD;
@@ -732,6 +896,23 @@ struct Oracle {
       for (int v = 0; v < nFlux; v++)
         Flux[v] = (WeightRight * FR[v] + WeightLeft * FL[v] - Diffusion * (ConsR[v] - ConsL[v]));
       Un = WeightRight * UnR + WeightLeft * UnL;
+    } else if (c.typeFlux == ORA_FLUX_ROE) {
+      // roe_solver_new (:2490-2500): the dissipation of the RS7 states, then
+      // the jump of Bn removed (:2302-2320) and modify_flux (:2477-2488)
+      double Diss[nFlux];
+      roe_dissipation(L, R, d, rs7[0], rs7[1], rs7[2], rs7[3], Diss, Cmax, Un);
+      const double dBn = 0.5 * (R[Bx_ + d] - L[Bx_ + d]);
+      L[Bx_ + d] = L[Bx_ + d] + dBn;
+      R[Bx_ + d] = R[Bx_ + d] - dBn;
+      const double DiffBb = dBn * dBn;
+      physical_flux(L, d, ConsL, FL, UnL);
+      physical_flux(R, d, ConsR, FR, UnR);
+      FL[RhoUx_ + d] = FL[RhoUx_ + d] + 0.5 * DiffBb;
+      FL[Energy_] = FL[Energy_] + UnL * DiffBb;
+      FR[RhoUx_ + d] = FR[RhoUx_ + d] + 0.5 * DiffBb;
+      FR[Energy_] = FR[Energy_] + UnR * DiffBb;
+      for (int v = 0; v < nFlux; v++) Flux[v] = 0.5 * (FL[v] + FR[v]) + Diss[v];
+      CmaxDt = Cmax;
     } else {
       if (hlld(L, R, d, Flux, Cmax, Un)) return 1;
       CmaxDt = Cmax;
@@ -754,9 +935,25 @@ struct Oracle {
     for (int d = 0; d < c.nDim; d++) {
       double Area = cellFace(b, d);
       long nf = (long)nFace[d][0] * nFace[d][1] * nFace[d][2];
-      for (long f = 0; f < nf; f++)
-        err |= numerical_flux(&s.Left[d][nVar * f], &s.Right[d][nVar * f], d, Area,
-                              &s.Flux[d][nFaceValue * f]);
+      for (long f = 0; f < nf; f++) {
+        double *L = &s.Left[d][nVar * f], *R = &s.Right[d][nVar * f];
+        double rs7[4];
+        if (c.typeFlux == ORA_FLUX_ROE) {
+          // UseRS7 (:600-625): the face normal field becomes that of the
+          // cell on each side, in the face arrays themselves, so the div B
+          // of the Powell source sees it too
+          const int i = (int)(f % nFace[d][0]) + 1, j = (int)(f / nFace[d][0] % nFace[d][1]) + 1;
+          const int k = (int)(f / ((long)nFace[d][0] * nFace[d][1])) + 1;
+          const double *PL = &s.Prim[nVar * cell(i - (d == 0), j - (d == 1), k - (d == 2))];
+          const double *PR = &s.Prim[nVar * cell(i, j, k)];
+          const double DeltaBnR = R[Bx_ + d] - PR[Bx_ + d];
+          R[Bx_ + d] = R[Bx_ + d] - DeltaBnR;
+          const double DeltaBnL = L[Bx_ + d] - PL[Bx_ + d];
+          L[Bx_ + d] = L[Bx_ + d] - DeltaBnL;
+          rs7[0] = PL[RhoUx_ + d]; rs7[1] = PR[RhoUx_ + d]; rs7[2] = DeltaBnL; rs7[3] = DeltaBnR;
+        }
+        err |= numerical_flux(L, R, d, Area, &s.Flux[d][nFaceValue * f], rs7);
+      }
     }
     (void)nCell;
     return err;

@@ -20,7 +20,7 @@ extern "C" {
 #endif
 
 /* flux / limiter selectors (same numbering as include/bx200.h) */
-enum { ORA_FLUX_RUSANOV = 0, ORA_FLUX_LINDE = 1, ORA_FLUX_HLLD = 2 };
+enum { ORA_FLUX_RUSANOV = 0, ORA_FLUX_LINDE = 1, ORA_FLUX_HLLD = 2, ORA_FLUX_ROE = 3 };
 enum { ORA_LIM_MINMOD = 0, ORA_LIM_MC = 1, ORA_LIM_MC3 = 2 };
 enum { ORA_BC_FLOAT = 0, ORA_BC_PERIODIC = 1 };
 

@@ -15,7 +15,7 @@ import numpy as np
 _HERE = os.path.dirname(os.path.abspath(__file__))
 _LIB = os.path.join(_HERE, "_build", "liboracle.so")
 
-FLUX = {"rusanov": 0, "linde": 1, "hlld": 2}
+FLUX = {"rusanov": 0, "linde": 1, "hlld": 2, "roe": 3}
 LIMITER = {"minmod": 0, "mc": 1, "mc3": 2, "koren": 2, "no": 0}
 BC = {"float": 0, "periodic": 1}
 

@@ -52,7 +52,7 @@ def test_neighbor_tables_bit_exact():
     assert np.array_equal(j.reshape(-1, 6, 4), jb + 1)
 
 
-@pytest.mark.parametrize("flux,limiter", [("Rusanov", "mc"), ("Linde", "mc3"), ("HLLD", "mc")])
+@pytest.mark.parametrize("flux,limiter", [("Rusanov", "mc"), ("Linde", "mc3"), ("HLLD", "mc"), ("Roe", "mc3")])
 def test_amr_fp64_steps_match_oracle(flux, limiter):
     g = grid(2, 2)
     s = scheme(flux, limiter)

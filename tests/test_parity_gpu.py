@@ -75,6 +75,9 @@ CASES = [
     ("Rusanov", "mc", 1.5, "pert"),
     ("HLLD", "mc", 1.5, "blast"),
     ("HLLD", "mc3", 1.2, "ot"),
+    ("Roe", "mc3", 1.5, "ot"),
+    ("Roe", "minmod", 1.0, "blast"),
+    ("Roe", "mc", 1.5, "pert"),
 ]
 
 
