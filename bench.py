@@ -153,7 +153,7 @@ def run_ours(args):
     out = {}
     st = None
     for prec in args.precisions.split(","):
-        g, s, st0, _ = configs.orszag_tang_3d(nRoot=args.nroot, precision=prec,
+        g, s, st0, _ = configs.orszag_tang_3d(nRoot=args.nroot, precision=prec, flux=args.flux,
                                               with_state=st is None)
         st = st0 if st is None else st
         nCell = g.nCell
@@ -522,7 +522,7 @@ def cpu_baseline(args, seconds=12.0):
     from batsrus_b200 import configs
     from oracle import Oracle
     cores = os.cpu_count()
-    g, s, st, _ = configs.orszag_tang_3d(nRoot=8)
+    g, s, st, _ = configs.orszag_tang_3d(nRoot=8, flux=args.flux)
     o = Oracle(g, s, n_thread=cores)
     o.set_state(st)
     o.exchange_messages()
@@ -535,7 +535,7 @@ def cpu_baseline(args, seconds=12.0):
         if el > seconds or n >= 40:
             break
     return {"value": g.nCell * n / el, "unit": UNIT, "cores": cores, "kind": "port",
-            "sample": "oracle/ C++ restatement, 64^3 Orszag-Tang (512 blocks of 8^3), Linde+Koren, "
+            "sample": "oracle/ C++ restatement, 64^3 Orszag-Tang (512 blocks of 8^3), " + args.flux + "+Koren, "
                       "FP64, %d full steps in %.1f s on %d threads" % (n, el, cores)}
 
 
@@ -547,7 +547,7 @@ def run_reference(args):
     from batsrus_b200 import configs
     from oracle import Oracle
     cores = os.cpu_count()
-    g, s, st, _ = configs.orszag_tang_3d(nRoot=8)
+    g, s, st, _ = configs.orszag_tang_3d(nRoot=8, flux=args.flux)
     o = Oracle(g, s, n_thread=cores)
     o.set_state(st)
     o.exchange_messages()
@@ -560,7 +560,9 @@ def run_reference(args):
             "warmup": args.warmup, "ms_per_step": el * 1e3 / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "impl": "reference",
-            "config": {"workload": WORKLOAD, "sample": "64^3 of the 256^3 domain per step",
+            "config": {"workload": WORKLOAD if args.flux == "Linde" else
+                       "orszag_tang_3d_256cubed_%s_koren" % args.flux.lower(),
+                       "sample": "64^3 of the 256^3 domain per step",
                        "blocks": "8x8x8", "flux": "Linde", "limiter": "mc3 beta=1.2", "cfl": 0.8},
             "cpu_baseline": {"value": v, "unit": UNIT, "cores": cores, "kind": "port",
                              "sample": "oracle/ C++ restatement of the orig path, 64^3 Orszag-Tang, "
@@ -579,6 +581,8 @@ def main():
     ap.add_argument("--no-e2e", dest="e2e", action="store_false")
     ap.add_argument("--no-cpu", dest="cpu", action="store_false")
     ap.add_argument("--precisions", default="fp64,fp32")
+    ap.add_argument("--flux", default="Linde", choices=["Rusanov", "Linde", "HLLD", "Roe"],
+                    help="TypeFlux of the explicit Orszag-Tang workload (Linde is the headline)")
     ap.add_argument("--jfnk-precond", default="BILU,NONE,LEARNED", help="'' to skip the implicit workload")
     ap.add_argument("--learned-epochs", type=int, default=64)
     ap.add_argument("--learned-blend", type=float, default=0.6)
@@ -610,7 +614,9 @@ def main():
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": r64["ms_per_step"],
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic",
-            "config": {"workload": WORKLOAD, "cells": (8 * args.nroot) ** 3, "blocks": args.nroot ** 3,
+            "config": {"workload": WORKLOAD if args.flux == "Linde" else
+                       "orszag_tang_3d_%dcubed_%s_koren" % (8 * args.nroot, args.flux.lower()),
+                       "cells": (8 * args.nroot) ** 3, "blocks": args.nroot ** 3,
                        "block_cells": "8x8x8", "flux": "Linde", "limiter": "mc3 beta=1.2", "cfl": 0.8,
                        "stages": 2, "l2": "inputs larger than L2 (state %.2f GB)" % ((8 * args.nroot) ** 3 * 64 / 1e9),
                        "parallelism": "one domain per GPU"},
