@@ -143,6 +143,8 @@ class SchemeParams(ctypes.Structure):
         ("UseDivbSource", ctypes.c_int), ("UseHalfStep", ctypes.c_int),
         ("UseDtFixed", ctypes.c_int), ("DtFixed", ctypes.c_double),
         ("Precision", ctypes.c_int),
+        ("RhoMin", ctypes.c_double), ("pMin", ctypes.c_double), ("TMin", ctypes.c_double),
+        ("MassIon", ctypes.c_double),
     ]
 
 
@@ -256,6 +258,10 @@ def scheme_params(s):
     p.UseDtFixed = int(s.useDtFixed)
     p.DtFixed = s.dtFixed
     p.Precision = PRECISION[s.precision.lower()]
+    p.RhoMin = getattr(s, "rhoMin", -1.0)
+    p.pMin = getattr(s, "pMin", -1.0)
+    p.TMin = getattr(s, "tMin", -1.0)
+    p.MassIon = getattr(s, "massIon", 1.0)
     return p
 
 

@@ -60,6 +60,7 @@ struct Ctx {
   double *dtBlock = nullptr;
   double *scrL[3] = {}, *scrR[3] = {}, *scrF[3] = {}, *scrSrc = nullptr, *scrDt = nullptr;
   std::vector<char> touched;
+  int *touchedDev = nullptr;  // device list of the blocks updated per block
   bool compatPending = false;
   int iStage = 1;
   cudaStream_t st = nullptr;
@@ -270,7 +271,7 @@ void free_all() {
     }
   if (g.nbr) cudaFree(g.nbr);
   if (g.order) cudaFree(g.order);
-  for (int **p : {&g.rcType, &g.rcSlab, &g.lcDev}) {
+  for (int **p : {&g.rcType, &g.rcSlab, &g.lcDev, &g.touchedDev}) {
     if (*p) cudaFree(*p);
     *p = nullptr;
   }
@@ -300,6 +301,7 @@ int check_scheme(const bx_scheme_params *s) {
   if (s->TypeLimiter < 0 || s->TypeLimiter > 2) return fail(BX_ERR_ARG, "TypeLimiter=%d unknown", s->TypeLimiter);
   if (s->Gamma <= 1.0) return fail(BX_ERR_ARG, "Gamma must exceed 1");
   if (s->Cfl <= 0.0) return fail(BX_ERR_ARG, "Cfl must be positive");
+  if (s->MassIon < 0.0) return fail(BX_ERR_ARG, "MassIon must not be negative");
   if (s->Precision == BX_FP32_BULK) {
     if (g.shape != kShape888 && g.shape != kShape444)
       return fail(BX_ERR_ARG, "FP32-bulk mode needs 3D 8x8x8 or 4x4x4 blocks");
@@ -310,6 +312,15 @@ int check_scheme(const bx_scheme_params *s) {
   return BX_OK;
 }
 
+Floors floors() {
+  Floors f;
+  f.rhoMin = g.sch.RhoMin;
+  f.pMin = g.sch.pMin;
+  f.tMin = g.sch.TMin;
+  f.massIon = g.sch.MassIon > 0.0 ? g.sch.MassIon : 1.0;
+  return f;
+}
+
 StageArgs stage_args(int iStage, bool computeDt) {
   StageArgs a;
   a.nbr = g.nbr; a.order = g.order; a.geom = g.geom; a.ts = g.ts; a.dtBlock = g.dtBlock;
@@ -318,6 +329,7 @@ StageArgs stage_args(int iStage, bool computeDt) {
   a.useDivb = g.sch.UseDivbSource; a.useHalfStep = g.sch.UseHalfStep; a.computeDt = computeDt;
   a.beta = g.sch.LimiterBeta; a.gamma = g.sch.Gamma; a.invGm1 = 1.0 / (g.sch.Gamma - 1.0);
   a.cfl = g.sch.Cfl;
+  a.fl = floors();
   a.old = g.A;
   if (g.nSlab) {
     a.rcType = g.rcType; a.rcSlab = g.rcSlab; a.rcGhost = g.rcGhost; a.rcFlux = g.rcFlux;
@@ -472,6 +484,7 @@ int ensure_compat() {
   }
   CK(cudaMalloc(&g.scrSrc, sizeof(double) * 9 * g.nCell));
   CK(cudaMalloc(&g.scrDt, sizeof(double) * g.nCell));
+  CK(cudaMalloc(&g.touchedDev, sizeof(int) * g.nBlock));
   g.touched.assign(g.nBlock, 0);
   return BX_OK;
 }
@@ -484,6 +497,7 @@ CompatArgs compat_args() {
   a.iStage = g.iStage; a.nStage = g.sch.nStage; a.nOrder = g.sch.nOrder; a.limiter = g.sch.TypeLimiter;
   a.useDivb = g.sch.UseDivbSource; a.useHalfStep = g.sch.UseHalfStep;
   a.beta = g.sch.LimiterBeta; a.gamma = g.sch.Gamma; a.invGm1 = 1.0 / (g.sch.Gamma - 1.0); a.cfl = g.sch.Cfl;
+  a.fl = floors();
   return a;
 }
 
@@ -876,13 +890,23 @@ int bx_get_time(double *t, double *dt, int *n) {
 }
 
 // ---- per-block entry points ----------------------------------------------
+// DoResChangeOnly: the prepass of advance_explicit over the faces next to a
+// finer block (src/ModAdvanceExplicit.f90:93-134).  A single-level grid has
+// no such faces, so the call has nothing to do; on a multi-level grid the
+// per-block path does not compute them, and the call fails like every other
+// per-block call there (the batched bx_update_state_fast covers AMR grids).
 int bx_calc_face_value(int iBlock, int DoResChangeOnly, int DoMonotoneRestrict) {
   (void)DoMonotoneRestrict;  // single-level grids have no restricted ghost cells
-  if (DoResChangeOnly) return BX_OK;  // no resolution-change faces on one level
+  if (DoResChangeOnly) {
+    NEED_READY();
+    if (g.nSlab) return fail(BX_ERR_ARG, "the per-block entry points work on single-level grids");
+    if (iBlock < 1 || iBlock > g.nBlock) return fail(BX_ERR_ARG, "iBlock=%d out of range 1..%d", iBlock, g.nBlock);
+    return BX_OK;
+  }
   return compat_phase(kPhaseFaceValue, iBlock);
 }
 int bx_calc_face_flux(int DoResChangeOnly, int iBlock) {
-  if (DoResChangeOnly) return BX_OK;
+  if (DoResChangeOnly) return bx_calc_face_value(iBlock, 1, 0);
   return compat_phase(kPhaseFaceFlux, iBlock);
 }
 int bx_calc_source(int iBlock) { return compat_phase(kPhaseSource, iBlock); }
@@ -942,13 +966,10 @@ int bx_exchange_messages(int DoResChangeOnly) {
     std::vector<int> list;
     for (int b = 0; b < g.nBlock; b++)
       if (g.touched[b]) list.push_back(b);
-    int *dl = nullptr;
-    CK(cudaMalloc(&dl, sizeof(int) * list.size()));
-    CK(cudaMemcpyAsync(dl, list.data(), sizeof(int) * list.size(), cudaMemcpyHostToDevice, g.st));
-    copy_blocks<<<592, 256, 0, g.st>>>(g.A, g.Nx, dl, (int)list.size(), 8 * g.nCell);
+    CK(cudaMemcpyAsync(g.touchedDev, list.data(), sizeof(int) * list.size(), cudaMemcpyHostToDevice, g.st));
+    copy_blocks<<<592, 256, 0, g.st>>>(g.A, g.Nx, g.touchedDev, (int)list.size(), 8 * g.nCell);
     CK(cudaGetLastError());
     CK(cudaStreamSynchronize(g.st));
-    cudaFree(dl);
     std::fill(g.touched.begin(), g.touched.end(), 0);
     g.compatPending = false;
   }

@@ -133,8 +133,9 @@ __global__ void compat_update(CompatArgs a, int b) {
   for (int c = threadIdx.x; c < S::NC; c += blockDim.x) {
     if (a.iStage == 1)
       for (int v = 0; v < 8; v++) O[v * S::NC + c] = U[v * S::NC + c];
-    if (DtNoCfl == 0.0) {
+    if (DtNoCfl == 0.0) {  // state unchanged, then limit_pressure
       for (int v = 0; v < 8; v++) N[v * S::NC + c] = U[v * S::NC + c];
+      N[kP * S::NC + c] = limit_pressure(U[c], U[kP * S::NC + c], a.fl.pMin, a.fl.tMin, a.fl.massIon);
       continue;
     }
     const int i = c % S::NI, j = (c / S::NI) % S::NJ, k = c / (S::NI * S::NJ);
@@ -156,8 +157,10 @@ __global__ void compat_update(CompatArgs a, int b) {
     e = e + 0.5 * (o[4] * o[4] + o[5] * o[5] + o[6] * o[6]);
     for (int v = 0; v < 7; v++) n[v] = o[v] + s[v];
     e = e + s[8];
+    if (a.fl.rhoMin > 0.0) n[0] = fmax(a.fl.rhoMin, n[0]);  // UseRhoMin
     const double p = e - 0.5 * (n[4] * n[4] + n[5] * n[5] + n[6] * n[6]);
     n[kP] = gm1 * (p - 0.5 * (n[1] * n[1] + n[2] * n[2] + n[3] * n[3]) / n[0]);
+    n[kP] = limit_pressure(n[0], n[kP], a.fl.pMin, a.fl.tMin, a.fl.massIon);
     for (int v = 0; v < 8; v++) N[v * S::NC + c] = n[v];
   }
 }

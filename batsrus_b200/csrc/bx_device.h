@@ -8,6 +8,10 @@ namespace bx {
 
 enum { kErrHlld = 1, kErrNonPhysical = 2, kErrTimeout = 4 };
 
+// SmallDouble of ModPartImplicit (src/ModPartImplicit.f90:34): a norm below
+// it is replaced by 1 (Norm_V :465, the matvec's rms(x) :1192)
+constexpr double kSmallDouble = 1.0e-30;
+
 // Time-step bookkeeping kept in device memory so that whole steps can be
 // captured in a CUDA graph (set_global_timestep, src/ModTimeStepControl.f90:
 // 306-524, runs on the device).
@@ -18,6 +22,13 @@ struct StepState {
   unsigned long long DtMinBits;   // running min of cell time steps (bits)
   int nStep;
   int errFlag;
+};
+
+// Floors of the updated state, each active where > 0: RhoMin_I (the
+// UseRhoMin clamp, src/ModUpdateState.f90:901-908), pMin_I and TMin_I of
+// limit_pressure (src/ModEnergy.f90:388-420) with NumDens = rho/MassIon
+struct Floors {
+  double rhoMin = 0.0, pMin = 0.0, tMin = 0.0, massIon = 1.0;
 };
 
 // per-block Cartesian geometry (BATL CellSize_DB, CellVolume_B,
@@ -58,6 +69,7 @@ struct StageArgs {
   const int *rcSlab = nullptr;
   const double *rcGhost = nullptr;
   const double *rcFlux = nullptr;
+  Floors fl;
 };
 
 constexpr int kNbrFloat = -1, kNbrResChange = -2;
@@ -77,6 +89,7 @@ struct CompatArgs {
   double *dtBlock;         // DtMax_B
   int iStage, nStage, nOrder, limiter, useDivb, useHalfStep;
   double beta, gamma, invGm1, cfl;
+  Floors fl;
 };
 
 // shape ids of the supported block sizes

@@ -6,6 +6,7 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include "bx_device.h"
 #include "bx_physics.cuh"
 
 namespace bx {
@@ -95,7 +96,7 @@ __global__ void k_perturb(double *__restrict__ Ueps, const double *__restrict__ 
                           const double *xx, const double *norm, double sqrtJacEps, long nCellBlock, long n,
                           double *epsOut) {
   double xn = sqrt(*xx / (double)n);
-  if (xn < 1e-300) xn = 1.0;
+  if (xn < kSmallDouble) xn = 1.0;
   const double eps = sqrtJacEps / xn;
   if (blockIdx.x == 0 && threadIdx.x == 0) *epsOut = eps;
   for (long q = blockIdx.x * (long)blockDim.x + threadIdx.x; q < n; q += (long)gridDim.x * blockDim.x) {

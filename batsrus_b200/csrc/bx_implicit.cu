@@ -269,7 +269,7 @@ int compute_norm() {
   CKI(cudaStreamSynchronize(c.st));
   for (int v = 0; v < 8; v++) {
     I.Norm[v] = std::sqrt(s[v] / (double)I.nCellTot);
-    if (I.Norm[v] < 1e-300) I.Norm[v] = 1.0;
+    if (I.Norm[v] < kSmallDouble) I.Norm[v] = 1.0;
   }
   CKI(cudaMemcpyAsync(I.dNorm, I.Norm, sizeof(I.Norm), cudaMemcpyHostToDevice, c.st));
   return BX_OK;

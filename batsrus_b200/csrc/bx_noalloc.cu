@@ -110,7 +110,7 @@ extern "C" int bx_impl_norm_noalloc(const double *Impl_dev, int nCellBlock, int 
   const double nCell = (double)nCellBlock * (double)nBlock;
   for (int v = 0; v < 8; v++) {
     Norm_V[v] = std::sqrt(s[v] / nCell);
-    if (Norm_V[v] < 1e-300) Norm_V[v] = 1.0;
+    if (Norm_V[v] < bx::kSmallDouble) Norm_V[v] = 1.0;
   }
   return BX_OK;
 }

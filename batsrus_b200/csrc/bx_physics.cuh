@@ -22,6 +22,15 @@ enum { kLimMinmod = 0, kLimMc = 1, kLimMc3 = 2 };
 template <typename R>
 __device__ __forceinline__ R sign25(R x) { return copysign(R(0.25), x); }
 
+// limit_pressure (src/ModEnergy.f90:388-420) for the single ion fluid: the
+// pressure floor pMin, then the temperature floor NumDens*TMin with
+// NumDens = rho/MassIon; a floor is active where it is > 0
+__device__ __forceinline__ double limit_pressure(double rho, double p, double pMin, double tMin, double massIon) {
+  if (pMin > 0.0) p = fmax(pMin, p);
+  if (tMin > 0.0) p = fmax(rho / massIon * tMin, p);
+  return p;
+}
+
 // limiter (src/ModFaceValue.f90:3689-3791) evaluated for one face from the
 // 4-cell stencil q0=P(i-2), q1=P(i-1), q2=P(i), q3=P(i+1):
 //   LeftState  = P(i-1) + dVarLimL(i-1)     (get_facex_second :2021-2027)

@@ -244,7 +244,8 @@ __global__ void __launch_bounds__(S::NTHREAD, 1) stage_kernel(StageArgs a) {
 #pragma unroll
     for (int v = 0; v < 8; v++) o[v] = old[v * S::NC + c];
     if (a.computeDt) dtmin = fmin(dtmin, V / acc[m].vdt);
-    if (DtNoCfl == 0.0) {  // IsTimeAccurate .and. Dt == 0: state unchanged
+    if (DtNoCfl == 0.0) {  // IsTimeAccurate .and. Dt == 0: state unchanged, floored
+      o[kP] = limit_pressure(o[kRho], o[kP], a.fl.pMin, a.fl.tMin, a.fl.massIon);
 #pragma unroll
       for (int v = 0; v < 8; v++) out[v * S::NC + c] = (OutT)o[v];
       continue;
@@ -272,9 +273,11 @@ __global__ void __launch_bounds__(S::NTHREAD, 1) stage_kernel(StageArgs a) {
 #pragma unroll
     for (int v = 0; v < 7; v++) n[v] = o[v] + s[v];
     e = e + s[kE];
-    // energy_to_pressure (src/ModEnergy.f90:243)
+    if (a.fl.rhoMin > 0.0) n[kRho] = fmax(a.fl.rhoMin, n[kRho]);  // UseRhoMin
+    // energy_to_pressure (src/ModEnergy.f90:243), then limit_pressure
     double p = e - 0.5 * (n[kBx] * n[kBx] + n[kBy] * n[kBy] + n[kBz] * n[kBz]);
     n[kP] = gm1 * (p - 0.5 * (n[kUx] * n[kUx] + n[kUy] * n[kUy] + n[kUz] * n[kUz]) / n[kRho]);
+    n[kP] = limit_pressure(n[kRho], n[kP], a.fl.pMin, a.fl.tMin, a.fl.massIon);
 #pragma unroll
     for (int v = 0; v < 8; v++) out[v * S::NC + c] = (OutT)n[v];
   }

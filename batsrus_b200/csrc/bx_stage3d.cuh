@@ -423,6 +423,9 @@ __global__ void __launch_bounds__(T::NTHR, 1)
           if (a.dtCellOut) a.dtCellOut[(size_t)b * T::NC + cc] = dtc;
         }
         if (DtNoCfl == 0.0) {
+          // update_state with Dt = 0: the state is unchanged, then
+          // limit_pressure (src/ModUpdateState.f90:169, 241)
+          o[kP] = limit_pressure(o[kRho], o[kP], a.fl.pMin, a.fl.tMin, a.fl.massIon);
 #pragma unroll
           for (int v = 0; v < 8; v++) out[v * T::NC + cc] = (OutT)o[v];
         } else {
@@ -443,8 +446,10 @@ __global__ void __launch_bounds__(T::NTHR, 1)
 #pragma unroll
           for (int v = 0; v < 7; v++) n[v] = o[v] + DtLocal * (src[v] + chg[r][v] * invV);
           e = e + DtLocal * (src[kE] + chg[r][kE] * invV);
+          if (a.fl.rhoMin > 0.0) n[kRho] = fmax(a.fl.rhoMin, n[kRho]);  // UseRhoMin
           const double p = e - 0.5 * (n[kBx] * n[kBx] + n[kBy] * n[kBy] + n[kBz] * n[kBz]);
           n[kP] = gm1 * (p - 0.5 * (n[kUx] * n[kUx] + n[kUy] * n[kUy] + n[kUz] * n[kUz]) / n[kRho]);
+          n[kP] = limit_pressure(n[kRho], n[kP], a.fl.pMin, a.fl.tMin, a.fl.massIon);
 #pragma unroll
           for (int v = 0; v < 8; v++) out[v * T::NC + cc] = (OutT)n[v];
         }

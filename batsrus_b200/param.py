@@ -91,6 +91,13 @@ class Scheme:
     isTimeAccurate: bool = True
     precision: str = "fp64"  # 'fp64' | 'fp32'
     useNonConservative: bool = False  # #NONCONSERVATIVE (oracle only; the GPU path solves for energy)
+    # floors (#MINIMUMDENSITY / #MINIMUMPRESSURE / #MINIMUMTEMPERATURE,
+    # normalized units), active where > 0 (RhoMinDim_I = pMinDim_I =
+    # TMinDim_I = -1 by default, src/ModPhysics.f90:170-172); massIon in amu
+    rhoMin: float = -1.0
+    pMin: float = -1.0
+    tMin: float = -1.0
+    massIon: float = 1.0
 
 
 @dataclass
@@ -129,6 +136,12 @@ def apply_commands(commands, scheme, nDim=3):
             scheme.gamma = float(v[0])
         elif name == "#DIVB":
             scheme.useDivbSource = bool(v[0])
+        elif name == "#MINIMUMDENSITY":  # src/ModSetParameters.f90:706-709
+            scheme.rhoMin = float(v[0])
+        elif name == "#MINIMUMPRESSURE":  # :711-714
+            scheme.pMin = float(v[0])
+        elif name == "#MINIMUMTEMPERATURE":  # :717-720
+            scheme.tMin = float(v[0])
         elif name == "#TIMEACCURATE":
             scheme.isTimeAccurate = bool(v[0])
         elif name == "#STOP":

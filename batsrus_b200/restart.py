@@ -20,6 +20,12 @@ A restart directory holds:
     markers: (DtMax_B, tSimulation), (CellSize_DB, Coord111_DB), and the
     state variable by variable: (State_VGB(iVar,1:nI,1:nJ,1:nK), iVar=1,nVar).
 
+  When the last step was implicit BDF2 (nStepPrev == nStep), the header has
+  ``#NPREVIOUS`` (nStepPrev, DtPrev, :457-461) and each block also carries
+  the previous step's state ImplOld_VCB: in ``one`` appended to the record
+  variable by variable (State8_CV, :1084-1091, read at :1002-1010), in
+  ``block`` as a fourth record (:828-829, read at :732-736).
+
 * ``octree_blocks.txt``: the block tree.  BATL writes ``octree.rst`` with
   ``write_tree_file`` (srcBATL, absent from the reference tree), whose
   layout cannot be restated.  This file is a plain text list instead: the
@@ -79,7 +85,7 @@ def block_geometry(grid):
     return cs, c111
 
 
-def _header(grid, tSimulation, nStep, typeRestart):
+def _header(grid, tSimulation, nStep, typeRestart, dtPrev=None):
     tab = "\t\t"
     L = []
 
@@ -103,6 +109,8 @@ def _header(grid, tSimulation, nStep, typeRestart):
     cmd("#NEWRESTART", (False, "DoRestartBFace"))
     cmd("#RESTARTINFILE", (typeRestart, "StringRestartInFile"))
     cmd("#NSTEP", (int(nStep), "nStep"))
+    if dtPrev is not None:
+        cmd("#NPREVIOUS", (int(nStep), "nPrev"), (float(dtPrev), "DtPrev"))
     cmd("#TIMESIMULATION", (float(tSimulation), "tSimulation"))
     cmd("#GRID", (int(grid.nRoot[0]), "nRootBlock1"), (int(grid.nRoot[1]), "nRootBlock2"),
         (int(grid.nRoot[2]), "nRootBlock3"),
@@ -114,9 +122,14 @@ def _header(grid, tSimulation, nStep, typeRestart):
     return "\n".join(L) + "\n"
 
 
-def write_restart_arrays(dirname, grid, State_VGB, tSimulation, nStep, DtMax_B, typeRestart="one"):
+def write_restart_arrays(dirname, grid, State_VGB, tSimulation, nStep, DtMax_B, typeRestart="one",
+                         ImplOld=None, DtPrev=None):
     """Write a restart directory from host arrays (State_VGB in the
-    reference layout, shape grid.state_shape_fortran())."""
+    reference layout, shape grid.state_shape_fortran()).  ImplOld (nBlock,
+    nK, nJ, nI, nVar) and DtPrev, given together, are the previous BDF2 step
+    (#NPREVIOUS with nStepPrev = nStep)."""
+    if (ImplOld is None) != (DtPrev is None):
+        raise ValueError("ImplOld and DtPrev go together")
     if typeRestart not in ("one", "block"):
         raise ValueError("TypeRestartOutFile %r: 'one' and 'block' are written" % typeRestart)
     os.makedirs(dirname, exist_ok=True)
@@ -126,7 +139,7 @@ def write_restart_arrays(dirname, grid, State_VGB, tSimulation, nStep, DtMax_B, 
     order = morton_order(grid)
     dtB = np.asarray(DtMax_B, dtype=np.float64)
     with open(os.path.join(dirname, NAME_HEADER), "w") as f:
-        f.write(_header(grid, tSimulation, nStep, typeRestart))
+        f.write(_header(grid, tSimulation, nStep, typeRestart, DtPrev))
     with open(os.path.join(dirname, NAME_TREE), "w") as f:
         f.write("%d %d %d %d\n" % (grid.nDim, grid.nI, grid.nJ, grid.nK))
         f.write(" ".join(grid.typeBc) + "\n")
@@ -134,23 +147,32 @@ def write_restart_arrays(dirname, grid, State_VGB, tSimulation, nStep, DtMax_B, 
         for c in grid.iLevelCoord.tolist():
             f.write("%d %d %d %d\n" % tuple(c))
     nCellVar = NVAR * grid.nI * grid.nJ * grid.nK
+    prev = None
+    if ImplOld is not None:
+        prev = np.asarray(ImplOld, dtype=np.float64).reshape(grid.nBlock, grid.nK, grid.nJ, grid.nI, NVAR)
+    nExtra = 0 if prev is None else nCellVar
     if typeRestart == "one":
-        rec = np.empty((grid.nBlock, 7 + nCellVar))
+        rec = np.empty((grid.nBlock, 7 + nCellVar + nExtra))
         for b in range(grid.nBlock):
             r = order[b] - 1
             rec[r, 0] = dtB[b]
             rec[r, 1:4] = cs[b]
             rec[r, 4:7] = c111[b]
             # (nVar, nI, nJ, nK) with the variable fastest = [k][j][i][v] in C order
-            rec[r, 7:] = inner[b].reshape(-1)
+            rec[r, 7:7 + nCellVar] = inner[b].reshape(-1)
+            if prev is not None:  # State8_CV: the variable slowest
+                rec[r, 7 + nCellVar:] = np.moveaxis(prev[b], -1, 0).reshape(-1)
         rec.tofile(os.path.join(dirname, NAME_DATA))
         return
     for b in range(grid.nBlock):
         nd = max(5, int(1 + np.log10(float(order[b]))))
         name = os.path.join(dirname, "blk%0*d.rst" % (nd, order[b]))
         with open(name, "wb") as f:
-            for payload in (np.array([dtB[b], tSimulation]), np.concatenate([cs[b], c111[b]]),
-                            np.ascontiguousarray(np.moveaxis(inner[b], -1, 0)).reshape(-1)):
+            payloads = [np.array([dtB[b], tSimulation]), np.concatenate([cs[b], c111[b]]),
+                        np.ascontiguousarray(np.moveaxis(inner[b], -1, 0)).reshape(-1)]
+            if prev is not None:
+                payloads.append(np.ascontiguousarray(np.moveaxis(prev[b], -1, 0)).reshape(-1))
+            for payload in payloads:
                 raw = payload.astype("<f8").tobytes()
                 f.write(struct.pack("<i", len(raw)) + raw + struct.pack("<i", len(raw)))
 
@@ -174,6 +196,16 @@ def read_header(dirname):
 
 def read_restart(dirname):
     """(grid, State_VGB, tSimulation, nStep, DtMax_B) of a restart directory"""
+    return _read(dirname)[:5]
+
+
+def read_restart_previous(dirname):
+    """(DtPrev, ImplOld (nBlock, nK, nJ, nI, nVar)) of a restart written
+    after a BDF2 step (#NPREVIOUS), else None"""
+    return _read(dirname)[5]
+
+
+def _read(dirname):
     h = read_header(dirname)
     if int(h["#PRECISION"][0]) != 8 or int(h["#EQUATION"][1]) != NVAR:
         raise ValueError("restart with nByteReal %s and nVar %s: 8 and %d are read" %
@@ -194,34 +226,43 @@ def read_restart(dirname):
     typeRestart = h["#RESTARTINFILE"][0]
     order = morton_order(grid)
     nCellVar = NVAR * nI * nJ * nK
+    hasPrev = "#NPREVIOUS" in h and int(h["#NPREVIOUS"][0]) == nStep
+    nExtra = nCellVar if hasPrev else 0
+    prev = np.empty((nBlock, nK, nJ, nI, NVAR)) if hasPrev else None
     S = np.zeros(grid.state_shape_fortran())
     inner = np.empty((nBlock, nK, nJ, nI, NVAR))
     dtB = np.empty(nBlock)
     if typeRestart == "one":
         rec = np.fromfile(os.path.join(dirname, NAME_DATA), dtype="<f8")
-        if rec.size != nBlock * (7 + nCellVar):
-            raise ValueError("data.rst holds %d reals, %d expected" % (rec.size, nBlock * (7 + nCellVar)))
-        rec = rec.reshape(nBlock, 7 + nCellVar)
+        nRec = 7 + nCellVar + nExtra
+        if rec.size != nBlock * nRec:
+            raise ValueError("data.rst holds %d reals, %d expected" % (rec.size, nBlock * nRec))
+        rec = rec.reshape(nBlock, nRec)
         for b in range(nBlock):
             r = rec[order[b] - 1]
             dtB[b] = r[0]
-            inner[b] = r[7:].reshape(nK, nJ, nI, NVAR)
+            inner[b] = r[7:7 + nCellVar].reshape(nK, nJ, nI, NVAR)
+            if hasPrev:
+                prev[b] = np.moveaxis(r[7 + nCellVar:].reshape(NVAR, nK, nJ, nI), 0, -1)
     elif typeRestart == "block":
         for b in range(nBlock):
             nd = max(5, int(1 + np.log10(float(order[b]))))
             with open(os.path.join(dirname, "blk%0*d.rst" % (nd, order[b])), "rb") as f:
                 recs = []
-                for _ in range(3):
+                for _ in range(4 if hasPrev else 3):
                     m = struct.unpack("<i", f.read(4))[0]
                     recs.append(np.frombuffer(f.read(m), dtype="<f8"))
                     if struct.unpack("<i", f.read(4))[0] != m:
                         raise ValueError("record markers of block file %d differ" % order[b])
             dtB[b] = recs[0][0]
             inner[b] = np.moveaxis(recs[2].reshape(NVAR, nK, nJ, nI), 0, -1)
+            if hasPrev:
+                prev[b] = np.moveaxis(recs[3].reshape(NVAR, nK, nJ, nI), 0, -1)
     else:
         raise ValueError("TypeRestartInFile %r: 'one' and 'block' are read" % typeRestart)
     S[grid.interior_slices()] = inner
-    return grid, S, tSimulation, nStep, dtB
+    prevOut = (float(h["#NPREVIOUS"][1]), prev) if hasPrev else None
+    return grid, S, tSimulation, nStep, dtB, prevOut
 
 
 def write_restart(dirname, solver, typeRestart="one"):

@@ -48,17 +48,19 @@ def peaks():
     return 6650.0, "fallback"
 
 
+# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) per cell of one
+# stage3d_kernel launch, from one ncu capture of a stage-1 launch of the
+# 160^3 Orszag-Tang case (20^3 blocks, 0.26 GB of state, larger than L2):
+#   python bench.py --nroot 20 --precisions <p> --steps 2 --warmup 3 --no-e2e --no-cpu \
+#       --jfnk-precond= --heat-precond= --no-amr
+#   ncu --set full --clock-control none -k regex:stage3d -s 2 -c 1 <same command>
+# Traffic grows in proportion to the blocks, so the bench scales it by the
+# cells of its own grid.
+DRAM_BYTES_PER_CELL_LAUNCH = {"fp64": 142.2, "fp32": 108.3}
+
+
 def profile_traffic(prec):
-    """DRAM bytes per cell and stage launch from the committed ncu summary
-    (profiles/stage_kernel_ot.md, lines 'dram_bytes_per_cell_launch[_fp32]: X')."""
-    p = os.path.join(ROOT, "profiles", "stage_kernel_ot.md")
-    if not os.path.exists(p):
-        return None
-    key = "dram_bytes_per_cell_launch:" if prec == "fp64" else "dram_bytes_per_cell_launch_fp32:"
-    for line in open(p):
-        if line.startswith(key):
-            return float(line.split(":")[1])
-    return None
+    return DRAM_BYTES_PER_CELL_LAUNCH.get(prec)
 
 
 class ClockSampler:
@@ -588,7 +590,8 @@ def main():
     ap.add_argument("--learned-blend", type=float, default=0.6)
     ap.add_argument("--amr", dest="amr", action="store_true", default=True)
     ap.add_argument("--no-amr", dest="amr", action="store_false")
-    ap.add_argument("--amr-nroot", type=int, default=16, help="root blocks per dimension of the blast grid")
+    ap.add_argument("--amr-nroot", type=int, default=19,
+                    help="root blocks per dimension of the blast grid (19: 20,544 blocks, 10.5 M cells)")
     ap.add_argument("--amr-steps", type=int, default=50)
     ap.add_argument("--amr-dyn-steps", type=int, default=50, help="steps of the dynamic-AMR blast (0: skip)")
     ap.add_argument("--amr-dyn-dn", type=int, default=10, help="steps between regrids (#DOAMR DnAmr)")
@@ -640,7 +643,48 @@ def main():
             line["jfnk"]["cpu_baseline"] = cpu_baseline_jfnk(args)
         if args.heat_precond:
             line["heat"]["cpu_baseline"] = cpu_baseline_heat(args)
+    line["summary"] = summary(line)  # last key: the end of the line shows every leg
     print(json.dumps(line))
+
+
+def summary(line):
+    """The key figure of every leg, compactly (rounded to 4 digits)."""
+    r = lambda v: None if v is None else float("%.4g" % v)
+    out = {"fp64": r(line["value"]), "fp64_frac": line["roofline"]["frac"],
+           "fp64_e2e": r(line.get("e2e", {}).get("value"))}
+    fb = line.get("fp32_bulk")
+    if fb:
+        out.update({"fp32_bulk": r(fb["value"]), "fp32_bulk_frac": fb["roofline"]["frac"],
+                    "fp32_bulk_e2e": r((fb.get("e2e") or {}).get("value"))})
+    j = line.get("jfnk")
+    if j:
+        sp = {k: r(j[k]["s_per_step"]) for k in ("bilu", "none", "learned") if "s_per_step" in j.get(k, {})}
+        mv = {k: r(j[k]["matvec_per_step"]) for k in sp}
+        out["jfnk_s_per_step"] = sp
+        out["jfnk_matvec_per_step"] = mv
+        if "learned" in sp:
+            for k in ("bilu", "none"):
+                if k in sp:
+                    out["jfnk_%s_over_learned" % k] = r(sp[k] / sp["learned"])
+        if "cpu_baseline" in j:
+            out["jfnk_cpu_s_per_step"] = r(j["cpu_baseline"]["value"])
+    a = line.get("amr")
+    if a:
+        out["amr"] = {"blocks": a["blocks"], "cells": a["cells"], "fp32": r(a["fp32"]["value"]),
+                      "fp64": r(a["fp64"]["value"])}
+        if "dynamic" in a:
+            out["amr"]["dynamic_steps"] = r(a["dynamic"]["steps_value"])
+            out["amr"]["dynamic_with_regrids"] = r(a["dynamic"]["value_with_regrids"])
+    h = line.get("heat")
+    if h:
+        sp = {k: r(h[k]["s_per_solve"]) for k in ("bilu", "none", "learned") if "s_per_solve" in h.get(k, {})}
+        out["heat_s_per_solve"] = sp
+        out["heat_matvec_per_solve"] = {k: r(h[k]["matvec_per_solve"]) for k in sp}
+        if "cpu_baseline" in h:
+            out["heat_cpu_s_per_solve"] = r(h["cpu_baseline"]["value"])
+    if "cpu_baseline" in line:
+        out["cpu"] = r(line["cpu_baseline"]["value"])
+    return out
 
 
 if __name__ == "__main__":

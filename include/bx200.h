@@ -88,6 +88,17 @@ typedef struct {
   int UseDtFixed;
   double DtFixed;
   int Precision;         /* BX_FP64 or BX_FP32_BULK */
+  /* Floors of the updated state (#MINIMUMDENSITY, #MINIMUMPRESSURE,
+   * #MINIMUMTEMPERATURE, normalized units), each active where > 0 as
+   * UseRhoMin / UsePMin (src/ModPhysics.f90:737-738):
+   * rho = max(RhoMin, rho) before the energy -> pressure conversion
+   * (src/ModUpdateState.f90:901-908), then limit_pressure
+   * (src/ModEnergy.f90:388): p = max(pMin, p), p = max(rho/MassIon*TMin, p).
+   * MassIon is the ion mass in amu (#PLASMA, MassFluid_I); 0 means 1. */
+  double RhoMin;
+  double pMin;
+  double TMin;
+  double MassIon;
 } bx_scheme_params;
 
 /* ---- set-up ------------------------------------------------------------ */
@@ -276,9 +287,11 @@ BX_API int bx_impl_get_x(double *x_I);
  * while other streams run.  It calls no cudaMalloc, cudaFree or allocating
  * library: the scratch is a static device array for at most
  * BX_NOALLOC_MAX_BLOCK blocks; larger nBlock is rejected with BX_ERR_ARG.
- * The first call on a device looks up the scratch address (make it before
- * any stream capture).  Calls that overlap on the GPU share the scratch and
- * race: serialize them.  Independent of bx_init. */
+ * The first call on a device looks up the scratch address; make that first
+ * call before any stream capture.  Every call copies Norm_V to host memory
+ * and synchronizes the stream before it returns.  All calls share the one
+ * scratch array, so calls that overlap on the GPU race: serialize them.
+ * Independent of bx_init. */
 #define BX_NOALLOC_MAX_BLOCK 32768
 BX_API int bx_impl_norm_noalloc(const double *Impl_dev, int nCellBlock, int nBlock, void *stream, double *Norm_V);
 

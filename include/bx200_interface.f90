@@ -72,6 +72,7 @@ module bx200_interface
      integer(c_int):: UseDivbSource, UseHalfStep, UseDtFixed
      real(c_double):: DtFixed
      integer(c_int):: Precision
+     real(c_double):: RhoMin, pMin, TMin, MassIon
   end type bx_scheme_params
 
   interface

@@ -36,6 +36,9 @@ const double cTiny = 1.0e-6;
 // ModNumConst::cTolerance (same library; the published value 1e-10 is
 // assumed), used only by the degenerate-case tests of the Roe solver
 const double cTolerance = 1.0e-10;
+// SmallDouble of src/ModPartImplicit.f90:34: Norm_V (:465) and the rms of
+// the matvec's x (:1192) below it are replaced by 1
+const double kSmallDouble = 1.0e-30;
 
 inline double sign25(double x) { return std::copysign(0.25, x); }
 inline double min3(double a, double b, double c) { return std::min(std::min(a, b), c); }
@@ -1053,11 +1056,28 @@ struct Oracle {
 
   // update_state (src/ModUpdateState.f90:83) -> update_state_normal
   // (:191-450) -> update_explicit (:453-1160), conservative energy update
+  // limit_pressure (src/ModEnergy.f90:388-420), single ion fluid: the
+  // pressure floor, then the temperature floor NumDens*TMin with
+  // NumDens = Rho/MassFluid; each active where it is > 0
+  void limit_pressure(double *X) const {
+    if (c.pMin > 0.0) X[P_] = std::max(c.pMin, X[P_]);
+    if (c.tMin > 0.0) {
+      const double NumDens = X[Rho_] / (c.massIon > 0.0 ? c.massIon : 1.0);
+      X[P_] = std::max(NumDens * c.tMin, X[P_]);
+    }
+  }
+
   void update_state(int b, Scratch &s) {
     if (iStage == 1)
       std::copy(State.begin() + nVar * nCellG * b, State.begin() + nVar * nCellG * (b + 1),
                 StateOld.begin() + nVar * nCellG * b);
-    if (Dt == 0.0) return;  // IsTimeAccurate .and. Dt == 0
+    if (Dt == 0.0) {  // IsTimeAccurate .and. Dt == 0 (src/ModUpdateState.f90:241)
+      // update_state still calls limit_pressure (:169)
+      for (int k = 1; k <= c.nK; k++)
+        for (int j = 1; j <= c.nJ; j++)
+          for (int i = 1; i <= c.nI; i++) limit_pressure(st(b, i, j, k));
+      return;
+    }
     double DtFactor = c.useHalfStep ? (c.cfl * iStage) / c.nStage : c.cfl;
     double V = cellVolume(b);
     const long nC = (long)c.nI * c.nJ * c.nK;
@@ -1082,6 +1102,8 @@ struct Oracle {
           if (c.useNonConservative) {  // pressure equation: no energy conversion
             double *U = st(b, i, j, k);
             for (int v = 0; v < nVar; v++) U[v] = O[v] + Src[v];
+            if (c.rhoMin > 0.0) U[Rho_] = std::max(c.rhoMin, U[Rho_]);  // :901-908
+            limit_pressure(U);  // energy_to_pressure, non-conservative branch
             continue;
           }
           // pressure_to_energy(StateOld) (src/ModEnergy.f90:47)
@@ -1090,11 +1112,15 @@ struct Oracle {
           Src[P_] = Src[Energy_];
           double *U = st(b, i, j, k);
           for (int v = 0; v < nVar; v++) U[v] = O[v] + Src[v];
+          // the minimum density (src/ModUpdateState.f90:901-908)
+          if (c.rhoMin > 0.0) U[Rho_] = std::max(c.rhoMin, U[Rho_]);
           // energy_to_pressure (src/ModEnergy.f90:243) on State and StateOld
           for (double *X : {U, O}) {
             X[P_] = X[P_] - 0.5 * (X[Bx_] * X[Bx_] + X[By_] * X[By_] + X[Bz_] * X[Bz_]);
             X[P_] = GammaMinus1 * (X[P_] - 0.5 * (X[RhoUx_] * X[RhoUx_] + X[RhoUy_] * X[RhoUy_] + X[RhoUz_] * X[RhoUz_]) / X[Rho_]);
           }
+          // then limit_pressure on State only (IsOld skips it, :320-324)
+          limit_pressure(U);
         }
   }
 
@@ -1333,7 +1359,7 @@ struct Implicit {
     double xn = 0;
     for (long n = 0; n < N; n++) xn += x[n] * x[n];
     xn = std::sqrt(xn / N);
-    if (xn < 1e-300) xn = 1.0;  // SmallDouble
+    if (xn < kSmallDouble) xn = 1.0;
     const double Eps = std::sqrt(c.jacobianEps) / xn;
     std::vector<double> Ueps(N), Reps(N);
     for (long n = 0; n < N; n++) Ueps[n] = Impl[n] + Eps * x[n] * Norm[n % nVar];
@@ -1727,7 +1753,7 @@ struct Implicit {
       double s = 0;
       for (long m = 0; m < nCellTot; m++) s += Impl[nVar * m + v] * Impl[nVar * m + v];
       Norm[v] = std::sqrt(s / nCellTot);
-      if (Norm[v] < 1e-300) Norm[v] = 1.0;
+      if (Norm[v] < kSmallDouble) Norm[v] = 1.0;
     }
     DtCoeff = c.cflImpl / 0.5;
     // BDF2 needs the previous step (and a nonzero previous time step)

@@ -43,6 +43,7 @@ typedef struct {
   int useHalfStep;     /* #TIMESTEPPING / #SCHEME with nStage<=2 */
   int nThread;         /* OpenMP threads (0 = default) */
   int useNonConservative; /* #NONCONSERVATIVE: pressure equation instead of energy */
+  double rhoMin, pMin, tMin, massIon; /* floors, active where > 0 (massIon 0 -> 1) */
 } ora_config;
 
 /* Create an oracle grid. iLevelCoord holds 4 ints per block: level and the

@@ -36,6 +36,8 @@ class OraConfig(ctypes.Structure):
         ("useHalfStep", ctypes.c_int),
         ("nThread", ctypes.c_int),
         ("useNonConservative", ctypes.c_int),
+        ("rhoMin", ctypes.c_double), ("pMin", ctypes.c_double), ("tMin", ctypes.c_double),
+        ("massIon", ctypes.c_double),
     ]
 
 
@@ -114,6 +116,10 @@ class Oracle:
         c.useHalfStep = int(scheme.useHalfStep)
         c.nThread = n_thread
         c.useNonConservative = int(getattr(scheme, "useNonConservative", False))
+        c.rhoMin = getattr(scheme, "rhoMin", -1.0)
+        c.pMin = getattr(scheme, "pMin", -1.0)
+        c.tMin = getattr(scheme, "tMin", -1.0)
+        c.massIon = getattr(scheme, "massIon", 1.0)
         self.cfg = c
         self.grid = grid
         lc = np.ascontiguousarray(grid.iLevelCoord, dtype=np.int32)

@@ -4,7 +4,8 @@ Reads the IDL ascii golden files of the reference (Param/*/TestOutput) and
 stores the columns the hot path produces as compact .npz fixtures, so that
 the tests never read the reference tree at run time.
 
-    python tests/golden/make_fixtures.py [/path/to/reference]
+    python tests/golden/make_fixtures.py <BATS-R-US source tree>
+    (or with the tree in the environment variable BATSRUS_REFERENCE)
 """
 import os
 import sys
@@ -43,4 +44,8 @@ def main(ref):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    # the BATS-R-US source tree: the first argument, else $BATSRUS_REFERENCE
+    ref = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("BATSRUS_REFERENCE")
+    if not ref:
+        sys.exit("usage: make_fixtures.py <BATS-R-US source tree> (or set BATSRUS_REFERENCE)")
+    main(ref)

@@ -231,3 +231,29 @@ def test_oracle_matches_reference_fast_wave_golden():
     mid = dist > 20.0
     bad = (d[mid] > float(ref["tolerance_abs"])) & (d[mid] > float(ref["tolerance_rel"]) * np.abs(R[mid]))
     assert not bad.any(), bad.sum(0)
+
+
+def test_floors_hold_and_trip():
+    """The oracle's floors: with RhoMin, pMin and TMin set, every updated
+    state respects them and each of the density and temperature floors
+    sets some cells; without them the blast's interior density drops below
+    the density floor."""
+    g, s, st, _ = configs.uniform_3d_case(2, "HLLD", "mc", 1.5, state="blast")
+    isl = g.interior_slices()
+    o = Oracle(g, s)
+    o.set_state(st)
+    o.exchange_messages()
+    o.advance(4)
+    assert o.get_state()[isl][..., 0].min() < 0.6
+    s.rhoMin, s.pMin, s.tMin, s.massIon = 0.6, 0.1, 0.15, 1.25
+    o = Oracle(g, s)
+    o.set_state(st)
+    o.exchange_messages()
+    o.advance(1)  # Dt = 0: limit_pressure only
+    S = o.get_state()[isl]
+    assert (S[..., 7] == S[..., 0] / 1.25 * 0.15).any() and (S[..., 0] == 1.0).all()
+    o.advance(3)
+    S = o.get_state()[isl]
+    rho, p = S[..., 0], S[..., 7]
+    assert (rho >= 0.6).all() and (rho == 0.6).any()
+    assert (p >= 0.1).all() and (p >= rho / 1.25 * 0.15).all()

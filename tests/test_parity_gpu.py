@@ -237,3 +237,28 @@ def test_gpu_hlld_error_status_is_reported_not_aborted():
     except BxError as e:
         assert e.code == 5
     assert np.isfinite(x.get_state()).all()
+
+
+def test_gpu_floors_match_oracle():
+    """#MINIMUMDENSITY / #MINIMUMPRESSURE / #MINIMUMTEMPERATURE on the blast:
+    the density floor (src/ModUpdateState.f90:901-908) trips in the
+    rarefied interior from the third step, the temperature floor
+    (limit_pressure, src/ModEnergy.f90:388-420, NumDens = rho/MassIon)
+    already at the Dt = 0 step; both in the GPU result and the oracle's, which
+    agree within 1e-12 per step."""
+    g, s, st, _ = configs.uniform_3d_case(2, "HLLD", "mc", 1.5, state="blast")
+    s.rhoMin, s.pMin, s.tMin, s.massIon = 0.6, 0.1, 0.15, 1.25
+    o, x = make_pair(g, s, st)
+    isl = g.interior_slices()
+    hitRho = hitT = 0
+    for step in range(6):
+        x.advance(1)
+        o.advance(1)
+        S, So = x.get_state()[isl], o.get_state()[isl]
+        assert rel_err(S, So) < TOL_FP64, step
+        rho, p = S[..., 0], S[..., 7]
+        assert (rho >= 0.6).all() and (p >= 0.1).all() and (p >= rho / 1.25 * 0.15).all()
+        hitRho += int((rho == 0.6).sum())
+        hitT += int((p == rho / 1.25 * 0.15).sum())
+    assert hitRho > 0 and hitT > 0
+    x.close()

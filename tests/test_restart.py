@@ -85,3 +85,37 @@ def test_morton_order_is_root_major_z_order():
     # inside a root: x fastest, then y, then z
     first = {tuple(c[1:]): o for c, o in zip(lc.tolist(), order) if c[1] < 2}
     assert [first[(0, 0, 0)], first[(1, 0, 0)], first[(0, 1, 0)], first[(1, 1, 0)], first[(0, 0, 1)]] == [1, 2, 3, 4, 5]
+
+
+@pytest.mark.parametrize("kind", ["one", "block"])
+def test_bdf2_previous_state_round_trip(tmp_path, kind):
+    """A restart after a BDF2 step (nStepPrev == nStep) carries #NPREVIOUS and
+    ImplOld_VCB per block (src/ModRestartFile.f90:457-461, 828-829,
+    1084-1091); the state and the previous state both come back."""
+    g, S, t, n, dtB = case()
+    prev = np.random.default_rng(9).normal(size=(g.nBlock, 8, 8, 8, 8))
+    restart.write_restart_arrays(str(tmp_path), g, S, t, n, dtB, kind, ImplOld=prev, DtPrev=3.5e-3)
+    g2, S2, t2, n2, dtB2 = restart.read_restart(str(tmp_path))
+    assert np.array_equal(S2[g.interior_slices()], S[g.interior_slices()]) and (t2, n2) == (t, n)
+    assert np.array_equal(dtB2, dtB)
+    dtPrev, prev2 = restart.read_restart_previous(str(tmp_path))
+    assert dtPrev == 3.5e-3 and np.array_equal(prev2, prev)
+    h = restart.read_header(str(tmp_path))
+    assert h["#NPREVIOUS"][0] == str(n)
+    if kind == "one":
+        raw = np.fromfile(os.path.join(str(tmp_path), "data.rst"), dtype="<f8")
+        nRec = 7 + 2 * 8 * 512
+        assert raw.size == g.nBlock * nRec
+        order = restart.morton_order(g)
+        b = 3
+        r = raw[(order[b] - 1) * nRec:order[b] * nRec]
+        # State8_CV(i, j, k, iVar): the variable slowest
+        i, j, k, v = 2, 5, 1, 6
+        assert r[7 + 8 * 512 + i + 8 * (j + 8 * (k + 8 * v))] == prev[b, k, j, i, v]
+    assert restart.read_restart_previous(str(tmp_path)) is not None
+
+
+def test_no_previous_state_without_bdf2(tmp_path):
+    g, S, t, n, dtB = case()
+    restart.write_restart_arrays(str(tmp_path), g, S, t, n, dtB, "one")
+    assert restart.read_restart_previous(str(tmp_path)) is None
