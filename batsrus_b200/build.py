@@ -25,6 +25,7 @@ UNITS = [
     ("bx_stage_fp32.cu", []),
     ("bx_stage3d.cu", []),
     ("bx_stage3d_fpt2.cu", []),
+    ("bx_stage3d_v2.cu", []),
     ("bx_amr.cu", []),
     ("bx_amr_plan.cu", []),
     ("bx_implicit.cu", ["--fmad=false"]),
@@ -34,7 +35,7 @@ UNITS = [
     ("bx_tune.cu", []),
     ("bx_capi.cu", []),
 ]
-HEADERS = ["bx_physics.cuh", "bx_stage.cuh", "bx_device.h", "bx_stage3d.cuh", "bx_stage3d_launch.cuh", "bx_tma.cuh", "bx_core.h",
+HEADERS = ["bx_physics.cuh", "bx_stage.cuh", "bx_device.h", "bx_stage3d.cuh", "bx_stage3d_v2.cuh", "bx_stage3d_launch.cuh", "bx_tma.cuh", "bx_core.h",
            "bx_impl_kernels.cuh", "bx_krylov.cuh", "bx_tune.h", "bx_tc.cuh", "bx_learned.cuh", "bx_learned_kernels.cuh", "bx_amr.h"]
 
 

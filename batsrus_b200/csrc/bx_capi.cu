@@ -386,11 +386,12 @@ int launch_stage_dt(int iStage, bool computeDt) {
 
 int launch_stage(int iStage) { return launch_stage_dt(iStage, iStage == g.sch.nStage); }
 
-// autotune the persistent grid of the stage kernel: time stage-1 launches
-// (they write only the stage buffer, the block time steps and the step
-// state, which are restored) for each candidate number of CTAs per SM
+// autotune the persistent grid and the variant of the stage kernel: time
+// the stages of one step for each candidate (stage 1 writes the stage
+// buffer; the last stage writes a scratch copy of the state instead of U;
+// the block time steps and the step state are restored)
 int tune_stage_impl() {
-  TuneKnobInfo &k = tune_knob(kTuneStageGrid), &kf = tune_knob(kTuneStageFpt);
+  TuneKnobInfo &k = tune_knob(kTuneStageGrid), &kf = tune_knob(kTuneStageVariant);
   if (!g.ready || !g.use3d || (k.tuned == 2 && kf.tuned == 2)) return BX_OK;
   StepState saved;
   std::vector<double> dtSaved(g.nBlock);
@@ -398,9 +399,12 @@ int tune_stage_impl() {
   CK(cudaMemcpyAsync(dtSaved.data(), g.dtBlock, sizeof(double) * g.nBlock, cudaMemcpyDeviceToHost, g.st));
   CK(cudaStreamSynchronize(g.st));
   const int v0 = k.value, f0 = kf.value;
-  const bool fixG = k.tuned == 2, fixF = kf.tuned == 2 || g.shape != kShape888;  // faces per thread: 8^3 only
+  const bool fixG = k.tuned == 2, fixF = kf.tuned == 2 || g.shape != kShape888;  // variants: 8^3 only
   float best = 1e30f;
   int bestV = v0, bestF = f0;
+  double *scratch = nullptr;
+  if (g.sch.nStage == 2 && cudaMalloc(&scratch, sizeof(double) * 8 * g.nCell * (size_t)g.nBlock) != cudaSuccess)
+    return fail(BX_ERR_NOMEM, "autotune of the stage kernel: scratch state");
   cudaEvent_t e0, e1;
   CK(cudaEventCreate(&e0));
   CK(cudaEventCreate(&e1));
@@ -413,16 +417,29 @@ int tune_stage_impl() {
       if (fixG && k.cand[i] != v0) continue;
       k.value = k.cand[i];
       kf.value = kf.cand[jf];
-      StageArgs a = stage_args(1, g.sch.nStage == 1);
-      const int kind = g.sch.Precision == BX_FP64 ? kKindFp64 : kKindFp32In64;
-      const TmaMaps *m = g.sch.Precision == BX_FP64 ? (a.in == g.bufX ? &g.mapX64 : &g.mapY64) : &g.mapX64;
       cudaError_t e = cudaSuccess;
       for (int rep = 0; rep < 4 && e == cudaSuccess; rep++) {
         if (rep == 1) e = cudaEventRecord(e0, g.st);
-        if (e == cudaSuccess && g.nSlab)
-          e = launch_reschange(g.shape, g.sch.TypeFlux, kind, a, g.slabs, g.nSlab, g.lcDev,
-                               make_int3(g.nRoot[0], g.nRoot[1], g.nRoot[2]), g.rcGhost, g.rcFlux, g.st);
-        if (e == cudaSuccess) e = launch_stage3d(g.shape, g.sch.TypeFlux, kind, *m, a, g.nSM, g.st);
+        for (int s = 1; s <= g.sch.nStage && e == cudaSuccess; s++) {
+          StageArgs a = stage_args(s, s == g.sch.nStage);
+          if (s == 2) a.out = scratch;
+          int kind;
+          const TmaMaps *m;
+          if (g.sch.Precision == BX_FP64) {
+            kind = kKindFp64;
+            m = a.in == g.bufX ? &g.mapX64 : &g.mapY64;
+          } else if (s == 1) {
+            kind = kKindFp32In64;
+            m = &g.mapX64;
+          } else {
+            kind = kKindFp32In32;
+            m = &g.mapY32;
+          }
+          if (g.nSlab)
+            e = launch_reschange(g.shape, g.sch.TypeFlux, kind, a, g.slabs, g.nSlab, g.lcDev,
+                                 make_int3(g.nRoot[0], g.nRoot[1], g.nRoot[2]), g.rcGhost, g.rcFlux, g.st);
+          if (e == cudaSuccess) e = launch_stage3d(g.shape, g.sch.TypeFlux, kind, *m, a, g.nSM, g.st);
+        }
       }
       if (e == cudaSuccess) e = cudaEventRecord(e1, g.st);
       if (e == cudaSuccess) e = cudaEventSynchronize(e1);
@@ -441,6 +458,10 @@ int tune_stage_impl() {
   }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
+  if (scratch) {
+    cudaStreamSynchronize(g.st);
+    cudaFree(scratch);
+  }
   k.value = r ? v0 : bestV;
   kf.value = r ? f0 : bestF;
   if (!r) {

@@ -22,6 +22,27 @@ enum { kLimMinmod = 0, kLimMc = 1, kLimMc3 = 2 };
 template <typename R>
 __device__ __forceinline__ R sign25(R x) { return copysign(R(0.25), x); }
 
+// Division, reciprocal and square root of the face arithmetic: IEEE in
+// double (the FP64 mode matches the CPU oracle to rounding); in float the
+// hardware approximations, div.approx.f32 (__fdividef), rcp.approx.ftz.f32
+// and sqrt.approx.ftz.f32 (PTX ISA), a few ulp, far inside the FP32-bulk
+// mode's bound on the error against FP64 (the operands are positive normal
+// numbers: densities, pressures, wave-speed sums)
+__device__ __forceinline__ double fdiv(double a, double b) { return a / b; }
+__device__ __forceinline__ float fdiv(float a, float b) { return __fdividef(a, b); }
+__device__ __forceinline__ double frcp(double a) { return 1.0 / a; }
+__device__ __forceinline__ float frcp(float a) {
+  float r;
+  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(a));
+  return r;
+}
+__device__ __forceinline__ double fsqrt(double a) { return sqrt(a); }
+__device__ __forceinline__ float fsqrt(float a) {
+  float r;
+  asm("sqrt.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(a));
+  return r;
+}
+
 // limit_pressure (src/ModEnergy.f90:388-420) for the single ion fluid: the
 // pressure floor pMin, then the temperature floor NumDens*TMin with
 // NumDens = rho/MassIon; a floor is active where it is > 0
@@ -341,13 +362,13 @@ __device__ __forceinline__ bool numerical_flux(R (&L)[8], R (&Rt)[8], R gamma, R
 template <int D, typename R>
 __device__ __forceinline__ void mhd_speed_lean(R rho, R un, R bn, R B2, R p, R gamma, R &fast,
                                                R &unOut) {
-  const R invRho = R(1) / rho;
+  const R invRho = frcp(rho);
   const R sound2 = gamma * p * invRho;
   const R alfven2 = B2 * invRho;
   const R alfven2n = invRho * (bn * bn);
   const R fast2 = sound2 + alfven2;
-  const R discr = sqrt(fmax(R(0), fast2 * fast2 - R(4) * sound2 * alfven2n));
-  fast = sqrt(R(0.5) * (fast2 + discr));
+  const R discr = fsqrt(fmax(R(0), fast2 * fast2 - R(4) * sound2 * alfven2n));
+  fast = fsqrt(R(0.5) * (fast2 + discr));
   unOut = un;
 }
 
@@ -385,7 +406,7 @@ __device__ __forceinline__ R flux_lean(R (&L)[8], R (&Rt)[8], R gamma, R invGm1,
       mhd_speed_lean<D>(Rt[kRho], Rt[un], Rt[bn], B2R, Rt[kP], gamma, fastR, uR);
       const R cleft = fmin(R(0), fmin(uL - fastL, unA - fastA));
       const R cright = fmax(R(0), fmax(uR + fastR, unA + fastA));
-      wL = cright / (cright - cleft);
+      wL = fdiv(cright, cright - cleft);
       wR = R(1) - wL;
       dif = cright * wR;
     }

@@ -1,6 +1,6 @@
 // bx_stage3d_fpt2.cu -- the stage kernel for 8^3 blocks with two faces per
 // thread (288 threads, two independent face computations each): the
-// instantiations that the autotuner's stage_faces_per_thread = 2 selects.
+// instantiations that the autotuner's stage_variant = 2 selects.
 #include "bx_stage3d_launch.cuh"
 
 namespace bx {

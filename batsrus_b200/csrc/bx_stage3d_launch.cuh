@@ -14,14 +14,19 @@ static cudaError_t launch_lim(const TmaMaps &maps, const StageArgs &a, int nSM, 
   auto k = stage3d_kernel<T, TileT, Real, OutT, FLUX, LIM>;
   constexpr size_t sm = T::template smem_bytes<Real>();
   static bool attr = false;
+  static int fit = 1;
   if (!attr) {
     cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
     if (e != cudaSuccess) return e;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&fit, k, T::NTHR, sm);
+    if (e != cudaSuccess) return e;
+    if (fit < 1) fit = 1;
     attr = true;
   }
   // persistent grid: the autotuned number of CTAs per SM (several fit for
-  // the small tiles of 4^3 blocks)
-  const int want = nSM * tune_value(kTuneStageGrid);
+  // the small tiles of 4^3 blocks), at most as many as are resident at once
+  const int perSM = tune_value(kTuneStageGrid) < fit ? tune_value(kTuneStageGrid) : fit;
+  const int want = nSM * perSM;
   const int grid = a.nBlock < want ? a.nBlock : want;
   k<<<grid, T::NTHR, sm, st>>>(maps, a);
   return cudaGetLastError();
@@ -63,5 +68,7 @@ static cudaError_t launch_kind(int flux, int kind, const TmaMaps &maps, const St
 // 8^3 blocks with two faces per thread (bx_stage3d_fpt2.cu)
 cudaError_t launch_stage3d_fpt2(int flux, int kind, const TmaMaps &maps, const StageArgs &a, int nSM,
                                 cudaStream_t st);
+// 8^3 blocks with one face phase per block (bx_stage3d_v2.cu)
+cudaError_t launch_stage8(int flux, int kind, const TmaMaps &maps, const StageArgs &a, int nSM, cudaStream_t st);
 
 }  // namespace bx

@@ -1,0 +1,68 @@
+// bx_stage3d_v2.cu -- instantiations and launcher of the single-face-phase
+// stage kernel for 8^3 blocks (bx_stage3d_v2.cuh), which the autotuner's
+// stage_variant = 0 selects.
+#include "bx_stage3d_v2.cuh"
+#include "bx_tune.h"
+
+namespace bx {
+
+namespace {
+
+template <int NTHR, int MINB, typename TileT, typename Real, typename OutT, int FLUX, int LIM>
+cudaError_t launch8_lim(const TmaMaps &maps, const StageArgs &a, int nSM, cudaStream_t st) {
+  using B = Blk8<TileT, Real, NTHR, MINB>;
+  auto k = stage8_kernel<B, TileT, Real, OutT, FLUX, LIM>;
+  constexpr size_t sm = B::smem_bytes;
+  static bool attr = false;
+  if (!attr) {
+    cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    if (e != cudaSuccess) return e;
+    attr = true;
+  }
+  // persistent grid of MINB CTAs per SM (what the shared memory and the
+  // registers of the instantiation hold together)
+  const int want = nSM * MINB;
+  const int grid = a.nBlock < want ? a.nBlock : want;
+  k<<<grid, NTHR, sm, st>>>(maps, a);
+  return cudaGetLastError();
+}
+
+template <int NTHR, int MINB, typename TileT, typename Real, typename OutT, int FLUX>
+cudaError_t launch8_flux(const TmaMaps &maps, const StageArgs &a, int nSM, cudaStream_t st) {
+  switch (a.limiter) {
+    case kLimMinmod: return launch8_lim<NTHR, MINB, TileT, Real, OutT, FLUX, kLimMinmod>(maps, a, nSM, st);
+    case kLimMc: return launch8_lim<NTHR, MINB, TileT, Real, OutT, FLUX, kLimMc>(maps, a, nSM, st);
+    case kLimMc3: return launch8_lim<NTHR, MINB, TileT, Real, OutT, FLUX, kLimMc3>(maps, a, nSM, st);
+  }
+  return cudaErrorInvalidValue;
+}
+
+template <int NTHR, int MINB, typename TileT, typename Real, typename OutT>
+cudaError_t launch8_kind(int flux, const TmaMaps &maps, const StageArgs &a, int nSM, cudaStream_t st) {
+  switch (flux) {
+    case kFluxRusanov: return launch8_flux<NTHR, MINB, TileT, Real, OutT, kFluxRusanov>(maps, a, nSM, st);
+    case kFluxLinde: return launch8_flux<NTHR, MINB, TileT, Real, OutT, kFluxLinde>(maps, a, nSM, st);
+    case kFluxHlld: return launch8_flux<NTHR, MINB, TileT, Real, OutT, kFluxHlld>(maps, a, nSM, st);
+    case kFluxRoe: return launch8_flux<NTHR, MINB, TileT, Real, OutT, kFluxRoe>(maps, a, nSM, st);
+  }
+  return cudaErrorInvalidValue;
+}
+
+}  // namespace
+
+cudaError_t launch_stage8(int flux, int kind, const TmaMaps &maps, const StageArgs &a, int nSM, cudaStream_t st) {
+  // FP64: one CTA of 512 threads per SM (the FP64 tile and face slots fill
+  // the shared memory).  FP32-bulk: stage 1 lands the FP64 state, one CTA
+  // of 512; stage 2 one CTA of 512 or, for stage_ctas_per_sm >= 2, two CTAs
+  // of 256 per SM, each on its own block
+  switch (kind) {
+    case kKindFp64: return launch8_kind<512, 1, double, double, double>(flux, maps, a, nSM, st);
+    case kKindFp32In64: return launch8_kind<512, 1, double, float, float>(flux, maps, a, nSM, st);
+    case kKindFp32In32:
+      if (tune_value(kTuneStageGrid) >= 2) return launch8_kind<256, 2, float, float, double>(flux, maps, a, nSM, st);
+      return launch8_kind<512, 1, float, float, double>(flux, maps, a, nSM, st);
+  }
+  return cudaErrorInvalidValue;
+}
+
+}  // namespace bx

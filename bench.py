@@ -152,6 +152,9 @@ def run_ours(args):
     from batsrus_b200.explicit import ExplicitSolver
 
     hbm_peak, peak_kind = peaks()
+    if args.stage_ctas:
+        from batsrus_b200 import capi
+        capi.tune_set("stage_ctas_per_sm", args.stage_ctas)
     out = {}
     st = None
     for prec in args.precisions.split(","):
@@ -598,6 +601,8 @@ def main():
     ap.add_argument("--jfnk-nroot", type=int, default=16, help="16 -> 128^3 cells")
     ap.add_argument("--jfnk-steps", type=int, default=5)
     ap.add_argument("--jfnk-warmup", type=int, default=2)
+    ap.add_argument("--stage-ctas", type=int, default=0,
+                    help="pin stage_ctas_per_sm (FP32-bulk stage 2: 2 -> two 256-thread CTAs per SM)")
     ap.add_argument("--no-autotune", dest="autotune", action="store_false",
                     help="keep the default launch shapes instead of bx_autotune")
     ap.add_argument("--heat-precond", default="BILU,NONE,LEARNED", help="'' to skip the heat conduction workload")

@@ -41,24 +41,33 @@ def test_stage_grid_candidates_bit_identical():
 
 
 @pytest.mark.parametrize("prec", ["fp64", "fp32"])
-def test_stage_faces_per_thread_bit_identical(prec):
-    # 8^3 blocks, HLLD and Linde with the Koren limiter, a blast state
+def test_stage_variants_agree(prec):
+    """The three 8^3 stage kernels (one face phase; one direction at a time
+    with one or two faces per thread) on a blast state with HLLD and Linde
+    and the Koren limiter, on a static AMR grid with resolution changes, and
+    in the implicit residual mode: the same state to rounding."""
     out = {}
+    cases = []
     for flux in ("Linde", "HLLD"):
-        g, s, st, _ = configs.uniform_3d_case(2, flux, "mc3", 1.2, precision=prec, state="blast")
-        for f in capi.tune_info()["stage_faces_per_thread"]["candidates"]:
-            capi.tune_set("stage_faces_per_thread", f)
+        cases.append((flux,) + configs.uniform_3d_case(2, flux, "mc3", 1.2, precision=prec, state="blast")[:3])
+    g, s, st, _ = configs.amr_blast(nRoot=2, maxLevel=2, precision=prec)
+    cases.append(("amr",) + (g, s, st))
+    for name, g, s, st in cases:
+        for f in capi.tune_info()["stage_variant"]["candidates"]:
+            capi.tune_set("stage_variant", f)
             x = ExplicitSolver(g, s)
             x.set_state(st)
             x.advance(3)
-            out[(flux, f)] = (x.get_state(), x.time())
+            out[(name, f)] = (x.get_state(), x.time())
             x.close()
         # the instantiations may contract multiply-adds differently, so the
-        # variants agree to rounding (FP64 came out identical here)
-        a, b = out[(flux, 2)][0], out[(flux, 1)][0]
-        rel = np.abs(a - b).max() / np.abs(b).max()
-        assert rel <= (1e-13 if prec == "fp64" else 1e-5), (flux, rel)
-        assert abs(out[(flux, 2)][1][0] - out[(flux, 1)][1][0]) <= 1e-12 * abs(out[(flux, 1)][1][0])
+        # variants agree to rounding
+        for f in (0, 2):
+            a, b = out[(name, f)][0], out[(name, 1)][0]
+            rel = np.abs(a - b).max() / np.abs(b).max()
+            assert rel <= (1e-13 if prec == "fp64" else 1e-5), (name, f, rel)
+            assert abs(out[(name, f)][1][0] - out[(name, 1)][1][0]) <= 1e-12 * abs(out[(name, 1)][1][0])
+    capi.tune_set("stage_variant", 0)
 
 
 def heat_case(nRoot=2, prec="BILU"):
@@ -121,7 +130,7 @@ def test_autotune_picks_candidates_and_keeps_caller_choice():
     x, h, _ = heat_case(nRoot=4)
     capi.tune_set("krylov_unroll", 1)
     knobs = x.autotune()
-    for name in ("stage_ctas_per_sm", "stage_faces_per_thread", "krylov_ctas_per_sm", "heat_ilu_warps"):
+    for name in ("stage_ctas_per_sm", "stage_variant", "krylov_ctas_per_sm", "heat_ilu_warps"):
         k = knobs[name]
         assert k["tuned"] == 1 and k["value"] in k["candidates"], (name, k)
         assert all(m > 0 for m in k["ms"]), (name, k)

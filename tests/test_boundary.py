@@ -55,7 +55,7 @@ def test_argument_errors_without_gpu():
     # the autotuner's table needs no device
     knobs = capi.tune_info()
     assert set(knobs) == {"stage_ctas_per_sm", "krylov_ctas_per_sm", "krylov_unroll", "heat_ilu_warps",
-                          "bilu_threads", "stage_faces_per_thread", "krylov_gs_steps"}
+                          "bilu_threads", "stage_variant", "krylov_gs_steps"}
     assert all(k["value"] in k["candidates"] and k["tuned"] == 0 for k in knobs.values())
     assert L.bx_tune_set(b"krylov_unroll", 3) == 1 and L.bx_tune_set(b"no_such_knob", 1) == 1
     capi.tune_set("krylov_unroll", 4)
