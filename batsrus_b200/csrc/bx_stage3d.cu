@@ -12,9 +12,11 @@ cudaError_t launch_stage3d(int shape, int flux, int kind, const TmaMaps &maps, c
                            cudaStream_t st) {
   switch (shape) {
     case kShape888:
-      // stage_variant 0: one face phase per block (bx_stage3d_v2.cuh);
-      // 1, 2: one direction at a time with one or two faces per thread
-      if (tune_value(kTuneStageVariant) == 0) return launch_stage8(flux, kind, maps, a, nSM, st);
+      // stage_variant 0, 3: one face phase per block (bx_stage3d_v2.cuh),
+      // 512 or 576 threads for FP64; 1, 2: one direction at a time with one
+      // or two faces per thread
+      if (tune_value(kTuneStageVariant) == 0 || tune_value(kTuneStageVariant) == 3)
+        return launch_stage8(flux, kind, maps, a, nSM, st);
       if (tune_value(kTuneStageVariant) == 2) return launch_stage3d_fpt2(flux, kind, maps, a, nSM, st);
       return launch_kind<8, 1>(flux, kind, maps, a, nSM, st);
     case kShape444: return launch_kind<4, 1>(flux, kind, maps, a, nSM, st);

@@ -51,15 +51,20 @@ cudaError_t launch8_kind(int flux, const TmaMaps &maps, const StageArgs &a, int 
 }  // namespace
 
 cudaError_t launch_stage8(int flux, int kind, const TmaMaps &maps, const StageArgs &a, int nSM, cudaStream_t st) {
-  // FP64: one CTA of 512 threads per SM (the FP64 tile and face slots fill
-  // the shared memory).  FP32-bulk: stage 1 lands the FP64 state, one CTA
-  // of 512; stage 2 one CTA of 512 or, for stage_ctas_per_sm >= 2, two CTAs
-  // of 256 per SM, each on its own block
+  // FP64: one CTA per SM (the FP64 tile and face slots fill the shared
+  // memory) of 512 threads, or 576 (stage_variant 3: three face groups per
+  // warp, 96 registers).  FP32-bulk: one CTA of 512 per SM or, for
+  // stage_ctas_per_sm >= 2, two CTAs of 256, each on its own block
+  const bool two = tune_value(kTuneStageGrid) >= 2;
   switch (kind) {
-    case kKindFp64: return launch8_kind<512, 1, double, double, double>(flux, maps, a, nSM, st);
-    case kKindFp32In64: return launch8_kind<512, 1, double, float, float>(flux, maps, a, nSM, st);
+    case kKindFp64:
+      if (tune_value(kTuneStageVariant) == 3) return launch8_kind<576, 1, double, double, double>(flux, maps, a, nSM, st);
+      return launch8_kind<512, 1, double, double, double>(flux, maps, a, nSM, st);
+    case kKindFp32In64:
+      if (two) return launch8_kind<256, 2, double, float, float>(flux, maps, a, nSM, st);
+      return launch8_kind<512, 1, double, float, float>(flux, maps, a, nSM, st);
     case kKindFp32In32:
-      if (tune_value(kTuneStageGrid) >= 2) return launch8_kind<256, 2, float, float, double>(flux, maps, a, nSM, st);
+      if (two) return launch8_kind<256, 2, float, float, double>(flux, maps, a, nSM, st);
       return launch8_kind<512, 1, float, float, double>(flux, maps, a, nSM, st);
   }
   return cudaErrorInvalidValue;

@@ -7,11 +7,12 @@
 // the floors (ModUpdateState, ModEnergy) and the cell time step
 // (ModTimeStepControl).  The work of a block is organised for occupancy:
 //
-// * Shared memory holds a primitive tile P and one region R.  R is first
-//   the TMA landing area of the block's state (the interior box and six
-//   2-layer halo boxes, the layout of Tile3<8>), then the face-slot buffer
-//   of all three directions.
-// * The conversion pass reads R and writes P with one variable stride
+// * Shared memory holds a primitive tile P and the face-slot buffer of all
+//   three directions.  The TMA landing area of a block's state (the
+//   interior box and six 2-layer halo boxes, the layout of Tile3<8>) ends
+//   where the face slots end: it lies inside them for an FP64 tile, and
+//   reaches back into P for an FP32 tile of the FP64 state.
+// * The conversion pass reads the landing area and writes P with one variable stride
 //   (1280 cells per variable): the interior rows with their x ghost cells
 //   as rows of 12 (so an x stencil is base + m), then the y ghost rows, then
 //   the z ghost planes.
@@ -19,10 +20,11 @@
 //   faces w, w + nWarp, ... (18 groups per direction, the direction uniform
 //   in a warp) and writes the ten slots of each face into R.  No cell
 //   accumulator is live during the flux arithmetic.
-// * Then each thread sums the flux differences of its cell(s); after a
-//   barrier R is free and the next block's TMA loads are issued into it,
-//   overlapping the update of this block.
-// Five barriers per block; every mbarrier wait is bounded.
+// * Then each thread sums the flux differences of its cell(s) and reads
+//   its cells' u and B from P; after a barrier the next block's TMA loads
+//   are issued into the landing area, overlapping the update of this block.
+// Five barriers per block (six when the landing area reaches into P);
+// every mbarrier wait is bounded.
 #pragma once
 #include "bx_stage3d.cuh"
 
@@ -40,9 +42,16 @@ struct Blk8 {
   static constexpr size_t primBytes = sizeof(Real) * 8 * PV;
   static constexpr size_t fluxBytes = sizeof(Real) * 3 * NSLOT * NF;
   static constexpr size_t stageBytes = sizeof(TileT) * (size_t)ST::nAll;
-  static constexpr size_t regionBytes = fluxBytes > stageBytes ? fluxBytes : stageBytes;
-  static constexpr size_t smem_bytes = primBytes + regionBytes;
-  static_assert(primBytes % 128 == 0, "the TMA landing area must be 128-byte aligned");
+  // P, then the face slots; the landing area of the next block's state ends
+  // where the face slots end, reaching back into P when it is the larger
+  // (an FP64 state below an FP32 tile)
+  static constexpr size_t smem_bytes =
+      primBytes + fluxBytes > stageBytes ? primBytes + fluxBytes : stageBytes;
+  static constexpr size_t stageOff = smem_bytes - stageBytes;
+  // variables of P at and above vDefer share bytes with the landing area:
+  // the conversion writes them after every thread has read its cells
+  static constexpr int vDefer = stageOff >= primBytes ? 8 : (int)(stageOff / (sizeof(Real) * PV));
+  static_assert(primBytes % 128 == 0 && stageOff % 128 == 0, "the TMA landing area must be 128-byte aligned");
   static_assert(NTHR % 32 == 0, "whole warps");
 };
 
@@ -209,9 +218,8 @@ __global__ void __launch_bounds__(B::NTHR, B::MINB)
   using ST = typename B::ST;
   extern __shared__ __align__(128) unsigned char smem_raw[];
   Real *P = reinterpret_cast<Real *>(smem_raw);
-  unsigned char *region = smem_raw + B::primBytes;
-  TileT *stg = reinterpret_cast<TileT *>(region);
-  Real *fb = reinterpret_cast<Real *>(region);
+  TileT *stg = reinterpret_cast<TileT *>(smem_raw + B::stageOff);
+  Real *fb = reinterpret_cast<Real *>(smem_raw + B::primBytes);
   __shared__ uint64_t bar;
   __shared__ double wmin[B::NW];
   __shared__ BlkMeta meta[2];
@@ -241,18 +249,24 @@ __global__ void __launch_bounds__(B::NTHR, B::MINB)
     __syncthreads();  // (A) the block's state has landed in R
     if (sTimeout) break;  // uniform: every thread read the flag after the barrier
     const int b = M.b;
-    int nb[6];
+    int floatMask = 0, rcMask = 0;
 #pragma unroll
-    for (int s = 0; s < 6; s++) nb[s] = M.nb[s];
+    for (int s = 0; s < 6; s++) {
+      floatMask |= (M.nb[s] == kNbrFloat) << s;
+      rcMask |= (M.nb[s] == kNbrResChange) << s;
+    }
     const int rcFine = M.rcFine, rcCoarse = M.rcCoarse;
 
-    // ---- calc_primitives: R (conservative) -> P (primitive) -------------
-#pragma unroll 1
-    for (int c = t; c < B::PV; c += B::NTHR) {
+    // ---- calc_primitives: landing area (conservative) -> P (primitive) ---
+    Real defer[B::CCV][8];
+#pragma unroll
+    for (int q = 0; q < B::CCV; q++) {
+      const int c = t + q * B::NTHR;
+      if (c >= B::PV) continue;
       int i, j, k, side;
       p8_cell(c, i, j, k, side);
       TileT w[8];
-      if (side >= 0 && nb[side] == kNbrResChange) {
+      if (side >= 0 && ((rcMask >> side) & 1)) {
         // ghost layers of a resolution-change side: its slab
         // [var][layer][t1][t0] (injection / restriction, bx_amr.cu)
         const int d = side >> 1, hi = side & 1;
@@ -264,7 +278,7 @@ __global__ void __launch_bounds__(B::NTHR, B::MINB)
         for (int v = 0; v < 8; v++) w[v] = (TileT)src[v * 128];
       } else {
         int si = i, sj = j, sk = k;
-        if (side >= 0 && nb[side] == kNbrFloat) {  // float boundary: copy of the boundary cell
+        if (side >= 0 && ((floatMask >> side) & 1)) {  // float boundary: copy of the boundary cell
           if (side == 0) si = 0;
           if (side == 1) si = 7;
           if (side == 2) sj = 0;
@@ -287,7 +301,20 @@ __global__ void __launch_bounds__(B::NTHR, B::MINB)
       w[kUy] = rhoInv * w[kUy];
       w[kUz] = rhoInv * w[kUz];
 #pragma unroll
-      for (int v = 0; v < 8; v++) P[c + v * B::PV] = (Real)w[v];
+      for (int v = 0; v < 8; v++) {
+        if (v < B::vDefer) P[c + v * B::PV] = (Real)w[v];
+        else defer[q][v] = (Real)w[v];
+      }
+    }
+    if (B::vDefer < 8) {
+      __syncthreads();  // every cell of the landing area is read
+#pragma unroll
+      for (int q = 0; q < B::CCV; q++) {
+        const int c = t + q * B::NTHR;
+        if (c >= B::PV) continue;
+#pragma unroll
+        for (int v = B::vDefer; v < 8; v++) P[c + v * B::PV] = defer[q][v];
+      }
     }
     __syncthreads();  // (B) P is complete; R becomes the face-slot buffer
 
@@ -317,11 +344,16 @@ __global__ void __launch_bounds__(B::NTHR, B::MINB)
 
     // ---- flux differences per cell (and StateOld, loaded early) ----------
     constexpr bool kFloatFlux = sizeof(Real) == sizeof(float);
-    double chg[B::CPC][8], divB[B::CPC], vdt[B::CPC], o[B::CPC][8];
+    double chg[B::CPC][8], divB[B::CPC], vdt[B::CPC], o[B::CPC][8], ub[B::CPC][6];
 #pragma unroll
     for (int r = 0; r < B::CPC; r++) {
       const int c = t + r * B::NTHR;
       if (c >= B::NC) continue;
+      {  // u and B of the cell for the Powell source (P is overwritten after (D))
+        const int c0 = p8(c & 7, (c >> 3) & 7, c >> 6);
+#pragma unroll
+        for (int q = 0; q < 6; q++) ub[r][q] = P[c0 + (kUx + q) * B::PV];
+      }
       if (!a.outputResidual) {
         const double *old = a.old + (size_t)b * 8 * B::NC;
 #pragma unroll
@@ -350,7 +382,7 @@ __global__ void __launch_bounds__(B::NTHR, B::MINB)
         }
       }
     }
-    __syncthreads();  // (D) R is free: the next block's state streams into it
+    __syncthreads();  // (D) the face slots and P are read: the next block's state streams in
     if (t == 0 && it + 1 < nIter) {
       fence_proxy_async_smem();
       const BlkMeta &Mn = meta[(it + 1) & 1];
@@ -364,11 +396,10 @@ __global__ void __launch_bounds__(B::NTHR, B::MINB)
     for (int r = 0; r < B::CPC; r++) {
       const int cc = t + r * B::NTHR;
       if (cc >= B::NC) continue;
-      const int c0 = p8(cc & 7, (cc >> 3) & 7, cc >> 6);
       double src[8] = {0, 0, 0, 0, 0, 0, 0, 0};
       if (a.useDivb) {
-        const double ux = P[c0 + kUx * B::PV], uy = P[c0 + kUy * B::PV], uz = P[c0 + kUz * B::PV];
-        const double bx = P[c0 + kBx * B::PV], by = P[c0 + kBy * B::PV], bz = P[c0 + kBz * B::PV];
+        const double ux = ub[r][0], uy = ub[r][1], uz = ub[r][2];
+        const double bx = ub[r][3], by = ub[r][4], bz = ub[r][5];
         src[kBx] = -divB[r] * ux; src[kBy] = -divB[r] * uy; src[kBz] = -divB[r] * uz;
         src[kE] = -divB[r] * (bx * ux + by * uy + bz * uz);
         src[kUx] = -divB[r] * bx; src[kUy] = -divB[r] * by; src[kUz] = -divB[r] * bz;
@@ -411,7 +442,7 @@ __global__ void __launch_bounds__(B::NTHR, B::MINB)
       for (int off = 16; off > 0; off >>= 1) dtmin = fmin(dtmin, __shfl_xor_sync(0xffffffffu, dtmin, off));
       if (lane == 0) wmin[warp] = dtmin;
     }
-    __syncthreads();  // (E) P is read; the next conversion may overwrite it
+    __syncthreads();  // (E) wmin is complete
     if (a.computeDt && t == 0) {
       double m = wmin[0];
       for (int w = 1; w < B::NW; w++) m = fmin(m, wmin[w]);

@@ -16,8 +16,8 @@ enum TuneKnob {
   kTuneKryUnroll,      // Krylov MGS step: independent 16-byte loads in flight per thread and vector
   kTuneHeatIluWarps,   // heat ILU sweeps: warps (groups of 32 blocks) per CTA
   kTuneBiluThreads,    // JFNK BILU sweeps: threads per block CTA (8 per cell of a wavefront)
-  kTuneStageVariant,   // stage kernel, 8^3 blocks: 0 one face phase (512 threads); one direction at a
-                       // time with 1: one face per thread (576 threads), 2: two faces per thread (288)
+  kTuneStageVariant,   // stage kernel, 8^3 blocks: 0 one face phase (FP64: 512 threads, 3: 576); one
+                       // direction at a time with 1: one face per thread (576 threads), 2: two (288)
   kTuneKryGsSteps,     // Gram-Schmidt steps per pass over w (1 to 4); set, not timed
   kNumTune
 };

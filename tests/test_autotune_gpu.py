@@ -62,7 +62,7 @@ def test_stage_variants_agree(prec):
             x.close()
         # the instantiations may contract multiply-adds differently, so the
         # variants agree to rounding
-        for f in (0, 2):
+        for f in (0, 2, 3):
             a, b = out[(name, f)][0], out[(name, 1)][0]
             rel = np.abs(a - b).max() / np.abs(b).max()
             assert rel <= (1e-13 if prec == "fp64" else 1e-5), (name, f, rel)
