@@ -145,6 +145,8 @@ class SchemeParams(ctypes.Structure):
         ("Precision", ctypes.c_int),
         ("RhoMin", ctypes.c_double), ("pMin", ctypes.c_double), ("TMin", ctypes.c_double),
         ("MassIon", ctypes.c_double),
+        ("UseTvdResChange", ctypes.c_int), ("BetaLimiterResChange", ctypes.c_double),
+        ("nFaceLimiterResChange", ctypes.c_int),
     ]
 
 
@@ -262,6 +264,9 @@ def scheme_params(s):
     p.pMin = getattr(s, "pMin", -1.0)
     p.TMin = getattr(s, "tMin", -1.0)
     p.MassIon = getattr(s, "massIon", 1.0)
+    p.UseTvdResChange = int(getattr(s, "useTvdResChange", True))
+    p.BetaLimiterResChange = getattr(s, "betaLimiterResChange", 2.0)
+    p.nFaceLimiterResChange = getattr(s, "nFaceLimiterResChange", 2)
     return p
 
 

@@ -2,16 +2,22 @@
 // each stage launch:
 //
 //   k_rc_ghost  the two ghost layers of every block side that borders a
-//               block of another level (BATL message_pass_cell with
-//               nProlongOrder = 1): a coarser neighbour's cell is copied into
-//               the finer ghost cells it covers, a finer neighbour's 2x2x2
-//               cells are averaged into the coarse ghost cell
+//               block of another level, as BATL message_pass_cell fills them
+//               for exchange_messages with nProlongOrder = 1
+//               (src/ModMessagePass.f90:176-210): a coarser neighbour's cell
+//               is copied into the finer ghost cells it covers (injection),
+//               with two coarse layers (the outer ghost layer takes the next
+//               coarse cell) when the faces at resolution changes are TVD;
+//               a coarse ghost cell takes the mean of the 2x2 finer cells
+//               next to its face toward the block (DoRestrictFace), then,
+//               with TVD faces, correct_monotone_restrict
+//               (src/ModFaceValue.f90:233-408)
 //   k_rc_flux   save_cons_flux + message_pass_face: for every face of a
-//               coarse block next to finer blocks, the sum of the first-order
-//               fluxes (src/ModFaceValue.f90:1118-1137, get_faceX_first) of
-//               the 2x2 finer faces, their Vdt and their normal fields times
-//               FaceRatio = 1/4 (src/ModConserveFlux.f90:79-265), computed
-//               with the stage kernel's own primitive conversion and
+//               coarse block next to finer blocks, the sum of the fluxes of
+//               the 2x2 finer faces (tvd_reschange states, or the first-order
+//               states of get_faceX_first), their Vdt and their normal fields
+//               times FaceRatio = 1/4 (src/ModConserveFlux.f90:79-265),
+//               computed with the stage kernel's own primitive conversion and
 //               face_slots so that the coarse side and the finer blocks see
 //               the same fluxes
 //
@@ -29,14 +35,18 @@ __device__ __forceinline__ long gidx(const int *lc, int blk, int e, int N, int x
 }
 
 // state value (variable v) of the ghost cell x3 (block-local coordinates,
-// x3[d] = -1 - l or N + l) across the resolution-change side S: a coarser
-// neighbour's cell copied into the finer ghost cells it covers (injection),
-// or the mean of the 2x2x2 finer cells in a fixed order (restriction)
+// x3[d] = -1 - l or N + l) across the resolution-change side S, as
+// exchange_messages leaves it: a coarser neighbour's cell copied into the
+// finer ghost cells it covers (injection; with twoLayers the outer layer
+// l = 1 takes the next coarse cell), or the mean of the 2x2 finer cells next
+// to the face of the ghost cell toward the block, in a fixed order
+// (DoRestrictFace restriction).  The outer coarse ghost layer only enters
+// the resolution-change face, whose slots the summed finer fluxes replace.
 template <int N, typename InT>
 __device__ __forceinline__ double rc_ghost_value(const InT *in, const RcSlab &S, const int *lc, const int nr[3],
-                                                 const int x3[3], int v) {
+                                                 const int x3[3], int v, bool twoLayers) {
   constexpr int NC = N * N * N;
-  const int d = S.side >> 1;
+  const int d = S.side >> 1, hi = S.side & 1;
   const int e0 = d == 0 ? 1 : 0, e1 = d == 2 ? 1 : 2;
   const int lev = lc[4 * S.block];
   if (S.type == 1) {
@@ -48,6 +58,7 @@ __device__ __forceinline__ double rc_ghost_value(const InT *in, const RcSlab &S,
       gf = (gf + tot) % tot;
       c3[e] = (int)((gf >> 1) - (long)lc[4 * C + 1 + e] * N);
     }
+    if (twoLayers && (hi ? x3[d] - N : -1 - x3[d]) == 1) c3[d] += hi ? 1 : -1;
     return (double)in[((size_t)C * 8 + v) * NC + c3[0] + N * (c3[1] + N * c3[2])];
   }
   // the finer neighbour covering this transverse quadrant
@@ -58,30 +69,61 @@ __device__ __forceinline__ double rc_ghost_value(const InT *in, const RcSlab &S,
     const long gc = (gidx(lc, S.block, e, N, x3[e]) + tot) % tot;
     f0[e] = 2 * gc - (long)lc[4 * F + 1 + e] * N;
   }
+  f0[d] += hi ? 0 : 1;
   double sum = 0.0;
-  for (int kk = 0; kk < 2; kk++)
-    for (int jj = 0; jj < 2; jj++)
-      for (int ii = 0; ii < 2; ii++)
-        sum = sum + (double)in[((size_t)F * 8 + v) * NC + (f0[0] + ii) + N * ((f0[1] + jj) + N * (f0[2] + kk))];
-  return sum * 0.125;
+  for (int u1 = 0; u1 < 2; u1++)
+    for (int u0 = 0; u0 < 2; u0++) {
+      long g3[3] = {f0[0], f0[1], f0[2]};
+      g3[e0] += u0;
+      g3[e1] += u1;
+      sum = sum + (double)in[((size_t)F * 8 + v) * NC + g3[0] + N * (g3[1] + N * g3[2])];
+    }
+  return sum * 0.25;
 }
 
+// one thread per ghost cell of the slab (both layers), all variables; the
+// slab layout is [var][layer][t1][t0]
 template <int N, typename InT>
 __global__ void k_rc_ghost(const InT *__restrict__ in, const RcSlab *__restrict__ slabs, const int *__restrict__ lc,
-                           int3 nRoot, double *ghost) {
+                           int3 nRoot, double *ghost, int tvd) {
+  constexpr int NC = N * N * N;
   const RcSlab S = slabs[blockIdx.x];
   const int d = S.side >> 1, hi = S.side & 1;
   const int e0 = d == 0 ? 1 : 0, e1 = d == 2 ? 1 : 2;
   const int nr[3] = {nRoot.x, nRoot.y, nRoot.z};
   constexpr int nSlab = 8 * 2 * N * N;
   double *out = ghost + (size_t)blockIdx.x * nSlab;
-  for (int q = threadIdx.x; q < nSlab; q += blockDim.x) {
-    const int t0 = q % N, t1 = (q / N) % N, l = (q / (N * N)) % 2, v = q / (2 * N * N);
+  for (int q = threadIdx.x; q < 2 * N * N; q += blockDim.x) {
+    const int t0 = q % N, t1 = (q / N) % N, l = q / (N * N);
     int x3[3];
     x3[d] = hi ? N + l : -1 - l;
     x3[e0] = t0;
     x3[e1] = t1;
-    out[q] = rc_ghost_value<N>(in, S, lc, nr, x3, v);
+    double w[8];
+#pragma unroll
+    for (int v = 0; v < 8; v++) w[v] = rc_ghost_value<N>(in, S, lc, nr, x3, v, tvd != 0);
+    if (tvd && S.type == -1 && l == 0) {
+      // correct_monotone_restrict: G + (G - C1)/3 in the primitive form, C1
+      // the block's cell next to the ghost cell; density and pressure at
+      // least 1e-30 (DefaultState_V > 0)
+      int c3[3] = {x3[0], x3[1], x3[2]};
+      c3[d] = hi ? N - 1 : 0;
+      double q1[8];
+#pragma unroll
+      for (int v = 0; v < 8; v++) q1[v] = (double)in[((size_t)S.block * 8 + v) * NC + c3[0] + N * (c3[1] + N * c3[2])];
+      const double invG = 1.0 / w[kRho], invC = 1.0 / q1[kRho];
+#pragma unroll
+      for (int v = kUx; v <= kUz; v++) { w[v] = w[v] * invG; q1[v] = q1[v] * invC; }
+      const double cThird = 1.0 / 3.0;
+#pragma unroll
+      for (int v = 0; v < 8; v++) w[v] = w[v] + cThird * (w[v] - q1[v]);
+      w[kRho] = fmax(w[kRho], 1e-30);
+      w[kP] = fmax(w[kP], 1e-30);
+#pragma unroll
+      for (int v = kUx; v <= kUz; v++) w[v] = w[v] * w[kRho];
+    }
+#pragma unroll
+    for (int v = 0; v < 8; v++) out[((v * 2 + l) * N + t1) * N + t0] = w[v];
   }
 }
 
@@ -114,29 +156,47 @@ __device__ __forceinline__ void rc_face_sum(const StageArgs &a, const RcSlab &S,
     x3[D == 2 ? 1 : 2] = u1;
     return x3[0] + N * (x3[1] + N * x3[2]);
   };
-  Real Pc[8];
+  // the coarse cell next to the face (the finer block's first coarse ghost
+  // layer) and, for the TVD faces, the coarse cell beyond it and the finer
+  // block's 2x2 cells next to the face and behind them
+  Real Pc[8], Pc2[8], F1[4][8], F2[4][8];
   rc_prim<N, TileT, Real>(in, S.block, cell(hi ? N - 1 : 0, t0, t1), Pc);
+  const bool tvd = a.tvdRc != 0;
+  if (tvd) rc_prim<N, TileT, Real>(in, S.block, cell(hi ? N - 2 : 1, t0, t1), Pc2);
+#pragma unroll
+  for (int u = 0; u < 4; u++) {
+    rc_prim<N, TileT, Real>(in, F, cell(hi ? 0 : N - 1, a0 + (u & 1), a1 + (u >> 1)), F1[u]);
+    if (tvd) rc_prim<N, TileT, Real>(in, F, cell(hi ? 1 : N - 2, a0 + (u & 1), a1 + (u >> 1)), F2[u]);
+  }
+  const Real beta = (Real)fmin(a.betaRc, a.beta);
   const Real area = (Real)a.geom[F].area[D];
   double sum[kRcSlots] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
   double bnL = 0.0, bnR = 0.0;
   bool ok = true;
-  for (int u1 = 0; u1 < 2; u1++)
-    for (int u0 = 0; u0 < 2; u0++) {
-      Real Pf[8], L[8], R[8], o[kRcSlots];
-      rc_prim<N, TileT, Real>(in, F, cell(hi ? 0 : N - 1, a0 + u0, a1 + u1), Pf);
+  for (int u = 0; u < 4; u++) {
+    Real L[8], R[8], o[kRcSlots];
 #pragma unroll
-      for (int v = 0; v < 8; v++) {
-        L[v] = hi ? Pc[v] : Pf[v];
-        R[v] = hi ? Pf[v] : Pc[v];
+    for (int v = 0; v < 8; v++) {
+      Real c = Pc[v], f = F1[u][v];  // first-order states: the cell values
+      if (tvd) {
+        Real ff;
+        tvd_reschange_var<Real>(Pc[v], Pc2[v], F1[0][v], F1[1][v], F1[2][v], F1[3][v], F1[u][v], F2[u][v], beta, c,
+                                f, ff);
       }
-      // first-order faces: the face states are the cell values
-      ok = face_slots<D, FLUX, Real>(L, R, (Real)a.gamma, (Real)a.invGm1, area, o, 1, L[kBx + D], R[kBx + D],
-                                     L[kUx + D], R[kUx + D]) && ok;
-#pragma unroll
-      for (int m = 0; m < 9; m++) sum[m] = sum[m] + (double)o[m];
-      bnL = bnL + (double)L[kBx + D] * 0.25;
-      bnR = bnR + (double)R[kBx + D] * 0.25;
+      // the coarse side is on the left of the face when the finer block
+      // lies on the coarse block's high side
+      L[v] = hi ? c : f;
+      R[v] = hi ? f : c;
     }
+    ok = face_slots<D, FLUX, Real>(L, R, (Real)a.gamma, (Real)a.invGm1, area, o, 1,
+                                   hi ? Pc[kBx + D] : F1[u][kBx + D], hi ? F1[u][kBx + D] : Pc[kBx + D],
+                                   hi ? Pc[kUx + D] : F1[u][kUx + D], hi ? F1[u][kUx + D] : Pc[kUx + D]) &&
+         ok;
+#pragma unroll
+    for (int m = 0; m < 9; m++) sum[m] = sum[m] + (double)o[m];
+    bnL = bnL + (double)L[kBx + D] * 0.25;
+    bnR = bnR + (double)R[kBx + D] * 0.25;
+  }
   sum[9] = bnL + bnR;
 #pragma unroll
   for (int m = 0; m < kRcSlots; m++) out[m] = sum[m];
@@ -161,7 +221,8 @@ __global__ void k_rc_flux(const StageArgs a, const RcSlab *__restrict__ slabs, d
 template <int N, typename TileT, typename Real>
 static cudaError_t rc_launch(int flux, const StageArgs &a, const RcSlab *slabs, int nSlab, const int *lc, int3 nRoot,
                              double *ghost, double *fluxBuf, cudaStream_t st) {
-  k_rc_ghost<N, TileT><<<nSlab, 256, 0, st>>>(reinterpret_cast<const TileT *>(a.in), slabs, lc, nRoot, ghost);
+  k_rc_ghost<N, TileT><<<nSlab, 2 * N * N, 0, st>>>(reinterpret_cast<const TileT *>(a.in), slabs, lc, nRoot, ghost,
+                                                    a.tvdRc);
   switch (flux) {
     case kFluxRusanov: k_rc_flux<N, TileT, Real, kFluxRusanov><<<nSlab, N * N, 0, st>>>(a, slabs, fluxBuf); break;
     case kFluxLinde: k_rc_flux<N, TileT, Real, kFluxLinde><<<nSlab, N * N, 0, st>>>(a, slabs, fluxBuf); break;
@@ -233,8 +294,8 @@ __global__ void __launch_bounds__(N * N * N) k_amr_crit(AmrCritArgs a) {
           x3[d] = side ? N - 1 : 0;
         } else {
           const RcSlab S = a.slabs[a.rcSlab[6 * b + s]];
-          rho[m] = rc_ghost_value<N>(a.in, S, a.lc, nr, x3, kRho);
-          p[m] = rc_ghost_value<N>(a.in, S, a.lc, nr, x3, kP);
+          rho[m] = rc_ghost_value<N>(a.in, S, a.lc, nr, x3, kRho, false);
+          p[m] = rc_ghost_value<N>(a.in, S, a.lc, nr, x3, kP, false);
           continue;
         }
       }
@@ -288,7 +349,7 @@ __global__ void __launch_bounds__(N * N * N) k_amr_crit(AmrCritArgs a) {
 
 // new block b from the old state: a copy, the injection from its parent
 // (octant a + 2 b + 4 c of the parent), or the mean of the 2x2x2 cells of
-// its eight children (in the order of rc_ghost_value)
+// its eight children (x fastest, then y, then z)
 template <int N>
 __global__ void k_amr_remap(const double *__restrict__ in, double *__restrict__ out, const int *__restrict__ remap) {
   constexpr int NC = N * N * N;

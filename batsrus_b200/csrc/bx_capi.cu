@@ -302,6 +302,11 @@ int check_scheme(const bx_scheme_params *s) {
   if (s->Gamma <= 1.0) return fail(BX_ERR_ARG, "Gamma must exceed 1");
   if (s->Cfl <= 0.0) return fail(BX_ERR_ARG, "Cfl must be positive");
   if (s->MassIon < 0.0) return fail(BX_ERR_ARG, "MassIon must not be negative");
+  if (s->BetaLimiterResChange > 0.0 && s->BetaLimiterResChange < s->LimiterBeta && s->nOrder > 1 &&
+      s->nFaceLimiterResChange > 0 && g.shape != kShape888 && g.shape != kShape444)
+    return fail(BX_ERR_ARG, "BetaLimiterResChange below LimiterBeta is supported on 3D blocks only");
+  if (s->BetaLimiterResChange > 0.0 && s->nFaceLimiterResChange < 0)
+    return fail(BX_ERR_ARG, "nFaceLimiterResChange=%d", s->nFaceLimiterResChange);
   if (s->Precision == BX_FP32_BULK) {
     if (g.shape != kShape888 && g.shape != kShape444)
       return fail(BX_ERR_ARG, "FP32-bulk mode needs 3D 8x8x8 or 4x4x4 blocks");
@@ -321,6 +326,15 @@ Floors floors() {
   return f;
 }
 
+// #RESOLUTIONCHANGE of the scheme: TVD faces at resolution changes of 3D
+// grids at second order; BetaLimiterResChange <= 0 means 2.0 with 2 faces
+void set_reschange(StageArgs &a) {
+  a.tvdRc = g.sch.UseTvdResChange && g.sch.nOrder > 1 && g.use3d;
+  const bool set = g.sch.BetaLimiterResChange > 0.0;
+  a.betaRc = set ? g.sch.BetaLimiterResChange : 2.0;
+  a.nFaceRc = set ? g.sch.nFaceLimiterResChange : 2;
+}
+
 StageArgs stage_args(int iStage, bool computeDt) {
   StageArgs a;
   a.nbr = g.nbr; a.order = g.order; a.geom = g.geom; a.ts = g.ts; a.dtBlock = g.dtBlock;
@@ -330,6 +344,7 @@ StageArgs stage_args(int iStage, bool computeDt) {
   a.beta = g.sch.LimiterBeta; a.gamma = g.sch.Gamma; a.invGm1 = 1.0 / (g.sch.Gamma - 1.0);
   a.cfl = g.sch.Cfl;
   a.fl = floors();
+  set_reschange(a);
   a.old = g.A;
   if (g.nSlab) {
     a.rcType = g.rcType; a.rcSlab = g.rcSlab; a.rcGhost = g.rcGhost; a.rcFlux = g.rcFlux;
@@ -527,6 +542,9 @@ int compat_phase(int phase, int iBlock) {
   if (g.nSlab) return fail(BX_ERR_ARG, "the per-block entry points work on single-level grids");
   if (iBlock < 1 || iBlock > g.nBlock) return fail(BX_ERR_ARG, "iBlock=%d out of range 1..%d", iBlock, g.nBlock);
   if (g.sch.TypeFlux == BX_FLUX_ROE) return fail(BX_ERR_ARG, "the per-block entry points have no Roe flux");
+  if (g.sch.BetaLimiterResChange > 0.0 && g.sch.BetaLimiterResChange < g.sch.LimiterBeta && g.sch.nOrder > 1 &&
+      g.sch.nFaceLimiterResChange > 0)
+    return fail(BX_ERR_ARG, "the per-block entry points have no BetaLimiterResChange below LimiterBeta");
   int r = ensure_compat();
   if (r) return r;
   cudaError_t e = launch_compat(g.shape, g.sch.TypeFlux, phase, iBlock - 1, compat_args(), g.st);

@@ -70,6 +70,12 @@ struct StageArgs {
   const double *rcGhost = nullptr;
   const double *rcFlux = nullptr;
   Floors fl;
+  // #RESOLUTIONCHANGE: TVD faces next to a coarser block (tvd_reschange),
+  // and BetaLimiterResChange for the nFaceRc cells next to a side with a
+  // resolution change or an outer boundary when it is below beta
+  int tvdRc = 0;
+  double betaRc = 2.0;
+  int nFaceRc = 2;
 };
 
 constexpr int kNbrFloat = -1, kNbrResChange = -2;

@@ -100,6 +100,57 @@ __device__ __forceinline__ void limited_face_t(R beta, R q0, R q1, R q2, R q3, R
   right = q2 - dR;
 }
 
+// limited_face_t with separate Beta for the two cells of the face: betaL for
+// the left cell (q1), betaR for the right cell (q2), as get_facex_second
+// uses BetaLimiterResChange for the cells next to a resolution change
+// (src/ModFaceValue.f90:1979-2014)
+template <int LIM, typename R>
+__device__ __forceinline__ void limited_face_t2(R betaL, R betaR, R q0, R q1, R q2, R q3, R &left, R &right) {
+  const R a = q1 - q0, b = q2 - q1, c = q3 - q2;
+  const R sab = sign25(a) + sign25(b);
+  const R sbc = sign25(b) + sign25(c);
+  R dL, dR;
+  if (LIM == kLimMinmod) {
+    dL = sab * fmin(fabs(a), fabs(b));
+    dR = sbc * fmin(fabs(b), fabs(c));
+  } else if (LIM == kLimMc) {
+    dL = sab * fmin(fmin(betaL * fabs(a), betaL * fabs(b)), R(0.5) * fabs(a + b));
+    dR = sbc * fmin(fmin(betaR * fabs(b), betaR * fabs(c)), R(0.5) * fabs(b + c));
+  } else {
+    const R cThird = R(1) / R(3);
+    dL = sab * fmin(fmin(betaL * fabs(a), betaL * fabs(b)), cThird * fabs(a + 2 * b));
+    dR = sbc * fmin(fmin(betaR * fabs(b), betaR * fabs(c)), cThird * fabs(2 * b + c));
+  }
+  left = q1 + dL;
+  right = q2 - dR;
+}
+
+// tvd_reschange (src/ModFaceValue.f90:2269-2343) for one variable of one
+// fine face next to a coarser block: c1, c2 the two coarse ghost cells
+// (next to the face and beyond), f00..f11 the 2x2 fine cells next to the
+// face (first transverse index fastest), own1 / own2 this face's fine cell
+// and the one behind it, beta = min(BetaLimiterResChange, LimiterBeta).
+// Returns the state in the coarse ghost cell at the face (CoarseToFineF),
+// the state of the fine cell at the face (FineToCoarseF) and the fine
+// cell's state at its other face (FineF).
+template <typename R>
+__device__ __forceinline__ void tvd_reschange_var(R c1, R c2, R f00, R f10, R f01, R f11, R own1, R own2, R beta,
+                                                  R &cToF, R &fToC, R &ff) {
+  const R cThird = R(1) / R(3), cTwoThird = R(2) / R(3), cSixth = R(1) / R(6);
+  const R avg = R(0.25) * (((f00 + f10) + f01) + f11);
+  const R grad = avg - c1;
+  const R sg = copysign(R(1), grad);
+  const R gradLtd = sg * fmax(R(0), fmin(fmin(beta * cTwoThird * fabs(grad), beta * R(0.5) * sg * (c1 - c2)),
+                                        cThird * fabs(grad) + R(0.25) * sg * (c1 - c2)));
+  const R dT = own1 - avg;
+  cToF = c1 + gradLtd + copysign(fmin(fabs(gradLtd), fabs(dT)), dT);
+  const R gf = sg * fmax(R(0), fmin(fmin(sg * (own1 - c1), beta * cThird * fabs(grad)),
+                                   fmin(beta * R(0.5) * sg * (own2 - own1),
+                                        cSixth * fabs(grad) + R(0.25) * sg * (own2 - own1))));
+  fToC = own1 - gf;
+  ff = own1 + gf;
+}
+
 // get_physical_flux -> get_mhd_flux -> get_magnetic_flux
 // (src/ModFaceFlux.f90:1166-1410, 1550-1617, 1619-1900)
 template <int D, typename R>
@@ -139,15 +190,15 @@ __device__ __forceinline__ void physical_flux(const R (&S)[8], R invGm1, R (&U)[
 template <int D, typename R>
 __device__ __forceinline__ void mhd_speed(const R (&S)[8], R gamma, R &cmax, R &cleft, R &cright) {
   const R rho = S[kRho];
-  const R sound2 = S[kP] * gamma / rho;
+  const R sound2 = fdiv(S[kP] * gamma, rho);
   const R un = S[kUx + D];
-  const R invRho = R(1) / rho;
+  const R invRho = frcp(rho);
   const R alfven2 = (S[kBx] * S[kBx] + S[kBy] * S[kBy] + S[kBz] * S[kBz]) * invRho;
   const R bn = S[kBx + D];
   const R alfven2n = invRho * (bn * bn);
   const R fast2 = sound2 + alfven2;
-  const R discr = sqrt(fmax(R(0), fast2 * fast2 - R(4) * sound2 * alfven2n));
-  const R fast = sqrt(R(0.5) * (fast2 + discr));
+  const R discr = fsqrt(fmax(R(0), fast2 * fast2 - R(4) * sound2 * alfven2n));
+  const R fast = fsqrt(R(0.5) * (fast2 + discr));
   cmax = fabs(un) + fast;
   cleft = un - fast;
   cright = un + fast;
@@ -186,20 +237,20 @@ __device__ __forceinline__ bool hlld_flux(const R (&L)[8], const R (&Rt)[8], R g
   const R PtotL = pL + PbL, PtotR = pR + PbR;
   const R DsL = sL - UnL, DsR = sR - UnR;
   const R DsRhoL = DsL * RhoL, DsRhoR = DsR * RhoR;
-  R Tmp = R(1) / (DsRhoR - DsRhoL);
+  R Tmp = frcp(DsRhoR - DsRhoL);
   const R Un = (DsRhoR * UnR - DsRhoL * UnL - PtotR + PtotL) * Tmp;
   const R Ptot12 = (DsRhoR * PtotL - DsRhoL * PtotR + DsRhoR * DsRhoL * (UnR - UnL)) * Tmp;
   R Rho, Ut1, Ut2, B1t1, B1t2, uDotB1, e;
   R Ut1L1, Ut2L1, B1t1L1, B1t2L1, Ut1R1, Ut2R1, B1t1R1, B1t2R1;
   bool ok = true;
   if (Un >= R(0)) {
-    const R InvSLUn = R(1) / (sL - Un);
+    const R InvSLUn = frcp(sL - Un);
     Rho = DsRhoL * InvSLUn;
     Tmp = DsRhoL * (sL - Un) - Bn2;
     if (Tmp < cTiny) {
       Ut1L1 = Ut1L; Ut2L1 = Ut2L; B1t1L1 = B1t1L; B1t2L1 = B1t2L;
     } else {
-      Tmp = R(1) / Tmp;
+      Tmp = frcp(Tmp);
       Ut1L1 = Ut1L - Bn * B1t1L * (Un - UnL) * Tmp;
       Ut2L1 = Ut2L - Bn * B1t2L * (Un - UnL) * Tmp;
       B1t1L1 = B1t1L * (DsRhoL * DsL - Bn2) * Tmp;
@@ -209,25 +260,25 @@ __device__ __forceinline__ bool hlld_flux(const R (&L)[8], const R (&Rt)[8], R g
     const R uDotB1L = UnL * B1n + Ut1L * B1t1L + Ut2L * B1t2L;
     const R uDotB1L1 = Un * B1n + Ut1L1 * B1t1L1 + Ut2L1 * B1t2L1;
     e = (DsL * eL - PtotL * UnL + Ptot12 * Un + Bn * (uDotB1L - uDotB1L1)) * InvSLUn;
-    const R SqRhoL1 = sqrt(Rho);
-    const R sL1 = Un - fabs(Bn) / SqRhoL1;
+    const R SqRhoL1 = fsqrt(Rho);
+    const R sL1 = Un - fdiv(fabs(Bn), SqRhoL1);
     if (sL1 >= R(0)) {
       Ut1 = Ut1L1; Ut2 = Ut2L1; B1t1 = B1t1L1; B1t2 = B1t2L1; uDotB1 = uDotB1L1;
     } else {
-      const R ratio = DsRhoR / (sR - Un);
+      const R ratio = fdiv(DsRhoR, sR - Un);
       if (ratio < R(0)) ok = false;
-      const R SqRhoR1 = sqrt(fabs(ratio));
+      const R SqRhoR1 = fsqrt(fabs(ratio));
       Tmp = DsRhoR * (sR - Un) - Bn2;
       if (Tmp < cTiny) {
         Ut1R1 = Ut1R; Ut2R1 = Ut2R; B1t1R1 = B1t1R; B1t2R1 = B1t2R;
       } else {
-        Tmp = R(1) / Tmp;
+        Tmp = frcp(Tmp);
         Ut1R1 = Ut1R - Bn * B1t1R * (Un - UnR) * Tmp;
         Ut2R1 = Ut2R - Bn * B1t2R * (Un - UnR) * Tmp;
         B1t1R1 = B1t1R * (DsRhoR * DsR - Bn2) * Tmp;
         B1t2R1 = B1t2R * (DsRhoR * DsR - Bn2) * Tmp;
       }
-      Tmp = R(1) / (SqRhoL1 + SqRhoR1);
+      Tmp = frcp(SqRhoL1 + SqRhoR1);
       const R SqRhoLR1 = SqRhoL1 * SqRhoR1 * SignBn;
       Ut1 = (SqRhoL1 * Ut1L1 + SqRhoR1 * Ut1R1 + (B1t1R1 - B1t1L1) * SignBn) * Tmp;
       Ut2 = (SqRhoL1 * Ut2L1 + SqRhoR1 * Ut2R1 + (B1t2R1 - B1t2L1) * SignBn) * Tmp;
@@ -237,13 +288,13 @@ __device__ __forceinline__ bool hlld_flux(const R (&L)[8], const R (&Rt)[8], R g
       e = e - SqRhoL1 * (uDotB1L1 - uDotB1) * SignBn;
     }
   } else {
-    const R InvSRUn = R(1) / (sR - Un);
+    const R InvSRUn = frcp(sR - Un);
     Rho = DsRhoR * InvSRUn;
     Tmp = DsRhoR * (sR - Un) - Bn2;
     if (Tmp < cTiny) {
       Ut1R1 = Ut1R; Ut2R1 = Ut2R; B1t1R1 = B1t1R; B1t2R1 = B1t2R;
     } else {
-      Tmp = R(1) / Tmp;
+      Tmp = frcp(Tmp);
       Ut1R1 = Ut1R - Bn * B1t1R * (Un - UnR) * Tmp;
       Ut2R1 = Ut2R - Bn * B1t2R * (Un - UnR) * Tmp;
       B1t1R1 = B1t1R * (DsRhoR * DsR - Bn2) * Tmp;
@@ -253,25 +304,25 @@ __device__ __forceinline__ bool hlld_flux(const R (&L)[8], const R (&Rt)[8], R g
     const R uDotB1R = UnR * B1n + Ut1R * B1t1R + Ut2R * B1t2R;
     const R uDotB1R1 = Un * B1n + Ut1R1 * B1t1R1 + Ut2R1 * B1t2R1;
     e = (DsR * eR - PtotR * UnR + Ptot12 * Un + Bn * (uDotB1R - uDotB1R1)) * InvSRUn;
-    const R SqRhoR1 = sqrt(Rho);
-    const R sR1 = Un + fabs(Bn) / SqRhoR1;
+    const R SqRhoR1 = fsqrt(Rho);
+    const R sR1 = Un + fdiv(fabs(Bn), SqRhoR1);
     if (sR1 <= R(0)) {
       Ut1 = Ut1R1; Ut2 = Ut2R1; B1t1 = B1t1R1; B1t2 = B1t2R1; uDotB1 = uDotB1R1;
     } else {
-      const R ratio = DsRhoL / (sL - Un);
+      const R ratio = fdiv(DsRhoL, sL - Un);
       if (ratio < R(0)) ok = false;
-      const R SqRhoL1 = sqrt(fabs(ratio));
+      const R SqRhoL1 = fsqrt(fabs(ratio));
       Tmp = DsRhoL * (sL - Un) - Bn2;
       if (Tmp < cTiny) {
         Ut1L1 = Ut1L; Ut2L1 = Ut2L; B1t1L1 = B1t1L; B1t2L1 = B1t2L;
       } else {
-        Tmp = R(1) / Tmp;
+        Tmp = frcp(Tmp);
         Ut1L1 = Ut1L - Bn * B1t1L * (Un - UnL) * Tmp;
         Ut2L1 = Ut2L - Bn * B1t2L * (Un - UnL) * Tmp;
         B1t1L1 = B1t1L * (DsRhoL * DsL - Bn2) * Tmp;
         B1t2L1 = B1t2L * (DsRhoL * DsL - Bn2) * Tmp;
       }
-      Tmp = R(1) / (SqRhoL1 + SqRhoR1);
+      Tmp = frcp(SqRhoL1 + SqRhoR1);
       const R SqRhoLR1 = SqRhoL1 * SqRhoR1 * SignBn;
       Ut1 = (SqRhoL1 * Ut1L1 + SqRhoR1 * Ut1R1 + (B1t1R1 - B1t1L1) * SignBn) * Tmp;
       Ut2 = (SqRhoL1 * Ut2L1 + SqRhoR1 * Ut2R1 + (B1t2R1 - B1t2L1) * SignBn) * Tmp;

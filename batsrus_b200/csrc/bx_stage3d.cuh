@@ -182,12 +182,76 @@ __device__ __forceinline__ bool face_slots(Real (&L)[8], Real (&R)[8], Real gamm
   return true;
 }
 
+// The face states of a face normal to D at index n (0..N) and transverse
+// cell (t0, t1) that differ from the plain limited reconstruction near a
+// resolution change or an outer boundary (ModFaceValue), applied after it
+// in the reference's order:
+//  * get_facex_second with BetaLimiterResChange below LimiterBeta: the
+//    nFaceRc cells next to a side with a resolution change or an outer
+//    boundary (DiLevel_EB /= 0, nb < 0 here) use BetaLimiterResChange
+//    (src/ModFaceValue.f90:1979-2014);
+//  * get_faceX_first (UseTvdResChange = F, given as `first` by the caller)
+//    has already set the first-order states at a coarser side;
+//  * get_face_tvd (UseTvdResChange = T): the tvd_reschange states at the
+//    resolution-change face and the next one on the fine side of a coarser
+//    neighbour (src/ModFaceValue.f90:680-852, 2269-2343).
+// val(v, i, j, k): variable v of block-local cell (i, j, k) of the tile.
+template <int N, int D, int LIM, typename Real, class Val>
+__device__ __forceinline__ void reschange_face_states(const StageArgs &a, int n, int t0, int t1, int nbLo, int nbHi,
+                                                      int rcFine, bool first, Real (&L)[8], Real (&R)[8],
+                                                      const Val &val) {
+  constexpr int e0 = D == 0 ? 1 : 0, e1 = D == 2 ? 1 : 2;
+  auto at = [&](int v, int nrm, int u0, int u1) {
+    int x[3];
+    x[D] = nrm;
+    x[e0] = u0;
+    x[e1] = u1;
+    return (Real)val(v, x[0], x[1], x[2]);
+  };
+  if (!first && a.nOrder > 1 && a.betaRc < a.beta) {
+    const bool lo = nbLo < 0, hi = nbHi < 0;
+    const int nf = a.nFaceRc;
+    const bool sL = (lo && n - 1 <= nf - 1) || (hi && n - 1 >= N - nf);
+    const bool sR = (lo && n <= nf - 1) || (hi && n >= N - nf);
+    if (sL || sR) {
+      const Real bL = (Real)(sL ? a.betaRc : a.beta), bR = (Real)(sR ? a.betaRc : a.beta);
+#pragma unroll
+      for (int v = 0; v < 8; v++)
+        limited_face_t2<LIM>(bL, bR, at(v, n - 2, t0, t1), at(v, n - 1, t0, t1), at(v, n, t0, t1),
+                             at(v, n + 1, t0, t1), L[v], R[v]);
+    }
+  }
+  if (a.tvdRc) {
+    const bool lo = ((rcFine >> (2 * D)) & 1) && n <= 1;
+    const bool hi = ((rcFine >> (2 * D + 1)) & 1) && n >= N - 1;
+    if (lo || hi) {
+      const Real beta = (Real)fmin(a.betaRc, a.beta);
+      const int p0 = t0 & ~1, p1 = t1 & ~1;
+      const int nc1 = lo ? -1 : N, nc2 = lo ? -2 : N + 1, nf1 = lo ? 0 : N - 1, nf2 = lo ? 1 : N - 2;
+#pragma unroll
+      for (int v = 0; v < 8; v++) {
+        Real cToF, fToC, ff;
+        tvd_reschange_var<Real>(at(v, nc1, p0, p1), at(v, nc2, p0, p1), at(v, nf1, p0, p1), at(v, nf1, p0 + 1, p1),
+                                at(v, nf1, p0, p1 + 1), at(v, nf1, p0 + 1, p1 + 1), at(v, nf1, t0, t1),
+                                at(v, nf2, t0, t1), beta, cToF, fToC, ff);
+        if (lo) {
+          if (n == 0) { L[v] = cToF; R[v] = fToC; }
+          else L[v] = ff;
+        } else {
+          if (n == N) { R[v] = cToF; L[v] = fToC; }
+          else R[v] = ff;
+        }
+      }
+    }
+  }
+}
+
 // one direction: faces (one per thread) then the cell sums.  rcFine / rcCoarse:
 // bit s set where side s borders a coarser / finer block
 template <class T, int D, int FLUX, int LIM, typename TileT, typename Real>
 __device__ __forceinline__ void sweep3(const StageArgs &a, const BlockGeom &g, const TileT *tile, Real *fbuf,
                                        double (&chg)[T::CPC][8], double (&divB)[T::CPC], double (&vdt)[T::CPC],
-                                       int &err, int rcFine, int rcCoarse, int b) {
+                                       int &err, int rcFine, int rcCoarse, int b, int nbLo, int nbHi) {
   const int t = threadIdx.x;
 #pragma unroll
   for (int r = 0; r < T::FPT; r++) {
@@ -197,7 +261,7 @@ __device__ __forceinline__ void sweep3(const StageArgs &a, const BlockGeom &g, c
     face_ijk<T, D>(f, i, j, k);
     const int fn = D == 0 ? i : (D == 1 ? j : k);  // face index along D
     const int side = fn == 0 ? 2 * D : (fn == T::N ? 2 * D + 1 : -1);
-    const bool first = a.nOrder == 1 || (side >= 0 && ((rcFine >> side) & 1));
+    const bool first = a.nOrder == 1 || (!a.tvdRc && side >= 0 && ((rcFine >> side) & 1));
     int idx[4];
 #pragma unroll
     for (int m = 0; m < 4; m++)
@@ -218,6 +282,10 @@ __device__ __forceinline__ void sweep3(const StageArgs &a, const BlockGeom &g, c
       if (FLUX == kFluxRoe && v == kBx + D) { cbL = q1; cbR = q2; }
       if (FLUX == kFluxRoe && v == kUx + D) { cuL = q1; cuR = q2; }
     }
+    reschange_face_states<T::N, D, LIM, Real>(a, fn, D == 0 ? j : i, D == 2 ? j : k, nbLo, nbHi, rcFine, first, L, R,
+                                              [&](int v, int ci, int cj, int ck) {
+                                                return tile[tile_index<T, TileT>(v, ci, cj, ck)];
+                                              });
     if (!face_slots<D, FLUX, Real>(L, R, (Real)a.gamma, (Real)a.invGm1, (Real)g.area[D], fbuf + f, T::NF, cbL,
                                    cbR, cuL, cuR))
       err = 1;
@@ -378,9 +446,9 @@ __global__ void __launch_bounds__(T::NTHR, 1)
     }
 
     double chg[T::CPC][8], divB[T::CPC], vdt[T::CPC];
-    sweep3<T, 0, FLUX, LIM, Real, Real>(a, g, tv, fbuf, chg, divB, vdt, err, rcFine, rcCoarse, b);
-    sweep3<T, 1, FLUX, LIM, Real, Real>(a, g, tv, fbuf, chg, divB, vdt, err, rcFine, rcCoarse, b);
-    sweep3<T, 2, FLUX, LIM, Real, Real>(a, g, tv, fbuf, chg, divB, vdt, err, rcFine, rcCoarse, b);
+    sweep3<T, 0, FLUX, LIM, Real, Real>(a, g, tv, fbuf, chg, divB, vdt, err, rcFine, rcCoarse, b, nb[0], nb[1]);
+    sweep3<T, 1, FLUX, LIM, Real, Real>(a, g, tv, fbuf, chg, divB, vdt, err, rcFine, rcCoarse, b, nb[2], nb[3]);
+    sweep3<T, 2, FLUX, LIM, Real, Real>(a, g, tv, fbuf, chg, divB, vdt, err, rcFine, rcCoarse, b, nb[4], nb[5]);
 
     // update_state_normal / update_explicit for the thread's cells
     double dtmin = 1e300;

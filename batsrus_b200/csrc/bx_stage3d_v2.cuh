@@ -109,10 +109,12 @@ __device__ __forceinline__ int face_of_lane(int gg, int lane) {
 // one face normal to D: limited face states from P, the face slots into fb
 // (slot-major, stride 576); the coarse side of a resolution change takes
 // the summed finer fluxes (apply_cons_flux).  False where hlld_flux stops.
+// special: bit s set where side s needs reschange_face_states (a coarser
+// neighbour with TVD faces, or the softer limiter of BetaLimiterResChange)
 template <int D, int FLUX, int LIM, typename Real>
 __device__ __forceinline__ bool face8(const StageArgs &a, const Real *__restrict__ P, Real *__restrict__ fb,
-                                      int f, int rcFine, int rcCoarse, const int *rcSlab, Real beta, Real gamma,
-                                      Real invGm1, Real area) {
+                                      int f, int rcFine, int rcCoarse, const int *rcSlab, const int *nbs, int special,
+                                      Real beta, Real gamma, Real invGm1, Real area) {
   int i, j, k, n;
   int ad[4];
   if (D == 0) {
@@ -126,15 +128,27 @@ __device__ __forceinline__ bool face8(const StageArgs &a, const Real *__restrict
     i = f & 7;
     const int r = f >> 3;  // j + 9 k
     k = r / 9; n = r - 9 * k; j = n;
+    // p8(i, p, k) for p = n - 2 + m without branches: the interior row, or
+    // the y ghost row (p < 0: p + 2, p >= 8: p - 6)
 #pragma unroll
-    for (int m = 0; m < 4; m++) ad[m] = p8(i, n - 2 + m, k);
+    for (int m = 0; m < 4; m++) {
+      const int p = n - 2 + m;
+      const int in = (k * 8 + p) * 12 + i + 2;
+      const int gh = 768 + (k * 4 + p + (p < 0 ? 2 : -6)) * 8 + i;
+      ad[m] = (unsigned)p < 8u ? in : gh;
+    }
   } else {
     i = f & 7; j = (f >> 3) & 7; n = f >> 6; k = n;
 #pragma unroll
-    for (int m = 0; m < 4; m++) ad[m] = p8(i, j, n - 2 + m);
+    for (int m = 0; m < 4; m++) {
+      const int p = n - 2 + m;
+      const int in = (p * 8 + j) * 12 + i + 2;
+      const int gh = 1024 + ((p + (p < 0 ? 2 : -6)) * 8 + j) * 8 + i;
+      ad[m] = (unsigned)p < 8u ? in : gh;
+    }
   }
   const int side = n == 0 ? 2 * D : (n == 8 ? 2 * D + 1 : -1);
-  const bool first = a.nOrder == 1 || (side >= 0 && ((rcFine >> side) & 1));
+  const bool first = a.nOrder == 1 || (!a.tvdRc && side >= 0 && ((rcFine >> side) & 1));
   Real L[8], R[8], cbL = Real(0), cbR = Real(0), cuL = Real(0), cuR = Real(0);
   if (first) {  // first order: the cell values (one branch per face)
 #pragma unroll
@@ -154,6 +168,10 @@ __device__ __forceinline__ bool face8(const StageArgs &a, const Real *__restrict
     cbL = P[ad[1] + (kBx + D) * 1280]; cbR = P[ad[2] + (kBx + D) * 1280];
     cuL = P[ad[1] + (kUx + D) * 1280]; cuR = P[ad[2] + (kUx + D) * 1280];
   }
+  if ((special >> (2 * D)) & 3)
+    reschange_face_states<8, D, LIM, Real>(a, n, D == 0 ? j : i, D == 2 ? j : k, nbs[2 * D], nbs[2 * D + 1], rcFine,
+                                           first, L, R,
+                                           [&](int v, int ci, int cj, int ck) { return P[p8(ci, cj, ck) + v * 1280]; });
   Real *out = fb + D * 10 * 576 + f;
   const bool ok = face_slots<D, FLUX, Real>(L, R, gamma, invGm1, area, out, 576, cbL, cbR, cuL, cuR);
   if (side >= 0 && ((rcCoarse >> side) & 1)) {
@@ -256,6 +274,8 @@ __global__ void __launch_bounds__(B::NTHR, B::MINB)
       rcMask |= (M.nb[s] == kNbrResChange) << s;
     }
     const int rcFine = M.rcFine, rcCoarse = M.rcCoarse;
+    const bool sharp = a.nOrder > 1 && a.betaRc < a.beta;
+    const int special = (a.tvdRc ? rcFine : 0) | (sharp ? (floatMask | rcMask) : 0);
 
     // ---- calc_primitives: landing area (conservative) -> P (primitive) ---
     Real defer[B::CCV][8];
@@ -330,13 +350,13 @@ __global__ void __launch_bounds__(B::NTHR, B::MINB)
       const int gg = gi - D * B::GPD;
       bool ok;
       if (D == 0)
-        ok = face8<0, FLUX, LIM, Real>(a, P, fb, face_of_lane<0>(gg, lane), rcFine, rcCoarse, M.rcSlab, beta,
+        ok = face8<0, FLUX, LIM, Real>(a, P, fb, face_of_lane<0>(gg, lane), rcFine, rcCoarse, M.rcSlab, M.nb, special, beta,
                                        gammaR, invGm1R, area0);
       else if (D == 1)
-        ok = face8<1, FLUX, LIM, Real>(a, P, fb, face_of_lane<1>(gg, lane), rcFine, rcCoarse, M.rcSlab, beta,
+        ok = face8<1, FLUX, LIM, Real>(a, P, fb, face_of_lane<1>(gg, lane), rcFine, rcCoarse, M.rcSlab, M.nb, special, beta,
                                        gammaR, invGm1R, area1);
       else
-        ok = face8<2, FLUX, LIM, Real>(a, P, fb, face_of_lane<2>(gg, lane), rcFine, rcCoarse, M.rcSlab, beta,
+        ok = face8<2, FLUX, LIM, Real>(a, P, fb, face_of_lane<2>(gg, lane), rcFine, rcCoarse, M.rcSlab, M.nb, special, beta,
                                        gammaR, invGm1R, area2);
       if (!ok) err = 1;
     }

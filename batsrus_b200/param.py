@@ -94,6 +94,12 @@ class Scheme:
     # floors (#MINIMUMDENSITY / #MINIMUMPRESSURE / #MINIMUMTEMPERATURE,
     # normalized units), active where > 0 (RhoMinDim_I = pMinDim_I =
     # TMinDim_I = -1 by default, src/ModPhysics.f90:170-172); massIon in amu
+    # #RESOLUTIONCHANGE (src/ModFaceValue.f90:44-76): TVD faces at
+    # resolution changes (the reference's default), the softer limiter near
+    # them when limiterBeta > betaLimiterResChange
+    useTvdResChange: bool = True
+    betaLimiterResChange: float = 2.0
+    nFaceLimiterResChange: int = 2
     rhoMin: float = -1.0
     pMin: float = -1.0
     tMin: float = -1.0
@@ -136,6 +142,14 @@ def apply_commands(commands, scheme, nDim=3):
             scheme.gamma = float(v[0])
         elif name == "#DIVB":
             scheme.useDivbSource = bool(v[0])
+        elif name == "#RESOLUTIONCHANGE":  # src/ModFaceValue.f90:168-177
+            if bool(v[0]):
+                raise ValueError("#RESOLUTIONCHANGE: UseAccurateResChange is not on the GPU path")
+            scheme.useTvdResChange = bool(v[1])
+            scheme.betaLimiterResChange = float(v[2])
+            scheme.nFaceLimiterResChange = int(v[3])
+        elif name == "#TVDRESCHANGE":  # :182-184
+            scheme.useTvdResChange = bool(v[0])
         elif name == "#MINIMUMDENSITY":  # src/ModSetParameters.f90:706-709
             scheme.rhoMin = float(v[0])
         elif name == "#MINIMUMPRESSURE":  # :711-714

@@ -327,6 +327,7 @@ def run_amr(args, lrank):
         x = ExplicitSolver(g, s, device=lrank)
         x.set_state(st)
         x.advance(1)  # Dt = 0 step
+        tuned = x.autotune() if args.autotune else None
         x.set_graph_steps(args.amr_steps)
         x.advance(1 + args.amr_steps)  # one uncaptured step, capture, one graph launch
         x.synchronize()
@@ -334,7 +335,9 @@ def run_amr(args, lrank):
         x.advance(args.amr_steps)  # one graph launch
         ms = x.region_end()
         lev = np.bincount(g.iLevelCoord[:, 0])
-        out[prec] = {"value": g.nCell * args.amr_steps / (ms * 1e-3), "ms_per_step": ms / args.amr_steps}
+        out[prec] = {"value": g.nCell * args.amr_steps / (ms * 1e-3), "ms_per_step": ms / args.amr_steps,
+                     "autotune": ({k: v["value"] for k, v in tuned.items() if k.startswith("stage")}
+                                  if tuned else None)}
         x.close()
     out.update({"workload": "amr_blast_levels0-3_nroot%d_hlld_mc" % args.amr_nroot, "unit": UNIT,
                 "blocks": int(g.nBlock), "cells": int(g.nCell), "blocks_per_level": [int(v) for v in lev],
@@ -356,6 +359,8 @@ def run_amr_dynamic(args, lrank):
     x = ExplicitSolver(g, s, device=lrank)
     x.set_state(st)
     x.advance(2)  # Dt = 0 step, then one step
+    if args.autotune:
+        x.autotune()
     p = amr.AmrParams(dnRefine=args.amr_dyn_dn, criteria=[amr.AmrCriterion("pjumpratio", 1.02, 1.3)],
                       minBlockLevel=0, maxBlockLevel=4, maxTotalBlocks=3 * g.nBlock)
     blocks0 = g.nBlock

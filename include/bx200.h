@@ -99,6 +99,14 @@ typedef struct {
   double pMin;
   double TMin;
   double MassIon;
+  /* #RESOLUTIONCHANGE (src/ModFaceValue.f90:44-76; the reference's defaults
+   * are .true., 2.0, 2): UseTvdResChange selects tvd_reschange faces next to
+   * a coarser block with two coarse ghost layers and
+   * correct_monotone_restrict (3D grids), 0 the first-order faces;
+   * BetaLimiterResChange <= 0 means the default 2.0 with 2 faces. */
+  int UseTvdResChange;
+  double BetaLimiterResChange;
+  int nFaceLimiterResChange;
 } bx_scheme_params;
 
 /* ---- set-up ------------------------------------------------------------ */

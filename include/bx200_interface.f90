@@ -73,6 +73,9 @@ module bx200_interface
      real(c_double):: DtFixed
      integer(c_int):: Precision
      real(c_double):: RhoMin, pMin, TMin, MassIon
+     integer(c_int):: UseTvdResChange
+     real(c_double):: BetaLimiterResChange
+     integer(c_int):: nFaceLimiterResChange
   end type bx_scheme_params
 
   interface

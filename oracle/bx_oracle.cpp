@@ -76,6 +76,7 @@ struct Oracle {
   static constexpr int kNoNei = -99;
   std::vector<int> dil, jbl;
   bool hasResChange = false;
+  bool ghostsCorrected = false;  // correct_monotone_restrict done since the last ghost fill
   // face values kept per resolution-change face: nFaceValue slots, BnL, BnR
   static constexpr int nCorr = nFaceValue + 2;
   std::vector<double> fineFlux, corrFlux;  // [block][side][face][nCorr]
@@ -198,13 +199,28 @@ struct Oracle {
     }
   }
 
-  // ghost cells of the sides with a resolution change (message_pass_cell of
-  // BATL with nProlongOrder = 1, documented in PARAM.XML #RESCHANGE /
-  // Doc/Tex/grid.tex): a coarser neighbour's cell is copied into the fine
-  // ghost cells it covers (injection); a finer neighbour's 2x2x2 cells are
-  // averaged into the coarse ghost cell they fill (restriction)
+  // nCoarseLayer of message_pass_cell: 2 (DoTwoCoarseLayers) when the faces
+  // at resolution changes are TVD at second order (src/ModMessagePass.f90:
+  // 105-108, DoOneCoarserLayer of src/ModSetParameters.f90:4353-4355)
+  bool two_coarse_layers() const { return c.useTvdResChange && c.nOrder > 1; }
+  bool tvd_reschange_on() const { return c.useTvdResChange && c.nOrder > 1 && c.nDim == 3; }
+
+  // ghost cells of the sides with a resolution change: BATL message_pass_cell
+  // (srcBATL, absent from the tree) as exchange_messages calls it with
+  // nProlongOrder = 1 (src/ModMessagePass.f90:176-210):
+  //  * a coarser neighbour's cell is copied into the fine ghost cells it
+  //    covers (injection); with two coarse layers the outer ghost layer
+  //    takes the next coarse cell;
+  //  * DoRestrictFace (nOrderProlong == 1): a coarse ghost cell takes the
+  //    mean of the finer cells next to its face toward the block (2x2 in 3D),
+  //    the first-order "monotone restriction" that correct_monotone_restrict
+  //    (src/ModFaceValue.f90:233-247) moves to the coarse cell distance.
+  //    The outer coarse ghost layer (the same rule one coarse cell out) only
+  //    enters the resolution-change face, whose fluxes apply_cons_flux
+  //    replaces.
   void fill_reschange_ghosts() {
     const int nCell[3] = {c.nI, c.nJ, c.nK};
+    ghostsCorrected = false;
 #pragma omp parallel for schedule(static) num_threads((int)scr.size())
     for (int b = 0; b < nBlock; b++)
       for (int sd = 0; sd < 2 * c.nDim; sd++) {
@@ -229,6 +245,8 @@ struct Oracle {
                   gf = (gf + tot) % tot;
                   lc[e] = (int)((gf >> 1) - (long)ic[3 * C + e] * nCell[e]) + 1;
                 }
+                const int layer = hi ? idx[d] - nCell[d] - 1 : -idx[d];  // 0 inner, 1 outer
+                if (layer == 1 && two_coarse_layers()) lc[d] += hi ? 1 : -1;
                 const double *src = st(C, lc[0], lc[1], lc[2]);
                 for (int v = 0; v < nVar; v++) t[v] = src[v];
               } else {
@@ -237,27 +255,144 @@ struct Oracle {
                   const long tot = (long)nCell[e] * (c.nRoot[e] << lev[b]);
                   gc[e] = ((long)ic[3 * b + e] * nCell[e] + idx[e] - 1 + tot) % tot;
                 }
+                // the finer cells: along d the one next to the face toward b,
+                // across d the 2 (2D) or 2x2 (3D) cells covered
                 long f0[3] = {2 * gc[0], c.nDim > 1 ? 2 * gc[1] : 0, c.nDim > 2 ? 2 * gc[2] : 0};
+                f0[d] += hi ? 0 : 1;
                 const int F = find_block(lev[b] + 1, (int)(f0[0] / nCell[0]),
                                          c.nDim > 1 ? (int)(f0[1] / nCell[1]) : 0,
                                          c.nDim > 2 ? (int)(f0[2] / nCell[2]) : 0);
+                int e0 = -1, e1 = -1;
+                for (int e = 0; e < c.nDim; e++)
+                  if (e != d) (e0 < 0 ? e0 : e1) = e;
                 double sum[nVar] = {0, 0, 0, 0, 0, 0, 0, 0};
-                for (int kk = 0; kk < (c.nDim > 2 ? 2 : 1); kk++)
-                  for (int jj = 0; jj < (c.nDim > 1 ? 2 : 1); jj++)
-                    for (int ii = 0; ii < 2; ii++) {
-                      const long g3[3] = {f0[0] + ii, f0[1] + jj, f0[2] + kk};
-                      int lf[3] = {1, 1, 1};
-                      for (int e = 0; e < c.nDim; e++)
-                        lf[e] = (int)(g3[e] - (long)ic[3 * F + e] * nCell[e]) + 1;
-                      const double *src = st(F, lf[0], lf[1], lf[2]);
-                      for (int v = 0; v < nVar; v++) sum[v] = sum[v] + src[v];
-                    }
-                const double w = c.nDim == 3 ? 0.125 : (c.nDim == 2 ? 0.25 : 0.5);
+                for (int u1 = 0; u1 < (e1 >= 0 ? 2 : 1); u1++)
+                  for (int u0 = 0; u0 < (e0 >= 0 ? 2 : 1); u0++) {
+                    long g3[3] = {f0[0], f0[1], f0[2]};
+                    if (e0 >= 0) g3[e0] += u0;
+                    if (e1 >= 0) g3[e1] += u1;
+                    int lf[3] = {1, 1, 1};
+                    for (int e = 0; e < c.nDim; e++)
+                      lf[e] = (int)(g3[e] - (long)ic[3 * F + e] * nCell[e]) + 1;
+                    const double *src = st(F, lf[0], lf[1], lf[2]);
+                    for (int v = 0; v < nVar; v++) sum[v] = sum[v] + src[v];
+                  }
+                const double w = c.nDim == 3 ? 0.25 : (c.nDim == 2 ? 0.5 : 1.0);
                 for (int v = 0; v < nVar; v++) t[v] = sum[v] * w;
               }
             }
       }
   }
+
+  // correct_monotone_restrict (src/ModFaceValue.f90:233-408) for every block
+  // with a finer neighbour, once per exchange of ghost cells: the first
+  // coarse ghost layer on a finer side becomes G + (G - C1)/3 in the
+  // primitive (velocity) form, where C1 is the block's cell next to it, and
+  // density and pressure (DefaultState_V > 0, srcEquation/ModEquationMhd.f90:
+  // 50-59) at least 1e-30.  The reference converts all momenta of the block
+  // to velocities and back; here only the ghost cell is converted back, so
+  // the interior keeps its momenta (the round trip changes them by at most
+  // a rounding error).
+  void correct_monotone_restrict_all() {
+    if (ghostsCorrected || !tvd_reschange_on() || !hasResChange) return;
+    ghostsCorrected = true;
+    const int nCell[3] = {c.nI, c.nJ, c.nK};
+    const double cThird = 1.0 / 3.0;
+#pragma omp parallel for schedule(static) num_threads((int)scr.size())
+    for (int b = 0; b < nBlock; b++)
+      for (int sd = 0; sd < 2 * c.nDim; sd++) {
+        if (dil[6 * b + sd] != -1) continue;
+        const int d = sd / 2, hi = sd % 2;
+        int lo3[3], hi3[3];
+        for (int e = 0; e < 3; e++) { lo3[e] = 1; hi3[e] = e < c.nDim ? nCell[e] : 1; }
+        lo3[d] = hi3[d] = hi ? nCell[d] + 1 : 0;
+        for (int k = lo3[2]; k <= hi3[2]; k++)
+          for (int j = lo3[1]; j <= hi3[1]; j++)
+            for (int i = lo3[0]; i <= hi3[0]; i++) {
+              int in3[3] = {i, j, k};
+              in3[d] = hi ? nCell[d] : 1;
+              double *G = st(b, i, j, k);
+              const double *C1 = st(b, in3[0], in3[1], in3[2]);
+              double g[nVar], q[nVar];
+              for (int v = 0; v < nVar; v++) { g[v] = G[v]; q[v] = C1[v]; }
+              const double InvRhoG = 1.0 / g[Rho_], InvRhoC = 1.0 / q[Rho_];
+              for (int v = RhoUx_; v <= RhoUz_; v++) { g[v] = g[v] * InvRhoG; q[v] = q[v] * InvRhoC; }
+              for (int v = 0; v < nVar; v++) g[v] = g[v] + cThird * (g[v] - q[v]);
+              g[Rho_] = std::max(g[Rho_], 1e-30);
+              g[P_] = std::max(g[P_], 1e-30);
+              for (int v = RhoUx_; v <= RhoUz_; v++) g[v] = g[v] * g[Rho_];
+              for (int v = 0; v < nVar; v++) G[v] = g[v];
+            }
+      }
+  }
+
+  // tvd_reschange (src/ModFaceValue.f90:2269-2343) as get_face_tvd calls it
+  // (:680-852) for the side sd next to a coarser block: for each 2x2 group
+  // of fine faces, from the two coarse ghost cells (Coarse1 next to the
+  // face, Coarse2 beyond), the four fine cells next to the face (Fine1) and
+  // the four behind them (Fine2), the states on both sides of the
+  // resolution-change face and the fine-side state of the next face
+  void get_face_tvd(int b, int sd, Scratch &s) {
+    const int nCell[3] = {c.nI, c.nJ, c.nK};
+    const int d = sd / 2, hi = sd % 2, n = nCell[d];
+    const int e0 = d == 0 ? 1 : 0, e1 = d == 2 ? 1 : 2;
+    const double cThird = 1.0 / 3.0, cTwoThird = 2.0 / 3.0, cSixth = 1.0 / 6.0;
+    const double Beta = std::min(betaRC(), c.limiterBeta);
+    auto P = [&](int nrm, int t0, int t1) {
+      int x[3];
+      x[d] = nrm; x[e0] = t0; x[e1] = t1;
+      return &s.Prim[nVar * cell(x[0], x[1], x[2])];
+    };
+    auto fc = [&](int nrm, int t0, int t1) {
+      int x[3];
+      x[d] = nrm; x[e0] = t0; x[e1] = t1;
+      return face(d, x[0], x[1], x[2]);
+    };
+    const int nC1 = hi ? n + 1 : 0, nC2 = hi ? n + 2 : -1, nF1 = hi ? n : 1, nF2 = hi ? n - 1 : 2;
+    const int fRes = hi ? n + 1 : 1, fNext = hi ? n : 2;  // face indices (1-based)
+    for (int t1 = 1; t1 <= nCell[e1]; t1 += 2)
+      for (int t0 = 1; t0 <= nCell[e0]; t0 += 2)
+        for (int v = 0; v < nVar; v++) {
+          const double Coarse1 = P(nC1, t0, t1)[v], Coarse2 = P(nC2, t0, t1)[v];
+          double F1[2][2], F2[2][2];
+          for (int j2 = 0; j2 < 2; j2++)
+            for (int i2 = 0; i2 < 2; i2++) {
+              F1[i2][j2] = P(nF1, t0 + i2, t1 + j2)[v];
+              F2[i2][j2] = P(nF2, t0 + i2, t1 + j2)[v];
+            }
+          const double Avg = 0.25 * (((F1[0][0] + F1[1][0]) + F1[0][1]) + F1[1][1]);
+          const double Grad = Avg - Coarse1;
+          const double Sg = std::copysign(1.0, Grad);
+          const double GradLtd = Sg * std::max(0.0, min3(Beta * cTwoThird * std::fabs(Grad),
+                                                          Beta * 0.5 * Sg * (Coarse1 - Coarse2),
+                                                          cThird * std::fabs(Grad) + 0.25 * Sg * (Coarse1 - Coarse2)));
+          for (int j2 = 0; j2 < 2; j2++)
+            for (int i2 = 0; i2 < 2; i2++) {
+              const double dT = F1[i2][j2] - Avg;
+              const double CToF = Coarse1 + GradLtd + std::copysign(std::min(std::fabs(GradLtd), std::fabs(dT)), dT);
+              const double Gf = Sg * std::max(0.0, std::min(std::min(Sg * (F1[i2][j2] - Coarse1),
+                                                                      Beta * cThird * std::fabs(Grad)),
+                                                             std::min(Beta * 0.5 * Sg * (F2[i2][j2] - F1[i2][j2]),
+                                                                      cSixth * std::fabs(Grad) + 0.25 * Sg *
+                                                                      (F2[i2][j2] - F1[i2][j2]))));
+              const double FToC = F1[i2][j2] - Gf, FF = F1[i2][j2] + Gf;
+              const long fr = fc(fRes, t0 + i2, t1 + j2), fn = fc(fNext, t0 + i2, t1 + j2);
+              if (hi) {
+                s.Right[d][nVar * fr + v] = CToF;
+                s.Left[d][nVar * fr + v] = FToC;
+                s.Right[d][nVar * fn + v] = FF;
+              } else {
+                s.Left[d][nVar * fr + v] = CToF;
+                s.Right[d][nVar * fr + v] = FToC;
+                s.Left[d][nVar * fn + v] = FF;
+              }
+            }
+        }
+  }
+
+  // BetaLimiterResChange (src/ModFaceValue.f90:75): 2 unless set (> 0)
+  double betaRC() const { return c.betaLimiterResChange > 0.0 ? c.betaLimiterResChange : 2.0; }
+  int nFaceRC() const { return c.betaLimiterResChange > 0.0 ? c.nFaceLimiterResChange : 2; }
 
   // face index (1-based) of side sd at the transverse position (t0, t1)
   long side_face(int sd, int t0, int t1) const {
@@ -428,7 +563,9 @@ struct Oracle {
   // primitive values q[l], l = lMin-1 .. lMax (+1 neighbours available)
   void limiter_pencil(const double *q /* q[l] for l=-1..n+2 via offset */,
                       int lMin, int lMax, double *dL, double *dR) const {
-    const double Beta = c.limiterBeta;
+    limiter_pencil(q, lMin, lMax, c.limiterBeta, dL, dR);
+  }
+  void limiter_pencil(const double *q, int lMin, int lMax, double Beta, double *dL, double *dR) const {
     const double cThird = 1. / 3.;
     for (int l = lMin - 1; l <= lMax; l++) {
       double d1 = q[l] - q[l - 1];   // left slope dVar1
@@ -473,7 +610,20 @@ struct Oracle {
               idx[d] = l; idx[a1] = p1; idx[a2] = p2;
               q[l] = s.Prim[nVar * cell(idx[0], idx[1], idx[2]) + v];
             }
-            if (c.nOrder == 2) limiter_pencil(q, 1, n + 1, dL, dR);
+            if (c.nOrder == 2) {
+              // get_facex_second (src/ModFaceValue.f90:1979-2014): with
+              // LimiterBeta > BetaLimiterResChange the cells next to a side
+              // with DiLevel /= 0 (another level or an outer boundary) take
+              // BetaLimiterResChange
+              int iMinSharp = 1, iMaxSharp = n + 1;
+              if (c.limiterBeta > betaRC()) {
+                if (dil[6 * b + 2 * d] != 0) iMinSharp = std::max(1, std::min(n + 2, 1 + nFaceRC()));
+                if (dil[6 * b + 2 * d + 1] != 0) iMaxSharp = std::min(n + 1, std::max(0, n + 1 - nFaceRC()));
+              }
+              if (iMinSharp <= iMaxSharp) limiter_pencil(q, iMinSharp, iMaxSharp, c.limiterBeta, dL, dR);
+              if (1 < iMinSharp) limiter_pencil(q, 1, iMinSharp - 1, betaRC(), dL, dR);
+              if (n + 1 > iMaxSharp) limiter_pencil(q, iMaxSharp + 1, n + 1, betaRC(), dL, dR);
+            }
             for (int f = 1; f <= n + 1; f++) {
               int idx[3];
               idx[d] = f; idx[a1] = p1; idx[a2] = p2;
@@ -488,7 +638,7 @@ struct Oracle {
             }
             // get_faceX_first at a side next to a coarser block
             // (src/ModFaceValue.f90:1118-1137, UseTvdResChange = F)
-            for (int hi = 0; hi < 2 && hasResChange && c.nOrder == 2; hi++) {
+            for (int hi = 0; hi < 2 && hasResChange && c.nOrder == 2 && !tvd_reschange_on(); hi++) {
               if (dil[6 * b + 2 * d + hi] != 1) continue;
               const int f = hi ? n + 1 : 1;
               int idx[3];
@@ -498,6 +648,9 @@ struct Oracle {
               s.Right[d][nVar * fi + v] = q[f];
             }
           }
+      // get_face_tvd (UseTvdResChange = T, the reference's default)
+      for (int hi = 0; hi < 2 && hasResChange && tvd_reschange_on(); hi++)
+        if (dil[6 * b + 2 * d + hi] == 1) get_face_tvd(b, 2 * d + hi, s);
     }
   }
 
@@ -1163,6 +1316,9 @@ struct Oracle {
         }
         message_pass_face();
       }
+      // calc_face_value(DoMonotoneRestrict = .true.) of each block starts with
+      // correct_monotone_restrict (src/ModFaceValue.f90:965-969)
+      correct_monotone_restrict_all();
 #pragma omp parallel for schedule(dynamic, 4) num_threads((int)scr.size()) reduction(| : err)
       for (int b = 0; b < nBlock; b++) {
         int t = 0;
@@ -1207,6 +1363,7 @@ struct Oracle {
       }
       message_pass_face();
     }
+    correct_monotone_restrict_all();
 #pragma omp parallel for schedule(dynamic, 4) num_threads((int)scr.size()) reduction(| : err)
     for (int b = 0; b < nBlock; b++) {
       int t = 0;

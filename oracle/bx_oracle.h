@@ -44,6 +44,13 @@ typedef struct {
   int nThread;         /* OpenMP threads (0 = default) */
   int useNonConservative; /* #NONCONSERVATIVE: pressure equation instead of energy */
   double rhoMin, pMin, tMin, massIon; /* floors, active where > 0 (massIon 0 -> 1) */
+  /* #RESOLUTIONCHANGE (src/ModFaceValue.f90:44-76): the TVD faces at
+     resolution changes (with nCoarseLayer = 2 and correct_monotone_restrict),
+     and the softer limiter near resolution changes and outer boundaries;
+     betaLimiterResChange <= 0 selects the defaults 2.0 and 2 faces */
+  int useTvdResChange;
+  double betaLimiterResChange;
+  int nFaceLimiterResChange;
 } ora_config;
 
 /* Create an oracle grid. iLevelCoord holds 4 ints per block: level and the

@@ -38,6 +38,8 @@ class OraConfig(ctypes.Structure):
         ("useNonConservative", ctypes.c_int),
         ("rhoMin", ctypes.c_double), ("pMin", ctypes.c_double), ("tMin", ctypes.c_double),
         ("massIon", ctypes.c_double),
+        ("useTvdResChange", ctypes.c_int), ("betaLimiterResChange", ctypes.c_double),
+        ("nFaceLimiterResChange", ctypes.c_int),
     ]
 
 
@@ -120,6 +122,9 @@ class Oracle:
         c.pMin = getattr(scheme, "pMin", -1.0)
         c.tMin = getattr(scheme, "tMin", -1.0)
         c.massIon = getattr(scheme, "massIon", 1.0)
+        c.useTvdResChange = int(getattr(scheme, "useTvdResChange", True))
+        c.betaLimiterResChange = getattr(scheme, "betaLimiterResChange", 2.0)
+        c.nFaceLimiterResChange = getattr(scheme, "nFaceLimiterResChange", 2)
         self.cfg = c
         self.grid = grid
         lc = np.ascontiguousarray(grid.iLevelCoord, dtype=np.int32)

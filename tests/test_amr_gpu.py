@@ -31,9 +31,10 @@ def grid(nRoot=2, maxLevel=2):
     return configs.amr_blast(nRoot=nRoot, maxLevel=maxLevel, with_state=False)[0]
 
 
-def scheme(flux, limiter="mc", precision="fp64"):
+def scheme(flux, limiter="mc", precision="fp64", tvd=True):
     return Scheme(nOrder=2, nStage=2, typeFlux=flux, typeLimiter=limiter, limiterBeta=1.5, cfl=0.8,
-                  gamma=5.0 / 3.0, useDivbSource=True, useHalfStep=True, precision=precision)
+                  gamma=5.0 / 3.0, useDivbSource=True, useHalfStep=True, precision=precision,
+                  useTvdResChange=tvd)
 
 
 def test_neighbor_tables_bit_exact():
@@ -52,11 +53,16 @@ def test_neighbor_tables_bit_exact():
     assert np.array_equal(j.reshape(-1, 6, 4), jb + 1)
 
 
+@pytest.mark.parametrize("tvd", [True, False], ids=["tvd_reschange", "first_order_reschange"])
 @pytest.mark.parametrize("flux,limiter", [("Rusanov", "mc"), ("Linde", "mc3"), ("HLLD", "mc"), ("Roe", "mc3")])
-def test_amr_fp64_steps_match_oracle(flux, limiter):
+def test_amr_fp64_steps_match_oracle(flux, limiter, tvd):
+    """#RESOLUTIONCHANGE T (the reference's default: tvd_reschange faces, two
+    coarse ghost layers, correct_monotone_restrict) and F (first-order faces)
+    on a perturbed Orszag-Tang state, which varies across the resolution
+    changes from the first step."""
     g = grid(2, 2)
-    s = scheme(flux, limiter)
-    st = initial.blast(g)
+    s = scheme(flux, limiter, tvd=tvd)
+    st = initial.perturbed_ot(g, seed=3, amplitude=5e-2, kmax=4)
     o = Oracle(g, s)
     o.set_state(st)
     o.exchange_messages()
@@ -74,10 +80,13 @@ def test_amr_fp64_steps_match_oracle(flux, limiter):
     x.close()
 
 
-def test_amr_conserves_mass_and_momentum():
+@pytest.mark.parametrize("tvd", [True, False], ids=["tvd_reschange", "first_order_reschange"])
+def test_amr_conserves_mass_and_momentum(tvd):
+    import dataclasses
     g = grid(2, 2)
-    s = scheme("HLLD")
-    st = initial.blast(g)
+    # the Powell source would change the momentum of a state with div B /= 0
+    s = dataclasses.replace(scheme("HLLD", tvd=tvd), useDivbSource=False)
+    st = initial.perturbed_ot(g, seed=3, amplitude=5e-2, kmax=4)
     x = ExplicitSolver(g, s)
     x.set_state(st)
     isl = g.interior_slices()
@@ -112,3 +121,32 @@ def test_amr_fp32_bulk_l1():
     l1 = np.abs(a - b).sum() / np.abs(b).sum()
     x.close()
     assert l1 < 1e-6, l1
+
+
+def test_amr_beta_limiter_reschange_matches_oracle():
+    """#RESOLUTIONCHANGE with BetaLimiterResChange 1.1 below the MC limiter's
+    1.5: the two cells next to every resolution change and every outer
+    (float) boundary take the softer limiter (src/ModFaceValue.f90:1979-2014),
+    on top of the TVD faces."""
+    import dataclasses
+    g = configs.amr_blast(nRoot=2, maxLevel=2, with_state=False)[0]
+    g = BlockGrid(g.nDim, g.nI, g.nJ, g.nK, g.nRoot, g.xyzMin, g.xyzMax, ("float",) * 6, g.iLevelCoord)
+    s = dataclasses.replace(scheme("Linde", "mc"), betaLimiterResChange=1.1, nFaceLimiterResChange=2)
+    st = initial.perturbed_ot(g, seed=4, amplitude=5e-2, kmax=4)
+    o = Oracle(g, s)
+    o.set_state(st)
+    o.exchange_messages()
+    x = ExplicitSolver(g, s)
+    x.set_state(st)
+    isl = g.interior_slices()
+    for step in range(3):
+        o.advance(1)
+        x.advance(1)
+        assert rel_err(x.get_state()[isl], o.get_state()[isl]) < 1e-12, step
+    # the softer limiter changes the result
+    o2 = Oracle(g, scheme("Linde", "mc"))
+    o2.set_state(st)
+    o2.exchange_messages()
+    o2.advance(3)
+    assert rel_err(o2.get_state()[isl], o.get_state()[isl]) > 1e-8
+    x.close()

@@ -257,3 +257,82 @@ def test_floors_hold_and_trip():
     rho, p = S[..., 0], S[..., 7]
     assert (rho >= 0.6).all() and (rho == 0.6).any()
     assert (p >= 0.1).all() and (p >= rho / 1.25 * 0.15).all()
+
+
+def _amr_case(tvd):
+    g, s, _, _ = configs.amr_blast(nRoot=2, maxLevel=2, precision="fp64", with_state=False)
+    s.useTvdResChange = tvd
+    return g, s, initial.perturbed_ot(g, seed=3, amplitude=5e-2, kmax=4)
+
+
+def test_tvd_reschange_conserves_and_differs():
+    """The oracle's #RESOLUTIONCHANGE T path (tvd_reschange faces, two coarse
+    ghost layers, correct_monotone_restrict) on a periodic two-level grid:
+    mass and momentum stay conserved through the flux correction, a uniform
+    state stays uniform, and the result differs from the first-order faces of
+    UseTvdResChange = F."""
+    out = {}
+    for tvd in (True, False):
+        g, s, st = _amr_case(tvd)
+        s.useDivbSource = False  # the Powell source does not conserve momentum
+        isl = g.interior_slices()
+        vol = g.block_geometry()[1].prod(1)
+        tot = lambda u: np.array([(u[isl][..., v].sum(axis=(1, 2, 3)) * vol).sum() for v in range(4)])
+        o = Oracle(g, s)
+        o.set_state(st)
+        o.exchange_messages()
+        m0 = tot(o.get_state())
+        o.advance(4)
+        out[tvd] = o.get_state()[isl]
+        m1 = tot(o.get_state())
+        assert abs(m1[0] - m0[0]) <= 1e-14 * m0[0] and np.abs(m1[1:] - m0[1:]).max() <= 1e-14 * m0[0]
+    assert np.abs(out[True] - out[False]).max() > 1e-4
+    g, s, st = _amr_case(True)
+    st[...] = 0.0
+    st[..., 0], st[..., 1], st[..., 4], st[..., 7] = 1.0, 0.3, 0.5, 0.7
+    o = Oracle(g, s)
+    o.set_state(st)
+    o.exchange_messages()
+    o.advance(3)
+    isl = g.interior_slices()
+    assert np.abs(o.get_state()[isl] - st[isl]).max() == 0.0
+
+
+def test_tvd_reschange_first_step_is_second_order_on_linear_data():
+    """tvd_reschange reproduces linear data exactly (its limited slopes equal
+    the true slope when the ratios are within the limiter's bounds): a density
+    ramp along x with a uniform velocity is advected by the TVD faces as on
+    the uniform grid of the finest level, to rounding, in the first step,
+    while the first-order faces of UseTvdResChange = F are not."""
+    from batsrus_b200.grid import BlockGrid
+    lc = []
+    # one x-row of root blocks, the middle ones refined: levels 0 and 1
+    for i in range(4):
+        if i in (1, 2):
+            for o in range(8):
+                lc.append((1, 2 * i + (o & 1), (o >> 1) & 1, o >> 2))
+        else:
+            lc.append((0, i, 0, 0))
+    g = BlockGrid(3, 8, 8, 8, (4, 1, 1), (0.0, 0.0, 0.0), (4.0, 1.0, 1.0), ("float",) * 6,
+                  np.array(lc, dtype=np.int32))
+    xc = g.cell_centers(with_ghost=True)[..., 0]
+    st = np.zeros(g.state_shape_fortran())
+    st[..., 0] = 1.0 + 0.01 * xc
+    st[..., 1] = st[..., 0] * 0.5
+    st[..., 7] = 1.0
+    res = {}
+    for tvd in (True, False):
+        s = Scheme(nOrder=2, nStage=2, typeFlux="Rusanov", typeLimiter="mc", limiterBeta=1.5, cfl=1.0,
+                   gamma=5.0 / 3.0, useDivbSource=False, useDtFixed=True, dtFixed=0.01, useTvdResChange=tvd)
+        o = Oracle(g, s)
+        o.set_state(st)
+        o.exchange_messages()
+        o.advance(1)
+        res[tvd] = o.get_state()[g.interior_slices()]
+    # away from the float boundaries the exact update of a linear profile
+    # advected at u = 0.5 with dt = 0.01 is rho - 0.5*0.01*0.01
+    xin = g.cell_centers(with_ghost=False)[..., 0]
+    inner = (xin > 1.2) & (xin < 2.8)
+    exact = 1.0 + 0.01 * xin - 0.5 * 0.01 * 0.01
+    assert np.abs(res[True][..., 0] - exact)[inner].max() < 1e-13
+    assert np.abs(res[False][..., 0] - exact)[inner].max() > 1e-9
