@@ -77,6 +77,10 @@ struct Oracle {
   std::vector<int> dil, jbl;
   bool hasResChange = false;
   bool ghostsCorrected = false;  // correct_monotone_restrict done since the last ghost fill
+  // blocks this rank updates (all of them on one domain); the others are
+  // copies of remote neighbours that only supply ghost cells and, at
+  // resolution changes, the finer faces' fluxes
+  std::vector<char> owned;
   // face values kept per resolution-change face: nFaceValue slots, BnL, BnR
   static constexpr int nCorr = nFaceValue + 2;
   std::vector<double> fineFlux, corrFlux;  // [block][side][face][nCorr]
@@ -152,6 +156,7 @@ struct Oracle {
       s.Source.assign((nVar + 1) * (long)c.nI * c.nJ * c.nK, 0.0);
       s.DivB1.assign((long)c.nI * c.nJ * c.nK, 0.0);
     }
+    owned.assign(nBlock, 1);
     build_neighbors();
   }
 
@@ -181,14 +186,21 @@ struct Oracle {
           int t[2], nt = 0;
           for (int e = 0; e < c.nDim; e++) if (e != d) t[nt++] = e;
           int m = 0;
+          bool all = true;
           for (int q1 = 0; q1 < (nt > 1 ? 2 : 1); q1++)
             for (int q0 = 0; q0 < (nt > 0 ? 2 : 1); q0++) {
               int f[3] = {2 * cc[0], c.nDim > 1 ? 2 * cc[1] : 0, c.nDim > 2 ? 2 * cc[2] : 0};
               f[d] += side ? 0 : 1;
               if (nt > 0) f[t[0]] += q0;
               if (nt > 1) f[t[1]] += q1;
-              jbl[24 * b + 4 * sd + m++] = find_block(lev[b] + 1, f[0], f[1], f[2]);
+              const int q2 = find_block(lev[b] + 1, f[0], f[1], f[2]);
+              all = all && q2 >= 0;
+              jbl[24 * b + 4 * sd + m++] = q2;
             }
+          if (!all) {  // outside a rank's block set: no neighbour there
+            for (int q2 = 0; q2 < 4; q2++) jbl[24 * b + 4 * sd + q2] = -1;
+            continue;
+          }
           dil[6 * b + sd] = -1;
           hasResChange = true;
         }
@@ -1278,14 +1290,22 @@ struct Oracle {
   }
 
   // set_global_timestep (src/ModTimeStepControl.f90:306-524), one process
-  void set_global_timestep(double tLimit) {
+  // the smallest DtMax_B of the blocks this rank updates
+  double local_dtmin() const {
+    double DtMin = 1e300;
+    for (int b = 0; b < nBlock; b++)
+      if (owned[b]) DtMin = std::min(DtMin, DtMax_B[b]);
+    return DtMin;
+  }
+  void set_global_timestep(double tLimit) { set_global_timestep(local_dtmin(), tLimit); }
+  // DtMin: the minimum of DtMax_B over all blocks of all ranks (the
+  // MPI_allreduce MIN of src/ModTimeStepControl.f90:392)
+  void set_global_timestep(double DtMin, double tLimit) {
     if (c.useDtFixed) {
       Dt = c.dtFixed;
     } else if (nStep <= 1) {  // TimeSimulationLimit is positive (or huge) in BATS_advance
       Dt = 0.0;
     } else {
-      double DtMin = 1e300;
-      for (int b = 0; b < nBlock; b++) DtMin = std::min(DtMin, DtMax_B[b]);
       Dt = DtMin;
     }
     if (tLimit > 0.0 && tSimulation + c.cfl * Dt > tLimit) Dt = (tLimit - tSimulation) / c.cfl;
@@ -1296,7 +1316,21 @@ struct Oracle {
   // advance_explicit (src/ModAdvanceExplicit.f90:18-325), orig CPU branch
   int advance_explicit() {
     int err = 0;
-    for (iStage = 1; iStage <= c.nStage; iStage++) {
+    for (int st = 1; st <= c.nStage; st++) {
+      err |= stage_run(st);
+      if (st < c.nStage) exchange_messages();
+    }
+    iStage = c.nStage;
+    return err;
+  }
+
+  // one stage of advance_explicit over the blocks this rank updates (the
+  // resolution-change fluxes of every finer block it holds, then the owned
+  // blocks); the ghost cells must be current
+  int stage_run(int st) {
+    int err = 0;
+    iStage = st;
+    {
       if (hasResChange) {
         // DoConserveFlux (src/ModAdvanceExplicit.f90:101-131): fluxes of the
         // finer blocks at resolution changes, then message_pass_face
@@ -1321,6 +1355,7 @@ struct Oracle {
       correct_monotone_restrict_all();
 #pragma omp parallel for schedule(dynamic, 4) num_threads((int)scr.size()) reduction(| : err)
       for (int b = 0; b < nBlock; b++) {
+        if (!owned[b]) continue;
         int t = 0;
 #ifdef _OPENMP
         t = omp_get_thread_num();
@@ -1334,9 +1369,7 @@ struct Oracle {
         if (iStage == c.nStage && !c.useDtFixed) calc_timestep(b, s);
       }
       tSimulation = tSimulation + Dt / c.nStage;
-      if (iStage < c.nStage) exchange_messages();
     }
-    iStage = c.nStage;
     return err;
   }
 
@@ -1385,9 +1418,12 @@ struct Oracle {
     nStep = nStep + 1;
     set_global_timestep(tLimit);
     int err = advance_explicit();
-    if (tLimit > 0 && tSimulation < tLimit && tLimit - tSimulation <= 1e-3 * Dt) tSimulation = tLimit;
+    end_step(tLimit);
     exchange_messages();
     return err;
+  }
+  void end_step(double tLimit) {
+    if (tLimit > 0 && tSimulation < tLimit && tLimit - tSimulation <= 1e-3 * Dt) tSimulation = tLimit;
   }
 };
 
@@ -2013,6 +2049,26 @@ void ora_get_state(void *h, double *S) {
 }
 void ora_exchange_messages(void *h) { ((Oracle *)h)->exchange_messages(); }
 int ora_advance(void *h, double tLimit) { return ((Oracle *)h)->advance(tLimit); }
+// one rank of a partitioned grid (the block list holds the owned blocks and
+// copies of the remote neighbours they read): which blocks are updated, the
+// rank's smallest DtMax_B, and a step driven stage by stage with the global
+// minimum and the ghost exchange done by the caller
+void ora_set_owned(void *h, const int *owned) {
+  Oracle *o = (Oracle *)h;
+  for (int b = 0; b < o->nBlock; b++) o->owned[b] = owned[b] != 0;
+}
+double ora_local_dtmin(void *h) { return ((Oracle *)h)->local_dtmin(); }
+void ora_begin_step(void *h, double DtMinGlobal, double tLimit) {
+  Oracle *o = (Oracle *)h;
+  o->nStep = o->nStep + 1;
+  o->set_global_timestep(DtMinGlobal, tLimit);
+}
+int ora_stage(void *h, int iStage) { return ((Oracle *)h)->stage_run(iStage); }
+void ora_end_step(void *h, double tLimit) {
+  Oracle *o = (Oracle *)h;
+  o->iStage = o->c.nStage;
+  o->end_step(tLimit);
+}
 int ora_advance_n(void *h, int n, double tLimit) {
   int err = 0;
   for (int m = 0; m < n; m++) err |= ((Oracle *)h)->advance(tLimit);

@@ -69,6 +69,15 @@ void ora_exchange_messages(void *h);
 /* One call of BATS_advance (time accurate): set_global_timestep +
  * advance_explicit + exchange_messages. Returns 0 on success. */
 int ora_advance(void *h, double tSimulationLimit);
+/* one rank of a partitioned grid: owned[b] != 0 for the blocks it updates
+ * (the others copy remote neighbours); its smallest DtMax_B; a step run as
+ * begin_step(global minimum), stage 1..nStage with the caller's ghost
+ * exchange before each, end_step */
+void ora_set_owned(void *h, const int *owned);
+double ora_local_dtmin(void *h);
+void ora_begin_step(void *h, double DtMinGlobal, double tSimulationLimit);
+int ora_stage(void *h, int iStage);
+void ora_end_step(void *h, double tSimulationLimit);
 /* nStep calls of ora_advance */
 int ora_advance_n(void *h, int nStep, double tSimulationLimit);
 void ora_get_time(void *h, double *tSimulation, double *Dt, int *nStep);

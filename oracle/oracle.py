@@ -79,6 +79,13 @@ def lib():
         L.ora_get_face_values.argtypes = [vp, ctypes.c_int, dp, dp]
         L.ora_get_face_flux.argtypes = [vp, ctypes.c_int, dp]
         L.ora_get_dtmax.argtypes = [vp, dp, dp]
+        L.ora_set_owned.argtypes = [vp, ip]
+        L.ora_local_dtmin.restype = ctypes.c_double
+        L.ora_local_dtmin.argtypes = [vp]
+        L.ora_begin_step.argtypes = [vp, ctypes.c_double, ctypes.c_double]
+        L.ora_stage.restype = ctypes.c_int
+        L.ora_stage.argtypes = [vp, ctypes.c_int]
+        L.ora_end_step.argtypes = [vp, ctypes.c_double]
         L.ora_recompute_timestep.restype = ctypes.c_int
         L.ora_recompute_timestep.argtypes = [vp]
         _lib = L
@@ -154,6 +161,24 @@ class Oracle:
         err = lib().ora_advance_n(self.h, n, t_limit)
         if err:
             raise RuntimeError("oracle advance failed (HLLD negative density ratio)")
+
+    # one rank of a partitioned grid (batsrus_b200.shard)
+    def set_owned(self, owned):
+        a = np.ascontiguousarray(owned, dtype=np.int32)
+        lib().ora_set_owned(self.h, a.ctypes.data_as(ctypes.POINTER(ctypes.c_int)))
+
+    def local_dtmin(self):
+        return lib().ora_local_dtmin(self.h)
+
+    def begin_step(self, dt_min_global, t_limit=-1.0):
+        lib().ora_begin_step(self.h, dt_min_global, t_limit)
+
+    def stage(self, i_stage):
+        if lib().ora_stage(self.h, i_stage):
+            raise RuntimeError("oracle stage failed (HLLD negative density ratio)")
+
+    def end_step(self, t_limit=-1.0):
+        lib().ora_end_step(self.h, t_limit)
 
     def recompute_timestep(self):
         """cell time steps of the current state, no update (after a regrid)"""
