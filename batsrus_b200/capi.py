@@ -41,6 +41,7 @@ EXPORTS = (
     "bx_autotune", "bx_tune_info", "bx_tune_set", "bx_tune_reset",
     "bx_amr_criteria", "bx_regrid", "bx_amr_plan", "bx_do_amr", "bx_get_grid",
     "bx_get_block_dt", "bx_set_block_dt",
+    "bx_halo_bytes", "bx_halo_pack", "bx_halo_unpack", "bx_get_dtmin", "bx_set_dtmin", "bx_end_step",
 )
 # #AMRCRITERIA TypeRefine -> BX_AMR_*
 AMR_CRIT = {"gradt": 1, "gradlogrho": 2, "gradlogp": 3, "gradp": 4, "pjumpratio": 5}
@@ -132,6 +133,7 @@ class GridDesc(ctypes.Structure):
         ("nBlock", ctypes.c_int),
         ("iLevelCoord_IB", ctypes.POINTER(ctypes.c_int)),
         ("iDevice", ctypes.c_int),
+        ("nOwned", ctypes.c_int),
     ]
 
 
@@ -176,6 +178,8 @@ def load():
         "bx_get_face_values": [i, dp, dp], "bx_get_face_flux": [i, dp], "bx_get_source": [dp],
         "bx_set_stage": [i], "bx_update_state_fast": [], "bx_exchange_messages": [i],
         "bx_set_global_timestep": [d, dp], "bx_advance_explicit": [i], "bx_advance": [i, d],
+        "bx_halo_bytes": [i, ip], "bx_halo_pack": [i, ip, i, p], "bx_halo_unpack": [i, ip, i, p],
+        "bx_get_dtmin": [dp], "bx_set_dtmin": [d], "bx_end_step": [d],
         "bx_set_graph_steps": [i], "bx_synchronize": [], "bx_timing_enable": [i], "bx_timing_get": [dp, ip, ip],
         "bx_timing_reset": [], "bx_region_begin": [], "bx_region_end": [dp],
         "bx_implicit_init": [ctypes.POINTER(ImplicitParamsC)],
@@ -225,7 +229,7 @@ def fptr(a):
     return a.ctypes.data_as(ctypes.POINTER(ctypes.c_float))
 
 
-def grid_desc(grid, device=0):
+def grid_desc(grid, device=0, nOwned=0):
     g = GridDesc()
     g.nDim = grid.nDim
     g.nI, g.nJ, g.nK = grid.nI, grid.nJ, grid.nK
@@ -240,6 +244,7 @@ def grid_desc(grid, device=0):
     g.iLevelCoord_IB = lc.ctypes.data_as(ctypes.POINTER(ctypes.c_int))
     g._keep = lc  # keep the array alive while the struct is used
     g.iDevice = device
+    g.nOwned = nOwned
     return g
 
 

@@ -61,6 +61,8 @@ struct Ctx {
   double *scrL[3] = {}, *scrR[3] = {}, *scrF[3] = {}, *scrSrc = nullptr, *scrDt = nullptr;
   std::vector<char> touched;
   int *touchedDev = nullptr;  // device list of the blocks updated per block
+  int nOwned = 0;             // blocks 0..nOwned-1 are updated (one rank of a partitioned grid)
+  int *haloIdx = nullptr;     // device list of blocks for bx_halo_pack / bx_halo_unpack
   bool compatPending = false;
   int iStage = 1;
   cudaStream_t st = nullptr;
@@ -271,7 +273,7 @@ void free_all() {
     }
   if (g.nbr) cudaFree(g.nbr);
   if (g.order) cudaFree(g.order);
-  for (int **p : {&g.rcType, &g.rcSlab, &g.lcDev, &g.touchedDev}) {
+  for (int **p : {&g.rcType, &g.rcSlab, &g.lcDev, &g.touchedDev, &g.haloIdx}) {
     if (*p) cudaFree(*p);
     *p = nullptr;
   }
@@ -338,7 +340,7 @@ void set_reschange(StageArgs &a) {
 StageArgs stage_args(int iStage, bool computeDt) {
   StageArgs a;
   a.nbr = g.nbr; a.order = g.order; a.geom = g.geom; a.ts = g.ts; a.dtBlock = g.dtBlock;
-  a.nBlock = g.nBlock;
+  a.nBlock = g.nOwned;  // the processing order lists the owned blocks
   a.iStage = iStage; a.nStage = g.sch.nStage; a.nOrder = g.sch.nOrder; a.limiter = g.sch.TypeLimiter;
   a.useDivb = g.sch.UseDivbSource; a.useHalfStep = g.sch.UseHalfStep; a.computeDt = computeDt;
   a.beta = g.sch.LimiterBeta; a.gamma = g.sch.Gamma; a.invGm1 = 1.0 / (g.sch.Gamma - 1.0);
@@ -540,7 +542,7 @@ CompatArgs compat_args() {
 int compat_phase(int phase, int iBlock) {
   NEED_READY();
   if (g.nSlab) return fail(BX_ERR_ARG, "the per-block entry points work on single-level grids");
-  if (iBlock < 1 || iBlock > g.nBlock) return fail(BX_ERR_ARG, "iBlock=%d out of range 1..%d", iBlock, g.nBlock);
+  if (iBlock < 1 || iBlock > g.nOwned) return fail(BX_ERR_ARG, "iBlock=%d out of range 1..%d", iBlock, g.nOwned);
   if (g.sch.TypeFlux == BX_FLUX_ROE) return fail(BX_ERR_ARG, "the per-block entry points have no Roe flux");
   if (g.sch.BetaLimiterResChange > 0.0 && g.sch.BetaLimiterResChange < g.sch.LimiterBeta && g.sch.nOrder > 1 &&
       g.sch.nFaceLimiterResChange > 0)
@@ -575,6 +577,7 @@ Core core() {
   c.dev = g.dev; c.nDim = g.nDim; c.nI = g.nI; c.nJ = g.nJ; c.nK = g.nK; c.shape = g.shape;
   c.nBlock = g.nBlock; c.nSM = g.nSM; c.nCell = g.nCell; c.sch = g.sch;
   c.A = g.A; c.nbr = g.nbr; c.order = g.order; c.geom = g.geom; c.ts = g.ts; c.dtBlock = g.dtBlock; c.nSlab = g.nSlab;
+  c.nOwned = g.nOwned;
   c.st = g.st;
   return c;
 }
@@ -621,9 +624,12 @@ int bx_init(const bx_grid_desc *gd, const bx_scheme_params *sp) {
   if (gd->nBlock < 1 || !gd->iLevelCoord_IB) return fail(BX_ERR_ARG, "empty block list");
   if (sp->TypeFlux == BX_FLUX_ROE && shape != kShape888 && shape != kShape444)
     return fail(BX_ERR_ARG, "the Roe flux is built for 3D blocks of 8^3 or 4^3 cells");
+  if (gd->nOwned < 0 || gd->nOwned > gd->nBlock)
+    return fail(BX_ERR_ARG, "nOwned=%d outside 0..nBlock=%d", gd->nOwned, gd->nBlock);
   g.shape = shape;
   g.nDim = gd->nDim; g.nI = gd->nI; g.nJ = gd->nJ; g.nK = gd->nK;
   g.nBlock = gd->nBlock; g.nCell = (long)gd->nI * gd->nJ * gd->nK;
+  g.nOwned = gd->nOwned > 0 ? gd->nOwned : gd->nBlock;
   for (int d = 0; d < 3; d++) { g.nRoot[d] = gd->nRootBlock[d]; g.cmin[d] = gd->CoordMin[d]; g.cmax[d] = gd->CoordMax[d]; }
   for (int s = 0; s < 6; s++) g.typeBc[s] = gd->TypeBc[s];
   int r = check_scheme(sp);
@@ -693,6 +699,7 @@ int bx_init(const bx_grid_desc *gd, const bx_scheme_params *sp) {
           int t[2], nt = 0;
           for (int e = 0; e < g.nDim; e++) if (e != d) t[nt++] = e;
           int m = 0;
+          bool all = true;
           for (int q1 = 0; q1 < (nt > 1 ? 2 : 1); q1++)
             for (int q0 = 0; q0 < (nt > 0 ? 2 : 1); q0++) {
               int f[3] = {2 * c[0], g.nDim > 1 ? 2 * c[1] : 0, g.nDim > 2 ? 2 * c[2] : 0};
@@ -700,10 +707,16 @@ int bx_init(const bx_grid_desc *gd, const bx_scheme_params *sp) {
               if (nt > 0) f[t[0]] += q0;
               if (nt > 1) f[t[1]] += q1;
               S.nb[m] = findb(g.lev[b] + 1, f[0], f[1], f[2]);
-              if (S.nb[m] < 0)
-                return fail(BX_ERR_ARG, "block %d side %d: neighbours differ by more than one level", b + 1, sd);
+              all = all && S.nb[m] >= 0;
               m++;
             }
+          if (!all) {
+            // a halo block at the edge of a rank's block list has no
+            // neighbour there (it is not updated); an owned block must
+            if (b >= g.nOwned) continue;
+            return fail(BX_ERR_ARG, "block %d side %d: no neighbour in the block list (levels differ by more than "
+                        "one, or a remote neighbour's copy is missing)", b + 1, sd);
+          }
         }
         g.nbrH[6 * b + sd] = kNbrResChange;
         g.dilH[6 * b + sd] = S.type;
@@ -717,9 +730,10 @@ int bx_init(const bx_grid_desc *gd, const bx_scheme_params *sp) {
   g.nSlab = (int)g.slabsH.size();
   if (g.nSlab && g.shape != kShape888 && g.shape != kShape444)
     return fail(BX_ERR_ARG, "resolution changes need 3D 8x8x8 or 4x4x4 blocks");
-  // Morton processing order (L2 reuse of the neighbours' interiors)
-  g.orderH.resize(g.nBlock);
-  for (int b = 0; b < g.nBlock; b++) g.orderH[b] = b;
+  // Morton processing order (L2 reuse of the neighbours' interiors) of the
+  // blocks this rank updates
+  g.orderH.resize(g.nOwned);
+  for (int b = 0; b < g.nOwned; b++) g.orderH[b] = b;
   std::stable_sort(g.orderH.begin(), g.orderH.end(), [&](int x, int y) {
     if (g.lev[x] != g.lev[y]) return g.lev[x] < g.lev[y];
     return morton3(g.ic[3 * x], g.ic[3 * x + 1], g.ic[3 * x + 2]) <
@@ -778,7 +792,8 @@ int bx_init(const bx_grid_desc *gd, const bx_scheme_params *sp) {
   CK(cudaMalloc(&g.ts, sizeof(StepState)));
   CK(cudaMalloc(&g.dtBlock, sizeof(double) * g.nBlock));
   CK(cudaMemcpyAsync(g.nbr, g.nbrH.data(), sizeof(int) * 6 * g.nBlock, cudaMemcpyHostToDevice, g.st));
-  CK(cudaMemcpyAsync(g.order, g.orderH.data(), sizeof(int) * g.nBlock, cudaMemcpyHostToDevice, g.st));
+  CK(cudaMemcpyAsync(g.order, g.orderH.data(), sizeof(int) * g.nOwned, cudaMemcpyHostToDevice, g.st));
+  if (g.nOwned < g.nBlock) CK(cudaMalloc(&g.haloIdx, sizeof(int) * g.nBlock));
   CK(cudaMemcpyAsync(g.geom, g.geomH.data(), sizeof(BlockGeom) * g.nBlock, cudaMemcpyHostToDevice, g.st));
   CK(cudaMemsetAsync(g.dtBlock, 0, sizeof(double) * g.nBlock, g.st));
   if (g.nSlab) {
@@ -1033,6 +1048,109 @@ int bx_set_global_timestep(double tLimit, double *Dt) {
   return BX_OK;
 }
 
+// ---- one rank of a partitioned grid ------------------------------------------
+}  // extern "C"
+namespace {
+template <typename T>
+__global__ void k_gather_blocks(const T *__restrict__ state, T *__restrict__ buf, const int *__restrict__ list,
+                                int nList, long nPerBlock) {
+  const long total = (long)nList * nPerBlock;
+  for (long q = blockIdx.x * (long)blockDim.x + threadIdx.x; q < total; q += (long)gridDim.x * blockDim.x)
+    buf[q] = state[(long)list[q / nPerBlock] * nPerBlock + q % nPerBlock];
+}
+template <typename T>
+__global__ void k_scatter_blocks(T *__restrict__ state, const T *__restrict__ buf, const int *__restrict__ list,
+                                 int nList, long nPerBlock) {
+  const long total = (long)nList * nPerBlock;
+  for (long q = blockIdx.x * (long)blockDim.x + threadIdx.x; q < total; q += (long)gridDim.x * blockDim.x)
+    state[(long)list[q / nPerBlock] * nPerBlock + q % nPerBlock] = buf[q];
+}
+
+// the state array that stage iStage reads, and whether it is FP32
+int halo_source(int iStage, void *&base, bool &fp32) {
+  if (iStage < 1 || iStage > g.sch.nStage) return fail(BX_ERR_ARG, "iStage=%d", iStage);
+  StageArgs a = stage_args(iStage, false);
+  base = const_cast<void *>(a.in);
+  fp32 = g.sch.Precision == BX_FP32_BULK && iStage == 2;
+  return BX_OK;
+}
+
+int halo_move(int iStage, const int *iBlock_I, int nBlock, void *buf, bool pack) {
+  NEED_READY();
+  if (nBlock < 0 || nBlock > g.nBlock || (nBlock && (!iBlock_I || !buf))) return fail(BX_ERR_ARG, "halo list");
+  if (nBlock == 0) return BX_OK;
+  if (!g.haloIdx) CK(cudaMalloc(&g.haloIdx, sizeof(int) * g.nBlock));
+  void *base;
+  bool fp32;
+  int r = halo_source(iStage, base, fp32);
+  if (r) return r;
+  std::vector<int> idx(nBlock);
+  for (int n = 0; n < nBlock; n++) {
+    if (iBlock_I[n] < 1 || iBlock_I[n] > g.nBlock) return fail(BX_ERR_ARG, "block %d not in 1..%d", iBlock_I[n], g.nBlock);
+    // a rank writes only the copies of remote blocks and sends its own
+    if (!pack && iBlock_I[n] <= g.nOwned) return fail(BX_ERR_ARG, "block %d is owned, not a halo copy", iBlock_I[n]);
+    idx[n] = iBlock_I[n] - 1;
+  }
+  CK(cudaMemcpyAsync(g.haloIdx, idx.data(), sizeof(int) * nBlock, cudaMemcpyHostToDevice, g.st));
+  const long per = 8 * g.nCell;
+  if (fp32) {
+    if (pack) k_gather_blocks<float><<<592, 256, 0, g.st>>>((const float *)base, (float *)buf, g.haloIdx, nBlock, per);
+    else k_scatter_blocks<float><<<592, 256, 0, g.st>>>((float *)base, (const float *)buf, g.haloIdx, nBlock, per);
+  } else {
+    if (pack) k_gather_blocks<double><<<592, 256, 0, g.st>>>((const double *)base, (double *)buf, g.haloIdx, nBlock, per);
+    else k_scatter_blocks<double><<<592, 256, 0, g.st>>>((double *)base, (const double *)buf, g.haloIdx, nBlock, per);
+  }
+  CK(cudaGetLastError());
+  // the index list is reused by the next call: finish this one
+  CK(cudaStreamSynchronize(g.st));
+  return BX_OK;
+}
+}  // namespace
+extern "C" {
+
+int bx_halo_bytes(int iStage, int *BytesPerBlock) {
+  NEED_READY();
+  void *base;
+  bool fp32;
+  int r = halo_source(iStage, base, fp32);
+  if (r) return r;
+  if (!BytesPerBlock) return fail(BX_ERR_ARG, "null argument");
+  *BytesPerBlock = (int)((fp32 ? sizeof(float) : sizeof(double)) * 8 * g.nCell);
+  return BX_OK;
+}
+int bx_halo_pack(int iStage, const int *iBlock_I, int nBlock, void *Buf_dev) {
+  return halo_move(iStage, iBlock_I, nBlock, Buf_dev, true);
+}
+int bx_halo_unpack(int iStage, const int *iBlock_I, int nBlock, const void *Buf_dev) {
+  return halo_move(iStage, iBlock_I, nBlock, const_cast<void *>(Buf_dev), false);
+}
+int bx_get_dtmin(double *DtMin) {
+  NEED_READY();
+  if (!DtMin) return fail(BX_ERR_ARG, "null argument");
+  StepState s;
+  CK(cudaMemcpyAsync(&s, g.ts, sizeof(s), cudaMemcpyDeviceToHost, g.st));
+  CK(cudaStreamSynchronize(g.st));
+  const unsigned long long bits = s.DtMinBits;
+  std::memcpy(DtMin, &bits, sizeof(double));
+  return BX_OK;
+}
+int bx_set_dtmin(double DtMin) {
+  NEED_READY();
+  StepState s;
+  CK(cudaMemcpyAsync(&s, g.ts, sizeof(s), cudaMemcpyDeviceToHost, g.st));
+  CK(cudaStreamSynchronize(g.st));
+  std::memcpy(&s.DtMinBits, &DtMin, sizeof(double));
+  CK(cudaMemcpyAsync(g.ts, &s, sizeof(s), cudaMemcpyHostToDevice, g.st));
+  CK(cudaStreamSynchronize(g.st));
+  return BX_OK;
+}
+int bx_end_step(double tLimit) {
+  NEED_READY();
+  end_step_kernel<<<1, 1, 0, g.st>>>(g.ts, g.sch.nStage, tLimit);
+  CK(cudaGetLastError());
+  return BX_OK;
+}
+
 int bx_advance_explicit(int DoCalcTimestep) {
   NEED_READY();
   (void)DoCalcTimestep;
@@ -1110,6 +1228,7 @@ int bx_regrid(const bx_grid_desc *gd, const int *iRemap_IB) {
   NEED_READY();
   if (!gd || !iRemap_IB) return fail(BX_ERR_ARG, "null argument");
   if (!g.use3d) return fail(BX_ERR_ARG, "regrid needs 3D 8x8x8 or 4x4x4 blocks");
+  if (g.nOwned < g.nBlock) return fail(BX_ERR_ARG, "regrid of one rank of a partitioned grid is not built");
   if (gd->nDim != g.nDim || gd->nI != g.nI || gd->nJ != g.nJ || gd->nK != g.nK)
     return fail(BX_ERR_ARG, "regrid cannot change the block size");
   for (int d = 0; d < 3; d++)
@@ -1220,6 +1339,7 @@ int bx_get_grid(int *iLevelCoord_IB) {
 int bx_do_amr(const bx_amr_params *p, int *nBlockNew, int *IsChanged) {
   NEED_READY();
   if (!p) return fail(BX_ERR_ARG, "null argument");
+  if (g.nOwned < g.nBlock) return fail(BX_ERR_ARG, "dynamic AMR of one rank of a partitioned grid is not built");
   if (p->nCrit < 1 || p->nCrit > 3) return fail(BX_ERR_ARG, "nCrit=%d (1..3)", p->nCrit);
   std::vector<double> crit((size_t)p->nCrit * g.nBlock);
   int r = bx_amr_criteria(p->nCrit, p->iTypeCrit, crit.data());

@@ -20,6 +20,7 @@ struct Core {
   double *dtBlock;
   cudaStream_t st;
   int nSlab;  // resolution-change sides (0 on a single-level grid)
+  int nOwned;  // blocks updated by this rank (nBlock on one domain)
 };
 
 Core core();

@@ -951,6 +951,7 @@ int bx_heat_init(const bx_heat_params *prm, const double *Te, const double *bhat
   Core c = core();
   if (!c.ready) return core_fail(BX_ERR_STATE, "bx_init has not been called");
   if (!prm || !Te || !bhat || !used) return core_fail(BX_ERR_ARG, "null argument");
+  if (c.nOwned < c.nBlock) return core_fail(BX_ERR_ARG, "the heat conduction solve of a partitioned grid is not built");
   if (prm->nKrylovVector < 1 || prm->nKrylovVector > 64 || prm->MaxMatvec < 1 || !(prm->Dt > 0) || !(prm->Cv > 0))
     return core_fail(BX_ERR_ARG, "bad heat conduction parameters");
   if (prm->TypePrecond != BX_PRECOND_NONE && prm->TypePrecond != BX_PRECOND_BILU &&

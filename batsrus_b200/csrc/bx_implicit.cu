@@ -336,6 +336,7 @@ int bx_implicit_init(const bx_implicit_params *prm) {
   Core c = core();
   if (!c.ready) return core_fail(BX_ERR_STATE, "bx_init has not been called");
   if (!prm) return core_fail(BX_ERR_ARG, "null argument");
+  if (c.nOwned < c.nBlock) return core_fail(BX_ERR_ARG, "the implicit step of a partitioned grid is not built");
   if (c.shape != kShape888 && c.shape != kShape444)
     return core_fail(BX_ERR_ARG, "the implicit scheme needs 3D 8x8x8 or 4x4x4 blocks");
   if (c.sch.Precision != BX_FP64) return core_fail(BX_ERR_ARG, "the implicit scheme runs in FP64 mode");

@@ -29,11 +29,15 @@ from .capi import check, dptr
 
 
 class ExplicitSolver:
-    def __init__(self, grid, scheme, device=0):
+    def __init__(self, grid, scheme, device=0, nOwned=0):
+        """nOwned > 0: one rank of a partitioned grid whose first nOwned
+        blocks it updates (batsrus_b200.shard.RankDomain); the other blocks
+        are copies of remote neighbours."""
         self.L = capi.load()
         self.grid = grid
         self.scheme = scheme
-        self._gd = capi.grid_desc(grid, device)
+        self.nOwned = nOwned if nOwned > 0 else grid.nBlock
+        self._gd = capi.grid_desc(grid, device, nOwned)
         self._sp = capi.scheme_params(scheme)
         check(self.L.bx_init(ctypes.byref(self._gd), ctypes.byref(self._sp)))
 
@@ -131,6 +135,35 @@ class ExplicitSolver:
         dt = ctypes.c_double()
         check(self.L.bx_set_global_timestep(TimeSimulationLimit, ctypes.byref(dt)))
         return dt.value
+
+    # -- one rank of a partitioned grid ------------------------------------
+    def halo_bytes(self, iStage):
+        n = ctypes.c_int()
+        check(self.L.bx_halo_bytes(iStage, ctypes.byref(n)))
+        return n.value
+
+    def halo_pack(self, iStage, blocks, buf_ptr):
+        """the interiors of blocks (0-based local indices) that stage iStage
+        reads, into the device buffer at buf_ptr"""
+        b = np.ascontiguousarray(np.asarray(blocks) + 1, dtype=np.int32)
+        check(self.L.bx_halo_pack(iStage, b.ctypes.data_as(ctypes.POINTER(ctypes.c_int)), len(b),
+                                  ctypes.c_void_p(buf_ptr)))
+
+    def halo_unpack(self, iStage, blocks, buf_ptr):
+        b = np.ascontiguousarray(np.asarray(blocks) + 1, dtype=np.int32)
+        check(self.L.bx_halo_unpack(iStage, b.ctypes.data_as(ctypes.POINTER(ctypes.c_int)), len(b),
+                                    ctypes.c_void_p(buf_ptr)))
+
+    def get_dtmin(self):
+        v = ctypes.c_double()
+        check(self.L.bx_get_dtmin(ctypes.byref(v)))
+        return v.value
+
+    def set_dtmin(self, v):
+        check(self.L.bx_set_dtmin(float(v)))
+
+    def end_step(self, TimeSimulationLimit=-1.0):
+        check(self.L.bx_end_step(TimeSimulationLimit))
 
     def advance_explicit(self, DoCalcTimestep=True):
         check(self.L.bx_advance_explicit(int(DoCalcTimestep)))

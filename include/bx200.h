@@ -71,6 +71,10 @@ typedef struct {
   int nBlock;
   const int *iLevelCoord_IB; /* 4 ints per block: level, ix, iy, iz */
   int iDevice;           /* CUDA device ordinal */
+  int nOwned;            /* one rank of a partitioned grid: blocks 1..nOwned
+                            are updated, the others are copies of remote
+                            neighbours (halo blocks) that supply ghost cells
+                            and resolution-change fluxes; 0: all blocks */
 } bx_grid_desc;
 
 /* Scheme: the #SCHEME / #TIMESTEPPING / #FIXEDTIMESTEP / #GAMMA state that
@@ -302,6 +306,38 @@ BX_API int bx_impl_get_x(double *x_I);
  * Independent of bx_init. */
 #define BX_NOALLOC_MAX_BLOCK 32768
 BX_API int bx_impl_norm_noalloc(const double *Impl_dev, int nCellBlock, int nBlock, void *stream, double *Norm_V);
+
+/* ---- one rank of a partitioned grid --------------------------------------
+ * The reference's MPI ranks exchange ghost cells inside BATL's
+ * message_pass_cell / message_pass_face (call sites src/ModMessagePass.f90:
+ * 147-226, src/ModAdvanceExplicit.f90:127) and reduce the time step with
+ * MPI_allreduce MIN (src/ModTimeStepControl.f90:392).  Here a rank's grid
+ * (bx_init with nOwned > 0) holds full copies of the remote blocks its
+ * blocks read; the caller moves their interiors between ranks before every
+ * stage and reduces the time step:
+ *   bx_set_dtmin(global minimum of bx_get_dtmin over the ranks)
+ *   bx_set_global_timestep(tLimit, &Dt)
+ *   for iStage = 1..nStage:
+ *     bx_halo_pack(iStage, sent blocks, buffer)   -> send to the peers
+ *     receive from the peers -> bx_halo_unpack(iStage, halo blocks, buffer)
+ *     bx_set_stage(iStage); bx_update_state_fast()
+ *   bx_end_step(tLimit)
+ * Buffers are device memory of the caller: nBlock interiors of the state
+ * that stage iStage reads, bx_halo_bytes(iStage) bytes each (FP64, or FP32
+ * for stage 2 of FP32-bulk), in the block order of the list (1-based local
+ * block indices).  bx_halo_pack returns with the buffer complete;
+ * bx_halo_unpack is ordered before the next stage on the library's stream.
+ * No kernel reads another GPU's memory. */
+BX_API int bx_halo_bytes(int iStage, int *BytesPerBlock);
+BX_API int bx_halo_pack(int iStage, const int *iBlock_I, int nBlock, void *Buf_dev);
+BX_API int bx_halo_unpack(int iStage, const int *iBlock_I, int nBlock, const void *Buf_dev);
+/* the smallest cell time step of this rank's blocks from the last step, and
+ * the global minimum that the next bx_set_global_timestep uses */
+BX_API int bx_get_dtmin(double *DtMin);
+BX_API int bx_set_dtmin(double DtMin);
+/* end of BATS_advance after the stages: tSimulation += Dt and the final
+ * adjustment to the time limit (src/ModBatsrusMethods.f90:606-640) */
+BX_API int bx_end_step(double tLimit);
 
 /* ---- learned per-block preconditioner -------------------------------------
  * No counterpart in the reference: a new #PRECONDITIONER value LEARNED for

@@ -29,6 +29,7 @@ module bx200_interface
      integer(c_int):: nBlock
      type(c_ptr)   :: iLevelCoord_IB   ! c_loc of integer(c_int) (4,nBlock)
      integer(c_int):: iDevice
+     integer(c_int):: nOwned           ! 0: all blocks are this rank's
   end type bx_grid_desc
 
   integer(c_int), parameter:: BX_PRECOND_NONE = 0, BX_PRECOND_BILU = 1, &
@@ -164,6 +165,35 @@ module bx200_interface
        real(c_double), value:: TimeSimulationLimit
        real(c_double), intent(out):: Dt
      end function bx_set_global_timestep
+     integer(c_int) function bx_halo_bytes(iStage, BytesPerBlock) bind(C, name='bx_halo_bytes')
+       import:: c_int
+       integer(c_int), value:: iStage
+       integer(c_int), intent(out):: BytesPerBlock
+     end function bx_halo_bytes
+     integer(c_int) function bx_halo_pack(iStage, iBlock_I, nBlock, Buf_dev) bind(C, name='bx_halo_pack')
+       import:: c_int, c_ptr
+       integer(c_int), value:: iStage, nBlock
+       integer(c_int), intent(in):: iBlock_I(*)
+       type(c_ptr), value:: Buf_dev
+     end function bx_halo_pack
+     integer(c_int) function bx_halo_unpack(iStage, iBlock_I, nBlock, Buf_dev) bind(C, name='bx_halo_unpack')
+       import:: c_int, c_ptr
+       integer(c_int), value:: iStage, nBlock
+       integer(c_int), intent(in):: iBlock_I(*)
+       type(c_ptr), value:: Buf_dev
+     end function bx_halo_unpack
+     integer(c_int) function bx_get_dtmin(DtMin) bind(C, name='bx_get_dtmin')
+       import:: c_int, c_double
+       real(c_double), intent(out):: DtMin
+     end function bx_get_dtmin
+     integer(c_int) function bx_set_dtmin(DtMin) bind(C, name='bx_set_dtmin')
+       import:: c_int, c_double
+       real(c_double), value:: DtMin
+     end function bx_set_dtmin
+     integer(c_int) function bx_end_step(tLimit) bind(C, name='bx_end_step')
+       import:: c_int, c_double
+       real(c_double), value:: tLimit
+     end function bx_end_step
 
      integer(c_int) function bx_advance_explicit(DoCalcTimestep) &
           bind(C, name='bx_advance_explicit')
