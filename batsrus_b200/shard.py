@@ -128,3 +128,84 @@ class RankDomain:
             got = send_recv(p, np.ascontiguousarray(out), (n,) + interiors.shape[1:])
             if n:
                 interiors[self.recv[p]] = got
+
+
+class GpuRank:
+    """One rank of the partitioned explicit update on its GPU: an
+    ExplicitSolver over the rank's block list (owned blocks, then halo
+    copies) and, before every stage, the pairwise exchange of halo interiors
+    through torch.distributed; the time step is an all_reduce MIN.  With
+    the NCCL backend the buffers stay on the GPU; with gloo they go through
+    host memory.  Every exchange completes on the host before the next
+    stage is launched, so no kernel waits on another rank.
+
+    The sequence per step is the one of the C ABI (include/bx200.h, "one
+    rank of a partitioned grid"): bx_get_dtmin -> MIN -> bx_set_dtmin ->
+    bx_set_global_timestep -> (exchange, bx_set_stage, bx_update_state_fast)
+    per stage -> bx_end_step."""
+
+    def __init__(self, grid, scheme, nRank, rank, device=0, weights=None):
+        from .explicit import ExplicitSolver
+        self.dom = RankDomain(grid, partition(grid, nRank, weights), rank)
+        self.device = device
+        self.x = ExplicitSolver(self.dom.grid, scheme, device=device, nOwned=self.dom.nOwned)
+        self.nStage = scheme.nStage
+
+    def set_state(self, State_VGB):
+        """the global State_VGB (all blocks, reference layout): this rank's
+        owned blocks and halo copies are taken from it"""
+        self.x.set_state(np.ascontiguousarray(State_VGB[self.dom.glob]))
+
+    def get_owned_state(self):
+        """State_VGB of the owned blocks (their global indices: dom.glob[:nOwned])"""
+        return self.x.get_state()[:self.dom.nOwned]
+
+    def time(self):
+        return self.x.time()
+
+    def close(self):
+        self.x.close()
+
+    def _exchange(self, iStage):
+        import torch
+        import torch.distributed as dist
+        nb = self.x.halo_bytes(iStage)
+        dtype = torch.float32 if nb == 4 * 8 * self.x.grid.nI * self.x.grid.nJ * self.x.grid.nK else torch.float64
+        per = nb // (4 if dtype == torch.float32 else 8)
+        dev = torch.device("cuda", self.device)
+        onGpu = dist.get_backend() == "nccl"
+        d = self.dom
+        for p in range(d.nRank):
+            if p == d.rank or (p not in d.send and p not in d.recv):
+                continue
+            reqs = []
+            if p in d.send:
+                out = torch.empty(len(d.send[p]) * per, dtype=dtype, device=dev)
+                self.x.halo_pack(iStage, d.send[p], out.data_ptr())
+                reqs.append(dist.isend(out if onGpu else out.cpu(), dst=p))
+            got = None
+            if p in d.recv:
+                got = torch.empty(len(d.recv[p]) * per, dtype=dtype, device=dev if onGpu else "cpu")
+                reqs.append(dist.irecv(got, src=p))
+            for r in reqs:
+                r.wait()
+            if got is not None:
+                g = got if onGpu else got.to(dev)
+                torch.cuda.current_stream(dev).synchronize()
+                self.x.halo_unpack(iStage, d.recv[p], g.data_ptr())
+
+    def advance(self, nStep=1, TimeSimulationLimit=-1.0):
+        import torch
+        import torch.distributed as dist
+        for _ in range(nStep):
+            onGpu = dist.get_backend() == "nccl"
+            dt = torch.tensor([self.x.get_dtmin()], dtype=torch.float64,
+                              device=torch.device("cuda", self.device) if onGpu else "cpu")
+            dist.all_reduce(dt, op=dist.ReduceOp.MIN)
+            self.x.set_dtmin(float(dt.item()))
+            self.x.set_global_timestep(TimeSimulationLimit)
+            for s in range(1, self.nStage + 1):
+                self._exchange(s)
+                self.x.set_stage(s)
+                self.x.update_state_fast()
+            self.x.end_step(TimeSimulationLimit)

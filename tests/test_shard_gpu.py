@@ -144,3 +144,48 @@ def test_rank_api_rejects_misuse():
     with pytest.raises(capi.BxError):
         x.calc_face_value(d.nOwned + 1)
     x.close()
+
+
+def _gpu_rank_process(rank, world, port, out_dir, name, precision):
+    import datetime
+    import os
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port), RANK=str(rank), WORLD_SIZE=str(world))
+    import torch.distributed as dist
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=120))
+    g, s, st = case(name, precision)
+    r = shard.GpuRank(g, s, world, rank, device=0)
+    r.set_state(st)
+    r.advance(3)
+    np.save(os.path.join(out_dir, "s%d.npy" % rank), r.get_owned_state()[g.interior_slices()])
+    np.save(os.path.join(out_dir, "g%d.npy" % rank), r.dom.glob[:r.dom.nOwned])
+    r.close()
+    dist.barrier()
+    dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("name,world", [("ot", 2), ("amr", 2)])
+def test_gpu_ranks_in_two_processes(tmp_path, name, world):
+    """shard.GpuRank in two processes (gloo through host memory, both
+    contexts on GPU 0; each exchange completes on the host before the next
+    launch): the owned blocks of both ranks match the single-domain oracle
+    within 1e-12 after three steps."""
+    import os
+    import socket
+    import torch.multiprocessing as mp
+    with socket.socket() as so:
+        so.bind(("127.0.0.1", 0))
+        port = so.getsockname()[1]
+    mp.spawn(_gpu_rank_process, args=(world, port, str(tmp_path), name, "fp64"), nprocs=world, join=True)
+    g, s, st = case(name, "fp64")
+    ref = Oracle(g, s)
+    ref.set_state(st)
+    ref.exchange_messages()
+    ref.advance(3)
+    R = ref.get_state()[g.interior_slices()]
+    seen = np.zeros(g.nBlock, dtype=bool)
+    for q in range(world):
+        S = np.load(os.path.join(str(tmp_path), "s%d.npy" % q))
+        glob = np.load(os.path.join(str(tmp_path), "g%d.npy" % q))
+        seen[glob] = True
+        assert rel_err(S, R[glob]) < 1e-12, q
+    assert seen.all()
