@@ -197,15 +197,18 @@ class GpuRank:
     def advance(self, nStep=1, TimeSimulationLimit=-1.0):
         import torch
         import torch.distributed as dist
+        multi = dist.is_available() and dist.is_initialized() and self.dom.nRank > 1
         for _ in range(nStep):
-            onGpu = dist.get_backend() == "nccl"
-            dt = torch.tensor([self.x.get_dtmin()], dtype=torch.float64,
-                              device=torch.device("cuda", self.device) if onGpu else "cpu")
-            dist.all_reduce(dt, op=dist.ReduceOp.MIN)
-            self.x.set_dtmin(float(dt.item()))
+            if multi:
+                onGpu = dist.get_backend() == "nccl"
+                dt = torch.tensor([self.x.get_dtmin()], dtype=torch.float64,
+                                  device=torch.device("cuda", self.device) if onGpu else "cpu")
+                dist.all_reduce(dt, op=dist.ReduceOp.MIN)
+                self.x.set_dtmin(float(dt.item()))
             self.x.set_global_timestep(TimeSimulationLimit)
             for s in range(1, self.nStage + 1):
-                self._exchange(s)
+                if multi:
+                    self._exchange(s)
                 self.x.set_stage(s)
                 self.x.update_state_fast()
             self.x.end_step(TimeSimulationLimit)
