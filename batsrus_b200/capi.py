@@ -54,7 +54,7 @@ class ImplicitParamsC(ctypes.Structure):
         ("CflImpl", ctypes.c_double), ("ImplCoeff", ctypes.c_double), ("UseBdf2", ctypes.c_int),
         ("nOrderImpl", ctypes.c_int), ("TypeFluxImpl", ctypes.c_int), ("JacobianEps", ctypes.c_double),
         ("nKrylovVector", ctypes.c_int), ("MaxMatvec", ctypes.c_int), ("ErrorMax", ctypes.c_double),
-        ("TypePrecond", ctypes.c_int),
+        ("TypePrecond", ctypes.c_int), ("PrecondPrecision", ctypes.c_int),
     ]
 
 
@@ -115,6 +115,7 @@ def implicit_params(p):
     c.MaxMatvec = p.maxMatvec
     c.ErrorMax = p.errorMax
     c.TypePrecond = PRECOND[p.typePrecond.lower()]
+    c.PrecondPrecision = PRECISION[p.precondPrecision.lower()]
     return c
 
 

@@ -108,13 +108,16 @@ def uniform_3d_case(nRoot, flux, limiter="mc3", beta=1.2, precision="fp64", nCel
     return g, s, st, {}
 
 
-def jfnk_ot(nRoot=16, precond="BILU", seed=2024, with_state=True):
+def jfnk_ot(nRoot=16, precond="BILU", seed=2024, with_state=True, precondPrecision="fp32"):
+    """The implicit workload: perturbed Orszag-Tang on (8 nRoot)^3 cells,
+    BDF2 at CFL 20, GMRES(30) to 1e-3; BILU factors stored in FP32 unless
+    precondPrecision says otherwise."""
     from .implicit_params import ImplicitParams
     g = BlockGrid.uniform(3, (8, 8, 8), (nRoot,) * 3, (0.0, 0.0, 0.0), (1.0, 1.0, 1.0), ("periodic",) * 6)
     s = Scheme(nOrder=2, nStage=2, typeFlux="Linde", typeLimiter="mc3", limiterBeta=1.2, cfl=0.8,
                gamma=5.0 / 3.0, useDivbSource=True, useHalfStep=True)
     p = ImplicitParams(cflImpl=20.0, useBdf2=True, nKrylovVector=30, maxMatvec=100, errorMax=1e-3,
-                       typePrecond=precond)
+                       typePrecond=precond, precondPrecision=precondPrecision)
     st = initial.perturbed_ot(g, seed=seed, amplitude=1e-2, kmax=8) if with_state else None
     return g, s, p, st
 

@@ -180,7 +180,8 @@ struct JacArgs {
   const double *U;      // implicit state U^n (SoA)
   const int *nbr;       // neighbour table
   const BlockGeom *geom;
-  double *Jac;          // [block][cell][7][8][8]
+  void *F;              // BILU storage (see BiluLayout), element type of the launch
+  const int *wfPos;     // position of every cell of a block in wavefront order
   const double *norm;   // Norm_V
   double gamma, gm1, invGm1, sqrtJacEps, dtImplCoeff;
   int useDivb, nBlock;
@@ -203,12 +204,93 @@ __device__ __forceinline__ void load_cell(const JacArgs &a, int b, int i, int j,
   for (int v = 0; v < 8; v++) U[v] = p[v * NC];
 }
 
-// one thread per (cell, perturbed variable jv): column jv of the 7 stencil
-// blocks of the cell's rows
-template <int N, int D>
+// Storage of the block ILU(0) of one grid block of NC cells, element type T,
+// 7 x 64 values per cell; p is the position of cell c in wavefront order
+// (cells with i+j+k = 0 first, then 1, ...), so that the cells of one
+// wavefront are contiguous:
+//   fwd [p][4][8][8]  blocks 0..2: A(c, c-e_d) for d = x, y, z (absent on
+//                     the low faces of the block); block 3: A(c, c), which
+//                     the factorisation replaces by D_c^-1
+//   bwd [p][3][8][8]  A(c, c+e_d) (absent on the high faces); with FP32
+//                     storage the factorisation replaces it by
+//                     D_c^-1 A(c, c+e_d), so that the backward sweep reads
+//                     three blocks per cell instead of four.  FP64 storage
+//                     keeps A(c, c+e_d) and the operation order of the
+//                     reference's solver (D_c^-1 applied to the sum).
+// fwd is what the forward sweep reads, bwd what the backward sweep reads.
+// The storage of grid block b starts at b NC 448 elements, its bwd part
+// NC 256 elements later.  Blocks are row-major (row = equation iv, column =
+// perturbed variable jv).  Absent blocks are never written nor read.
+template <int N>
+struct BiluLayout {
+  static constexpr int NC = N * N * N;
+  static constexpr long kPerBlock = (long)NC * 7 * 64;
+  __device__ static __forceinline__ long fwd(int b, int p, int blk) { return b * kPerBlock + ((long)p * 4 + blk) * 64; }
+  __device__ static __forceinline__ long bwd(int b, int p, int d) {
+    return b * kPerBlock + (long)NC * 256 + ((long)p * 3 + d) * 64;
+  }
+};
+
+__device__ __forceinline__ void store_t(double *p, double v) { *p = v; }
+__device__ __forceinline__ void store_t(float *p, double v) { *p = (float)v; }
+
+// one row of 8 elements (32 or 64 contiguous bytes) into FP64 registers
+__device__ __forceinline__ void load_row8(const double *p, double (&r)[8]) {
+  const double2 *q = reinterpret_cast<const double2 *>(p);
+#pragma unroll
+  for (int m = 0; m < 4; m++) {
+    const double2 t = q[m];
+    r[2 * m] = t.x;
+    r[2 * m + 1] = t.y;
+  }
+}
+__device__ __forceinline__ void load_row8(const float *p, double (&r)[8]) {
+  const float4 *q = reinterpret_cast<const float4 *>(p);
+#pragma unroll
+  for (int m = 0; m < 2; m++) {
+    const float4 t = q[m];
+    r[4 * m] = t.x; r[4 * m + 1] = t.y; r[4 * m + 2] = t.z; r[4 * m + 3] = t.w;
+  }
+}
+__device__ __forceinline__ void store_row8(double *p, const double (&r)[8]) {
+  double2 *q = reinterpret_cast<double2 *>(p);
+#pragma unroll
+  for (int m = 0; m < 4; m++) q[m] = make_double2(r[2 * m], r[2 * m + 1]);
+}
+__device__ __forceinline__ void store_row8(float *p, const double (&r)[8]) {
+  float4 *q = reinterpret_cast<float4 *>(p);
+#pragma unroll
+  for (int m = 0; m < 2; m++)
+    q[m] = make_float4((float)r[4 * m], (float)r[4 * m + 1], (float)r[4 * m + 2], (float)r[4 * m + 3]);
+}
+
+// the div B source coefficient of row iv of the row cell (state Uc) that
+// enters the column Bx+D of its off-diagonal blocks (impl_divbsrc_init,
+// src/ModPartImplicit.f90)
+__device__ __forceinline__ double pow_coeff(const double (&Uc)[8], int iv) {
+  switch (iv) {
+    case kUx: return Uc[kBx];
+    case kUy: return Uc[kBy];
+    case kUz: return Uc[kBz];
+    case kBx: return Uc[kUx] / Uc[kRho];
+    case kBy: return Uc[kUy] / Uc[kRho];
+    case kBz: return Uc[kUz] / Uc[kRho];
+    case kP: return (Uc[kBx] * Uc[kUx] + Uc[kBy] * Uc[kUy] + Uc[kBz] * Uc[kUz]) / Uc[kRho];
+    default: return 0.0;
+  }
+}
+
+// Column jv of the derivative of the flux of cell n in direction D enters
+// three blocks of the 7-point Jacobian: the diagonal block of n, the block
+// A(n+e_D, n) of the cell above (its lower-neighbour block, through the
+// face n+1/2) and the block A(n-e_D, n) of the cell below (its
+// upper-neighbour block, through the face n-1/2).  Thread (n, jv) evaluates
+// the derivative once and writes its column of the last two; every column
+// of every block has one writer.  The face Rusanov coefficients are
+// cmaxLo = -Cmax(n-1/2)/2 and cmaxHi = -Cmax(n+1/2)/2 of get_cmax_face.
+template <int N, int D, typename T>
 __device__ __forceinline__ void jac_dir(const JacArgs &a, int b, int i, int j, int k, int jv, const double (&U0)[8],
-                                        const double (&sPow)[8], const BlockGeom &g, double (&diag)[8],
-                                        double *Jrow) {
+                                        const BlockGeom &g, double (&diag)[8], T *F, const double (&sc)[8]) {
   const int idx[3] = {i, j, k};
   double UL[8], UR[8];
   load_cell<N>(a, b, i - (D == 0), j - (D == 1), k - (D == 2), UL);
@@ -220,55 +302,51 @@ __device__ __forceinline__ void jac_dir(const JacArgs &a, int b, int i, int j, i
   const double coeff = -0.5 / (a.sqrtJacEps * a.norm[jv]);
   const double coeffPow = -0.5 / g.cellSize[D];
   const bool powCol = a.useDivb && jv == kBx + D;
-  double F0[8], Fe[8], Ue[8];
-  // own cell: diagonal block
+  double F0[8], Fe[8], Ue[8], dF[8];
   cell_flux_e<D>(U0, a.gm1, a.invGm1, area, F0);
 #pragma unroll
-  for (int v = 0; v < 8; v++) Ue[v] = U0[v];
-  Ue[jv] = U0[jv] + epsj;
+  for (int v = 0; v < 8; v++) Ue[v] = v == jv ? U0[v] + epsj : U0[v];  // no dynamic index: stays in registers
   cell_flux_e<D>(Ue, a.gm1, a.invGm1, area, Fe);
 #pragma unroll
   for (int iv = 0; iv < 8; iv++) {
-    const double dF = coeff * (Fe[iv] - F0[iv]);
-    double left = dF, right = dF;
+    dF[iv] = coeff * (Fe[iv] - F0[iv]);
+    double left = dF[iv], right = dF[iv];
     if (iv == jv) { left = left + cmaxHi; right = right - cmaxLo; }
     diag[iv] = diag[iv] - right / V + left / V;
   }
-  // lower neighbour in the block: -dFdWLeft(face c) from cell c-1
-  if (idx[D] > 0) {
-    cell_flux_e<D>(UL, a.gm1, a.invGm1, area, F0);
-#pragma unroll
-    for (int v = 0; v < 8; v++) Ue[v] = UL[v];
-    Ue[jv] = UL[jv] + epsj;
-    cell_flux_e<D>(Ue, a.gm1, a.invGm1, area, Fe);
+  const int c = i + N * (j + N * k);
+  constexpr int st = D == 0 ? 1 : (D == 1 ? N : N * N);
+  // A(n+e_D, n) = -dFdWLeft(face n+1/2): lower-neighbour block D of cell n+e_D
+  if (idx[D] < N - 1) {
+    T *dst = F + BiluLayout<N>::fwd(b, a.wfPos[c + st], D) + jv;
 #pragma unroll
     for (int iv = 0; iv < 8; iv++) {
-      double left = coeff * (Fe[iv] - F0[iv]);
-      if (iv == jv) left = left + cmaxLo;
+      double left = dF[iv];
+      if (iv == jv) left = left + cmaxHi;
       left = left / V;
-      if (powCol && iv != kRho) left = left + coeffPow * sPow[iv];
-      Jrow[(1 + 2 * D) * 64 + iv * 8] = -left;
+      if (powCol && iv != kRho) left = left + coeffPow * pow_coeff(UR, iv);
+      store_t(dst + iv * 8, left * sc[iv]);
     }
   }
-  // upper neighbour in the block: +dFdWRight(face c+1) from cell c+1
-  if (idx[D] < N - 1) {
-    cell_flux_e<D>(UR, a.gm1, a.invGm1, area, F0);
-#pragma unroll
-    for (int v = 0; v < 8; v++) Ue[v] = UR[v];
-    Ue[jv] = UR[jv] + epsj;
-    cell_flux_e<D>(Ue, a.gm1, a.invGm1, area, Fe);
+  // A(n-e_D, n) = +dFdWRight(face n-1/2): upper-neighbour block D of cell n-e_D
+  if (idx[D] > 0) {
+    T *dst = F + BiluLayout<N>::bwd(b, a.wfPos[c - st], D) + jv;
 #pragma unroll
     for (int iv = 0; iv < 8; iv++) {
-      double right = coeff * (Fe[iv] - F0[iv]);
-      if (iv == jv) right = right - cmaxHi;
+      double right = dF[iv];
+      if (iv == jv) right = right - cmaxLo;
       right = right / V;
-      if (powCol && iv != kRho) right = right + coeffPow * sPow[iv];
-      Jrow[(2 + 2 * D) * 64 + iv * 8] = right;
+      if (powCol && iv != kRho) right = right + coeffPow * pow_coeff(UL, iv);
+      store_t(dst + iv * 8, -right * sc[iv]);
     }
   }
 }
 
-template <int N>
+// impl_jacobian: the normalised matrix I - dt ImplCoeff dR/dU of the
+// first-order Rusanov residual with Powell source, one thread per (cell,
+// perturbed variable jv), written straight into the BILU storage (every
+// element once, no clearing pass)
+template <int N, typename T>
 __global__ void k_jacobian(JacArgs a) {
   constexpr int NC = N * N * N;
   const long q = blockIdx.x * (long)blockDim.x + threadIdx.x;
@@ -278,14 +356,16 @@ __global__ void k_jacobian(JacArgs a) {
   const int b = (int)(cg / NC), c = (int)(cg % NC);
   const int i = c % N, j = (c / N) % N, k = c / (N * N);
   const BlockGeom g = a.geom[b];
+  T *F = static_cast<T *>(a.F);
   double U0[8];
   load_cell<N>(a, b, i, j, k, U0);
-  double *Jrow = a.Jac + ((size_t)b * NC + c) * 7 * 64 + jv;  // column jv
-  for (int s = 0; s < 7; s++)
+  // time-accurate scaling of row iv, column jv
+  double sc[8];
+  const double nj = a.norm[jv];
 #pragma unroll
-    for (int iv = 0; iv < 8; iv++) Jrow[s * 64 + iv * 8] = 0.0;
-  // impl_divbsrc_init
-  double sPow[8] = {0, 0, 0, 0, 0, 0, 0, 0}, divB = 0;
+  for (int iv = 0; iv < 8; iv++) sc[iv] = a.dtImplCoeff * nj / a.norm[iv];
+  // impl_divbsrc_init: div B of the cell
+  double divB = 0;
   if (a.useDivb) {
     double Up[8], Um[8];
     load_cell<N>(a, b, i + 1, j, k, Up); load_cell<N>(a, b, i - 1, j, k, Um);
@@ -295,14 +375,11 @@ __global__ void k_jacobian(JacArgs a) {
     load_cell<N>(a, b, i, j, k + 1, Up); load_cell<N>(a, b, i, j, k - 1, Um);
     dv = dv + (Up[kBz] - Um[kBz]) / g.cellSize[2];
     divB = 0.5 * dv;
-    for (int m = 0; m < 3; m++) sPow[kUx + m] = U0[kBx + m];
-    for (int m = 0; m < 3; m++) sPow[kBx + m] = U0[kUx + m] / U0[kRho];
-    sPow[kP] = (U0[kBx] * U0[kUx] + U0[kBy] * U0[kUy] + U0[kBz] * U0[kUz]) / U0[kRho];
   }
   double diag[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-  jac_dir<N, 0>(a, b, i, j, k, jv, U0, sPow, g, diag, Jrow);
-  jac_dir<N, 1>(a, b, i, j, k, jv, U0, sPow, g, diag, Jrow);
-  jac_dir<N, 2>(a, b, i, j, k, jv, U0, sPow, g, diag, Jrow);
+  jac_dir<N, 0>(a, b, i, j, k, jv, U0, g, diag, F, sc);
+  jac_dir<N, 1>(a, b, i, j, k, jv, U0, g, diag, F, sc);
+  jac_dir<N, 2>(a, b, i, j, k, jv, U0, g, diag, F, sc);
   // impl_divbsrc_middle: diagonal Powell terms of column jv
   if (a.useDivb) {
     const double rho = U0[kRho];
@@ -316,14 +393,9 @@ __global__ void k_jacobian(JacArgs a) {
     if (jv == kRho)
       diag[kP] = diag[kP] + divB * (U0[kUx] * U0[kBx] + U0[kUy] * U0[kBy] + U0[kUz] * U0[kBz]) / (rho * rho);
   }
-  // time-accurate scaling and the identity
-  const double nj = a.norm[jv];
+  T *dst = F + BiluLayout<N>::fwd(b, a.wfPos[c], 3) + jv;
 #pragma unroll
-  for (int iv = 0; iv < 8; iv++) {
-    const double sc = a.dtImplCoeff * nj / a.norm[iv];
-    Jrow[iv * 8] = -diag[iv] * sc + (iv == jv ? 1.0 : 0.0);
-    for (int s = 1; s < 7; s++) Jrow[s * 64 + iv * 8] = -Jrow[s * 64 + iv * 8] * sc;
-  }
+  for (int iv = 0; iv < 8; iv++) store_t(dst + iv * 8, -diag[iv] * sc[iv] + (iv == jv ? 1.0 : 0.0));
 }
 
 // ---------------------------------------------------------------------------
@@ -332,9 +404,9 @@ __global__ void k_jacobian(JacArgs a) {
 // ones).  Eight lanes of a warp hold the eight rows of a cell's 8x8 blocks.
 
 struct BiluArgs {
-  const double *Jac;   // [block][cell][7][8][8]
-  double *Dinv;        // [block][cell][8][8]
-  const int *wfCell;   // cells sorted by wavefront
+  void *F;             // BILU storage (BiluLayout), element type of the launch
+  const int *wfCell;   // cells sorted by wavefront (position -> cell)
+  const int *wfPos;    // cell -> position
   const int *wfStart;  // nWave+1 offsets
   int nWave, nBlock;
   const double *r;     // solve: input vector (SoA)
@@ -378,131 +450,164 @@ __device__ __forceinline__ void group_inverse8(double (&a)[8], double (&inv)[8],
   }
 }
 
-template <int N>
+// D_c = A(c,c) - sum_d A(c,c-e_d) D_{c-e_d}^-1 A(c-e_d,c), stored as D_c^-1
+// (FP64 arithmetic, stored with the element type T).  FP64 storage follows
+// the reference's order, (A(c,c-e_d) D^-1) A(c-e_d,c); FP32 storage reads
+// the premultiplied D^-1 A(c-e_d,c) of the lower neighbour and replaces
+// A(c,c+e_d) by D_c^-1 A(c,c+e_d) once D_c^-1 is known.
+template <int N, typename T>
 __global__ void k_bilu_factor(BiluArgs a) {
-  constexpr int NC = N * N * N;
+  constexpr bool kPre = sizeof(T) == 4;
   const int b = blockIdx.x;
   const int slot = threadIdx.x >> 3, row = threadIdx.x & 7;
-  const double *J = a.Jac + (size_t)b * NC * 7 * 64;
-  double *Di = a.Dinv + (size_t)b * NC * 64;
+  T *F = static_cast<T *>(a.F);
   for (int w = 0; w < a.nWave; w++) {
     const int s0 = a.wfStart[w], n = a.wfStart[w + 1] - s0;
     for (int base = 0; base < n; base += (int)(blockDim.x >> 3)) {
       const bool active = base + slot < n;
-      const int c = active ? a.wfCell[s0 + base + slot] : 0;
+      const int p = s0 + base + slot;
+      const int c = active ? a.wfCell[p] : 0;
       const int i = c % N, j = (c / N) % N, k = c / (N * N);
-      double D[8];
-#pragma unroll
-      for (int q = 0; q < 8; q++) D[q] = active ? J[((size_t)c * 7) * 64 + row * 8 + q] : (q == row ? 1.0 : 0.0);
       const int idx[3] = {i, j, k};
+      double D[8];
+      if (active) load_row8(F + BiluLayout<N>::fwd(b, p, 3) + row * 8, D);
+      else
+#pragma unroll
+        for (int q = 0; q < 8; q++) D[q] = q == row ? 1.0 : 0.0;
 #pragma unroll
       for (int d = 0; d < 3; d++) {
         if (!active || idx[d] == 0) continue;
-        const int cl = c - (d == 0 ? 1 : (d == 1 ? N : N * N));
-        const double *L = J + ((size_t)c * 7 + 1 + 2 * d) * 64 + row * 8;   // A_cn row
-        const double *Dn = Di + (size_t)cl * 64;
-        const double *U = J + ((size_t)cl * 7 + 2 + 2 * d) * 64;            // A_nc
-        double T1[8];
+        const int pl = a.wfPos[c - (d == 0 ? 1 : (d == 1 ? N : N * N))];
+        double L[8];
+        load_row8(F + BiluLayout<N>::fwd(b, p, d) + row * 8, L);
+        const T *Un = F + BiluLayout<N>::bwd(b, pl, d);  // A(cl, c), or D_cl^-1 A(cl, c)
+        if (!kPre) {
+          const T *Dn = F + BiluLayout<N>::fwd(b, pl, 3);
+          double T1[8] = {0, 0, 0, 0, 0, 0, 0, 0};
 #pragma unroll
-        for (int q = 0; q < 8; q++) {
-          double s = 0;
+          for (int m = 0; m < 8; m++) {
+            double dr[8];
+            load_row8(Dn + m * 8, dr);
 #pragma unroll
-          for (int m = 0; m < 8; m++) s += L[m] * Dn[m * 8 + q];
-          T1[q] = s;
+            for (int q = 0; q < 8; q++) T1[q] += L[m] * dr[q];
+          }
+#pragma unroll
+          for (int q = 0; q < 8; q++) L[q] = T1[q];
+        }
+        double T2[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+#pragma unroll
+        for (int m = 0; m < 8; m++) {
+          double u[8];
+          load_row8(Un + m * 8, u);
+#pragma unroll
+          for (int q = 0; q < 8; q++) T2[q] += L[m] * u[q];
         }
 #pragma unroll
-        for (int q = 0; q < 8; q++) {
-          double s = 0;
-#pragma unroll
-          for (int m = 0; m < 8; m++) s += T1[m] * U[m * 8 + q];
-          D[q] -= s;
-        }
+        for (int q = 0; q < 8; q++) D[q] -= T2[q];
       }
       double inv[8];
       group_inverse8(D, inv, row);
-      if (active)
+      if (active) store_row8(F + BiluLayout<N>::fwd(b, p, 3) + row * 8, inv);
+      if (kPre) {
 #pragma unroll
-        for (int q = 0; q < 8; q++) Di[(size_t)c * 64 + row * 8 + q] = inv[q];
+        for (int d = 0; d < 3; d++) {
+          const bool has = active && idx[d] < N - 1;
+          double A[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+          if (has) load_row8(F + BiluLayout<N>::bwd(b, p, d) + row * 8, A);
+          double out[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+#pragma unroll
+          for (int m = 0; m < 8; m++)
+#pragma unroll
+            for (int q = 0; q < 8; q++) out[q] += inv[m] * __shfl_sync(0xffffffffu, A[q], m, 8);
+          if (has) store_row8(F + BiluLayout<N>::bwd(b, p, d) + row * 8, out);
+        }
+      }
     }
     __syncthreads();
   }
 }
 
-template <int N>
+// z = (LU)^-1 r on every grid block: forward v_c = D_c^-1 (r_c - sum_d
+// A(c,c-e_d) v_{c-e_d}), backward x_c = v_c - D_c^-1 sum_d A(c,c+e_d)
+// x_{c+e_d} (FP32 storage: the premultiplied blocks), in shared memory;
+// FP64 arithmetic on factors of type T
+template <int N, typename T>
 __global__ void k_bilu_solve(BiluArgs a) {
+  constexpr bool kPre = sizeof(T) == 4;
   constexpr int NC = N * N * N;
   __shared__ double v[NC * 8];  // [cell][var]
   const int b = blockIdx.x;
   const int slot = threadIdx.x >> 3, row = threadIdx.x & 7;
-  const double *J = a.Jac + (size_t)b * NC * 7 * 64;
-  const double *Di = a.Dinv + (size_t)b * NC * 64;
+  const T *F = static_cast<const T *>(a.F);
   const double *rb = a.r + (size_t)b * 8 * NC;
   double *zb = a.z + (size_t)b * 8 * NC;
   const int groups = blockDim.x >> 3;
-  // forward: v_c = D_c^-1 (r_c - sum_lower A_cn v_n)
+  for (int q = threadIdx.x; q < NC * 8; q += blockDim.x) v[(q % NC) * 8 + q / NC] = rb[q];
+  __syncthreads();
   for (int w = 0; w < a.nWave; w++) {
     const int s0 = a.wfStart[w], n = a.wfStart[w + 1] - s0;
     for (int base = 0; base < n; base += groups) {
       const bool active = base + slot < n;
-      const int c = active ? a.wfCell[s0 + base + slot] : 0;
+      const int p = s0 + base + slot;
+      const int c = active ? a.wfCell[p] : 0;
       const int i = c % N, j = (c / N) % N, k = c / (N * N);
-      double wr = active ? rb[row * NC + c] : 0.0;
+      double wr = active ? v[c * 8 + row] : 0.0;
       const int idx[3] = {i, j, k};
 #pragma unroll
       for (int d = 0; d < 3; d++) {
         if (!active || idx[d] == 0) continue;
         const int cl = c - (d == 0 ? 1 : (d == 1 ? N : N * N));
-        const double *L = J + ((size_t)c * 7 + 1 + 2 * d) * 64 + row * 8;
+        double L[8];
+        load_row8(F + BiluLayout<N>::fwd(b, p, d) + row * 8, L);
         double s = 0;
 #pragma unroll
         for (int m = 0; m < 8; m++) s += L[m] * v[cl * 8 + m];
         wr -= s;
       }
+      double Di[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+      if (active) load_row8(F + BiluLayout<N>::fwd(b, p, 3) + row * 8, Di);
       double s = 0;
 #pragma unroll
-      for (int q = 0; q < 8; q++) {
-        const double wq = __shfl_sync(0xffffffffu, wr, q, 8);
-        s += (active ? Di[(size_t)c * 64 + row * 8 + q] : 0.0) * wq;
-      }
+      for (int q = 0; q < 8; q++) s += Di[q] * __shfl_sync(0xffffffffu, wr, q, 8);
       if (active) v[c * 8 + row] = s;
     }
     __syncthreads();
   }
-  // backward: x_c = v_c - D_c^-1 sum_upper A_cn x_n (x overwrites v)
   for (int w = a.nWave - 1; w >= 0; w--) {
     const int s0 = a.wfStart[w], n = a.wfStart[w + 1] - s0;
     for (int base = 0; base < n; base += groups) {
       const bool active = base + slot < n;
-      const int c = active ? a.wfCell[s0 + base + slot] : 0;
+      const int p = s0 + base + slot;
+      const int c = active ? a.wfCell[p] : 0;
       const int i = c % N, j = (c / N) % N, k = c / (N * N);
-      double wr = 0;
-      bool any = false;
       const int idx[3] = {i, j, k};
+      double s = 0;
+      bool any = false;
 #pragma unroll
       for (int d = 0; d < 3; d++) {
         if (!active || idx[d] == N - 1) continue;
         any = true;
         const int cu = c + (d == 0 ? 1 : (d == 1 ? N : N * N));
-        const double *U = J + ((size_t)c * 7 + 2 + 2 * d) * 64 + row * 8;
-        double s = 0;
+        double U[8];
+        load_row8(F + BiluLayout<N>::bwd(b, p, d) + row * 8, U);
+        double t = 0;
 #pragma unroll
-        for (int m = 0; m < 8; m++) s += U[m] * v[cu * 8 + m];
-        wr += s;
+        for (int m = 0; m < 8; m++) t += U[m] * v[cu * 8 + m];
+        s += t;
       }
-      double s = 0;
+      if (!kPre) {  // D_c^-1 applied to the sum
+        double Di[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+        if (any) load_row8(F + BiluLayout<N>::fwd(b, p, 3) + row * 8, Di);
+        double t = 0;
 #pragma unroll
-      for (int q = 0; q < 8; q++) {
-        const double wq = __shfl_sync(0xffffffffu, wr, q, 8);
-        s += (active ? Di[(size_t)c * 64 + row * 8 + q] : 0.0) * wq;
+        for (int q = 0; q < 8; q++) t += Di[q] * __shfl_sync(0xffffffffu, s, q, 8);
+        s = t;
       }
-      if (active && any) v[c * 8 + row] = v[c * 8 + row] - s;
+      if (any) v[c * 8 + row] = v[c * 8 + row] - s;
     }
     __syncthreads();
   }
-  for (int q = threadIdx.x; q < NC * 8; q += blockDim.x) {
-    const int c = q >> 3, r = q & 7;
-    zb[r * NC + c] = v[c * 8 + r];
-  }
+  for (int q = threadIdx.x; q < NC * 8; q += blockDim.x) zb[q] = v[(q % NC) * 8 + q / NC];
 }
 
 // r = rhs - y

@@ -39,11 +39,12 @@ struct ImplCtx {
   double *Ueps = nullptr, *Reps = nullptr, *W = nullptr, *R = nullptr;
   double *V = nullptr, *Z = nullptr;           // Krylov bases (m+1 and m vectors)
   double *dtCell = nullptr;                    // DtMax_CB left by calc_timestep
-  double *Jac = nullptr, *Dinv = nullptr;
+  void *F = nullptr;                           // BILU storage (BiluLayout), FP64 or FP32
+  bool precF32 = false;                        // FP32 factor storage
   double *partial = nullptr, *scal = nullptr;  // reduction scratch, device scalars
   unsigned *cnt = nullptr;                     // CTA counter of the one-launch reductions
   double *dNorm = nullptr;
-  int *wfCell = nullptr, *wfStart = nullptr;
+  int *wfCell = nullptr, *wfStart = nullptr, *wfPos = nullptr;
   int nWave = 0, maxWave = 0;
   TmaMaps mapU, mapUeps;
   double Norm[8];
@@ -69,15 +70,18 @@ constexpr int kG = 1184, kT = 256;  // grid-stride launch shape (8 x 148 SMs)
 
 void free_impl() {
   for (double **p : {&I.U, &I.Uold, &I.ResExpl, &I.ResImpl, &I.Rhs, &I.X, &I.Ueps, &I.Reps, &I.W, &I.R, &I.V,
-                     &I.Z, &I.dtCell, &I.Jac, &I.Dinv, &I.partial, &I.scal, &I.dNorm}) {
+                     &I.Z, &I.dtCell, &I.partial, &I.scal, &I.dNorm}) {
     if (*p) cudaFree(*p);
     *p = nullptr;
   }
   if (I.cnt) cudaFree(I.cnt);
   I.cnt = nullptr;
+  if (I.F) cudaFree(I.F);
+  I.F = nullptr;
   if (I.wfCell) cudaFree(I.wfCell);
   if (I.wfStart) cudaFree(I.wfStart);
-  I.wfCell = I.wfStart = nullptr;
+  if (I.wfPos) cudaFree(I.wfPos);
+  I.wfCell = I.wfStart = I.wfPos = nullptr;
   I.ready = false;
 }
 
@@ -159,12 +163,17 @@ int precond(const double *r, double *z) {
   }
   if (I.p.TypePrecond == BX_PRECOND_BILU && I.havePrec) {
     BiluArgs b;
-    b.Jac = I.Jac; b.Dinv = I.Dinv; b.wfCell = I.wfCell; b.wfStart = I.wfStart; b.nWave = I.nWave;
+    b.F = I.F; b.wfCell = I.wfCell; b.wfPos = I.wfPos; b.wfStart = I.wfStart; b.nWave = I.nWave;
     b.nBlock = c.nBlock; b.r = r; b.z = z;
     const int tv = tune_value(kTuneBiluThreads);  // 0: 8 x the widest wavefront
     const int thr = tv > 0 ? tv : ((8 * I.maxWave + 31) / 32) * 32;
-    if (c.nI == 8) k_bilu_solve<8><<<c.nBlock, thr, 0, c.st>>>(b);
-    else k_bilu_solve<4><<<c.nBlock, thr, 0, c.st>>>(b);
+    if (c.nI == 8) {
+      if (I.precF32) k_bilu_solve<8, float><<<c.nBlock, thr, 0, c.st>>>(b);
+      else k_bilu_solve<8, double><<<c.nBlock, thr, 0, c.st>>>(b);
+    } else {
+      if (I.precF32) k_bilu_solve<4, float><<<c.nBlock, thr, 0, c.st>>>(b);
+      else k_bilu_solve<4, double><<<c.nBlock, thr, 0, c.st>>>(b);
+    }
     CKI(cudaGetLastError());
   } else {
     CKI(cudaMemcpyAsync(z, r, sizeof(double) * I.N, cudaMemcpyDeviceToDevice, c.st));
@@ -278,21 +287,31 @@ int compute_norm() {
 int build_precond() {
   Core c = core();
   JacArgs ja;
-  ja.U = I.U; ja.nbr = c.nbr; ja.geom = c.geom; ja.Jac = I.Jac; ja.norm = I.dNorm;
+  ja.U = I.U; ja.nbr = c.nbr; ja.geom = c.geom; ja.F = I.F; ja.wfPos = I.wfPos; ja.norm = I.dNorm;
   ja.gamma = c.sch.Gamma; ja.gm1 = c.sch.Gamma - 1.0; ja.invGm1 = 1.0 / (c.sch.Gamma - 1.0);
   ja.sqrtJacEps = std::sqrt(I.p.JacobianEps); ja.dtImplCoeff = I.Dt * I.ImplCoeff;
   ja.useDivb = c.sch.UseDivbSource; ja.nBlock = c.nBlock;
   const long nThr = I.nCellTot * 8;
   const int blocks = (int)((nThr + 255) / 256);
-  if (c.nI == 8) k_jacobian<8><<<blocks, 256, 0, c.st>>>(ja);
-  else k_jacobian<4><<<blocks, 256, 0, c.st>>>(ja);
+  if (c.nI == 8) {
+    if (I.precF32) k_jacobian<8, float><<<blocks, 256, 0, c.st>>>(ja);
+    else k_jacobian<8, double><<<blocks, 256, 0, c.st>>>(ja);
+  } else {
+    if (I.precF32) k_jacobian<4, float><<<blocks, 256, 0, c.st>>>(ja);
+    else k_jacobian<4, double><<<blocks, 256, 0, c.st>>>(ja);
+  }
   CKI(cudaGetLastError());
   BiluArgs b;
-  b.Jac = I.Jac; b.Dinv = I.Dinv; b.wfCell = I.wfCell; b.wfStart = I.wfStart; b.nWave = I.nWave;
+  b.F = I.F; b.wfCell = I.wfCell; b.wfPos = I.wfPos; b.wfStart = I.wfStart; b.nWave = I.nWave;
   b.nBlock = c.nBlock; b.r = nullptr; b.z = nullptr;
   const int thr = ((8 * I.maxWave + 31) / 32) * 32;
-  if (c.nI == 8) k_bilu_factor<8><<<c.nBlock, thr, 0, c.st>>>(b);
-  else k_bilu_factor<4><<<c.nBlock, thr, 0, c.st>>>(b);
+  if (c.nI == 8) {
+    if (I.precF32) k_bilu_factor<8, float><<<c.nBlock, thr, 0, c.st>>>(b);
+    else k_bilu_factor<8, double><<<c.nBlock, thr, 0, c.st>>>(b);
+  } else {
+    if (I.precF32) k_bilu_factor<4, float><<<c.nBlock, thr, 0, c.st>>>(b);
+    else k_bilu_factor<4, double><<<c.nBlock, thr, 0, c.st>>>(b);
+  }
   CKI(cudaGetLastError());
   I.havePrec = true;
   return BX_OK;
@@ -344,6 +363,8 @@ int bx_implicit_init(const bx_implicit_params *prm) {
   if (prm->nKrylovVector < 1 || prm->nKrylovVector > 32)
     return core_fail(BX_ERR_ARG, "nKrylovVector=%d outside 1..32", prm->nKrylovVector);
   if (prm->TypePrecond < 0 || prm->TypePrecond > 2) return core_fail(BX_ERR_ARG, "TypePrecond=%d", prm->TypePrecond);
+  if (prm->PrecondPrecision != BX_FP64 && prm->PrecondPrecision != BX_FP32_BULK)
+    return core_fail(BX_ERR_ARG, "PrecondPrecision=%d", prm->PrecondPrecision);
   if (I.ready) free_impl();
   I.p = *prm;
   I.m = prm->nKrylovVector;
@@ -361,11 +382,12 @@ int bx_implicit_init(const bx_implicit_params *prm) {
     free_impl();
     return core_fail(BX_ERR_NOMEM, "Krylov bases");
   }
+  I.precF32 = prm->PrecondPrecision == BX_FP32_BULK;
   if (prm->TypePrecond == BX_PRECOND_BILU) {
-    if (cudaMalloc(&I.Jac, sizeof(double) * I.nCellTot * 7 * 64) != cudaSuccess ||
-        cudaMalloc(&I.Dinv, sizeof(double) * I.nCellTot * 64) != cudaSuccess) {
+    const size_t fb = (I.precF32 ? sizeof(float) : sizeof(double)) * (size_t)I.nCellTot * 7 * 64;
+    if (cudaMalloc(&I.F, fb) != cudaSuccess) {
       free_impl();
-      return core_fail(BX_ERR_NOMEM, "Jacobian (%.2f GB)", 8.0 * I.nCellTot * 7 * 64 / 1e9);
+      return core_fail(BX_ERR_NOMEM, "Jacobian and BILU factors (%.2f GB)", fb / 1e9);
     }
   }
   // wavefronts i+j+k = w of a block
@@ -382,9 +404,13 @@ int bx_implicit_init(const bx_implicit_params *prm) {
     I.maxWave = std::max(I.maxWave, (int)cells.size() - start.back());
   }
   start.push_back((int)cells.size());
+  std::vector<int> pos(cells.size());
+  for (size_t q = 0; q < cells.size(); q++) pos[cells[q]] = (int)q;
   CKI(cudaMalloc(&I.wfCell, sizeof(int) * cells.size()));
+  CKI(cudaMalloc(&I.wfPos, sizeof(int) * cells.size()));
   CKI(cudaMalloc(&I.wfStart, sizeof(int) * start.size()));
   CKI(cudaMemcpy(I.wfCell, cells.data(), sizeof(int) * cells.size(), cudaMemcpyHostToDevice));
+  CKI(cudaMemcpy(I.wfPos, pos.data(), sizeof(int) * pos.size(), cudaMemcpyHostToDevice));
   CKI(cudaMemcpy(I.wfStart, start.data(), sizeof(int) * start.size(), cudaMemcpyHostToDevice));
   int r = core_encode_maps(I.U, false, I.mapU);
   if (!r) r = core_encode_maps(I.Ueps, false, I.mapUeps);

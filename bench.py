@@ -722,10 +722,10 @@ def summary(line):
         mv = {k: r(j[k]["matvec_per_step"]) for k in sp}
         out["jfnk_s_per_step"] = sp
         out["jfnk_matvec_per_step"] = mv
-        if "learned" in sp:
+        if "learned" in sp:  # time per step of the learned preconditioner / of BILU, of NONE
             for k in ("bilu", "none"):
                 if k in sp:
-                    out["jfnk_%s_over_learned" % k] = r(sp[k] / sp["learned"])
+                    out["jfnk_learned_over_%s" % k] = r(sp["learned"] / sp[k])
         if "cpu_baseline" in j:
             out["jfnk_cpu_s_per_step"] = r(j["cpu_baseline"]["value"])
     a = line.get("amr")

@@ -261,6 +261,10 @@ typedef struct {
   int MaxMatvec;
   double ErrorMax;       /* relative Krylov tolerance */
   int TypePrecond;       /* BX_PRECOND_* */
+  int PrecondPrecision;  /* BILU factor storage: BX_FP64, or BX_FP32_BULK for
+                            FP32 factors with FP64 arithmetic (half the bytes
+                            of every preconditioner apply; FGMRES still
+                            solves to ErrorMax) */
 } bx_implicit_params;
 
 typedef struct {

@@ -41,7 +41,7 @@ module bx200_interface
      real(c_double):: JacobianEps
      integer(c_int):: nKrylovVector, MaxMatvec
      real(c_double):: ErrorMax
-     integer(c_int):: TypePrecond
+     integer(c_int):: TypePrecond, PrecondPrecision
   end type bx_implicit_params
 
   type, bind(C):: bx_krylov_stats
