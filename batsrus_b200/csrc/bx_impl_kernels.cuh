@@ -183,9 +183,12 @@ struct JacArgs {
   void *F;              // BILU storage (see BiluLayout), element type of the launch
   const int *wfPos;     // position of every cell of a block in wavefront order
   const double *norm;   // Norm_V
+  double *pre;          // per-cell terms shared by the 8 columns (k_jac_cells), [31][cell]
   double gamma, gm1, invGm1, sqrtJacEps, dtImplCoeff;
   int useDivb, nBlock;
 };
+constexpr int kJacPre = 31;  // F0 (3 directions x 8), cmaxLo/Hi (3 x 2), div B
+constexpr int kJacThreads = 128;  // k_jacobian: 4 CTAs (16 warps) per SM at <= 128 registers
 
 // state of cell (i,j,k) of block b where one index may be -1 or N: the
 // neighbour block's cell (same level) or the boundary cell (float)
@@ -234,6 +237,11 @@ struct BiluLayout {
 __device__ __forceinline__ void store_t(double *p, double v) { *p = v; }
 __device__ __forceinline__ void store_t(float *p, double v) { *p = (float)v; }
 
+// a b + c: fused in FP32; in FP64 a product and a sum, the rounding of the
+// reference's loops (this file is compiled without contraction)
+__device__ __forceinline__ float madd(float a, float b, float c) { return fmaf(a, b, c); }
+__device__ __forceinline__ double madd(double a, double b, double c) { return a * b + c; }
+
 // one row of 8 elements (32 or 64 contiguous bytes) into FP64 registers
 __device__ __forceinline__ void load_row8(const double *p, double (&r)[8]) {
   const double2 *q = reinterpret_cast<const double2 *>(p);
@@ -252,10 +260,26 @@ __device__ __forceinline__ void load_row8(const float *p, double (&r)[8]) {
     r[4 * m] = t.x; r[4 * m + 1] = t.y; r[4 * m + 2] = t.z; r[4 * m + 3] = t.w;
   }
 }
+// one row of 8 elements kept in its storage type (fewer registers while the
+// loads of a wavefront are in flight)
+__device__ __forceinline__ void load_raw8(const double *p, double (&r)[8]) { load_row8(p, r); }
+__device__ __forceinline__ void load_raw8(const float *p, float (&r)[8]) {
+  const float4 *q = reinterpret_cast<const float4 *>(p);
+#pragma unroll
+  for (int m = 0; m < 2; m++) {
+    const float4 t = q[m];
+    r[4 * m] = t.x; r[4 * m + 1] = t.y; r[4 * m + 2] = t.z; r[4 * m + 3] = t.w;
+  }
+}
 __device__ __forceinline__ void store_row8(double *p, const double (&r)[8]) {
   double2 *q = reinterpret_cast<double2 *>(p);
 #pragma unroll
   for (int m = 0; m < 4; m++) q[m] = make_double2(r[2 * m], r[2 * m + 1]);
+}
+__device__ __forceinline__ void store_row8(float *p, const float (&r)[8]) {
+  float4 *q = reinterpret_cast<float4 *>(p);
+#pragma unroll
+  for (int m = 0; m < 2; m++) q[m] = make_float4(r[4 * m], r[4 * m + 1], r[4 * m + 2], r[4 * m + 3]);
 }
 __device__ __forceinline__ void store_row8(float *p, const double (&r)[8]) {
   float4 *q = reinterpret_cast<float4 *>(p);
@@ -280,62 +304,106 @@ __device__ __forceinline__ double pow_coeff(const double (&Uc)[8], int iv) {
   }
 }
 
+// The terms of cell n that all 8 columns of its Jacobian share: the
+// unperturbed flux in each direction, the Rusanov coefficients of its six
+// faces, cmaxLo = -Cmax(n-1/2)/2 and cmaxHi = -Cmax(n+1/2)/2 of
+// get_cmax_face, and div B (impl_divbsrc_init); one thread per cell,
+// stored [term][cell] for k_jacobian
+template <int N>
+__global__ void k_jac_cells(JacArgs a) {
+  constexpr int NC = N * N * N;
+  const long cg = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  const long nCell = (long)a.nBlock * NC;
+  if (cg >= nCell) return;
+  const int b = (int)(cg / NC), c = (int)(cg % NC);
+  const int i = c % N, j = (c / N) % N, k = c / (N * N);
+  const BlockGeom g = a.geom[b];
+  double U0[8], UL[8], UR[8], F0[8];
+  load_cell<N>(a, b, i, j, k, U0);
+  double *out = a.pre + cg;
+  double dv = 0;
+#pragma unroll
+  for (int D = 0; D < 3; D++) {
+    load_cell<N>(a, b, i - (D == 0), j - (D == 1), k - (D == 2), UL);
+    load_cell<N>(a, b, i + (D == 0), j + (D == 1), k + (D == 2), UR);
+    double cLo, cHi;
+    if (D == 0) {
+      cLo = face_cmax<0>(UL, U0, a.gm1, a.gamma); cHi = face_cmax<0>(U0, UR, a.gm1, a.gamma);
+      cell_flux_e<0>(U0, a.gm1, a.invGm1, g.area[0], F0);
+    } else if (D == 1) {
+      cLo = face_cmax<1>(UL, U0, a.gm1, a.gamma); cHi = face_cmax<1>(U0, UR, a.gm1, a.gamma);
+      cell_flux_e<1>(U0, a.gm1, a.invGm1, g.area[1], F0);
+    } else {
+      cLo = face_cmax<2>(UL, U0, a.gm1, a.gamma); cHi = face_cmax<2>(U0, UR, a.gm1, a.gamma);
+      cell_flux_e<2>(U0, a.gm1, a.invGm1, g.area[2], F0);
+    }
+    out[(24 + 2 * D) * nCell] = -0.5 * cLo;
+    out[(25 + 2 * D) * nCell] = -0.5 * cHi;
+#pragma unroll
+    for (int v = 0; v < 8; v++) out[(8 * D + v) * nCell] = F0[v];
+    const double t = (UR[kBx + D] - UL[kBx + D]) / g.cellSize[D];
+    dv = D == 0 ? t : dv + t;
+  }
+  out[30 * nCell] = 0.5 * dv;
+}
+
 // Column jv of the derivative of the flux of cell n in direction D enters
 // three blocks of the 7-point Jacobian: the diagonal block of n, the block
 // A(n+e_D, n) of the cell above (its lower-neighbour block, through the
 // face n+1/2) and the block A(n-e_D, n) of the cell below (its
 // upper-neighbour block, through the face n-1/2).  Thread (n, jv) evaluates
-// the derivative once and writes its column of the last two; every column
-// of every block has one writer.  The face Rusanov coefficients are
-// cmaxLo = -Cmax(n-1/2)/2 and cmaxHi = -Cmax(n+1/2)/2 of get_cmax_face.
+// the perturbed flux once and writes its column of the last two; every
+// column of every block has one writer.
 template <int N, int D, typename T>
 __device__ __forceinline__ void jac_dir(const JacArgs &a, int b, int i, int j, int k, int jv, const double (&U0)[8],
-                                        const BlockGeom &g, double (&diag)[8], T *F, const double (&sc)[8]) {
+                                        const BlockGeom &g, double (&diag)[8], T *F, const double *sc,
+                                        const double *pre, long nCell, double epsj, double coeff, bool mulV,
+                                        double invV) {
   const int idx[3] = {i, j, k};
-  double UL[8], UR[8];
-  load_cell<N>(a, b, i - (D == 0), j - (D == 1), k - (D == 2), UL);
-  load_cell<N>(a, b, i + (D == 0), j + (D == 1), k + (D == 2), UR);
-  const double cmaxLo = -0.5 * face_cmax<D>(UL, U0, a.gm1, a.gamma);
-  const double cmaxHi = -0.5 * face_cmax<D>(U0, UR, a.gm1, a.gamma);
+  const double cmaxLo = pre[(24 + 2 * D) * nCell], cmaxHi = pre[(25 + 2 * D) * nCell];
   const double area = g.area[D], V = g.volume;
-  const double epsj = a.sqrtJacEps * a.norm[jv];
-  const double coeff = -0.5 / (a.sqrtJacEps * a.norm[jv]);
+  // x / V, or x invV where that is the same number (V a power of two) or
+  // the result is stored in FP32
+  auto perV = [&](double x) { return mulV ? x * invV : x / V; };
   const double coeffPow = -0.5 / g.cellSize[D];
   const bool powCol = a.useDivb && jv == kBx + D;
-  double F0[8], Fe[8], Ue[8], dF[8];
-  cell_flux_e<D>(U0, a.gm1, a.invGm1, area, F0);
+  double Fe[8], Ue[8], dF[8];
 #pragma unroll
   for (int v = 0; v < 8; v++) Ue[v] = v == jv ? U0[v] + epsj : U0[v];  // no dynamic index: stays in registers
   cell_flux_e<D>(Ue, a.gm1, a.invGm1, area, Fe);
 #pragma unroll
   for (int iv = 0; iv < 8; iv++) {
-    dF[iv] = coeff * (Fe[iv] - F0[iv]);
+    dF[iv] = coeff * (Fe[iv] - pre[(8 * D + iv) * nCell]);
     double left = dF[iv], right = dF[iv];
     if (iv == jv) { left = left + cmaxHi; right = right - cmaxLo; }
-    diag[iv] = diag[iv] - right / V + left / V;
+    diag[iv] = diag[iv] - perV(right) + perV(left);
   }
   const int c = i + N * (j + N * k);
   constexpr int st = D == 0 ? 1 : (D == 1 ? N : N * N);
   // A(n+e_D, n) = -dFdWLeft(face n+1/2): lower-neighbour block D of cell n+e_D
   if (idx[D] < N - 1) {
+    double UR[8];
+    if (powCol) load_cell<N>(a, b, i + (D == 0), j + (D == 1), k + (D == 2), UR);
     T *dst = F + BiluLayout<N>::fwd(b, a.wfPos[c + st], D) + jv;
 #pragma unroll
     for (int iv = 0; iv < 8; iv++) {
       double left = dF[iv];
       if (iv == jv) left = left + cmaxHi;
-      left = left / V;
+      left = perV(left);
       if (powCol && iv != kRho) left = left + coeffPow * pow_coeff(UR, iv);
       store_t(dst + iv * 8, left * sc[iv]);
     }
   }
   // A(n-e_D, n) = +dFdWRight(face n-1/2): upper-neighbour block D of cell n-e_D
   if (idx[D] > 0) {
+    double UL[8];
+    if (powCol) load_cell<N>(a, b, i - (D == 0), j - (D == 1), k - (D == 2), UL);
     T *dst = F + BiluLayout<N>::bwd(b, a.wfPos[c - st], D) + jv;
 #pragma unroll
     for (int iv = 0; iv < 8; iv++) {
       double right = dF[iv];
       if (iv == jv) right = right - cmaxLo;
-      right = right / V;
+      right = perV(right);
       if (powCol && iv != kRho) right = right + coeffPow * pow_coeff(UL, iv);
       store_t(dst + iv * 8, -right * sc[iv]);
     }
@@ -345,43 +413,38 @@ __device__ __forceinline__ void jac_dir(const JacArgs &a, int b, int i, int j, i
 // impl_jacobian: the normalised matrix I - dt ImplCoeff dR/dU of the
 // first-order Rusanov residual with Powell source, one thread per (cell,
 // perturbed variable jv), written straight into the BILU storage (every
-// element once, no clearing pass)
+// element once, no clearing pass); the shared terms come from k_jac_cells
 template <int N, typename T>
-__global__ void k_jacobian(JacArgs a) {
+__global__ void __launch_bounds__(kJacThreads, 4) k_jacobian(JacArgs a) {
   constexpr int NC = N * N * N;
+  __shared__ double scs[64];  // time-accurate scaling dt ImplCoeff Norm(jv)/Norm(iv), [jv][iv]
+  if (threadIdx.x < 64) scs[threadIdx.x] = a.dtImplCoeff * a.norm[threadIdx.x >> 3] / a.norm[threadIdx.x & 7];
+  __syncthreads();
   const long q = blockIdx.x * (long)blockDim.x + threadIdx.x;
-  if (q >= (long)a.nBlock * NC * 8) return;
+  const long nCell = (long)a.nBlock * NC;
+  if (q >= nCell * 8) return;
   const int jv = (int)(q % 8);
   const long cg = q / 8;
   const int b = (int)(cg / NC), c = (int)(cg % NC);
   const int i = c % N, j = (c / N) % N, k = c / (N * N);
   const BlockGeom g = a.geom[b];
   T *F = static_cast<T *>(a.F);
+  const double *pre = a.pre + cg;
   double U0[8];
   load_cell<N>(a, b, i, j, k, U0);
-  // time-accurate scaling of row iv, column jv
-  double sc[8];
-  const double nj = a.norm[jv];
-#pragma unroll
-  for (int iv = 0; iv < 8; iv++) sc[iv] = a.dtImplCoeff * nj / a.norm[iv];
-  // impl_divbsrc_init: div B of the cell
-  double divB = 0;
-  if (a.useDivb) {
-    double Up[8], Um[8];
-    load_cell<N>(a, b, i + 1, j, k, Up); load_cell<N>(a, b, i - 1, j, k, Um);
-    double dv = (Up[kBx] - Um[kBx]) / g.cellSize[0];
-    load_cell<N>(a, b, i, j + 1, k, Up); load_cell<N>(a, b, i, j - 1, k, Um);
-    dv = dv + (Up[kBy] - Um[kBy]) / g.cellSize[1];
-    load_cell<N>(a, b, i, j, k + 1, Up); load_cell<N>(a, b, i, j, k - 1, Um);
-    dv = dv + (Up[kBz] - Um[kBz]) / g.cellSize[2];
-    divB = 0.5 * dv;
-  }
+  const double *sc = scs + 8 * jv;
+  const double epsj = a.sqrtJacEps * a.norm[jv];
+  const double coeff = -0.5 / (a.sqrtJacEps * a.norm[jv]);
+  int e2;
+  const bool mulV = sizeof(T) == 4 || frexp(g.volume, &e2) == 0.5;  // FP32 storage, or V = 2^k
+  const double invV = 1.0 / g.volume;
   double diag[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-  jac_dir<N, 0>(a, b, i, j, k, jv, U0, g, diag, F, sc);
-  jac_dir<N, 1>(a, b, i, j, k, jv, U0, g, diag, F, sc);
-  jac_dir<N, 2>(a, b, i, j, k, jv, U0, g, diag, F, sc);
+  jac_dir<N, 0>(a, b, i, j, k, jv, U0, g, diag, F, sc, pre, nCell, epsj, coeff, mulV, invV);
+  jac_dir<N, 1>(a, b, i, j, k, jv, U0, g, diag, F, sc, pre, nCell, epsj, coeff, mulV, invV);
+  jac_dir<N, 2>(a, b, i, j, k, jv, U0, g, diag, F, sc, pre, nCell, epsj, coeff, mulV, invV);
   // impl_divbsrc_middle: diagonal Powell terms of column jv
   if (a.useDivb) {
+    const double divB = pre[30 * nCell];
     const double rho = U0[kRho];
     for (int m = 0; m < 3; m++) {
       if (jv == kBx + m) diag[kUx + m] = diag[kUx + m] - divB;
@@ -414,111 +477,129 @@ struct BiluArgs {
 };
 
 // Gauss-Jordan inverse with partial pivoting of the 8x8 matrix whose row
-// `row` is held by this lane (lanes of an aligned 8-lane group)
-__device__ __forceinline__ void group_inverse8(double (&a)[8], double (&inv)[8], int row) {
+// `row` is held by this lane (lanes of an aligned 8-lane group).  Rows are
+// not moved between lanes: each lane tracks the position its row would have
+// after the row interchanges of the textbook elimination (pivot = first
+// largest |a| at or below the diagonal), so the pivots, ties included, and
+// every operation are those of the interchanging version; one shuffle of
+// the inverse rows at the end puts row r of the inverse on lane r.
+template <typename R>
+__device__ __forceinline__ void group_inverse8(R (&a)[8], R (&inv)[8], int row) {
+  const int lane = threadIdx.x & 31, base = lane & ~7;
+  int pos = row;
 #pragma unroll
-  for (int q = 0; q < 8; q++) inv[q] = q == row ? 1.0 : 0.0;
+  for (int q = 0; q < 8; q++) inv[q] = q == row ? R(1) : R(0);
 #pragma unroll
   for (int col = 0; col < 8; col++) {
-    double val = row >= col ? fabs(a[col]) : -1.0;
-    int idx = row;
+    R val = pos >= col ? fabs(a[col]) : R(-1);
+    int ip = pos;
 #pragma unroll
     for (int off = 4; off > 0; off >>= 1) {
-      const double ov = __shfl_xor_sync(0xffffffffu, val, off, 8);
-      const int oi = __shfl_xor_sync(0xffffffffu, idx, off, 8);
-      if (ov > val || (ov == val && oi < idx)) { val = ov; idx = oi; }
+      const R ov = __shfl_xor_sync(0xffffffffu, val, off, 8);
+      const int oi = __shfl_xor_sync(0xffffffffu, ip, off, 8);
+      if (ov > val || (ov == val && oi < ip)) { val = ov; ip = oi; }
     }
-    const int p = idx;
-#pragma unroll
-    for (int q = 0; q < 8; q++) {  // swap rows col and p
-      const double fromP = __shfl_sync(0xffffffffu, a[q], p, 8), fromC = __shfl_sync(0xffffffffu, a[q], col, 8);
-      const double iP = __shfl_sync(0xffffffffu, inv[q], p, 8), iC = __shfl_sync(0xffffffffu, inv[q], col, 8);
-      if (row == col) { a[q] = fromP; inv[q] = iP; }
-      else if (row == p) { a[q] = fromC; inv[q] = iC; }
-    }
-    if (row == col) {
-      const double s = 1.0 / a[col];
+    const bool piv = pos == ip;
+    if (pos == col) pos = ip;  // the interchange of positions col and ip
+    else if (piv) pos = col;
+    const int src = __ffs((__ballot_sync(0xffffffffu, piv) >> base) & 0xffu) - 1;
+    if (piv) {
+      const R s = R(1) / a[col];
 #pragma unroll
       for (int q = 0; q < 8; q++) { a[q] *= s; inv[q] *= s; }
     }
-    const double f = a[col];
+    const R f = a[col];
 #pragma unroll
     for (int q = 0; q < 8; q++) {
-      const double pa = __shfl_sync(0xffffffffu, a[q], col, 8), pi = __shfl_sync(0xffffffffu, inv[q], col, 8);
-      if (row != col && f != 0.0) { a[q] -= f * pa; inv[q] -= f * pi; }
+      const R pa = __shfl_sync(0xffffffffu, a[q], src, 8), pi = __shfl_sync(0xffffffffu, inv[q], src, 8);
+      if (!piv && f != R(0)) { a[q] = madd(-f, pa, a[q]); inv[q] = madd(-f, pi, inv[q]); }
     }
   }
+  int from = 0;  // the lane whose row ended at position `row`
+#pragma unroll
+  for (int t = 0; t < 8; t++)
+    if (__shfl_sync(0xffffffffu, pos, t, 8) == row) from = t;
+  R out[8];
+#pragma unroll
+  for (int q = 0; q < 8; q++) out[q] = __shfl_sync(0xffffffffu, inv[q], from, 8);
+#pragma unroll
+  for (int q = 0; q < 8; q++) inv[q] = out[q];
 }
 
-// D_c = A(c,c) - sum_d A(c,c-e_d) D_{c-e_d}^-1 A(c-e_d,c), stored as D_c^-1
-// (FP64 arithmetic, stored with the element type T).  FP64 storage follows
-// the reference's order, (A(c,c-e_d) D^-1) A(c-e_d,c); FP32 storage reads
-// the premultiplied D^-1 A(c-e_d,c) of the lower neighbour and replaces
-// A(c,c+e_d) by D_c^-1 A(c,c+e_d) once D_c^-1 is known.
+// D_c = A(c,c) - sum_d A(c,c-e_d) D_{c-e_d}^-1 A(c-e_d,c), stored as D_c^-1,
+// in the arithmetic of the storage type T.  FP64 follows the reference's
+// order, (A(c,c-e_d) D^-1) A(c-e_d,c); FP32 reads the premultiplied
+// D^-1 A(c-e_d,c) of the lower neighbour and replaces A(c,c+e_d) by
+// D_c^-1 A(c,c+e_d) once D_c^-1 is known.
 template <int N, typename T>
-__global__ void k_bilu_factor(BiluArgs a) {
+__global__ void __launch_bounds__(384, 2) k_bilu_factor(BiluArgs a) {  // two CTAs of 8 x 48 lanes per SM
   constexpr bool kPre = sizeof(T) == 4;
+  constexpr int NC = N * N * N, kWave = 3 * N - 2;
+  __shared__ int sCell[NC], sPos[NC], sStart[kWave + 1];
   const int b = blockIdx.x;
   const int slot = threadIdx.x >> 3, row = threadIdx.x & 7;
   T *F = static_cast<T *>(a.F);
-  for (int w = 0; w < a.nWave; w++) {
-    const int s0 = a.wfStart[w], n = a.wfStart[w + 1] - s0;
+  for (int q = threadIdx.x; q < NC; q += blockDim.x) { sCell[q] = a.wfCell[q]; sPos[q] = a.wfPos[q]; }
+  for (int q = threadIdx.x; q <= kWave; q += blockDim.x) sStart[q] = a.wfStart[q];
+  __syncthreads();
+  for (int w = 0; w < kWave; w++) {
+    const int s0 = sStart[w], n = sStart[w + 1] - s0;
     for (int base = 0; base < n; base += (int)(blockDim.x >> 3)) {
       const bool active = base + slot < n;
       const int p = s0 + base + slot;
-      const int c = active ? a.wfCell[p] : 0;
+      const int c = active ? sCell[p] : 0;
       const int i = c % N, j = (c / N) % N, k = c / (N * N);
       const int idx[3] = {i, j, k};
-      double D[8];
-      if (active) load_row8(F + BiluLayout<N>::fwd(b, p, 3) + row * 8, D);
+      T D[8];
+      if (active) load_raw8(F + BiluLayout<N>::fwd(b, p, 3) + row * 8, D);
       else
 #pragma unroll
-        for (int q = 0; q < 8; q++) D[q] = q == row ? 1.0 : 0.0;
+        for (int q = 0; q < 8; q++) D[q] = q == row ? T(1) : T(0);
 #pragma unroll
       for (int d = 0; d < 3; d++) {
         if (!active || idx[d] == 0) continue;
-        const int pl = a.wfPos[c - (d == 0 ? 1 : (d == 1 ? N : N * N))];
-        double L[8];
-        load_row8(F + BiluLayout<N>::fwd(b, p, d) + row * 8, L);
+        const int pl = sPos[c - (d == 0 ? 1 : (d == 1 ? N : N * N))];
+        T L[8];
+        load_raw8(F + BiluLayout<N>::fwd(b, p, d) + row * 8, L);
         const T *Un = F + BiluLayout<N>::bwd(b, pl, d);  // A(cl, c), or D_cl^-1 A(cl, c)
         if (!kPre) {
           const T *Dn = F + BiluLayout<N>::fwd(b, pl, 3);
-          double T1[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+          T T1[8] = {0, 0, 0, 0, 0, 0, 0, 0};
 #pragma unroll
           for (int m = 0; m < 8; m++) {
-            double dr[8];
-            load_row8(Dn + m * 8, dr);
+            T dr[8];
+            load_raw8(Dn + m * 8, dr);
 #pragma unroll
-            for (int q = 0; q < 8; q++) T1[q] += L[m] * dr[q];
+            for (int q = 0; q < 8; q++) T1[q] = madd(L[m], dr[q], T1[q]);
           }
 #pragma unroll
           for (int q = 0; q < 8; q++) L[q] = T1[q];
         }
-        double T2[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+        T T2[8] = {0, 0, 0, 0, 0, 0, 0, 0};
 #pragma unroll
         for (int m = 0; m < 8; m++) {
-          double u[8];
-          load_row8(Un + m * 8, u);
+          T u[8];
+          load_raw8(Un + m * 8, u);
 #pragma unroll
-          for (int q = 0; q < 8; q++) T2[q] += L[m] * u[q];
+          for (int q = 0; q < 8; q++) T2[q] = madd(L[m], u[q], T2[q]);
         }
 #pragma unroll
         for (int q = 0; q < 8; q++) D[q] -= T2[q];
       }
-      double inv[8];
+      T inv[8];
       group_inverse8(D, inv, row);
       if (active) store_row8(F + BiluLayout<N>::fwd(b, p, 3) + row * 8, inv);
       if (kPre) {
 #pragma unroll
         for (int d = 0; d < 3; d++) {
           const bool has = active && idx[d] < N - 1;
-          double A[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-          if (has) load_row8(F + BiluLayout<N>::bwd(b, p, d) + row * 8, A);
-          double out[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+          T A[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+          if (has) load_raw8(F + BiluLayout<N>::bwd(b, p, d) + row * 8, A);
+          T out[8] = {0, 0, 0, 0, 0, 0, 0, 0};
 #pragma unroll
           for (int m = 0; m < 8; m++)
 #pragma unroll
-            for (int q = 0; q < 8; q++) out[q] += inv[m] * __shfl_sync(0xffffffffu, A[q], m, 8);
+            for (int q = 0; q < 8; q++) out[q] = madd(inv[m], __shfl_sync(0xffffffffu, A[q], m, 8), out[q]);
           if (has) store_row8(F + BiluLayout<N>::bwd(b, p, d) + row * 8, out);
         }
       }
@@ -530,84 +611,93 @@ __global__ void k_bilu_factor(BiluArgs a) {
 // z = (LU)^-1 r on every grid block: forward v_c = D_c^-1 (r_c - sum_d
 // A(c,c-e_d) v_{c-e_d}), backward x_c = v_c - D_c^-1 sum_d A(c,c+e_d)
 // x_{c+e_d} (FP32 storage: the premultiplied blocks), in shared memory;
-// FP64 arithmetic on factors of type T
+// FP64 arithmetic on factors of type T.  The wavefront tables are copied to
+// shared memory first, so that the only global loads of a wavefront are the
+// matrix rows, whose addresses follow from the position alone; v is stored
+// [var][cell] with one pad cell per variable, which keeps the copies in and
+// out and the eight row lanes of a cell on distinct banks.
 template <int N, typename T>
-__global__ void k_bilu_solve(BiluArgs a) {
+__global__ void __launch_bounds__(384, sizeof(T) == 4 ? 3 : 2) k_bilu_solve(BiluArgs a) {  // 3 (FP32) or 2 CTAs of 8 x 48 lanes per SM
   constexpr bool kPre = sizeof(T) == 4;
-  constexpr int NC = N * N * N;
-  __shared__ double v[NC * 8];  // [cell][var]
+  constexpr int NC = N * N * N, NP = NC + 1, kWave = 3 * N - 2;
+  __shared__ double v[8 * NP];  // [var][cell]
+  __shared__ int sCell[NC], sStart[kWave + 1];
   const int b = blockIdx.x;
   const int slot = threadIdx.x >> 3, row = threadIdx.x & 7;
   const T *F = static_cast<const T *>(a.F);
   const double *rb = a.r + (size_t)b * 8 * NC;
   double *zb = a.z + (size_t)b * 8 * NC;
   const int groups = blockDim.x >> 3;
-  for (int q = threadIdx.x; q < NC * 8; q += blockDim.x) v[(q % NC) * 8 + q / NC] = rb[q];
+  for (int q = threadIdx.x; q < NC; q += blockDim.x) sCell[q] = a.wfCell[q];
+  for (int q = threadIdx.x; q <= kWave; q += blockDim.x) sStart[q] = a.wfStart[q];
+  for (int q = threadIdx.x; q < NC * 8; q += blockDim.x) v[(q / NC) * NP + q % NC] = rb[q];
   __syncthreads();
-  for (int w = 0; w < a.nWave; w++) {
-    const int s0 = a.wfStart[w], n = a.wfStart[w + 1] - s0;
+  double *vr = v + row * NP;
+  for (int w = 0; w < kWave; w++) {
+    const int s0 = sStart[w], n = sStart[w + 1] - s0;
     for (int base = 0; base < n; base += groups) {
       const bool active = base + slot < n;
       const int p = s0 + base + slot;
-      const int c = active ? a.wfCell[p] : 0;
+      const int c = active ? sCell[p] : 0;
       const int i = c % N, j = (c / N) % N, k = c / (N * N);
-      double wr = active ? v[c * 8 + row] : 0.0;
       const int idx[3] = {i, j, k};
+      T L[3][8], Di[8];
+#pragma unroll
+      for (int d = 0; d < 3; d++)
+        if (active && idx[d] > 0) load_raw8(F + BiluLayout<N>::fwd(b, p, d) + row * 8, L[d]);
+      if (active) load_raw8(F + BiluLayout<N>::fwd(b, p, 3) + row * 8, Di);
+      double wr = active ? vr[c] : 0.0;
 #pragma unroll
       for (int d = 0; d < 3; d++) {
         if (!active || idx[d] == 0) continue;
         const int cl = c - (d == 0 ? 1 : (d == 1 ? N : N * N));
-        double L[8];
-        load_row8(F + BiluLayout<N>::fwd(b, p, d) + row * 8, L);
         double s = 0;
 #pragma unroll
-        for (int m = 0; m < 8; m++) s += L[m] * v[cl * 8 + m];
+        for (int m = 0; m < 8; m++) s += (double)L[d][m] * v[m * NP + cl];
         wr -= s;
       }
-      double Di[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-      if (active) load_row8(F + BiluLayout<N>::fwd(b, p, 3) + row * 8, Di);
       double s = 0;
 #pragma unroll
-      for (int q = 0; q < 8; q++) s += Di[q] * __shfl_sync(0xffffffffu, wr, q, 8);
-      if (active) v[c * 8 + row] = s;
+      for (int q = 0; q < 8; q++) s += (active ? (double)Di[q] : 0.0) * __shfl_sync(0xffffffffu, wr, q, 8);
+      if (active) vr[c] = s;
     }
     __syncthreads();
   }
-  for (int w = a.nWave - 1; w >= 0; w--) {
-    const int s0 = a.wfStart[w], n = a.wfStart[w + 1] - s0;
+  for (int w = kWave - 1; w >= 0; w--) {
+    const int s0 = sStart[w], n = sStart[w + 1] - s0;
     for (int base = 0; base < n; base += groups) {
       const bool active = base + slot < n;
       const int p = s0 + base + slot;
-      const int c = active ? a.wfCell[p] : 0;
+      const int c = active ? sCell[p] : 0;
       const int i = c % N, j = (c / N) % N, k = c / (N * N);
       const int idx[3] = {i, j, k};
+      const bool any = active && (i < N - 1 || j < N - 1 || k < N - 1);
+      T U[3][8], Di[8];
+#pragma unroll
+      for (int d = 0; d < 3; d++)
+        if (active && idx[d] < N - 1) load_raw8(F + BiluLayout<N>::bwd(b, p, d) + row * 8, U[d]);
+      if (!kPre && any) load_raw8(F + BiluLayout<N>::fwd(b, p, 3) + row * 8, Di);
       double s = 0;
-      bool any = false;
 #pragma unroll
       for (int d = 0; d < 3; d++) {
         if (!active || idx[d] == N - 1) continue;
-        any = true;
         const int cu = c + (d == 0 ? 1 : (d == 1 ? N : N * N));
-        double U[8];
-        load_row8(F + BiluLayout<N>::bwd(b, p, d) + row * 8, U);
         double t = 0;
 #pragma unroll
-        for (int m = 0; m < 8; m++) t += U[m] * v[cu * 8 + m];
+        for (int m = 0; m < 8; m++) t += (double)U[d][m] * v[m * NP + cu];
         s += t;
       }
       if (!kPre) {  // D_c^-1 applied to the sum
-        double Di[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-        if (any) load_row8(F + BiluLayout<N>::fwd(b, p, 3) + row * 8, Di);
         double t = 0;
 #pragma unroll
-        for (int q = 0; q < 8; q++) t += Di[q] * __shfl_sync(0xffffffffu, s, q, 8);
+        for (int q = 0; q < 8; q++) t += (any ? (double)Di[q] : 0.0) * __shfl_sync(0xffffffffu, s, q, 8);
         s = t;
       }
-      if (any) v[c * 8 + row] = v[c * 8 + row] - s;
+      if (any) vr[c] = vr[c] - s;
     }
     __syncthreads();
   }
-  for (int q = threadIdx.x; q < NC * 8; q += blockDim.x) zb[q] = v[(q % NC) * 8 + q / NC];
+  for (int q = threadIdx.x; q < NC * 8; q += blockDim.x) zb[q] = v[(q / NC) * NP + q % NC];
 }
 
 // r = rhs - y

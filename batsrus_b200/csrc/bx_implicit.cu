@@ -40,6 +40,7 @@ struct ImplCtx {
   double *V = nullptr, *Z = nullptr;           // Krylov bases (m+1 and m vectors)
   double *dtCell = nullptr;                    // DtMax_CB left by calc_timestep
   void *F = nullptr;                           // BILU storage (BiluLayout), FP64 or FP32
+  double *jacPre = nullptr;                    // k_jac_cells terms when the Krylov basis V is too small
   bool precF32 = false;                        // FP32 factor storage
   double *partial = nullptr, *scal = nullptr;  // reduction scratch, device scalars
   unsigned *cnt = nullptr;                     // CTA counter of the one-launch reductions
@@ -70,7 +71,7 @@ constexpr int kG = 1184, kT = 256;  // grid-stride launch shape (8 x 148 SMs)
 
 void free_impl() {
   for (double **p : {&I.U, &I.Uold, &I.ResExpl, &I.ResImpl, &I.Rhs, &I.X, &I.Ueps, &I.Reps, &I.W, &I.R, &I.V,
-                     &I.Z, &I.dtCell, &I.partial, &I.scal, &I.dNorm}) {
+                     &I.Z, &I.dtCell, &I.partial, &I.scal, &I.dNorm, &I.jacPre}) {
     if (*p) cudaFree(*p);
     *p = nullptr;
   }
@@ -288,17 +289,23 @@ int build_precond() {
   Core c = core();
   JacArgs ja;
   ja.U = I.U; ja.nbr = c.nbr; ja.geom = c.geom; ja.F = I.F; ja.wfPos = I.wfPos; ja.norm = I.dNorm;
+  // the Krylov basis is idle while the preconditioner is built
+  ja.pre = (I.m + 1) * 8 >= kJacPre ? I.V : I.jacPre;
   ja.gamma = c.sch.Gamma; ja.gm1 = c.sch.Gamma - 1.0; ja.invGm1 = 1.0 / (c.sch.Gamma - 1.0);
   ja.sqrtJacEps = std::sqrt(I.p.JacobianEps); ja.dtImplCoeff = I.Dt * I.ImplCoeff;
   ja.useDivb = c.sch.UseDivbSource; ja.nBlock = c.nBlock;
+  const int cellBlocks = (int)((I.nCellTot + 255) / 256);
+  if (c.nI == 8) k_jac_cells<8><<<cellBlocks, 256, 0, c.st>>>(ja);
+  else k_jac_cells<4><<<cellBlocks, 256, 0, c.st>>>(ja);
+  CKI(cudaGetLastError());
   const long nThr = I.nCellTot * 8;
-  const int blocks = (int)((nThr + 255) / 256);
+  const int blocks = (int)((nThr + kJacThreads - 1) / kJacThreads);
   if (c.nI == 8) {
-    if (I.precF32) k_jacobian<8, float><<<blocks, 256, 0, c.st>>>(ja);
-    else k_jacobian<8, double><<<blocks, 256, 0, c.st>>>(ja);
+    if (I.precF32) k_jacobian<8, float><<<blocks, kJacThreads, 0, c.st>>>(ja);
+    else k_jacobian<8, double><<<blocks, kJacThreads, 0, c.st>>>(ja);
   } else {
-    if (I.precF32) k_jacobian<4, float><<<blocks, 256, 0, c.st>>>(ja);
-    else k_jacobian<4, double><<<blocks, 256, 0, c.st>>>(ja);
+    if (I.precF32) k_jacobian<4, float><<<blocks, kJacThreads, 0, c.st>>>(ja);
+    else k_jacobian<4, double><<<blocks, kJacThreads, 0, c.st>>>(ja);
   }
   CKI(cudaGetLastError());
   BiluArgs b;
@@ -385,7 +392,8 @@ int bx_implicit_init(const bx_implicit_params *prm) {
   I.precF32 = prm->PrecondPrecision == BX_FP32_BULK;
   if (prm->TypePrecond == BX_PRECOND_BILU) {
     const size_t fb = (I.precF32 ? sizeof(float) : sizeof(double)) * (size_t)I.nCellTot * 7 * 64;
-    if (cudaMalloc(&I.F, fb) != cudaSuccess) {
+    if (cudaMalloc(&I.F, fb) != cudaSuccess ||
+        ((I.m + 1) * 8 < kJacPre && cudaMalloc(&I.jacPre, sizeof(double) * kJacPre * I.nCellTot) != cudaSuccess)) {
       free_impl();
       return core_fail(BX_ERR_NOMEM, "Jacobian and BILU factors (%.2f GB)", fb / 1e9);
     }

@@ -18,7 +18,7 @@ static TuneKnobInfo g_knobs[kNumTune] = {
     {"krylov_ctas_per_sm", 4, {2, 4, 6, 8}, 4, 0, {}},
     {"krylov_unroll", 3, {1, 2, 4}, 2, 0, {}},
     {"heat_ilu_warps", 3, {1, 2, 4}, 1, 0, {}},
-    {"bilu_threads", 4, {0, 128, 256, 512}, 0, 0, {}},  // 0: 8 x the widest wavefront
+    {"bilu_threads", 4, {0, 128, 192, 256}, 0, 0, {}},  // 0: 8 x the widest wavefront (at most 384)
     {"stage_variant", 4, {0, 1, 2, 3}, 0, 0, {}},
     // changes the rounding of the Krylov coefficients: a setting, not timed
     {"krylov_gs_steps", 4, {1, 2, 3, 4}, 3, 0, {}},
