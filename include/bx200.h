@@ -261,10 +261,11 @@ typedef struct {
   int MaxMatvec;
   double ErrorMax;       /* relative Krylov tolerance */
   int TypePrecond;       /* BX_PRECOND_* */
-  int PrecondPrecision;  /* BILU factor storage: BX_FP64, or BX_FP32_BULK for
-                            FP32 factors with FP64 arithmetic (half the bytes
-                            of every preconditioner apply; FGMRES still
-                            solves to ErrorMax) */
+  int PrecondPrecision;  /* BILU: BX_FP64, or BX_FP32_BULK for FP32 factors
+                            (FP64 Jacobian, FP32 factorisation, sweeps in
+                            FP64 arithmetic): half the bytes of every
+                            preconditioner apply; FGMRES still solves to
+                            ErrorMax */
 } bx_implicit_params;
 
 typedef struct {

@@ -90,11 +90,12 @@ def test_gpu_jfnk_system_matches_oracle():
 
 
 def test_gpu_jfnk_fp32_factors(one_step_gram_schmidt):
-    """BILU factors stored in FP32 with FP64 arithmetic (the FP32 blocks of
-    the Jacobian, D^-1 and the premultiplied D^-1 A of the backward sweep).
+    """BILU factors in FP32: the FP64 Jacobian stored in FP32, factorised in
+    FP32 (D^-1 and the premultiplied D^-1 A of the backward sweep), the
+    sweeps in FP64 arithmetic.
     The apply agrees with the oracle's FP64 BILU to 1e-6 relative: FP32
-    rounding (6e-8) of the stored blocks, grown by the condition of the
-    8x8 pivots (7e-8 measured on this case).  A preconditioner only steers the flexible
+    rounding (6e-8) of the blocks and of the factorisation, grown by the
+    condition of the 8x8 pivots.  A preconditioner only steers the flexible
     GMRES: every step's matrix-vector count stays within two of the
     oracle's, its Krylov solution satisfies the tolerance 1e-3 on the
     oracle's operator, and the states agree to 1e-6 relative, far inside
