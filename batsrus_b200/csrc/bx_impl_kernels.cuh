@@ -391,7 +391,7 @@ __device__ __forceinline__ void jac_dir(const JacArgs &a, int b, int i, int j, i
       if (iv == jv) left = left + cmaxHi;
       left = perV(left);
       if (powCol && iv != kRho) left = left + coeffPow * pow_coeff(UR, iv);
-      store_t(dst + iv * 8, left * sc[iv]);
+      store_t(dst + iv * 8, left * sc[8 * iv]);
     }
   }
   // A(n-e_D, n) = +dFdWRight(face n-1/2): upper-neighbour block D of cell n-e_D
@@ -405,7 +405,7 @@ __device__ __forceinline__ void jac_dir(const JacArgs &a, int b, int i, int j, i
       if (iv == jv) right = right - cmaxLo;
       right = perV(right);
       if (powCol && iv != kRho) right = right + coeffPow * pow_coeff(UL, iv);
-      store_t(dst + iv * 8, -right * sc[iv]);
+      store_t(dst + iv * 8, -right * sc[8 * iv]);
     }
   }
 }
@@ -417,8 +417,8 @@ __device__ __forceinline__ void jac_dir(const JacArgs &a, int b, int i, int j, i
 template <int N, typename T>
 __global__ void __launch_bounds__(kJacThreads, 4) k_jacobian(JacArgs a) {
   constexpr int NC = N * N * N;
-  __shared__ double scs[64];  // time-accurate scaling dt ImplCoeff Norm(jv)/Norm(iv), [jv][iv]
-  if (threadIdx.x < 64) scs[threadIdx.x] = a.dtImplCoeff * a.norm[threadIdx.x >> 3] / a.norm[threadIdx.x & 7];
+  __shared__ double scs[64];  // time-accurate scaling dt ImplCoeff Norm(jv)/Norm(iv), [iv][jv]
+  if (threadIdx.x < 64) scs[threadIdx.x] = a.dtImplCoeff * a.norm[threadIdx.x & 7] / a.norm[threadIdx.x >> 3];
   __syncthreads();
   const long q = blockIdx.x * (long)blockDim.x + threadIdx.x;
   const long nCell = (long)a.nBlock * NC;
@@ -432,7 +432,7 @@ __global__ void __launch_bounds__(kJacThreads, 4) k_jacobian(JacArgs a) {
   const double *pre = a.pre + cg;
   double U0[8];
   load_cell<N>(a, b, i, j, k, U0);
-  const double *sc = scs + 8 * jv;
+  const double *sc = scs + jv;  // sc[8 iv]: the 8 columns of a cell read 8 adjacent words
   const double epsj = a.sqrtJacEps * a.norm[jv];
   const double coeff = -0.5 / (a.sqrtJacEps * a.norm[jv]);
   int e2;
@@ -458,7 +458,7 @@ __global__ void __launch_bounds__(kJacThreads, 4) k_jacobian(JacArgs a) {
   }
   T *dst = F + BiluLayout<N>::fwd(b, a.wfPos[c], 3) + jv;
 #pragma unroll
-  for (int iv = 0; iv < 8; iv++) store_t(dst + iv * 8, -diag[iv] * sc[iv] + (iv == jv ? 1.0 : 0.0));
+  for (int iv = 0; iv < 8; iv++) store_t(dst + iv * 8, -diag[iv] * sc[8 * iv] + (iv == jv ? 1.0 : 0.0));
 }
 
 // ---------------------------------------------------------------------------

@@ -265,11 +265,13 @@ def run_jfnk(args, lrank):
     from batsrus_b200.implicit import ImplicitSolver
     g, s, _, st = configs.jfnk_ot(nRoot=args.jfnk_nroot)
     out = {"workload": "perturbed_orszag_tang_%dcubed_bdf2_cfl20_gmres30_1e-3" % (8 * args.jfnk_nroot),
+           "bilu_factors": args.bilu_factors,
            "cells": g.nCell, "blocks": g.nBlock, "steps": args.jfnk_steps, "warmup": args.jfnk_warmup,
            "unit": "s/step", "higher_is_better": False}
     net = None
     for prec in args.jfnk_precond.split(","):
-        p = configs.jfnk_ot(nRoot=args.jfnk_nroot, precond=prec, with_state=False)[2]
+        p = configs.jfnk_ot(nRoot=args.jfnk_nroot, precond=prec, with_state=False,
+                            precondPrecision=args.bilu_factors)[2]
         if prec.upper() == "LEARNED" and net is None:
             net, out["learned_training"] = train_learned(args, g, s, lrank)
         x = ExplicitSolver(g, s, device=lrank)
@@ -640,6 +642,8 @@ def main():
     ap.add_argument("--amr-dyn-dn", type=int, default=10, help="steps between regrids (#DOAMR DnAmr)")
     ap.add_argument("--jfnk-nroot", type=int, default=16, help="16 -> 128^3 cells")
     ap.add_argument("--jfnk-steps", type=int, default=5)
+    ap.add_argument("--bilu-factors", default="fp32", choices=["fp64", "fp32"],
+                    help="storage of the BILU factors of the implicit workload")
     ap.add_argument("--jfnk-warmup", type=int, default=2)
     ap.add_argument("--sharded", action="store_true",
                     help="one domain partitioned over the ranks (shard.GpuRank) instead of replicas")
