@@ -380,25 +380,49 @@ __global__ void __launch_bounds__(B::NTHR, B::MINB)
         for (int v = 0; v < 8; v++) o[r][v] = old[v * B::NC + c];
       }
       const int i = c & 7, j = (c >> 3) & 7, k = c >> 6;
+      if (kFloatFlux) {
+        // FP32 fluxes: the three directions' differences summed in FP32
+        // (each difference of neighbouring faces is exact when they are
+        // within a factor of two), one conversion per variable
+        Real cs[8], dbs = Real(0), vs = Real(0);
 #pragma unroll
-      for (int D = 0; D < 3; D++) {
-        const Real *F = fb + D * 10 * 576;
-        const int f0 = D == 0 ? i + 9 * (j + 8 * k) : (D == 1 ? i + 8 * (j + 9 * k) : c);
-        const int f1 = f0 + (D == 0 ? 1 : (D == 1 ? 8 : 64));
+        for (int D = 0; D < 3; D++) {
+          const Real *F = fb + D * 10 * 576;
+          const int f0 = D == 0 ? i + 9 * (j + 8 * k) : (D == 1 ? i + 8 * (j + 9 * k) : c);
+          const int f1 = f0 + (D == 0 ? 1 : (D == 1 ? 8 : 64));
 #pragma unroll
-        for (int v = 0; v < 8; v++) {
-          // FP32 fluxes: the difference of neighbouring faces in FP32 (exact
-          // when they are within a factor of two) and one conversion
-          const double d = kFloatFlux ? (double)(F[v * 576 + f0] - F[v * 576 + f1])
-                                      : (double)F[v * 576 + f0] - (double)F[v * 576 + f1];
-          chg[r][v] = D == 0 ? d : chg[r][v] + d;
+          for (int v = 0; v < 8; v++) {
+            const Real d = F[v * 576 + f0] - F[v * 576 + f1];
+            cs[v] = D == 0 ? d : cs[v] + d;
+          }
+          const Real db = (Real)M.g.invHalf[D] * (F[9 * 576 + f1] - F[9 * 576 + f0]);
+          dbs = D == 0 ? db : dbs + db;
+          if (a.computeDt) {
+            const Real vm = fmax(F[8 * 576 + f0], F[8 * 576 + f1]);
+            vs = D == 0 ? vm : vs + vm;
+          }
         }
-        const double db = M.g.invHalf[D] * (kFloatFlux ? (double)(F[9 * 576 + f1] - F[9 * 576 + f0])
-                                                       : (double)F[9 * 576 + f1] - (double)F[9 * 576 + f0]);
-        divB[r] = D == 0 ? db : divB[r] + db;
-        if (a.computeDt) {
-          const double vm = (double)fmax(F[8 * 576 + f0], F[8 * 576 + f1]);
-          vdt[r] = D == 0 ? vm : vdt[r] + vm;
+#pragma unroll
+        for (int v = 0; v < 8; v++) chg[r][v] = (double)cs[v];
+        divB[r] = (double)dbs;
+        vdt[r] = (double)vs;
+      } else {
+#pragma unroll
+        for (int D = 0; D < 3; D++) {
+          const Real *F = fb + D * 10 * 576;
+          const int f0 = D == 0 ? i + 9 * (j + 8 * k) : (D == 1 ? i + 8 * (j + 9 * k) : c);
+          const int f1 = f0 + (D == 0 ? 1 : (D == 1 ? 8 : 64));
+#pragma unroll
+          for (int v = 0; v < 8; v++) {
+            const double d = (double)F[v * 576 + f0] - (double)F[v * 576 + f1];
+            chg[r][v] = D == 0 ? d : chg[r][v] + d;
+          }
+          const double db = M.g.invHalf[D] * ((double)F[9 * 576 + f1] - (double)F[9 * 576 + f0]);
+          divB[r] = D == 0 ? db : divB[r] + db;
+          if (a.computeDt) {
+            const double vm = (double)fmax(F[8 * 576 + f0], F[8 * 576 + f1]);
+            vdt[r] = D == 0 ? vm : vdt[r] + vm;
+          }
         }
       }
     }
