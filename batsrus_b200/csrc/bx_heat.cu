@@ -65,8 +65,9 @@ struct HeatCtx {
   int *blkAt = nullptr, *blkXYZ = nullptr;
   double *b = nullptr, *x = nullptr, *w = nullptr, *t = nullptr, *r = nullptr, *V = nullptr;
   double *K = nullptr;  // face conduction tensor [block][dim][dir][face]
-  double4 *coef = nullptr;   // forward and backward sweep coefficients, interleaved by 32 blocks
-  double *yI = nullptr;      // forward-sweep scratch, interleaved
+  void *coef = nullptr;      // forward and backward sweep coefficients (double4 or float4), interleaved by 32 blocks
+  void *yI = nullptr;        // forward-sweep scratch (double or float), interleaved
+  bool ilu32 = false;        // FP32 coefficients, scratch and sweep arithmetic
   double *V8 = nullptr, *Z8 = nullptr;  // learned preconditioner: embedded input and output [block][8][512]
   double *Zb = nullptr;                 // flexible GMRES: preconditioned basis (m vectors)
   unsigned *usedM = nullptr; // used masks [group][cell]
@@ -303,11 +304,18 @@ __device__ __forceinline__ void load_wave_table(const WaveTable *g, WaveTable &s
   for (int q = threadIdx.x; q < (int)(sizeof(WaveTable) / sizeof(short)); q += blockDim.x) dst[q] = src[q];
 }
 
-// matrix + factorisation; coef[q] = {lower x, lower y, lower z, 1 / pivot}
+__device__ __forceinline__ void put4(double4 *p, double x, double y, double z, double w) { *p = make_double4(x, y, z, w); }
+__device__ __forceinline__ void put4(float4 *p, double x, double y, double z, double w) {
+  *p = make_float4((float)x, (float)y, (float)z, (float)w);
+}
+
+// matrix + factorisation (FP64); coef[q] = {lower x, lower y, lower z,
+// 1 / pivot}, stored as double4 or, for the FP32 sweeps, float4
+template <typename C4>
 __global__ void __launch_bounds__(32 * kWarpsPerCta) k_heat_factor(HeatArgs a, const double *__restrict__ K,
                                                                  const unsigned char *__restrict__ used,
-                                                                 const WaveTable *__restrict__ wtab, double4 *coefL,
-                                                                 double4 *coefU, int nBlock) {
+                                                                 const WaveTable *__restrict__ wtab, C4 *coefL,
+                                                                 C4 *coefU, int nBlock) {
   __shared__ IluSmem sm;
   load_wave_table(wtab, sm.wt);
   __syncthreads();
@@ -359,9 +367,9 @@ __global__ void __launch_bounds__(32 * kWarpsPerCta) k_heat_factor(HeatArgs a, c
   for (int c = lane; c < kNC; c += 32) {
     const double iv = 1.0 / dp[c];
     const long o = ((long)(blk >> 5) * kNC + c) * 32 + (blk & 31);  // interleaved by 32 blocks
-    coefL[o] = make_double4(lx[c], ly[c], lz[c], iv);
-    coefU[o] = make_double4((c & 7) != 7 ? lx[c + 1] : 0.0, ((c >> 3) & 7) != 7 ? ly[c + 8] : 0.0,
-                            (c >> 6) != 7 ? lz[c + 64] : 0.0, iv);
+    put4(coefL + o, lx[c], ly[c], lz[c], iv);
+    put4(coefU + o, (c & 7) != 7 ? lx[c + 1] : 0.0, ((c >> 3) & 7) != 7 ? ly[c + 8] : 0.0,
+         (c >> 6) != 7 ? lz[c + 64] : 0.0, iv);
   }
 }
 
@@ -372,53 +380,67 @@ __global__ void __launch_bounds__(32 * kWarpsPerCta) k_heat_factor(HeatArgs a, c
 // p * 32 + (l ^ (p & 31)): rows and columns are free of bank conflicts.
 __device__ __forceinline__ int swz(int p, int l) { return p * 32 + (l ^ (p & 31)); }
 
+template <typename T> struct Vec4T;
+template <> struct Vec4T<double> { using type = double4; };
+template <> struct Vec4T<float> { using type = float4; };
+
+template <typename T>
 struct IluRow {
-  double4 v[kNB];
+  typename Vec4T<T>::type v[kNB];
   unsigned m[kNB];
 };
 
+__device__ __forceinline__ double4 ldg4(const double4 *p) {
+  const double2 *p2 = reinterpret_cast<const double2 *>(p);
+  const double2 lo = __ldg(p2), hi = __ldg(p2 + 1);
+  return make_double4(lo.x, lo.y, hi.x, hi.y);
+}
+__device__ __forceinline__ float4 ldg4(const float4 *p) { return __ldg(p); }
+
 // the coefficients and used masks of one x row (8 cells from c0), loaded
 // ahead of the row's arithmetic
-__device__ __forceinline__ void load_row(IluRow &row, const double4 *__restrict__ cf, const unsigned *__restrict__ um,
-                                         int c0) {
+template <typename T>
+__device__ __forceinline__ void load_row(IluRow<T> &row, const typename Vec4T<T>::type *__restrict__ cf,
+                                         const unsigned *__restrict__ um, int c0) {
 #pragma unroll
   for (int i = 0; i < kNB; i++) {
-    const double2 *p2 = reinterpret_cast<const double2 *>(cf + (long)(c0 + i) * 32);
-    const double2 lo = __ldg(p2), hi = __ldg(p2 + 1);
-    row.v[i] = make_double4(lo.x, lo.y, hi.x, hi.y);
+    row.v[i] = ldg4(cf + (long)(c0 + i) * 32);
     row.m[i] = __ldg(um + c0 + i);
   }
 }
 
 // W warps per CTA (autotuned), each with its own group of 32 blocks and
-// its two plane buffers (32 KB) in dynamic shared memory
-template <int W>
-__global__ void __launch_bounds__(32 * W) k_heat_ilu(const double4 *__restrict__ coefL,
-                                                     const double4 *__restrict__ coefU,
+// its two plane buffers (32 KB in FP64, 16 KB in FP32) in dynamic shared
+// memory; T is the type of the coefficients, the scratch and the
+// arithmetic (r and z are FP64)
+template <int W, typename T>
+__global__ void __launch_bounds__(32 * W) k_heat_ilu(const typename Vec4T<T>::type *__restrict__ coefL,
+                                                     const typename Vec4T<T>::type *__restrict__ coefU,
                                                      const unsigned *__restrict__ usedM,
-                                                     const double *__restrict__ r, double *__restrict__ yI,
+                                                     const double *__restrict__ r, T *__restrict__ yI,
                                                      double *__restrict__ z, int nBlock, int nGroup) {
-  extern __shared__ double dyn[];
+  using V4 = typename Vec4T<T>::type;
+  extern __shared__ __align__(16) unsigned char dynb[];
   const int wp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int g = blockIdx.x * W + wp;
   if (g >= nGroup) return;  // the warps work independently (no CTA barrier)
-  double(*plane)[64 * 32] = reinterpret_cast<double(*)[64 * 32]>(dyn + (size_t)wp * 2 * 64 * 32);
+  T(*plane)[64 * 32] = reinterpret_cast<T(*)[64 * 32]>(dynb + sizeof(T) * (size_t)wp * 2 * 64 * 32);
   const long gb = (long)g * 32;  // first block of the group
   const unsigned *um = usedM + (long)g * kNC;
-  const double4 *cL = coefL + (long)g * kNC * 32 + lane, *cU = coefU + (long)g * kNC * 32 + lane;
-  double *yl = yI + (long)g * kNC * 32 + lane;
-  double *cur = plane[0], *prv = plane[1];
-  IluRow A, B;
+  const V4 *cL = coefL + (long)g * kNC * 32 + lane, *cU = coefU + (long)g * kNC * 32 + lane;
+  T *yl = yI + (long)g * kNC * 32 + lane;
+  T *cur = plane[0], *prv = plane[1];
+  IluRow<T> A, B;
   // forward, rows (j, k) in natural order
   load_row(A, cL, um, 0);
   for (int k = 0; k < kNB; k++) {
 #pragma unroll 8
     for (int bb = 0; bb < 32; bb++) {
       const long blk = gb + bb;
-      double v0 = 0.0, v1 = 0.0;
+      T v0 = T(0), v1 = T(0);
       if (blk < nBlock) {
-        v0 = __ldg(r + blk * kNC + 64 * k + lane);
-        v1 = __ldg(r + blk * kNC + 64 * k + 32 + lane);
+        v0 = (T)__ldg(r + blk * kNC + 64 * k + lane);
+        v1 = (T)__ldg(r + blk * kNC + 64 * k + 32 + lane);
       }
       cur[swz(lane, bb)] = v0;
       cur[swz(32 + lane, bb)] = v1;
@@ -428,19 +450,19 @@ __global__ void __launch_bounds__(32 * W) k_heat_ilu(const double4 *__restrict__
     for (int j = 0; j < kNB; j++) {
       const int c0 = 64 * k + 8 * j;
       if (c0 + 8 < kNC) load_row(B, cL, um, c0 + 8);
-      double ym = 0.0;  // y of the cell at x - 1
+      T ym = T(0);  // y of the cell at x - 1
 #pragma unroll
       for (int i = 0; i < kNB; i++) {
         const int p = i + 8 * j, c = c0 + i;
         const unsigned m = A.m[i];
-        const double4 v = A.v[i];
-        double s = cur[swz(p, lane)];
+        const V4 v = A.v[i];
+        T s = cur[swz(p, lane)];
         if ((m >> lane) & 1) {
           if (i > 0 && ((A.m[i - 1] >> lane) & 1)) s = s - v.x * ym;
           if (j > 0 && ((mDn[i] >> lane) & 1)) s = s - v.y * cur[swz(p - 8, lane)];
           if (k > 0 && ((__ldg(um + c - 64) >> lane) & 1)) s = s - v.z * prv[swz(p, lane)];
         }
-        const double y = s * v.w;
+        const T y = s * v.w;
         cur[swz(p, lane)] = y;
         yl[(long)c * 32] = y;
         ym = y;
@@ -450,7 +472,7 @@ __global__ void __launch_bounds__(32 * W) k_heat_ilu(const double4 *__restrict__
       A = B;
     }
     __syncwarp();
-    double *t = cur; cur = prv; prv = t;
+    T *t = cur; cur = prv; prv = t;
   }
   __syncwarp();
   // backward, rows in reverse order
@@ -460,22 +482,22 @@ __global__ void __launch_bounds__(32 * W) k_heat_ilu(const double4 *__restrict__
     for (int j = kNB - 1; j >= 0; j--) {
       const int c0 = 64 * k + 8 * j;
       if (c0 > 0) load_row(B, cU, um, c0 - 8);
-      double yv[kNB];
+      T yv[kNB];
 #pragma unroll
       for (int i = 0; i < kNB; i++) yv[i] = yl[(long)(c0 + i) * 32];
-      double zp = 0.0;  // z of the cell at x + 1
+      T zp = T(0);  // z of the cell at x + 1
 #pragma unroll
       for (int i = kNB - 1; i >= 0; i--) {
         const int p = i + 8 * j, c = c0 + i;
         const unsigned m = A.m[i];
-        const double4 v = A.v[i];
-        double s = 0.0;
+        const V4 v = A.v[i];
+        T s = T(0);
         if ((m >> lane) & 1) {
           if (i < kNB - 1 && ((A.m[i + 1] >> lane) & 1)) s = s + v.x * zp;
           if (j < kNB - 1 && ((mUp[i] >> lane) & 1)) s = s + v.y * cur[swz(p + 8, lane)];
           if (k < kNB - 1 && ((__ldg(um + c + 64) >> lane) & 1)) s = s + v.z * prv[swz(p, lane)];
         }
-        const double zc = yv[i] - s * v.w;
+        const T zc = yv[i] - s * v.w;
         cur[swz(p, lane)] = zc;
         zp = zc;
       }
@@ -488,12 +510,12 @@ __global__ void __launch_bounds__(32 * W) k_heat_ilu(const double4 *__restrict__
     for (int bb = 0; bb < 32; bb++) {
       const long blk = gb + bb;
       if (blk < nBlock) {
-        z[blk * kNC + 64 * k + lane] = cur[swz(lane, bb)];
-        z[blk * kNC + 64 * k + 32 + lane] = cur[swz(32 + lane, bb)];
+        z[blk * kNC + 64 * k + lane] = (double)cur[swz(lane, bb)];
+        z[blk * kNC + 64 * k + 32 + lane] = (double)cur[swz(32 + lane, bb)];
       }
     }
     __syncwarp();
-    double *t = cur; cur = prv; prv = t;
+    T *t = cur; cur = prv; prv = t;
   }
 }
 
@@ -517,18 +539,39 @@ __global__ void k_h_te_update(double *Te, const double *x, const unsigned char *
     if (used[q]) Te[q] = Te[q] + x[q];
 }
 
-template <int W>
-cudaError_t launch_ilu_w(const double *r, double *z, cudaStream_t st) {
-  constexpr size_t smem = sizeof(double) * W * 2 * 64 * 32;
+template <int W, typename T>
+cudaError_t launch_ilu_wt(const double *r, double *z, cudaStream_t st) {
+  using V4 = typename Vec4T<T>::type;
+  constexpr size_t smem = sizeof(T) * W * 2 * 64 * 32;
   static bool attr = false;
   if (!attr) {
-    const cudaError_t e = cudaFuncSetAttribute(k_heat_ilu<W>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    const cudaError_t e =
+        cudaFuncSetAttribute(k_heat_ilu<W, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     attr = true;
   }
-  k_heat_ilu<W><<<(H.nGroup + W - 1) / W, 32 * W, smem, st>>>(H.coef, H.coef + H.nIl, H.usedM, r, H.yI, z,
-                                                               H.nBlock, H.nGroup);
+  const V4 *cf = static_cast<const V4 *>(H.coef);
+  k_heat_ilu<W, T><<<(H.nGroup + W - 1) / W, 32 * W, smem, st>>>(cf, cf + H.nIl, H.usedM, r, static_cast<T *>(H.yI),
+                                                                  z, H.nBlock, H.nGroup);
   return cudaGetLastError();
+}
+
+template <int W>
+cudaError_t launch_ilu_w(const double *r, double *z, cudaStream_t st) {
+  return H.ilu32 ? launch_ilu_wt<W, float>(r, z, st) : launch_ilu_wt<W, double>(r, z, st);
+}
+
+// the ILU(0) factors of the current system (FP64 arithmetic, stored in the
+// sweeps' precision)
+void launch_factor(cudaStream_t st) {
+  const int grid = (H.nBlock + kWarpsPerCta - 1) / kWarpsPerCta;
+  if (H.ilu32) {
+    float4 *cf = static_cast<float4 *>(H.coef);
+    k_heat_factor<<<grid, 32 * kWarpsPerCta, 0, st>>>(H.a, H.K, H.used, H.wtab, cf, cf + H.nIl, H.nBlock);
+  } else {
+    double4 *cf = static_cast<double4 *>(H.coef);
+    k_heat_factor<<<grid, 32 * kWarpsPerCta, 0, st>>>(H.a, H.K, H.used, H.wtab, cf, cf + H.nIl, H.nBlock);
+  }
 }
 
 cudaError_t launch_ilu(int w, const double *r, double *z, cudaStream_t st) {
@@ -644,7 +687,9 @@ int collect_pair(const double *t, const double *z, cudaStream_t st) {
   embed(t, st);
   k_heat_target<<<1184, 256, 0, st>>>(z, H.Z8, H.nCell);
   CKH(cudaGetLastError());
-  return learned_collect_scalar(H.V8, H.Z8, H.coef, H.used, H.nBlock, st);
+  if (H.ilu32)
+    return core_fail(BX_ERR_STATE, "the learned preconditioner's training pairs need FP64 ILU factors (PrecondPrecision)");
+  return learned_collect_scalar(H.V8, H.Z8, static_cast<const double4 *>(H.coef), H.used, H.nBlock, st);
 }
 
 int precond(const double *r, double *z, cudaStream_t st) {
@@ -922,8 +967,7 @@ int bx::tune_heat() {
   if (!H.ready || H.p.TypePrecond != BX_PRECOND_BILU || k.tuned == 2) return BX_OK;
   Core c = core();
   k_heat_apply<<<H.nBlock, 512, kApplySmem, c.st>>>(H.a, H.Te, H.K, H.used, H.b, kModeRhs);
-  k_heat_factor<<<(H.nBlock + kWarpsPerCta - 1) / kWarpsPerCta, 32 * kWarpsPerCta, 0, c.st>>>(
-      H.a, H.K, H.used, H.wtab, H.coef, H.coef + H.nIl, H.nBlock);
+  launch_factor(c.st);
   CKH(cudaGetLastError());
   cudaEvent_t e0 = H.ev[0], e1 = H.ev[1];
   float best = 1e30f;
@@ -958,7 +1002,10 @@ int bx_heat_init(const bx_heat_params *prm, const double *Te, const double *bhat
       prm->TypePrecond != BX_PRECOND_LEARNED)
     return core_fail(BX_ERR_ARG, "TypePrecond=%d: the heat conduction solve takes NONE, BILU or LEARNED",
                      prm->TypePrecond);
+  if (prm->PrecondPrecision != BX_FP64 && prm->PrecondPrecision != BX_FP32_BULK)
+    return core_fail(BX_ERR_ARG, "PrecondPrecision=%d", prm->PrecondPrecision);
   if (H.ready) free_heat();
+  H.ilu32 = prm->PrecondPrecision == BX_FP32_BULK;
   std::vector<int> atH, xyzH;
   const int r0 = grid_tables(c, atH, xyzH);
   if (r0) return r0;
@@ -985,8 +1032,8 @@ int bx_heat_init(const bx_heat_params *prm, const double *Te, const double *bhat
   H.nGroup = (H.nBlock + 31) / 32;
   H.nIl = (long)H.nGroup * 32 * kNC;
   ok = ok && cudaMalloc(&H.B3, 3 * vb) == cudaSuccess &&
-       cudaMalloc(&H.coef, 2 * sizeof(double4) * H.nIl) == cudaSuccess &&
-       cudaMalloc(&H.yI, sizeof(double) * H.nIl) == cudaSuccess &&
+       cudaMalloc(&H.coef, 2 * (H.ilu32 ? sizeof(float4) : sizeof(double4)) * H.nIl) == cudaSuccess &&
+       cudaMalloc(&H.yI, (H.ilu32 ? sizeof(float) : sizeof(double)) * H.nIl) == cudaSuccess &&
        cudaMalloc(&H.usedM, sizeof(unsigned) * H.nGroup * kNC) == cudaSuccess &&
        cudaMalloc(&H.K, sizeof(double) * kKBlock * H.nBlock) == cudaSuccess &&
        cudaMalloc(&H.wtab, sizeof(WaveTable)) == cudaSuccess && cudaMalloc(&H.cnt, sizeof(unsigned)) == cudaSuccess &&
@@ -1016,7 +1063,7 @@ int bx_heat_init(const bx_heat_params *prm, const double *Te, const double *bhat
   CKH(cudaMemsetAsync(H.errDev, 0, sizeof(int), c.st));
   H.a.err = H.errDev;
   CKH(cudaFuncSetAttribute(k_heat_apply, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kApplySmem));
-  CKH(cudaMemsetAsync(H.coef, 0, 2 * sizeof(double4) * H.nIl, c.st));
+  CKH(cudaMemsetAsync(H.coef, 0, 2 * (H.ilu32 ? sizeof(float4) : sizeof(double4)) * H.nIl, c.st));
   {
     std::vector<unsigned> um((size_t)H.nGroup * kNC, 0u);
     for (long b = 0; b < H.nBlock; b++)
@@ -1038,8 +1085,7 @@ int bx_advance_semi_impl(bx_krylov_stats *stats) {
   CKH(cudaEventRecord(H.ev[0], c.st));
   k_heat_apply<<<H.nBlock, 512, kApplySmem, c.st>>>(H.a, H.Te, H.K, H.used, H.b, kModeRhs);
   if (H.p.TypePrecond == BX_PRECOND_BILU) {
-    k_heat_factor<<<(H.nBlock + kWarpsPerCta - 1) / kWarpsPerCta, 32 * kWarpsPerCta, 0, c.st>>>(
-        H.a, H.K, H.used, H.wtab, H.coef, H.coef + H.nIl, H.nBlock);
+    launch_factor(c.st);
   }
   CKH(cudaGetLastError());
   int iError = 0;
@@ -1106,8 +1152,7 @@ int bx_heat_precond(const double *rv, double *z) {
   if (!rv || !z) return core_fail(BX_ERR_ARG, "null argument");
   Core c = core();
   if (H.p.TypePrecond == BX_PRECOND_BILU) {
-    k_heat_factor<<<(H.nBlock + kWarpsPerCta - 1) / kWarpsPerCta, 32 * kWarpsPerCta, 0, c.st>>>(
-        H.a, H.K, H.used, H.wtab, H.coef, H.coef + H.nIl, H.nBlock);
+    launch_factor(c.st);
     CKH(cudaGetLastError());
   }
   if (H.p.TypePrecond == BX_PRECOND_LEARNED && (r = learned_scalar_setup(H.nBlock, c.st))) return r;

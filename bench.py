@@ -444,7 +444,8 @@ def run_heat(args, lrank):
     Te, b, used = tb(Te), tb(b), tb(used)
     out = {"workload": "dipole_heat_conduction_%dcubed_kpar_kperp_1e6_gmres30_1e-6" % n, "cells": g.nCell,
            "blocks": g.nBlock, "used_fraction": float(used.mean()), "solves": args.heat_steps,
-           "warmup": args.heat_warmup, "unit": "s/solve", "higher_is_better": False}
+           "warmup": args.heat_warmup, "unit": "s/solve", "higher_is_better": False,
+           "bilu_sweeps": args.heat_ilu}
     net = None
     for prec in args.heat_precond.split(","):
         x = None
@@ -452,7 +453,7 @@ def run_heat(args, lrank):
             if prec.upper() == "LEARNED" and net is None:
                 net, out["learned_training"] = train_learned_heat(args, g, lrank)
             x = ExplicitSolver(g, Scheme(), device=lrank)
-            h = HeatSolver(x, HeatParams(typePrecond=prec), Te, b, used)
+            h = HeatSolver(x, HeatParams(typePrecond=prec, precondPrecision=args.heat_ilu), Te, b, used)
             if args.autotune:
                 x.autotune()
             for _ in range(args.heat_warmup):
@@ -644,6 +645,8 @@ def main():
     ap.add_argument("--jfnk-steps", type=int, default=5)
     ap.add_argument("--bilu-factors", default="fp32", choices=["fp64", "fp32"],
                     help="storage of the BILU factors of the implicit workload")
+    ap.add_argument("--heat-ilu", default="fp32", choices=["fp64", "fp32"],
+                    help="precision of the BILU sweeps of the heat conduction workload")
     ap.add_argument("--jfnk-warmup", type=int, default=2)
     ap.add_argument("--sharded", action="store_true",
                     help="one domain partitioned over the ranks (shard.GpuRank) instead of replicas")

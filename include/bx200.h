@@ -416,6 +416,10 @@ typedef struct {
   int MaxMatvec;               /* #SEMIKRYLOV MaxMatvecSemi */
   double ErrorMax;             /* #SEMIKRYLOV ErrorMaxSemi (relative, preconditioned) */
   int TypePrecond;             /* #SEMIPRECOND: BX_PRECOND_BILU or BX_PRECOND_NONE */
+  int PrecondPrecision;        /* BILU sweeps: BX_FP64, or BX_FP32_BULK for FP32
+                                  coefficients, scratch and arithmetic (the
+                                  factorisation stays FP64; GMRES still solves
+                                  the FP64 system to ErrorMax) */
 } bx_heat_params;
 
 /* init_mod_semi_impl (src/ModSemiImplicit.f90:110) and the state the solve
