@@ -1,11 +1,12 @@
 // bx_heat.cu -- semi-implicit field-aligned heat conduction
 // (TypeSemiImplicit = 'parcond'): one linear solve per call of
 // bx_advance_semi_impl on a uniform single-level grid of 8^3 blocks with
-// float outer boundaries.
+// float or periodic outer boundaries.
 //
 //   k_heat_apply   per block: a 10^3 tile of the scalar, HeatCoef and the
 //                  unit field (the block, its face, edge and corner ghosts,
-//                  clamped into the domain for the float boundary), then per
+//                  clamped into the domain at a float boundary, wrapped at
+//                  a periodic one), then per
 //                  cell the six face fluxes -HeatCond . FaceGrad
 //                  (get_face_gradient, src/ModFaceGradient.f90:933-1140;
 //                  get_heat_cond_tensor / get_impl_heat_cond_state,
@@ -45,6 +46,7 @@ constexpr int kNB = 8, kNC = 512, kTile = 10;
 struct HeatArgs {
   int n[3];        // global cells per dimension
   int nbx[3];      // blocks per dimension
+  int periodic[3]; // 1: periodic dimension, 0: float boundary
   double dx[3], V, area[3];
   double invDx[3], gA[3], gC[3];  // 1/dx and the transverse gradient weights -0.25/dx, +0.25/dx
   double invV, cvDt;              // 1/V and Cv/Dt
@@ -92,12 +94,20 @@ HeatCtx H;
                        __LINE__);                                                                     \
   } while (0)
 
-// index of the cell at global cell coordinates (gi, gj, gk), clamped into
-// the domain (float boundary); cell = i + 8 (j + 8 k) inside its block
+// a global cell coordinate brought into the domain: clamped at a float
+// boundary (the ghost cell copies the boundary cell), wrapped at a periodic
+// one (the coordinate is at most one cell outside)
+__device__ __forceinline__ int gwrap(int x, int n, int periodic) {
+  if (periodic) return x < 0 ? x + n : (x >= n ? x - n : x);
+  return min(max(x, 0), n - 1);
+}
+
+// index of the cell at global cell coordinates (gi, gj, gk) brought into
+// the domain; cell = i + 8 (j + 8 k) inside its block
 __device__ __forceinline__ long gidx(const HeatArgs &a, int gi, int gj, int gk) {
-  gi = min(max(gi, 0), a.n[0] - 1);
-  gj = min(max(gj, 0), a.n[1] - 1);
-  gk = min(max(gk, 0), a.n[2] - 1);
+  gi = gwrap(gi, a.n[0], a.periodic[0]);
+  gj = gwrap(gj, a.n[1], a.periodic[1]);
+  gk = gwrap(gk, a.n[2], a.periodic[2]);
   const long blk = a.blkAt[gi / kNB + a.nbx[0] * (gj / kNB + a.nbx[1] * (gk / kNB))];
   return blk * kNC + (gi % kNB) + kNB * ((gj % kNB) + kNB * (gk % kNB));
 }
@@ -885,14 +895,18 @@ int fgmres(int &iError, cudaStream_t st) {
   }
 }
 
-// block tables of a single-level grid of 8^3 blocks that covers the domain
-// with float boundaries
+// block tables of a single-level grid of 8^3 blocks that covers the domain,
+// with float or periodic boundaries (both sides of a dimension alike)
 int grid_tables(const Core &c, std::vector<int> &at, std::vector<int> &xyz) {
   const CoreGrid gr = core_grid();
   if (c.nDim != 3 || c.shape != kShape888 || c.nSlab)
     return core_fail(BX_ERR_ARG, "heat conduction needs a 3D single-level grid of 8^3 blocks");
-  for (int s = 0; s < 6; s++)
-    if (gr.typeBc[s] != BX_BC_FLOAT) return core_fail(BX_ERR_ARG, "heat conduction needs float outer boundaries");
+  for (int d = 0; d < 3; d++) {
+    const int lo = gr.typeBc[2 * d], hi = gr.typeBc[2 * d + 1];
+    if (lo != hi || (lo != BX_BC_FLOAT && lo != BX_BC_PERIODIC))
+      return core_fail(BX_ERR_ARG, "heat conduction needs float or periodic boundaries, alike on both sides");
+    H.a.periodic[d] = lo == BX_BC_PERIODIC;
+  }
   const int lev = gr.lev[0];
   long nTot = 1;
   for (int d = 0; d < 3; d++) {

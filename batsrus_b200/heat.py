@@ -3,7 +3,7 @@
 
 ``HeatSolver`` works on the grid of an
 :class:`~batsrus_b200.explicit.ExplicitSolver` (all blocks of 8^3 at one
-level, float boundaries):
+level, float or periodic boundaries):
 
 * ``advance_semi_impl()`` -- one solve of advance_semi_impl (:240): the
   right-hand side, the block ILU(0) preconditioner, left-preconditioned

@@ -401,7 +401,8 @@ BX_API int bx_learned_apply_blocks(const double *v, const float *feat, int nBloc
 
 /* ---- semi-implicit field-aligned heat conduction ---------------------------
  * TypeSemiImplicit = 'parcond' of src/ModSemiImplicit.f90 on the grid given
- * to bx_init (all blocks of 8^3 at one level, float outer boundaries): one
+ * to bx_init (all blocks of 8^3 at one level, float or periodic outer
+ * boundaries, alike on the two sides of a dimension): one
  * linear solve per call, the electron temperature as the semi-implicit
  * variable, HeatCoef = HeatCondPar Te^2.5 and the tensor
  * FractionFieldAligned b b + (1 - FractionFieldAligned) I of
@@ -426,7 +427,7 @@ typedef struct {
  * reads: Te (nI, nJ, nK, nBlock), the unit field direction bhat
  * (3, nI, nJ, nK, nBlock) and used (nI, nJ, nK, nBlock): 1 for cells of the
  * solve, 0 for cells whose temperature is held (Used_GB of the body).
- * Rejected on multi-level grids and periodic boundaries. */
+ * Rejected on multi-level grids and mixed boundaries in one dimension. */
 BX_API int bx_heat_init(const bx_heat_params *params, const double *Te, const double *bhat,
                         const unsigned char *used);
 /* advance_semi_impl (src/ModSemiImplicit.f90:240): the right-hand side

@@ -2147,12 +2147,13 @@ struct Heat {
   std::vector<double> dIlu;
 
   long id(int i, int j, int k) const { return i + (long)n[0] * (j + (long)n[1] * k); }
-  long idc(int i, int j, int k) const {  // float boundary: clamp into the domain
-    i = std::min(std::max(i, 0), n[0] - 1);
-    j = std::min(std::max(j, 0), n[1] - 1);
-    k = std::min(std::max(k, 0), n[2] - 1);
-    return id(i, j, k);
+  // the cell of (i,j,k) inside the domain: clamped at a float boundary
+  // (the ghost cell copies the boundary cell), wrapped at a periodic one
+  int bnd(int x, int d) const {
+    if (c.periodic[d]) return (x % n[d] + n[d]) % n[d];
+    return std::min(std::max(x, 0), n[d] - 1);
   }
+  long idc(int i, int j, int k) const { return id(bnd(i, 0), bnd(j, 1), bnd(k, 2)); }
   long nCell() const { return (long)n[0] * n[1] * n[2]; }
 
   void init(const int *nc, int nb, const double *d, const double *te, const double *bh, const unsigned char *u,

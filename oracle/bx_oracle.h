@@ -128,8 +128,9 @@ void ora_impl_get_x(void *h, double *x);
 
 /* ---- semi-implicit field-aligned heat conduction (ModSemiImplicit with
  * TypeSemiImplicit = 'parcond', ModHeatConduction) on a uniform Cartesian
- * grid of nCell[0] x nCell[1] x nCell[2] cells (x fastest), float outer
- * boundaries, blocks of nB^3 cells for the block ILU */
+ * grid of nCell[0] x nCell[1] x nCell[2] cells (x fastest), float or
+ * periodic outer boundaries per dimension, blocks of nB^3 cells for the
+ * block ILU */
 typedef struct {
   double heatCondPar;     /* HeatCondPar: HeatCoef = HeatCondPar * Te^2.5 */
   double fieldAligned;    /* FractionFieldAligned: Bb = f bb + (1 - f) I */
@@ -140,6 +141,7 @@ typedef struct {
   int maxMatvec;
   double errorMax;        /* relative tolerance on the preconditioned residual */
   int typePrecond;        /* 0 none, 1 block ILU(0) */
+  int periodic[3];        /* 1: periodic in that dimension, 0: float boundary */
 } ora_heat_config;
 
 void *ora_heat_new(const int nCell[3], int nB, const double dx[3], const double *Te, const double *bhat,

@@ -319,14 +319,15 @@ Oracle.impl_x = _oracle_impl_x
 class HeatConfig(ctypes.Structure):
     _fields_ = [("heatCondPar", ctypes.c_double), ("fieldAligned", ctypes.c_double), ("cv", ctypes.c_double),
                 ("dt", ctypes.c_double), ("semiImplCoeff", ctypes.c_double), ("nKrylovVector", ctypes.c_int),
-                ("maxMatvec", ctypes.c_int), ("errorMax", ctypes.c_double), ("typePrecond", ctypes.c_int)]
+                ("maxMatvec", ctypes.c_int), ("errorMax", ctypes.c_double), ("typePrecond", ctypes.c_int),
+                ("periodic", ctypes.c_int * 3)]
 
 
 class HeatOracle:
     """Semi-implicit heat conduction restated on the CPU (global arrays,
     x fastest; blocks of 8^3 for the block ILU)."""
 
-    def __init__(self, n, dx, Te, bhat, used, params):
+    def __init__(self, n, dx, Te, bhat, used, params, periodic=(False, False, False)):
         L = lib()
         for name, res in (("ora_heat_new", ctypes.c_void_p), ("ora_heat_solve", ctypes.c_int)):
             getattr(L, name).restype = res
@@ -337,7 +338,8 @@ class HeatOracle:
             getattr(L, name).argtypes = None
         c = HeatConfig(params.heatCondPar, params.fieldAligned, params.cv, params.dt, params.semiImplCoeff,
                        params.nKrylovVector, params.maxMatvec, params.errorMax,
-                       {"none": 0, "bilu": 1}[params.typePrecond.lower()])
+                       {"none": 0, "bilu": 1}[params.typePrecond.lower()],
+                       (ctypes.c_int * 3)(*[int(bool(q)) for q in periodic]))
         self.N = n ** 3
         self._keep = [np.ascontiguousarray(Te, dtype=np.float64), np.ascontiguousarray(bhat, dtype=np.float64),
                       np.ascontiguousarray(used, dtype=np.uint8)]

@@ -19,10 +19,11 @@ from oracle import HeatOracle
 pytestmark = pytest.mark.gpu
 
 
-def setup(nRoot=2, seed=7, order="x", **kw):
+def setup(nRoot=2, seed=7, order="x", periodic=False, **kw):
     g, Te, b, used, dx = heat_dipole(nRoot=nRoot, seed=seed)
-    if order != "x":
-        g = BlockGrid.uniform(3, (8, 8, 8), (nRoot,) * 3, (-0.5,) * 3, (0.5,) * 3, ("float",) * 6, order=order)
+    if order != "x" or periodic:
+        bc = ("periodic" if periodic else "float",) * 6
+        g = BlockGrid.uniform(3, (8, 8, 8), (nRoot,) * 3, (-0.5,) * 3, (0.5,) * 3, bc, order=order)
     p = HeatParams(**kw)
     n = 8 * nRoot
     x = ExplicitSolver(g, Scheme())
@@ -30,7 +31,7 @@ def setup(nRoot=2, seed=7, order="x", **kw):
     def to_blocks(a):
         return global_to_blocks(a.reshape((n, n, n) + a.shape[1:]), nRoot)[perm]
     h = HeatSolver(x, p, to_blocks(Te), to_blocks(b), to_blocks(used))
-    o = HeatOracle(n, dx, Te, b, used, p)
+    o = HeatOracle(n, dx, Te, b, used, p, periodic=(periodic,) * 3)
 
     def to_global(a):
         out = np.empty_like(a)
@@ -49,9 +50,11 @@ def close(x, o):
     o.close()
 
 
-@pytest.mark.parametrize("order", ["x", "morton"])
-def test_rhs_matvec_precond_match_oracle(order):
-    x, h, o, tb, tg, _ = setup(order=order)
+@pytest.mark.parametrize("order,periodic", [("x", False), ("morton", False), ("morton", True)])
+def test_rhs_matvec_precond_match_oracle(order, periodic):
+    """float and periodic outer boundaries (periodic: the ghost layer of the
+    tile wraps around the domain)"""
+    x, h, o, tb, tg, _ = setup(order=order, periodic=periodic)
     ref = o.rhs()
     got = tg(h.rhs())
     assert np.abs(got - ref).max() <= 1e-12 * np.abs(ref).max()
@@ -65,9 +68,9 @@ def test_rhs_matvec_precond_match_oracle(order):
     close(x, o)
 
 
-@pytest.mark.parametrize("prec", ["BILU", "NONE"])
-def test_solve_matches_oracle(prec):
-    x, h, o, tb, tg, (Te, _, used) = setup(nRoot=3, seed=5, typePrecond=prec)
+@pytest.mark.parametrize("prec,periodic", [("BILU", False), ("NONE", False), ("BILU", True)])
+def test_solve_matches_oracle(prec, periodic):
+    x, h, o, tb, tg, (Te, _, used) = setup(nRoot=3, seed=5, typePrecond=prec, periodic=periodic)
     s = h.advance_semi_impl()
     r, xo, nm, err = o.solve()
     assert r == 0 and s["iError"] == 0
@@ -124,16 +127,9 @@ def test_maxmatvec_reached_is_an_error():
     close(x, o)
 
 
-def test_rejects_multilevel_and_periodic_grids():
+def test_rejects_multilevel_grids():
     from batsrus_b200 import configs
     g = configs.amr_blast(nRoot=2, maxLevel=2, with_state=False)[0]
-    x = ExplicitSolver(g, Scheme())
-    z = np.zeros(g.nCell)
-    with pytest.raises(capi.BxError) as e:
-        HeatSolver(x, HeatParams(), z + 1, np.zeros((g.nCell, 3)), z.astype(np.uint8))
-    assert e.value.code == 1
-    x.close()
-    g = BlockGrid.uniform(3, (8, 8, 8), (2, 2, 2), (-0.5,) * 3, (0.5,) * 3, ("periodic",) * 6)
     x = ExplicitSolver(g, Scheme())
     z = np.zeros(g.nCell)
     with pytest.raises(capi.BxError) as e:

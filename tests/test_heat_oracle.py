@@ -107,6 +107,32 @@ def test_rhs_and_matvec_match_numpy_restatement():
     o.close()
 
 
+def test_periodic_boundaries_commute_with_a_cyclic_shift():
+    """Periodic in all three dimensions, every cell used: the right-hand side
+    of the cyclically shifted temperature and field is the shifted
+    right-hand side (the boundary faces couple the opposite sides), and the
+    fluxes through the periodic faces cancel: the sum of V Res is zero to
+    rounding.  With float boundaries the shift changes the result."""
+    n, dx, Te, b, used, p = case()
+    used = np.ones_like(used)
+    T3, b3 = Te.reshape(n, n, n), b.reshape(n, n, n, 3)
+    sh = (3, 5, 7)
+    roll = lambda a: np.roll(a, sh, axis=(0, 1, 2))
+    per = (True, True, True)
+    o = HeatOracle(n, dx, Te, b, used, p, periodic=per)
+    o2 = HeatOracle(n, dx, roll(T3).ravel(), roll(b3).reshape(-1, 3), used, p, periodic=per)
+    r1, r2 = o.rhs().reshape(n, n, n), o2.rhs().reshape(n, n, n)
+    assert np.abs(roll(r1) - r2).max() <= 1e-12 * np.abs(r1).max()
+    assert abs(r1.sum()) <= 1e-10 * np.abs(r1).sum()
+    o.close()
+    o2.close()
+    f = HeatOracle(n, dx, Te, b, used, p)
+    f2 = HeatOracle(n, dx, roll(T3).ravel(), roll(b3).reshape(-1, 3), used, p)
+    assert np.abs(roll(f.rhs().reshape(n, n, n)) - f2.rhs().reshape(n, n, n)).max() > 1e-6 * np.abs(r1).max()
+    f.close()
+    f2.close()
+
+
 def test_isotropic_limit_is_the_7_point_laplacian():
     n = 16
     dx = 1.0 / n
