@@ -1229,6 +1229,8 @@ int bx_regrid(const bx_grid_desc *gd, const int *iRemap_IB) {
   if (!gd || !iRemap_IB) return fail(BX_ERR_ARG, "null argument");
   if (!g.use3d) return fail(BX_ERR_ARG, "regrid needs 3D 8x8x8 or 4x4x4 blocks");
   if (g.nOwned < g.nBlock) return fail(BX_ERR_ARG, "regrid of one rank of a partitioned grid is not built");
+  if (gd->nOwned != 0 && gd->nOwned != gd->nBlock)
+    return fail(BX_ERR_ARG, "regrid builds an unpartitioned grid: nOwned=%d must be 0 or nBlock", gd->nOwned);
   if (gd->nDim != g.nDim || gd->nI != g.nI || gd->nJ != g.nJ || gd->nK != g.nK)
     return fail(BX_ERR_ARG, "regrid cannot change the block size");
   for (int d = 0; d < 3; d++)
@@ -1295,7 +1297,9 @@ int bx_regrid(const bx_grid_desc *gd, const int *iRemap_IB) {
     g_hand.cap = newCap;
   }
   const bx_scheme_params sch = g.sch;
-  int r = bx_init(gd, &sch);
+  bx_grid_desc gdNew = *gd;
+  gdNew.nOwned = 0;  // a regrid builds an unpartitioned grid
+  int r = bx_init(&gdNew, &sch);
   if (g_hand.A) {  // not taken over (bx_init failed before the state)
     cudaFree(g_hand.A); cudaFree(g_hand.B);
     g_hand = StateHandoff();
@@ -1346,7 +1350,7 @@ int bx_do_amr(const bx_amr_params *p, int *nBlockNew, int *IsChanged) {
   if (r) return r;
   std::vector<int> lc(4 * (size_t)g.nBlock);
   bx_get_grid(lc.data());
-  bx_grid_desc gd;
+  bx_grid_desc gd{};  // nOwned = 0: the new grid is not partitioned
   gd.nDim = g.nDim; gd.nI = g.nI; gd.nJ = g.nJ; gd.nK = g.nK;
   for (int d = 0; d < 3; d++) { gd.nRootBlock[d] = g.nRoot[d]; gd.CoordMin[d] = g.cmin[d]; gd.CoordMax[d] = g.cmax[d]; }
   for (int s = 0; s < 6; s++) gd.TypeBc[s] = g.typeBc[s];

@@ -221,3 +221,19 @@ def test_do_amr_in_the_library_matches_the_host_restatement():
     x.advance(1)
     assert np.isfinite(x.get_state()[isl]).all()
     x.close()
+
+
+def test_do_amr_repeatedly():
+    """Consecutive bx_do_amr calls (each a regrid that rebuilds the context)
+    keep the grid unpartitioned: every call succeeds, the block count
+    follows the tree, and the state stays finite."""
+    g, s, x, o = setup()
+    for it in range(4):
+        x.advance(1)
+        c = x.amr_criteria(["gradlogp"])
+        p = amr.AmrParams(criteria=[amr.AmrCriterion("gradlogp", gap_limit(c[:, 0], 40 + 5 * it),
+                                                     gap_limit(c[:, 0], 80))], maxBlockLevel=3)
+        x.do_amr(p)
+        assert x.grid.nBlock == len(x.grid.iLevelCoord)
+        assert np.isfinite(x.get_state()[x.grid.interior_slices()]).all()
+    x.close()
