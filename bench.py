@@ -49,14 +49,16 @@ def peaks():
 
 
 # DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) per cell of one
-# stage3d_kernel launch, from one ncu capture of a stage-1 launch of the
-# 160^3 Orszag-Tang case (20^3 blocks, 0.26 GB of state, larger than L2):
+# stage8_kernel launch, the mean of a stage-1 and a stage-2 launch, from ncu
+# captures of the 160^3 Orszag-Tang case (20^3 blocks, 0.26 GB of state,
+# larger than L2):
 #   python bench.py --nroot 20 --precisions <p> --steps 2 --warmup 3 --no-e2e --no-cpu \
-#       --jfnk-precond= --heat-precond= --no-amr
-#   ncu --set full --clock-control none -k regex:stage3d -s 2 -c 1 <same command>
-# Traffic grows in proportion to the blocks, so the bench scales it by the
-# cells of its own grid.
-DRAM_BYTES_PER_CELL_LAUNCH = {"fp64": 142.2, "fp32": 108.3}
+#       --no-amr --jfnk-precond= --heat-precond= --no-autotune
+#   ncu --metrics gpu__time_duration.sum,dram__bytes_read.sum,dram__bytes_write.sum \
+#       --clock-control none -k regex:stage8 -s 2 -c 2 --csv <same command>
+# FP64: 136.2 and 199.9 B; FP32-bulk: 110.0 and 158.8 B.  Traffic grows in
+# proportion to the blocks, so the bench scales it by the cells of its grid.
+DRAM_BYTES_PER_CELL_LAUNCH = {"fp64": 168.0, "fp32": 134.4}
 
 
 def profile_traffic(prec):
