@@ -133,14 +133,16 @@ uint64_t morton3(uint32_t x, uint32_t y, uint32_t z) {
 // kernels of the host boundary
 
 // State_VGB (var fastest, ghost cells) -> SoA interior
+// the interior of a [block][k][j][i][var] array whose rows hold sI cells,
+// planes sJ rows and blocks sK planes, the interior starting at (oi, oj, ok)
 __global__ void aos_to_soa(const double *__restrict__ aos, double *__restrict__ soa, int nBlock,
-                           int nI, int nJ, int nK, int nIg, int nJg, int nKg, int gi, int gj, int gk) {
+                           int nI, int nJ, int nK, int sI, int sJ, int sK, int oi, int oj, int ok) {
   const long nC = (long)nI * nJ * nK;
   const long total = nC * nBlock;
   for (long q = blockIdx.x * (long)blockDim.x + threadIdx.x; q < total; q += (long)gridDim.x * blockDim.x) {
     const long b = q / nC, c = q % nC;
     const int i = c % nI, j = (c / nI) % nJ, k = c / ((long)nI * nJ);
-    const double *s = aos + 8 * ((i + gi) + (long)nIg * ((j + gj) + (long)nJg * ((k + gk) + (long)nKg * b)));
+    const double *s = aos + 8 * ((i + oi) + (long)sI * ((j + oj) + (long)sJ * ((k + ok) + (long)sK * b)));
     double *t = soa + b * 8 * nC + c;
 #pragma unroll
     for (int v = 0; v < 8; v++) t[v * nC] = s[v];
@@ -861,11 +863,23 @@ int bx_upload_state(const double *State_VGB, int nBlock) {
   if (!State_VGB || nBlock != g.nBlock) return fail(BX_ERR_ARG, "nBlock=%d, expected %d", nBlock, g.nBlock);
   int nIg, nJg, nKg, gi, gj, gk;
   ghost_extent(nIg, nJg, nKg, gi, gj, gk);
-  const size_t bytes = sizeof(double) * 8 * (size_t)nIg * nJg * nKg * g.nBlock;
+  // only the x runs of the interior rows cross the bus (one strided copy):
+  // the ghost cells of State_VGB are rebuilt on the device before every
+  // stage, so rows 1..nJ of every plane, cells 1..nI of a row, are all the
+  // state there is; k ghost planes come along because the plane stride is
+  // uniform only over all planes
+  const size_t row = sizeof(double) * 8 * (size_t)g.nI;
+  const size_t bytes = row * g.nJ * nKg * g.nBlock;
   int r = ensure_stage_aos(bytes);
   if (r) return r;
-  CK(cudaMemcpyAsync(g.stageAoS, State_VGB, bytes, cudaMemcpyHostToDevice, g.st));
-  aos_to_soa<<<1184, 256, 0, g.st>>>(g.stageAoS, g.A, g.nBlock, g.nI, g.nJ, g.nK, nIg, nJg, nKg, gi, gj, gk);
+  cudaMemcpy3DParms cp = {};
+  cp.srcPtr = make_cudaPitchedPtr(const_cast<double *>(State_VGB) + 8 * (gi + (size_t)nIg * gj),
+                                  sizeof(double) * 8 * (size_t)nIg, sizeof(double) * 8 * (size_t)nIg, nJg);
+  cp.dstPtr = make_cudaPitchedPtr(g.stageAoS, row, row, g.nJ);
+  cp.extent = make_cudaExtent(row, g.nJ, (size_t)nKg * g.nBlock);
+  cp.kind = cudaMemcpyHostToDevice;
+  CK(cudaMemcpy3DAsync(&cp, g.st));
+  aos_to_soa<<<1184, 256, 0, g.st>>>(g.stageAoS, g.A, g.nBlock, g.nI, g.nJ, g.nK, g.nI, g.nJ, nKg, 0, 0, gk);
   CK(cudaGetLastError());
   if (g.Nx) {
     const size_t sb = sizeof(double) * 8 * g.nCell * g.nBlock;

@@ -306,20 +306,33 @@ __device__ __forceinline__ void sweep3(const StageArgs &a, const BlockGeom &g, c
     const int i = c % T::N, j = (c / T::N) % T::N, k = c / (T::N * T::N);
     const int f0 = face_id<T, D>(i, j, k);
     const int f1 = face_id<T, D>(i + (D == 0), j + (D == 1), k + (D == 2));
+    if constexpr (kFloatFlux) {
+      // FP32 fluxes: the three directions' differences summed in FP32 (the
+      // running sum is an FP32 value held in the FP64 accumulator), as
+      // stage8_kernel sums them, so that every variant gives the same bits
+      // (the product is not contracted into the sum: __fmul_rn)
 #pragma unroll
-    for (int v = 0; v < 8; v++) {
-      // FP32 fluxes: the difference of neighbouring faces in FP32 (exact
-      // when they are within a factor of two) and one conversion
-      const double d = kFloatFlux ? (double)(fbuf[v * T::NF + f0] - fbuf[v * T::NF + f1])
-                                  : (double)fbuf[v * T::NF + f0] - (double)fbuf[v * T::NF + f1];
-      chg[r][v] = D == 0 ? d : chg[r][v] + d;
+      for (int v = 0; v < 8; v++) {
+        const Real d = fbuf[v * T::NF + f0] - fbuf[v * T::NF + f1];
+        chg[r][v] = D == 0 ? (double)d : (double)((Real)chg[r][v] + d);
+      }
+      // div B from the face normal field, (L+R)/2 differences over the cell
+      const float db = __fmul_rn((float)g.invHalf[D], fbuf[9 * T::NF + f1] - fbuf[9 * T::NF + f0]);
+      divB[r] = D == 0 ? (double)db : (double)((float)divB[r] + db);
+      const Real vm = fmax(fbuf[8 * T::NF + f0], fbuf[8 * T::NF + f1]);
+      vdt[r] = D == 0 ? (double)vm : (double)((Real)vdt[r] + vm);
+    } else {
+#pragma unroll
+      for (int v = 0; v < 8; v++) {
+        const double d = (double)fbuf[v * T::NF + f0] - (double)fbuf[v * T::NF + f1];
+        chg[r][v] = D == 0 ? d : chg[r][v] + d;
+      }
+      // div B from the face normal field, (L+R)/2 differences over the cell
+      const double db = g.invHalf[D] * ((double)fbuf[9 * T::NF + f1] - (double)fbuf[9 * T::NF + f0]);
+      divB[r] = D == 0 ? db : divB[r] + db;
+      const double vm = (double)fmax(fbuf[8 * T::NF + f0], fbuf[8 * T::NF + f1]);
+      vdt[r] = D == 0 ? vm : vdt[r] + vm;
     }
-    // div B from the face normal field, (L+R)/2 differences over the cell
-    const double db = g.invHalf[D] * (kFloatFlux ? (double)(fbuf[9 * T::NF + f1] - fbuf[9 * T::NF + f0])
-                                                 : (double)fbuf[9 * T::NF + f1] - (double)fbuf[9 * T::NF + f0]);
-    divB[r] = D == 0 ? db : divB[r] + db;
-    const double vm = (double)fmax(fbuf[8 * T::NF + f0], fbuf[8 * T::NF + f1]);
-    vdt[r] = D == 0 ? vm : vdt[r] + vm;
   }
   __syncthreads();
 }

@@ -380,10 +380,12 @@ __global__ void __launch_bounds__(B::NTHR, B::MINB)
         for (int v = 0; v < 8; v++) o[r][v] = old[v * B::NC + c];
       }
       const int i = c & 7, j = (c >> 3) & 7, k = c >> 6;
-      if (kFloatFlux) {
+      if constexpr (kFloatFlux) {
         // FP32 fluxes: the three directions' differences summed in FP32
         // (each difference of neighbouring faces is exact when they are
-        // within a factor of two), one conversion per variable
+        // within a factor of two), one conversion per variable; the div B
+        // product is not contracted into its sum (__fmul_rn), as in
+        // stage3d_kernel
         Real cs[8], dbs = Real(0), vs = Real(0);
 #pragma unroll
         for (int D = 0; D < 3; D++) {
@@ -395,7 +397,7 @@ __global__ void __launch_bounds__(B::NTHR, B::MINB)
             const Real d = F[v * 576 + f0] - F[v * 576 + f1];
             cs[v] = D == 0 ? d : cs[v] + d;
           }
-          const Real db = (Real)M.g.invHalf[D] * (F[9 * 576 + f1] - F[9 * 576 + f0]);
+          const Real db = __fmul_rn((float)M.g.invHalf[D], F[9 * 576 + f1] - F[9 * 576 + f0]);
           dbs = D == 0 ? db : dbs + db;
           if (a.computeDt) {
             const Real vm = fmax(F[8 * 576 + f0], F[8 * 576 + f1]);

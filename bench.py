@@ -211,9 +211,14 @@ def run_ours(args):
                 x2.get_state(back.numpy())
                 return x2.region_end()
             evalue, ems = replica_rate(timed_e2e, nCell * args.steps, world)
-            nbytes = host.numel() * 8
+            # bx_download_state returns all of State_VGB, ghost cells included;
+            # bx_upload_state moves the interior x runs of the interior rows of
+            # every plane (one strided copy: nI x nJ of nIg x nJg cells per plane)
+            sh = g.state_shape_fortran()  # (8, nIg, nJg, nKg, nBlock)
+            d2h = host.numel() * 8
+            h2d = d2h * (g.nI * g.nJ) // (sh[1] * sh[2])
             res["e2e"] = {"value": evalue, "unit": UNIT,
-                          "h2d_bytes_per_step": nbytes / args.steps, "d2h_bytes_per_step": nbytes / args.steps,
+                          "h2d_bytes_per_step": h2d / args.steps, "d2h_bytes_per_step": d2h / args.steps,
                           "ms": ems}
             x2.close()
         else:
