@@ -20,6 +20,7 @@ FLUX = {"rusanov": 0, "linde": 1, "hlld": 2, "roe": 3}
 LIMITER = {"minmod": 0, "mc": 1, "mc3": 2, "koren": 2, "no": 0}
 BC = {"float": 0, "periodic": 1}
 PRECISION = {"fp64": 0, "fp32": 1, "fp32-bulk": 1}
+PRECOND_PRECISION = {"fp64": 0, "fp32": 1, "bf16": 2}  # BILU factor storage of the implicit step
 
 # every entry point declared in include/bx200.h
 EXPORTS = (
@@ -117,7 +118,7 @@ def implicit_params(p):
     c.MaxMatvec = p.maxMatvec
     c.ErrorMax = p.errorMax
     c.TypePrecond = PRECOND[p.typePrecond.lower()]
-    c.PrecondPrecision = PRECISION[p.precondPrecision.lower()]
+    c.PrecondPrecision = PRECOND_PRECISION[p.precondPrecision.lower()]
     return c
 
 

@@ -108,9 +108,9 @@ def uniform_3d_case(nRoot, flux, limiter="mc3", beta=1.2, precision="fp64", nCel
     return g, s, st, {}
 
 
-def jfnk_ot(nRoot=16, precond="BILU", seed=2024, with_state=True, precondPrecision="fp32"):
+def jfnk_ot(nRoot=16, precond="BILU", seed=2024, with_state=True, precondPrecision="bf16"):
     """The implicit workload: perturbed Orszag-Tang on (8 nRoot)^3 cells,
-    BDF2 at CFL 20, GMRES(30) to 1e-3; BILU factors stored in FP32 unless
+    BDF2 at CFL 20, GMRES(30) to 1e-3; BILU factors stored in BF16 unless
     precondPrecision says otherwise."""
     from .implicit_params import ImplicitParams
     g = BlockGrid.uniform(3, (8, 8, 8), (nRoot,) * 3, (0.0, 0.0, 0.0), (1.0, 1.0, 1.0), ("periodic",) * 6)

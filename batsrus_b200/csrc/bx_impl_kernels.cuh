@@ -4,7 +4,10 @@
 // tree).  Vectors use the state layout [block][var][cell] (SoA), the
 // implicit variables hold total energy in the pressure slot.
 #pragma once
+#include <cuda_bf16.h>
 #include <cuda_runtime.h>
+
+#include <type_traits>
 
 #include "bx_device.h"
 #include "bx_physics.cuh"
@@ -214,8 +217,8 @@ __device__ __forceinline__ void load_cell(const JacArgs &a, int b, int i, int j,
 //   fwd [p][4][8][8]  blocks 0..2: A(c, c-e_d) for d = x, y, z (absent on
 //                     the low faces of the block); block 3: A(c, c), which
 //                     the factorisation replaces by D_c^-1
-//   bwd [p][3][8][8]  A(c, c+e_d) (absent on the high faces); with FP32
-//                     storage the factorisation replaces it by
+//   bwd [p][3][8][8]  A(c, c+e_d) (absent on the high faces); with FP32 or
+//                     BF16 storage the factorisation replaces it by
 //                     D_c^-1 A(c, c+e_d), so that the backward sweep reads
 //                     three blocks per cell instead of four.  FP64 storage
 //                     keeps A(c, c+e_d) and the operation order of the
@@ -236,6 +239,15 @@ struct BiluLayout {
 
 __device__ __forceinline__ void store_t(double *p, double v) { *p = v; }
 __device__ __forceinline__ void store_t(float *p, double v) { *p = (float)v; }
+__device__ __forceinline__ void store_t(__nv_bfloat16 *p, double v) { *p = __float2bfloat16_rn((float)v); }
+
+// arithmetic type of the factorisation for a storage type: FP64 for FP64,
+// FP32 for FP32 and BF16
+template <typename T> struct BiluArith { using R = T; };
+template <> struct BiluArith<__nv_bfloat16> { using R = float; };
+__device__ __forceinline__ double to_d(double x) { return x; }
+__device__ __forceinline__ double to_d(float x) { return (double)x; }
+__device__ __forceinline__ double to_d(__nv_bfloat16 x) { return (double)__bfloat162float(x); }
 
 // a b + c: fused in FP32; in FP64 a product and a sum, the rounding of the
 // reference's loops (this file is compiled without contraction)
@@ -270,6 +282,32 @@ __device__ __forceinline__ void load_raw8(const float *p, float (&r)[8]) {
     const float4 t = q[m];
     r[4 * m] = t.x; r[4 * m + 1] = t.y; r[4 * m + 2] = t.z; r[4 * m + 3] = t.w;
   }
+}
+__device__ __forceinline__ void load_raw8(const __nv_bfloat16 *p, __nv_bfloat16 (&r)[8]) {
+  const uint4 t = *reinterpret_cast<const uint4 *>(p);
+  const __nv_bfloat162 *h = reinterpret_cast<const __nv_bfloat162 *>(&t);
+#pragma unroll
+  for (int m = 0; m < 4; m++) { r[2 * m] = h[m].x; r[2 * m + 1] = h[m].y; }
+}
+// one row in the factorisation's arithmetic type
+__device__ __forceinline__ void load_rowR(const double *p, double (&r)[8]) { load_row8(p, r); }
+__device__ __forceinline__ void load_rowR(const float *p, float (&r)[8]) { load_raw8(p, r); }
+__device__ __forceinline__ void load_rowR(const __nv_bfloat16 *p, float (&r)[8]) {
+  const uint4 t = *reinterpret_cast<const uint4 *>(p);
+  const __nv_bfloat162 *h = reinterpret_cast<const __nv_bfloat162 *>(&t);
+#pragma unroll
+  for (int m = 0; m < 4; m++) {
+    const float2 f = __bfloat1622float2(h[m]);
+    r[2 * m] = f.x;
+    r[2 * m + 1] = f.y;
+  }
+}
+__device__ __forceinline__ void store_row8(__nv_bfloat16 *p, const float (&r)[8]) {
+  uint4 t;
+  __nv_bfloat162 *h = reinterpret_cast<__nv_bfloat162 *>(&t);
+#pragma unroll
+  for (int m = 0; m < 4; m++) h[m] = __floats2bfloat162_rn(r[2 * m], r[2 * m + 1]);
+  *reinterpret_cast<uint4 *>(p) = t;
 }
 __device__ __forceinline__ void store_row8(double *p, const double (&r)[8]) {
   double2 *q = reinterpret_cast<double2 *>(p);
@@ -436,7 +474,7 @@ __global__ void __launch_bounds__(kJacThreads, 4) k_jacobian(JacArgs a) {
   const double epsj = a.sqrtJacEps * a.norm[jv];
   const double coeff = -0.5 / (a.sqrtJacEps * a.norm[jv]);
   int e2;
-  const bool mulV = sizeof(T) == 4 || frexp(g.volume, &e2) == 0.5;  // FP32 storage, or V = 2^k
+  const bool mulV = sizeof(T) < 8 || frexp(g.volume, &e2) == 0.5;  // FP32 / BF16 storage, or V = 2^k
   const double invV = 1.0 / g.volume;
   double diag[8] = {0, 0, 0, 0, 0, 0, 0, 0};
   jac_dir<N, 0>(a, b, i, j, k, jv, U0, g, diag, F, sc, pre, nCell, epsj, coeff, mulV, invV);
@@ -533,7 +571,8 @@ __device__ __forceinline__ void group_inverse8(R (&a)[8], R (&inv)[8], int row) 
 // D_c^-1 A(c,c+e_d) once D_c^-1 is known.
 template <int N, typename T>
 __global__ void __launch_bounds__(384, 2) k_bilu_factor(BiluArgs a) {  // two CTAs of 8 x 48 lanes per SM
-  constexpr bool kPre = sizeof(T) == 4;
+  constexpr bool kPre = !std::is_same<T, double>::value;
+  using R = typename BiluArith<T>::R;
   constexpr int NC = N * N * N, kWave = 3 * N - 2;
   __shared__ int sCell[NC], sPos[NC], sStart[kWave + 1];
   const int b = blockIdx.x;
@@ -550,52 +589,52 @@ __global__ void __launch_bounds__(384, 2) k_bilu_factor(BiluArgs a) {  // two CT
       const int c = active ? sCell[p] : 0;
       const int i = c % N, j = (c / N) % N, k = c / (N * N);
       const int idx[3] = {i, j, k};
-      T D[8];
-      if (active) load_raw8(F + BiluLayout<N>::fwd(b, p, 3) + row * 8, D);
+      R D[8];
+      if (active) load_rowR(F + BiluLayout<N>::fwd(b, p, 3) + row * 8, D);
       else
 #pragma unroll
-        for (int q = 0; q < 8; q++) D[q] = q == row ? T(1) : T(0);
+        for (int q = 0; q < 8; q++) D[q] = q == row ? R(1) : R(0);
 #pragma unroll
       for (int d = 0; d < 3; d++) {
         if (!active || idx[d] == 0) continue;
         const int pl = sPos[c - (d == 0 ? 1 : (d == 1 ? N : N * N))];
-        T L[8];
-        load_raw8(F + BiluLayout<N>::fwd(b, p, d) + row * 8, L);
+        R L[8];
+        load_rowR(F + BiluLayout<N>::fwd(b, p, d) + row * 8, L);
         const T *Un = F + BiluLayout<N>::bwd(b, pl, d);  // A(cl, c), or D_cl^-1 A(cl, c)
         if (!kPre) {
           const T *Dn = F + BiluLayout<N>::fwd(b, pl, 3);
-          T T1[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+          R T1[8] = {0, 0, 0, 0, 0, 0, 0, 0};
 #pragma unroll
           for (int m = 0; m < 8; m++) {
-            T dr[8];
-            load_raw8(Dn + m * 8, dr);
+            R dr[8];
+            load_rowR(Dn + m * 8, dr);
 #pragma unroll
             for (int q = 0; q < 8; q++) T1[q] = madd(L[m], dr[q], T1[q]);
           }
 #pragma unroll
           for (int q = 0; q < 8; q++) L[q] = T1[q];
         }
-        T T2[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+        R T2[8] = {0, 0, 0, 0, 0, 0, 0, 0};
 #pragma unroll
         for (int m = 0; m < 8; m++) {
-          T u[8];
-          load_raw8(Un + m * 8, u);
+          R u[8];
+          load_rowR(Un + m * 8, u);
 #pragma unroll
           for (int q = 0; q < 8; q++) T2[q] = madd(L[m], u[q], T2[q]);
         }
 #pragma unroll
         for (int q = 0; q < 8; q++) D[q] -= T2[q];
       }
-      T inv[8];
+      R inv[8];
       group_inverse8(D, inv, row);
       if (active) store_row8(F + BiluLayout<N>::fwd(b, p, 3) + row * 8, inv);
       if (kPre) {
 #pragma unroll
         for (int d = 0; d < 3; d++) {
           const bool has = active && idx[d] < N - 1;
-          T A[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-          if (has) load_raw8(F + BiluLayout<N>::bwd(b, p, d) + row * 8, A);
-          T out[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+          R A[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+          if (has) load_rowR(F + BiluLayout<N>::bwd(b, p, d) + row * 8, A);
+          R out[8] = {0, 0, 0, 0, 0, 0, 0, 0};
 #pragma unroll
           for (int m = 0; m < 8; m++)
 #pragma unroll
@@ -610,15 +649,15 @@ __global__ void __launch_bounds__(384, 2) k_bilu_factor(BiluArgs a) {  // two CT
 
 // z = (LU)^-1 r on every grid block: forward v_c = D_c^-1 (r_c - sum_d
 // A(c,c-e_d) v_{c-e_d}), backward x_c = v_c - D_c^-1 sum_d A(c,c+e_d)
-// x_{c+e_d} (FP32 storage: the premultiplied blocks), in shared memory;
+// x_{c+e_d} (FP32 and BF16 storage: the premultiplied blocks), in shared memory;
 // FP64 arithmetic on factors of type T.  The wavefront tables are copied to
 // shared memory first, so that the only global loads of a wavefront are the
 // matrix rows, whose addresses follow from the position alone; v is stored
 // [var][cell] with one pad cell per variable, which keeps the copies in and
 // out and the eight row lanes of a cell on distinct banks.
 template <int N, typename T>
-__global__ void __launch_bounds__(384, sizeof(T) == 4 ? 3 : 2) k_bilu_solve(BiluArgs a) {  // 3 (FP32) or 2 CTAs of 8 x 48 lanes per SM
-  constexpr bool kPre = sizeof(T) == 4;
+__global__ void __launch_bounds__(384, sizeof(T) < 8 ? 3 : 2) k_bilu_solve(BiluArgs a) {  // 3 (FP32, BF16) or 2 CTAs of 8 x 48 lanes per SM
+  constexpr bool kPre = !std::is_same<T, double>::value;
   constexpr int NC = N * N * N, NP = NC + 1, kWave = 3 * N - 2;
   __shared__ double v[8 * NP];  // [var][cell]
   __shared__ int sCell[NC], sStart[kWave + 1];
@@ -653,12 +692,12 @@ __global__ void __launch_bounds__(384, sizeof(T) == 4 ? 3 : 2) k_bilu_solve(Bilu
         const int cl = c - (d == 0 ? 1 : (d == 1 ? N : N * N));
         double s = 0;
 #pragma unroll
-        for (int m = 0; m < 8; m++) s += (double)L[d][m] * v[m * NP + cl];
+        for (int m = 0; m < 8; m++) s += to_d(L[d][m]) * v[m * NP + cl];
         wr -= s;
       }
       double s = 0;
 #pragma unroll
-      for (int q = 0; q < 8; q++) s += (active ? (double)Di[q] : 0.0) * __shfl_sync(0xffffffffu, wr, q, 8);
+      for (int q = 0; q < 8; q++) s += (active ? to_d(Di[q]) : 0.0) * __shfl_sync(0xffffffffu, wr, q, 8);
       if (active) vr[c] = s;
     }
     __syncthreads();
@@ -684,13 +723,13 @@ __global__ void __launch_bounds__(384, sizeof(T) == 4 ? 3 : 2) k_bilu_solve(Bilu
         const int cu = c + (d == 0 ? 1 : (d == 1 ? N : N * N));
         double t = 0;
 #pragma unroll
-        for (int m = 0; m < 8; m++) t += (double)U[d][m] * v[m * NP + cu];
+        for (int m = 0; m < 8; m++) t += to_d(U[d][m]) * v[m * NP + cu];
         s += t;
       }
       if (!kPre) {  // D_c^-1 applied to the sum
         double t = 0;
 #pragma unroll
-        for (int q = 0; q < 8; q++) t += (any ? (double)Di[q] : 0.0) * __shfl_sync(0xffffffffu, s, q, 8);
+        for (int q = 0; q < 8; q++) t += (any ? to_d(Di[q]) : 0.0) * __shfl_sync(0xffffffffu, s, q, 8);
         s = t;
       }
       if (any) vr[c] = vr[c] - s;

@@ -19,6 +19,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <type_traits>
 #include <vector>
 
 #include "bx_core.h"
@@ -41,7 +42,7 @@ struct ImplCtx {
   double *dtCell = nullptr;                    // DtMax_CB left by calc_timestep
   void *F = nullptr;                           // BILU storage (BiluLayout), FP64 or FP32
   double *jacPre = nullptr;                    // k_jac_cells terms when the Krylov basis V is too small
-  bool precF32 = false;                        // FP32 factor storage
+  int precKind = BX_FP64;                      // factor storage: BX_FP64, BX_FP32_BULK, BX_BF16_FACTORS
   double *partial = nullptr, *scal = nullptr;  // reduction scratch, device scalars
   unsigned *cnt = nullptr;                     // CTA counter of the one-launch reductions
   double *dNorm = nullptr;
@@ -68,6 +69,19 @@ ImplCtx I;
   } while (0)
 
 constexpr int kG = 1184, kT = 256;  // grid-stride launch shape (8 x 148 SMs)
+
+// calls fn(std::integral_constant<int, N>, T{}) for the block size and the
+// BILU storage type of the implicit context
+template <typename Fn>
+void by_storage(int nI, Fn fn) {
+  auto with_n = [&](auto n) {
+    if (I.precKind == BX_FP32_BULK) fn(n, float{});
+    else if (I.precKind == BX_BF16_FACTORS) fn(n, __nv_bfloat16{});
+    else fn(n, double{});
+  };
+  if (nI == 8) with_n(std::integral_constant<int, 8>{});
+  else with_n(std::integral_constant<int, 4>{});
+}
 
 void free_impl() {
   for (double **p : {&I.U, &I.Uold, &I.ResExpl, &I.ResImpl, &I.Rhs, &I.X, &I.Ueps, &I.Reps, &I.W, &I.R, &I.V,
@@ -168,13 +182,9 @@ int precond(const double *r, double *z) {
     b.nBlock = c.nBlock; b.r = r; b.z = z;
     const int tv = tune_value(kTuneBiluThreads);  // 0: 8 x the widest wavefront
     const int thr = tv > 0 ? tv : ((8 * I.maxWave + 31) / 32) * 32;
-    if (c.nI == 8) {
-      if (I.precF32) k_bilu_solve<8, float><<<c.nBlock, thr, 0, c.st>>>(b);
-      else k_bilu_solve<8, double><<<c.nBlock, thr, 0, c.st>>>(b);
-    } else {
-      if (I.precF32) k_bilu_solve<4, float><<<c.nBlock, thr, 0, c.st>>>(b);
-      else k_bilu_solve<4, double><<<c.nBlock, thr, 0, c.st>>>(b);
-    }
+    by_storage(c.nI, [&](auto n, auto t) {
+      k_bilu_solve<decltype(n)::value, decltype(t)><<<c.nBlock, thr, 0, c.st>>>(b);
+    });
     CKI(cudaGetLastError());
   } else {
     CKI(cudaMemcpyAsync(z, r, sizeof(double) * I.N, cudaMemcpyDeviceToDevice, c.st));
@@ -300,25 +310,17 @@ int build_precond() {
   CKI(cudaGetLastError());
   const long nThr = I.nCellTot * 8;
   const int blocks = (int)((nThr + kJacThreads - 1) / kJacThreads);
-  if (c.nI == 8) {
-    if (I.precF32) k_jacobian<8, float><<<blocks, kJacThreads, 0, c.st>>>(ja);
-    else k_jacobian<8, double><<<blocks, kJacThreads, 0, c.st>>>(ja);
-  } else {
-    if (I.precF32) k_jacobian<4, float><<<blocks, kJacThreads, 0, c.st>>>(ja);
-    else k_jacobian<4, double><<<blocks, kJacThreads, 0, c.st>>>(ja);
-  }
+  by_storage(c.nI, [&](auto n, auto t) {
+    k_jacobian<decltype(n)::value, decltype(t)><<<blocks, kJacThreads, 0, c.st>>>(ja);
+  });
   CKI(cudaGetLastError());
   BiluArgs b;
   b.F = I.F; b.wfCell = I.wfCell; b.wfPos = I.wfPos; b.wfStart = I.wfStart; b.nWave = I.nWave;
   b.nBlock = c.nBlock; b.r = nullptr; b.z = nullptr;
   const int thr = ((8 * I.maxWave + 31) / 32) * 32;
-  if (c.nI == 8) {
-    if (I.precF32) k_bilu_factor<8, float><<<c.nBlock, thr, 0, c.st>>>(b);
-    else k_bilu_factor<8, double><<<c.nBlock, thr, 0, c.st>>>(b);
-  } else {
-    if (I.precF32) k_bilu_factor<4, float><<<c.nBlock, thr, 0, c.st>>>(b);
-    else k_bilu_factor<4, double><<<c.nBlock, thr, 0, c.st>>>(b);
-  }
+  by_storage(c.nI, [&](auto n, auto t) {
+    k_bilu_factor<decltype(n)::value, decltype(t)><<<c.nBlock, thr, 0, c.st>>>(b);
+  });
   CKI(cudaGetLastError());
   I.havePrec = true;
   return BX_OK;
@@ -370,7 +372,8 @@ int bx_implicit_init(const bx_implicit_params *prm) {
   if (prm->nKrylovVector < 1 || prm->nKrylovVector > 32)
     return core_fail(BX_ERR_ARG, "nKrylovVector=%d outside 1..32", prm->nKrylovVector);
   if (prm->TypePrecond < 0 || prm->TypePrecond > 2) return core_fail(BX_ERR_ARG, "TypePrecond=%d", prm->TypePrecond);
-  if (prm->PrecondPrecision != BX_FP64 && prm->PrecondPrecision != BX_FP32_BULK)
+  if (prm->PrecondPrecision != BX_FP64 && prm->PrecondPrecision != BX_FP32_BULK &&
+      prm->PrecondPrecision != BX_BF16_FACTORS)
     return core_fail(BX_ERR_ARG, "PrecondPrecision=%d", prm->PrecondPrecision);
   if (I.ready) free_impl();
   I.p = *prm;
@@ -389,9 +392,10 @@ int bx_implicit_init(const bx_implicit_params *prm) {
     free_impl();
     return core_fail(BX_ERR_NOMEM, "Krylov bases");
   }
-  I.precF32 = prm->PrecondPrecision == BX_FP32_BULK;
+  I.precKind = prm->PrecondPrecision;
   if (prm->TypePrecond == BX_PRECOND_BILU) {
-    const size_t fb = (I.precF32 ? sizeof(float) : sizeof(double)) * (size_t)I.nCellTot * 7 * 64;
+    const size_t eb = I.precKind == BX_FP64 ? 8 : (I.precKind == BX_FP32_BULK ? 4 : 2);
+    const size_t fb = eb * (size_t)I.nCellTot * 7 * 64;
     if (cudaMalloc(&I.F, fb) != cudaSuccess ||
         ((I.m + 1) * 8 < kJacPre && cudaMalloc(&I.jacPre, sizeof(double) * kJacPre * I.nCellTot) != cudaSuccess)) {
       free_impl();

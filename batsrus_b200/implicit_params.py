@@ -17,7 +17,7 @@ class ImplicitParams:
     maxMatvec: int = 100           # MaxMatvec (#KRYLOV)
     errorMax: float = 1e-3         # relative tolerance (#KRYLOV)
     typePrecond: str = "BILU"      # BILU | NONE | LEARNED (#PRECONDITIONER)
-    precondPrecision: str = "fp64"  # BILU factors: fp64 (the reference's) | fp32 (FP32 factorisation)
+    precondPrecision: str = "fp64"  # BILU factors: fp64 (the reference's) | fp32 | bf16 (FP32 factorisation)
 
 
 def apply_implicit_commands(commands, p):

@@ -323,7 +323,8 @@ def train_learned(args, g, s, lrank, nPair=2000, blocksPerPair=32):
     from batsrus_b200.implicit import ImplicitSolver
     from batsrus_b200.learned import LearnedPreconditioner
     net = LearnedPreconditioner(nSampleMax=nPair * blocksPerPair, seed=2024)
-    _, _, p, st2 = configs.jfnk_ot(nRoot=args.jfnk_nroot, precond="BILU", seed=2025)
+    # the training targets BILU(v) from FP32 factors (closer to the exact block ILU)
+    _, _, p, st2 = configs.jfnk_ot(nRoot=args.jfnk_nroot, precond="BILU", seed=2025, precondPrecision="fp32")
     x = ExplicitSolver(g, s, device=lrank)
     x.set_state(st2)
     im = ImplicitSolver(x, p)
@@ -650,7 +651,7 @@ def main():
     ap.add_argument("--amr-dyn-dn", type=int, default=10, help="steps between regrids (#DOAMR DnAmr)")
     ap.add_argument("--jfnk-nroot", type=int, default=16, help="16 -> 128^3 cells")
     ap.add_argument("--jfnk-steps", type=int, default=5)
-    ap.add_argument("--bilu-factors", default="fp32", choices=["fp64", "fp32"],
+    ap.add_argument("--bilu-factors", default="bf16", choices=["fp64", "fp32", "bf16"],
                     help="storage of the BILU factors of the implicit workload")
     ap.add_argument("--heat-ilu", default="fp32", choices=["fp64", "fp32"],
                     help="precision of the BILU sweeps of the heat conduction workload")

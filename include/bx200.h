@@ -55,8 +55,9 @@ enum { BX_BC_FLOAT = 0, BX_BC_PERIODIC = 1 };
 /* arithmetic of the explicit update */
 enum {
   BX_FP64 = 0,      /* FP64 everywhere, reference operation order */
-  BX_FP32_BULK = 1  /* FP32 reconstruction/fluxes/intermediate stage state,
+  BX_FP32_BULK = 1, /* FP32 reconstruction/fluxes/intermediate stage state,
                        FP64 conserved-state accumulation and p recovery */
+  BX_BF16_FACTORS = 2 /* bx_implicit_params.PrecondPrecision only */
 };
 
 /* Grid: replaces the BATL tree / ModSize / ModGeometry data the Fortran
@@ -261,11 +262,12 @@ typedef struct {
   int MaxMatvec;
   double ErrorMax;       /* relative Krylov tolerance */
   int TypePrecond;       /* BX_PRECOND_* */
-  int PrecondPrecision;  /* BILU: BX_FP64, or BX_FP32_BULK for FP32 factors
+  int PrecondPrecision;  /* BILU: BX_FP64, BX_FP32_BULK for FP32 factors
                             (FP64 Jacobian, FP32 factorisation, sweeps in
-                            FP64 arithmetic): half the bytes of every
-                            preconditioner apply; FGMRES still solves to
-                            ErrorMax */
+                            FP64 arithmetic: half the bytes of every
+                            preconditioner apply) or BX_BF16_FACTORS (the
+                            same with BF16 storage: a quarter); FGMRES still
+                            solves to ErrorMax */
 } bx_implicit_params;
 
 typedef struct {

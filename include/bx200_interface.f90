@@ -19,7 +19,7 @@ module bx200_interface
        BX_FLUX_HLLD = 2, BX_FLUX_ROE = 3
   integer(c_int), parameter:: BX_LIM_MINMOD = 0, BX_LIM_MC = 1, BX_LIM_MC3 = 2
   integer(c_int), parameter:: BX_BC_FLOAT = 0, BX_BC_PERIODIC = 1
-  integer(c_int), parameter:: BX_FP64 = 0, BX_FP32_BULK = 1
+  integer(c_int), parameter:: BX_FP64 = 0, BX_FP32_BULK = 1, BX_BF16_FACTORS = 2
 
   type, bind(C):: bx_grid_desc
      integer(c_int):: nDim, nI, nJ, nK

@@ -132,7 +132,7 @@ def test_learned_fgmres_converges_and_gains():
     vectors of BILU-preconditioned steps of a differently seeded state, half
     from probe vectors at its last state, then 8 epochs of Adam."""
     from batsrus_b200.capi import BxError
-    g, s, p, st = configs.jfnk_ot(nRoot=4)
+    g, s, p, st = configs.jfnk_ot(nRoot=4, precondPrecision="fp32")
     _, _, _, st2 = configs.jfnk_ot(nRoot=4, seed=2025)
     nPair, bpp = 2000, 16
     net = LearnedPreconditioner(nSampleMax=nPair * bpp, seed=2024)
