@@ -395,8 +395,8 @@ __global__ void k_jac_cells(JacArgs a) {
 template <int N, int D, typename T>
 __device__ __forceinline__ void jac_dir(const JacArgs &a, int b, int i, int j, int k, int jv, const double (&U0)[8],
                                         const BlockGeom &g, double (&diag)[8], T *F, const double *sc,
-                                        const double *pre, long nCell, double epsj, double coeff, bool mulV,
-                                        double invV) {
+                                        const double *pre, long nCell, const double (&Pe)[8], double coeff,
+                                        bool mulV, double invV) {
   const int idx[3] = {i, j, k};
   const double cmaxLo = pre[(24 + 2 * D) * nCell], cmaxHi = pre[(25 + 2 * D) * nCell];
   const double area = g.area[D], V = g.volume;
@@ -405,10 +405,13 @@ __device__ __forceinline__ void jac_dir(const JacArgs &a, int b, int i, int j, i
   auto perV = [&](double x) { return mulV ? x * invV : x / V; };
   const double coeffPow = -0.5 / g.cellSize[D];
   const bool powCol = a.useDivb && jv == kBx + D;
-  double Fe[8], Ue[8], dF[8];
+  double Fe[8], dF[8];
+  {  // cell_flux_e of the perturbed state, whose primitives Pe the caller made once
+    double Cons[8], un;
+    physical_flux<D>(Pe, a.invGm1, Cons, Fe, un);
 #pragma unroll
-  for (int v = 0; v < 8; v++) Ue[v] = v == jv ? U0[v] + epsj : U0[v];  // no dynamic index: stays in registers
-  cell_flux_e<D>(Ue, a.gm1, a.invGm1, area, Fe);
+    for (int v = 0; v < 8; v++) Fe[v] = Fe[v] * area;
+  }
 #pragma unroll
   for (int iv = 0; iv < 8; iv++) {
     dF[iv] = coeff * (Fe[iv] - pre[(8 * D + iv) * nCell]);
@@ -473,13 +476,18 @@ __global__ void __launch_bounds__(kJacThreads, 4) k_jacobian(JacArgs a) {
   const double *sc = scs + jv;  // sc[8 iv]: the 8 columns of a cell read 8 adjacent words
   const double epsj = a.sqrtJacEps * a.norm[jv];
   const double coeff = -0.5 / (a.sqrtJacEps * a.norm[jv]);
+  // the perturbed state and its primitives, the same for the three directions
+  double Ue[8], Pe[8];
+#pragma unroll
+  for (int v = 0; v < 8; v++) Ue[v] = v == jv ? U0[v] + epsj : U0[v];  // no dynamic index: stays in registers
+  cons_to_prim_e(Ue, a.gm1, Pe);
   int e2;
   const bool mulV = sizeof(T) < 8 || frexp(g.volume, &e2) == 0.5;  // FP32 / BF16 storage, or V = 2^k
   const double invV = 1.0 / g.volume;
   double diag[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-  jac_dir<N, 0>(a, b, i, j, k, jv, U0, g, diag, F, sc, pre, nCell, epsj, coeff, mulV, invV);
-  jac_dir<N, 1>(a, b, i, j, k, jv, U0, g, diag, F, sc, pre, nCell, epsj, coeff, mulV, invV);
-  jac_dir<N, 2>(a, b, i, j, k, jv, U0, g, diag, F, sc, pre, nCell, epsj, coeff, mulV, invV);
+  jac_dir<N, 0>(a, b, i, j, k, jv, U0, g, diag, F, sc, pre, nCell, Pe, coeff, mulV, invV);
+  jac_dir<N, 1>(a, b, i, j, k, jv, U0, g, diag, F, sc, pre, nCell, Pe, coeff, mulV, invV);
+  jac_dir<N, 2>(a, b, i, j, k, jv, U0, g, diag, F, sc, pre, nCell, Pe, coeff, mulV, invV);
   // impl_divbsrc_middle: diagonal Powell terms of column jv
   if (a.useDivb) {
     const double divB = pre[30 * nCell];

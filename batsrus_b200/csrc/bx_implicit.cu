@@ -180,7 +180,7 @@ int precond(const double *r, double *z) {
     BiluArgs b;
     b.F = I.F; b.wfCell = I.wfCell; b.wfPos = I.wfPos; b.wfStart = I.wfStart; b.nWave = I.nWave;
     b.nBlock = c.nBlock; b.r = r; b.z = z;
-    const int tv = tune_value(kTuneBiluThreads);  // 0: 8 x the widest wavefront
+    const int tv = tune_value(kTuneBiluThreads);  // 0: 8 x the widest wavefront (one pass each)
     const int thr = tv > 0 ? tv : ((8 * I.maxWave + 31) / 32) * 32;
     by_storage(c.nI, [&](auto n, auto t) {
       k_bilu_solve<decltype(n)::value, decltype(t)><<<c.nBlock, thr, 0, c.st>>>(b);
