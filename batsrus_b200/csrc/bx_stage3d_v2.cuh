@@ -93,17 +93,20 @@ __device__ __forceinline__ void p8_cell(int c, int &i, int &j, int &k, int &side
 
 // the face a lane of face group gg (0..17) of direction D takes, as the
 // face index of the slot buffer.  The four 8-lane quarters of a group take
-// rows q = 0, 2, 1, 3, so that each half-warp reads rows two apart: 24
-// doubles, i.e. different shared-memory banks for the stencil loads.
+// rows two apart (row = 8 (gg / 2) + gg % 2 + 2 q), 24 elements of the tile
+// apart: in FP32 the four quarters of a warp read four disjoint 8-bank
+// windows (12 r mod 32 = 0, 24, 16, 8), in FP64 the two quarters of each
+// half-warp read disjoint 16-bank windows.
 //   x: groups 0..15 are 4 rows (j + 8k) x faces n = 0..7, groups 16, 17 the
 //      n = 8 faces of 32 rows each; y: 8 x-positions x 4 (n + 9k) pairs;
 //   z: 8 x-positions x 4 j at one n
 template <int D>
 __device__ __forceinline__ int face_of_lane(int gg, int lane) {
-  const int q = lane >> 3, qq = ((q & 1) << 1) | (q >> 1), e = lane & 7;
-  if (D == 0) return gg < 16 ? e + 9 * (4 * gg + qq) : 8 + 9 * (32 * (gg - 16) + lane);
-  if (D == 1) return e + 8 * (4 * gg + qq);
-  return e + 8 * (4 * (gg & 1) + qq) + 64 * (gg >> 1);
+  const int q = lane >> 3, e = lane & 7;
+  const int r = 8 * (gg >> 1) + (gg & 1) + 2 * q;
+  if (D == 0) return gg < 16 ? e + 9 * r : 8 + 9 * (32 * (gg - 16) + lane);
+  if (D == 1) return e + 8 * r;
+  return e + 8 * ((gg & 1) + 2 * q) + 64 * (gg >> 1);
 }
 
 // one face normal to D: limited face states from P, the face slots into fb
