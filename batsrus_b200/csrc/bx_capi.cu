@@ -337,6 +337,10 @@ void set_reschange(StageArgs &a) {
   const bool set = g.sch.BetaLimiterResChange > 0.0;
   a.betaRc = set ? g.sch.BetaLimiterResChange : 2.0;
   a.nFaceRc = set ? g.sch.nFaceLimiterResChange : 2;
+  const bool sharp = g.sch.nOrder > 1 && a.betaRc < g.sch.LimiterBeta;
+  bool anyFloat = false;
+  for (int q = 0; q < 6; q++) anyFloat = anyFloat || g.typeBc[q] == BX_BC_FLOAT;
+  a.anySpecial = g.nSlab > 0 || (sharp && anyFloat);
 }
 
 StageArgs stage_args(int iStage, bool computeDt) {

@@ -76,6 +76,10 @@ struct StageArgs {
   int tvdRc = 0;
   double betaRc = 2.0;
   int nFaceRc = 2;
+  // 0 when no block of the grid needs those resolution-change states (no
+  // resolution change, and no sharper limiter next to a float boundary):
+  // the stage kernel is then launched without that code
+  int anySpecial = 1;
 };
 
 constexpr int kNbrFloat = -1, kNbrResChange = -2;

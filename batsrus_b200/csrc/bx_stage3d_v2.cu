@@ -8,10 +8,10 @@ namespace bx {
 
 namespace {
 
-template <int NTHR, int MINB, typename TileT, typename Real, typename OutT, int FLUX, int LIM>
-cudaError_t launch8_lim(const TmaMaps &maps, const StageArgs &a, int nSM, cudaStream_t st) {
+template <int NTHR, int MINB, typename TileT, typename Real, typename OutT, int FLUX, int LIM, bool RC>
+cudaError_t launch8_rc(const TmaMaps &maps, const StageArgs &a, int nSM, cudaStream_t st) {
   using B = Blk8<TileT, Real, NTHR, MINB>;
-  auto k = stage8_kernel<B, TileT, Real, OutT, FLUX, LIM>;
+  auto k = stage8_kernel<B, TileT, Real, OutT, FLUX, LIM, RC>;
   constexpr size_t sm = B::smem_bytes;
   static bool attr = false;
   if (!attr) {
@@ -25,6 +25,13 @@ cudaError_t launch8_lim(const TmaMaps &maps, const StageArgs &a, int nSM, cudaSt
   const int grid = a.nBlock < want ? a.nBlock : want;
   k<<<grid, NTHR, sm, st>>>(maps, a);
   return cudaGetLastError();
+}
+
+// without the resolution-change face code where no block needs it
+template <int NTHR, int MINB, typename TileT, typename Real, typename OutT, int FLUX, int LIM>
+cudaError_t launch8_lim(const TmaMaps &maps, const StageArgs &a, int nSM, cudaStream_t st) {
+  if (a.anySpecial) return launch8_rc<NTHR, MINB, TileT, Real, OutT, FLUX, LIM, true>(maps, a, nSM, st);
+  return launch8_rc<NTHR, MINB, TileT, Real, OutT, FLUX, LIM, false>(maps, a, nSM, st);
 }
 
 template <int NTHR, int MINB, typename TileT, typename Real, typename OutT, int FLUX>

@@ -114,7 +114,7 @@ __device__ __forceinline__ int face_of_lane(int gg, int lane) {
 // the summed finer fluxes (apply_cons_flux).  False where hlld_flux stops.
 // special: bit s set where side s needs reschange_face_states (a coarser
 // neighbour with TVD faces, or the softer limiter of BetaLimiterResChange)
-template <int D, int FLUX, int LIM, typename Real>
+template <int D, int FLUX, int LIM, typename Real, bool RC>
 __device__ __forceinline__ bool face8(const StageArgs &a, const Real *__restrict__ P, Real *__restrict__ fb,
                                       int f, int rcFine, int rcCoarse, const int *rcSlab, const int *nbs, int special,
                                       Real beta, Real gamma, Real invGm1, Real area) {
@@ -171,7 +171,7 @@ __device__ __forceinline__ bool face8(const StageArgs &a, const Real *__restrict
     cbL = P[ad[1] + (kBx + D) * 1280]; cbR = P[ad[2] + (kBx + D) * 1280];
     cuL = P[ad[1] + (kUx + D) * 1280]; cuR = P[ad[2] + (kUx + D) * 1280];
   }
-  if ((special >> (2 * D)) & 3)
+  if (RC && ((special >> (2 * D)) & 3))
     reschange_face_states<8, D, LIM, Real>(a, n, D == 0 ? j : i, D == 2 ? j : k, nbs[2 * D], nbs[2 * D + 1], rcFine,
                                            first, L, R,
                                            [&](int v, int ci, int cj, int ck) { return P[p8(ci, cj, ck) + v * 1280]; });
@@ -233,7 +233,10 @@ __device__ __forceinline__ void issue_tile_nb(const TmaMaps &maps, TileT *buf, u
   if (nb[5] >= 0) tma_load_5d(buf + T::oZH, &maps.zh, bar, 0, 0, 0, 0, nb[5]);
 }
 
-template <class B, typename TileT, typename Real, typename OutT, int FLUX, int LIM>
+// RC = false: the launch's grid has no resolution change and no sharper
+// limiter at a float boundary (StageArgs::anySpecial = 0), so the code of
+// reschange_face_states is left out of the face phase
+template <class B, typename TileT, typename Real, typename OutT, int FLUX, int LIM, bool RC = true>
 __global__ void __launch_bounds__(B::NTHR, B::MINB)
     stage8_kernel(const __grid_constant__ TmaMaps maps, const StageArgs a) {
   using ST = typename B::ST;
@@ -353,13 +356,13 @@ __global__ void __launch_bounds__(B::NTHR, B::MINB)
       const int gg = gi - D * B::GPD;
       bool ok;
       if (D == 0)
-        ok = face8<0, FLUX, LIM, Real>(a, P, fb, face_of_lane<0>(gg, lane), rcFine, rcCoarse, M.rcSlab, M.nb, special, beta,
+        ok = face8<0, FLUX, LIM, Real, RC>(a, P, fb, face_of_lane<0>(gg, lane), rcFine, rcCoarse, M.rcSlab, M.nb, special, beta,
                                        gammaR, invGm1R, area0);
       else if (D == 1)
-        ok = face8<1, FLUX, LIM, Real>(a, P, fb, face_of_lane<1>(gg, lane), rcFine, rcCoarse, M.rcSlab, M.nb, special, beta,
+        ok = face8<1, FLUX, LIM, Real, RC>(a, P, fb, face_of_lane<1>(gg, lane), rcFine, rcCoarse, M.rcSlab, M.nb, special, beta,
                                        gammaR, invGm1R, area1);
       else
-        ok = face8<2, FLUX, LIM, Real>(a, P, fb, face_of_lane<2>(gg, lane), rcFine, rcCoarse, M.rcSlab, M.nb, special, beta,
+        ok = face8<2, FLUX, LIM, Real, RC>(a, P, fb, face_of_lane<2>(gg, lane), rcFine, rcCoarse, M.rcSlab, M.nb, special, beta,
                                        gammaR, invGm1R, area2);
       if (!ok) err = 1;
     }
