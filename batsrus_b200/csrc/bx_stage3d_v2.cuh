@@ -151,7 +151,7 @@ __device__ __forceinline__ bool face8(const StageArgs &a, const Real *__restrict
     }
   }
   const int side = n == 0 ? 2 * D : (n == 8 ? 2 * D + 1 : -1);
-  const bool first = a.nOrder == 1 || (!a.tvdRc && side >= 0 && ((rcFine >> side) & 1));
+  const bool first = a.nOrder == 1 || (RC && !a.tvdRc && side >= 0 && ((rcFine >> side) & 1));
   Real L[8], R[8], cbL = Real(0), cbR = Real(0), cuL = Real(0), cuR = Real(0);
   if (first) {  // first order: the cell values (one branch per face)
 #pragma unroll
@@ -177,7 +177,7 @@ __device__ __forceinline__ bool face8(const StageArgs &a, const Real *__restrict
                                            [&](int v, int ci, int cj, int ck) { return P[p8(ci, cj, ck) + v * 1280]; });
   Real *out = fb + D * 10 * 576 + f;
   const bool ok = face_slots<D, FLUX, Real>(L, R, gamma, invGm1, area, out, 576, cbL, cbR, cuL, cuR);
-  if (side >= 0 && ((rcCoarse >> side) & 1)) {
+  if (RC && side >= 0 && ((rcCoarse >> side) & 1)) {
     const int t0 = D == 0 ? j : i, t1 = D == 2 ? j : k;
     const double *cf = a.rcFlux + ((size_t)rcSlab[side] * 64 + t0 + 8 * t1) * kRcSlots;
 #pragma unroll
@@ -234,8 +234,9 @@ __device__ __forceinline__ void issue_tile_nb(const TmaMaps &maps, TileT *buf, u
 }
 
 // RC = false: the launch's grid has no resolution change and no sharper
-// limiter at a float boundary (StageArgs::anySpecial = 0), so the code of
-// reschange_face_states is left out of the face phase
+// limiter at a float boundary (StageArgs::anySpecial = 0), so the
+// resolution-change code (ghost slabs, reschange_face_states, the summed
+// finer fluxes) is left out
 template <class B, typename TileT, typename Real, typename OutT, int FLUX, int LIM, bool RC = true>
 __global__ void __launch_bounds__(B::NTHR, B::MINB)
     stage8_kernel(const __grid_constant__ TmaMaps maps, const StageArgs a) {
@@ -292,7 +293,7 @@ __global__ void __launch_bounds__(B::NTHR, B::MINB)
       int i, j, k, side;
       p8_cell(c, i, j, k, side);
       TileT w[8];
-      if (side >= 0 && ((rcMask >> side) & 1)) {
+      if (RC && side >= 0 && ((rcMask >> side) & 1)) {
         // ghost layers of a resolution-change side: its slab
         // [var][layer][t1][t0] (injection / restriction, bx_amr.cu)
         const int d = side >> 1, hi = side & 1;
