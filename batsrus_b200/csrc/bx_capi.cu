@@ -549,7 +549,6 @@ int compat_phase(int phase, int iBlock) {
   NEED_READY();
   if (g.nSlab) return fail(BX_ERR_ARG, "the per-block entry points work on single-level grids");
   if (iBlock < 1 || iBlock > g.nOwned) return fail(BX_ERR_ARG, "iBlock=%d out of range 1..%d", iBlock, g.nOwned);
-  if (g.sch.TypeFlux == BX_FLUX_ROE) return fail(BX_ERR_ARG, "the per-block entry points have no Roe flux");
   if (g.sch.BetaLimiterResChange > 0.0 && g.sch.BetaLimiterResChange < g.sch.LimiterBeta && g.sch.nOrder > 1 &&
       g.sch.nFaceLimiterResChange > 0)
     return fail(BX_ERR_ARG, "the per-block entry points have no BetaLimiterResChange below LimiterBeta");
@@ -628,8 +627,6 @@ int bx_init(const bx_grid_desc *gd, const bx_scheme_params *sp) {
   if (shape < 0)
     return fail(BX_ERR_ARG, "block size %dx%dx%d in %dD not supported", gd->nI, gd->nJ, gd->nK, gd->nDim);
   if (gd->nBlock < 1 || !gd->iLevelCoord_IB) return fail(BX_ERR_ARG, "empty block list");
-  if (sp->TypeFlux == BX_FLUX_ROE && shape != kShape888 && shape != kShape444)
-    return fail(BX_ERR_ARG, "the Roe flux is built for 3D blocks of 8^3 or 4^3 cells");
   if (gd->nOwned < 0 || gd->nOwned > gd->nBlock)
     return fail(BX_ERR_ARG, "nOwned=%d outside 0..nBlock=%d", gd->nOwned, gd->nBlock);
   g.shape = shape;

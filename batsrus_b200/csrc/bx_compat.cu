@@ -32,17 +32,46 @@ __global__ void compat_face_value(CompatArgs a, int b) {
     }
 }
 
-// calc_face_flux (src/ModFaceFlux.f90:483): 8 fluxes and Vdt per face
+// calc_face_flux (src/ModFaceFlux.f90:483): 8 fluxes and Vdt per face.
+// The Roe flux first gives each face state the normal field of its cell
+// (UseRS7, :600-625) in the face arrays themselves, as the reference does,
+// so calc_source sees the changed states; the cells' normal field and
+// velocity come from the block's primitive tile (ghost cells included).
 template <class S, int FLUX>
 __global__ void compat_face_flux(CompatArgs a, int b) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  double *tile = reinterpret_cast<double *>(smem_raw);
+  if (FLUX == kFluxRoe) {
+    int nb[6];
+    for (int q = 0; q < 6; q++) nb[q] = a.nbr[6 * b + q];
+    gather_tile<S, double, double>(a.state, nb, b, tile);
+    __syncthreads();
+  }
   const BlockGeom g = a.geom[b];
   const int nF[3] = {S::NFX, S::NFY, S::NFZ};
   for (int d = 0; d < S::NDIM; d++)
     for (int f = threadIdx.x; f < nF[d]; f += blockDim.x) {
       double L[8], R[8], F[8], vdt;
       for (int v = 0; v < 8; v++) { L[v] = a.left[d][8 * f + v]; R[v] = a.right[d][8 * f + v]; }
-      bool ok;
-      if (d == 0) ok = numerical_flux<0, FLUX>(L, R, a.gamma, a.invGm1, g.area[0], F, vdt);
+      bool ok = true;
+      if (FLUX == kFluxRoe) {
+        int i, j, k, st;
+        if (d == 0) { face_decode<S, 0>(f, i, j, k); st = 1; }
+        else if (d == 1) { face_decode<S, 1>(f, i, j, k); st = S::TX; }
+        else { face_decode<S, 2>(f, i, j, k); st = S::TX * S::TY; }
+        const int c = S::t(i, j, k);
+        const double cbL = tile[(kBx + d) * S::NT + c - st], cbR = tile[(kBx + d) * S::NT + c];
+        const double cuL = tile[(kUx + d) * S::NT + c - st], cuR = tile[(kUx + d) * S::NT + c];
+        const double dBnR = R[kBx + d] - cbR;
+        R[kBx + d] = R[kBx + d] - dBnR;
+        const double dBnL = L[kBx + d] - cbL;
+        L[kBx + d] = L[kBx + d] - dBnL;
+        a.left[d][8 * f + kBx + d] = L[kBx + d];
+        a.right[d][8 * f + kBx + d] = R[kBx + d];
+        if (d == 0) vdt = roe_flux<0>(L, R, cuL, cuR, dBnL, dBnR, a.gamma, a.invGm1, g.area[0], F, 1);
+        else if (d == 1) vdt = roe_flux<1>(L, R, cuL, cuR, dBnL, dBnR, a.gamma, a.invGm1, g.area[1], F, 1);
+        else vdt = roe_flux<2>(L, R, cuL, cuR, dBnL, dBnR, a.gamma, a.invGm1, g.area[2], F, 1);
+      } else if (d == 0) ok = numerical_flux<0, FLUX>(L, R, a.gamma, a.invGm1, g.area[0], F, vdt);
       else if (d == 1) ok = numerical_flux<1, FLUX>(L, R, a.gamma, a.invGm1, g.area[1], F, vdt);
       else ok = numerical_flux<2, FLUX>(L, R, a.gamma, a.invGm1, g.area[2], F, vdt);
       if (!ok) atomicOr(&a.ts->errFlag, kErrHlld);
@@ -180,7 +209,18 @@ static cudaError_t launch_phase(int phase, int b, const CompatArgs &a, cudaStrea
       compat_face_value<S><<<1, nt, sm, st>>>(a, b);
       break;
     }
-    case kPhaseFaceFlux: compat_face_flux<S, FLUX><<<1, nt, 0, st>>>(a, b); break;
+    case kPhaseFaceFlux: {
+      constexpr size_t sm = FLUX == kFluxRoe ? sizeof(double) * 8 * S::NT : 0;
+      static bool attr = false;
+      if (sm > 0 && !attr) {
+        cudaError_t e = cudaFuncSetAttribute(compat_face_flux<S, FLUX>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)sm);
+        if (e != cudaSuccess) return e;
+        attr = true;
+      }
+      compat_face_flux<S, FLUX><<<1, nt, sm, st>>>(a, b);
+      break;
+    }
     case kPhaseSource: compat_source<S><<<1, nt, 0, st>>>(a, b); break;
     case kPhaseUpdate: compat_update<S><<<1, nt, 0, st>>>(a, b); break;
     case kPhaseTimestep: compat_timestep<S><<<1, nt, 0, st>>>(a, b); break;
@@ -195,6 +235,7 @@ static cudaError_t launch_shape(int flux, int phase, int b, const CompatArgs &a,
     case kFluxRusanov: return launch_phase<S, kFluxRusanov>(phase, b, a, st);
     case kFluxLinde: return launch_phase<S, kFluxLinde>(phase, b, a, st);
     case kFluxHlld: return launch_phase<S, kFluxHlld>(phase, b, a, st);
+    case kFluxRoe: return launch_phase<S, kFluxRoe>(phase, b, a, st);
   }
   return cudaErrorInvalidValue;
 }

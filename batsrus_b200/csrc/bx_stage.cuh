@@ -168,9 +168,26 @@ __device__ __forceinline__ void sweep(const StageArgs &a, const BlockGeom &g, co
     face_decode<S, D>(f, i, j, k);
     Real L[8], R[8], F[8], vdt;
     face_states<S, D>(tile, i, j, k, a.nOrder, a.limiter, beta, L, R);
-    fbuf[9 * S::NFMAX + f] = L[kBx + D];
-    fbuf[10 * S::NFMAX + f] = R[kBx + D];
-    if (!numerical_flux<D, FLUX>(L, R, gamma, invGm1, area, F, vdt)) err = 1;
+    if (FLUX == kFluxRoe) {
+      // UseRS7 (src/ModFaceFlux.f90:600-625): each face state takes the
+      // normal field of its cell before the div B slots are formed; the
+      // Roe dissipation also uses the cells' normal velocities
+      constexpr int st = D == 0 ? 1 : (D == 1 ? S::TX : S::TX * S::TY);
+      const int c = S::t(i, j, k);
+      const Real cbL = tile[(kBx + D) * S::NT + c - st], cbR = tile[(kBx + D) * S::NT + c];
+      const Real cuL = tile[(kUx + D) * S::NT + c - st], cuR = tile[(kUx + D) * S::NT + c];
+      const Real dBnR = R[kBx + D] - cbR;
+      R[kBx + D] = R[kBx + D] - dBnR;
+      const Real dBnL = L[kBx + D] - cbL;
+      L[kBx + D] = L[kBx + D] - dBnL;
+      fbuf[9 * S::NFMAX + f] = L[kBx + D];
+      fbuf[10 * S::NFMAX + f] = R[kBx + D];
+      vdt = roe_flux<D>(L, R, cuL, cuR, dBnL, dBnR, gamma, invGm1, area, F, 1);
+    } else {
+      fbuf[9 * S::NFMAX + f] = L[kBx + D];
+      fbuf[10 * S::NFMAX + f] = R[kBx + D];
+      if (!numerical_flux<D, FLUX>(L, R, gamma, invGm1, area, F, vdt)) err = 1;
+    }
 #pragma unroll
     for (int v = 0; v < 8; v++) fbuf[v * S::NFMAX + f] = F[v];
     fbuf[8 * S::NFMAX + f] = vdt;

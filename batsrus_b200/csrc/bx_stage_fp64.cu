@@ -19,23 +19,28 @@ static cudaError_t launch_one(const StageArgs &a, cudaStream_t st) {
   return cudaGetLastError();
 }
 
-template <class S>
+// WITH_ROE: the Roe flux of 1D and 2D blocks (3D blocks have it in the
+// TMA stage kernels)
+template <class S, bool WITH_ROE>
 static cudaError_t launch_flux(int flux, const StageArgs &a, cudaStream_t st) {
   switch (flux) {
     case kFluxRusanov: return launch_one<S, kFluxRusanov>(a, st);
     case kFluxLinde: return launch_one<S, kFluxLinde>(a, st);
     case kFluxHlld: return launch_one<S, kFluxHlld>(a, st);
+    case kFluxRoe:
+      if constexpr (WITH_ROE) return launch_one<S, kFluxRoe>(a, st);
+      break;
   }
   return cudaErrorInvalidValue;
 }
 
 cudaError_t launch_stage_fp64(int shape, int flux, const StageArgs &a, cudaStream_t st) {
   switch (shape) {
-    case kShape888: return launch_flux<Shape<8, 8, 8>>(flux, a, st);
-    case kShape444: return launch_flux<Shape<4, 4, 4>>(flux, a, st);
-    case kShape881: return launch_flux<Shape<8, 8, 1>>(flux, a, st);
-    case kShape811: return launch_flux<Shape<8, 1, 1>>(flux, a, st);
-    case kShape6411: return launch_flux<Shape<64, 1, 1>>(flux, a, st);
+    case kShape888: return launch_flux<Shape<8, 8, 8>, false>(flux, a, st);
+    case kShape444: return launch_flux<Shape<4, 4, 4>, false>(flux, a, st);
+    case kShape881: return launch_flux<Shape<8, 8, 1>, true>(flux, a, st);
+    case kShape811: return launch_flux<Shape<8, 1, 1>, true>(flux, a, st);
+    case kShape6411: return launch_flux<Shape<64, 1, 1>, true>(flux, a, st);
   }
   return cudaErrorInvalidValue;
 }

@@ -46,7 +46,7 @@ enum {
 /* TypeFlux (src/ModFaceFlux.f90:396-417) */
 enum { BX_FLUX_RUSANOV = 0, BX_FLUX_LINDE = 1, BX_FLUX_HLLD = 2,
        /* 'Roe': roe_solver_new (src/ModFaceFlux.f90:2490) with the
-          7-wave solver of src/ModCharacteristic.f90; 3D blocks only */
+          7-wave solver of src/ModCharacteristic.f90 */
        BX_FLUX_ROE = 3 };
 /* TypeLimiter (src/ModFaceValue.f90:3689-3791) */
 enum { BX_LIM_MINMOD = 0, BX_LIM_MC = 1, BX_LIM_MC3 = 2 };
@@ -423,6 +423,12 @@ typedef struct {
                                   coefficients, scratch and arithmetic (the
                                   factorisation stays FP64; GMRES still solves
                                   the FP64 system to ErrorMax) */
+  int OperatorPrecision;       /* the face conduction tensor of the matrix-free
+                                  product inside the Krylov solve: BX_FP64, or
+                                  BX_FP32_BULK to store it in FP32 (products,
+                                  sums and inner products stay FP64; the
+                                  right-hand side and the BILU factorisation
+                                  use the FP64 tensor) */
 } bx_heat_params;
 
 /* init_mod_semi_impl (src/ModSemiImplicit.f90:110) and the state the solve

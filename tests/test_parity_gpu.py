@@ -14,8 +14,10 @@ import os
 import numpy as np
 import pytest
 
-from batsrus_b200 import configs
+from batsrus_b200 import configs, initial
 from batsrus_b200.explicit import ExplicitSolver
+from batsrus_b200.grid import BlockGrid
+from batsrus_b200.param import Scheme
 from oracle import Oracle
 
 pytestmark = pytest.mark.gpu
@@ -124,6 +126,45 @@ def test_gpu_brio_wu_to_time_limit():
     assert abs(x.time()[0] - tmax) < 1e-12 and abs(o.time()[0] - tmax) < 1e-12
 
 
+@pytest.mark.parametrize("nCellBlock,nBlock", [((8, 1, 1), 32), ((64, 1, 1), 4)])
+def test_gpu_roe_brio_wu_1d(nCellBlock, nBlock):
+    """Brio-Wu with the Roe flux (the flux of the reference's shock-tube
+    tests), MC beta 1.5, 2-stage, CFL 0.8, to t = 0.1 on blocks of 8 and 64
+    cells: within 1e-12 of the oracle at every step."""
+    g, s, st, run = configs.brio_wu_1d(nBlock)
+    if nCellBlock != (8, 1, 1):
+        g = BlockGrid.uniform(1, nCellBlock, (nBlock, 1, 1), (-0.5, -0.5, -0.5), (0.5, 0.5, 0.5), ("float",) * 6)
+        st = initial.shocktube(g, [1, 0, 0, 0, 0.75, 1, 0, 1], [0.125, 0, 0, 0, 0.75, -1, 0, 0.1])
+    s.typeFlux = "Roe"
+    o, x = make_pair(g, s, st)
+    tmax = run["tSimulationMax"]
+    isl = g.interior_slices()
+    n = 0
+    while o.time()[0] < tmax and n < 1000:
+        o.advance(1, tmax)
+        x.advance(1, tmax)
+        n += 1
+        assert rel_err(x.get_state()[isl], o.get_state()[isl]) < TOL_FP64, n
+    assert n > 20 and abs(x.time()[0] - tmax) < 1e-12
+
+
+@pytest.mark.parametrize("flux,limiter,beta", [("Roe", "mc3", 1.2), ("Linde", "mc", 1.5), ("HLLD", "minmod", 1.0)])
+def test_gpu_2d_blocks_match_oracle(flux, limiter, beta):
+    """2D blocks of 8x8 cells: Orszag-Tang on a periodic 4x4-block square with
+    the Powell source, five steps within 1e-12 of the oracle per step."""
+    g = BlockGrid.uniform(2, (8, 8, 1), (4, 4, 1), (0.0, 0.0, 0.0), (1.0, 1.0, 1.0), ("periodic",) * 6)
+    s = Scheme(nOrder=2, nStage=2, typeFlux=flux, typeLimiter=limiter, limiterBeta=beta, cfl=0.8,
+               gamma=5.0 / 3.0, useDivbSource=True, useHalfStep=True)
+    st = initial.orszag_tang_3d(g)
+    o, x = make_pair(g, s, st)
+    isl = g.interior_slices()
+    for step in range(5):
+        x.advance(1)
+        o.advance(1)
+        assert abs(x.time()[1] - o.time()[1]) <= 1e-14 * abs(o.time()[1]) + 1e-300, step
+        assert rel_err(x.get_state()[isl], o.get_state()[isl]) < TOL_FP64, step
+
+
 def test_gpu_download_fills_ghost_cells_like_exchange_messages():
     g, s, st, _ = configs.uniform_3d_case(2, "Linde", state="pert")
     o, x = make_pair(g, s, st)
@@ -135,7 +176,7 @@ def test_gpu_download_fills_ghost_cells_like_exchange_messages():
     assert rel_err(full_g.reshape(-1, 8), full_o.reshape(-1, 8)) < TOL_FP64
 
 
-@pytest.mark.parametrize("flux", ["Rusanov", "Linde", "HLLD"])
+@pytest.mark.parametrize("flux", ["Rusanov", "Linde", "HLLD", "Roe"])
 def test_gpu_per_block_orig_routines_match_oracle(flux):
     """calc_face_value / calc_face_flux / calc_source / update_state of the
     orig path, one block at a time, against the oracle's routines."""
