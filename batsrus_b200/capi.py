@@ -96,14 +96,14 @@ class HeatParamsC(ctypes.Structure):
         ("HeatCondPar", ctypes.c_double), ("FractionFieldAligned", ctypes.c_double), ("Cv", ctypes.c_double),
         ("Dt", ctypes.c_double), ("SemiImplCoeff", ctypes.c_double), ("nKrylovVector", ctypes.c_int),
         ("MaxMatvec", ctypes.c_int), ("ErrorMax", ctypes.c_double), ("TypePrecond", ctypes.c_int),
-        ("PrecondPrecision", ctypes.c_int),
+        ("PrecondPrecision", ctypes.c_int), ("OperatorPrecision", ctypes.c_int),
     ]
 
 
 def heat_params(p):
     return HeatParamsC(p.heatCondPar, p.fieldAligned, p.cv, p.dt, p.semiImplCoeff, p.nKrylovVector,
                        p.maxMatvec, p.errorMax, PRECOND[p.typePrecond.lower()],
-                       PRECISION[p.precondPrecision.lower()])
+                       PRECISION[p.precondPrecision.lower()], PRECISION[p.operatorPrecision.lower()])
 
 
 def implicit_params(p):

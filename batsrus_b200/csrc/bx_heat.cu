@@ -67,6 +67,8 @@ struct HeatCtx {
   int *blkAt = nullptr, *blkXYZ = nullptr;
   double *b = nullptr, *x = nullptr, *w = nullptr, *t = nullptr, *r = nullptr, *V = nullptr;
   double *K = nullptr;  // face conduction tensor [block][dim][dir][face]
+  float *K32 = nullptr; // the same in FP32 for the matrix-free product (op32)
+  bool op32 = false;    // OperatorPrecision = BX_FP32_BULK
   void *coef = nullptr;      // forward and backward sweep coefficients (double4 or float4), interleaved by 32 blocks
   void *yI = nullptr;        // forward-sweep scratch (double or float), interleaved
   bool ilu32 = false;        // FP32 coefficients, scratch and sweep arithmetic
@@ -165,8 +167,8 @@ __device__ __forceinline__ void face_tensor(const HeatArgs &a, const double *hc,
 // (get_face_gradient, src/ModFaceGradient.f90:933-1140, uniform Cartesian
 // grid; the flux of get_heat_conduction_rhs, src/ModHeatConduction.f90:
 // 1466-1477), stored at its x-fastest index in F
-template <int D>
-__device__ __forceinline__ void face_flux(const HeatArgs &a, const double *S, const double *Kd, double *F, int rk) {
+template <int D, typename KT>
+__device__ __forceinline__ void face_flux(const HeatArgs &a, const double *S, const KT *Kd, double *F, int rk) {
   constexpr int E1 = D == 0 ? 1 : 0, E2 = D == 2 ? 1 : 2;
   constexpr int O1 = E1 == 0 ? 1 : kTile, O2 = E2 == 1 ? kTile : kTile * kTile;
   const int an = rk / 64, u = rk % 8, v = (rk / 8) % 8;
@@ -182,7 +184,7 @@ __device__ __forceinline__ void face_flux(const HeatArgs &a, const double *S, co
   g[E2] = a.gA[E2] * (S[L - O2] + S[R - O2]) + a.gC[E2] * (S[L + O2] + S[R + O2]);
   double f = 0.0;
 #pragma unroll
-  for (int dir = 0; dir < 3; dir++) f = f + Kd[dir * kFacesDim + rk] * g[dir];
+  for (int dir = 0; dir < 3; dir++) f = f + (double)Kd[dir * kFacesDim + rk] * g[dir];
   const int rF = D == 0 ? an + 9 * (u + 8 * v) : (D == 1 ? u + 8 * (an + 9 * v) : u + 8 * (v + 8 * an));
   F[rF] = -f;
 }
@@ -218,19 +220,28 @@ __global__ void __launch_bounds__(512) k_heat_faces(HeatArgs a, const double *__
   }
 }
 
-// one CTA per block, 512 threads: the block's face tensor (41.5 KB,
-// contiguous) arrives by one bulk copy while the threads gather the 10^3
-// tile of the scalar; then each of the block's 3 x 576 face fluxes once, and
-// per cell Res = -sum (F+ - F-)/V (get_heat_conduction_rhs :1434-1545);
-// mode RHS writes b = V Res(Te), mode MATVEC y = V (x Cv/Dt - SemiImplCoeff
-// Res(x)) (semi_impl_matvec, src/ModSemiImplicit.f90:578-762)
-constexpr size_t kApplySmem = sizeof(double) * (kKBlock + kTile * kTile * kTile + 3 * kFacesDim);
+// one CTA per block, 512 threads: the block's face tensor (41.5 KB in
+// FP64, 20.7 KB in FP32, contiguous) arrives by one bulk copy while the
+// threads gather the 10^3 tile of the scalar; then each of the block's
+// 3 x 576 face fluxes once (FP64 products and sums), and per cell
+// Res = -sum (F+ - F-)/V (get_heat_conduction_rhs :1434-1545); mode RHS
+// writes b = V Res(Te), mode MATVEC y = V (x Cv/Dt - SemiImplCoeff Res(x))
+// (semi_impl_matvec, src/ModSemiImplicit.f90:578-762).  Shared memory per
+// CTA: 61.8 KB with the FP64 tensor (three CTAs per SM), 41.6 KB with the
+// FP32 one (four CTAs, the SM's 2048 threads).
+template <typename KT>
+constexpr size_t apply_smem() {
+  return sizeof(double) * (kTile * kTile * kTile + 3 * kFacesDim) + sizeof(KT) * kKBlock;
+}
 
+template <typename KT>
 __global__ void __launch_bounds__(512) k_heat_apply(HeatArgs a, const double *__restrict__ S,
-                                                    const double *__restrict__ K,
+                                                    const KT *__restrict__ K,
                                                     const unsigned char *__restrict__ used, double *out, int mode) {
   extern __shared__ __align__(128) double dsm[];
-  double *sK = dsm, *sS = sK + kKBlock, *sF = sS + kTile * kTile * kTile;
+  double *sS = dsm, *sF = sS + kTile * kTile * kTile;
+  KT *sK = reinterpret_cast<KT *>(sF + 3 * kFacesDim);
+  static_assert(sizeof(double) * (kTile * kTile * kTile + 3 * kFacesDim) % 16 == 0, "bulk copy destination alignment");
   __shared__ uint64_t bar;
   const int blk = blockIdx.x;
   if (threadIdx.x == 0) {
@@ -239,8 +250,8 @@ __global__ void __launch_bounds__(512) k_heat_apply(HeatArgs a, const double *__
   }
   __syncthreads();  // the barrier is initialised before any thread waits on it
   if (threadIdx.x == 0) {
-    mbar_arrive_expect_tx(&bar, sizeof(double) * kKBlock);
-    bulk_load(sK, K + (size_t)blk * kKBlock, sizeof(double) * kKBlock, &bar);
+    mbar_arrive_expect_tx(&bar, sizeof(KT) * kKBlock);
+    bulk_load(sK, K + (size_t)blk * kKBlock, sizeof(KT) * kKBlock, &bar);
   }
   for_tile(a, blk, [&](int q, long g) {
     double s = S[g];
@@ -642,7 +653,9 @@ void free_heat() {
     *p = nullptr;
   }
   if (H.K) cudaFree(H.K);
+  if (H.K32) cudaFree(H.K32);
   H.K = nullptr;
+  H.K32 = nullptr;
   for (double **p : {&H.V8, &H.Z8, &H.Zb}) {
     if (*p) cudaFree(*p);
     *p = nullptr;
@@ -670,8 +683,15 @@ int dotd(const double *x, const double *y, double *out, cudaStream_t st) {
   return BX_OK;
 }
 
+// the right-hand side always uses the FP64 tensor; the matrix-free product
+// of the Krylov solve the FP32 one when OperatorPrecision asks for it
+void apply_rhs(cudaStream_t st) {
+  k_heat_apply<double><<<H.nBlock, 512, apply_smem<double>(), st>>>(H.a, H.Te, H.K, H.used, H.b, kModeRhs);
+}
+
 int matvec(const double *x, double *y, cudaStream_t st) {
-  k_heat_apply<<<H.nBlock, 512, kApplySmem, st>>>(H.a, x, H.K, H.used, y, kModeMatvec);
+  if (H.op32) k_heat_apply<float><<<H.nBlock, 512, apply_smem<float>(), st>>>(H.a, x, H.K32, H.used, y, kModeMatvec);
+  else k_heat_apply<double><<<H.nBlock, 512, apply_smem<double>(), st>>>(H.a, x, H.K, H.used, y, kModeMatvec);
   CKH(cudaGetLastError());
   H.nMatvec++;
   return BX_OK;
@@ -932,10 +952,16 @@ int grid_tables(const Core &c, std::vector<int> &at, std::vector<int> &xyz) {
   return BX_OK;
 }
 
+__global__ void k_to_f32(const double *__restrict__ x, float *y, long n) {
+  for (long q = blockIdx.x * (long)blockDim.x + threadIdx.x; q < n; q += (long)gridDim.x * blockDim.x)
+    y[q] = (float)x[q];
+}
+
 // HeatCoef and the face tensor K from the current Te
 int update_coef(cudaStream_t st) {
   k_heat_coef<<<1184, 256, 0, st>>>(H.Te, H.HC, H.p.HeatCondPar, H.nCell);
   k_heat_faces<<<H.nBlock, 512, 0, st>>>(H.a, H.HC, H.B3, H.K);
+  if (H.op32) k_to_f32<<<1184, 256, 0, st>>>(H.K, H.K32, (long)kKBlock * H.nBlock);
   CKH(cudaGetLastError());
   return BX_OK;
 }
@@ -980,7 +1006,7 @@ int bx::tune_heat() {
   TuneKnobInfo &k = tune_knob(kTuneHeatIluWarps);
   if (!H.ready || H.p.TypePrecond != BX_PRECOND_BILU || k.tuned == 2) return BX_OK;
   Core c = core();
-  k_heat_apply<<<H.nBlock, 512, kApplySmem, c.st>>>(H.a, H.Te, H.K, H.used, H.b, kModeRhs);
+  apply_rhs(c.st);
   launch_factor(c.st);
   CKH(cudaGetLastError());
   cudaEvent_t e0 = H.ev[0], e1 = H.ev[1];
@@ -1018,8 +1044,11 @@ int bx_heat_init(const bx_heat_params *prm, const double *Te, const double *bhat
                      prm->TypePrecond);
   if (prm->PrecondPrecision != BX_FP64 && prm->PrecondPrecision != BX_FP32_BULK)
     return core_fail(BX_ERR_ARG, "PrecondPrecision=%d", prm->PrecondPrecision);
+  if (prm->OperatorPrecision != BX_FP64 && prm->OperatorPrecision != BX_FP32_BULK)
+    return core_fail(BX_ERR_ARG, "OperatorPrecision=%d", prm->OperatorPrecision);
   if (H.ready) free_heat();
   H.ilu32 = prm->PrecondPrecision == BX_FP32_BULK;
+  H.op32 = prm->OperatorPrecision == BX_FP32_BULK;
   std::vector<int> atH, xyzH;
   const int r0 = grid_tables(c, atH, xyzH);
   if (r0) return r0;
@@ -1050,6 +1079,7 @@ int bx_heat_init(const bx_heat_params *prm, const double *Te, const double *bhat
        cudaMalloc(&H.yI, (H.ilu32 ? sizeof(float) : sizeof(double)) * H.nIl) == cudaSuccess &&
        cudaMalloc(&H.usedM, sizeof(unsigned) * H.nGroup * kNC) == cudaSuccess &&
        cudaMalloc(&H.K, sizeof(double) * kKBlock * H.nBlock) == cudaSuccess &&
+       (!H.op32 || cudaMalloc(&H.K32, sizeof(float) * kKBlock * H.nBlock) == cudaSuccess) &&
        cudaMalloc(&H.wtab, sizeof(WaveTable)) == cudaSuccess && cudaMalloc(&H.cnt, sizeof(unsigned)) == cudaSuccess &&
        cudaMalloc(&H.errDev, sizeof(int)) == cudaSuccess &&
        cudaMalloc(&H.V, vb * (prm->nKrylovVector + 1)) == cudaSuccess &&
@@ -1076,7 +1106,10 @@ int bx_heat_init(const bx_heat_params *prm, const double *Te, const double *bhat
   CKH(cudaMemsetAsync(H.cnt, 0, sizeof(unsigned), c.st));
   CKH(cudaMemsetAsync(H.errDev, 0, sizeof(int), c.st));
   H.a.err = H.errDev;
-  CKH(cudaFuncSetAttribute(k_heat_apply, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kApplySmem));
+  CKH(cudaFuncSetAttribute(k_heat_apply<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)apply_smem<double>()));
+  CKH(cudaFuncSetAttribute(k_heat_apply<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)apply_smem<float>()));
   CKH(cudaMemsetAsync(H.coef, 0, 2 * (H.ilu32 ? sizeof(float4) : sizeof(double4)) * H.nIl, c.st));
   {
     std::vector<unsigned> um((size_t)H.nGroup * kNC, 0u);
@@ -1097,7 +1130,7 @@ int bx_advance_semi_impl(bx_krylov_stats *stats) {
   if (r) return r;
   Core c = core();
   CKH(cudaEventRecord(H.ev[0], c.st));
-  k_heat_apply<<<H.nBlock, 512, kApplySmem, c.st>>>(H.a, H.Te, H.K, H.used, H.b, kModeRhs);
+  apply_rhs(c.st);
   if (H.p.TypePrecond == BX_PRECOND_BILU) {
     launch_factor(c.st);
   }
@@ -1143,7 +1176,7 @@ int bx_heat_get_rhs(double *b) {
   if (r) return r;
   if (!b) return core_fail(BX_ERR_ARG, "null argument");
   Core c = core();
-  k_heat_apply<<<H.nBlock, 512, kApplySmem, c.st>>>(H.a, H.Te, H.K, H.used, H.b, kModeRhs);
+  apply_rhs(c.st);
   CKH(cudaGetLastError());
   return copy_out(b, H.b);
 }

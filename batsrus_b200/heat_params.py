@@ -30,6 +30,7 @@ class HeatParams:
     errorMax: float = 1e-6
     typePrecond: str = "BILU"         # BILU | NONE | LEARNED (#SEMIPRECOND)
     precondPrecision: str = "fp64"    # BILU sweeps: fp64 | fp32 (FP32 coefficients and arithmetic)
+    operatorPrecision: str = "fp64"   # face tensor of the Krylov matvec: fp64 | fp32 (FP64 arithmetic)
 
 
 def heat_dipole(nRoot=32, seed=2024, sigma=0.3, rExcl=0.2):

@@ -64,7 +64,7 @@ module bx200_interface
      real(c_double):: HeatCondPar, FractionFieldAligned, Cv, Dt, SemiImplCoeff
      integer(c_int):: nKrylovVector, MaxMatvec
      real(c_double):: ErrorMax
-     integer(c_int):: TypePrecond, PrecondPrecision
+     integer(c_int):: TypePrecond, PrecondPrecision, OperatorPrecision
   end type bx_heat_params
 
   type, bind(C):: bx_scheme_params

@@ -119,6 +119,37 @@ def test_fp32_sweeps_solve_the_fp64_system():
     close(x, o)
 
 
+def test_fp32_operator_tensor_solves_to_the_krylov_tolerance():
+    """The face tensor of the Krylov matvec stored in FP32 (FP64 products,
+    sums and inner products; the right-hand side and the BILU factors from
+    the FP64 tensor): the matvec within 1e-6 of the oracle's maximum (FP32
+    rounding of the tensor entries, 6e-8 relative each), the matrix-vector
+    count within two of the oracle's, the solution's residual on the FP64
+    system at most 2e-6 of the preconditioned right-hand side, and the
+    temperature within 1e-6 of the update, with FP64 and FP32 sweeps."""
+    for ilu in ("fp64", "fp32"):
+        x, h, o, tb, tg, (Te, _, used) = setup(nRoot=3, seed=5, precondPrecision=ilu, operatorPrecision="fp32")
+        v = np.random.default_rng(1).normal(size=Te.size)
+        ref = o.matvec(v)
+        got = tg(h.matvec(tb(v)))
+        assert np.abs(got - ref).max() <= 1e-6 * np.abs(ref).max()
+        assert np.abs(got - ref).max() > 0  # the FP32 tensor is the one used
+        b = o.rhs()
+        assert np.abs(tg(h.rhs()) - b).max() <= 1e-12 * np.abs(b).max()
+        Mb = o.precond(b)
+        s = h.advance_semi_impl()
+        te = tg(h.te())
+        res = o.precond(b - o.matvec(np.where(used == 1, te - Te, 0.0)))
+        assert np.linalg.norm(res) <= 2e-6 * np.linalg.norm(Mb)
+        r, xo, nm, err = o.solve()
+        assert r == 0 and s["iError"] == 0
+        assert abs(s["nMatvec"] - nm) <= 2, (s["nMatvec"], nm)
+        dT = np.abs(o.te() - Te).max()
+        assert np.abs(te - o.te()).max() <= 1e-6 * dT
+        assert np.array_equal(te[used == 0], Te[used == 0])
+        close(x, o)
+
+
 def test_maxmatvec_reached_is_an_error():
     x, h, o, *_ = setup(typePrecond="NONE", maxMatvec=3, errorMax=1e-12)
     with pytest.raises(capi.BxError) as e:
