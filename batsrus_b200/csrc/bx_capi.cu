@@ -864,23 +864,27 @@ int bx_upload_state(const double *State_VGB, int nBlock) {
   if (!State_VGB || nBlock != g.nBlock) return fail(BX_ERR_ARG, "nBlock=%d, expected %d", nBlock, g.nBlock);
   int nIg, nJg, nKg, gi, gj, gk;
   ghost_extent(nIg, nJg, nKg, gi, gj, gk);
-  // only the x runs of the interior rows cross the bus (one strided copy):
-  // the ghost cells of State_VGB are rebuilt on the device before every
-  // stage, so rows 1..nJ of every plane, cells 1..nI of a row, are all the
-  // state there is; k ghost planes come along because the plane stride is
-  // uniform only over all planes
+  // only the interior cells cross the bus, as the x runs of the interior
+  // rows: the ghost cells of State_VGB are rebuilt on the device before
+  // every stage.  One strided copy per interior plane k moves plane k of
+  // every block (the source slice is one block of State_VGB, the staging
+  // buffer holds [block][k][j][i] with nI x nJ x nK cells per block).
   const size_t row = sizeof(double) * 8 * (size_t)g.nI;
-  const size_t bytes = row * g.nJ * nKg * g.nBlock;
+  const size_t bytes = row * g.nJ * g.nK * g.nBlock;
   int r = ensure_stage_aos(bytes);
   if (r) return r;
-  cudaMemcpy3DParms cp = {};
-  cp.srcPtr = make_cudaPitchedPtr(const_cast<double *>(State_VGB) + 8 * (gi + (size_t)nIg * gj),
-                                  sizeof(double) * 8 * (size_t)nIg, sizeof(double) * 8 * (size_t)nIg, nJg);
-  cp.dstPtr = make_cudaPitchedPtr(g.stageAoS, row, row, g.nJ);
-  cp.extent = make_cudaExtent(row, g.nJ, (size_t)nKg * g.nBlock);
-  cp.kind = cudaMemcpyHostToDevice;
-  CK(cudaMemcpy3DAsync(&cp, g.st));
-  aos_to_soa<<<1184, 256, 0, g.st>>>(g.stageAoS, g.A, g.nBlock, g.nI, g.nJ, g.nK, g.nI, g.nJ, nKg, 0, 0, gk);
+  for (int k = 0; k < g.nK; k++) {
+    cudaMemcpy3DParms cp = {};
+    cp.srcPtr = make_cudaPitchedPtr(const_cast<double *>(State_VGB) + 8 * (gi + (size_t)nIg * (gj + (size_t)nJg * (gk + k))),
+                                    sizeof(double) * 8 * (size_t)nIg, sizeof(double) * 8 * (size_t)nIg,
+                                    (size_t)nJg * nKg);
+    cp.dstPtr = make_cudaPitchedPtr(reinterpret_cast<char *>(g.stageAoS) + row * g.nJ * k, row, row,
+                                    (size_t)g.nJ * g.nK);
+    cp.extent = make_cudaExtent(row, g.nJ, g.nBlock);
+    cp.kind = cudaMemcpyHostToDevice;
+    CK(cudaMemcpy3DAsync(&cp, g.st));
+  }
+  aos_to_soa<<<1184, 256, 0, g.st>>>(g.stageAoS, g.A, g.nBlock, g.nI, g.nJ, g.nK, g.nI, g.nJ, g.nK, 0, 0, 0);
   CK(cudaGetLastError());
   if (g.Nx) {
     const size_t sb = sizeof(double) * 8 * g.nCell * g.nBlock;

@@ -216,11 +216,11 @@ def run_ours(args):
             timed_e2e()
             evalue, ems = replica_rate(timed_e2e, nCell * args.steps, world)
             # bx_download_state returns all of State_VGB, ghost cells included;
-            # bx_upload_state moves the interior x runs of the interior rows of
-            # every plane (one strided copy: nI x nJ of nIg x nJg cells per plane)
+            # bx_upload_state moves the interior cells only (strided copies of
+            # the interior x runs: nI x nJ x nK of nIg x nJg x nKg per block)
             sh = g.state_shape_fortran()  # (8, nIg, nJg, nKg, nBlock)
             d2h = host.numel() * 8
-            h2d = d2h * (g.nI * g.nJ) // (sh[1] * sh[2])
+            h2d = d2h * (g.nI * g.nJ * g.nK) // (sh[1] * sh[2] * sh[3])
             res["e2e"] = {"value": evalue, "unit": UNIT,
                           "h2d_bytes_per_step": h2d / args.steps, "d2h_bytes_per_step": d2h / args.steps,
                           "ms": ems}
@@ -601,6 +601,11 @@ def cpu_baseline(args, seconds=12.0):
 
 
 def run_reference(args):
+    """The reference arm: the oracle (C++ restatement of the orig path,
+    OpenMP over blocks, all host threads) on the bench's own workload, the
+    full Orszag-Tang domain of --nroot^3 blocks (256^3 by default: about 2 s
+    per step on 16 threads, 11 GB of host memory), W untimed steps after the
+    Dt = 0 step, then K timed steps."""
     rank, world, _ = dist_env()
     if rank != 0:
         return
@@ -608,26 +613,29 @@ def run_reference(args):
     from batsrus_b200 import configs
     from oracle import Oracle
     cores = os.cpu_count()
-    g, s, st, _ = configs.orszag_tang_3d(nRoot=8, flux=args.flux)
+    g, s, st, _ = configs.orszag_tang_3d(nRoot=args.nroot, flux=args.flux)
     o = Oracle(g, s, n_thread=cores)
     o.set_state(st)
+    del st
     o.exchange_messages()
     o.advance(1 + args.warmup)
     t0 = time.perf_counter()
     o.advance(args.steps)
     el = time.perf_counter() - t0
     v = g.nCell * args.steps / el
+    n = 8 * args.nroot
     line = {"metric": METRIC, "value": v, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": el * 1e3 / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "impl": "reference",
-            "config": {"workload": WORKLOAD if args.flux == "Linde" else
-                       "orszag_tang_3d_256cubed_%s_koren" % args.flux.lower(),
-                       "sample": "64^3 of the 256^3 domain per step",
-                       "blocks": "8x8x8", "flux": "Linde", "limiter": "mc3 beta=1.2", "cfl": 0.8},
+            "config": {"workload": (WORKLOAD if args.flux == "Linde" else
+                                    "orszag_tang_3d_256cubed_%s_koren" % args.flux.lower())
+                       if args.nroot == 32 else "orszag_tang_3d_%dcubed_%s_koren" % (n, args.flux.lower()),
+                       "cells": g.nCell, "blocks": g.nBlock, "block_cells": "8x8x8", "flux": args.flux,
+                       "limiter": "mc3 beta=1.2", "cfl": 0.8, "stages": 2},
             "cpu_baseline": {"value": v, "unit": UNIT, "cores": cores, "kind": "port",
-                             "sample": "oracle/ C++ restatement of the orig path, 64^3 Orszag-Tang, "
-                                       "%d steps, %d threads" % (args.steps, cores)},
+                             "sample": "oracle/ C++ restatement of the orig path, the whole %d^3 Orszag-Tang "
+                                       "domain, %d steps, %d threads" % (n, args.steps, cores)},
             "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line))
 
