@@ -56,9 +56,9 @@ def peaks():
 #       --no-amr --jfnk-precond= --heat-precond= --no-autotune
 #   ncu --metrics gpu__time_duration.sum,dram__bytes_read.sum,dram__bytes_write.sum \
 #       --clock-control none -k regex:stage8 -s 2 -c 2 --csv <same command>
-# FP64: 136.2 and 199.9 B; FP32-bulk: 110.0 and 158.8 B.  Traffic grows in
+# FP64: 135.8 and 200.1 B; FP32-bulk: 111.8 and 159.0 B.  Traffic grows in
 # proportion to the blocks, so the bench scales it by the cells of its grid.
-DRAM_BYTES_PER_CELL_LAUNCH = {"fp64": 168.0, "fp32": 134.4}
+DRAM_BYTES_PER_CELL_LAUNCH = {"fp64": 168.0, "fp32": 135.4}
 
 
 def profile_traffic(prec):
