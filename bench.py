@@ -304,6 +304,7 @@ def run_jfnk(args, lrank):
             continue
         out[prec.lower()] = {
             "s_per_step": ms * 1e-3 / args.jfnk_steps,
+            "s_per_step_per_mcell": ms * 1e-3 / args.jfnk_steps / (g.nCell / 1e6),
             "matvec_per_step": float(np.mean([q["nMatvec"] for q in stats])),
             "matvec": [q["nMatvec"] for q in stats],
             "krylov_error": [q["Error"] for q in stats],
@@ -480,8 +481,10 @@ def run_heat(args, lrank):
             if x is not None:
                 x.close()
             continue
+        nmv = float(np.mean([q["nMatvec"] for q in stats]))
         out[prec.lower()] = {"s_per_solve": ms * 1e-3 / args.heat_steps,
-                             "matvec_per_solve": float(np.mean([q["nMatvec"] for q in stats])),
+                             "matvec_per_solve": nmv,
+                             "s_per_matvec_per_mcell": ms * 1e-3 / args.heat_steps / nmv / (g.nCell / 1e6),
                              "matvec": [q["nMatvec"] for q in stats],
                              "krylov_error": [q["Error"] for q in stats],
                              "criterion": ("true residual (flexible GMRES)" if prec.upper() in ("LEARNED", "NONE")
@@ -547,8 +550,11 @@ def cpu_baseline_heat(args, seconds=20.0):
     o.close()
     return {"value": el / n, "unit": "s/solve", "cores": os.cpu_count(), "kind": "port",
             "matvec_per_solve": nm / n,
+            "cells": (8 * nR) ** 3,
+            "s_per_matvec_per_mcell": el / nm / ((8 * nR) ** 3 / 1e6),
             "sample": "oracle/ C++ restatement of advance_semi_impl with BILU, 64^3 (512 blocks) of the "
-                      "dipole workload, %d solves (residual on all threads, Krylov and ILU on one)" % n}
+                      "dipole workload, %d solves (residual, block ILU and vector updates on all threads, "
+                      "inner products on one)" % n}
 
 
 def cpu_baseline_jfnk(args, seconds=20.0):
@@ -571,7 +577,7 @@ def cpu_baseline_jfnk(args, seconds=20.0):
         if el > seconds or n >= 10:
             break
     return {"value": el / n, "unit": "s/step", "cores": cores, "kind": "port",
-            "matvec_per_step": nm / n,
+            "matvec_per_step": nm / n, "cells": g.nCell, "s_per_step_per_mcell": el / n / (g.nCell / 1e6),
             "sample": "oracle/ C++ restatement of advance_part_impl with BILU, 32^3 (64 blocks) of the "
                       "perturbed Orszag-Tang workload, %d steps on %d threads" % (n, cores)}
 
@@ -758,6 +764,9 @@ def summary(line):
                     out["jfnk_learned_over_%s" % k] = r(sp["learned"] / sp[k])
         if "cpu_baseline" in j:
             out["jfnk_cpu_s_per_step"] = r(j["cpu_baseline"]["value"])
+            if "bilu" in sp:  # per cell: the CPU sample is 32^3, the GPU workload 128^3
+                out["jfnk_cpu_over_gpu_bilu_per_cell"] = r(j["cpu_baseline"]["s_per_step_per_mcell"] /
+                                                           j["bilu"]["s_per_step_per_mcell"])
     a = line.get("amr")
     if a:
         out["amr"] = {"blocks": a["blocks"], "cells": a["cells"], "fp32": r(a["fp32"]["value"]),
@@ -772,6 +781,9 @@ def summary(line):
         out["heat_matvec_per_solve"] = {k: r(h[k]["matvec_per_solve"]) for k in sp}
         if "cpu_baseline" in h:
             out["heat_cpu_s_per_solve"] = r(h["cpu_baseline"]["value"])
+            if "bilu" in sp:  # per matrix-vector product and cell: the CPU sample is 64^3
+                out["heat_cpu_over_gpu_bilu_per_matvec_cell"] = r(h["cpu_baseline"]["s_per_matvec_per_mcell"] /
+                                                                  h["bilu"]["s_per_matvec_per_mcell"])
     if "cpu_baseline" in line:
         out["cpu"] = r(line["cpu_baseline"]["value"])
     return out

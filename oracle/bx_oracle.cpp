@@ -2237,6 +2237,7 @@ struct Heat {
     for (long q = 0; q < nCell(); q++)
       if (!used[q]) S[q] = 0.0;
     residual(S, Res);
+#pragma omp parallel for schedule(static)
     for (long q = 0; q < nCell(); q++)
       y[q] = used[q] ? V * (S[q] * c.cv / c.dt - c.semiImplCoeff * Res[q]) : V * (x[q] * c.cv / c.dt);
   }
@@ -2245,6 +2246,7 @@ struct Heat {
   // -x, +x, -y, +y, -z, +z; diag in off[7*q]
   void jacobian() {
     off.assign(7 * nCell(), 0.0);
+#pragma omp parallel for schedule(static)
     for (int k = 0; k < n[2]; k++)
       for (int j = 0; j < n[1]; j++)
         for (int i = 0; i < n[0]; i++) {
@@ -2281,20 +2283,28 @@ struct Heat {
   void bilu_factor() {
     jacobian();
     dIlu.assign(nCell(), 0.0);
-    // natural order inside each block: lower neighbours are -x, -y, -z
-    for (int k = 0; k < n[2]; k++)
-      for (int j = 0; j < n[1]; j++)
-        for (int i = 0; i < n[0]; i++) {
-          const long q = id(i, j, k);
-          double d = off[7 * q];
-          if (used[q])
-            for (int s = 1; s <= 5; s += 2) {
-              const long m = nb_in_block(i, j, k, s);
-              if (m < 0) continue;
-              d = d - off[7 * q + s] * off[7 * m + s + 1] / dIlu[m];
-            }
-          dIlu[q] = d;
-        }
+    // natural order inside each block: lower neighbours are -x, -y, -z.
+    // Blocks are independent (couplings across block faces are dropped), so
+    // they run in parallel, each cell with the same operations as in one
+    // sweep over the domain in natural order
+    const int nb[3] = {(n[0] + nB - 1) / nB, (n[1] + nB - 1) / nB, (n[2] + nB - 1) / nB};
+#pragma omp parallel for schedule(static) collapse(3)
+    for (int bk = 0; bk < nb[2]; bk++)
+      for (int bj = 0; bj < nb[1]; bj++)
+        for (int bi = 0; bi < nb[0]; bi++)
+          for (int k = bk * nB; k < std::min((bk + 1) * nB, n[2]); k++)
+            for (int j = bj * nB; j < std::min((bj + 1) * nB, n[1]); j++)
+              for (int i = bi * nB; i < std::min((bi + 1) * nB, n[0]); i++) {
+                const long q = id(i, j, k);
+                double d = off[7 * q];
+                if (used[q])
+                  for (int s = 1; s <= 5; s += 2) {
+                    const long m = nb_in_block(i, j, k, s);
+                    if (m < 0) continue;
+                    d = d - off[7 * q + s] * off[7 * m + s + 1] / dIlu[m];
+                  }
+                dIlu[q] = d;
+              }
   }
   void precond(const double *r, double *z) const {
     if (c.typePrecond == 0) {
@@ -2302,29 +2312,40 @@ struct Heat {
       return;
     }
     std::vector<double> y(nCell());
-    for (int k = 0; k < n[2]; k++)
-      for (int j = 0; j < n[1]; j++)
-        for (int i = 0; i < n[0]; i++) {
-          const long q = id(i, j, k);
-          double s = r[q];
-          if (used[q])
-            for (int t = 1; t <= 5; t += 2) {
-              const long m = nb_in_block(i, j, k, t);
-              if (m >= 0) s = s - off[7 * q + t] * y[m];
-            }
-          y[q] = s / dIlu[q];
-        }
-    for (int k = n[2] - 1; k >= 0; k--)
-      for (int j = n[1] - 1; j >= 0; j--)
-        for (int i = n[0] - 1; i >= 0; i--) {
-          const long q = id(i, j, k);
-          double s = 0.0;
-          if (used[q])
-            for (int t = 2; t <= 6; t += 2) {
-              const long m = nb_in_block(i, j, k, t);
-              if (m >= 0) s = s + off[7 * q + t] * z[m];
-            }
-          z[q] = y[q] - s / dIlu[q];
+    // forward then backward sweep of each block; blocks in parallel (the
+    // sweeps never leave a block)
+    const int nb[3] = {(n[0] + nB - 1) / nB, (n[1] + nB - 1) / nB, (n[2] + nB - 1) / nB};
+#pragma omp parallel for schedule(static) collapse(3)
+    for (int bk = 0; bk < nb[2]; bk++)
+      for (int bj = 0; bj < nb[1]; bj++)
+        for (int bi = 0; bi < nb[0]; bi++) {
+          const int k0 = bk * nB, k1 = std::min(k0 + nB, n[2]);
+          const int j0 = bj * nB, j1 = std::min(j0 + nB, n[1]);
+          const int i0 = bi * nB, i1 = std::min(i0 + nB, n[0]);
+          for (int k = k0; k < k1; k++)
+            for (int j = j0; j < j1; j++)
+              for (int i = i0; i < i1; i++) {
+                const long q = id(i, j, k);
+                double s = r[q];
+                if (used[q])
+                  for (int t = 1; t <= 5; t += 2) {
+                    const long m = nb_in_block(i, j, k, t);
+                    if (m >= 0) s = s - off[7 * q + t] * y[m];
+                  }
+                y[q] = s / dIlu[q];
+              }
+          for (int k = k1 - 1; k >= k0; k--)
+            for (int j = j1 - 1; j >= j0; j--)
+              for (int i = i1 - 1; i >= i0; i--) {
+                const long q = id(i, j, k);
+                double s = 0.0;
+                if (used[q])
+                  for (int t = 2; t <= 6; t += 2) {
+                    const long m = nb_in_block(i, j, k, t);
+                    if (m >= 0) s = s + off[7 * q + t] * z[m];
+                  }
+                z[q] = y[q] - s / dIlu[q];
+              }
         }
   }
 
@@ -2363,6 +2384,7 @@ struct Heat {
         for (int q = 0; q <= k; q++) {
           const double h = dot(w, Vb[q]);
           H[q * m + k] = h;
+#pragma omp parallel for schedule(static)
           for (long p = 0; p < N; p++) w[p] = w[p] - h * Vb[q][p];
         }
         const double hn = std::sqrt(dot(w, w));
@@ -2395,6 +2417,7 @@ struct Heat {
         y[q] = s / H[q * m + q];
       }
       for (int q = 0; q < kdone; q++)
+#pragma omp parallel for schedule(static)
         for (long p = 0; p < N; p++) x[p] = x[p] + y[q] * Vb[q][p];
       if (conv) break;
       if (nMatvec >= c.maxMatvec) { std::copy(x.begin(), x.end(), xOut); return 1; }
