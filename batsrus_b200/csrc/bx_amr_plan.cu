@@ -163,7 +163,6 @@ struct Tree {
 int amr_plan(const bx_grid_desc *gd, const bx_amr_params *p, const double *Crit_IB, std::vector<int> &lcNew,
              std::vector<int> &remap, bool &changed) {
   const int nB = gd->nBlock, nC = p->nCrit;
-  Tree t(gd);
   std::vector<uint64_t> keys(nB);
   for (int b = 0; b < nB; b++) {
     const int *q = gd->iLevelCoord_IB + 4 * b;
@@ -185,6 +184,35 @@ int amr_plan(const bx_grid_desc *gd, const bx_amr_params *p, const double *Crit_
     wantCoa[b] = allCoa && lv > p->MinBlockLevel && lv < p->MaxBlockLevel && !wantRef[b];
     ratio[b] = r;
   }
+  // no block asks to refine or coarsen: the leaves stay, and when the old
+  // list already follows the Morton order of the finest level (every list
+  // this planner made does) the new grid is the old one, block for block
+  if (std::none_of(wantRef.begin(), wantRef.end(), [](char w) { return w != 0; }) &&
+      std::none_of(wantCoa.begin(), wantCoa.end(), [](char w) { return w != 0; })) {
+    int mx = 0;
+    for (int b = 0; b < nB; b++) mx = std::max(mx, gd->iLevelCoord_IB[4 * b]);
+    bool inOrder = true;
+    std::pair<uint64_t, int> prev{0, 0};
+    for (int b = 0; b < nB && inOrder; b++) {
+      const int *q = gd->iLevelCoord_IB + 4 * b;
+      const int sh = mx - q[0];
+      const std::pair<uint64_t, int> cur{morton((uint32_t)q[1] << sh, (uint32_t)q[2] << sh, (uint32_t)q[3] << sh),
+                                         q[0]};
+      inOrder = b == 0 || prev < cur;
+      prev = cur;
+    }
+    if (inOrder) {
+      lcNew.assign(gd->iLevelCoord_IB, gd->iLevelCoord_IB + 4 * (size_t)nB);
+      remap.assign((size_t)kRemapInts * nB, 0);
+      for (int b = 0; b < nB; b++) {
+        remap[(size_t)kRemapInts * b] = kRemapCopy;
+        remap[(size_t)kRemapInts * b + 1] = b + 1;
+      }
+      changed = false;
+      return BX_OK;
+    }
+  }
+  Tree t(gd);
   std::vector<int> cand;
   for (int b = 0; b < nB; b++)
     if (wantRef[b]) cand.push_back(b);

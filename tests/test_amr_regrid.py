@@ -215,3 +215,25 @@ def test_native_plan_matches_restatement(nRoot, maxLevel):
         a2, b2 = amr.regrid(a[0], c2, p2), amr.plan_native(a[0], c2, p2)
         assert np.array_equal(a2[0].iLevelCoord, b2[0].iLevelCoord) and np.array_equal(a2[1], b2[1])
     assert seen == {amr.COPY, amr.PROLONG, amr.RESTRICT}
+
+
+@pytest.mark.parametrize("order", ["morton", "x"])
+def test_native_plan_without_requests_keeps_or_reorders_the_grid(order):
+    """No block asks to refine or coarsen: on a grid in the planner's own
+    order (levels-mixed Morton of the finest level) bx_amr_plan returns the
+    grid unchanged with copies in place, without rebuilding the tree; on a
+    grid in another order it reorders, as the Python restatement does."""
+    g = configs.amr_blast(nRoot=3, maxLevel=2, with_state=False)[0]
+    p = params(coarsen=0.2, refine=1.0)
+    g = amr.plan_native(g, np.full((g.nBlock, 1), 0.5), p)[0]  # the planner's order
+    if order == "x":
+        perm = np.random.default_rng(3).permutation(g.nBlock)
+        g = BlockGrid(g.nDim, g.nI, g.nJ, g.nK, g.nRoot, g.xyzMin, g.xyzMax, g.typeBc, g.iLevelCoord[perm].copy())
+    c = np.full((g.nBlock, 1), 0.5)  # between the coarsen and refine limits
+    a, b = amr.regrid(g, c, p), amr.plan_native(g, c, p)
+    assert np.array_equal(a[0].iLevelCoord, b[0].iLevelCoord) and np.array_equal(a[1], b[1]) and a[2] == b[2]
+    if order == "morton":
+        assert not b[2] and np.array_equal(b[0].iLevelCoord, g.iLevelCoord)
+        assert (b[1][:, 0] == amr.COPY).all() and np.array_equal(b[1][:, 1], np.arange(1, g.nBlock + 1))
+    else:
+        assert b[2]
