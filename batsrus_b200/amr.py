@@ -25,7 +25,7 @@ Documented behaviour followed here (PARAM.XML:6658-6910, ``#AMRLEVELS``,
 
 The criteria themselves are computed on the GPU (``bx_amr_criteria``): the
 maximum over a block's cells of ``gradt``, ``gradlogrho``, ``gradlogp``,
-``gradp`` or ``pjumpratio`` (src/ModAMR.f90:388-723), in normalised units
+``gradp``, ``pjumpratio`` or ``-divu`` (src/ModAMR.f90:388-723), in normalised units
 (the reference multiplies some by No2Io_V, which is 1 for normalised I/O
 units).
 """

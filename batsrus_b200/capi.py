@@ -45,7 +45,7 @@ EXPORTS = (
     "bx_halo_bytes", "bx_halo_pack", "bx_halo_unpack", "bx_get_dtmin", "bx_set_dtmin", "bx_end_step",
 )
 # #AMRCRITERIA TypeRefine -> BX_AMR_*
-AMR_CRIT = {"gradt": 1, "gradlogrho": 2, "gradlogp": 3, "gradp": 4, "pjumpratio": 5}
+AMR_CRIT = {"gradt": 1, "gradlogrho": 2, "gradlogp": 3, "gradp": 4, "pjumpratio": 5, "-divu": 6, "-divudx": 6}
 PRECOND = {"none": 0, "bilu": 1, "learned": 2}
 NOALLOC_MAX_BLOCK = 32768  # BX_NOALLOC_MAX_BLOCK
 

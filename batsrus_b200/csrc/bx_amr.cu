@@ -273,8 +273,11 @@ __global__ void __launch_bounds__(N * N * N) k_amr_crit(AmrCritArgs a) {
   const int ijk[3] = {c % N, (c / N) % N, c / (N * N)};
   const int nr[3] = {a.nRoot.x, a.nRoot.y, a.nRoot.z};
   const BlockGeom g = a.geom[b];
-  // rho and p of the cell (0) and of its neighbours: 1 + 2 d + side
-  double rho[7], p[7];
+  // rho and p of the cell (0) and of its neighbours: 1 + 2 d + side; with
+  // the -divu criterion also the neighbours' momentum along their direction
+  bool needDivU = false;
+  for (int q = 0; q < a.nCrit; q++) needDivU = needDivU || a.type[q] == kAmrMinusDivU;
+  double rho[7], p[7], ru[7] = {0, 0, 0, 0, 0, 0, 0};
   rho[0] = a.in[((size_t)b * 8 + kRho) * NC + c];
   p[0] = a.in[((size_t)b * 8 + kP) * NC + c];
 #pragma unroll
@@ -296,12 +299,14 @@ __global__ void __launch_bounds__(N * N * N) k_amr_crit(AmrCritArgs a) {
           const RcSlab S = a.slabs[a.rcSlab[6 * b + s]];
           rho[m] = rc_ghost_value<N>(a.in, S, a.lc, nr, x3, kRho, false);
           p[m] = rc_ghost_value<N>(a.in, S, a.lc, nr, x3, kP, false);
+          if (needDivU) ru[m] = rc_ghost_value<N>(a.in, S, a.lc, nr, x3, kUx + d, false);  // rhoU_d
           continue;
         }
       }
       const int cc = x3[0] + N * (x3[1] + N * x3[2]);
       rho[m] = a.in[((size_t)blk * 8 + kRho) * NC + cc];
       p[m] = a.in[((size_t)blk * 8 + kP) * NC + cc];
+      if (needDivU) ru[m] = a.in[((size_t)blk * 8 + kUx + d) * NC + cc];  // rhoU_d
     }
   const double vInvHalf = 0.5 / g.volume;
   for (int q = 0; q < a.nCrit; q++) {
@@ -315,6 +320,19 @@ __global__ void __launch_bounds__(N * N * N) k_amr_crit(AmrCritArgs a) {
         const double mn = fmin(fmin(p[1 + 2 * d], p[0]), p[2 + 2 * d]);
         val = fmax(val, __ddiv_rn(mx, mn));
       }
+    } else if (type == kAmrMinusDivU) {
+      // '-divu' (src/ModAMR.f90:476-497): u = rhoU / rho in every cell,
+      // the central-difference divergence of calc_divergence on a Cartesian
+      // block (src/ModCellGradient.f90:72-83), and the block's -min(div u)
+      // as the maximum of -div u
+      double div = 0.0;
+#pragma unroll
+      for (int d = 0; d < 3; d++) {
+        const double up = __ddiv_rn(ru[2 + 2 * d], rho[2 + 2 * d]), um = __ddiv_rn(ru[1 + 2 * d], rho[1 + 2 * d]);
+        const double t = __dmul_rn(g.invHalf[d], __dsub_rn(up, um));
+        div = d == 0 ? t : __dadd_rn(div, t);
+      }
+      val = -div;
     } else {
       double f[7];
 #pragma unroll
@@ -341,7 +359,7 @@ __global__ void __launch_bounds__(N * N * N) k_amr_crit(AmrCritArgs a) {
       if (c == 0) {
         double m = red[0];
         for (int w = 1; w < NC / 32; w++) m = fmax(m, red[w]);
-        a.crit[(size_t)b * a.nCrit + q] = type == kAmrPJumpRatio ? m : __dsqrt_rn(m);
+        a.crit[(size_t)b * a.nCrit + q] = type == kAmrPJumpRatio || type == kAmrMinusDivU ? m : __dsqrt_rn(m);
       }
     }
   }

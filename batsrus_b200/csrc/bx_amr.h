@@ -24,7 +24,8 @@ struct RcSlab {
 };
 
 // dynamic AMR criteria (amr_criteria, src/ModAMR.f90:388-723)
-constexpr int kAmrGradT = 1, kAmrGradLogRho = 2, kAmrGradLogP = 3, kAmrGradP = 4, kAmrPJumpRatio = 5;
+constexpr int kAmrGradT = 1, kAmrGradLogRho = 2, kAmrGradLogP = 3, kAmrGradP = 4, kAmrPJumpRatio = 5,
+              kAmrMinusDivU = 6;
 
 struct AmrCritArgs {
   const double *in;  // U^n [block][var][cell]

@@ -1228,7 +1228,7 @@ int bx_amr_criteria(int nCrit, const int *iTypeCrit_I, double *Crit_IB) {
   a.nRoot = make_int3(g.nRoot[0], g.nRoot[1], g.nRoot[2]);
   a.nCrit = nCrit;
   for (int q = 0; q < nCrit; q++) {
-    if (iTypeCrit_I[q] < BX_AMR_GRADT || iTypeCrit_I[q] > BX_AMR_PJUMPRATIO)
+    if (iTypeCrit_I[q] < BX_AMR_GRADT || iTypeCrit_I[q] > BX_AMR_MINUSDIVU)
       return fail(BX_ERR_ARG, "criterion %d: type %d", q + 1, iTypeCrit_I[q]);
     a.type[q] = iTypeCrit_I[q];
   }

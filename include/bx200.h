@@ -195,7 +195,11 @@ BX_API int bx_synchronize(void);
 
 /* ---- dynamic AMR (src/ModAMR.f90) ---------------------------------------- */
 /* #AMRCRITERIA TypeRefine values (PARAM.XML:6814-6843) that are built */
-enum { BX_AMR_GRADT = 1, BX_AMR_GRADLOGRHO = 2, BX_AMR_GRADLOGP = 3, BX_AMR_GRADP = 4, BX_AMR_PJUMPRATIO = 5 };
+enum { BX_AMR_GRADT = 1, BX_AMR_GRADLOGRHO = 2, BX_AMR_GRADLOGP = 3, BX_AMR_GRADP = 4, BX_AMR_PJUMPRATIO = 5,
+       /* '-divu' (src/ModAMR.f90:476-497); '-divudx' computes the same
+          there (the scaling by the cell diagonal is tested against the name
+          'divudx', which the case selector never passes) */
+       BX_AMR_MINUSDIVU = 6 };
 /* prepare_amr -> amr_criteria (src/ModAMR.f90:171-229, 388-723) on the
  * current state: Crit_IB(nCrit, nBlock), the maximum over each block's cells
  * of criteria iTypeCrit_I(1:nCrit) (nCrit <= 3), in normalised units. The

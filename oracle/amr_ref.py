@@ -4,7 +4,10 @@ imports it).
 
 * ``criteria``: amr_criteria (src/ModAMR.f90:388-723) for gradt,
   gradlogrho, gradlogp, gradp (calc_gradient3 on Cartesian blocks,
-  src/ModCellGradient.f90:345-380) and pjumpratio (src/ModAMR.f90:483-495),
+  src/ModCellGradient.f90:345-380), pjumpratio (src/ModAMR.f90:483-495) and
+  -divu / -divudx (src/ModAMR.f90:476-497 with calc_divergence,
+  src/ModCellGradient.f90:72-83; the reference scales by the cell diagonal
+  only for a name 'divudx' that its case selector never passes),
   from a State_VGB whose ghost cells the oracle's exchange_messages filled.
   The operations and their order are those of the GPU kernel, so the values
   agree bit for bit except where log10 differs in the last place.
@@ -41,7 +44,7 @@ def criteria(State_VGB, grid, names):
     (nBlock, nKg, nJg, nIg, 8)"""
     S = np.asarray(State_VGB, dtype=np.float64)
     rho, p = S[..., 0], S[..., 7]
-    _, vol, area = block_geometry(grid)
+    cs, vol, area = block_geometry(grid)
     vInvHalf = 0.5 / vol
     g = NG
     inner = (slice(None), slice(g, -g), slice(g, -g), slice(g, -g))
@@ -56,13 +59,21 @@ def criteria(State_VGB, grid, names):
     out = np.empty((grid.nBlock, len(names)))
     # (edge and corner ghost cells, which no criterion reads, may be zero)
     with np.errstate(divide="ignore", invalid="ignore"):
-        _criteria(out, names, rho, p, area, vInvHalf, shifted, inner, grid)
+        _criteria(out, names, rho, p, area, vInvHalf, shifted, inner, grid, S, 0.5 / cs)
     return out
 
 
-def _criteria(out, names, rho, p, area, vInvHalf, shifted, inner, grid):
+def _criteria(out, names, rho, p, area, vInvHalf, shifted, inner, grid, S, invHalf):
     for q, name in enumerate(names):
         name = name.lower()
+        if name in ("-divu", "-divudx"):
+            div = None
+            for d in range(3):
+                u = S[..., 1 + d] / rho
+                t = invHalf[:, d][:, None, None, None] * (shifted(u, d, 1) - shifted(u, d, -1))
+                div = t if div is None else div + t
+            out[:, q] = (-div).reshape(grid.nBlock, -1).max(axis=1)
+            continue
         if name == "pjumpratio":
             val = np.zeros(p[inner].shape)
             for d in range(3):

@@ -21,7 +21,7 @@ from oracle import Oracle
 
 pytestmark = pytest.mark.gpu
 
-NAMES = ["gradt", "gradlogrho", "gradlogp", "gradp", "pjumpratio"]
+NAMES = ["gradt", "gradlogrho", "gradlogp", "gradp", "pjumpratio", "-divu"]
 
 
 def rel_err(a, b):

@@ -237,3 +237,23 @@ def test_native_plan_without_requests_keeps_or_reorders_the_grid(order):
         assert (b[1][:, 0] == amr.COPY).all() and np.array_equal(b[1][:, 1], np.arange(1, g.nBlock + 1))
     else:
         assert b[2]
+
+
+def test_minus_divu_criterion_is_exact_for_a_linear_velocity():
+    """'-divu' (src/ModAMR.f90:476-497) of the CPU restatement: the central
+    differences of calc_divergence are exact for a linear velocity field, so
+    every block of a two-level grid gets -div u = -(a + b + c), with the
+    ghost cells holding the same field; a uniform flow gives 0."""
+    from amr_ref import criteria
+    g = configs.amr_blast(nRoot=2, maxLevel=1, with_state=False)[0]
+    xyz = g.cell_centers(with_ghost=True)
+    S = np.zeros(xyz.shape[:-1] + (8,))
+    S[..., 0] = 2.0
+    S[..., 7] = 1.0
+    coef = (0.5, -1.5, 2.0)
+    for d in range(3):
+        S[..., 1 + d] = S[..., 0] * coef[d] * xyz[..., d]
+    c = criteria(S, g, ["-divu", "-divudx"])
+    assert np.allclose(c, -sum(coef), rtol=0, atol=1e-12)
+    S[..., 1:4] = 0.3
+    assert np.abs(criteria(S, g, ["-divu"])).max() == 0.0
